@@ -1,0 +1,253 @@
+"""Test oracle for the greedy-fluid / LDMM inner loop.
+
+TEST INFRASTRUCTURE. Only ``tests/``, ``__graft_entry__.smoke()`` and
+``bench.py``'s CPU-baseline leg import this package; the product package
+``atlaswerks_b200`` never does.
+
+Two libraries are wrapped, both taking planar float32 numpy arrays:
+
+* ``Oracle`` — ``oracle/liboracle.so``, the C restatement of the reference
+  CPU routines (``oracle/aw_oracle.c``), with the fluid operator in FP64.
+* ``Reference`` — ``oracle/_ref/libawref.so``, the reference's own CPU code
+  (``GreedyIteratorCPU``, ``HField3DUtils``, ``DiffOperT``) compiled from its
+  sources by ``oracle/ref/Makefile``. It pins the oracle; it exists where the
+  reference tree was present at build time (its ``.so`` travels with the
+  repository snapshot).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libawref.so")
+
+# HField3DUtils::VectorBackgroundStrategy (UtilitiesDataTypes/HField3DUtils.h:44-49)
+BG_PARTIAL_ID, BG_ID, BG_PARTIAL_ZERO, BG_ZERO, BG_CLAMP, BG_WRAP = range(6)
+
+_f = ctypes.POINTER(ctypes.c_float)
+_d = ctypes.POINTER(ctypes.c_double)
+_i = ctypes.c_int
+_dbl = ctypes.c_double
+
+
+def _fp(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_f)
+
+
+def _dp(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_d)
+
+
+def build_oracle() -> None:
+    """Compile liboracle.so (gcc only; no reference tree needed)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def build_reference(ref_root: str = "/root/reference") -> bool:
+    """Compile the reference CPU path into _ref/libawref.so when the
+    reference tree is present. Returns True when the library exists."""
+    if os.path.isdir(ref_root):
+        subprocess.run(["make", "-s", "-j8", "-C", os.path.join(HERE, "ref"), f"REF={ref_root}"],
+                       check=True)
+    return os.path.exists(REF_SO)
+
+
+def _shape(a: np.ndarray):
+    nz, ny, nx = a.shape[-3:]
+    return nx, ny, nz
+
+
+def identity(shape) -> np.ndarray:
+    """Identity h-field, planar [3, nz, ny, nx] (x, y, z components)."""
+    nz, ny, nx = shape
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    return np.stack([x, y, z]).astype(np.float32)
+
+
+class Oracle:
+    """ctypes wrapper of liboracle.so (arrays are [nz, ny, nx], fields [3, nz, ny, nx])."""
+
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            build_oracle()
+        self.lib = ctypes.CDLL(path)
+        L = self.lib
+        L.aw_oracle_greedy_iterate.restype = ctypes.c_double
+        L.aw_oracle_max_norm.restype = ctypes.c_float
+
+    # --- interpolation family -------------------------------------------------
+    def apply(self, img, h, bg=0.0):
+        out = np.empty_like(img)
+        self.lib.aw_oracle_apply(_fp(img), _fp(h[0]), _fp(h[1]), _fp(h[2]), _fp(out),
+                                 *_shape(img), ctypes.c_float(bg))
+        return out
+
+    def apply_u(self, img, v, sp=(1.0, 1.0, 1.0), bg=0.0):
+        out = np.empty_like(img)
+        self.lib.aw_oracle_apply_u(_fp(img), _fp(v[0]), _fp(v[1]), _fp(v[2]), _fp(out),
+                                   *_shape(img), *map(_dbl, sp), ctypes.c_float(bg))
+        return out
+
+    def gradient(self, img, sp=(1.0, 1.0, 1.0), wrap=False):
+        g = np.zeros((3,) + img.shape, np.float32)
+        self.lib.aw_oracle_gradient(_fp(img), _fp(g[0]), _fp(g[1]), _fp(g[2]), *_shape(img),
+                                    *map(_dbl, sp), _i(int(wrap)))
+        return g
+
+    def compose_hv(self, g, v, sp=(1.0, 1.0, 1.0), direction=1, bg=BG_PARTIAL_ID):
+        o = np.empty_like(g)
+        self.lib.aw_oracle_compose_hv(_fp(g[0]), _fp(g[1]), _fp(g[2]), _fp(v[0]), _fp(v[1]),
+                                      _fp(v[2]), _fp(o[0]), _fp(o[1]), _fp(o[2]), *_shape(g),
+                                      *map(_dbl, sp), _i(direction), _i(bg))
+        return o
+
+    def compose_vh(self, v, g, sp=(1.0, 1.0, 1.0), direction=-1, bg=BG_PARTIAL_ZERO):
+        o = np.empty_like(g)
+        self.lib.aw_oracle_compose_vh(_fp(v[0]), _fp(v[1]), _fp(v[2]), _fp(g[0]), _fp(g[1]),
+                                      _fp(g[2]), _fp(o[0]), _fp(o[1]), _fp(o[2]), *_shape(g),
+                                      *map(_dbl, sp), _i(direction), _i(bg))
+        return o
+
+    def splat(self, img, h, bg=0.0):
+        out = np.empty_like(img)
+        self.lib.aw_oracle_splat(_fp(img), _fp(h[0]), _fp(h[1]), _fp(h[2]), _fp(out),
+                                 *_shape(img), ctypes.c_float(bg))
+        return out
+
+    # --- fluid operator ---------------------------------------------------------
+    def fluid(self, v, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01, gamma=0.001, inverse=True):
+        """L^-1 v (inverse) or L v in FP64; float32 in -> float32 out."""
+        o = np.ascontiguousarray(v, dtype=np.float32).copy()
+        self.lib.aw_oracle_fluid_apply(_fp(o[0]), _fp(o[1]), _fp(o[2]), *_shape(o),
+                                       *map(_dbl, sp), _dbl(alpha), _dbl(beta), _dbl(gamma),
+                                       _i(int(inverse)))
+        return o
+
+    def fluid_f64(self, v, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01, gamma=0.001, inverse=True):
+        o = np.ascontiguousarray(v, dtype=np.float64).copy()
+        self.lib.aw_oracle_fluid_apply_f64(_dp(o[0]), _dp(o[1]), _dp(o[2]), *_shape(o),
+                                           *map(_dbl, sp), _dbl(alpha), _dbl(beta), _dbl(gamma),
+                                           _i(int(inverse)))
+        return o
+
+    def max_norm(self, v):
+        return float(self.lib.aw_oracle_max_norm(_fp(v[0]), _fp(v[1]), _fp(v[2]),
+                                                 ctypes.c_long(v[0].size)))
+
+    # --- greedy iteration -------------------------------------------------------
+    def greedy_iterate(self, I0, I1, h, hinv=None, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01,
+                       gamma=0.001, max_pert=0.5, update_step=False, step=0.0):
+        """One GreedyIteratorCPU::Iterate; h/hinv updated in place.
+        Returns (energy, step)."""
+        st = ctypes.c_float(step)
+        hi = hinv if hinv is not None else [None, None, None]
+        e = self.lib.aw_oracle_greedy_iterate(
+            _fp(I0), _fp(I1), _fp(h[0]), _fp(h[1]), _fp(h[2]), _fp(hi[0]), _fp(hi[1]),
+            _fp(hi[2]), *_shape(I0), *map(_dbl, sp), _dbl(alpha), _dbl(beta), _dbl(gamma),
+            ctypes.c_float(max_pert), _i(int(update_step)), ctypes.byref(st))
+        return float(e), float(st.value)
+
+    def greedy_run(self, I0, I1, iters, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01, gamma=0.001,
+                   max_pert=0.5, inverse=False):
+        """Single-scale greedy registration from the identity."""
+        h = identity(I0.shape)
+        hinv = identity(I0.shape) if inverse else None
+        energies, step = [], 0.0
+        for it in range(iters):
+            e, step = self.greedy_iterate(I0, I1, h, hinv, sp, alpha, beta, gamma, max_pert,
+                                          update_step=(it == 0), step=step)
+            energies.append(e)
+        return h, hinv, np.array(energies), step
+
+
+class Reference:
+    """ctypes wrapper of the reference's own CPU code (oracle/_ref/libawref.so)."""
+
+    def __init__(self, path: str = REF_SO):
+        self.lib = ctypes.CDLL(path)
+        self.lib.awref_last_error.restype = ctypes.c_char_p
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError(self.lib.awref_last_error().decode())
+
+    def apply(self, img, h):
+        out = np.empty_like(img)
+        self._check(self.lib.awref_apply(_fp(img), _fp(h[0]), _fp(h[1]), _fp(h[2]), _fp(out),
+                                         *_shape(img)))
+        return out
+
+    def gradient(self, img, sp=(1.0, 1.0, 1.0), wrap=False):
+        g = np.zeros((3,) + img.shape, np.float32)
+        self._check(self.lib.awref_gradient(_fp(img), _fp(g[0]), _fp(g[1]), _fp(g[2]),
+                                            *_shape(img), *map(_dbl, sp), _i(int(wrap))))
+        return g
+
+    def compose_hv(self, g, v, sp=(1.0, 1.0, 1.0), direction=1, bg=BG_PARTIAL_ID):
+        o = np.empty_like(g)
+        self._check(self.lib.awref_compose_hv(_fp(g[0]), _fp(g[1]), _fp(g[2]), _fp(v[0]),
+                                              _fp(v[1]), _fp(v[2]), _fp(o[0]), _fp(o[1]),
+                                              _fp(o[2]), *_shape(g), *map(_dbl, sp),
+                                              _i(direction), _i(bg)))
+        return o
+
+    def compose_vh(self, v, g, sp=(1.0, 1.0, 1.0), direction=-1, bg=BG_PARTIAL_ZERO):
+        o = np.empty_like(g)
+        self._check(self.lib.awref_compose_vh(_fp(v[0]), _fp(v[1]), _fp(v[2]), _fp(g[0]),
+                                              _fp(g[1]), _fp(g[2]), _fp(o[0]), _fp(o[1]),
+                                              _fp(o[2]), *_shape(g), *map(_dbl, sp),
+                                              _i(direction), _i(bg)))
+        return o
+
+    def splat(self, img, h):
+        out = np.empty_like(img)
+        self._check(self.lib.awref_splat(_fp(img), _fp(h[0]), _fp(h[1]), _fp(h[2]), _fp(out),
+                                         *_shape(img)))
+        return out
+
+    def fluid(self, v, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01, gamma=0.001, inverse=True):
+        o = np.ascontiguousarray(v, dtype=np.float32).copy()
+        self._check(self.lib.awref_fluid(_fp(o[0]), _fp(o[1]), _fp(o[2]), *_shape(o),
+                                         *map(_dbl, sp), _dbl(alpha), _dbl(beta), _dbl(gamma),
+                                         _i(int(inverse))))
+        return o
+
+    def fluid_f64(self, v, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01, gamma=0.001, inverse=True):
+        o = np.ascontiguousarray(v, dtype=np.float64).copy()
+        self._check(self.lib.awref_fluid_f64(_dp(o[0]), _dp(o[1]), _dp(o[2]), *_shape(o),
+                                             *map(_dbl, sp), _dbl(alpha), _dbl(beta),
+                                             _dbl(gamma), _i(int(inverse))))
+        return o
+
+    def greedy_run(self, I0, I1, factors: Sequence[int], iters: Sequence[int],
+                   max_pert: Sequence[float], sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01,
+                   gamma=0.001, inverse=False, h_init=None, hinv_init=None, init_step=0.0,
+                   skip_step_update=False):
+        """GreedyIteratorCPU driven through the GreedyWarp::RunWarp scale loop."""
+        ns = len(factors)
+        fa = (ctypes.c_int * ns)(*factors)
+        it = (ctypes.c_int * ns)(*iters)
+        mp = (ctypes.c_float * ns)(*max_pert)
+        h = np.empty((3,) + I0.shape, np.float32)
+        hinv = np.empty((3,) + I0.shape, np.float32) if inverse else None
+        total = int(sum(iters))
+        en = np.zeros(total, np.float64)
+        steps = np.zeros(total, np.float32)
+        hi = np.ascontiguousarray(h_init, np.float32) if h_init is not None else None
+        hii = np.ascontiguousarray(hinv_init, np.float32) if hinv_init is not None else None
+        self._check(self.lib.awref_greedy_run(
+            _fp(I0), _fp(I1), *_shape(I0), *map(_dbl, sp), _i(ns), fa, it, mp, _dbl(alpha),
+            _dbl(beta), _dbl(gamma), _i(int(inverse)), _fp(hi), _fp(hii),
+            ctypes.c_float(init_step), _i(int(skip_step_update)), _fp(h), _fp(hinv), _dp(en),
+            _fp(steps)))
+        return h, hinv, en, steps

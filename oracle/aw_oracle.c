@@ -1,0 +1,493 @@
+/*
+ * aw_oracle.c — CPU restatement of the AtlasWerks greedy-fluid / LDMM inner
+ * loop, used as the parity checker for the CUDA path.
+ *
+ * TEST INFRASTRUCTURE. Only tests/, __graft_entry__.smoke() and bench.py's
+ * cpu_baseline leg may load this library. The product (atlaswerks_b200/)
+ * never links or calls it.
+ *
+ * Every routine follows a reference CPU routine statement by statement and
+ * reproduces its floating-point types: float data, double interpolation
+ * weights, float position arithmetic. Build with -ffp-contract=off so that no
+ * fused multiply-add changes a rounding. The fluid operator is evaluated in
+ * FP64 end to end (the "FP64 oracle"): the reference applies it in FP32 with
+ * FFTW, which is not available here.
+ *
+ * Vector fields are planar (three float planes x|y|z, each nx*ny*nz, x
+ * fastest) — the same values the reference holds as Array3D<Vector3D<float>>.
+ */
+#include "aw_oracle.h"
+
+#include <math.h>
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+#include <stdlib.h>
+#include <string.h>
+
+#include "fft64.h"
+
+#define IDX(x, y, z) (((long)(z) * ny + (y)) * nx + (x))
+
+/* ------------------------------------------------------------------------
+ * Scalar trilinear interpolation, background value per corner.
+ * Follows Array3DUtils::trilerp<T, BACKGROUND_STRATEGY_VAL>
+ * (UtilitiesDataTypes/Array3DUtils.txx:59-232): positions and weights in
+ * double, result rounded to float.
+ * ---------------------------------------------------------------------- */
+static float trilerp_val(const float *a, int nx, int ny, int nz, double x, double y, double z,
+                         float bg) {
+  int fx = (int)x, fy = (int)y, fz = (int)z;
+  if (x < 0 && x != (int)x) --fx;
+  if (y < 0 && y != (int)y) --fy;
+  if (z < 0 && z != (int)z) --fz;
+  const int cx = fx + 1, cy = fy + 1, cz = fz + 1;
+  const double t = x - fx, u = y - fy, v = z - fz;
+  const double omt = 1.0 - t, omu = 1.0 - u, omv = 1.0 - v;
+  float v0, v1, v2, v3, v4, v5, v6, v7;
+  const int inside = fx >= 0 && cx < nx && fy >= 0 && cy < ny && fz >= 0 && cz < nz;
+  if (inside) {
+    v0 = a[IDX(fx, fy, fz)];
+    v1 = a[IDX(cx, fy, fz)];
+    v2 = a[IDX(cx, cy, fz)];
+    v3 = a[IDX(fx, cy, fz)];
+    v4 = a[IDX(fx, cy, cz)];
+    v5 = a[IDX(cx, cy, cz)];
+    v6 = a[IDX(cx, fy, cz)];
+    v7 = a[IDX(fx, fy, cz)];
+  } else {
+    const int fxi = fx >= 0 && fx < nx, fyi = fy >= 0 && fy < ny, fzi = fz >= 0 && fz < nz;
+    const int cxi = cx >= 0 && cx < nx, cyi = cy >= 0 && cy < ny, czi = cz >= 0 && cz < nz;
+    v0 = (fxi && fyi && fzi) ? a[IDX(fx, fy, fz)] : bg;
+    v1 = (cxi && fyi && fzi) ? a[IDX(cx, fy, fz)] : bg;
+    v2 = (cxi && cyi && fzi) ? a[IDX(cx, cy, fz)] : bg;
+    v3 = (fxi && cyi && fzi) ? a[IDX(fx, cy, fz)] : bg;
+    v4 = (fxi && cyi && czi) ? a[IDX(fx, cy, cz)] : bg;
+    v5 = (cxi && cyi && czi) ? a[IDX(cx, cy, cz)] : bg;
+    v6 = (cxi && fyi && czi) ? a[IDX(cx, fy, cz)] : bg;
+    v7 = (fxi && fyi && czi) ? a[IDX(fx, fy, cz)] : bg;
+  }
+  return (float)(omt * (omu * (v0 * omv + v7 * v) + u * (v3 * omv + v4 * v)) +
+                 t * (omu * (v1 * omv + v6 * v) + u * (v2 * omv + v5 * v)));
+}
+
+/* ------------------------------------------------------------------------
+ * Vector trilinear interpolation with the reference's background strategies.
+ * Follows HField3DUtils::trilerp (UtilitiesDataTypes/HField3DUtils.txx:
+ * 1972-2300). The position is float; the fractional part is formed in float
+ * (float - int), widened to double, and the corner sums run in double.
+ * ---------------------------------------------------------------------- */
+static int safe_mod(int r, int m) {
+  r %= m;
+  if (r < 0) r += m;
+  return r;
+}
+
+static void trilerp_vec(const float *hxp, const float *hyp, const float *hzp, int nx, int ny,
+                        int nz, float x, float y, float z, float *ox, float *oy, float *oz,
+                        int bgs) {
+  int fx = (int)x, fy = (int)y, fz = (int)z;
+  if (x < 0 && x != (float)(int)x) --fx;
+  if (y < 0 && y != (float)(int)y) --fy;
+  if (z < 0 && z != (float)(int)z) --fz;
+  int cx = fx + 1, cy = fy + 1, cz = fz + 1;
+  const double t = (double)(x - (float)fx), u = (double)(y - (float)fy),
+               v = (double)(z - (float)fz);
+  const double omt = 1.0 - t, omu = 1.0 - u, omv = 1.0 - v;
+  float vX[8] = {0}, vY[8] = {0}, vZ[8] = {0};
+  int inside = 1;
+  if (bgs == AW_BG_WRAP) {
+    fx = safe_mod(fx, nx); fy = safe_mod(fy, ny); fz = safe_mod(fz, nz);
+    cx = safe_mod(cx, nx); cy = safe_mod(cy, ny); cz = safe_mod(cz, nz);
+  } else if (bgs == AW_BG_CLAMP) {
+    if (fx < 0) { fx = 0; if (cx < 0) cx = 0; }
+    if (cx >= nx) { cx = nx - 1; if (fx >= nx) fx = nx - 1; }
+    if (fy < 0) { fy = 0; if (cy < 0) cy = 0; }
+    if (cy >= ny) { cy = ny - 1; if (fy >= ny) fy = ny - 1; }
+    if (fz < 0) { fz = 0; if (cz < 0) cz = 0; }
+    if (cz >= nz) { cz = nz - 1; if (fz >= nz) fz = nz - 1; }
+  } else {
+    inside = fx >= 0 && cx < nx && fy >= 0 && cy < ny && fz >= 0 && cz < nz;
+  }
+  /* corner order v0..v7 as in the reference */
+  const int X[8] = {fx, cx, cx, fx, fx, cx, cx, fx};
+  const int Y[8] = {fy, fy, cy, cy, cy, cy, fy, fy};
+  const int Z[8] = {fz, fz, fz, fz, cz, cz, cz, cz};
+  if (inside) {
+    for (int c = 0; c < 8; ++c) {
+      const long i = IDX(X[c], Y[c], Z[c]);
+      vX[c] = hxp[i]; vY[c] = hyp[i]; vZ[c] = hzp[i];
+    }
+  } else if (bgs == AW_BG_ID) {
+    *ox = x; *oy = y; *oz = z;
+    return;
+  } else if (bgs == AW_BG_ZERO) {
+    *ox = 0; *oy = 0; *oz = 0;
+    return;
+  } else { /* PARTIAL_ID / PARTIAL_ZERO */
+    for (int c = 0; c < 8; ++c) {
+      if (bgs == AW_BG_PARTIAL_ID) {
+        vX[c] = (float)X[c]; vY[c] = (float)Y[c]; vZ[c] = (float)Z[c];
+      }
+      const int in = X[c] >= 0 && X[c] < nx && Y[c] >= 0 && Y[c] < ny && Z[c] >= 0 && Z[c] < nz;
+      if (in) {
+        const long i = IDX(X[c], Y[c], Z[c]);
+        vX[c] = hxp[i]; vY[c] = hyp[i]; vZ[c] = hzp[i];
+      }
+    }
+  }
+  /* v0..v7 = index 0..7 */
+  *ox = (float)(omt * (omu * (vX[0] * omv + vX[7] * v) + u * (vX[3] * omv + vX[4] * v)) +
+                t * (omu * (vX[1] * omv + vX[6] * v) + u * (vX[2] * omv + vX[5] * v)));
+  *oy = (float)(omt * (omu * (vY[0] * omv + vY[7] * v) + u * (vY[3] * omv + vY[4] * v)) +
+                t * (omu * (vY[1] * omv + vY[6] * v) + u * (vY[2] * omv + vY[5] * v)));
+  *oz = (float)(omt * (omu * (vZ[0] * omv + vZ[7] * v) + u * (vZ[3] * omv + vZ[4] * v)) +
+                t * (omu * (vZ[1] * omv + vZ[6] * v) + u * (vZ[2] * omv + vZ[5] * v)));
+}
+
+/* I_def(x) = I(h(x)); HField3DUtils::apply (HField3DUtils.txx:734-752). */
+void aw_oracle_apply(const float *img, const float *hx, const float *hy, const float *hz,
+                     float *out, int nx, int ny, int nz, float bg) {
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const long i = IDX(x, y, z);
+        out[i] = trilerp_val(img, nx, ny, nz, (double)hx[i], (double)hy[i], (double)hz[i], bg);
+      }
+}
+
+/* I(x + v(x)/sp): HField3DUtils::applyU (HField3DUtils.txx, used by LDMM
+ * IterateOrig at LDMM/LDMMIteratorCPU.cxx:426). Position in float. */
+void aw_oracle_apply_u(const float *img, const float *vx, const float *vy, const float *vz,
+                       float *out, int nx, int ny, int nz, double spx, double spy, double spz,
+                       float bg) {
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const long i = IDX(x, y, z);
+        const float px = (float)x + vx[i] / (float)spx;
+        const float py = (float)y + vy[i] / (float)spy;
+        const float pz = (float)z + vz[i] / (float)spz;
+        out[i] = trilerp_val(img, nx, ny, nz, (double)px, (double)py, (double)pz, bg);
+      }
+}
+
+/* Array3DUtils::computeGradient (Array3DUtils.txx:783-900). */
+void aw_oracle_gradient(const float *a, float *gx, float *gy, float *gz, int nx, int ny, int nz,
+                        double spx, double spy, double spz, int wrap) {
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 1; x < nx - 1; ++x)
+        gx[IDX(x, y, z)] = (float)((double)(a[IDX(x + 1, y, z)] - a[IDX(x - 1, y, z)]) / (2.0 * spx));
+  for (int z = 0; z < nz; ++z)
+    for (int y = 1; y < ny - 1; ++y)
+      for (int x = 0; x < nx; ++x)
+        gy[IDX(x, y, z)] = (float)((double)(a[IDX(x, y + 1, z)] - a[IDX(x, y - 1, z)]) / (2.0 * spy));
+  for (int z = 1; z < nz - 1; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x)
+        gz[IDX(x, y, z)] = (float)((double)(a[IDX(x, y, z + 1)] - a[IDX(x, y, z - 1)]) / (2.0 * spz));
+  if (wrap) {
+    for (int z = 0; z < nz; ++z)
+      for (int y = 0; y < ny; ++y) {
+        gx[IDX(0, y, z)] = (float)((double)(a[IDX(1, y, z)] - a[IDX(nx - 1, y, z)]) / (2.0 * spx));
+        gx[IDX(nx - 1, y, z)] = (float)((double)(a[IDX(0, y, z)] - a[IDX(nx - 2, y, z)]) / (2.0 * spx));
+      }
+    for (int z = 0; z < nz; ++z)
+      for (int x = 0; x < nx; ++x) {
+        gy[IDX(x, 0, z)] = (float)((double)(a[IDX(x, 1, z)] - a[IDX(x, ny - 1, z)]) / (2.0 * spy));
+        gy[IDX(x, ny - 1, z)] = (float)((double)(a[IDX(x, 0, z)] - a[IDX(x, ny - 2, z)]) / (2.0 * spy));
+      }
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        gz[IDX(x, y, 0)] = (float)((double)(a[IDX(x, y, 1)] - a[IDX(x, y, nz - 1)]) / (2.0 * spz));
+        gz[IDX(x, y, nz - 1)] = (float)((double)(a[IDX(x, y, 0)] - a[IDX(x, y, nz - 2)]) / (2.0 * spz));
+      }
+  } else {
+    for (int z = 0; z < nz; ++z)
+      for (int y = 0; y < ny; ++y) {
+        gx[IDX(0, y, z)] = (float)((double)(a[IDX(1, y, z)] - a[IDX(0, y, z)]) / spx);
+        gx[IDX(nx - 1, y, z)] = (float)((double)(a[IDX(nx - 1, y, z)] - a[IDX(nx - 2, y, z)]) / spx);
+      }
+    for (int z = 0; z < nz; ++z)
+      for (int x = 0; x < nx; ++x) {
+        gy[IDX(x, 0, z)] = (float)((double)(a[IDX(x, 1, z)] - a[IDX(x, 0, z)]) / spy);
+        gy[IDX(x, ny - 1, z)] = (float)((double)(a[IDX(x, ny - 1, z)] - a[IDX(x, ny - 2, z)]) / spy);
+      }
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        gz[IDX(x, y, 0)] = (float)((double)(a[IDX(x, y, 1)] - a[IDX(x, y, 0)]) / spz);
+        gz[IDX(x, y, nz - 1)] = (float)((double)(a[IDX(x, y, nz - 1)] - a[IDX(x, y, nz - 2)]) / spz);
+      }
+  }
+}
+
+/* h(x) = g(x + dir * v(x)/sp): composeHV (dir=+1, HField3DUtils.txx:436-455)
+ * and composeHVInv (dir=-1, HField3DUtils.txx:461-480). */
+void aw_oracle_compose_hv(const float *gx, const float *gy, const float *gz, const float *vx,
+                          const float *vy, const float *vz, float *ox, float *oy, float *oz,
+                          int nx, int ny, int nz, double spx, double spy, double spz, int dir,
+                          int bgs) {
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const long i = IDX(x, y, z);
+        float px, py, pz;
+        if (dir > 0) {
+          px = (float)x + vx[i] / (float)spx;
+          py = (float)y + vy[i] / (float)spy;
+          pz = (float)z + vz[i] / (float)spz;
+        } else {
+          px = (float)x - vx[i] / (float)spx;
+          py = (float)y - vy[i] / (float)spy;
+          pz = (float)z - vz[i] / (float)spz;
+        }
+        trilerp_vec(gx, gy, gz, nx, ny, nz, px, py, pz, &ox[i], &oy[i], &oz[i], bgs);
+      }
+}
+
+/* h(x) = g(x) + dir * v(g(x))/sp: composeVH (dir=+1) and composeVHInv
+ * (dir=-1, HField3DUtils.txx:405-430). The interpolated value is rounded to
+ * float, divided by (dir*sp) in float, then g(x) is added in float. */
+void aw_oracle_compose_vh(const float *vx, const float *vy, const float *vz, const float *gx,
+                          const float *gy, const float *gz, float *ox, float *oy, float *oz,
+                          int nx, int ny, int nz, double spx, double spy, double spz, int dir,
+                          int bgs) {
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const long i = IDX(x, y, z);
+        float hx, hy, hz;
+        trilerp_vec(vx, vy, vz, nx, ny, nz, gx[i], gy[i], gz[i], &hx, &hy, &hz, bgs);
+        if (dir > 0) {
+          hx /= (float)spx; hy /= (float)spy; hz /= (float)spz;
+        } else {
+          hx /= -((float)spx); hy /= -((float)spy); hz /= -((float)spz);
+        }
+        ox[i] = hx + gx[i];
+        oy[i] = hy + gy[i];
+        oz[i] = hz + gz[i];
+      }
+}
+
+/* Splat, the adjoint of interpolation: HField3DUtils::forwardApply with
+ * hFieldStart = 0 and normalize = false (HField3DUtils.txx:1058-1279).
+ * Contributions land in source (z,y,x) order, accumulated in float. */
+void aw_oracle_splat(const float *img, const float *hx, const float *hy, const float *hz,
+                     float *out, int nx, int ny, int nz, float bg) {
+  const long n = (long)nx * ny * nz;
+  for (long i = 0; i < n; ++i) out[i] = bg;
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const long i = IDX(x, y, z);
+        const float ix = img[i];
+        const float px = hx[i], py = hy[i], pz = hz[i];
+        int fx = (int)px, fy = (int)py, fz = (int)pz;
+        if (px < 0 && px != (float)(int)px) --fx;
+        if (py < 0 && py != (float)(int)py) --fy;
+        if (pz < 0 && pz != (float)(int)pz) --fz;
+        if (px > -1 && px < (float)nx && py > -1 && py < (float)ny && pz > -1 && pz < (float)nz) {
+          const float rx = px - (float)fx, ry = py - (float)fy, rz = pz - (float)fz;
+          const float w000 = (float)((1.0 - rx) * (1.0 - ry) * (1.0 - rz));
+          const float w001 = (float)((1.0 - rx) * (1.0 - ry) * (rz));
+          const float w010 = (float)((1.0 - rx) * (ry) * (1.0 - rz));
+          const float w011 = (float)((1.0 - rx) * (ry) * (rz));
+          const float w100 = (float)((rx) * (1.0 - ry) * (1.0 - rz));
+          const float w101 = (float)((rx) * (1.0 - ry) * (rz));
+          const float w110 = (float)((rx) * (ry) * (1.0 - rz));
+          const float w111 = (float)((rx) * (ry) * (rz));
+          const int fxi = fx >= 0, cxi = fx < nx - 1, fyi = fy >= 0, cyi = fy < ny - 1,
+                    fzi = fz >= 0, czi = fz < nz - 1;
+          if (fxi && fyi && fzi) out[IDX(fx, fy, fz)] += w000 * ix;
+          if (fxi && fyi && czi) out[IDX(fx, fy, fz + 1)] += w001 * ix;
+          if (fxi && cyi && fzi) out[IDX(fx, fy + 1, fz)] += w010 * ix;
+          if (fxi && cyi && czi) out[IDX(fx, fy + 1, fz + 1)] += w011 * ix;
+          if (cxi && fyi && fzi) out[IDX(fx + 1, fy, fz)] += w100 * ix;
+          if (cxi && fyi && czi) out[IDX(fx + 1, fy, fz + 1)] += w101 * ix;
+          if (cxi && cyi && fzi) out[IDX(fx + 1, fy + 1, fz)] += w110 * ix;
+          if (cxi && cyi && czi) out[IDX(fx + 1, fy + 1, fz + 1)] += w111 * ix;
+        }
+      }
+}
+
+/* ------------------------------------------------------------------------
+ * Fluid operator L = -alpha*Lap - beta*grad(div) + gamma and its inverse,
+ * evaluated per wavenumber exactly as DiffOperT::ApplyInverseOperatorOnTheFly
+ * / ApplyOperatorOnTheFly (Algorithms/Common/DiffOper.cxx:755-905) with the
+ * LUT of DiffOper.cxx:590-639 and the Cholesky solve of DiffOper.cxx:
+ * 1005-1083, all in double. The forward transform covers the full complex
+ * spectrum of the real input; the result is its real part (equal to FFTW's
+ * r2c -> solve -> c2r on the non-redundant half).
+ * ---------------------------------------------------------------------- */
+static void lut_axis(int n, double sp, double *cw, double *sw) {
+  const double s = 2.0 * M_PI / n;
+  for (int k = 0; k < n; ++k) {
+    cw[k] = (2.0 * cos(s * (double)k) - 2.0) / (sp * sp);
+    sw[k] = sin(s * (double)k) / sp;
+  }
+}
+
+void aw_oracle_fluid_apply_f64(double *vx, double *vy, double *vz, int nx, int ny, int nz,
+                               double spx, double spy, double spz, double alpha, double beta,
+                               double gamma, int inverse) {
+  const long n = (long)nx * ny * nz;
+  fft64_cplx *F[3];
+  double *V[3] = {vx, vy, vz};
+  for (int c = 0; c < 3; ++c) {
+    F[c] = (fft64_cplx *)malloc(sizeof(fft64_cplx) * (size_t)n);
+    for (long i = 0; i < n; ++i) {
+      F[c][i].re = V[c][i] / (double)n;
+      F[c][i].im = 0.0;
+    }
+    fft64_3d(F[c], nx, ny, nz, -1);
+  }
+  double *cwx = (double *)malloc(sizeof(double) * (size_t)(2 * (nx + ny + nz)));
+  double *swx = cwx + nx, *cwy = swx + nx, *swy = cwy + ny, *cwz = swy + ny, *swz = cwz + nz;
+  lut_axis(nx, spx, cwx, swx);
+  lut_axis(ny, spy, cwy, swy);
+  lut_axis(nz, spz, cwz, swz);
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const long i = IDX(x, y, z);
+        const double lambda = -alpha * (cwx[x] + cwy[y] + cwz[z]) + gamma;
+        const double L00 = lambda - beta * cwx[x];
+        const double L11 = lambda - beta * cwy[y];
+        const double L22 = lambda - beta * cwz[z];
+        const double L10 = beta * swx[x] * swy[y];
+        const double L20 = beta * swx[x] * swz[z];
+        const double L21 = beta * swy[y] * swz[z];
+        double b[2][3] = {{F[0][i].re, F[1][i].re, F[2][i].re},
+                          {F[0][i].im, F[1][i].im, F[2][i].im}};
+        double o[2][3];
+        if (inverse) {
+          const double G00 = sqrt(L00);
+          const double G10 = L10 / G00;
+          const double G20 = L20 / G00;
+          double G11 = L11 - G10 * G10;
+          double G21 = L21 - G20 * G10;
+          G11 = sqrt(G11);
+          G21 = G21 / G11;
+          double G22 = L22 - (G20 * G20 + G21 * G21);
+          G22 = sqrt(G22);
+          for (int p = 0; p < 2; ++p) {
+            const double y0 = b[p][0] / G00;
+            const double y1 = (b[p][1] - G10 * y0) / G11;
+            const double y2 = (b[p][2] - G20 * y0 - G21 * y1) / G22;
+            o[p][2] = y2 / G22;
+            o[p][1] = (y1 - G21 * o[p][2]) / G11;
+            o[p][0] = (y0 - G10 * o[p][1] - G20 * o[p][2]) / G00;
+          }
+        } else {
+          for (int p = 0; p < 2; ++p) {
+            o[p][0] = L00 * b[p][0] + L10 * b[p][1] + L20 * b[p][2];
+            o[p][1] = L10 * b[p][0] + L11 * b[p][1] + L21 * b[p][2];
+            o[p][2] = L20 * b[p][0] + L21 * b[p][1] + L22 * b[p][2];
+          }
+        }
+        for (int c = 0; c < 3; ++c) {
+          F[c][i].re = o[0][c];
+          F[c][i].im = o[1][c];
+        }
+      }
+  for (int c = 0; c < 3; ++c) {
+    fft64_3d(F[c], nx, ny, nz, +1);
+    for (long i = 0; i < n; ++i) V[c][i] = F[c][i].re;
+    free(F[c]);
+  }
+  free(cwx);
+}
+
+/* float in/out wrapper: widen, apply in FP64, round back */
+void aw_oracle_fluid_apply(float *vx, float *vy, float *vz, int nx, int ny, int nz, double spx,
+                           double spy, double spz, double alpha, double beta, double gamma,
+                           int inverse) {
+  const long n = (long)nx * ny * nz;
+  double *d = (double *)malloc(sizeof(double) * (size_t)(3 * n));
+  float *V[3] = {vx, vy, vz};
+  for (int c = 0; c < 3; ++c)
+    for (long i = 0; i < n; ++i) d[c * n + i] = V[c][i];
+  aw_oracle_fluid_apply_f64(d, d + n, d + 2 * n, nx, ny, nz, spx, spy, spz, alpha, beta, gamma,
+                            inverse);
+  for (int c = 0; c < 3; ++c)
+    for (long i = 0; i < n; ++i) V[c][i] = (float)d[c * n + i];
+  free(d);
+}
+
+/* max_x |v(x)|, the float norm of Vector3D::normL2 (DataTypes/Vector3D.txx:
+ * 100-103) as used by GreedyIteratorCPU::calcMaxDisplacement
+ * (Greedy/GreedyIteratorCPU.cxx:65-79). */
+float aw_oracle_max_norm(const float *vx, const float *vy, const float *vz, long n) {
+  float m = 0.0f;
+  for (long i = 0; i < n; ++i) {
+    const float l = sqrtf(vx[i] * vx[i] + vy[i] * vy[i] + vz[i] * vz[i]);
+    if (l > m) m = l;
+  }
+  return m;
+}
+
+/* ------------------------------------------------------------------------
+ * One greedy-fluid iteration, GreedyIteratorCPU::Iterate
+ * (Algorithms/Greedy/GreedyIteratorCPU.cxx:99-138) with updateDeformation
+ * (:83-95). h (and hinv when non-NULL) are updated in place. *step is read,
+ * and replaced by maxPert / max|v| when update_step is set. Returns the
+ * energy spacing^3 * sum (I1 - I0(h))^2 of the incoming h, accumulated in
+ * double (the reference accumulates in float).
+ * ---------------------------------------------------------------------- */
+double aw_oracle_greedy_iterate(const float *I0, const float *I1, float *hx, float *hy, float *hz,
+                                float *hix, float *hiy, float *hiz, int nx, int ny, int nz,
+                                double spx, double spy, double spz, double alpha, double beta,
+                                double gamma, float max_pert, int update_step, float *step) {
+  const long n = (long)nx * ny * nz;
+  float *idef = (float *)malloc(sizeof(float) * (size_t)n);
+  float *f = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *o = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *fx = f, *fy = f + n, *fz = f + 2 * n;
+  aw_oracle_apply(I0, hx, hy, hz, idef, nx, ny, nz, 0.0f);
+  aw_oracle_gradient(idef, fx, fy, fz, nx, ny, nz, spx, spy, spz, 0);
+  double e = 0.0;
+  for (long i = 0; i < n; ++i) {
+    float r = idef[i] - I1[i];
+    r = r * -1.0f;
+    fx[i] *= r;
+    fy[i] *= r;
+    fz[i] *= r;
+    e += (double)r * (double)r;
+  }
+  e *= spx * spy * spz;
+  aw_oracle_fluid_apply(fx, fy, fz, nx, ny, nz, spx, spy, spz, alpha, beta, gamma, 1);
+  if (update_step) {
+    const float m = aw_oracle_max_norm(fx, fy, fz, n);
+    *step = max_pert / m;
+  }
+  const float s = *step;
+  for (long i = 0; i < 3 * n; ++i) f[i] *= s;
+  aw_oracle_compose_hv(hx, hy, hz, fx, fy, fz, o, o + n, o + 2 * n, nx, ny, nz, spx, spy, spz, 1,
+                       AW_BG_PARTIAL_ID);
+  memcpy(hx, o, sizeof(float) * (size_t)n);
+  memcpy(hy, o + n, sizeof(float) * (size_t)n);
+  memcpy(hz, o + 2 * n, sizeof(float) * (size_t)n);
+  if (hix) {
+    aw_oracle_compose_vh(fx, fy, fz, hix, hiy, hiz, o, o + n, o + 2 * n, nx, ny, nz, spx, spy,
+                         spz, -1, AW_BG_PARTIAL_ZERO);
+    memcpy(hix, o, sizeof(float) * (size_t)n);
+    memcpy(hiy, o + n, sizeof(float) * (size_t)n);
+    memcpy(hiz, o + 2 * n, sizeof(float) * (size_t)n);
+  }
+  free(idef);
+  free(f);
+  free(o);
+  return e;
+}
+
+void aw_oracle_identity(float *hx, float *hy, float *hz, int nx, int ny, int nz) {
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const long i = IDX(x, y, z);
+        hx[i] = (float)x;
+        hy[i] = (float)y;
+        hz[i] = (float)z;
+      }
+}

@@ -1,0 +1,57 @@
+/*
+ * aw_oracle.h — CPU restatement of the AtlasWerks registration inner loop.
+ *
+ * TEST INFRASTRUCTURE: the checker for the CUDA path. Only tests/,
+ * __graft_entry__.smoke() and bench.py's cpu_baseline leg use it.
+ */
+#ifndef AW_ORACLE_H
+#define AW_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* HField3DUtils::VectorBackgroundStrategy order (UtilitiesDataTypes/HField3DUtils.h:44-49) */
+enum {
+  AW_BG_PARTIAL_ID = 0,
+  AW_BG_ID = 1,
+  AW_BG_PARTIAL_ZERO = 2,
+  AW_BG_ZERO = 3,
+  AW_BG_CLAMP = 4,
+  AW_BG_WRAP = 5
+};
+
+void aw_oracle_identity(float *hx, float *hy, float *hz, int nx, int ny, int nz);
+void aw_oracle_apply(const float *img, const float *hx, const float *hy, const float *hz,
+                     float *out, int nx, int ny, int nz, float bg);
+void aw_oracle_apply_u(const float *img, const float *vx, const float *vy, const float *vz,
+                       float *out, int nx, int ny, int nz, double spx, double spy, double spz,
+                       float bg);
+void aw_oracle_gradient(const float *a, float *gx, float *gy, float *gz, int nx, int ny, int nz,
+                        double spx, double spy, double spz, int wrap);
+void aw_oracle_compose_hv(const float *gx, const float *gy, const float *gz, const float *vx,
+                          const float *vy, const float *vz, float *ox, float *oy, float *oz,
+                          int nx, int ny, int nz, double spx, double spy, double spz, int dir,
+                          int bgs);
+void aw_oracle_compose_vh(const float *vx, const float *vy, const float *vz, const float *gx,
+                          const float *gy, const float *gz, float *ox, float *oy, float *oz,
+                          int nx, int ny, int nz, double spx, double spy, double spz, int dir,
+                          int bgs);
+void aw_oracle_splat(const float *img, const float *hx, const float *hy, const float *hz,
+                     float *out, int nx, int ny, int nz, float bg);
+void aw_oracle_fluid_apply_f64(double *vx, double *vy, double *vz, int nx, int ny, int nz,
+                               double spx, double spy, double spz, double alpha, double beta,
+                               double gamma, int inverse);
+void aw_oracle_fluid_apply(float *vx, float *vy, float *vz, int nx, int ny, int nz, double spx,
+                           double spy, double spz, double alpha, double beta, double gamma,
+                           int inverse);
+float aw_oracle_max_norm(const float *vx, const float *vy, const float *vz, long n);
+double aw_oracle_greedy_iterate(const float *I0, const float *I1, float *hx, float *hy, float *hz,
+                                float *hix, float *hiy, float *hiz, int nx, int ny, int nz,
+                                double spx, double spy, double spz, double alpha, double beta,
+                                double gamma, float max_pert, int update_step, float *step);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,299 @@
+/*
+ * aw_ref_harness.cxx — C entry points over the reference's own CPU code,
+ * compiled from the reference sources (recipe: oracle/ref/Makefile) into
+ * oracle/_ref/libawref.so.
+ *
+ * TEST INFRASTRUCTURE: used to pin the oracle (oracle/aw_oracle.c) against
+ * the reference itself and, in bench.py's reference arm, as the timed CPU
+ * baseline. The harness only converts planar float arrays to the
+ * reference's Array3D<Vector3D<float>> / Image<float> types and calls the
+ * reference routines; the drivers below repeat the steps of
+ * GreedyWarp::RunWarp (Algorithms/Greedy/GreedyWarp.txx:71-125) and
+ * LDMMWarp::RunWarp (Algorithms/LDMM/LDMMWarp.txx:71-130) without their
+ * ITK file output.
+ */
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "DiffOper.h"
+#include "GreedyDeformationData.h"
+#include "GreedyIteratorCPU.h"
+#include "GreedyParam.h"
+#include "HField3DUtils.h"
+#include "LDMMDeformationData.h"
+#include "LDMMIteratorCPU.h"
+#include "LDMMParam.h"
+#include "MultiscaleManager.h"
+#include "tinyxml.h"
+
+namespace {
+
+std::string g_err;
+
+void to_vf(const float *x, const float *y, const float *z, VectorField &vf) {
+  const unsigned n = vf.getNumElements();
+  for (unsigned i = 0; i < n; ++i) {
+    vf(i).x = x[i];
+    vf(i).y = y[i];
+    vf(i).z = z[i];
+  }
+}
+
+void from_vf(const VectorField &vf, float *x, float *y, float *z) {
+  const unsigned n = vf.getNumElements();
+  for (unsigned i = 0; i < n; ++i) {
+    x[i] = vf(i).x;
+    y[i] = vf(i).y;
+    z[i] = vf(i).z;
+  }
+}
+
+void to_im(const float *a, Array3D<float> &im) {
+  std::memcpy(im.getDataPointer(), a, sizeof(float) * im.getNumElements());
+}
+
+void from_im(const Array3D<float> &im, float *a) {
+  std::memcpy(a, im.getDataPointer(), sizeof(float) * im.getNumElements());
+}
+
+HField3DUtils::VectorBackgroundStrategy bg_of(int b) {
+  return static_cast<HField3DUtils::VectorBackgroundStrategy>(b);
+}
+
+std::string diffoper_xml(double alpha, double beta, double gamma) {
+  std::ostringstream s;
+  s.precision(17);
+  s << "<DiffOper><Alpha val=\"" << alpha << "\"/><Beta val=\"" << beta << "\"/><Gamma val=\""
+    << gamma << "\"/><UseEigenLUT val=\"false\"/><DivergenceFree val=\"false\"/>"
+    << "<FFTWNumberOfThreads val=\"1\"/><FFTWMeasure val=\"false\"/></DiffOper>";
+  return s.str();
+}
+
+template <class P>
+void parse_into(P &param, const std::string &xml) {
+  TiXmlDocument doc;
+  doc.Parse(xml.c_str());
+  if (doc.Error()) throw std::runtime_error(std::string("param xml: ") + doc.ErrorDesc());
+  param.Parse(doc.RootElement());
+}
+
+#define GUARD_BEGIN try {
+#define GUARD_END                          \
+  }                                        \
+  catch (const std::exception &e) {        \
+    g_err = e.what();                      \
+    return -1;                             \
+  }                                        \
+  catch (...) {                            \
+    g_err = "unknown exception";           \
+    return -1;                             \
+  }                                        \
+  return 0;
+
+}  // namespace
+
+extern "C" {
+
+const char *awref_last_error() { return g_err.c_str(); }
+
+/* HField3DUtils::apply, default (zero) background */
+int awref_apply(const float *img, const float *hx, const float *hy, const float *hz, float *out,
+                int nx, int ny, int nz) {
+  GUARD_BEGIN
+  Array3D<float> I(nx, ny, nz), O(nx, ny, nz);
+  VectorField h(nx, ny, nz);
+  to_im(img, I);
+  to_vf(hx, hy, hz, h);
+  HField3DUtils::apply(I, h, O);
+  from_im(O, out);
+  GUARD_END
+}
+
+/* Array3DUtils::computeGradient */
+int awref_gradient(const float *img, float *gx, float *gy, float *gz, int nx, int ny, int nz,
+                   double spx, double spy, double spz, int wrap) {
+  GUARD_BEGIN
+  Array3D<float> I(nx, ny, nz);
+  VectorField g(nx, ny, nz);
+  to_im(img, I);
+  Array3DUtils::computeGradient(I, g, Vector3D<double>(spx, spy, spz), wrap != 0);
+  from_vf(g, gx, gy, gz);
+  GUARD_END
+}
+
+/* composeHV (dir=+1) / composeHVInv (dir=-1): h(x) = g(x +- v(x)/sp) */
+int awref_compose_hv(const float *gx, const float *gy, const float *gz, const float *vx,
+                     const float *vy, const float *vz, float *ox, float *oy, float *oz, int nx,
+                     int ny, int nz, double spx, double spy, double spz, int dir, int bgs) {
+  GUARD_BEGIN
+  VectorField g(nx, ny, nz), v(nx, ny, nz), h(nx, ny, nz);
+  to_vf(gx, gy, gz, g);
+  to_vf(vx, vy, vz, v);
+  Vector3D<double> sp(spx, spy, spz);
+  if (dir > 0)
+    HField3DUtils::composeHV(g, v, h, sp, bg_of(bgs));
+  else
+    HField3DUtils::composeHVInv(g, v, h, sp, bg_of(bgs));
+  from_vf(h, ox, oy, oz);
+  GUARD_END
+}
+
+/* composeVH (dir=+1) / composeVHInv (dir=-1): h(x) = g(x) +- v(g(x))/sp */
+int awref_compose_vh(const float *vx, const float *vy, const float *vz, const float *gx,
+                     const float *gy, const float *gz, float *ox, float *oy, float *oz, int nx,
+                     int ny, int nz, double spx, double spy, double spz, int dir, int bgs) {
+  GUARD_BEGIN
+  VectorField g(nx, ny, nz), v(nx, ny, nz), h(nx, ny, nz);
+  to_vf(gx, gy, gz, g);
+  to_vf(vx, vy, vz, v);
+  Vector3D<double> sp(spx, spy, spz);
+  if (dir > 0)
+    HField3DUtils::composeVH(v, g, h, sp, bg_of(bgs));
+  else
+    HField3DUtils::composeVHInv(v, g, h, sp, bg_of(bgs));
+  from_vf(h, ox, oy, oz);
+  GUARD_END
+}
+
+/* HField3DUtils::forwardApply(image, h, out, 0, false): splatting */
+int awref_splat(const float *img, const float *hx, const float *hy, const float *hz, float *out,
+                int nx, int ny, int nz) {
+  GUARD_BEGIN
+  Array3D<float> I(nx, ny, nz), O(nx, ny, nz);
+  VectorField h(nx, ny, nz);
+  to_im(img, I);
+  to_vf(hx, hy, hz, h);
+  HField3DUtils::forwardApply(I, h, O, 0.0f, false);
+  from_im(O, out);
+  GUARD_END
+}
+
+/* DiffOperT<float>: L (inverse=0) or L^-1 (inverse=1), in place */
+int awref_fluid(float *vx, float *vy, float *vz, int nx, int ny, int nz, double spx, double spy,
+                double spz, double alpha, double beta, double gamma, int inverse) {
+  GUARD_BEGIN
+  DiffOperParam param;
+  parse_into(param, diffoper_xml(alpha, beta, gamma));
+  SizeType size(nx, ny, nz);
+  SpacingType sp(spx, spy, spz);
+  DiffOperT<float> op(size, sp, param);
+  VectorField v(nx, ny, nz);
+  to_vf(vx, vy, vz, v);
+  op.CopyIn(v);
+  if (inverse)
+    op.ApplyInverseOperator();
+  else
+    op.ApplyOperator();
+  op.CopyOut(v);
+  from_vf(v, vx, vy, vz);
+  GUARD_END
+}
+
+/* DiffOperT<double>: the same operator in FP64 (DiffOper.cxx:1221) */
+int awref_fluid_f64(double *vx, double *vy, double *vz, int nx, int ny, int nz, double spx,
+                    double spy, double spz, double alpha, double beta, double gamma, int inverse) {
+  GUARD_BEGIN
+  DiffOperParam param;
+  parse_into(param, diffoper_xml(alpha, beta, gamma));
+  SizeType size(nx, ny, nz);
+  SpacingType sp(spx, spy, spz);
+  DiffOperT<double> op(size, sp, param);
+  typename DiffOperT<double>::FFTWVectorField *f = op.GetInternalFFTWVectorField();
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const long i = ((long)z * ny + y) * nx + x;
+        (*f)(x, y, z) = Vector3D<double>(vx[i], vy[i], vz[i]);
+      }
+  if (inverse)
+    op.ApplyInverseOperator();
+  else
+    op.ApplyOperator();
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const long i = ((long)z * ny + y) * nx + x;
+        vx[i] = (*f)(x, y, z).x;
+        vy[i] = (*f)(x, y, z).y;
+        vz[i] = (*f)(x, y, z).z;
+      }
+  GUARD_END
+}
+
+/*
+ * Greedy registration through GreedyIteratorCPU, scale loop of
+ * GreedyWarp::RunWarp. factors[s] / iters[s] / maxpert[s] per scale level,
+ * listed coarse to fine. h (and hinv when compute_inverse) are returned at
+ * full resolution; energies[] receives one value per Iterate call.
+ * If h_init is non-NULL it replaces the identity initial deformation at the
+ * first (and only) scale, with init_step as the starting step size and the
+ * step-size update at iteration 0 skipped when skip_step_update is set —
+ * this lets a test run single iterations from any state.
+ */
+int awref_greedy_run(const float *i0, const float *i1, int nx, int ny, int nz, double spx,
+                     double spy, double spz, int nscales, const int *factors, const int *iters,
+                     const float *maxpert, double alpha, double beta, double gamma,
+                     int compute_inverse, const float *h_init, const float *hinv_init,
+                     float init_step, int skip_step_update, float *h_out, float *hinv_out,
+                     double *energies, float *steps_out) {
+  GUARD_BEGIN
+  std::ostringstream xml;
+  xml.precision(17);
+  xml << "<GreedyWarpParameterFile>";
+  for (int s = 0; s < nscales; ++s) {
+    xml << "<GreedyScaleLevel><ScaleLevel><DownsampleFactor val=\"" << factors[s]
+        << "\"/></ScaleLevel><GreedyIterator>" << diffoper_xml(alpha, beta, gamma)
+        << "<MaxPert val=\"" << maxpert[s] << "\"/></GreedyIterator><NIterations val=\""
+        << iters[s] << "\"/></GreedyScaleLevel>";
+  }
+  xml << "<AutoStepReduce val=\"false\"/></GreedyWarpParameterFile>";
+  GreedyParam param;
+  parse_into(param, xml.str());
+
+  SizeType size(nx, ny, nz);
+  SpacingType sp(spx, spy, spz);
+  OriginType origin(0, 0, 0);
+  RealImage I0(size, origin, sp), I1(size, origin, sp);
+  to_im(i0, I0);
+  to_im(i1, I1);
+
+  MultiscaleManager scaleManager(size, sp, origin, param);
+  scaleManager.SetScaleVectorFields(true);
+  GreedyDeformationData data(&I0, &I1, param);
+  data.ComputeInverseHField(compute_inverse != 0);
+  GreedyIteratorCPU iterator(size, origin, sp, true);
+  const unsigned nlev = param.GetNumberOfScaleLevels();
+  int e = 0;
+  data.InitializeWarp();
+  for (unsigned level = 0; level < nlev; ++level) {
+    scaleManager.SetScaleLevel(level);
+    iterator.SetScaleLevel(scaleManager, param.GetScaleLevel(level).Iterator());
+    data.SetScaleLevel(scaleManager);
+    if (h_init && level == 0) {
+      to_vf(h_init, h_init + (long)nx * ny * nz, h_init + 2L * nx * ny * nz, data.Def1To0());
+      if (compute_inverse && hinv_init)
+        to_vf(hinv_init, hinv_init + (long)nx * ny * nz, hinv_init + 2L * nx * ny * nz,
+              data.Def0To1());
+      data.StepSize(init_step);
+    }
+    const unsigned nIters = param.GetScaleLevel(level).NIterations();
+    for (unsigned iter = 0; iter < nIters; ++iter) {
+      data.SetCurIter(iter);
+      if (iter == 0 && !(h_init && skip_step_update)) iterator.UpdateStepSizeNextIteration();
+      iterator.Iterate(data);
+      if (energies) energies[e] = data.GetEnergyHistory().LastEnergy()->GetEnergy();
+      if (steps_out) steps_out[e] = data.StepSize();
+      ++e;
+    }
+  }
+  const long n = (long)nx * ny * nz;
+  from_vf(data.Def1To0(), h_out, h_out + n, h_out + 2 * n);
+  if (compute_inverse && hinv_out) from_vf(data.Def0To1(), hinv_out, hinv_out + n, hinv_out + 2 * n);
+  GUARD_END
+}
+
+}  // extern "C"
