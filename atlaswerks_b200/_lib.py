@@ -1,0 +1,92 @@
+"""Loader for libaw_b200.so, the C ABI declared in include/aw_b200.h.
+
+The library is built in-tree (``atlaswerks_b200/csrc/Makefile``) for sm_100a.
+There is no fallback: if the library is missing or fails to load, every
+entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+import subprocess
+from typing import List
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+LIB_PATH = os.path.join(PKG, "libaw_b200.so")
+HEADER_DIR = os.path.join(ROOT, "include")
+
+_lib = None
+
+
+class AwError(RuntimeError):
+    """A C-ABI call returned non-zero; the message is aw_last_error()."""
+
+
+def build(force: bool = False) -> str:
+    """Compile the CUDA library for sm_100a (nvcc cross-compiles without a GPU)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-j8", "-C", os.path.join(PKG, "csrc")], check=True)
+    return LIB_PATH
+
+
+_c = ctypes
+_fp = ctypes.c_void_p
+_i = ctypes.c_int
+_f = ctypes.c_float
+_d = ctypes.c_double
+
+# argument types of every entry point, in header order
+SIGNATURES = {
+    "aw_last_error": ([], ctypes.c_char_p),
+    "aw_version": ([], ctypes.c_char_p),
+    "aw_apply": ([_fp] * 5 + [_i] * 3 + [_f, _fp], _i),
+    "aw_gradient": ([_fp] * 4 + [_i] * 3 + [_d] * 3 + [_i, _fp], _i),
+    "aw_compose_hv": ([_fp] * 9 + [_i] * 3 + [_d] * 3 + [_f, _i, _i, _fp], _i),
+    "aw_compose_vh": ([_fp] * 9 + [_i] * 3 + [_d] * 3 + [_f, _i, _i, _fp], _i),
+    "aw_fluid_create": ([_i] * 3 + [_d] * 3 + [_f] * 3 + [_fp], _i),
+    "aw_fluid_apply": ([_fp] * 4 + [_i, _fp], _i),
+    "aw_fluid_destroy": ([_fp], _i),
+    "aw_greedy_create": ([_i] * 3 + [_d] * 3 + [_f] * 4 + [_fp], _i),
+    "aw_greedy_destroy": ([_fp], _i),
+    "aw_greedy_set_step": ([_fp, _f], _i),
+    "aw_greedy_get_step": ([_fp, _fp], _i),
+    "aw_greedy_set_auto_step_reduce": ([_fp, _i], _i),
+    "aw_greedy_iterate": ([_fp] * 15 + [_i, _fp], _i),
+    "aw_greedy_run": ([_fp] * 15 + [_i, _i, _fp], _i),
+    "aw_greedy_get_energies": ([_fp, _fp, _i, _fp], _i),
+}
+
+
+def header_symbols() -> List[str]:
+    """Every function name declared in include/*.h."""
+    names = []
+    for fn in sorted(os.listdir(HEADER_DIR)):
+        if not fn.endswith(".h"):
+            continue
+        text = open(os.path.join(HEADER_DIR, fn)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names += re.findall(r"\b(aw_[a-z0-9_]+)\s*\(", text)
+    return sorted(set(names))
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded library (raises if it cannot be loaded)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise AwError(f"{LIB_PATH} is missing: build it with `make -C atlaswerks_b200/csrc` "
+                          "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        raise AwError(lib().aw_last_error().decode())

@@ -1,0 +1,368 @@
+// capi.cu — the extern "C" boundary declared in include/aw_b200.h.
+//
+// Thin: argument checks, handle lifetime, error strings, and the CUDA-graph
+// replay of the greedy loop. All arithmetic lives in the kernels.
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/aw_b200.h"
+#include "greedy.cuh"
+#include "interp.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(const std::string &msg) {
+  g_last_error = msg;
+  return 1;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return 2;
+}
+
+#define AW_CUDA(call, what)                        \
+  do {                                             \
+    cudaError_t _e = (call);                       \
+    if (_e != cudaSuccess) return cuda_fail(_e, what); \
+  } while (0)
+
+bool dims_ok(int nx, int ny, int nz, std::string &why) {
+  if (nx < 2 || ny < 2 || nz < 2) {
+    why = "every grid axis must be >= 2";
+    return false;
+  }
+  if (nx > 512 || ny > 512 || nz > 512) {
+    why = "grid axes are limited to 512 (the reference's FFT LUT cap)";
+    return false;
+  }
+  return true;
+}
+
+bool spacing_ok(double a, double b, double c) { return a > 0 && b > 0 && c > 0; }
+
+const char *plan_error(int rc) {
+  switch (rc) {
+    case 1: return "unsupported grid size for the fluid FFT plan";
+    case 2: return "z-slab spectrum does not fit in shared memory (nx*ny too large)";
+    case 3: return "device allocation failed";
+    default: return "kernel configuration failed";
+  }
+}
+
+inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+}  // namespace
+
+struct aw_fluid_s {
+  aw::FluidPlan plan;
+};
+
+struct GraphKey {
+  const void *p[14];
+  int n;
+  bool operator<(const GraphKey &o) const {
+    for (int i = 0; i < 14; ++i)
+      if (p[i] != o.p[i]) return p[i] < o.p[i];
+    return n < o.n;
+  }
+};
+
+struct aw_greedy_s {
+  aw::GreedyCtx ctx;
+  int auto_reduce = 0;
+  cudaStream_t gstream = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  std::map<GraphKey, cudaGraphExec_t> graphs;
+};
+
+extern "C" {
+
+const char *aw_last_error(void) { return g_last_error.c_str(); }
+
+const char *aw_version(void) { return "atlaswerks_b200 0.1 (sm_100a)"; }
+
+int aw_apply(const float *img, const float *hx, const float *hy, const float *hz, float *out,
+             int nx, int ny, int nz, float background, void *stream) {
+  std::string why;
+  if (!img || !hx || !hy || !hz || !out) return fail("aw_apply: null pointer");
+  if (nx < 1 || ny < 1 || nz < 1) return fail("aw_apply: empty grid");
+  AW_CUDA(aw::launch_apply(img, hx, hy, hz, out, aw::Dims{nx, ny, nz}, background, S(stream)),
+          "aw_apply");
+  return 0;
+}
+
+int aw_gradient(const float *img, float *gx, float *gy, float *gz, int nx, int ny, int nz,
+                double spx, double spy, double spz, int wrap, void *stream) {
+  std::string why;
+  if (!img || !gx || !gy || !gz) return fail("aw_gradient: null pointer");
+  if (nx < 2 || ny < 2 || nz < 2) return fail("aw_gradient: every grid axis must be >= 2");
+  if (!spacing_ok(spx, spy, spz)) return fail("aw_gradient: spacing must be positive");
+  AW_CUDA(aw::launch_gradient(img, gx, gy, gz, aw::Dims{nx, ny, nz}, aw::Spacing{spx, spy, spz},
+                              wrap, S(stream)),
+          "aw_gradient");
+  return 0;
+}
+
+int aw_compose_hv(const float *gx, const float *gy, const float *gz, const float *vx,
+                  const float *vy, const float *vz, float *ox, float *oy, float *oz, int nx,
+                  int ny, int nz, double spx, double spy, double spz, float scale, int direction,
+                  int background, void *stream) {
+  if (!gx || !gy || !gz || !vx || !vy || !vz || !ox || !oy || !oz)
+    return fail("aw_compose_hv: null pointer");
+  if (nx < 1 || ny < 1 || nz < 1) return fail("aw_compose_hv: empty grid");
+  if (!spacing_ok(spx, spy, spz)) return fail("aw_compose_hv: spacing must be positive");
+  if (background < 0 || background > 5) return fail("aw_compose_hv: unknown background strategy");
+  const float *g[3] = {gx, gy, gz}, *v[3] = {vx, vy, vz};
+  float *o[3] = {ox, oy, oz};
+  AW_CUDA(aw::launch_compose_hv(g, v, o, aw::Dims{nx, ny, nz}, aw::Spacing{spx, spy, spz},
+                                direction >= 0 ? 1 : -1, background, nullptr, scale, S(stream)),
+          "aw_compose_hv");
+  return 0;
+}
+
+int aw_compose_vh(const float *vx, const float *vy, const float *vz, const float *gx,
+                  const float *gy, const float *gz, float *ox, float *oy, float *oz, int nx,
+                  int ny, int nz, double spx, double spy, double spz, float scale, int direction,
+                  int background, void *stream) {
+  if (!gx || !gy || !gz || !vx || !vy || !vz || !ox || !oy || !oz)
+    return fail("aw_compose_vh: null pointer");
+  if (nx < 1 || ny < 1 || nz < 1) return fail("aw_compose_vh: empty grid");
+  if (!spacing_ok(spx, spy, spz)) return fail("aw_compose_vh: spacing must be positive");
+  if (background < 0 || background > 5) return fail("aw_compose_vh: unknown background strategy");
+  const float *g[3] = {gx, gy, gz}, *v[3] = {vx, vy, vz};
+  float *o[3] = {ox, oy, oz};
+  AW_CUDA(aw::launch_compose_vh(v, g, o, aw::Dims{nx, ny, nz}, aw::Spacing{spx, spy, spz},
+                                direction >= 0 ? 1 : -1, background, nullptr, scale, S(stream)),
+          "aw_compose_vh");
+  return 0;
+}
+
+int aw_fluid_create(int nx, int ny, int nz, double spx, double spy, double spz, float alpha,
+                    float beta, float gamma, aw_fluid_t *out) {
+  std::string why;
+  if (!out) return fail("aw_fluid_create: null handle pointer");
+  *out = nullptr;
+  if (!dims_ok(nx, ny, nz, why)) return fail("aw_fluid_create: " + why);
+  if (!spacing_ok(spx, spy, spz)) return fail("aw_fluid_create: spacing must be positive");
+  if (!(gamma > 0.0f) || alpha < 0.0f || beta < 0.0f)
+    return fail("aw_fluid_create: need gamma > 0, alpha >= 0, beta >= 0 (L must be SPD)");
+  aw_fluid_s *k = new (std::nothrow) aw_fluid_s;
+  if (!k) return fail("aw_fluid_create: out of host memory");
+  const int rc = aw::fluid_plan_create(&k->plan, nx, ny, nz, spx, spy, spz, alpha, beta, gamma);
+  if (rc) {
+    aw::fluid_plan_destroy(&k->plan);
+    delete k;
+    return fail(std::string("aw_fluid_create: ") + plan_error(rc));
+  }
+  *out = k;
+  return 0;
+}
+
+int aw_fluid_apply(aw_fluid_t k, float *vx, float *vy, float *vz, int inverse, void *stream) {
+  if (!k) return fail("aw_fluid_apply: null handle");
+  if (!vx || !vy || !vz) return fail("aw_fluid_apply: null pointer");
+  cudaStream_t s = S(stream);
+  AW_CUDA(aw::fluid_forward_field(k->plan, vx, vy, vz, s), "aw_fluid_apply (xy forward)");
+  AW_CUDA(aw::fluid_solve(k->plan, inverse ? 1 : 0, s), "aw_fluid_apply (z solve)");
+  AW_CUDA(aw::fluid_inverse_store(k->plan, vx, vy, vz, s), "aw_fluid_apply (xy inverse)");
+  return 0;
+}
+
+int aw_fluid_destroy(aw_fluid_t k) {
+  if (!k) return 0;
+  aw::fluid_plan_destroy(&k->plan);
+  delete k;
+  return 0;
+}
+
+int aw_greedy_create(int nx, int ny, int nz, double spx, double spy, double spz, float alpha,
+                     float beta, float gamma, float max_pert, aw_greedy_t *out) {
+  std::string why;
+  if (!out) return fail("aw_greedy_create: null handle pointer");
+  *out = nullptr;
+  if (!dims_ok(nx, ny, nz, why)) return fail("aw_greedy_create: " + why);
+  if (!spacing_ok(spx, spy, spz)) return fail("aw_greedy_create: spacing must be positive");
+  if (!(gamma > 0.0f) || alpha < 0.0f || beta < 0.0f)
+    return fail("aw_greedy_create: need gamma > 0, alpha >= 0, beta >= 0 (L must be SPD)");
+  if (!(max_pert > 0.0f)) return fail("aw_greedy_create: MaxPert must be positive");
+  aw_greedy_s *g = new (std::nothrow) aw_greedy_s;
+  if (!g) return fail("aw_greedy_create: out of host memory");
+  const int rc =
+      aw::greedy_create(&g->ctx, nx, ny, nz, spx, spy, spz, alpha, beta, gamma, max_pert, 4096);
+  if (rc) {
+    aw::greedy_destroy(&g->ctx);
+    delete g;
+    return fail(std::string("aw_greedy_create: ") + plan_error(rc));
+  }
+  if (cudaStreamCreateWithFlags(&g->gstream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&g->ev_in, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&g->ev_out, cudaEventDisableTiming) != cudaSuccess) {
+    aw::greedy_destroy(&g->ctx);
+    delete g;
+    return fail("aw_greedy_create: stream/event creation failed");
+  }
+  *out = g;
+  return 0;
+}
+
+int aw_greedy_destroy(aw_greedy_t g) {
+  if (!g) return 0;
+  cudaDeviceSynchronize();
+  for (auto &kv : g->graphs) cudaGraphExecDestroy(kv.second);
+  if (g->gstream) cudaStreamDestroy(g->gstream);
+  if (g->ev_in) cudaEventDestroy(g->ev_in);
+  if (g->ev_out) cudaEventDestroy(g->ev_out);
+  aw::greedy_destroy(&g->ctx);
+  delete g;
+  return 0;
+}
+
+int aw_greedy_set_step(aw_greedy_t g, float step) {
+  if (!g) return fail("aw_greedy_set_step: null handle");
+  AW_CUDA(cudaMemcpy(g->ctx.st.step, &step, sizeof(float), cudaMemcpyHostToDevice),
+          "aw_greedy_set_step");
+  return 0;
+}
+
+int aw_greedy_get_step(aw_greedy_t g, float *step) {
+  if (!g || !step) return fail("aw_greedy_get_step: null pointer");
+  AW_CUDA(cudaDeviceSynchronize(), "aw_greedy_get_step (pending work)");
+  AW_CUDA(cudaMemcpy(step, g->ctx.st.step, sizeof(float), cudaMemcpyDeviceToHost),
+          "aw_greedy_get_step");
+  return 0;
+}
+
+int aw_greedy_set_auto_step_reduce(aw_greedy_t g, int on) {
+  if (!g) return fail("aw_greedy_set_auto_step_reduce: null handle");
+  g->auto_reduce = on ? 1 : 0;
+  return 0;
+}
+
+int aw_greedy_iterate(aw_greedy_t g, const float *I0, const float *I1, const float *hx,
+                      const float *hy, const float *hz, float *ox, float *oy, float *oz,
+                      const float *hix, const float *hiy, const float *hiz, float *hiox,
+                      float *hioy, float *hioz, int update_step, void *stream) {
+  if (!g) return fail("aw_greedy_iterate: null handle");
+  if (!I0 || !I1 || !hx || !hy || !hz || !ox || !oy || !oz)
+    return fail("aw_greedy_iterate: null pointer");
+  if (ox == hx || oy == hy || oz == hz) return fail("aw_greedy_iterate: h_out must not alias h");
+  const bool inv = hix != nullptr;
+  if (inv && (!hiy || !hiz || !hiox || !hioy || !hioz))
+    return fail("aw_greedy_iterate: incomplete inverse field pointers");
+  if (inv && (hiox == hix || hioy == hiy || hioz == hiz))
+    return fail("aw_greedy_iterate: hinv_out must not alias hinv");
+  const float *h[3] = {hx, hy, hz}, *hi[3] = {hix, hiy, hiz};
+  float *o[3] = {ox, oy, oz}, *hio[3] = {hiox, hioy, hioz};
+  AW_CUDA(aw::greedy_iterate(&g->ctx, I0, I1, h, o, inv ? hi : nullptr, inv ? hio : nullptr,
+                             update_step, g->auto_reduce, S(stream)),
+          "aw_greedy_iterate");
+  return 0;
+}
+
+int aw_greedy_run(aw_greedy_t g, const float *I0, const float *I1, float *hx, float *hy,
+                  float *hz, float *sx, float *sy, float *sz, float *hix, float *hiy, float *hiz,
+                  float *six, float *siy, float *siz, int n_iters, int update_first,
+                  void *stream) {
+  if (!g) return fail("aw_greedy_run: null handle");
+  if (!I0 || !I1 || !hx || !hy || !hz || !sx || !sy || !sz)
+    return fail("aw_greedy_run: null pointer");
+  if (n_iters < 0) return fail("aw_greedy_run: negative iteration count");
+  const bool inv = hix != nullptr;
+  if (inv && (!hiy || !hiz || !six || !siy || !siz))
+    return fail("aw_greedy_run: incomplete inverse field pointers");
+  if (n_iters == 0) return 0;
+  cudaStream_t user = S(stream);
+  cudaStream_t s = g->gstream;
+  AW_CUDA(cudaEventRecord(g->ev_in, user), "aw_greedy_run (event)");
+  AW_CUDA(cudaStreamWaitEvent(s, g->ev_in, 0), "aw_greedy_run (wait)");
+  float *A[3] = {hx, hy, hz}, *B[3] = {sx, sy, sz};
+  float *AI[3] = {hix, hiy, hiz}, *BI[3] = {six, siy, siz};
+  int done = 0;
+  bool in_a = true;
+  auto one = [&](int upd) -> cudaError_t {
+    float **src = in_a ? A : B, **dst = in_a ? B : A;
+    float **isrc = in_a ? AI : BI, **idst = in_a ? BI : AI;
+    const float *cs[3] = {src[0], src[1], src[2]}, *ci[3] = {isrc[0], isrc[1], isrc[2]};
+    cudaError_t e = aw::greedy_iterate(&g->ctx, I0, I1, cs, dst, inv ? ci : nullptr,
+                                       inv ? idst : nullptr, upd, g->auto_reduce, s);
+    in_a = !in_a;
+    return e;
+  };
+  if (update_first) {
+    AW_CUDA(one(1), "aw_greedy_run (first iteration)");
+    ++done;
+  }
+  // replay a captured pair of iterations (src->dst->src) as often as possible
+  const int pairs = (n_iters - done) / 2;
+  if (pairs > 0) {
+    GraphKey key;
+    std::memset(&key, 0, sizeof(key));
+    float **src = in_a ? A : B, **dst = in_a ? B : A;
+    float **isrc = in_a ? AI : BI, **idst = in_a ? BI : AI;
+    const void *ptrs[14] = {I0,      I1,      src[0],  src[1],  src[2],  dst[0],  dst[1],
+                            dst[2],  isrc[0], isrc[1], isrc[2], idst[0], idst[1], idst[2]};
+    for (int i = 0; i < 14; ++i) key.p[i] = ptrs[i];
+    key.n = 2;
+    auto it = g->graphs.find(key);
+    cudaGraphExec_t exec = nullptr;
+    if (it == g->graphs.end()) {
+      cudaGraph_t graph;
+      AW_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "aw_greedy_run (capture)");
+      const bool start = in_a;
+      cudaError_t e1 = one(0), e2 = one(0);
+      cudaError_t ec = cudaStreamEndCapture(s, &graph);
+      in_a = start;
+      if (e1 != cudaSuccess) return cuda_fail(e1, "aw_greedy_run (captured iteration)");
+      if (e2 != cudaSuccess) return cuda_fail(e2, "aw_greedy_run (captured iteration)");
+      if (ec != cudaSuccess) return cuda_fail(ec, "aw_greedy_run (end capture)");
+      AW_CUDA(cudaGraphInstantiate(&exec, graph, 0), "aw_greedy_run (instantiate)");
+      cudaGraphDestroy(graph);
+      g->graphs[key] = exec;
+    } else {
+      exec = it->second;
+    }
+    for (int p = 0; p < pairs; ++p) AW_CUDA(cudaGraphLaunch(exec, s), "aw_greedy_run (launch)");
+    done += 2 * pairs;
+  }
+  if (done < n_iters) {
+    AW_CUDA(one(0), "aw_greedy_run (last iteration)");
+    ++done;
+  }
+  if (!in_a) {  // final field is in the scratch buffers: bring it home
+    const size_t bytes = sizeof(float) * (size_t)g->ctx.d.n();
+    for (int c = 0; c < 3; ++c) {
+      AW_CUDA(cudaMemcpyAsync(A[c], B[c], bytes, cudaMemcpyDeviceToDevice, s), "aw_greedy_run (copy)");
+      if (inv) AW_CUDA(cudaMemcpyAsync(AI[c], BI[c], bytes, cudaMemcpyDeviceToDevice, s), "aw_greedy_run (copy)");
+    }
+  }
+  AW_CUDA(cudaEventRecord(g->ev_out, s), "aw_greedy_run (event)");
+  AW_CUDA(cudaStreamWaitEvent(user, g->ev_out, 0), "aw_greedy_run (wait)");
+  return 0;
+}
+
+int aw_greedy_get_energies(aw_greedy_t g, double *out, int max_count, int *count) {
+  if (!g || !count) return fail("aw_greedy_get_energies: null pointer");
+  AW_CUDA(cudaDeviceSynchronize(), "aw_greedy_get_energies (pending work)");
+  int n = 0;
+  AW_CUDA(cudaMemcpy(&n, g->ctx.st.count, sizeof(int), cudaMemcpyDeviceToHost),
+          "aw_greedy_get_energies");
+  const int cap = g->ctx.st.cap;
+  const int avail = n < cap ? n : cap;
+  std::vector<double> ring(cap);
+  AW_CUDA(cudaMemcpy(ring.data(), g->ctx.st.energy, sizeof(double) * cap, cudaMemcpyDeviceToHost),
+          "aw_greedy_get_energies");
+  const int m = (out && max_count < avail) ? max_count : avail;
+  for (int i = 0; i < m && out; ++i) out[i] = ring[(n - avail + i) % cap];
+  *count = avail;
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,330 @@
+// fluid.cu — fused FFT kernels of the fluid operator solve (see fluid.cuh).
+//
+// Reference behaviour (Algorithms/Common/DiffOper.cxx:825-905 on the CPU,
+// CUDACommon/src/cudaFFTSolver.cu:675-704 on the old GPU path): the force is
+// scaled by 1/N, transformed, multiplied per wavenumber by L(k)^-1 (or L(k)),
+// and transformed back, with
+//   lambda = -alpha*(cx+cy+cz) + gamma,  L_ii = lambda - beta*c_i,
+//   L_ij = beta*s_i*s_j,  c = (2cos(2 pi k/n) - 2)/sp^2,  s = sin(2 pi k/n)/sp
+// (LUT: DiffOper.cxx:590-639; Cholesky: DiffOper.cxx:1005-1083). Here the
+// 1/N scaling is folded into the per-wavenumber step.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "fluid.cuh"
+
+namespace aw {
+
+namespace {
+
+// Radix plan: as many 8s as possible, a 4 instead of an 8*2 tail, then 3,
+// then any remaining prime (direct DFT).
+bool factorize(int n, FFTAxis &ax) {
+  int e = 0, m = n;
+  while (m % 2 == 0) { m /= 2; ++e; }
+  std::vector<int> r;
+  int e8 = e / 3, rem = e % 3;
+  if (rem == 1 && e8 > 0) { --e8; r.push_back(4); r.push_back(4); rem = 0; }
+  for (int i = 0; i < e8; ++i) r.insert(r.begin(), 8);
+  if (rem == 2) r.push_back(4);
+  if (rem == 1) r.push_back(2);
+  while (m % 3 == 0) { r.push_back(3); m /= 3; }
+  for (int p = 5; m > 1; p += 2)
+    while (m % p == 0) { r.push_back(p); m /= p; }
+  if ((int)r.size() > kMaxStages) return false;
+  ax.n = n;
+  ax.nstages = (int)r.size();
+  for (int i = 0; i < ax.nstages; ++i) ax.radix[i] = r[i];
+  return true;
+}
+
+void fill_twiddles(int n, std::vector<float2> &out) {
+  for (int m = 0; m < n; ++m) {
+    const double a = -2.0 * M_PI * (double)m / (double)n;
+    out.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+  }
+}
+
+// reference LUT, computed in double and stored as float like DiffOperT<float>
+void fill_lut(int n, double sp, std::vector<float> &out) {
+  const double s = 2.0 * M_PI / n;
+  for (int k = 0; k < n; ++k) out.push_back((float)((2.0 * std::cos(s * k) - 2.0) / (sp * sp)));
+  for (int k = 0; k < n; ++k) out.push_back((float)(std::sin(s * k) / sp));
+}
+
+template <class Src>
+__global__ void __launch_bounds__(256) k_fft_xy_fwd(FluidPlan p, Src src) {
+  extern __shared__ float2 sm[];
+  const Dims d = p.d;
+  const int z = blockIdx.x, comp = blockIdx.y;
+  const int nx = d.nx, ny = d.ny, nxh = p.nxh;
+  const int P = p.pairs_per_batch, Q = p.cols_per_batch;
+  const int ws = max(P * nx, Q * ny);
+  float2 *C = sm;
+  float2 *A = C + ny * nxh;
+  float2 *B = A + ws;
+  const int npairs = (ny + 1) >> 1;
+  for (int p0 = 0; p0 < npairs; p0 += P) {
+    const int pb = min(P, npairs - p0);
+    for (int t = threadIdx.x; t < pb * nx; t += blockDim.x) {
+      const int b = t / nx, x = t - b * nx;
+      const int y0 = 2 * (p0 + b), y1 = y0 + 1;
+      const float a0 = src.value(comp, x, y0, z, d);
+      const float a1 = (y1 < ny) ? src.value(comp, x, y1, z, d) : 0.f;
+      A[b * nx + x] = make_float2(a0, a1);
+    }
+    __syncthreads();
+    const float2 *R = fft_lines<-1>(A, B, pb, nx, p.ax);
+    // two real rows from one complex transform:
+    // X0[k] = (Z[k] + conj Z[n-k]) / 2,  X1[k] = (Z[k] - conj Z[n-k]) / 2i
+    for (int t = threadIdx.x; t < pb * nxh; t += blockDim.x) {
+      const int b = t / nxh, k = t - b * nxh;
+      const float2 Z = R[b * nx + k];
+      const float2 Zm = R[b * nx + (k == 0 ? 0 : nx - k)];
+      const int y0 = 2 * (p0 + b), y1 = y0 + 1;
+      C[y0 * nxh + k] = make_float2(0.5f * (Z.x + Zm.x), 0.5f * (Z.y - Zm.y));
+      if (y1 < ny) C[y1 * nxh + k] = make_float2(0.5f * (Z.y + Zm.y), -0.5f * (Z.x - Zm.x));
+    }
+    __syncthreads();
+  }
+  float2 *out = p.spec + ((long)comp * d.nz + z) * ny * nxh;
+  for (int k0 = 0; k0 < nxh; k0 += Q) {
+    const int qb = min(Q, nxh - k0);
+    for (int t = threadIdx.x; t < qb * ny; t += blockDim.x) {
+      const int y = t / qb, q = t - y * qb;
+      A[q * ny + y] = C[y * nxh + k0 + q];
+    }
+    __syncthreads();
+    const float2 *R = fft_lines<-1>(A, B, qb, ny, p.ay);
+    for (int t = threadIdx.x; t < qb * ny; t += blockDim.x) {
+      const int y = t / qb, q = t - y * qb;
+      out[(long)y * nxh + k0 + q] = R[q * ny + y];
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) k_fft_z_solve(FluidPlan p, int inverse) {
+  extern __shared__ float2 sm[];
+  const int nz = p.d.nz, nxh = p.nxh;
+  const int K = p.zcols_per_cta;
+  const long ncols = (long)p.d.ny * nxh;
+  const long j0 = (long)blockIdx.x * K;
+  const int kb = (int)min((long)K, ncols - j0);
+  const long plane = ncols;  // complex elements per z-plane of one component
+  float2 *A = sm;
+  float2 *B = A + 3 * K * nz;
+  for (int t = threadIdx.x; t < 3 * kb * nz; t += blockDim.x) {
+    const int q = t % kb;
+    const int r = t / kb;  // r = c*nz + kz
+    const int c = r / nz, kz = r - c * nz;
+    A[(c * K + q) * nz + kz] = p.spec[((long)c * nz + kz) * plane + j0 + q];
+  }
+  __syncthreads();
+  // lines: c*K + q for c in 0..2, q in 0..kb-1 (unused q in [kb,K) skipped via ld stride)
+  float2 *R = fft_lines<-1>(A, B, 3 * K, nz, p.az);
+  float2 *W = (R == A) ? B : A;
+  const float *cwx = p.lut, *swx = cwx + p.d.nx, *cwy = swx + p.d.nx, *swy = cwy + p.d.ny,
+              *cwz = swy + p.d.ny, *swz = cwz + nz;
+  const float invN = 1.0f / (float)p.d.n();
+  for (int t = threadIdx.x; t < kb * nz; t += blockDim.x) {
+    const int q = t % kb, kz = t / kb;
+    const long j = j0 + q;
+    const int ky = (int)(j / nxh), kx = (int)(j - (long)ky * nxh);
+    const float cx = __ldg(cwx + kx), cy = __ldg(cwy + ky), cz = __ldg(cwz + kz);
+    const float sx = __ldg(swx + kx), sy = __ldg(swy + ky), sz = __ldg(swz + kz);
+    const float lambda = -p.alpha * (cx + cy + cz) + p.gamma;
+    const float L00 = lambda - p.beta * cx, L11 = lambda - p.beta * cy, L22 = lambda - p.beta * cz;
+    const float L10 = p.beta * sx * sy, L20 = p.beta * sx * sz, L21 = p.beta * sy * sz;
+    float2 b0 = R[(0 * K + q) * nz + kz], b1 = R[(1 * K + q) * nz + kz], b2 = R[(2 * K + q) * nz + kz];
+    b0.x *= invN; b0.y *= invN; b1.x *= invN; b1.y *= invN; b2.x *= invN; b2.y *= invN;
+    float2 o0, o1, o2;
+    if (inverse) {
+      // Cholesky L = G G^T, then G y = b, G^T x = y (real matrix, complex rhs)
+      const float G00 = sqrtf(L00);
+      const float G10 = L10 / G00, G20 = L20 / G00;
+      const float G11 = sqrtf(L11 - G10 * G10);
+      const float G21 = (L21 - G20 * G10) / G11;
+      const float G22 = sqrtf(L22 - (G20 * G20 + G21 * G21));
+      float2 y0, y1, y2;
+      y0.x = b0.x / G00;                              y0.y = b0.y / G00;
+      y1.x = (b1.x - G10 * y0.x) / G11;               y1.y = (b1.y - G10 * y0.y) / G11;
+      y2.x = (b2.x - G20 * y0.x - G21 * y1.x) / G22;  y2.y = (b2.y - G20 * y0.y - G21 * y1.y) / G22;
+      o2.x = y2.x / G22;                              o2.y = y2.y / G22;
+      o1.x = (y1.x - G21 * o2.x) / G11;               o1.y = (y1.y - G21 * o2.y) / G11;
+      o0.x = (y0.x - G10 * o1.x - G20 * o2.x) / G00;  o0.y = (y0.y - G10 * o1.y - G20 * o2.y) / G00;
+    } else {
+      o0.x = L00 * b0.x + L10 * b1.x + L20 * b2.x;  o0.y = L00 * b0.y + L10 * b1.y + L20 * b2.y;
+      o1.x = L10 * b0.x + L11 * b1.x + L21 * b2.x;  o1.y = L10 * b0.y + L11 * b1.y + L21 * b2.y;
+      o2.x = L20 * b0.x + L21 * b1.x + L22 * b2.x;  o2.y = L20 * b0.y + L21 * b1.y + L22 * b2.y;
+    }
+    W[(0 * K + q) * nz + kz] = o0;
+    W[(1 * K + q) * nz + kz] = o1;
+    W[(2 * K + q) * nz + kz] = o2;
+  }
+  __syncthreads();
+  const float2 *V = fft_lines<+1>(W, R, 3 * K, nz, p.az);
+  for (int t = threadIdx.x; t < 3 * kb * nz; t += blockDim.x) {
+    const int q = t % kb;
+    const int r = t / kb;
+    const int c = r / nz, kz = r - c * nz;
+    p.spec[((long)c * nz + kz) * plane + j0 + q] = V[(c * K + q) * nz + kz];
+  }
+}
+
+template <class Dst>
+__global__ void __launch_bounds__(256) k_fft_xy_inv(FluidPlan p, Dst dst) {
+  extern __shared__ float2 sm[];
+  const Dims d = p.d;
+  const int z = blockIdx.x, comp = blockIdx.y;
+  const int nx = d.nx, ny = d.ny, nxh = p.nxh;
+  const int P = p.pairs_per_batch, Q = p.cols_per_batch;
+  const int ws = max(P * nx, Q * ny);
+  float2 *C = sm;
+  float2 *A = C + ny * nxh;
+  float2 *B = A + ws;
+  const float2 *in = p.spec + ((long)comp * d.nz + z) * ny * nxh;
+  for (int k0 = 0; k0 < nxh; k0 += Q) {
+    const int qb = min(Q, nxh - k0);
+    for (int t = threadIdx.x; t < qb * ny; t += blockDim.x) {
+      const int y = t / qb, q = t - y * qb;
+      A[q * ny + y] = in[(long)y * nxh + k0 + q];
+    }
+    __syncthreads();
+    const float2 *R = fft_lines<+1>(A, B, qb, ny, p.ay);
+    for (int t = threadIdx.x; t < qb * ny; t += blockDim.x) {
+      const int y = t / qb, q = t - y * qb;
+      C[y * nxh + k0 + q] = R[q * ny + y];
+    }
+    __syncthreads();
+  }
+  const int npairs = (ny + 1) >> 1;
+  const bool even = (nx & 1) == 0;
+  for (int p0 = 0; p0 < npairs; p0 += P) {
+    const int pb = min(P, npairs - p0);
+    // Z[k] = X0[k] + i X1[k] over the Hermitian completion; the imaginary
+    // parts of the DC (and even-n Nyquist) terms are dropped, as c2r does.
+    for (int t = threadIdx.x; t < pb * nx; t += blockDim.x) {
+      const int b = t / nx, k = t - b * nx;
+      const int y0 = 2 * (p0 + b), y1 = y0 + 1;
+      const bool upper = k >= nxh;
+      const int kk = upper ? nx - k : k;
+      float2 X0 = C[y0 * nxh + kk];
+      float2 X1 = (y1 < ny) ? C[y1 * nxh + kk] : make_float2(0.f, 0.f);
+      if (kk == 0 || (even && kk == nx / 2)) { X0.y = 0.f; X1.y = 0.f; }
+      if (upper) { X0.y = -X0.y; X1.y = -X1.y; }
+      A[b * nx + k] = make_float2(X0.x - X1.y, X0.y + X1.x);
+    }
+    __syncthreads();
+    const float2 *R = fft_lines<+1>(A, B, pb, nx, p.ax);
+    for (int t = threadIdx.x; t < pb * nx; t += blockDim.x) {
+      const int b = t / nx, x = t - b * nx;
+      const int y0 = 2 * (p0 + b), y1 = y0 + 1;
+      const float2 v = R[b * nx + x];
+      dst.store(comp, d.idx(x, y0, z), v.x);
+      if (y1 < ny) dst.store(comp, d.idx(x, y1, z), v.y);
+    }
+    __syncthreads();
+  }
+}
+
+template <class K>
+cudaError_t set_smem(K kernel, size_t bytes) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+}  // namespace
+
+int fluid_plan_create(FluidPlan *p, int nx, int ny, int nz, double spx, double spy, double spz,
+                      float alpha, float beta, float gamma) {
+  std::memset(p, 0, sizeof(*p));
+  if (nx < 2 || ny < 2 || nz < 2 || nx > 512 || ny > 512 || nz > 512) return 1;
+  p->d = Dims{nx, ny, nz};
+  p->sp = Spacing{spx, spy, spz};
+  p->alpha = alpha;
+  p->beta = beta;
+  p->gamma = gamma;
+  p->nxh = nx / 2 + 1;
+  if (!factorize(nx, p->ax) || !factorize(ny, p->ay) || !factorize(nz, p->az)) return 1;
+  const int npairs = (ny + 1) / 2;
+  p->pairs_per_batch = std::max(1, std::min(npairs, (2048 + nx - 1) / nx));
+  p->cols_per_batch = std::max(1, std::min(p->nxh, (2048 + ny - 1) / ny));
+  p->zcols_per_cta = std::max(1, std::min(16, 3072 / (3 * nz)));
+  const size_t ws = std::max((size_t)p->pairs_per_batch * nx, (size_t)p->cols_per_batch * ny);
+  p->smem_xy = sizeof(float2) * ((size_t)ny * p->nxh + 2 * ws);
+  p->smem_z = sizeof(float2) * (size_t)(2 * 3 * p->zcols_per_cta * nz);
+  int dev = 0, maxsm = 0;
+  cudaGetDevice(&dev);
+  p->device = dev;
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (p->smem_xy > (size_t)maxsm || p->smem_z > (size_t)maxsm) return 2;
+
+  std::vector<float2> tw;
+  fill_twiddles(nx, tw);
+  fill_twiddles(ny, tw);
+  fill_twiddles(nz, tw);
+  std::vector<float> lut;
+  fill_lut(nx, spx, lut);
+  fill_lut(ny, spy, lut);
+  fill_lut(nz, spz, lut);
+  if (cudaMalloc(&p->tw, tw.size() * sizeof(float2)) != cudaSuccess) return 3;
+  if (cudaMalloc(&p->lut, lut.size() * sizeof(float)) != cudaSuccess) return 3;
+  if (cudaMalloc(&p->spec, sizeof(float2) * 3 * (size_t)nz * ny * p->nxh) != cudaSuccess) return 3;
+  cudaMemcpy(p->tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice);
+  cudaMemcpy(p->lut, lut.data(), lut.size() * sizeof(float), cudaMemcpyHostToDevice);
+  p->ax.tw = p->tw;
+  p->ay.tw = p->tw + nx;
+  p->az.tw = p->tw + nx + ny;
+  if (set_smem(k_fft_xy_fwd<SrcField>, p->smem_xy) != cudaSuccess ||
+      set_smem(k_fft_xy_fwd<SrcForce>, p->smem_xy) != cudaSuccess ||
+      set_smem(k_fft_xy_inv<DstField>, p->smem_xy) != cudaSuccess ||
+      set_smem(k_fft_xy_inv<DstAxpby>, p->smem_xy) != cudaSuccess ||
+      set_smem(k_fft_z_solve, p->smem_z) != cudaSuccess)
+    return 4;
+  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+
+void fluid_plan_destroy(FluidPlan *p) {
+  if (p->tw) cudaFree(p->tw);
+  if (p->lut) cudaFree(p->lut);
+  if (p->spec) cudaFree(p->spec);
+  std::memset(p, 0, sizeof(*p));
+}
+
+cudaError_t fluid_forward_field(const FluidPlan &p, const float *fx, const float *fy,
+                                const float *fz, cudaStream_t s) {
+  SrcField src{{fx, fy, fz}};
+  k_fft_xy_fwd<SrcField><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, src);
+  return cudaGetLastError();
+}
+
+cudaError_t fluid_forward_force(const FluidPlan &p, const float *G, const float *A, int diff,
+                                cudaStream_t s) {
+  SrcForce src{G, A, diff, p.sp};
+  k_fft_xy_fwd<SrcForce><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, src);
+  return cudaGetLastError();
+}
+
+cudaError_t fluid_solve(const FluidPlan &p, int inverse, cudaStream_t s) {
+  const long ncols = (long)p.d.ny * p.nxh;
+  const int grid = (int)((ncols + p.zcols_per_cta - 1) / p.zcols_per_cta);
+  k_fft_z_solve<<<grid, 256, p.smem_z, s>>>(p, inverse);
+  return cudaGetLastError();
+}
+
+cudaError_t fluid_inverse_store(const FluidPlan &p, float *ox, float *oy, float *oz,
+                                cudaStream_t s) {
+  DstField dst{{ox, oy, oz}};
+  k_fft_xy_inv<DstField><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, dst);
+  return cudaGetLastError();
+}
+
+cudaError_t fluid_inverse_axpby(const FluidPlan &p, float *vx, float *vy, float *vz, float vfac,
+                                float ufac, cudaStream_t s) {
+  DstAxpby dst{{vx, vy, vz}, vfac, ufac};
+  k_fft_xy_inv<DstAxpby><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, dst);
+  return cudaGetLastError();
+}
+
+}  // namespace aw

@@ -1,0 +1,113 @@
+// fluid.cuh — the fluid operator L = -alpha*Lap - beta*grad(div) + gamma and
+// its inverse, applied in Fourier space by three fused kernels:
+//
+//   xy-forward  one CTA per (z-slab, component): producer (a field, or the
+//               greedy/LDMM body force computed on the fly) -> real-to-complex
+//               FFT along x (two real rows packed per complex line) -> FFT
+//               along y -> half spectrum to HBM.
+//   z-solve     one CTA per tile of K (ky,kx) columns, all three components:
+//               FFT along z -> per-wavenumber 3x3 Cholesky solve (or multiply)
+//               with 1/N scaling -> inverse FFT along z -> back to HBM.
+//   xy-inverse  one CTA per (z-slab, component): inverse FFT along y ->
+//               complex-to-real along x -> consumer epilogue (store, or the
+//               LDMM velocity update).
+//
+// The half spectrum (3 x nz x ny x (nx/2+1) complex64) makes two HBM round
+// trips instead of the six of a pass-per-axis transform.
+#pragma once
+
+#include "aw_common.cuh"
+#include "fft_smem.cuh"
+
+namespace aw {
+
+struct FluidPlan {
+  Dims d;
+  Spacing sp;
+  float alpha, beta, gamma;
+  int nxh;
+  FFTAxis ax, ay, az;
+  float2 *tw;      // device twiddle tables (x | y | z)
+  float *lut;      // device LUT: cos x | sin x | cos y | sin y | cos z | sin z
+  float2 *spec;    // device half spectrum [3][nz][ny][nxh]
+  int pairs_per_batch, cols_per_batch, zcols_per_cta;
+  size_t smem_xy, smem_z;
+  int device;
+};
+
+// --- producers for the forward pass ----------------------------------------
+// plain vector field input
+struct SrcField {
+  const float *c[3];
+  AW_D float value(int comp, int x, int y, int z, const Dims &d) const {
+    return __ldg(c[comp] + d.idx(x, y, z));
+  }
+};
+
+// body force f_c = d/dc(G) * M, with M = A - G (greedy: G = I0(h), A = I1)
+// or M = A (LDMM: G = J0_{t-1}, A = splatted residual). The gradient is
+// Array3DUtils::computeGradient with wrap = false (Array3DUtils.txx:783-900):
+// central differences / (2 sp), one-sided at the borders, the float
+// difference divided in double.
+struct SrcForce {
+  const float *G;
+  const float *A;
+  int diff;
+  Spacing sp;
+  AW_D float value(int comp, int x, int y, int z, const Dims &d) const {
+    const long i = d.idx(x, y, z);
+    const float g0 = __ldg(G + i);
+    int lo, hi, pos, n;
+    long stride;
+    double s;
+    if (comp == 0) { pos = x; n = d.nx; stride = 1; s = sp.x; }
+    else if (comp == 1) { pos = y; n = d.ny; stride = d.nx; s = sp.y; }
+    else { pos = z; n = d.nz; stride = (long)d.nx * d.ny; s = sp.z; }
+    float grad;
+    if (pos > 0 && pos < n - 1) {
+      lo = -1; hi = 1;
+      grad = __double2float_rn((double)fsub(__ldg(G + i + hi * stride), __ldg(G + i + lo * stride)) /
+                               (2.0 * s));
+    } else if (pos == 0) {
+      grad = __double2float_rn((double)fsub(__ldg(G + i + stride), g0) / s);
+    } else {
+      grad = __double2float_rn((double)fsub(g0, __ldg(G + i - stride)) / s);
+    }
+    const float a = __ldg(A + i);
+    const float m = diff ? -fsub(g0, a) : a;
+    return fmul(grad, m);
+  }
+};
+
+// --- consumers for the inverse pass ----------------------------------------
+struct DstField {
+  float *c[3];
+  AW_D void store(int comp, long i, float v) const { c[comp][i] = v; }
+};
+
+// LDMM velocity update v = vfac * v + ufac * u (LDMMIteratorCPU::updateVelocity,
+// LDMM/LDMMIteratorCPU.cxx:177-190), float arithmetic in that order.
+struct DstAxpby {
+  float *c[3];
+  float vfac, ufac;
+  AW_D void store(int comp, long i, float u) const {
+    c[comp][i] = fadd(fmul(vfac, c[comp][i]), fmul(ufac, u));
+  }
+};
+
+// host API (fluid.cu)
+int fluid_plan_create(FluidPlan *p, int nx, int ny, int nz, double spx, double spy, double spz,
+                      float alpha, float beta, float gamma);
+void fluid_plan_destroy(FluidPlan *p);
+
+cudaError_t fluid_forward_field(const FluidPlan &p, const float *fx, const float *fy,
+                                const float *fz, cudaStream_t s);
+cudaError_t fluid_forward_force(const FluidPlan &p, const float *G, const float *A, int diff,
+                                cudaStream_t s);
+cudaError_t fluid_solve(const FluidPlan &p, int inverse, cudaStream_t s);
+cudaError_t fluid_inverse_store(const FluidPlan &p, float *ox, float *oy, float *oz,
+                                cudaStream_t s);
+cudaError_t fluid_inverse_axpby(const FluidPlan &p, float *vx, float *vy, float *vz, float vfac,
+                                float ufac, cudaStream_t s);
+
+}  // namespace aw

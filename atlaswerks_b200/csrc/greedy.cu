@@ -1,0 +1,204 @@
+// greedy.cu — one greedy-fluid iteration on the device, GreedyIteratorGPU /
+// GreedyIteratorCPU::Iterate (Algorithms/Greedy/GreedyIteratorCPU.cxx:99-138)
+// restated as six stream-ordered launches with no host synchronisation:
+//
+//   1 force_prep     I0(h) and the energy partial sums of (I1 - I0(h))^2
+//   2 energy_final   deterministic block-ordered sum -> energy history,
+//                    optional AutoStepReduce (GreedyDeformationData.cxx:176-183)
+//   3 xy-forward     body force grad(I0(h)) * (I1 - I0(h)) fused into the FFT
+//   4 z-solve        L^-1 per wavenumber
+//   5 xy-inverse     v = K f
+//   6 update         h' = h(x + eps*v/sp) [PARTIAL_ID], optionally
+//                    hinv' = hinv - (eps*v)(hinv)/sp [PARTIAL_ZERO]
+//
+// plus, at a step-size update (iteration 0 of a scale level,
+// GreedyWarp.txx:99), a max|v| reduction and eps = MaxPert / max|v| computed
+// on the device (GreedyIteratorCPU.cxx:125-131).
+#include <cstring>
+
+#include "greedy.cuh"
+#include "interp.cuh"
+
+namespace aw {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__global__ void __launch_bounds__(kThreads)
+    k_force_prep(const float *__restrict__ I0, const float *__restrict__ I1,
+                 const float *__restrict__ hx, const float *__restrict__ hy,
+                 const float *__restrict__ hz, float *__restrict__ idef, double *__restrict__ partials,
+                 Dims d) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0.0;
+  if (i < d.n()) {
+    const float v = trilerp_scalar(I0, d, (double)hx[i], (double)hy[i], (double)hz[i], 0.0f);
+    idef[i] = v;
+    const float r = -fsub(v, I1[i]);
+    e = (double)r * (double)r;
+  }
+  __shared__ double ws[kThreads / 32];
+  e = warp_sum(e);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = e;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = threadIdx.x < kThreads / 32 ? ws[threadIdx.x] : 0.0;
+    t = warp_sum(t);
+    if (threadIdx.x == 0) partials[blockIdx.x] = t;
+  }
+}
+
+// Fixed-order reduction of the block partials, so the energy is bitwise
+// reproducible run to run.
+__global__ void __launch_bounds__(kThreads)
+    k_energy_final(const double *__restrict__ partials, int nparts, double scale,
+                   GreedyDevState st, int auto_reduce) {
+  double t = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) t += partials[i];
+  __shared__ double ws[kThreads / 32];
+  t = warp_sum(t);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) s += ws[w];
+    const double e = s * scale;
+    const int k = *st.count;
+    if (auto_reduce && k > 0) {
+      const double prev = st.energy[(k - 1) % st.cap];
+      if ((float)e - (float)prev > 0.0f) *st.step = *st.step / 2.0f;
+    }
+    st.energy[k % st.cap] = e;
+    *st.count = k + 1;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_max_norm(const float *__restrict__ vx, const float *__restrict__ vy,
+               const float *__restrict__ vz, long n, unsigned *__restrict__ maxbits) {
+  float m = 0.0f;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const float a = vx[i], b = vy[i], c = vz[i];
+    const float l = sqrtf(fadd(fadd(fmul(a, a), fmul(b, b)), fmul(c, c)));
+    m = fmaxf(m, l);
+  }
+  m = warp_max(m);
+  if ((threadIdx.x & 31) == 0) atomicMax(maxbits, __float_as_uint(m));
+}
+
+__global__ void k_set_step(const unsigned *__restrict__ maxbits, float max_pert, float *step) {
+  *step = fdiv(max_pert, __uint_as_float(*maxbits));
+}
+
+// composeHV(h, eps*v, PARTIAL_ID) and, when hinv is given,
+// composeVHInv(eps*v, hinv, PARTIAL_ZERO) — GreedyIteratorCPU::updateDeformation
+// (GreedyIteratorCPU.cxx:83-95), both from one read of v.
+__global__ void __launch_bounds__(kThreads)
+    k_update(const float *__restrict__ hx, const float *__restrict__ hy, const float *__restrict__ hz,
+             const float *__restrict__ vx, const float *__restrict__ vy, const float *__restrict__ vz,
+             float *__restrict__ ox, float *__restrict__ oy, float *__restrict__ oz,
+             const float *__restrict__ gx, const float *__restrict__ gy, const float *__restrict__ gz,
+             float *__restrict__ qx, float *__restrict__ qy, float *__restrict__ qz, Dims d,
+             Spacing sp, const float *__restrict__ step_ptr) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n()) return;
+  const float eps = *step_ptr;
+  const int x = (int)(i % d.nx);
+  const int y = (int)((i / d.nx) % d.ny);
+  const int z = (int)(i / ((long)d.nx * d.ny));
+  const float sx = (float)sp.x, sy = (float)sp.y, sz = (float)sp.z;
+  const float px = fadd(__int2float_rn(x), fdiv(fmul(vx[i], eps), sx));
+  const float py = fadd(__int2float_rn(y), fdiv(fmul(vy[i], eps), sy));
+  const float pz = fadd(__int2float_rn(z), fdiv(fmul(vz[i], eps), sz));
+  float rx, ry, rz;
+  trilerp_vector(hx, hy, hz, d, px, py, pz, BG_PARTIAL_ID, 1.0f, rx, ry, rz);
+  ox[i] = rx;
+  oy[i] = ry;
+  oz[i] = rz;
+  if (gx) {
+    const float g0 = gx[i], g1 = gy[i], g2 = gz[i];
+    float a, b, c;
+    trilerp_vector(vx, vy, vz, d, g0, g1, g2, BG_PARTIAL_ZERO, eps, a, b, c);
+    qx[i] = fadd(fdiv(a, -sx), g0);
+    qy[i] = fadd(fdiv(b, -sy), g1);
+    qz[i] = fadd(fdiv(c, -sz), g2);
+  }
+}
+
+inline int grid_for(long n) { return (int)((n + kThreads - 1) / kThreads); }
+
+#define AW_TRY(x)                         \
+  do {                                    \
+    cudaError_t _e = (x);                 \
+    if (_e != cudaSuccess) return _e;     \
+  } while (0)
+
+}  // namespace
+
+int greedy_create(GreedyCtx *g, int nx, int ny, int nz, double spx, double spy, double spz,
+                  float alpha, float beta, float gamma, float max_pert, int history_cap) {
+  std::memset(g, 0, sizeof(*g));
+  const int rc = fluid_plan_create(&g->plan, nx, ny, nz, spx, spy, spz, alpha, beta, gamma);
+  if (rc) return rc;
+  g->d = g->plan.d;
+  g->sp = g->plan.sp;
+  g->max_pert = max_pert;
+  const long n = g->d.n();
+  g->nparts = grid_for(n);
+  g->st.cap = history_cap > 0 ? history_cap : 4096;
+  if (cudaMalloc(&g->idef, sizeof(float) * n) != cudaSuccess) return 3;
+  if (cudaMalloc(&g->vbuf, sizeof(float) * 3 * n) != cudaSuccess) return 3;
+  if (cudaMalloc(&g->partials, sizeof(double) * g->nparts) != cudaSuccess) return 3;
+  if (cudaMalloc(&g->st.energy, sizeof(double) * g->st.cap) != cudaSuccess) return 3;
+  if (cudaMalloc(&g->scalars, 64) != cudaSuccess) return 3;
+  cudaMemset(g->scalars, 0, 64);
+  g->st.step = reinterpret_cast<float *>(g->scalars);
+  g->st.count = reinterpret_cast<int *>(g->scalars + 4);
+  g->maxbits = reinterpret_cast<unsigned *>(g->scalars + 8);
+  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+
+void greedy_destroy(GreedyCtx *g) {
+  fluid_plan_destroy(&g->plan);
+  if (g->idef) cudaFree(g->idef);
+  if (g->vbuf) cudaFree(g->vbuf);
+  if (g->partials) cudaFree(g->partials);
+  if (g->st.energy) cudaFree(g->st.energy);
+  if (g->scalars) cudaFree(g->scalars);
+  std::memset(g, 0, sizeof(*g));
+}
+
+cudaError_t greedy_iterate(GreedyCtx *g, const float *I0, const float *I1, const float *const h[3],
+                           float *const h_out[3], const float *const hinv[3],
+                           float *const hinv_out[3], int update_step, int auto_reduce,
+                           cudaStream_t s) {
+  const Dims d = g->d;
+  const long n = d.n();
+  float *v[3] = {g->vbuf, g->vbuf + n, g->vbuf + 2 * n};
+  k_force_prep<<<g->nparts, kThreads, 0, s>>>(I0, I1, h[0], h[1], h[2], g->idef, g->partials, d);
+  AW_TRY(cudaGetLastError());
+  const double spprod = g->sp.x * g->sp.y * g->sp.z;
+  k_energy_final<<<1, kThreads, 0, s>>>(g->partials, g->nparts, spprod, g->st, auto_reduce);
+  AW_TRY(cudaGetLastError());
+  AW_TRY(fluid_forward_force(g->plan, g->idef, I1, 1, s));
+  AW_TRY(fluid_solve(g->plan, 1, s));
+  AW_TRY(fluid_inverse_store(g->plan, v[0], v[1], v[2], s));
+  if (update_step) {
+    AW_TRY(cudaMemsetAsync(g->maxbits, 0, sizeof(unsigned), s));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->plan.device);
+    k_max_norm<<<sms * 4, kThreads, 0, s>>>(v[0], v[1], v[2], n, g->maxbits);
+    AW_TRY(cudaGetLastError());
+    k_set_step<<<1, 1, 0, s>>>(g->maxbits, g->max_pert, g->st.step);
+    AW_TRY(cudaGetLastError());
+  }
+  const bool inv = hinv && hinv[0] && hinv_out && hinv_out[0];
+  k_update<<<grid_for(n), kThreads, 0, s>>>(
+      h[0], h[1], h[2], v[0], v[1], v[2], h_out[0], h_out[1], h_out[2], inv ? hinv[0] : nullptr,
+      inv ? hinv[1] : nullptr, inv ? hinv[2] : nullptr, inv ? hinv_out[0] : nullptr,
+      inv ? hinv_out[1] : nullptr, inv ? hinv_out[2] : nullptr, d, g->sp, g->st.step);
+  return cudaGetLastError();
+}
+
+}  // namespace aw

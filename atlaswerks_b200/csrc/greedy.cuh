@@ -1,0 +1,38 @@
+// greedy.cuh — device state of the greedy-fluid iterator (greedy.cu).
+#pragma once
+
+#include "fluid.cuh"
+
+namespace aw {
+
+// scalars the iteration keeps on the device (no host round trip per step)
+struct GreedyDevState {
+  float *step;     // current step size (GreedyDeformationData::StepSize)
+  int *count;      // number of energies recorded
+  double *energy;  // energy history ring, cap entries
+  int cap;
+};
+
+struct GreedyCtx {
+  FluidPlan plan;
+  Dims d;
+  Spacing sp;
+  float max_pert;
+  float *idef;      // I0(h), N
+  float *vbuf;      // v = K f, 3N
+  double *partials; // per-block energy sums
+  int nparts;
+  char *scalars;    // step | count | maxbits
+  unsigned *maxbits;
+  GreedyDevState st;
+};
+
+int greedy_create(GreedyCtx *g, int nx, int ny, int nz, double spx, double spy, double spz,
+                  float alpha, float beta, float gamma, float max_pert, int history_cap);
+void greedy_destroy(GreedyCtx *g);
+cudaError_t greedy_iterate(GreedyCtx *g, const float *I0, const float *I1, const float *const h[3],
+                           float *const h_out[3], const float *const hinv[3],
+                           float *const hinv_out[3], int update_step, int auto_reduce,
+                           cudaStream_t s);
+
+}  // namespace aw

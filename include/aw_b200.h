@@ -1,0 +1,136 @@
+/*
+ * aw_b200.h — C ABI of the B200-native greedy-fluid / LDMM registration path.
+ *
+ * Every entry point takes plain device pointers (planar float32 arrays,
+ * x fastest, nx*ny*nz elements each; vector fields as three such planes, the
+ * layout of the reference's cplVector3DArray), sizes, spacings and an
+ * optional CUDA stream passed as void* (NULL = legacy default stream). All
+ * work is stream-ordered; only the explicit *_get_* readbacks synchronise.
+ *
+ * Return value: 0 on success, non-zero on error; aw_last_error() gives the
+ * message (thread-local). The reference raises AtlasWerksException for the
+ * same conditions (Algorithms/Common/DiffOperGPU.cxx:127-182,
+ * Base/CUDAUtilities.cxx:137-170).
+ *
+ * Grid limits: every axis in [2, 512] (the reference caps FFT axes at 512,
+ * CUDACommon/src/cudaFFTSolver.cu:21), and one z-slab's half spectrum,
+ * ny*(nx/2+1)*8 bytes plus batch buffers, must fit one CTA's shared memory
+ * (227 KB: e.g. up to 224 x 224 slabs).
+ */
+#ifndef AW_B200_H
+#define AW_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* HField3DUtils::VectorBackgroundStrategy (UtilitiesDataTypes/HField3DUtils.h:44-49) */
+enum aw_background {
+  AW_BG_PARTIAL_ID = 0,
+  AW_BG_ID = 1,
+  AW_BG_PARTIAL_ZERO = 2,
+  AW_BG_ZERO = 3,
+  AW_BG_CLAMP = 4,
+  AW_BG_WRAP = 5
+};
+
+/* Message of the last failed call on this thread. */
+const char *aw_last_error(void);
+
+/* Library build/version string. */
+const char *aw_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Device primitives. Replace CUDACommon's cudaHField3DUtils / cudaImage3D
+ * free functions (CUDACommon/inc/cudaHField3DUtils.h:150-353,
+ * CUDACommon/inc/cudaImage3D.h:95-110) and the CPU HField3DUtils templates
+ * they mirror (UtilitiesDataTypes/HField3DUtils.txx).
+ * ------------------------------------------------------------------------- */
+
+/* out(x) = img(h(x)), trilinear, `background` outside (per corner).
+ * Replaces cudaHField3DUtils::apply (CUDACommon/src/cudaHField3DUtils.cu:636-642)
+ * and HField3DUtils::apply (UtilitiesDataTypes/HField3DUtils.txx:734-752). */
+int aw_apply(const float *img, const float *hx, const float *hy, const float *hz, float *out,
+             int nx, int ny, int nz, float background, void *stream);
+
+/* Central-difference gradient / (2 sp), one-sided at the borders unless wrap.
+ * Replaces cplComputeGradient (CUDACommon/inc/cudaImage3D.h:95-110) and
+ * Array3DUtils::computeGradient (UtilitiesDataTypes/Array3DUtils.txx:783-900). */
+int aw_gradient(const float *img, float *gx, float *gy, float *gz, int nx, int ny, int nz,
+                double spx, double spy, double spz, int wrap, void *stream);
+
+/* o(x) = g(x + direction * scale * v(x) / sp).
+ * direction=+1: composeHV (UtilitiesDataTypes/HField3DUtils.txx:436-455,
+ * CUDACommon/src/cudaHField3DUtilsSp.cu:453-511); direction=-1: composeHVInv
+ * (HField3DUtils.txx:461-480). `scale` multiplies v first (1 for none). */
+int aw_compose_hv(const float *gx, const float *gy, const float *gz, const float *vx,
+                  const float *vy, const float *vz, float *ox, float *oy, float *oz, int nx,
+                  int ny, int nz, double spx, double spy, double spz, float scale, int direction,
+                  int background, void *stream);
+
+/* o(x) = g(x) + direction * (scale * v)(g(x)) / sp.
+ * direction=-1: composeVHInv (HField3DUtils.txx:405-430,
+ * CUDACommon/src/cudaHField3DUtilsSp.cu:359-445); +1: composeVH. */
+int aw_compose_vh(const float *vx, const float *vy, const float *vz, const float *gx,
+                  const float *gy, const float *gz, float *ox, float *oy, float *oz, int nx,
+                  int ny, int nz, double spx, double spy, double spz, float scale, int direction,
+                  int background, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Fluid kernel. Replaces KernelInterfaceGPU / DiffOperGPU
+ * (Algorithms/Common/KernelInterfaceGPU.h:20-43, Common/DiffOperGPU.cxx:32-205)
+ * and FFTSolverPlan3D (CUDACommon/inc/cudaFFTSolver.h:99-176).
+ * ------------------------------------------------------------------------- */
+typedef struct aw_fluid_s *aw_fluid_t;
+
+/* KernelInterfaceGPU::SetSize + DiffOperParam{Alpha, Beta, Gamma}. */
+int aw_fluid_create(int nx, int ny, int nz, double spx, double spy, double spz, float alpha,
+                    float beta, float gamma, aw_fluid_t *out);
+/* In place: inverse=1 ApplyInverseOperator (v <- L^-1 v), inverse=0
+ * ApplyOperator (v <- L v). */
+int aw_fluid_apply(aw_fluid_t k, float *vx, float *vy, float *vz, int inverse, void *stream);
+int aw_fluid_destroy(aw_fluid_t k);
+
+/* ---------------------------------------------------------------------------
+ * Greedy iterator. Replaces GreedyIteratorGPU / GreedyIteratorCPU
+ * (Algorithms/Greedy/GreedyIteratorGPU.h:32-58, GreedyIteratorCPU.cxx:99-138).
+ * The step size, energy history and iteration count live on the device.
+ * ------------------------------------------------------------------------- */
+typedef struct aw_greedy_s *aw_greedy_t;
+
+/* ctor + SetScaleLevel: grid, spacing, DiffOper parameters, MaxPert. */
+int aw_greedy_create(int nx, int ny, int nz, double spx, double spy, double spz, float alpha,
+                     float beta, float gamma, float max_pert, aw_greedy_t *out);
+int aw_greedy_destroy(aw_greedy_t g);
+
+/* GreedyDeformationData::StepSize(s) / StepSize(); get synchronises. */
+int aw_greedy_set_step(aw_greedy_t g, float step);
+int aw_greedy_get_step(aw_greedy_t g, float *step);
+/* GreedyParam::AutoStepReduce (Greedy/GreedyParam.h:61-65); off by default. */
+int aw_greedy_set_auto_step_reduce(aw_greedy_t g, int on);
+
+/* One Iterate(): reads h (and hinv when non-NULL), writes the updated fields
+ * to h_out / hinv_out (distinct buffers). update_step=1 recomputes the step
+ * as MaxPert / max|v| first (UpdateStepSizeNextIteration). Records the
+ * energy sp^3 * sum (I1 - I0(h))^2 of the incoming h. */
+int aw_greedy_iterate(aw_greedy_t g, const float *I0, const float *I1, const float *hx,
+                      const float *hy, const float *hz, float *ox, float *oy, float *oz,
+                      const float *hix, const float *hiy, const float *hiz, float *hiox,
+                      float *hioy, float *hioz, int update_step, void *stream);
+
+/* n_iters iterations, ping-ponging between h (holds the initial field and
+ * receives the final one) and the scratch field s; hinv / sinv likewise when
+ * non-NULL. The loop body is captured once as a CUDA graph and replayed.
+ * update_first=1 recomputes the step at the first iteration. */
+int aw_greedy_run(aw_greedy_t g, const float *I0, const float *I1, float *hx, float *hy,
+                  float *hz, float *sx, float *sy, float *sz, float *hix, float *hiy, float *hiz,
+                  float *six, float *siy, float *siz, int n_iters, int update_first,
+                  void *stream);
+
+/* Copies the energy history (oldest first) to host; synchronises. */
+int aw_greedy_get_energies(aw_greedy_t g, double *out, int max_count, int *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AW_B200_H */

@@ -1,0 +1,186 @@
+"""GPU parity of the greedy-fluid path against the oracle (C restatement of
+the reference CPU routines), through the C ABI.
+
+Tolerances:
+* interpolation, gradient, compose (apply / composeHV / composeVHInv ...):
+  bit-exact — same float/double operation sequence as the reference.
+* fluid operator L^-1 and L: max |gpu - fp64| / max |fp64| <= 1e-5.
+* greedy run (deformation fields): RMS of (h_gpu - h_oracle) <= 1e-3 voxel
+  after the full iteration count; energies within 1e-4 relative.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from atlaswerks_b200 import device as D  # noqa: E402
+from atlaswerks_b200.greedy import (DiffOperB200, DiffOperParam, GreedyDeformationDataB200,  # noqa: E402
+                                    GreedyIteratorB200, GreedyIteratorParam, greedy_register)
+from atlaswerks_b200.synth import greedy_pair  # noqa: E402
+from oracle import identity  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(16, 16, 16), (12, 11, 10), (9, 17, 31), (36, 31, 32)]
+SPACINGS = [(1.0, 1.0, 1.0), (2.0, 2.06452, 1.77778)]
+
+
+def cu(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_apply_bit_exact(oracle, shape):
+    rng = np.random.default_rng(1)
+    img = rng.random(shape, dtype=np.float32)
+    h = identity(shape) + rng.normal(0, 2.0, (3,) + shape).astype(np.float32)
+    want = oracle.apply(img, h)
+    got = host(D.apply(cu(img), cu(h)))
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("sp", SPACINGS)
+@pytest.mark.parametrize("wrap", [False, True])
+def test_gradient_bit_exact(oracle, shape, sp, wrap):
+    rng = np.random.default_rng(2)
+    img = rng.random(shape, dtype=np.float32)
+    want = oracle.gradient(img, sp, wrap)
+    got = host(D.gradient(cu(img), sp, wrap))
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("bg", range(6))
+@pytest.mark.parametrize("direction", [1, -1])
+def test_compose_bit_exact(oracle, bg, direction):
+    shape, sp = (12, 11, 10), (1.0, 1.3, 0.8)
+    rng = np.random.default_rng(3)
+    g = identity(shape) + rng.normal(0, 1.5, (3,) + shape).astype(np.float32)
+    v = rng.normal(0, 1.5, (3,) + shape).astype(np.float32)
+    want = oracle.compose_hv(g, v, sp, direction, bg)
+    got = host(D.compose_hv(cu(g), cu(v), sp, 1.0, direction, bg))
+    assert np.array_equal(got, want)
+    want = oracle.compose_vh(v, g, sp, direction, bg)
+    got = host(D.compose_vh(cu(v), cu(g), sp, 1.0, direction, bg))
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("shape", SHAPES + [(64, 64, 64), (32, 48, 40)])
+@pytest.mark.parametrize("inverse", [True, False])
+def test_fluid_operator_vs_fp64(oracle, shape, inverse):
+    rng = np.random.default_rng(4)
+    sp = (1.0, 1.3, 0.8)
+    f = rng.normal(0, 1, (3,) + shape).astype(np.float32)
+    want = oracle.fluid_f64(f, sp, inverse=inverse)
+    op = DiffOperB200()
+    op.SetSize((shape[2], shape[1], shape[0]), sp, DiffOperParam())
+    v = cu(f)
+    (op.ApplyInverseOperator if inverse else op.ApplyOperator)(v)
+    got = host(v).astype(np.float64)
+    err = np.abs(got - want).max() / np.abs(want).max()
+    assert err <= 1e-5, err
+
+
+def test_fluid_roundtrip_identity():
+    """L^-1 L = I (DiffOperRoutineTests.cxx:120-203, sum of squared diff <= 0.1)."""
+    rng = np.random.default_rng(5)
+    shape = (32, 32, 32)
+    f = rng.normal(0, 1, (3,) + shape).astype(np.float32)
+    op = DiffOperB200()
+    op.SetSize((32, 32, 32), (1.0, 1.25, 1.0), DiffOperParam())
+    v = cu(f)
+    op.ApplyOperator(v)
+    op.ApplyInverseOperator(v)
+    d = host(v) - f
+    assert float((d.astype(np.float64) ** 2).sum()) <= 0.1
+
+
+def test_diffoper_rejects_unsupported():
+    op = DiffOperB200()
+    with pytest.raises(ValueError):
+        op.SetSize((16, 16, 16), (1, 1, 1), DiffOperParam(LPow=2.0))
+    with pytest.raises(ValueError):
+        op.SetSize((16, 16, 16), (1, 1, 1), DiffOperParam(DivergenceFree=True))
+
+
+@pytest.mark.parametrize("shape", [(16, 16, 16), (24, 20, 18)])
+@pytest.mark.parametrize("inverse", [False, True])
+def test_greedy_single_iterations(oracle, shape, inverse):
+    """Each Iterate from the same state as the oracle's (fields re-synchronised
+    every step, so only one step of FP32 FFT error separates them)."""
+    I0, I1 = greedy_pair(shape, seed=7, n_blobs=4, umax=2.0)
+    sp = (1.0, 1.0, 1.0)
+    nz, ny, nx = shape
+    it = GreedyIteratorB200((nx, ny, nz), spacing=sp)
+    it.SetScaleLevel((nx, ny, nz), sp, GreedyIteratorParam(DiffOperParam(), 0.5))
+    data = GreedyDeformationDataB200(cu(I0), cu(I1), sp, compute_inverse=inverse)
+    h = identity(shape)
+    hi = identity(shape) if inverse else None
+    step = 0.0
+    for k in range(4):
+        if k == 0:
+            it.UpdateStepSizeNextIteration()
+        e_o, step = oracle.greedy_iterate(I0, I1, h, hi, sp, max_pert=0.5,
+                                          update_step=(k == 0), step=step)
+        it.Iterate(data)
+        assert abs(it.StepSize() - step) <= 1e-5 * step
+        got = host(data.Def1To0())
+        assert np.abs(got - h).max() <= 1e-4
+        data.Def1To0().copy_(cu(h))  # re-sync
+        if inverse:
+            goti = host(data.Def0To1())
+            assert np.abs(goti - hi).max() <= 1e-4
+            data.Def0To1().copy_(cu(hi))
+        e_g = it.Energies()[-1]
+        assert abs(e_g - e_o) <= 1e-6 * max(1.0, e_o)
+
+
+def test_greedy_run_matches_oracle_64(oracle):
+    """Config-1 shape: 64^3, 50 iterations, MaxPert 0.5; final field within
+    1e-3 voxel RMS of the oracle."""
+    shape = (64, 64, 64)
+    I0, I1 = greedy_pair(shape, seed=11, n_blobs=8, umax=3.0)
+    h_o, _, e_o, step_o = oracle.greedy_run(I0, I1, 50, max_pert=0.5)
+    h_g, _, e_g, step_g = greedy_register(cu(I0), cu(I1), 50, max_pert=0.5)
+    h_g = host(h_g)
+    rms = float(np.sqrt(((h_g - h_o).astype(np.float64) ** 2).sum(0).mean()))
+    assert rms <= 1e-3, rms
+    assert len(e_g) == 50
+    assert np.allclose(e_g, e_o, rtol=1e-4)
+    assert abs(step_g - step_o) <= 1e-5 * step_o
+
+
+def test_greedy_run_iterate_equivalence():
+    """aw_greedy_run (graph replay) == repeated aw_greedy_iterate, bitwise."""
+    shape = (20, 18, 16)
+    I0, I1 = greedy_pair(shape, seed=3, n_blobs=4, umax=2.0)
+    sp = (1.0, 1.0, 1.0)
+    p = GreedyIteratorParam(DiffOperParam(), 0.5)
+    a = GreedyIteratorB200((16, 18, 20))
+    a.SetScaleLevel((16, 18, 20), sp, p)
+    da = GreedyDeformationDataB200(cu(I0), cu(I1), sp, True)
+    a.Run(da, 7, update_first=True)
+    b = GreedyIteratorB200((16, 18, 20))
+    b.SetScaleLevel((16, 18, 20), sp, p)
+    db = GreedyDeformationDataB200(cu(I0), cu(I1), sp, True)
+    for k in range(7):
+        if k == 0:
+            b.UpdateStepSizeNextIteration()
+        b.Iterate(db)
+    assert torch.equal(da.Def1To0(), db.Def1To0())
+    assert torch.equal(da.Def0To1(), db.Def0To1())
+    assert np.array_equal(a.Energies(), b.Energies())
+
+
+def test_greedy_deterministic():
+    shape = (32, 32, 32)
+    I0, I1 = greedy_pair(shape, seed=5)
+    r1 = greedy_register(cu(I0), cu(I1), 10)
+    r2 = greedy_register(cu(I0), cu(I1), 10)
+    assert torch.equal(r1[0], r2[0])
+    assert np.array_equal(r1[2], r2[2])
