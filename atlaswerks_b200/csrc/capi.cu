@@ -348,6 +348,42 @@ int aw_greedy_run(aw_greedy_t g, const float *I0, const float *I1, float *hx, fl
   return 0;
 }
 
+int aw_greedy_profile(aw_greedy_t g, const float *I0, const float *I1, const float *hx,
+                      const float *hy, const float *hz, float *ox, float *oy, float *oz,
+                      const float *hix, const float *hiy, const float *hiz, float *hiox,
+                      float *hioy, float *hioz, int reps, void *stream, float *ms_out) {
+  if (!g || !ms_out) return fail("aw_greedy_profile: null pointer");
+  if (!I0 || !I1 || !hx || !hy || !hz || !ox || !oy || !oz)
+    return fail("aw_greedy_profile: null pointer");
+  if (reps < 1) return fail("aw_greedy_profile: reps must be >= 1");
+  const bool inv = hix != nullptr;
+  const float *h[3] = {hx, hy, hz}, *hi[3] = {hix, hiy, hiz};
+  float *o[3] = {ox, oy, oz}, *hio[3] = {hiox, hioy, hioz};
+  cudaStream_t s = S(stream);
+  cudaEvent_t e0, e1;
+  AW_CUDA(cudaEventCreate(&e0), "aw_greedy_profile (event)");
+  AW_CUDA(cudaEventCreate(&e1), "aw_greedy_profile (event)");
+  int rc = 0;
+  for (int stage = 0; stage < aw::kNumStages && rc == 0; ++stage) {
+    cudaError_t e = cudaEventRecord(e0, s);
+    for (int r = 0; r < reps && e == cudaSuccess; ++r)
+      e = aw::greedy_stage(&g->ctx, stage, I0, I1, h, o, inv ? hi : nullptr, inv ? hio : nullptr,
+                           0, (r & 1) ? 0 : 1, s);
+    // an even number of solves leaves the spectrum at its original scale
+    if (e == cudaSuccess && stage == aw::kStageZSolve && (reps & 1))
+      e = aw::greedy_stage(&g->ctx, stage, I0, I1, h, o, nullptr, nullptr, 0, 0, s);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e != cudaSuccess) rc = cuda_fail(e, "aw_greedy_profile");
+    ms_out[stage] = ms / reps;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
 int aw_greedy_get_energies(aw_greedy_t g, double *out, int max_count, int *count) {
   if (!g || !count) return fail("aw_greedy_get_energies: null pointer");
   AW_CUDA(cudaDeviceSynchronize(), "aw_greedy_get_energies (pending work)");

@@ -146,6 +146,8 @@ int greedy_create(GreedyCtx *g, int nx, int ny, int nz, double spx, double spy, 
   g->max_pert = max_pert;
   const long n = g->d.n();
   g->nparts = grid_for(n);
+  g->sms = 148;
+  cudaDeviceGetAttribute(&g->sms, cudaDevAttrMultiProcessorCount, g->plan.device);
   g->st.cap = history_cap > 0 ? history_cap : 4096;
   if (cudaMalloc(&g->idef, sizeof(float) * n) != cudaSuccess) return 3;
   if (cudaMalloc(&g->vbuf, sizeof(float) * 3 * n) != cudaSuccess) return 3;
@@ -169,36 +171,60 @@ void greedy_destroy(GreedyCtx *g) {
   std::memset(g, 0, sizeof(*g));
 }
 
+cudaError_t greedy_stage(GreedyCtx *g, int stage, const float *I0, const float *I1,
+                         const float *const h[3], float *const h_out[3], const float *const hinv[3],
+                         float *const hinv_out[3], int auto_reduce, int solve_inverse,
+                         cudaStream_t s) {
+  const Dims d = g->d;
+  const long n = d.n();
+  float *v[3] = {g->vbuf, g->vbuf + n, g->vbuf + 2 * n};
+  switch (stage) {
+    case kStageForcePrep:
+      k_force_prep<<<g->nparts, kThreads, 0, s>>>(I0, I1, h[0], h[1], h[2], g->idef, g->partials, d);
+      return cudaGetLastError();
+    case kStageEnergy: {
+      const double spprod = g->sp.x * g->sp.y * g->sp.z;
+      k_energy_final<<<1, kThreads, 0, s>>>(g->partials, g->nparts, spprod, g->st, auto_reduce);
+      return cudaGetLastError();
+    }
+    case kStageXYForward:
+      return fluid_forward_force(g->plan, g->idef, I1, 1, s);
+    case kStageZSolve:
+      return fluid_solve(g->plan, solve_inverse, s);
+    case kStageXYInverse:
+      return fluid_inverse_store(g->plan, v[0], v[1], v[2], s);
+    case kStageMaxNorm: {
+      AW_TRY(cudaMemsetAsync(g->maxbits, 0, sizeof(unsigned), s));
+      k_max_norm<<<g->sms * 4, kThreads, 0, s>>>(v[0], v[1], v[2], n, g->maxbits);
+      AW_TRY(cudaGetLastError());
+      k_set_step<<<1, 1, 0, s>>>(g->maxbits, g->max_pert, g->st.step);
+      return cudaGetLastError();
+    }
+    case kStageUpdate: {
+      const bool inv = hinv && hinv[0] && hinv_out && hinv_out[0];
+      k_update<<<grid_for(n), kThreads, 0, s>>>(
+          h[0], h[1], h[2], v[0], v[1], v[2], h_out[0], h_out[1], h_out[2],
+          inv ? hinv[0] : nullptr, inv ? hinv[1] : nullptr, inv ? hinv[2] : nullptr,
+          inv ? hinv_out[0] : nullptr, inv ? hinv_out[1] : nullptr, inv ? hinv_out[2] : nullptr,
+          d, g->sp, g->st.step);
+      return cudaGetLastError();
+    }
+  }
+  return cudaErrorInvalidValue;
+}
+
 cudaError_t greedy_iterate(GreedyCtx *g, const float *I0, const float *I1, const float *const h[3],
                            float *const h_out[3], const float *const hinv[3],
                            float *const hinv_out[3], int update_step, int auto_reduce,
                            cudaStream_t s) {
-  const Dims d = g->d;
-  const long n = d.n();
-  float *v[3] = {g->vbuf, g->vbuf + n, g->vbuf + 2 * n};
-  k_force_prep<<<g->nparts, kThreads, 0, s>>>(I0, I1, h[0], h[1], h[2], g->idef, g->partials, d);
-  AW_TRY(cudaGetLastError());
-  const double spprod = g->sp.x * g->sp.y * g->sp.z;
-  k_energy_final<<<1, kThreads, 0, s>>>(g->partials, g->nparts, spprod, g->st, auto_reduce);
-  AW_TRY(cudaGetLastError());
-  AW_TRY(fluid_forward_force(g->plan, g->idef, I1, 1, s));
-  AW_TRY(fluid_solve(g->plan, 1, s));
-  AW_TRY(fluid_inverse_store(g->plan, v[0], v[1], v[2], s));
-  if (update_step) {
-    AW_TRY(cudaMemsetAsync(g->maxbits, 0, sizeof(unsigned), s));
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->plan.device);
-    k_max_norm<<<sms * 4, kThreads, 0, s>>>(v[0], v[1], v[2], n, g->maxbits);
-    AW_TRY(cudaGetLastError());
-    k_set_step<<<1, 1, 0, s>>>(g->maxbits, g->max_pert, g->st.step);
-    AW_TRY(cudaGetLastError());
-  }
-  const bool inv = hinv && hinv[0] && hinv_out && hinv_out[0];
-  k_update<<<grid_for(n), kThreads, 0, s>>>(
-      h[0], h[1], h[2], v[0], v[1], v[2], h_out[0], h_out[1], h_out[2], inv ? hinv[0] : nullptr,
-      inv ? hinv[1] : nullptr, inv ? hinv[2] : nullptr, inv ? hinv_out[0] : nullptr,
-      inv ? hinv_out[1] : nullptr, inv ? hinv_out[2] : nullptr, d, g->sp, g->st.step);
-  return cudaGetLastError();
+  AW_TRY(greedy_stage(g, kStageForcePrep, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
+  AW_TRY(greedy_stage(g, kStageEnergy, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
+  AW_TRY(greedy_stage(g, kStageXYForward, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
+  AW_TRY(greedy_stage(g, kStageZSolve, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
+  AW_TRY(greedy_stage(g, kStageXYInverse, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
+  if (update_step)
+    AW_TRY(greedy_stage(g, kStageMaxNorm, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
+  return greedy_stage(g, kStageUpdate, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s);
 }
 
 }  // namespace aw

@@ -22,14 +22,31 @@ struct GreedyCtx {
   float *vbuf;      // v = K f, 3N
   double *partials; // per-block energy sums
   int nparts;
+  int sms;
   char *scalars;    // step | count | maxbits
   unsigned *maxbits;
   GreedyDevState st;
 };
 
+// stages of one iteration, in launch order
+enum GreedyStage {
+  kStageForcePrep = 0,
+  kStageEnergy = 1,
+  kStageXYForward = 2,
+  kStageZSolve = 3,
+  kStageXYInverse = 4,
+  kStageMaxNorm = 5,
+  kStageUpdate = 6,
+  kNumStages = 7
+};
+
 int greedy_create(GreedyCtx *g, int nx, int ny, int nz, double spx, double spy, double spz,
                   float alpha, float beta, float gamma, float max_pert, int history_cap);
 void greedy_destroy(GreedyCtx *g);
+cudaError_t greedy_stage(GreedyCtx *g, int stage, const float *I0, const float *I1,
+                         const float *const h[3], float *const h_out[3], const float *const hinv[3],
+                         float *const hinv_out[3], int auto_reduce, int solve_inverse,
+                         cudaStream_t s);
 cudaError_t greedy_iterate(GreedyCtx *g, const float *I0, const float *I1, const float *const h[3],
                            float *const h_out[3], const float *const hinv[3],
                            float *const hinv_out[3], int update_step, int auto_reduce,

@@ -1,0 +1,396 @@
+#!/usr/bin/env python
+"""Benchmark: greedy-fluid registration iterations at 128^3 on B200.
+
+Metric: 128^3 fluid iterations/s (whole job, all ranks) with the achieved
+HBM GB/s of the dominant kernel against the measured B200 copy bandwidth.
+
+Workload (one "step"): every rank holds 4 independent 128^3 pairs resident
+in HBM (config-2 generator: 16 Gaussian blobs + N(0, 0.02^2) noise, smooth
+warp with max |u| = 6 voxels; alpha = beta = 0.01, gamma = 0.001,
+MaxPert 0.5) and runs 2 greedy iterations on each pair, so a step is 8
+iterations. The 4 pairs' working sets (~120 MB each) exceed the 126 MB L2,
+so consecutive steps find none of their data in L2.
+
+Pair registrations are independent: with N GPUs every rank runs its own
+pairs (replicas, weak scaling); the only collective is the max of the
+per-rank device times.
+
+--impl reference times the reference's own CPU implementation
+(GreedyIteratorCPU, built from its sources into oracle/_ref) on the host
+cores, one 128^3 pair per thread.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 128
+PAIRS = 4
+ITERS_PER_PAIR = 2
+ALPHA, BETA, GAMMA, MAX_PERT = 0.01, 0.01, 0.001, 0.5
+E2E_ITERS = 25  # the 128^3 level of the 3-level multiscale config
+
+# algorithmic HBM bytes per voxel of each kernel of one iteration (minimum
+# traffic of that kernel's function; spectrum = 3 complex64 x (nx/2+1)/nx)
+SPEC = 3 * 8 * (N // 2 + 1) / N  # bytes/voxel of the 3-channel half spectrum
+STAGE_NAMES = ["force_prep", "energy", "xy_forward_fft", "z_solve", "xy_inverse_fft",
+               "max_norm", "update"]
+STAGE_BYTES = {
+    "force_prep": 12 + 4 + 4 + 4,        # h, I1, I0 gather (once), I0(h) write
+    "energy": 0,
+    "xy_forward_fft": 4 + 4 + SPEC,      # I0(h), I1, spectrum write
+    "z_solve": 2 * SPEC,                 # spectrum read + write
+    "xy_inverse_fft": SPEC + 12,         # spectrum read, v write
+    "max_norm": 12,
+    "update": 12 + 12 + 12,              # v, h gather (once), h' write
+}
+B_ITER = 92  # bytes/voxel of the fully fused 3-pass iteration (the survey's B_greedy)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200",
+                                          "-i", str(self.index)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_iteration_rate(I0, I1, iters=2):
+    """Reference CPU (oracle/_ref) or, without it, the oracle port: 128^3
+    greedy iterations on one host thread. Returns (iters/s, kind)."""
+    import numpy as np  # noqa: F401
+    from oracle import REF_SO, Oracle, Reference
+    if os.path.exists(REF_SO):
+        ref = Reference()
+        t = time.perf_counter()
+        ref.greedy_run(I0, I1, [1], [iters], [MAX_PERT], alpha=ALPHA, beta=BETA, gamma=GAMMA)
+        return iters / (time.perf_counter() - t), "reference"
+    o = Oracle()
+    t = time.perf_counter()
+    o.greedy_run(I0, I1, iters, max_pert=MAX_PERT, alpha=ALPHA, beta=BETA, gamma=GAMMA)
+    return iters / (time.perf_counter() - t), "port"
+
+
+def make_pair(seed):
+    from atlaswerks_b200.synth import greedy_pair
+    return greedy_pair((N, N, N), seed, n_blobs=16, umax=6.0, noise_sd=0.02)
+
+
+def config(extra=None):
+    c = {"workload": f"greedy-fluid pair registration, {N}^3 float32, single scale "
+                     f"(finest level of the 3-level config), {PAIRS} resident pairs x "
+                     f"{ITERS_PER_PAIR} iterations per step",
+         "grid": [N, N, N], "alpha": ALPHA, "beta": BETA, "gamma": GAMMA, "max_pert": MAX_PERT,
+         "pairs_per_rank": PAIRS, "iterations_per_step_per_rank": PAIRS * ITERS_PER_PAIR,
+         "l2": "inputs larger than L2: 4 pairs x ~120 MB working set, round-robin",
+         "inverse_field": False}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def run_reference(args):
+    """CPU reference arm: all host threads (one 128^3 pair each, capped at 32
+    for memory), the reference's GreedyIteratorCPU through oracle/_ref."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import REF_SO, Oracle, Reference
+    kind = "reference" if os.path.exists(REF_SO) else "port"
+    cores = max(1, min(os.cpu_count() or 1, 32))
+    pairs = [make_pair(1000 + t) for t in range(cores)]
+
+    def worker(t, n_iters, out):
+        I0, I1 = pairs[t]
+        if kind == "reference":
+            Reference().greedy_run(I0, I1, [1], [n_iters], [MAX_PERT], alpha=ALPHA, beta=BETA,
+                                   gamma=GAMMA)
+        else:
+            Oracle().greedy_run(I0, I1, n_iters, max_pert=MAX_PERT, alpha=ALPHA, beta=BETA,
+                                gamma=GAMMA)
+        out[t] = n_iters
+
+    def one_step():
+        out = [0] * cores
+        th = [threading.Thread(target=worker, args=(t, 1, out)) for t in range(cores)]
+        for x in th:
+            x.start()
+        for x in th:
+            x.join()
+        return sum(out)
+
+    for _ in range(min(args.warmup, 1)):
+        one_step()
+    t = time.perf_counter()
+    done = 0
+    for _ in range(args.steps):
+        done += one_step()
+    dt = time.perf_counter() - t
+    value = done / dt
+    line = {"metric": "128^3 fluid iters/s", "value": value, "unit": "iters/s",
+            "impl": "reference", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+            "steps": args.steps, "warmup": min(args.warmup, 1),
+            "ms_per_step": 1000 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded blobs + smooth warp)",
+            "config": config({"pairs_per_rank": cores, "iterations_per_step_per_rank": cores,
+                              "workload": f"greedy-fluid pair registration, {N}^3 float32, one "
+                                          f"iteration of one pair per host thread per step"}),
+            "cpu_baseline": {"value": value, "unit": "iters/s", "cores": cores, "kind": kind,
+                             "sample": f"{args.steps} steps x {cores} threads x 1 iteration of "
+                                       f"a {N}^3 pair (GreedyIteratorCPU; FFT = FP64 shim, "
+                                       f"not FFTW)"},
+            "e2e": {"value": value, "unit": "iters/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_b200(args):
+    import numpy as np
+    import torch
+
+    from atlaswerks_b200 import _lib
+    from atlaswerks_b200.greedy import (DiffOperParam, GreedyDeformationDataB200,
+                                        GreedyIteratorB200, GreedyIteratorParam)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    _lib.lib()
+    param = GreedyIteratorParam(DiffOperParam(ALPHA, BETA, GAMMA), MAX_PERT)
+    iters, datas = [], []
+    host_pairs = []
+    for p in range(PAIRS):
+        I0, I1 = make_pair(rank * 100 + p)
+        host_pairs.append((I0, I1))
+        it = GreedyIteratorB200((N, N, N))
+        it.SetScaleLevel((N, N, N), (1.0, 1.0, 1.0), param)
+        d = GreedyDeformationDataB200(torch.from_numpy(I0).cuda(), torch.from_numpy(I1).cuda())
+        it.Run(d, 1, update_first=True)
+        iters.append(it)
+        datas.append(d)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        for it, d in zip(iters, datas):
+            it.Run(d, ITERS_PER_PAIR, update_first=False)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        end.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = start.elapsed_time(end)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    per_rank_iters = args.steps * PAIRS * ITERS_PER_PAIR
+    value = world * per_rank_iters / (ms / 1000.0)
+    ms_per_step = ms / args.steps
+    ms_per_iter = ms / per_rank_iters
+
+    # --- per-kernel roofline (pair 0, each stage timed alone with events) ---
+    peak, peak_kind = peaks()
+    it0, d0 = iters[0], datas[0]
+    h, ho = d0.Def1To0(), d0._next()[0]
+    ms7 = (ctypes.c_float * 7)()
+    z = [None, None, None]
+    _lib.check(_lib.lib().aw_greedy_profile(
+        it0._h, d0.I0.data_ptr(), d0.I1.data_ptr(), *[t.data_ptr() for t in h],
+        *[t.data_ptr() for t in ho], *z, *z, 20, stream.cuda_stream, ms7))
+    stage_ms = {n: float(ms7[i]) for i, n in enumerate(STAGE_NAMES)}
+    per_iter_stages = [n for n in STAGE_NAMES if n != "max_norm"]
+    dom = max(per_iter_stages, key=lambda n: stage_ms[n])
+    nvox = N ** 3
+    dom_bytes = STAGE_BYTES[dom] * nvox
+    achieved = dom_bytes / (stage_ms[dom] / 1000.0) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "greedy_128_dram_traffic.json")
+    if os.path.exists(tfile):
+        traffic = json.load(open(tfile)).get(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                "algorithmic_bytes_per_launch": dom_bytes,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)"
+                if peak_kind == "measured" else "fallback 6.65 TB/s"}
+    iter_gbs = B_ITER * nvox / (ms_per_iter / 1000.0) / 1e9
+    iteration_roofline = {"bytes_per_iteration": B_ITER * nvox, "achieved": iter_gbs,
+                          "peak": peak, "unit": "GB/s", "frac": iter_gbs / peak,
+                          "stage_ms": stage_ms}
+
+    # --- end to end through the public API with host buffers ---
+    e2e = None
+    if rank == 0 or world > 1:
+        I0h = torch.from_numpy(host_pairs[0][0]).pin_memory()
+        I1h = torch.from_numpy(host_pairs[0][1]).pin_memory()
+        hh = torch.empty((3, N, N, N), dtype=torch.float32).pin_memory()
+        I0d = torch.empty((N, N, N), device="cuda")
+        I1d = torch.empty((N, N, N), device="cuda")
+        it = GreedyIteratorB200((N, N, N))
+        it.SetScaleLevel((N, N, N), (1.0, 1.0, 1.0), param)
+        de = GreedyDeformationDataB200(I0d, I1d)
+
+        def e2e_step():
+            I0d.copy_(I0h, non_blocking=True)
+            I1d.copy_(I1h, non_blocking=True)
+            de._cur = 0
+            de._h[0].copy_(_identity(N))
+            it.Run(de, E2E_ITERS, update_first=True)
+            hh.copy_(de.Def1To0(), non_blocking=True)
+
+        ident = {}
+
+        def _identity(n):
+            if n not in ident:
+                from atlaswerks_b200.device import identity
+                ident[n] = identity((n, n, n))
+            return ident[n]
+
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        reps = 3
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(reps):
+            e2e_step()
+        s1.record(stream)
+        torch.cuda.synchronize()
+        ems = s0.elapsed_time(s1) / reps
+        e2e_val = E2E_ITERS / (ems / 1000.0)
+        if dist:
+            t = torch.tensor([ems], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_val = world * E2E_ITERS / (float(t.item()) / 1000.0)
+        e2e = {"value": e2e_val, "unit": "iters/s", "h2d_bytes_per_step": 2 * 4 * nvox,
+               "d2h_bytes_per_step": 3 * 4 * nvox,
+               "step": f"H2D of I0, I1 (pinned) + identity init + {E2E_ITERS}-iteration "
+                       f"registration (step update at iteration 0) + D2H of h, "
+                       f"via GreedyIteratorB200.Run"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, kind = cpu_reference_iteration_rate(*host_pairs[0], iters=2)
+        cpu = {"value": rate, "unit": "iters/s", "cores": 1, "kind": kind,
+               "sample": f"2 greedy iterations of one {N}^3 pair on 1 host thread "
+                         f"(GreedyIteratorCPU{'' if kind == 'reference' else ' port'}; FFT = "
+                         f"FP64 shim, not FFTW)"}
+
+    launches_per_iter = 6
+    line = {"metric": "128^3 fluid iters/s", "value": value, "unit": "iters/s",
+            "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
+            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Gaussian blobs + smooth random warp, no dataset)",
+            "config": config(), "roofline": roofline,
+            "iteration_roofline": iteration_roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches_per_iter * per_rank_iters,
+            "clocks": clk.summary()}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -127,6 +127,16 @@ int aw_greedy_run(aw_greedy_t g, const float *I0, const float *I1, float *hx, fl
                   float *six, float *siy, float *siz, int n_iters, int update_first,
                   void *stream);
 
+/* Per-kernel device time of one iteration: each stage (0 force-prep,
+ * 1 energy, 2 xy-forward FFT, 3 z-solve, 4 xy-inverse FFT, 5 max-norm,
+ * 6 update) is launched `reps` times back to back between CUDA events on
+ * `stream`; ms_out[7] receives the mean milliseconds per launch. Leaves h_out
+ * holding one iteration's result; records extra energies. Synchronises. */
+int aw_greedy_profile(aw_greedy_t g, const float *I0, const float *I1, const float *hx,
+                      const float *hy, const float *hz, float *ox, float *oy, float *oz,
+                      const float *hix, const float *hiy, const float *hiz, float *hiox,
+                      float *hioy, float *hioz, int reps, void *stream, float *ms_out);
+
 /* Copies the energy history (oldest first) to host; synchronises. */
 int aw_greedy_get_energies(aw_greedy_t g, double *out, int max_count, int *count);
 

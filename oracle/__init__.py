@@ -16,9 +16,12 @@ Two libraries are wrapped, both taking planar float32 numpy arrays:
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import os
 import subprocess
+import sys
+import threading
 from typing import Optional, Sequence
 
 import numpy as np
@@ -170,6 +173,37 @@ class Oracle:
         return h, hinv, np.array(energies), step
 
 
+_quiet_lock = threading.Lock()
+_quiet_depth = 0
+_quiet_saved = None
+
+
+@contextlib.contextmanager
+def quiet_stdout():
+    """Send fd 1 to /dev/null while the reference code runs: its parameter
+    parser prints diagnostics on std::cout. Re-entrant across threads."""
+    global _quiet_depth, _quiet_saved
+    with _quiet_lock:
+        if _quiet_depth == 0:
+            sys.stdout.flush()
+            _quiet_saved = os.dup(1)
+            devnull = os.open(os.devnull, os.O_WRONLY)
+            os.dup2(devnull, 1)
+            os.close(devnull)
+        _quiet_depth += 1
+    try:
+        yield
+    finally:
+        with _quiet_lock:
+            _quiet_depth -= 1
+            if _quiet_depth == 0:
+                libc = ctypes.CDLL(None)
+                libc.fflush(None)
+                os.dup2(_quiet_saved, 1)
+                os.close(_quiet_saved)
+                _quiet_saved = None
+
+
 class Reference:
     """ctypes wrapper of the reference's own CPU code (oracle/_ref/libawref.so)."""
 
@@ -245,9 +279,11 @@ class Reference:
         steps = np.zeros(total, np.float32)
         hi = np.ascontiguousarray(h_init, np.float32) if h_init is not None else None
         hii = np.ascontiguousarray(hinv_init, np.float32) if hinv_init is not None else None
-        self._check(self.lib.awref_greedy_run(
+        with quiet_stdout():
+            rc = self.lib.awref_greedy_run(
             _fp(I0), _fp(I1), *_shape(I0), *map(_dbl, sp), _i(ns), fa, it, mp, _dbl(alpha),
             _dbl(beta), _dbl(gamma), _i(int(inverse)), _fp(hi), _fp(hii),
             ctypes.c_float(init_step), _i(int(skip_step_update)), _fp(h), _fp(hinv), _dp(en),
-            _fp(steps)))
+            _fp(steps))
+        self._check(rc)
         return h, hinv, en, steps
