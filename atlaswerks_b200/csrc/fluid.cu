@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "fluid.cuh"
+#include "fluid_fast.cuh"
 
 namespace aw {
 
@@ -258,7 +259,15 @@ int fluid_plan_create(FluidPlan *p, int nx, int ny, int nz, double spx, double s
   cudaGetDevice(&dev);
   p->device = dev;
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  if (p->smem_xy > (size_t)maxsm || p->smem_z > (size_t)maxsm) return 2;
+  if (fast_supported(nx) && fast_supported(ny) && fast_supported(nz)) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    p->fast_kq = fast_z_kq(*p, sms);
+    p->fast_smem_xy = fast_xy_smem(nx, ny);
+    p->fast_smem_z = fast_z_smem(nz, p->fast_kq);
+    p->fast = p->fast_smem_xy <= (size_t)maxsm && p->fast_smem_z <= (size_t)maxsm;
+  }
+  if (!p->fast && (p->smem_xy > (size_t)maxsm || p->smem_z > (size_t)maxsm)) return 2;
 
   std::vector<float2> tw;
   fill_twiddles(nx, tw);
@@ -282,6 +291,7 @@ int fluid_plan_create(FluidPlan *p, int nx, int ny, int nz, double spx, double s
       set_smem(k_fft_xy_inv<DstAxpby>, p->smem_xy) != cudaSuccess ||
       set_smem(k_fft_z_solve, p->smem_z) != cudaSuccess)
     return 4;
+  if (p->fast && fast_configure(*p) != cudaSuccess) return 4;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
@@ -295,6 +305,7 @@ void fluid_plan_destroy(FluidPlan *p) {
 cudaError_t fluid_forward_field(const FluidPlan &p, const float *fx, const float *fy,
                                 const float *fz, cudaStream_t s) {
   SrcField src{{fx, fy, fz}};
+  if (p.fast) return fast_xy_forward(p, src, s);
   k_fft_xy_fwd<SrcField><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, src);
   return cudaGetLastError();
 }
@@ -302,11 +313,13 @@ cudaError_t fluid_forward_field(const FluidPlan &p, const float *fx, const float
 cudaError_t fluid_forward_force(const FluidPlan &p, const float *G, const float *A, int diff,
                                 cudaStream_t s) {
   SrcForce src{G, A, diff, p.sp};
+  if (p.fast) return fast_xy_forward(p, src, s);
   k_fft_xy_fwd<SrcForce><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, src);
   return cudaGetLastError();
 }
 
 cudaError_t fluid_solve(const FluidPlan &p, int inverse, cudaStream_t s) {
+  if (p.fast) return fast_z_solve(p, inverse, s);
   const long ncols = (long)p.d.ny * p.nxh;
   const int grid = (int)((ncols + p.zcols_per_cta - 1) / p.zcols_per_cta);
   k_fft_z_solve<<<grid, 256, p.smem_z, s>>>(p, inverse);
@@ -316,6 +329,7 @@ cudaError_t fluid_solve(const FluidPlan &p, int inverse, cudaStream_t s) {
 cudaError_t fluid_inverse_store(const FluidPlan &p, float *ox, float *oy, float *oz,
                                 cudaStream_t s) {
   DstField dst{{ox, oy, oz}};
+  if (p.fast) return fast_xy_inverse(p, dst, s);
   k_fft_xy_inv<DstField><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, dst);
   return cudaGetLastError();
 }
@@ -323,6 +337,7 @@ cudaError_t fluid_inverse_store(const FluidPlan &p, float *ox, float *oy, float 
 cudaError_t fluid_inverse_axpby(const FluidPlan &p, float *vx, float *vy, float *vz, float vfac,
                                 float ufac, cudaStream_t s) {
   DstAxpby dst{{vx, vy, vz}, vfac, ufac};
+  if (p.fast) return fast_xy_inverse(p, dst, s);
   k_fft_xy_inv<DstAxpby><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, dst);
   return cudaGetLastError();
 }

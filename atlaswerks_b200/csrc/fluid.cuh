@@ -33,6 +33,10 @@ struct FluidPlan {
   int pairs_per_batch, cols_per_batch, zcols_per_cta;
   size_t smem_xy, smem_z;
   int device;
+  // register-FFT path (fluid_fast.cu): power-of-two axes
+  int fast;
+  int fast_kq;
+  size_t fast_smem_xy, fast_smem_z;
 };
 
 // --- producers for the forward pass ----------------------------------------

@@ -70,7 +70,13 @@ def test_compose_bit_exact(oracle, bg, direction):
     assert np.array_equal(got, want)
 
 
-@pytest.mark.parametrize("shape", SHAPES + [(64, 64, 64), (32, 48, 40)])
+# power-of-two grids take the register-FFT kernels, the others the generic
+# shared-memory Stockham kernels
+FLUID_SHAPES = SHAPES + [(64, 64, 64), (32, 48, 40), (128, 128, 128), (32, 64, 128),
+                         (128, 16, 64), (16, 32, 16), (256, 32, 16)]
+
+
+@pytest.mark.parametrize("shape", FLUID_SHAPES)
 @pytest.mark.parametrize("inverse", [True, False])
 def test_fluid_operator_vs_fp64(oracle, shape, inverse):
     rng = np.random.default_rng(4)
