@@ -29,6 +29,24 @@ struct Spacing {
   double x, y, z;
 };
 
+// Elementwise launch shape: 128 threads along x, one grid row per (y, z), so
+// a thread finds its voxel without any integer division.
+constexpr int kRowThreads = 128;
+inline dim3 row_grid(const Dims &d) {
+  return dim3((unsigned)((d.nx + kRowThreads - 1) / kRowThreads), (unsigned)d.ny, (unsigned)d.nz);
+}
+struct Voxel {
+  int x, y, z;
+  long i;
+};
+AW_D bool voxel_of(const Dims &d, Voxel &v) {
+  v.x = blockIdx.x * kRowThreads + threadIdx.x;
+  v.y = blockIdx.y;
+  v.z = blockIdx.z;
+  v.i = ((long)v.z * d.ny + v.y) * d.nx + v.x;
+  return v.x < d.nx;
+}
+
 // ---- exact-rounding arithmetic -------------------------------------------
 AW_D double dmul(double a, double b) { return __dmul_rn(a, b); }
 AW_D double dadd(double a, double b) { return __dadd_rn(a, b); }

@@ -25,27 +25,29 @@ namespace {
 
 constexpr int kThreads = 256;
 
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kRowThreads)
     k_force_prep(const float *__restrict__ I0, const float *__restrict__ I1,
                  const float *__restrict__ hx, const float *__restrict__ hy,
                  const float *__restrict__ hz, float *__restrict__ idef, double *__restrict__ partials,
                  Dims d) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  Voxel vox;
   double e = 0.0;
-  if (i < d.n()) {
+  if (voxel_of(d, vox)) {
+    const long i = vox.i;
     const float v = trilerp_scalar(I0, d, (double)hx[i], (double)hy[i], (double)hz[i], 0.0f);
     idef[i] = v;
     const float r = -fsub(v, I1[i]);
     e = (double)r * (double)r;
   }
-  __shared__ double ws[kThreads / 32];
+  __shared__ double ws[kRowThreads / 32];
   e = warp_sum(e);
   if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = e;
   __syncthreads();
   if (threadIdx.x < 32) {
-    double t = threadIdx.x < kThreads / 32 ? ws[threadIdx.x] : 0.0;
+    double t = threadIdx.x < kRowThreads / 32 ? ws[threadIdx.x] : 0.0;
     t = warp_sum(t);
-    if (threadIdx.x == 0) partials[blockIdx.x] = t;
+    if (threadIdx.x == 0)
+      partials[((long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = t;
   }
 }
 
@@ -94,19 +96,18 @@ __global__ void k_set_step(const unsigned *__restrict__ maxbits, float max_pert,
 // composeHV(h, eps*v, PARTIAL_ID) and, when hinv is given,
 // composeVHInv(eps*v, hinv, PARTIAL_ZERO) — GreedyIteratorCPU::updateDeformation
 // (GreedyIteratorCPU.cxx:83-95), both from one read of v.
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kRowThreads)
     k_update(const float *__restrict__ hx, const float *__restrict__ hy, const float *__restrict__ hz,
              const float *__restrict__ vx, const float *__restrict__ vy, const float *__restrict__ vz,
              float *__restrict__ ox, float *__restrict__ oy, float *__restrict__ oz,
              const float *__restrict__ gx, const float *__restrict__ gy, const float *__restrict__ gz,
              float *__restrict__ qx, float *__restrict__ qy, float *__restrict__ qz, Dims d,
              Spacing sp, const float *__restrict__ step_ptr) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.n()) return;
+  Voxel vox;
+  if (!voxel_of(d, vox)) return;
+  const long i = vox.i;
+  const int x = vox.x, y = vox.y, z = vox.z;
   const float eps = *step_ptr;
-  const int x = (int)(i % d.nx);
-  const int y = (int)((i / d.nx) % d.ny);
-  const int z = (int)(i / ((long)d.nx * d.ny));
   const float sx = (float)sp.x, sy = (float)sp.y, sz = (float)sp.z;
   const float px = fadd(__int2float_rn(x), fdiv(fmul(vx[i], eps), sx));
   const float py = fadd(__int2float_rn(y), fdiv(fmul(vy[i], eps), sy));
@@ -145,7 +146,10 @@ int greedy_create(GreedyCtx *g, int nx, int ny, int nz, double spx, double spy, 
   g->sp = g->plan.sp;
   g->max_pert = max_pert;
   const long n = g->d.n();
-  g->nparts = grid_for(n);
+  {
+    const dim3 gr = row_grid(g->d);
+    g->nparts = (int)(gr.x * gr.y * gr.z);
+  }
   g->sms = 148;
   cudaDeviceGetAttribute(&g->sms, cudaDevAttrMultiProcessorCount, g->plan.device);
   g->st.cap = history_cap > 0 ? history_cap : 4096;
@@ -180,7 +184,7 @@ cudaError_t greedy_stage(GreedyCtx *g, int stage, const float *I0, const float *
   float *v[3] = {g->vbuf, g->vbuf + n, g->vbuf + 2 * n};
   switch (stage) {
     case kStageForcePrep:
-      k_force_prep<<<g->nparts, kThreads, 0, s>>>(I0, I1, h[0], h[1], h[2], g->idef, g->partials, d);
+      k_force_prep<<<row_grid(d), kRowThreads, 0, s>>>(I0, I1, h[0], h[1], h[2], g->idef, g->partials, d);
       return cudaGetLastError();
     case kStageEnergy: {
       const double spprod = g->sp.x * g->sp.y * g->sp.z;
@@ -202,7 +206,7 @@ cudaError_t greedy_stage(GreedyCtx *g, int stage, const float *I0, const float *
     }
     case kStageUpdate: {
       const bool inv = hinv && hinv[0] && hinv_out && hinv_out[0];
-      k_update<<<grid_for(n), kThreads, 0, s>>>(
+      k_update<<<row_grid(d), kRowThreads, 0, s>>>(
           h[0], h[1], h[2], v[0], v[1], v[2], h_out[0], h_out[1], h_out[2],
           inv ? hinv[0] : nullptr, inv ? hinv[1] : nullptr, inv ? hinv[2] : nullptr,
           inv ? hinv_out[0] : nullptr, inv ? hinv_out[1] : nullptr, inv ? hinv_out[2] : nullptr,

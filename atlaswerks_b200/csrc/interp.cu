@@ -12,16 +12,15 @@ namespace aw {
 
 namespace {
 
-constexpr int kThreads = 256;
-
-inline int grid_for(long n) { return (int)((n + kThreads - 1) / kThreads); }
+constexpr int kThreads = kRowThreads;
 
 // HField3DUtils::apply (UtilitiesDataTypes/HField3DUtils.txx:734-752)
 __global__ void __launch_bounds__(kThreads)
     k_apply(const float *__restrict__ img, const float *__restrict__ hx, const float *__restrict__ hy,
             const float *__restrict__ hz, float *__restrict__ out, Dims d, float bg) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.n()) return;
+  Voxel vx;
+  if (!voxel_of(d, vx)) return;
+  const long i = vx.i;
   out[i] = trilerp_scalar(img, d, (double)hx[i], (double)hy[i], (double)hz[i], bg);
 }
 
@@ -29,12 +28,10 @@ __global__ void __launch_bounds__(kThreads)
 __global__ void __launch_bounds__(kThreads)
     k_gradient(const float *__restrict__ a, float *__restrict__ gx, float *__restrict__ gy,
                float *__restrict__ gz, Dims d, Spacing sp, int wrap) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.n()) return;
-  const int x = (int)(i % d.nx);
-  const int y = (int)((i / d.nx) % d.ny);
-  const int z = (int)(i / ((long)d.nx * d.ny));
-  const int pos[3] = {x, y, z};
+  Voxel vx;
+  if (!voxel_of(d, vx)) return;
+  const long i = vx.i;
+  const int pos[3] = {vx.x, vx.y, vx.z};
   const int n[3] = {d.nx, d.ny, d.nz};
   const long stride[3] = {1, d.nx, (long)d.nx * d.ny};
   const double s[3] = {sp.x, sp.y, sp.z};
@@ -64,12 +61,11 @@ __global__ void __launch_bounds__(kThreads)
                  const float *__restrict__ vx, const float *__restrict__ vy, const float *__restrict__ vz,
                  float *__restrict__ ox, float *__restrict__ oy, float *__restrict__ oz, Dims d,
                  Spacing sp, int dir, int bgs, const float *__restrict__ scale_ptr, float scale_val) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.n()) return;
+  Voxel vox;
+  if (!voxel_of(d, vox)) return;
+  const long i = vox.i;
+  const int x = vox.x, y = vox.y, z = vox.z;
   const float scale = scale_ptr ? *scale_ptr : scale_val;
-  const int x = (int)(i % d.nx);
-  const int y = (int)((i / d.nx) % d.ny);
-  const int z = (int)(i / ((long)d.nx * d.ny));
   const float dx = fdiv(fmul(vx[i], scale), (float)sp.x);
   const float dy = fdiv(fmul(vy[i], scale), (float)sp.y);
   const float dz = fdiv(fmul(vz[i], scale), (float)sp.z);
@@ -93,8 +89,9 @@ __global__ void __launch_bounds__(kThreads)
                  const float *__restrict__ gx, const float *__restrict__ gy, const float *__restrict__ gz,
                  float *__restrict__ ox, float *__restrict__ oy, float *__restrict__ oz, Dims d,
                  Spacing sp, int dir, int bgs, const float *__restrict__ scale_ptr, float scale_val) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.n()) return;
+  Voxel vox;
+  if (!voxel_of(d, vox)) return;
+  const long i = vox.i;
   const float scale = scale_ptr ? *scale_ptr : scale_val;
   const float g0 = gx[i], g1 = gy[i], g2 = gz[i];
   float hx, hy, hz;
@@ -114,20 +111,20 @@ __global__ void __launch_bounds__(kThreads)
 
 cudaError_t launch_apply(const float *img, const float *hx, const float *hy, const float *hz,
                          float *out, Dims d, float bg, cudaStream_t s) {
-  k_apply<<<grid_for(d.n()), kThreads, 0, s>>>(img, hx, hy, hz, out, d, bg);
+  k_apply<<<row_grid(d), kThreads, 0, s>>>(img, hx, hy, hz, out, d, bg);
   return cudaGetLastError();
 }
 
 cudaError_t launch_gradient(const float *a, float *gx, float *gy, float *gz, Dims d, Spacing sp,
                             int wrap, cudaStream_t s) {
-  k_gradient<<<grid_for(d.n()), kThreads, 0, s>>>(a, gx, gy, gz, d, sp, wrap);
+  k_gradient<<<row_grid(d), kThreads, 0, s>>>(a, gx, gy, gz, d, sp, wrap);
   return cudaGetLastError();
 }
 
 cudaError_t launch_compose_hv(const float *const g[3], const float *const v[3], float *const o[3],
                               Dims d, Spacing sp, int dir, int bgs, const float *scale_ptr,
                               float scale_val, cudaStream_t s) {
-  k_compose_hv<<<grid_for(d.n()), kThreads, 0, s>>>(g[0], g[1], g[2], v[0], v[1], v[2], o[0], o[1],
+  k_compose_hv<<<row_grid(d), kThreads, 0, s>>>(g[0], g[1], g[2], v[0], v[1], v[2], o[0], o[1],
                                                     o[2], d, sp, dir, bgs, scale_ptr, scale_val);
   return cudaGetLastError();
 }
@@ -135,7 +132,7 @@ cudaError_t launch_compose_hv(const float *const g[3], const float *const v[3], 
 cudaError_t launch_compose_vh(const float *const v[3], const float *const g[3], float *const o[3],
                               Dims d, Spacing sp, int dir, int bgs, const float *scale_ptr,
                               float scale_val, cudaStream_t s) {
-  k_compose_vh<<<grid_for(d.n()), kThreads, 0, s>>>(v[0], v[1], v[2], g[0], g[1], g[2], o[0], o[1],
+  k_compose_vh<<<row_grid(d), kThreads, 0, s>>>(v[0], v[1], v[2], g[0], g[1], g[2], o[0], o[1],
                                                     o[2], d, sp, dir, bgs, scale_ptr, scale_val);
   return cudaGetLastError();
 }
