@@ -45,6 +45,7 @@ SIGNATURES = {
     "aw_gradient": ([_fp] * 4 + [_i] * 3 + [_d] * 3 + [_i, _fp], _i),
     "aw_compose_hv": ([_fp] * 9 + [_i] * 3 + [_d] * 3 + [_f, _i, _i, _fp], _i),
     "aw_compose_vh": ([_fp] * 9 + [_i] * 3 + [_d] * 3 + [_f, _i, _i, _fp], _i),
+    "aw_splat": ([_fp] * 5 + [_i] * 3 + [_f, _fp], _i),
     "aw_fluid_create": ([_i] * 3 + [_d] * 3 + [_f] * 3 + [_fp], _i),
     "aw_fluid_apply": ([_fp] * 4 + [_i, _fp], _i),
     "aw_fluid_destroy": ([_fp], _i),
@@ -57,6 +58,13 @@ SIGNATURES = {
     "aw_greedy_run": ([_fp] * 15 + [_i, _i, _fp], _i),
     "aw_greedy_profile": ([_fp] * 15 + [_i, _fp, _fp], _i),
     "aw_greedy_get_energies": ([_fp, _fp, _i, _fp], _i),
+    "aw_ldmm_create": ([_i] * 3 + [_d] * 3 + [_f] * 3 + [_i, _f, _f, _fp], _i),
+    "aw_ldmm_destroy": ([_fp], _i),
+    "aw_ldmm_set_step": ([_fp, _f], _i),
+    "aw_ldmm_get_step": ([_fp, _fp], _i),
+    "aw_ldmm_iterate": ([_fp] * 4 + [_i, _fp], _i),
+    "aw_ldmm_run": ([_fp] * 4 + [_i, _i, _fp], _i),
+    "aw_ldmm_get_energies": ([_fp, _fp, _i, _fp], _i),
 }
 
 

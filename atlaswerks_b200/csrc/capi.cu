@@ -13,6 +13,8 @@
 #include "../../include/aw_b200.h"
 #include "greedy.cuh"
 #include "interp.cuh"
+#include "ldmm.cuh"
+#include "splat.cuh"
 
 namespace {
 
@@ -73,6 +75,13 @@ struct GraphKey {
       if (p[i] != o.p[i]) return p[i] < o.p[i];
     return n < o.n;
   }
+};
+
+struct aw_ldmm_s {
+  aw::LdmmCtx ctx;
+  cudaStream_t gstream = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  std::map<std::pair<const void *, const void *>, std::pair<const void *, cudaGraphExec_t>> graphs;
 };
 
 struct aw_greedy_s {
@@ -142,6 +151,24 @@ int aw_compose_vh(const float *vx, const float *vy, const float *vz, const float
   AW_CUDA(aw::launch_compose_vh(v, g, o, aw::Dims{nx, ny, nz}, aw::Spacing{spx, spy, spz},
                                 direction >= 0 ? 1 : -1, background, nullptr, scale, S(stream)),
           "aw_compose_vh");
+  return 0;
+}
+
+int aw_splat(const float *img, const float *hx, const float *hy, const float *hz, float *out,
+             int nx, int ny, int nz, float background, void *stream) {
+  if (!img || !hx || !hy || !hz || !out) return fail("aw_splat: null pointer");
+  if (nx < 1 || ny < 1 || nz < 1) return fail("aw_splat: empty grid");
+  if ((long)(nx + 1) * (ny + 1) * (nz + 1) >= (1L << 31))
+    return fail("aw_splat: grid too large for 32-bit bucket offsets");
+  const aw::Dims d{nx, ny, nz};
+  cudaStream_t s = S(stream);
+  void *scratch = nullptr;
+  AW_CUDA(cudaMallocAsync(&scratch, aw::splat_scratch_bytes(d), s), "aw_splat (scratch)");
+  aw::SplatWork w;
+  aw::splat_work_bind(&w, d, scratch);
+  const cudaError_t e = aw::splat(w, img, hx, hy, hz, out, background, s);
+  cudaFreeAsync(scratch, s);
+  if (e != cudaSuccess) return cuda_fail(e, "aw_splat");
   return 0;
 }
 
@@ -395,6 +422,127 @@ int aw_greedy_get_energies(aw_greedy_t g, double *out, int max_count, int *count
   std::vector<double> ring(cap);
   AW_CUDA(cudaMemcpy(ring.data(), g->ctx.st.energy, sizeof(double) * cap, cudaMemcpyDeviceToHost),
           "aw_greedy_get_energies");
+  const int m = (out && max_count < avail) ? max_count : avail;
+  for (int i = 0; i < m && out; ++i) out[i] = ring[(n - avail + i) % cap];
+  *count = avail;
+  return 0;
+}
+
+int aw_ldmm_create(int nx, int ny, int nz, double spx, double spy, double spz, float alpha,
+                   float beta, float gamma, int n_time_steps, float sigma, float max_pert,
+                   aw_ldmm_t *out) {
+  std::string why;
+  if (!out) return fail("aw_ldmm_create: null handle pointer");
+  *out = nullptr;
+  if (!dims_ok(nx, ny, nz, why)) return fail("aw_ldmm_create: " + why);
+  if (!spacing_ok(spx, spy, spz)) return fail("aw_ldmm_create: spacing must be positive");
+  if (!(gamma > 0.0f) || alpha < 0.0f || beta < 0.0f)
+    return fail("aw_ldmm_create: need gamma > 0, alpha >= 0, beta >= 0 (L must be SPD)");
+  if (n_time_steps < 1) return fail("aw_ldmm_create: NTimeSteps must be >= 1");
+  if (!(sigma > 0.0f)) return fail("aw_ldmm_create: Sigma must be positive");
+  aw_ldmm_s *l = new (std::nothrow) aw_ldmm_s;
+  if (!l) return fail("aw_ldmm_create: out of host memory");
+  const int rc = aw::ldmm_create(&l->ctx, nx, ny, nz, spx, spy, spz, alpha, beta, gamma,
+                                 n_time_steps, sigma, max_pert);
+  if (rc) {
+    aw::ldmm_destroy(&l->ctx);
+    delete l;
+    return fail(std::string("aw_ldmm_create: ") + plan_error(rc));
+  }
+  if (cudaStreamCreateWithFlags(&l->gstream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&l->ev_in, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&l->ev_out, cudaEventDisableTiming) != cudaSuccess) {
+    aw::ldmm_destroy(&l->ctx);
+    delete l;
+    return fail("aw_ldmm_create: stream/event creation failed");
+  }
+  *out = l;
+  return 0;
+}
+
+int aw_ldmm_destroy(aw_ldmm_t l) {
+  if (!l) return 0;
+  cudaDeviceSynchronize();
+  for (auto &kv : l->graphs) cudaGraphExecDestroy(kv.second.second);
+  if (l->gstream) cudaStreamDestroy(l->gstream);
+  if (l->ev_in) cudaEventDestroy(l->ev_in);
+  if (l->ev_out) cudaEventDestroy(l->ev_out);
+  aw::ldmm_destroy(&l->ctx);
+  delete l;
+  return 0;
+}
+
+int aw_ldmm_set_step(aw_ldmm_t l, float step) {
+  if (!l) return fail("aw_ldmm_set_step: null handle");
+  AW_CUDA(cudaMemcpy(l->ctx.step, &step, sizeof(float), cudaMemcpyHostToDevice),
+          "aw_ldmm_set_step");
+  return 0;
+}
+
+int aw_ldmm_get_step(aw_ldmm_t l, float *step) {
+  if (!l || !step) return fail("aw_ldmm_get_step: null pointer");
+  AW_CUDA(cudaDeviceSynchronize(), "aw_ldmm_get_step (pending work)");
+  AW_CUDA(cudaMemcpy(step, l->ctx.step, sizeof(float), cudaMemcpyDeviceToHost),
+          "aw_ldmm_get_step");
+  return 0;
+}
+
+int aw_ldmm_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *v, int update_step,
+                    void *stream) {
+  if (!l) return fail("aw_ldmm_iterate: null handle");
+  if (!I0 || !I1 || !v) return fail("aw_ldmm_iterate: null pointer");
+  AW_CUDA(aw::ldmm_iterate(&l->ctx, I0, I1, v, update_step, S(stream)), "aw_ldmm_iterate");
+  return 0;
+}
+
+int aw_ldmm_run(aw_ldmm_t l, const float *I0, const float *I1, float *v, int n_iters,
+                int adaptive_first, void *stream) {
+  if (!l) return fail("aw_ldmm_run: null handle");
+  if (!I0 || !I1 || !v) return fail("aw_ldmm_run: null pointer");
+  if (n_iters < 0) return fail("aw_ldmm_run: negative iteration count");
+  cudaStream_t user = S(stream), s = l->gstream;
+  AW_CUDA(cudaEventRecord(l->ev_in, user), "aw_ldmm_run (event)");
+  AW_CUDA(cudaStreamWaitEvent(s, l->ev_in, 0), "aw_ldmm_run (wait)");
+  if (adaptive_first) AW_CUDA(aw::ldmm_iterate(&l->ctx, I0, I1, v, 1, s), "aw_ldmm_run (step)");
+  if (n_iters > 0) {
+    const auto key = std::make_pair((const void *)I0, (const void *)I1);
+    auto it = l->graphs.find(key);
+    cudaGraphExec_t exec = nullptr;
+    if (it != l->graphs.end() && it->second.first == v) {
+      exec = it->second.second;
+    } else {
+      if (it != l->graphs.end()) {
+        cudaGraphExecDestroy(it->second.second);
+        l->graphs.erase(it);
+      }
+      cudaGraph_t graph;
+      AW_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "aw_ldmm_run (capture)");
+      const cudaError_t e1 = aw::ldmm_iterate(&l->ctx, I0, I1, v, 0, s);
+      const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+      if (e1 != cudaSuccess) return cuda_fail(e1, "aw_ldmm_run (captured iteration)");
+      if (ec != cudaSuccess) return cuda_fail(ec, "aw_ldmm_run (end capture)");
+      AW_CUDA(cudaGraphInstantiate(&exec, graph, 0), "aw_ldmm_run (instantiate)");
+      cudaGraphDestroy(graph);
+      l->graphs[key] = std::make_pair((const void *)v, exec);
+    }
+    for (int k = 0; k < n_iters; ++k) AW_CUDA(cudaGraphLaunch(exec, s), "aw_ldmm_run (launch)");
+  }
+  AW_CUDA(cudaEventRecord(l->ev_out, s), "aw_ldmm_run (event)");
+  AW_CUDA(cudaStreamWaitEvent(user, l->ev_out, 0), "aw_ldmm_run (wait)");
+  return 0;
+}
+
+int aw_ldmm_get_energies(aw_ldmm_t l, double *out, int max_count, int *count) {
+  if (!l || !count) return fail("aw_ldmm_get_energies: null pointer");
+  AW_CUDA(cudaDeviceSynchronize(), "aw_ldmm_get_energies (pending work)");
+  int n = 0;
+  AW_CUDA(cudaMemcpy(&n, l->ctx.count, sizeof(int), cudaMemcpyDeviceToHost),
+          "aw_ldmm_get_energies");
+  const int cap = l->ctx.cap;
+  const int avail = n < cap ? n : cap;
+  std::vector<double> ring(cap);
+  AW_CUDA(cudaMemcpy(ring.data(), l->ctx.energy, sizeof(double) * cap, cudaMemcpyDeviceToHost),
+          "aw_ldmm_get_energies");
   const int m = (out && max_count < avail) ? max_count : avail;
   for (int i = 0; i < m && out; ++i) out[i] = ring[(n - avail + i) % cap];
   *count = avail;

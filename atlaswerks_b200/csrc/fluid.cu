@@ -334,9 +334,9 @@ cudaError_t fluid_inverse_store(const FluidPlan &p, float *ox, float *oy, float 
   return cudaGetLastError();
 }
 
-cudaError_t fluid_inverse_axpby(const FluidPlan &p, float *vx, float *vy, float *vz, float vfac,
-                                float ufac, cudaStream_t s) {
-  DstAxpby dst{{vx, vy, vz}, vfac, ufac};
+cudaError_t fluid_inverse_axpby(const FluidPlan &p, float *vx, float *vy, float *vz,
+                                const float *step, float sigma, cudaStream_t s) {
+  DstAxpby dst{{vx, vy, vz}, step, sigma};
   if (p.fast) return fast_xy_inverse(p, dst, s);
   k_fft_xy_inv<DstAxpby><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, dst);
   return cudaGetLastError();

@@ -90,11 +90,17 @@ struct DstField {
 };
 
 // LDMM velocity update v = vfac * v + ufac * u (LDMMIteratorCPU::updateVelocity,
-// LDMM/LDMMIteratorCPU.cxx:177-190), float arithmetic in that order.
+// LDMM/LDMMIteratorCPU.cxx:177-190) with vfac = 1 - 2*eps and
+// ufac = 2*eps / sigma^2 formed from the device-resident step eps, float
+// arithmetic in the reference's order (LDMMIteratorCPU.cxx:606-609).
 struct DstAxpby {
   float *c[3];
-  float vfac, ufac;
+  const float *step;
+  float sigma;
   AW_D void store(int comp, long i, float u) const {
+    const float eps = *step;
+    const float vfac = fsub(1.0f, fmul(2.0f, eps));
+    const float ufac = fdiv(fmul(2.0f, eps), fmul(sigma, sigma));
     c[comp][i] = fadd(fmul(vfac, c[comp][i]), fmul(ufac, u));
   }
 };
@@ -111,7 +117,7 @@ cudaError_t fluid_forward_force(const FluidPlan &p, const float *G, const float 
 cudaError_t fluid_solve(const FluidPlan &p, int inverse, cudaStream_t s);
 cudaError_t fluid_inverse_store(const FluidPlan &p, float *ox, float *oy, float *oz,
                                 cudaStream_t s);
-cudaError_t fluid_inverse_axpby(const FluidPlan &p, float *vx, float *vy, float *vz, float vfac,
-                                float ufac, cudaStream_t s);
+cudaError_t fluid_inverse_axpby(const FluidPlan &p, float *vx, float *vy, float *vz,
+                                const float *step, float sigma, cudaStream_t s);
 
 }  // namespace aw

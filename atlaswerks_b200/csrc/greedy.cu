@@ -25,19 +25,28 @@ namespace {
 
 constexpr int kThreads = 256;
 
+// Rows per force-prep block: each block sums the energy of kPrepRows rows, so
+// the fixed-order final sum has few partials to read.
+constexpr int kPrepRows = 16;
+
 __global__ void __launch_bounds__(kRowThreads)
     k_force_prep(const float *__restrict__ I0, const float *__restrict__ I1,
                  const float *__restrict__ hx, const float *__restrict__ hy,
                  const float *__restrict__ hz, float *__restrict__ idef, double *__restrict__ partials,
                  Dims d) {
-  Voxel vox;
+  const int x = blockIdx.x * kRowThreads + threadIdx.x;
+  const int z = blockIdx.z;
   double e = 0.0;
-  if (voxel_of(d, vox)) {
-    const long i = vox.i;
-    const float v = trilerp_scalar(I0, d, (double)hx[i], (double)hy[i], (double)hz[i], 0.0f);
-    idef[i] = v;
-    const float r = -fsub(v, I1[i]);
-    e = (double)r * (double)r;
+  if (x < d.nx) {
+    const int y0 = blockIdx.y * kPrepRows;
+    const int y1 = min(y0 + kPrepRows, d.ny);
+    for (int y = y0; y < y1; ++y) {
+      const long i = ((long)z * d.ny + y) * d.nx + x;
+      const float v = trilerp_scalar(I0, d, (double)hx[i], (double)hy[i], (double)hz[i], 0.0f);
+      idef[i] = v;
+      const float r = -fsub(v, I1[i]);
+      e += (double)r * (double)r;
+    }
   }
   __shared__ double ws[kRowThreads / 32];
   e = warp_sum(e);
@@ -51,6 +60,11 @@ __global__ void __launch_bounds__(kRowThreads)
   }
 }
 
+inline dim3 prep_grid(const Dims &d) {
+  return dim3((unsigned)((d.nx + kRowThreads - 1) / kRowThreads),
+              (unsigned)((d.ny + kPrepRows - 1) / kPrepRows), (unsigned)d.nz);
+}
+
 // Fixed-order reduction of the block partials, so the energy is bitwise
 // reproducible run to run.
 __global__ void __launch_bounds__(kThreads)
@@ -58,7 +72,7 @@ __global__ void __launch_bounds__(kThreads)
                    GreedyDevState st, int auto_reduce) {
   double t = 0.0;
   for (int i = threadIdx.x; i < nparts; i += blockDim.x) t += partials[i];
-  __shared__ double ws[kThreads / 32];
+  __shared__ double ws[kThreads / 32];  // fixed order: thread-strided, then warp tree
   t = warp_sum(t);
   if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = t;
   __syncthreads();
@@ -127,8 +141,6 @@ __global__ void __launch_bounds__(kRowThreads)
   }
 }
 
-inline int grid_for(long n) { return (int)((n + kThreads - 1) / kThreads); }
-
 #define AW_TRY(x)                         \
   do {                                    \
     cudaError_t _e = (x);                 \
@@ -147,7 +159,7 @@ int greedy_create(GreedyCtx *g, int nx, int ny, int nz, double spx, double spy, 
   g->max_pert = max_pert;
   const long n = g->d.n();
   {
-    const dim3 gr = row_grid(g->d);
+    const dim3 gr = prep_grid(g->d);
     g->nparts = (int)(gr.x * gr.y * gr.z);
   }
   g->sms = 148;
@@ -184,7 +196,7 @@ cudaError_t greedy_stage(GreedyCtx *g, int stage, const float *I0, const float *
   float *v[3] = {g->vbuf, g->vbuf + n, g->vbuf + 2 * n};
   switch (stage) {
     case kStageForcePrep:
-      k_force_prep<<<row_grid(d), kRowThreads, 0, s>>>(I0, I1, h[0], h[1], h[2], g->idef, g->partials, d);
+      k_force_prep<<<prep_grid(d), kRowThreads, 0, s>>>(I0, I1, h[0], h[1], h[2], g->idef, g->partials, d);
       return cudaGetLastError();
     case kStageEnergy: {
       const double spprod = g->sp.x * g->sp.y * g->sp.z;

@@ -1,0 +1,41 @@
+// ldmm.cuh — device state of the LDMM relaxation iterator (ldmm.cu).
+#pragma once
+
+#include "fluid.cuh"
+#include "splat.cuh"
+
+namespace aw {
+
+struct LdmmCtx {
+  FluidPlan plan;
+  Dims d;
+  Spacing sp;
+  int T;
+  float sigma;
+  float max_pert;
+  float *J0;        // T x N: I0 deformed to each time point
+  float *hbuf;      // 2 x 3N ping-pong deformation
+  float *diff;      // N: J0_{T-1} - I1
+  float *S;         // N: splatted residual
+  float *u;         // 3N: K f when the step size is being computed
+  void *splat_scratch;
+  SplatWork sw;
+  double *partials;
+  int nparts;
+  char *scalars;    // step | count | maxbits
+  float *step;
+  int *count;
+  unsigned *maxbits;
+  double *energy;   // image-energy history ring
+  int cap;
+};
+
+int ldmm_create(LdmmCtx *c, int nx, int ny, int nz, double spx, double spy, double spz,
+                float alpha, float beta, float gamma, int T, float sigma, float max_pert);
+void ldmm_destroy(LdmmCtx *c);
+// One IterateNew; v is [T][3][N]. update_step: compute the step from
+// max |2v - (2/sigma^2) K f| and leave v unchanged.
+cudaError_t ldmm_iterate(LdmmCtx *c, const float *I0, const float *I1, float *v, int update_step,
+                         cudaStream_t s);
+
+}  // namespace aw

@@ -1,0 +1,259 @@
+// splat.cu — deterministic counting-sort splat (see splat.cuh).
+#include <climits>
+
+#include "splat.cuh"
+
+namespace aw {
+
+namespace {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 4;
+constexpr int kScanBlock = kScanThreads * kScanItems;
+
+inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// bucket of a source: the cell of its h, shifted by one so that
+// h in (-1, 0) lands in bucket 0. Returns -1 for sources the reference
+// skips: those outside the volume grown by one voxel
+// (HField3DUtils.txx:1110-1112).
+AW_D long bucket_of(const Dims &d, float px, float py, float pz) {
+  if (!(px > -1.0f && px < (float)d.nx && py > -1.0f && py < (float)d.ny && pz > -1.0f &&
+        pz < (float)d.nz))
+    return -1;
+  const int fx = ref_floor_f(px), fy = ref_floor_f(py), fz = ref_floor_f(pz);
+  return ((long)(fz + 1) * (d.ny + 1) + (fy + 1)) * (d.nx + 1) + (fx + 1);
+}
+
+__global__ void __launch_bounds__(kRowThreads)
+    k_count(const float *__restrict__ hx, const float *__restrict__ hy, const float *__restrict__ hz,
+            Dims d, int *__restrict__ counts) {
+  Voxel v;
+  if (!voxel_of(d, v)) return;
+  const long b = bucket_of(d, hx[v.i], hy[v.i], hz[v.i]);
+  if (b >= 0) atomicAdd(counts + b, 1);
+}
+
+// block-local exclusive scan of kScanBlock ints held 4 per thread
+AW_D int block_scan(int (&a)[kScanItems], int *wsum) {
+  int tsum = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int x = a[k];
+    a[k] = tsum;
+    tsum += x;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int incl = tsum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int w = lane < kScanThreads / 32 ? wsum[lane] : 0;
+    int wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    if (lane < kScanThreads / 32) wsum[lane] = wi - w;  // exclusive warp offsets
+    if (lane == kScanThreads / 32 - 1) wsum[kScanThreads / 32] = wi;  // block total
+  }
+  __syncthreads();
+  const int base = wsum[warp] + (incl - tsum);
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) a[k] += base;
+  const int total = wsum[kScanThreads / 32];
+  __syncthreads();
+  return total;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    k_scan_reduce(const int *__restrict__ x, long n, int *__restrict__ blocksums) {
+  const long b0 = (long)blockIdx.x * kScanBlock;
+  int s = 0;
+  for (int k = 0; k < kScanItems; ++k) {
+    const long i = b0 + (long)k * kScanThreads + threadIdx.x;
+    if (i < n) s += x[i];
+  }
+  __shared__ int ws[kScanThreads / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < kScanThreads / 32; ++w) t += ws[w];
+    blocksums[blockIdx.x] = t;
+  }
+}
+
+// one block: exclusive scan of the block sums, chunk by chunk
+__global__ void __launch_bounds__(kScanThreads) k_scan_blocksums(int *__restrict__ bs, int nb) {
+  __shared__ int wsum[kScanThreads / 32 + 1];
+  int carry = 0;
+  for (int c0 = 0; c0 < nb; c0 += kScanBlock) {
+    int a[kScanItems];
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      const int i = c0 + threadIdx.x * kScanItems + k;
+      a[k] = i < nb ? bs[i] : 0;
+    }
+    const int total = block_scan(a, wsum);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      const int i = c0 + threadIdx.x * kScanItems + k;
+      if (i < nb) bs[i] = a[k] + carry;
+    }
+    carry += total;
+    __syncthreads();
+  }
+}
+
+// exclusive scan in place; x[n] receives the total
+__global__ void __launch_bounds__(kScanThreads)
+    k_scan_apply(int *__restrict__ x, long n, const int *__restrict__ blocksums) {
+  __shared__ int wsum[kScanThreads / 32 + 1];
+  const long b0 = (long)blockIdx.x * kScanBlock;
+  int a[kScanItems];
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const long i = b0 + (long)threadIdx.x * kScanItems + k;
+    a[k] = i < n ? x[i] : 0;
+  }
+  const int total = block_scan(a, wsum);
+  const int off = blocksums[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const long i = b0 + (long)threadIdx.x * kScanItems + k;
+    if (i < n) x[i] = a[k] + off;
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) x[n] = off + total;
+}
+
+__global__ void __launch_bounds__(kRowThreads)
+    k_scatter(const float *__restrict__ hx, const float *__restrict__ hy,
+              const float *__restrict__ hz, Dims d, const int *__restrict__ offsets,
+              int *__restrict__ cursor, int *__restrict__ order) {
+  Voxel v;
+  if (!voxel_of(d, v)) return;
+  const long b = bucket_of(d, hx[v.i], hy[v.i], hz[v.i]);
+  if (b < 0) return;
+  const int pos = offsets[b] + atomicAdd(cursor + b, 1);
+  order[pos] = (int)v.i;
+}
+
+// insertion sort of each bucket by source index (buckets are short)
+__global__ void __launch_bounds__(256)
+    k_bucket_sort(const int *__restrict__ offsets, int *__restrict__ order, long next) {
+  const long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= next) return;
+  const int s = offsets[b], e = offsets[b + 1];
+  for (int i = s + 1; i < e; ++i) {
+    const int key = order[i];
+    int j = i - 1;
+    while (j >= s && order[j] > key) {
+      order[j + 1] = order[j];
+      --j;
+    }
+    order[j + 1] = key;
+  }
+}
+
+// weight of corner (cx, cy, cz) of source i, rounded to float as
+// forwardApply does: ((ax)*(ay))*(az) in double, ax = 1 - rx or rx
+AW_D float corner_weight(float px, float py, float pz, int cx, int cy, int cz) {
+  const int fx = ref_floor_f(px), fy = ref_floor_f(py), fz = ref_floor_f(pz);
+  const float rx = fsub(px, __int2float_rn(fx)), ry = fsub(py, __int2float_rn(fy)),
+              rz = fsub(pz, __int2float_rn(fz));
+  const double ax = cx ? (double)rx : dsub(1.0, (double)rx);
+  const double ay = cy ? (double)ry : dsub(1.0, (double)ry);
+  const double az = cz ? (double)rz : dsub(1.0, (double)rz);
+  return __double2float_rn(dmul(dmul(ax, ay), az));
+}
+
+// every destination merges its eight candidate buckets in source order
+__global__ void __launch_bounds__(kRowThreads)
+    k_gather(const float *__restrict__ img, const float *__restrict__ hx,
+             const float *__restrict__ hy, const float *__restrict__ hz, Dims d,
+             const int *__restrict__ offsets, const int *__restrict__ order,
+             float *__restrict__ out, float bg) {
+  Voxel v;
+  if (!voxel_of(d, v)) return;
+  int pos[8], end[8], cur[8];
+  const long sy = d.nx + 1, sz = (long)(d.nx + 1) * (d.ny + 1);
+  // bucket k = (dz, dy, dx) bits; source in bucket b contributes corner
+  // (dx, dy, dz) to this voxel
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
+    const long b = (long)(v.z - dz + 1) * sz + (long)(v.y - dy + 1) * sy + (v.x - dx + 1);
+    pos[k] = offsets[b];
+    end[k] = offsets[b + 1];
+    cur[k] = pos[k] < end[k] ? order[pos[k]] : INT_MAX;
+  }
+  float acc = bg;
+  while (true) {
+    int m = INT_MAX, sel = -1;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (cur[k] < m) { m = cur[k]; sel = k; }
+    if (sel < 0) break;
+    const float px = hx[m], py = hy[m], pz = hz[m];
+    const float w = corner_weight(px, py, pz, sel & 1, (sel >> 1) & 1, (sel >> 2) & 1);
+    acc = fadd(acc, fmul(w, img[m]));
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (k == sel) {
+        ++pos[k];
+        cur[k] = pos[k] < end[k] ? order[pos[k]] : INT_MAX;
+      }
+    }
+  }
+  out[v.i] = acc;
+}
+
+}  // namespace
+
+size_t splat_scratch_bytes(const Dims &d) {
+  const long next = (long)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
+  const long nb = (next + kScanBlock - 1) / kScanBlock;
+  return align256(sizeof(int) * (next + 1)) + align256(sizeof(int) * next) +
+         align256(sizeof(int) * d.n()) + align256(sizeof(int) * nb);
+}
+
+void splat_work_bind(SplatWork *w, const Dims &d, void *scratch) {
+  char *p = static_cast<char *>(scratch);
+  w->d = d;
+  w->next = (long)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
+  w->nblocks = (int)((w->next + kScanBlock - 1) / kScanBlock);
+  w->offsets = reinterpret_cast<int *>(p);
+  p += align256(sizeof(int) * (w->next + 1));
+  w->cursor = reinterpret_cast<int *>(p);
+  p += align256(sizeof(int) * w->next);
+  w->order = reinterpret_cast<int *>(p);
+  p += align256(sizeof(int) * d.n());
+  w->blocksums = reinterpret_cast<int *>(p);
+}
+
+cudaError_t splat(const SplatWork &w, const float *img, const float *hx, const float *hy,
+                  const float *hz, float *out, float bg, cudaStream_t s) {
+  const Dims d = w.d;
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(w.offsets, 0, sizeof(int) * (w.next + 1), s)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(w.cursor, 0, sizeof(int) * w.next, s)) != cudaSuccess) return e;
+  k_count<<<row_grid(d), kRowThreads, 0, s>>>(hx, hy, hz, d, w.offsets);
+  k_scan_reduce<<<w.nblocks, kScanThreads, 0, s>>>(w.offsets, w.next, w.blocksums);
+  k_scan_blocksums<<<1, kScanThreads, 0, s>>>(w.blocksums, w.nblocks);
+  k_scan_apply<<<w.nblocks, kScanThreads, 0, s>>>(w.offsets, w.next, w.blocksums);
+  k_scatter<<<row_grid(d), kRowThreads, 0, s>>>(hx, hy, hz, d, w.offsets, w.cursor, w.order);
+  k_bucket_sort<<<(int)((w.next + 255) / 256), 256, 0, s>>>(w.offsets, w.order, w.next);
+  k_gather<<<row_grid(d), kRowThreads, 0, s>>>(img, hx, hy, hz, d, w.offsets, w.order, out, bg);
+  return cudaGetLastError();
+}
+
+}  // namespace aw

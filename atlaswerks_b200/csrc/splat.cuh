@@ -1,0 +1,41 @@
+// splat.cuh — deterministic splatting (the adjoint of trilinear
+// interpolation), HField3DUtils::forwardApply with normalize = false
+// (UtilitiesDataTypes/HField3DUtils.txx:1058-1279).
+//
+// The reference CPU adds each source voxel's eight weighted corner
+// contributions in source (z, y, x) order, in float; the reference GPU path
+// uses int32 fixed-point atomics (CUDACommon/src/cudaSplatAtomic.cu:379-448).
+// Here the sources are bucketed by the cell their h lands in (counting sort:
+// count, exclusive scan, scatter, per-bucket sort by source index), then
+// every destination voxel merges the eight buckets that can reach it in
+// source-index order and adds the contributions sequentially. No float
+// atomics, run-to-run bitwise identical, and with identical inputs bitwise
+// equal to the reference CPU.
+#pragma once
+
+#include "aw_common.cuh"
+
+namespace aw {
+
+// device scratch of one splat, sized for a grid (extended by one cell per
+// axis for sources landing in (-1, 0))
+struct SplatWork {
+  Dims d;
+  long next;        // (nx+1)(ny+1)(nz+1)
+  int *offsets;     // next + 1: bucket counts, then exclusive offsets
+  int *cursor;      // next: scatter cursors
+  int *order;       // n: source indices grouped by bucket
+  int *blocksums;   // scan partials
+  int nblocks;
+};
+
+// bytes of device scratch one splat of grid d needs
+size_t splat_scratch_bytes(const Dims &d);
+// lays out a SplatWork inside caller-provided device memory (256-aligned)
+void splat_work_bind(SplatWork *w, const Dims &d, void *scratch);
+
+// out = splat of img by h (three planes), background bg; stream-ordered
+cudaError_t splat(const SplatWork &w, const float *img, const float *hx, const float *hy,
+                  const float *hz, float *out, float bg, cudaStream_t s);
+
+}  // namespace aw

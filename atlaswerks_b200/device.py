@@ -89,3 +89,15 @@ def compose_vh(v: torch.Tensor, g: torch.Tensor, spacing=(1.0, 1.0, 1.0), scale:
                                    _p(o[0]), _p(o[1]), _p(o[2]), *_dims(g), *spacing, scale,
                                    direction, background, _stream()))
     return o
+
+
+def splat(img: torch.Tensor, h: torch.Tensor, background: float = 0.0) -> torch.Tensor:
+    """Adjoint of apply: HField3DUtils::forwardApply(normalize=false) /
+    cplSplat3DH, deterministic (no float atomics)."""
+    _check_image(img, "img")
+    _check_field(h, "h")
+    out = torch.empty_like(img)
+    check(_lib.lib().aw_splat(_p(img), _p(h[0]), _p(h[1]), _p(h[2]), _p(out), *_dims(img),
+                              background, _stream()))
+    return out
+

@@ -1,0 +1,133 @@
+"""Host-side mirror of the reference's LDMM relaxation interfaces.
+
+* ``LDMMIteratorB200`` — LDMMIteratorGPU / LDMMIteratorCPU
+  (Algorithms/LDMM/LDMMIteratorCPU.h:30-70): ``SetScaleLevel``, ``Iterate``,
+  ``UpdateStepSizeNextIteration``; the splatting gradient (IterateNew,
+  LDMM/LDMMIteratorCPU.cxx:529-631).
+* ``LDMMDeformationDataB200`` — LDMMDeformationData (LDMM/LDMMDeformationData.h):
+  images, the T velocity fields ``v(t)`` and ``StepSize``.
+
+Computation runs in libaw_b200.so through the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check
+from .device import _check_image, _stream
+from .greedy import DiffOperParam
+
+
+@dataclass
+class LDMMIteratorParam:
+    """LDMMIteratorParam (Algorithms/LDMM/LDMMIteratorParam.h:28-54) defaults."""
+    Kernel: DiffOperParam = field(default_factory=DiffOperParam)
+    Sigma: float = 5.0
+    StepSize: float = 0.005
+    UseAdaptiveStepSize: bool = True
+    MaxPert: float = 0.1
+
+
+class LDMMDeformationDataB200:
+    def __init__(self, I0: torch.Tensor, I1: torch.Tensor, n_time_steps: int,
+                 spacing=(1.0, 1.0, 1.0)):
+        _check_image(I0, "I0")
+        _check_image(I1, "I1")
+        if I0.shape != I1.shape:
+            raise ValueError("I0 and I1 must have the same grid")
+        self.I0, self.I1 = I0, I1
+        self.T = int(n_time_steps)
+        self.spacing = tuple(float(s) for s in spacing)
+        self.V = torch.zeros((self.T, 3) + tuple(I0.shape), device=I0.device,
+                             dtype=torch.float32)
+
+    def v(self, t: int) -> torch.Tensor:
+        return self.V[t]
+
+
+class LDMMIteratorB200:
+    DeformationDataType = LDMMDeformationDataB200
+    ParamType = LDMMIteratorParam
+
+    def __init__(self, size: Sequence[int], origin=(0.0, 0.0, 0.0), spacing=(1.0, 1.0, 1.0),
+                 n_time_steps: int = 5, debug: bool = True):
+        self.size = tuple(size)
+        self.spacing = tuple(float(s) for s in spacing)
+        self.T = int(n_time_steps)
+        self._h = ctypes.c_void_p()
+        self._update_step = False
+
+    def SetScaleLevel(self, size: Sequence[int], spacing: Sequence[float],
+                      param: LDMMIteratorParam):
+        k = param.Kernel
+        if k.LPow != 1.0 or k.UseEigenLUT or k.DivergenceFree:
+            raise ValueError("LPow != 1, UseEigenLUT and DivergenceFree are not supported on the "
+                             "GPU path (DiffOperGPU)")
+        self._free()
+        nx, ny, nz = size
+        check(_lib.lib().aw_ldmm_create(nx, ny, nz, *map(float, spacing), k.Alpha, k.Beta,
+                                        k.Gamma, self.T, param.Sigma, param.MaxPert,
+                                        ctypes.byref(self._h)))
+        self.param = param
+        self.SetStepSize(param.StepSize)
+
+    def UpdateStepSizeNextIteration(self):
+        self._update_step = True
+
+    def SetStepSize(self, step: float):
+        check(_lib.lib().aw_ldmm_set_step(self._h, float(step)))
+
+    def StepSize(self) -> float:
+        s = ctypes.c_float()
+        check(_lib.lib().aw_ldmm_get_step(self._h, ctypes.byref(s)))
+        return float(s.value)
+
+    def Iterate(self, data: LDMMDeformationDataB200):
+        if data.T != self.T:
+            raise ValueError("data has a different number of time steps")
+        check(_lib.lib().aw_ldmm_iterate(self._h, data.I0.data_ptr(), data.I1.data_ptr(),
+                                         data.V.data_ptr(), int(self._update_step), _stream()))
+        self._update_step = False
+
+    def Run(self, data: LDMMDeformationDataB200, n_iters: int, adaptive_first: bool = False):
+        check(_lib.lib().aw_ldmm_run(self._h, data.I0.data_ptr(), data.I1.data_ptr(),
+                                     data.V.data_ptr(), int(n_iters), int(adaptive_first),
+                                     _stream()))
+
+    def Energies(self) -> np.ndarray:
+        n = ctypes.c_int()
+        check(_lib.lib().aw_ldmm_get_energies(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros(max(n.value, 1), np.float64)
+        check(_lib.lib().aw_ldmm_get_energies(self._h, out.ctypes.data, n.value,
+                                              ctypes.byref(n)))
+        return out[: n.value]
+
+    def _free(self):
+        if self._h:
+            _lib.lib().aw_ldmm_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self._free()
+        except Exception:
+            pass
+
+
+def ldmm_register(I0: torch.Tensor, I1: torch.Tensor, n_time_steps: int, n_iters: int,
+                  spacing=(1.0, 1.0, 1.0), sigma=0.1, step=0.005, adaptive=False, max_pert=0.1,
+                  alpha=0.01, beta=0.01, gamma=0.001):
+    """LDMMWarp at one scale level (LDMM/LDMMWarp.txx:71-130)."""
+    nz, ny, nx = I0.shape
+    it = LDMMIteratorB200((nx, ny, nz), spacing=spacing, n_time_steps=n_time_steps)
+    p = LDMMIteratorParam(DiffOperParam(alpha, beta, gamma), sigma, step, adaptive, max_pert)
+    it.SetScaleLevel((nx, ny, nz), spacing, p)
+    data = LDMMDeformationDataB200(I0, I1, n_time_steps, spacing)
+    it.Run(data, n_iters, adaptive_first=adaptive)
+    return data.V, it.Energies(), it.StepSize()

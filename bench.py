@@ -379,6 +379,24 @@ def run_b200(args):
     return 0
 
 
+def run_ncu_case(args):
+    """A short, untimed workload for ncu captures: one 128^3 pair, a step
+    update, then `--steps` iterations through the graph path."""
+    import torch
+
+    from atlaswerks_b200.greedy import (DiffOperParam, GreedyDeformationDataB200,
+                                        GreedyIteratorB200, GreedyIteratorParam)
+    I0, I1 = make_pair(0)
+    it = GreedyIteratorB200((N, N, N))
+    it.SetScaleLevel((N, N, N), (1.0, 1.0, 1.0),
+                     GreedyIteratorParam(DiffOperParam(ALPHA, BETA, GAMMA), MAX_PERT))
+    d = GreedyDeformationDataB200(torch.from_numpy(I0).cuda(), torch.from_numpy(I1).cuda())
+    it.Run(d, 1 + args.steps, update_first=True)
+    torch.cuda.synchronize()
+    print(json.dumps({"ncu_case": "greedy 128^3", "iterations": 1 + args.steps}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -386,7 +404,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ncu-case", action="store_true",
+                    help="run a short untimed 128^3 workload for ncu captures")
     args = ap.parse_args()
+    if args.ncu_case:
+        return run_ncu_case(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)

@@ -76,6 +76,15 @@ int aw_compose_vh(const float *vx, const float *vy, const float *vz, const float
                   int ny, int nz, double spx, double spy, double spz, float scale, int direction,
                   int background, void *stream);
 
+/* Splat img by h (the adjoint of aw_apply): out(y) = bg + sum over sources
+ * x of w(h(x) -> y) * img(x), in source order, no float atomics; bitwise
+ * reproducible. Replaces cplSplat3DH (CUDACommon/inc/cudaSplat.h:119-131,
+ * CUDACommon/src/cudaSplatAtomic.cu:569-599) and HField3DUtils::forwardApply
+ * with normalize=false (UtilitiesDataTypes/HField3DUtils.txx:1058-1279).
+ * Scratch (about 16 bytes per voxel) comes from the stream-ordered allocator. */
+int aw_splat(const float *img, const float *hx, const float *hy, const float *hz, float *out,
+             int nx, int ny, int nz, float background, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Fluid kernel. Replaces KernelInterfaceGPU / DiffOperGPU
  * (Algorithms/Common/KernelInterfaceGPU.h:20-43, Common/DiffOperGPU.cxx:32-205)
@@ -139,6 +148,35 @@ int aw_greedy_profile(aw_greedy_t g, const float *I0, const float *I1, const flo
 
 /* Copies the energy history (oldest first) to host; synchronises. */
 int aw_greedy_get_energies(aw_greedy_t g, double *out, int max_count, int *count);
+
+/* ---------------------------------------------------------------------------
+ * LDMM iterator (relaxation, splatting gradient). Replaces LDMMIteratorGPU /
+ * LDMMIteratorCPU::IterateNew (Algorithms/LDMM/LDMMIteratorGPU.cxx:159-293,
+ * LDMMIteratorCPU.cxx:529-631). Velocity fields are one device buffer
+ * [T][3][nz][ny][nx].
+ * ------------------------------------------------------------------------- */
+typedef struct aw_ldmm_s *aw_ldmm_t;
+
+/* ctor + SetScaleLevel: grid, spacing, DiffOper parameters, NTimeSteps,
+ * Sigma and MaxPert (LDMM/LDMMIteratorParam.h:28-54). */
+int aw_ldmm_create(int nx, int ny, int nz, double spx, double spy, double spz, float alpha,
+                   float beta, float gamma, int n_time_steps, float sigma, float max_pert,
+                   aw_ldmm_t *out);
+int aw_ldmm_destroy(aw_ldmm_t l);
+/* LDMMDeformationData::StepSize(s) / StepSize(); get synchronises. */
+int aw_ldmm_set_step(aw_ldmm_t l, float step);
+int aw_ldmm_get_step(aw_ldmm_t l, float *step);
+/* One Iterate(): updates v in place. update_step=1 instead computes the step
+ * from max |2v - (2/sigma^2) K f| and leaves v unchanged
+ * (UseAdaptiveStepSize, LDMM/LDMMWarp.txx:99-104). */
+int aw_ldmm_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *v, int update_step,
+                    void *stream);
+/* n_iters iterations replayed from a captured CUDA graph; adaptive_first=1
+ * runs the step-size pass before the first iteration. */
+int aw_ldmm_run(aw_ldmm_t l, const float *I0, const float *I1, float *v, int n_iters,
+                int adaptive_first, void *stream);
+/* Image energies sp^3 * sum (I0(h_T) - I1)^2, oldest first; synchronises. */
+int aw_ldmm_get_energies(aw_ldmm_t l, double *out, int max_count, int *count);
 
 #ifdef __cplusplus
 }

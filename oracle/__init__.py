@@ -87,6 +87,7 @@ class Oracle:
         L = self.lib
         L.aw_oracle_greedy_iterate.restype = ctypes.c_double
         L.aw_oracle_max_norm.restype = ctypes.c_float
+        L.aw_oracle_ldmm_iterate.restype = ctypes.c_double
 
     # --- interpolation family -------------------------------------------------
     def apply(self, img, h, bg=0.0):
@@ -158,6 +159,18 @@ class Oracle:
             _fp(I0), _fp(I1), _fp(h[0]), _fp(h[1]), _fp(h[2]), _fp(hi[0]), _fp(hi[1]),
             _fp(hi[2]), *_shape(I0), *map(_dbl, sp), _dbl(alpha), _dbl(beta), _dbl(gamma),
             ctypes.c_float(max_pert), _i(int(update_step)), ctypes.byref(st))
+        return float(e), float(st.value)
+
+    def ldmm_iterate(self, I0, I1, v, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01, gamma=0.001,
+                     sigma=0.1, step=0.005, update_step=False, max_pert=0.1):
+        """One LDMMIteratorCPU::IterateNew; v [T,3,nz,ny,nx] updated in place.
+        Returns (image energy sp^3*sum diff^2, step)."""
+        assert v.dtype == np.float32 and v.flags.c_contiguous
+        st = ctypes.c_float(step)
+        e = self.lib.aw_oracle_ldmm_iterate(_fp(I0), _fp(I1), v.ctypes.data_as(_f), _i(v.shape[0]),
+                                            *_shape(I0), *map(_dbl, sp), _dbl(alpha), _dbl(beta),
+                                            _dbl(gamma), ctypes.c_float(sigma), ctypes.byref(st),
+                                            _i(int(update_step)), ctypes.c_float(max_pert))
         return float(e), float(st.value)
 
     def greedy_run(self, I0, I1, iters, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01, gamma=0.001,
@@ -287,3 +300,23 @@ class Reference:
             _fp(steps))
         self._check(rc)
         return h, hinv, en, steps
+
+    def ldmm_run(self, I0, I1, T, iters, sp=(1.0, 1.0, 1.0), sigma=0.1, step=0.005,
+                 adaptive=False, max_pert=0.1, alpha=0.01, beta=0.01, gamma=0.001,
+                 use_new=True, debug=True, v_init=None):
+        """LDMMIteratorCPU (IterateNew when use_new) through the LDMMWarp loop
+        at one scale. Returns (v [T,3,...], image energies, step)."""
+        n = I0.size
+        v = (np.ascontiguousarray(v_init, np.float32).copy() if v_init is not None
+             else np.zeros((T, 3) + I0.shape, np.float32))
+        en = np.zeros(iters, np.float64)
+        st = ctypes.c_float()
+        with quiet_stdout():
+            rc = self.lib.awref_ldmm_run(
+                _fp(I0), _fp(I1), *_shape(I0), *map(_dbl, sp), _i(T), _i(iters),
+                ctypes.c_float(sigma), ctypes.c_float(step), _i(int(adaptive)),
+                ctypes.c_float(max_pert), _dbl(alpha), _dbl(beta), _dbl(gamma), _i(int(use_new)),
+                _i(int(debug)), _i(int(v_init is not None)), v.ctypes.data_as(_f), _dp(en),
+                ctypes.byref(st))
+        self._check(rc)
+        return v, en, float(st.value)

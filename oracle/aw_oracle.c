@@ -491,3 +491,80 @@ void aw_oracle_identity(float *hx, float *hy, float *hz, int nx, int ny, int nz)
         hz[i] = (float)z;
       }
 }
+
+/* ------------------------------------------------------------------------
+ * LDMM relaxation, LDMMIteratorCPU::IterateNew (LDMM/LDMMIteratorCPU.cxx:
+ * 529-631): forward integration by composeHVInv + apply, the residual
+ * J0_{T-1} - I1, then for t = T-1..0: composeVHInv (PARTIAL_ZERO), splat of
+ * the residual (forwardApply), body force grad(J0_{t-1}) * splat, K, and
+ * v_t <- (1 - 2 eps) v_t + (2 eps / sigma^2) K f (updateVelocity, :177-190).
+ * With update_step set, v is left unchanged and *step becomes
+ * max_pert / max_t max_x |2 v_t - (2/sigma^2) K f_t| (calcMaxDisplacement,
+ * :192-212). v is [T][3][N]. Returns the image energy sp^3 * sum diff^2
+ * (accumulated in double).
+ * ---------------------------------------------------------------------- */
+double aw_oracle_ldmm_iterate(const float *I0, const float *I1, float *v, int T, int nx, int ny,
+                              int nz, double spx, double spy, double spz, double alpha,
+                              double beta, double gamma, float sigma, float *step,
+                              int update_step, float max_pert) {
+  const long n = (long)nx * ny * nz;
+  float *h = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *o = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *J0 = (float *)malloc(sizeof(float) * (size_t)(T * n));
+  float *diff = (float *)malloc(sizeof(float) * (size_t)n);
+  float *S = (float *)malloc(sizeof(float) * (size_t)n);
+  float *f = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  aw_oracle_identity(h, h + n, h + 2 * n, nx, ny, nz);
+  for (int i = 0; i < T; ++i) {
+    float *vi = v + (long)i * 3 * n;
+    aw_oracle_compose_hv(h, h + n, h + 2 * n, vi, vi + n, vi + 2 * n, o, o + n, o + 2 * n, nx, ny,
+                         nz, spx, spy, spz, -1, AW_BG_PARTIAL_ID);
+    memcpy(h, o, sizeof(float) * (size_t)(3 * n));
+    aw_oracle_apply(I0, h, h + n, h + 2 * n, J0 + (long)i * n, nx, ny, nz, 0.0f);
+  }
+  double e = 0.0;
+  for (long k = 0; k < n; ++k) {
+    diff[k] = J0[(long)(T - 1) * n + k] - I1[k];
+    e += (double)diff[k] * (double)diff[k];
+  }
+  e *= spx * spy * spz;
+  const float vfac = 1.f - 2 * *step;
+  const float ufac = 2 * *step / (sigma * sigma);
+  float total_max = 0.f;
+  aw_oracle_identity(h, h + n, h + 2 * n, nx, ny, nz);
+  for (int t = T - 1; t >= 0; --t) {
+    float *vt = v + (long)t * 3 * n;
+    aw_oracle_compose_vh(vt, vt + n, vt + 2 * n, h, h + n, h + 2 * n, o, o + n, o + 2 * n, nx, ny,
+                         nz, spx, spy, spz, -1, AW_BG_PARTIAL_ZERO);
+    memcpy(h, o, sizeof(float) * (size_t)(3 * n));
+    aw_oracle_splat(diff, h, h + n, h + 2 * n, S, nx, ny, nz, 0.0f);
+    const float *G = (t > 0) ? J0 + (long)(t - 1) * n : I0;
+    aw_oracle_gradient(G, f, f + n, f + 2 * n, nx, ny, nz, spx, spy, spz, 0);
+    for (long k = 0; k < n; ++k) {
+      f[k] *= S[k];
+      f[n + k] *= S[k];
+      f[2 * n + k] *= S[k];
+    }
+    aw_oracle_fluid_apply(f, f + n, f + 2 * n, nx, ny, nz, spx, spy, spz, alpha, beta, gamma, 1);
+    if (update_step) {
+      const float a = 2.0f, b = -2.0f / (sigma * sigma);
+      for (long k = 0; k < n; ++k) {
+        const float x = a * vt[k] + b * f[k];
+        const float y = a * vt[n + k] + b * f[n + k];
+        const float zz = a * vt[2 * n + k] + b * f[2 * n + k];
+        const float len = (float)sqrt((double)(x * x + y * y + zz * zz));
+        if (len > total_max) total_max = len;
+      }
+    } else {
+      for (long k = 0; k < 3 * n; ++k) vt[k] = vfac * vt[k] + ufac * f[k];
+    }
+  }
+  if (update_step) *step = max_pert / total_max;
+  free(h);
+  free(o);
+  free(J0);
+  free(diff);
+  free(S);
+  free(f);
+  return e;
+}

@@ -51,6 +51,11 @@ double aw_oracle_greedy_iterate(const float *I0, const float *I1, float *hx, flo
                                 double spx, double spy, double spz, double alpha, double beta,
                                 double gamma, float max_pert, int update_step, float *step);
 
+double aw_oracle_ldmm_iterate(const float *I0, const float *I1, float *v, int T, int nx, int ny,
+                              int nz, double spx, double spy, double spz, double alpha,
+                              double beta, double gamma, float sigma, float *step,
+                              int update_step, float max_pert);
+
 #ifdef __cplusplus
 }
 #endif

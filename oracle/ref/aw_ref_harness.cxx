@@ -25,6 +25,7 @@
 #include "GreedyParam.h"
 #include "HField3DUtils.h"
 #include "LDMMDeformationData.h"
+#include "LDMMEnergy.h"
 #include "LDMMIteratorCPU.h"
 #include "LDMMParam.h"
 #include "MultiscaleManager.h"
@@ -93,6 +94,18 @@ void parse_into(P &param, const std::string &xml) {
     return -1;                             \
   }                                        \
   return 0;
+
+// LDMMIteratorCPU with the splatting gradient (IterateNew) selected: the
+// reference keeps the selector protected (LDMM/LDMMIteratorCPU.cxx:33,
+// LDMMIteratorCPU.h:115), so a subclass sets it before SetScaleLevel.
+class LDMMIteratorNewCPU : public LDMMIteratorCPU {
+ public:
+  LDMMIteratorNewCPU(const SizeType &size, const OriginType &origin, const SpacingType &spacing,
+                     unsigned int nTimeSteps, bool debug, bool use_new)
+      : LDMMIteratorCPU(size, origin, spacing, nTimeSteps, debug) {
+    mUseOrigGradientCalc = !use_new;
+  }
+};
 
 }  // namespace
 
@@ -293,6 +306,70 @@ int awref_greedy_run(const float *i0, const float *i1, int nx, int ny, int nz, d
   const long n = (long)nx * ny * nz;
   from_vf(data.Def1To0(), h_out, h_out + n, h_out + 2 * n);
   if (compute_inverse && hinv_out) from_vf(data.Def0To1(), hinv_out, hinv_out + n, hinv_out + 2 * n);
+  GUARD_END
+}
+
+/*
+ * LDMM registration through LDMMIteratorCPU, scale loop of LDMMWarp::RunWarp
+ * at one scale level (factor 1). use_new selects IterateNew (splatting) over
+ * the default IterateOrig (Jacobian). v is [T][3][N]: read as the initial
+ * velocity when v_init is set (else zero), written back at the end.
+ * energies[] receives the image energy of each iteration when debug is set.
+ */
+int awref_ldmm_run(const float *i0, const float *i1, int nx, int ny, int nz, double spx,
+                   double spy, double spz, int T, int iters, float sigma, float step,
+                   int adaptive, float max_pert, double alpha, double beta, double gamma,
+                   int use_new, int debug, int v_init, float *v, double *energies,
+                   float *step_out) {
+  GUARD_BEGIN
+  std::ostringstream xml;
+  xml.precision(17);
+  xml << "<LDMMWarpParameterFile><LDMMScaleLevel><ScaleLevel><DownsampleFactor val=\"1\"/>"
+      << "</ScaleLevel><LDMMIterator>" << diffoper_xml(alpha, beta, gamma) << "<Sigma val=\""
+      << sigma << "\"/><StepSize val=\"" << step << "\"/><UseAdaptiveStepSize val=\""
+      << (adaptive ? "true" : "false") << "\"/><MaxPert val=\"" << max_pert
+      << "\"/></LDMMIterator><NIterations val=\"" << iters
+      << "\"/></LDMMScaleLevel><NTimeSteps val=\"" << T
+      << "\"/><AutoStepReduce val=\"false\"/></LDMMWarpParameterFile>";
+  LDMMParam param;
+  parse_into(param, xml.str());
+  SizeType size(nx, ny, nz);
+  SpacingType sp(spx, spy, spz);
+  OriginType origin(0, 0, 0);
+  RealImage I0(size, origin, sp), I1(size, origin, sp);
+  to_im(i0, I0);
+  to_im(i1, I1);
+  MultiscaleManager scaleManager(size, sp, origin, param);
+  scaleManager.SetScaleVectorFields(false);
+  LDMMDeformationData data(&I0, &I1, param);
+  LDMMIteratorNewCPU iterator(size, origin, sp, T, debug != 0, use_new != 0);
+  const long n = (long)nx * ny * nz;
+  data.InitializeWarp();
+  scaleManager.SetScaleLevel(0);
+  const LDMMScaleLevelParam &lp = param.GetScaleLevel(0);
+  iterator.SetScaleLevel(scaleManager, lp.Iterator());
+  data.SetScaleLevel(scaleManager);
+  data.StepSize(lp.Iterator().StepSize());
+  if (v_init)
+    for (int t = 0; t < T; ++t)
+      to_vf(v + t * 3 * n, v + t * 3 * n + n, v + t * 3 * n + 2 * n, data.v(t));
+  for (int iter = 0; iter < iters; ++iter) {
+    if (iter == 0 && lp.Iterator().UseAdaptiveStepSize()) {
+      iterator.UpdateStepSizeNextIteration();
+      iterator.Iterate(data);
+    }
+    data.SetCurIter(iter);
+    iterator.Iterate(data);
+    if (energies) {
+      // image term sum (J0_{T-1} - I1)^2 * sp^3 (LDMMEnergy::ImageEnergy is
+      // that divided by sigma^2)
+      LDMMEnergy *e = dynamic_cast<LDMMEnergy *>(data.GetEnergyHistory().LastEnergy());
+      energies[iter] = e ? (double)e->ImageEnergy() * sigma * sigma : 0.0;
+    }
+  }
+  for (int t = 0; t < T; ++t)
+    from_vf(data.v(t), v + t * 3 * n, v + t * 3 * n + n, v + t * 3 * n + 2 * n);
+  if (step_out) *step_out = data.StepSize();
   GUARD_END
 }
 
