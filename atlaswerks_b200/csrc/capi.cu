@@ -14,6 +14,7 @@
 #include "greedy.cuh"
 #include "interp.cuh"
 #include "ldmm.cuh"
+#include "multiscale.cuh"
 #include "splat.cuh"
 
 namespace {
@@ -169,6 +170,41 @@ int aw_splat(const float *img, const float *hx, const float *hy, const float *hz
   const cudaError_t e = aw::splat(w, img, hx, hy, hz, out, background, s);
   cudaFreeAsync(scratch, s);
   if (e != cudaSuccess) return cuda_fail(e, "aw_splat");
+  return 0;
+}
+
+int aw_downsample(const float *in, int nx, int ny, int nz, double spx, double spy, double spz,
+                  float *out, int mx, int my, int mz, void *stream) {
+  if (!in || !out) return fail("aw_downsample: null pointer");
+  if (nx < 2 || ny < 2 || nz < 2 || mx < 1 || my < 1 || mz < 1 || mx > nx || my > ny || mz > nz)
+    return fail("aw_downsample: output grid must be non-empty and no larger than the input");
+  if (!spacing_ok(spx, spy, spz)) return fail("aw_downsample: spacing must be positive");
+  const aw::Dims din{nx, ny, nz}, dout{mx, my, mz};
+  cudaStream_t s = S(stream);
+  void *scratch = nullptr;
+  AW_CUDA(cudaMallocAsync(&scratch, aw::downsample_scratch_bytes(din), s), "aw_downsample (scratch)");
+  const cudaError_t e =
+      aw::downsample(in, din, aw::Spacing{spx, spy, spz}, out, dout, scratch, s);
+  cudaFreeAsync(scratch, s);
+  if (e != cudaSuccess) return cuda_fail(e, "aw_downsample");
+  return 0;
+}
+
+int aw_upsample_hfield(const float *hx, const float *hy, const float *hz, int nx, int ny, int nz,
+                       float *ox, float *oy, float *oz, int mx, int my, int mz, int rescale,
+                       void *stream) {
+  if (!hx || !hy || !hz || !ox || !oy || !oz) return fail("aw_upsample_hfield: null pointer");
+  if (nx < 1 || ny < 1 || nz < 1 || mx < 1 || my < 1 || mz < 1)
+    return fail("aw_upsample_hfield: empty grid");
+  const aw::Dims din{nx, ny, nz}, dout{mx, my, mz};
+  cudaStream_t s = S(stream);
+  void *scratch = nullptr;
+  AW_CUDA(cudaMallocAsync(&scratch, sizeof(float) * 3 * din.n(), s), "aw_upsample_hfield (scratch)");
+  const float *h[3] = {hx, hy, hz};
+  float *o[3] = {ox, oy, oz};
+  const cudaError_t e = aw::upsample_hfield(h, din, o, dout, rescale, scratch, s);
+  cudaFreeAsync(scratch, s);
+  if (e != cudaSuccess) return cuda_fail(e, "aw_upsample_hfield");
   return 0;
 }
 

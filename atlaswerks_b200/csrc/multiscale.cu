@@ -1,0 +1,175 @@
+// multiscale.cu — scale-level changes on the device: Gaussian downsampling
+// of images and trilinear upsampling of deformation fields, so a multiscale
+// registration never leaves HBM (the reference round-trips through the
+// host, Greedy/GreedyDeformationDataGPU.cxx:91-130).
+//
+// Arithmetic follows the reference CPU routines exactly:
+//  * GaussianFilter3D::filter_symmetric_full (separable x, y, z passes with
+//    border-renormalised filters, Utilities/DownsampleFilter/GaussianFilter3D.cxx)
+//    and ImageUtils::gaussianDownsample + resampleNew
+//    (UtilitiesDataTypes/ImageUtils.txx:259-349);
+//  * hToVelocity, HField3DUtils::resampleNew with CLAMP and rescaled vectors,
+//    velocityToH (UtilitiesDataTypes/HField3DUtils.txx:57-110, 1816-1881).
+#include <cmath>
+#include <vector>
+
+#include "multiscale.cuh"
+
+namespace aw {
+
+namespace {
+
+// one axis of the separable blur; rows = (K+1) x (K+1) filter table
+__global__ void __launch_bounds__(kRowThreads)
+    k_gauss_axis(const float *__restrict__ in, float *__restrict__ out, Dims d, int axis, int K,
+                 const float *__restrict__ rows) {
+  Voxel v;
+  if (!voxel_of(d, v)) return;
+  const int pos = axis == 0 ? v.x : (axis == 1 ? v.y : v.z);
+  const int n = axis == 0 ? d.nx : (axis == 1 ? d.ny : d.nz);
+  const long st = axis == 0 ? 1 : (axis == 1 ? (long)d.nx : (long)d.nx * d.ny);
+  const long i = v.i;
+  float o;
+  if (pos >= K && pos < n - K) {
+    const float *f = rows;
+    o = fmul(in[i], f[0]);
+    for (int k = 1; k <= K; ++k) o = fadd(o, fmul(fadd(in[i - k * st], in[i + k * st]), f[k]));
+  } else if (pos < K) {
+    const int x = pos;
+    const float *f = rows + (K - x) * (K + 1);
+    o = fmul(in[i], f[0]);
+    for (int k = 1; k <= x; ++k) o = fadd(o, fmul(fadd(in[i - k * st], in[i + k * st]), f[k]));
+    for (int k = x + 1; k <= K; ++k) o = fadd(o, fmul(in[i + k * st], f[k]));
+  } else {
+    const int x = n - 1 - pos;
+    const float *f = rows + (K - x) * (K + 1);
+    o = fmul(in[i], f[0]);
+    for (int k = 1; k <= x; ++k) o = fadd(o, fmul(fadd(in[i + k * st], in[i - k * st]), f[k]));
+    for (int k = x + 1; k <= K; ++k) o = fadd(o, fmul(in[i - k * st], f[k]));
+  }
+  out[i] = o;
+}
+
+// coarse voxel centres sampled from the blurred fine image
+__global__ void __launch_bounds__(kRowThreads)
+    k_resample_down(const float *__restrict__ blur, Dims din, float *__restrict__ out, Dims dout,
+                    Spacing sin, Spacing sout) {
+  Voxel v;
+  if (!voxel_of(dout, v)) return;
+  const double ox = (sout.x - sin.x) / 2.0, oy = (sout.y - sin.y) / 2.0,
+               oz = (sout.z - sin.z) / 2.0;
+  const double wx = dadd(dadd(dmul(sout.x, (double)v.x), 0.0), ox);
+  const double wy = dadd(dadd(dmul(sout.y, (double)v.y), 0.0), oy);
+  const double wz = dadd(dadd(dmul(sout.z, (double)v.z), 0.0), oz);
+  const double px = __ddiv_rn(dsub(wx, 0.0), sin.x), py = __ddiv_rn(dsub(wy, 0.0), sin.y),
+               pz = __ddiv_rn(dsub(wz, 0.0), sin.z);
+  out[v.i] = trilerp_scalar(blur, din, px, py, pz, 0.0f);
+}
+
+// v = (h - x) * 1.0, the field hToVelocity hands to resampleNew
+__global__ void __launch_bounds__(kRowThreads)
+    k_h_to_v(const float *__restrict__ hx, const float *__restrict__ hy,
+             const float *__restrict__ hz, float *__restrict__ v, Dims d) {
+  Voxel p;
+  if (!voxel_of(d, p)) return;
+  const long n = d.n();
+  v[p.i] = fsub(hx[p.i], __int2float_rn(p.x));
+  v[n + p.i] = fsub(hy[p.i], __int2float_rn(p.y));
+  v[2 * n + p.i] = fsub(hz[p.i], __int2float_rn(p.z));
+}
+
+__global__ void __launch_bounds__(kRowThreads)
+    k_upsample_field(const float *__restrict__ v, Dims din, float *__restrict__ ox,
+                     float *__restrict__ oy, float *__restrict__ oz, Dims dout, int rescale) {
+  Voxel p;
+  if (!voxel_of(dout, p)) return;
+  const double rX = (double)din.nx / dout.nx, rY = (double)din.ny / dout.ny,
+               rZ = (double)din.nz / dout.nz;
+  const double oX = (rX - 1.0) / 2.0, oY = (rY - 1.0) / 2.0, oZ = (rZ - 1.0) / 2.0;
+  const float ix = __double2float_rn(dadd(oX, dmul((double)p.x, rX)));
+  const float iy = __double2float_rn(dadd(oY, dmul((double)p.y, rY)));
+  const float iz = __double2float_rn(dadd(oZ, dmul((double)p.z, rZ)));
+  const long n = din.n();
+  float a, b, c;
+  trilerp_vector(v, v + n, v + 2 * n, din, ix, iy, iz, BG_CLAMP, 1.0f, a, b, c);
+  if (rescale) {
+    a = fmul(a, __double2float_rn(1.0 / rX));
+    b = fmul(b, __double2float_rn(1.0 / rY));
+    c = fmul(c, __double2float_rn(1.0 / rZ));
+  }
+  ox[p.i] = fadd(__int2float_rn(p.x), a);
+  oy[p.i] = fadd(__int2float_rn(p.y), b);
+  oz[p.i] = fadd(__int2float_rn(p.z), c);
+}
+
+// GaussianFilter3D::filter_generate_gauss_full, float arithmetic as there
+void gauss_rows(float sigma, int size, std::vector<float> &rows) {
+  rows.assign((size_t)(size + 1) * (size + 1), 0.0f);
+  float *f0 = rows.data();
+  const float exp_scale = (float)(1.0 / (2.0 * sigma * sigma));
+  float scale = f0[0] = 1.0f;
+  for (int i = 1; i <= size; ++i) {
+    f0[i] = expf(-(float)(i * i) * exp_scale);
+    scale = (float)(scale + 2.0 * f0[i]);
+  }
+  scale = (float)(1.0 / scale);
+  for (int i = 0; i <= size; ++i) f0[i] *= scale;
+  scale = 0.0f;
+  for (int j = 1; j <= size; ++j) {
+    scale += f0[size + 1 - j];
+    for (int i = 0; i <= size; ++i) rows[(size_t)j * (size + 1) + i] = (float)(f0[i] / (1. - scale));
+  }
+}
+
+}  // namespace
+
+size_t downsample_scratch_bytes(const Dims &din) {
+  // two blur buffers + three filter tables of at most (2*ceil(sqrt(n/2))+1)^2
+  const size_t fl = 3 * 64 * 64;
+  return sizeof(float) * (2 * (size_t)din.n() + fl);
+}
+
+cudaError_t downsample(const float *in, Dims din, Spacing sin, float *out, Dims dout,
+                       void *scratch, cudaStream_t s) {
+  const double f[3] = {(double)din.nx / dout.nx, (double)din.ny / dout.ny,
+                       (double)din.nz / dout.nz};
+  const int n[3] = {din.nx, din.ny, din.nz};
+  float *b1 = static_cast<float *>(scratch);
+  float *b2 = b1 + din.n();
+  float *tab = b2 + din.n();
+  const float *src = in;
+  float *dst[3] = {b1, b2, b1};
+  for (int a = 0; a < 3; ++a) {
+    const double sg = std::sqrt(f[a] / 2.0);
+    int K = 2 * (int)std::ceil(sg);
+    if (K > n[a] / 2 - 1) K = n[a] / 2 - 1;
+    if (K < 0) K = 0;
+    if ((K + 1) * (K + 1) > 64 * 64) return cudaErrorInvalidValue;
+    std::vector<float> rows;
+    gauss_rows((float)sg, K, rows);
+    float *t = tab + a * 64 * 64;
+    // from pageable memory: the call returns once the table has been staged
+    cudaError_t e = cudaMemcpyAsync(t, rows.data(), rows.size() * sizeof(float),
+                                    cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+    k_gauss_axis<<<row_grid(din), kRowThreads, 0, s>>>(src, dst[a], din, a, K, t);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    src = dst[a];
+  }
+  // the blur's output spacing is the input's; the coarse grid's is
+  // sin * (nin / nout) (gaussianDownsample)
+  const Spacing sout{sin.x * f[0], sin.y * f[1], sin.z * f[2]};
+  k_resample_down<<<row_grid(dout), kRowThreads, 0, s>>>(src, din, out, dout, sin, sout);
+  return cudaGetLastError();
+}
+
+cudaError_t upsample_hfield(const float *const h[3], Dims din, float *const out[3], Dims dout,
+                            int rescale, void *scratch, cudaStream_t s) {
+  float *v = static_cast<float *>(scratch);
+  k_h_to_v<<<row_grid(din), kRowThreads, 0, s>>>(h[0], h[1], h[2], v, din);
+  k_upsample_field<<<row_grid(dout), kRowThreads, 0, s>>>(v, din, out[0], out[1], out[2], dout,
+                                                          rescale);
+  return cudaGetLastError();
+}
+
+}  // namespace aw

@@ -164,12 +164,18 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// weight of corner (cx, cy, cz) of source i, rounded to float as
-// forwardApply does: ((ax)*(ay))*(az) in double, ax = 1 - rx or rx
+// weight of corner (cx, cy, cz) of a source at p, rounded to float as
+// forwardApply writes it (HField3DUtils.txx:1116-1123): the product runs left
+// to right, in double once a (1.0 - r) factor has entered it and in float
+// before, so w110 = (rx*ry in float) * (1.0 - rz) and w111 = rx*ry*rz in float.
 AW_D float corner_weight(float px, float py, float pz, int cx, int cy, int cz) {
   const int fx = ref_floor_f(px), fy = ref_floor_f(py), fz = ref_floor_f(pz);
   const float rx = fsub(px, __int2float_rn(fx)), ry = fsub(py, __int2float_rn(fy)),
               rz = fsub(pz, __int2float_rn(fz));
+  if (cx && cy) {
+    const float rxy = fmul(rx, ry);
+    return cz ? fmul(rxy, rz) : __double2float_rn(dmul((double)rxy, dsub(1.0, (double)rz)));
+  }
   const double ax = cx ? (double)rx : dsub(1.0, (double)rx);
   const double ay = cy ? (double)ry : dsub(1.0, (double)ry);
   const double az = cz ? (double)rz : dsub(1.0, (double)rz);

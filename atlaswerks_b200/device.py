@@ -101,3 +101,24 @@ def splat(img: torch.Tensor, h: torch.Tensor, background: float = 0.0) -> torch.
                               background, _stream()))
     return out
 
+
+def downsample(img: torch.Tensor, new_shape, spacing=(1.0, 1.0, 1.0)) -> torch.Tensor:
+    """ImageUtils::gaussianDownsample to new_shape = (nz, ny, nx)."""
+    _check_image(img, "img")
+    out = torch.empty(tuple(new_shape), device=img.device, dtype=torch.float32)
+    mz, my, mx = new_shape
+    check(_lib.lib().aw_downsample(_p(img), *_dims(img), *map(float, spacing), _p(out), mx, my,
+                                   mz, _stream()))
+    return out
+
+
+def upsample_hfield(h: torch.Tensor, new_shape, rescale: bool = True) -> torch.Tensor:
+    """hToVelocity + resampleNew(CLAMP) + velocityToH to new_shape."""
+    _check_field(h, "h")
+    out = torch.empty((3,) + tuple(new_shape), device=h.device, dtype=torch.float32)
+    mz, my, mx = new_shape
+    check(_lib.lib().aw_upsample_hfield(_p(h[0]), _p(h[1]), _p(h[2]), *_dims(h), _p(out[0]),
+                                        _p(out[1]), _p(out[2]), mx, my, mz, int(rescale),
+                                        _stream()))
+    return out
+

@@ -51,7 +51,8 @@ def smooth_displacement(shape: Shape, umax: float, rng: np.random.Generator,
     ky = np.fft.fftfreq(ny)[None, :, None]
     kx = np.fft.rfftfreq(nx)[None, None, :]
     g = np.exp(-2.0 * (np.pi * sigma) ** 2 * (kx ** 2 + ky ** 2 + kz ** 2))
-    u = np.stack([np.fft.irfftn(np.fft.rfftn(noise[c]) * g, s=shape) for c in range(3)])
+    u = np.stack([np.fft.irfftn(np.fft.rfftn(noise[c]) * g, s=shape, axes=(0, 1, 2))
+                  for c in range(3)])
     mag = np.sqrt((u ** 2).sum(0)).max()
     u *= umax / mag
     return u.astype(np.float32)

@@ -85,6 +85,23 @@ int aw_compose_vh(const float *vx, const float *vy, const float *vz, const float
 int aw_splat(const float *img, const float *hx, const float *hy, const float *hz, float *out,
              int nx, int ny, int nz, float background, void *stream);
 
+/* Gaussian downsampling of an image to a coarser grid (out: mx*my*mz):
+ * ImageUtils::gaussianDownsample (UtilitiesDataTypes/ImageUtils.txx:259-298),
+ * sigma = sqrt(n/m / 2) per axis, as MultiscaleManager::DownsampleToLevel
+ * uses it (Algorithms/Common/MultiscaleManager.cxx:344-366). (spx, spy, spz)
+ * is the input spacing. Scratch from the stream-ordered allocator. */
+int aw_downsample(const float *in, int nx, int ny, int nz, double spx, double spy, double spz,
+                  float *out, int mx, int my, int mz, void *stream);
+
+/* Deformation upsampling to a finer grid: hToVelocity, trilinear resampling
+ * with CLAMP background and vectors rescaled by the size ratio when rescale
+ * is set, velocityToH — GreedyDeformationData::SetScaleLevel
+ * (Algorithms/Greedy/GreedyDeformationData.cxx:211-221) through
+ * MultiscaleManager::UpsampleToLevel (MultiscaleManager.cxx:326-342). */
+int aw_upsample_hfield(const float *hx, const float *hy, const float *hz, int nx, int ny, int nz,
+                       float *ox, float *oy, float *oz, int mx, int my, int mz, int rescale,
+                       void *stream);
+
 /* ---------------------------------------------------------------------------
  * Fluid kernel. Replaces KernelInterfaceGPU / DiffOperGPU
  * (Algorithms/Common/KernelInterfaceGPU.h:20-43, Common/DiffOperGPU.cxx:32-205)

@@ -144,6 +144,50 @@ class Oracle:
                                            _i(int(inverse)))
         return o
 
+    def downsample(self, img, new_shape, sp=(1.0, 1.0, 1.0)):
+        """ImageUtils::gaussianDownsample to new_shape = (nz, ny, nx)."""
+        out = np.empty(new_shape, np.float32)
+        mz, my, mx = new_shape
+        self.lib.aw_oracle_downsample(_fp(img), *_shape(img), *map(_dbl, sp), _fp(out),
+                                      _i(mx), _i(my), _i(mz))
+        return out
+
+    def upsample_hfield(self, h, new_shape, rescale=True):
+        out = np.empty((3,) + tuple(new_shape), np.float32)
+        mz, my, mx = new_shape
+        self.lib.aw_oracle_upsample_hfield(_fp(np.ascontiguousarray(h)), *_shape(h), _fp(out),
+                                           _i(mx), _i(my), _i(mz), _i(int(rescale)))
+        return out
+
+    def greedy_warp(self, I0, I1, levels, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01,
+                    gamma=0.001, inverse=False):
+        """Multiscale greedy (GreedyWarp::RunWarp); levels = [(factor, iters,
+        max_pert)], any order. Returns (h, hinv, energies per level)."""
+        levels = sorted(levels, key=lambda l: -l[0])
+        shape = I0.shape
+        h = hinv = None
+        energies = []
+        for li, (f, iters, mp) in enumerate(levels):
+            size = tuple(n // f for n in shape)
+            lsp = tuple(float(np.float32(s) * np.float32(f)) for s in sp)
+            if size == tuple(shape):
+                a, b = I0, I1
+            else:
+                a, b = self.downsample(I0, size, sp), self.downsample(I1, size, sp)
+            if li == 0:
+                h = identity(size)
+                hinv = identity(size) if inverse else None
+            else:
+                h = self.upsample_hfield(h, size, True)
+                hinv = self.upsample_hfield(hinv, size, True) if inverse else None
+            step, es = 0.0, []
+            for it in range(iters):
+                e, step = self.greedy_iterate(a, b, h, hinv, lsp, alpha, beta, gamma, mp,
+                                              update_step=(it == 0), step=step)
+                es.append(e)
+            energies.append(np.array(es))
+        return h, hinv, energies
+
     def max_norm(self, v):
         return float(self.lib.aw_oracle_max_norm(_fp(v[0]), _fp(v[1]), _fp(v[2]),
                                                  ctypes.c_long(v[0].size)))
@@ -260,6 +304,23 @@ class Reference:
         out = np.empty_like(img)
         self._check(self.lib.awref_splat(_fp(img), _fp(h[0]), _fp(h[1]), _fp(h[2]), _fp(out),
                                          *_shape(img)))
+        return out
+
+    def downsample(self, img, new_shape, sp=(1.0, 1.0, 1.0)):
+        out = np.empty(new_shape, np.float32)
+        mz, my, mx = new_shape
+        with quiet_stdout():
+            rc = self.lib.awref_downsample(_fp(img), *_shape(img), *map(_dbl, sp), _fp(out),
+                                           _i(mx), _i(my), _i(mz))
+        self._check(rc)
+        return out
+
+    def upsample_hfield(self, h, new_shape, rescale=True):
+        out = np.empty((3,) + tuple(new_shape), np.float32)
+        mz, my, mx = new_shape
+        self._check(self.lib.awref_upsample_hfield(_fp(np.ascontiguousarray(h)), *_shape(h),
+                                                   _fp(out), _i(mx), _i(my), _i(mz),
+                                                   _i(int(rescale))))
         return out
 
     def fluid(self, v, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01, gamma=0.001, inverse=True):

@@ -568,3 +568,150 @@ double aw_oracle_ldmm_iterate(const float *I0, const float *I1, float *v, int T,
   free(f);
   return e;
 }
+
+/* ------------------------------------------------------------------------
+ * Multiscale (Algorithms/Common/MultiscaleManager.cxx:301-366).
+ * ---------------------------------------------------------------------- */
+
+/* GaussianFilter3D::filter_generate_gauss_full
+ * (Utilities/DownsampleFilter/GaussianFilter3D.cxx): row 0 is the
+ * normalised half filter, row j the filter renormalised for an element j
+ * voxels from the border. float arithmetic as written there. */
+static void gauss_filter_rows(float sigma, int size, float *rows /* (size+1)^2 */) {
+  float *f0 = rows;
+  const float exp_scale = (float)(1.0 / (2.0 * sigma * sigma));
+  float scale = f0[0] = 1.0f;
+  for (int i = 1; i <= size; ++i) {
+    f0[i] = expf(-(float)(i * i) * exp_scale);
+    scale = (float)(scale + 2.0 * f0[i]);
+  }
+  scale = (float)(1.0 / scale);
+  for (int i = 0; i <= size; ++i) f0[i] *= scale;
+  scale = 0.0f;
+  for (int j = 1; j <= size; ++j) {
+    scale += f0[size + 1 - j];
+    for (int i = 0; i <= size; ++i) rows[j * (size + 1) + i] = (float)(f0[i] / (1. - scale));
+  }
+}
+
+/* one axis of GaussianFilter3D::filter_symmetric_full: n samples spaced
+ * `stride` apart, K the half kernel size */
+static void gauss_line(const float *in, float *out, int n, long stride, int K, const float *rows) {
+  const float *f = rows;
+  for (int x = K; x < n - K; ++x) {
+    float o = in[x * stride] * f[0];
+    for (int i = 1; i <= K; ++i) o += (in[(x - i) * stride] + in[(x + i) * stride]) * f[i];
+    out[x * stride] = o;
+  }
+  for (int x = K - 1; x >= 0; --x) {
+    f = rows + (K - x) * (K + 1);
+    float o = in[x * stride] * f[0];
+    for (int i = 1; i <= x; ++i) o += (in[(x - i) * stride] + in[(x + i) * stride]) * f[i];
+    for (int i = x + 1; i <= K; ++i) o += in[(x + i) * stride] * f[i];
+    out[x * stride] = o;
+    const int r = n - 1 - x;
+    o = in[r * stride] * f[0];
+    for (int i = 1; i <= x; ++i) o += (in[(r + i) * stride] + in[(r - i) * stride]) * f[i];
+    for (int i = x + 1; i <= K; ++i) o += in[(r - i) * stride] * f[i];
+    out[r * stride] = o;
+  }
+}
+
+/* Separable Gaussian blur, x then y then z; kernel half sizes clamped to
+ * n/2 - 1 as filter_symmetric_full does. */
+void aw_oracle_gauss_blur(const float *in, float *out, int nx, int ny, int nz, float sx, float sy,
+                          float sz, int kx, int ky, int kz) {
+  const long n = (long)nx * ny * nz;
+  int K[3] = {kx, ky, kz};
+  const int N[3] = {nx, ny, nz};
+  for (int a = 0; a < 3; ++a)
+    if (K[a] > N[a] / 2 - 1) K[a] = N[a] / 2 - 1;
+  float *b1 = (float *)calloc((size_t)n, sizeof(float));
+  float *b2 = (float *)calloc((size_t)n, sizeof(float));
+  float *rows;
+  rows = (float *)malloc(sizeof(float) * (size_t)((K[0] + 1) * (K[0] + 1)));
+  gauss_filter_rows(sx, K[0], rows);
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y) gauss_line(in + IDX(0, y, z), b1 + IDX(0, y, z), nx, 1, K[0], rows);
+  free(rows);
+  rows = (float *)malloc(sizeof(float) * (size_t)((K[1] + 1) * (K[1] + 1)));
+  gauss_filter_rows(sy, K[1], rows);
+  for (int z = 0; z < nz; ++z)
+    for (int x = 0; x < nx; ++x) gauss_line(b1 + IDX(x, 0, z), b2 + IDX(x, 0, z), ny, nx, K[1], rows);
+  free(rows);
+  rows = (float *)malloc(sizeof(float) * (size_t)((K[2] + 1) * (K[2] + 1)));
+  gauss_filter_rows(sz, K[2], rows);
+  for (int y = 0; y < ny; ++y)
+    for (int x = 0; x < nx; ++x)
+      gauss_line(b2 + IDX(x, y, 0), out + IDX(x, y, 0), nz, (long)nx * ny, K[2], rows);
+  free(rows);
+  free(b1);
+  free(b2);
+}
+
+/* ImageUtils::gaussianDownsample + resampleNew (UtilitiesDataTypes/
+ * ImageUtils.txx:259-349): sigma = sqrt(factor/2), half kernel 2*ceil(sigma),
+ * then a trilinear sample of the blurred image at the centres of the
+ * coarse voxels, background 0. Spacing of the input is (spx, spy, spz). */
+void aw_oracle_downsample(const float *in, int nx, int ny, int nz, double spx, double spy,
+                          double spz, float *out, int mx, int my, int mz) {
+  const double fx = (double)nx / mx, fy = (double)ny / my, fz = (double)nz / mz;
+  const double sgx = sqrt(fx / 2.0), sgy = sqrt(fy / 2.0), sgz = sqrt(fz / 2.0);
+  const int kx = 2 * (int)ceil(sgx), ky = 2 * (int)ceil(sgy), kz = 2 * (int)ceil(sgz);
+  const long n = (long)nx * ny * nz;
+  float *blur = (float *)malloc(sizeof(float) * (size_t)n);
+  aw_oracle_gauss_blur(in, blur, nx, ny, nz, (float)sgx, (float)sgy, (float)sgz, kx, ky, kz);
+  const double dsx = spx * fx, dsy = spy * fy, dsz = spz * fz;
+  const double ox = (dsx - spx) / 2.0, oy = (dsy - spy) / 2.0, oz = (dsz - spz) / 2.0;
+  for (int z = 0; z < mz; ++z)
+    for (int y = 0; y < my; ++y)
+      for (int x = 0; x < mx; ++x) {
+        const double wx = dsx * x + 0.0 + ox, wy = dsy * y + 0.0 + oy, wz = dsz * z + 0.0 + oz;
+        const double vx = (wx - 0.0) / spx, vy = (wy - 0.0) / spy, vz = (wz - 0.0) / spz;
+        out[((long)z * my + y) * mx + x] = trilerp_val(blur, nx, ny, nz, vx, vy, vz, 0.0f);
+      }
+  free(blur);
+}
+
+/* Upsampling a deformation to the next scale level, as
+ * GreedyDeformationData::SetScaleLevel does it (Greedy/GreedyDeformationData.cxx:
+ * 211-221): hToVelocity, HField3DUtils::resampleNew with CLAMP and the
+ * vectors rescaled by out/in size (HField3DUtils.txx:1816-1881), velocityToH. */
+void aw_oracle_upsample_hfield(const float *h, int nx, int ny, int nz, float *out, int mx, int my,
+                               int mz, int rescale) {
+  const long n = (long)nx * ny * nz, m = (long)mx * my * mz;
+  float *v = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const long i = IDX(x, y, z);
+        v[i] = (float)((double)(h[i] - (float)x) * 1.0);
+        v[n + i] = (float)((double)(h[n + i] - (float)y) * 1.0);
+        v[2 * n + i] = (float)((double)(h[2 * n + i] - (float)z) * 1.0);
+      }
+  const double rX = (double)nx / mx, rY = (double)ny / my, rZ = (double)nz / mz;
+  const double oX = (rX - 1.0) / 2.0, oY = (rY - 1.0) / 2.0, oZ = (rZ - 1.0) / 2.0;
+  const float s[3] = {(float)(1.0 / rX), (float)(1.0 / rY), (float)(1.0 / rZ)};
+  for (int z = 0; z < mz; ++z) {
+    const double iz = oZ + z * rZ;
+    for (int y = 0; y < my; ++y) {
+      const double iy = oY + y * rY;
+      for (int x = 0; x < mx; ++x) {
+        const double ix = oX + x * rX;
+        const long o = ((long)z * my + y) * mx + x;
+        float a, b, c;
+        trilerp_vec(v, v + n, v + 2 * n, nx, ny, nz, (float)ix, (float)iy, (float)iz, &a, &b, &c,
+                    AW_BG_CLAMP);
+        if (rescale) {
+          a *= s[0];
+          b *= s[1];
+          c *= s[2];
+        }
+        out[o] = (float)(x + a / 1.0);
+        out[m + o] = (float)(y + b / 1.0);
+        out[2 * m + o] = (float)(z + c / 1.0);
+      }
+    }
+  }
+  free(v);
+}

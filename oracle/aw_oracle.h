@@ -56,6 +56,13 @@ double aw_oracle_ldmm_iterate(const float *I0, const float *I1, float *v, int T,
                               double beta, double gamma, float sigma, float *step,
                               int update_step, float max_pert);
 
+void aw_oracle_gauss_blur(const float *in, float *out, int nx, int ny, int nz, float sx, float sy,
+                          float sz, int kx, int ky, int kz);
+void aw_oracle_downsample(const float *in, int nx, int ny, int nz, double spx, double spy,
+                          double spz, float *out, int mx, int my, int mz);
+void aw_oracle_upsample_hfield(const float *h, int nx, int ny, int nz, float *out, int mx, int my,
+                               int mz, int rescale);
+
 #ifdef __cplusplus
 }
 #endif

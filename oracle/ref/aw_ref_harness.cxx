@@ -24,6 +24,7 @@
 #include "GreedyIteratorCPU.h"
 #include "GreedyParam.h"
 #include "HField3DUtils.h"
+#include "ImageUtils.h"
 #include "LDMMDeformationData.h"
 #include "LDMMEnergy.h"
 #include "LDMMIteratorCPU.h"
@@ -306,6 +307,35 @@ int awref_greedy_run(const float *i0, const float *i1, int nx, int ny, int nz, d
   const long n = (long)nx * ny * nz;
   from_vf(data.Def1To0(), h_out, h_out + n, h_out + 2 * n);
   if (compute_inverse && hinv_out) from_vf(data.Def0To1(), hinv_out, hinv_out + n, hinv_out + 2 * n);
+  GUARD_END
+}
+
+/* ImageUtils::gaussianDownsample (MultiscaleManager::DownsampleToLevel) */
+int awref_downsample(const float *in, int nx, int ny, int nz, double spx, double spy, double spz,
+                     float *out, int mx, int my, int mz) {
+  GUARD_BEGIN
+  RealImage I(SizeType(nx, ny, nz), OriginType(0, 0, 0), SpacingType(spx, spy, spz));
+  to_im(in, I);
+  RealImage O;
+  ImageUtils::gaussianDownsample(I, O, Vector3D<unsigned int>(mx, my, mz));
+  from_im(O, out);
+  GUARD_END
+}
+
+/* hToVelocity + resampleNew(CLAMP, rescale) + velocityToH, the deformation
+ * upsampling of GreedyDeformationData::SetScaleLevel */
+int awref_upsample_hfield(const float *h, int nx, int ny, int nz, float *out, int mx, int my,
+                          int mz, int rescale) {
+  GUARD_BEGIN
+  VectorField f(nx, ny, nz);
+  const long n = (long)nx * ny * nz, m = (long)mx * my * mz;
+  to_vf(h, h + n, h + 2 * n, f);
+  HField3DUtils::hToVelocity(f);
+  VectorField t(mx, my, mz);
+  HField3DUtils::resampleNew(f, t, Vector3D<unsigned int>(mx, my, mz),
+                             HField3DUtils::BACKGROUND_STRATEGY_CLAMP, rescale != 0);
+  HField3DUtils::velocityToH(t);
+  from_vf(t, out, out + m, out + 2 * m);
   GUARD_END
 }
 

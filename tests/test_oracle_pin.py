@@ -1,0 +1,81 @@
+"""The oracle (C restatement, oracle/aw_oracle.c) against the reference's own
+CPU code built from its sources (oracle/_ref): CPU only.
+
+Interpolation, gradient, compose and splat must agree bit for bit; the fluid
+operator to FP64 rounding of float-valued parameters; greedy and LDMM
+iterations to the FP32 rounding of the reference's FFT.
+"""
+import numpy as np
+import pytest
+
+from atlaswerks_b200.synth import greedy_pair
+from oracle import BG_PARTIAL_ID, identity
+
+SHAPES = [(12, 11, 10), (8, 9, 17), (16, 16, 16)]
+SP = (1.0, 1.3, 0.8)
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_interpolation_family_bit_exact(oracle, reference, shape):
+    rng = np.random.default_rng(0)
+    img = rng.random(shape, dtype=np.float32)
+    h = identity(shape) + rng.normal(0, 1.5, (3,) + shape).astype(np.float32)
+    v = rng.normal(0, 1.0, (3,) + shape).astype(np.float32)
+    assert np.array_equal(oracle.apply(img, h), reference.apply(img, h))
+    for wrap in (False, True):
+        assert np.array_equal(oracle.gradient(img, SP, wrap), reference.gradient(img, SP, wrap))
+    for bg in range(6):
+        for d in (1, -1):
+            assert np.array_equal(oracle.compose_hv(h, v, SP, d, bg),
+                                  reference.compose_hv(h, v, SP, d, bg))
+            assert np.array_equal(oracle.compose_vh(v, h, SP, d, bg),
+                                  reference.compose_vh(v, h, SP, d, bg))
+    assert np.array_equal(oracle.splat(img, h), reference.splat(img, h))
+
+
+@pytest.mark.parametrize("inverse", [True, False])
+def test_fluid_fp64_matches_reference_fp64(oracle, reference, inverse):
+    rng = np.random.default_rng(1)
+    f = rng.normal(0, 1, (3, 12, 11, 10)).astype(np.float32)
+    # the reference holds alpha, beta, gamma as float (Real)
+    a, b, g = (float(np.float32(x)) for x in (0.01, 0.01, 0.001))
+    want = reference.fluid_f64(f, SP, a, b, g, inverse)
+    got = oracle.fluid_f64(f, SP, a, b, g, inverse)
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+    # the reference's FP32 operator (FFT in FP64 through the shim, solve in FP32)
+    w32 = reference.fluid(f, SP, a, b, g, inverse)
+    assert np.abs(w32 - want).max() <= 1e-6 * np.abs(want).max()
+
+
+def test_greedy_iterations_match_reference(oracle, reference):
+    shape = (24, 20, 16)
+    I0, I1 = greedy_pair(shape, 1, n_blobs=4, umax=2.0)
+    hr, hir, er, sr = reference.greedy_run(I0, I1, [1], [10], [0.5], inverse=True)
+    ho, hio, eo, so = oracle.greedy_run(I0, I1, 10, max_pert=0.5, inverse=True)
+    assert np.abs(ho - hr).max() <= 1e-5
+    assert abs(sr[-1] - so) <= 1e-6 * so
+    assert np.allclose(eo, er, rtol=1e-5)
+    # the inverse field agrees except where the reference interpolates v in
+    # the padded FFTW array (x >= nx - 1; see the restatement's notes)
+    m = hio[0] < shape[2] - 1.0
+    assert np.abs(hio - hir)[:, m].max() <= 1e-5
+
+
+def test_ldmm_iterations_match_reference(oracle, reference):
+    shape, T = (16, 14, 12), 4
+    I0, I1 = greedy_pair(shape, 3, n_blobs=4, umax=2.0)
+    vr, er, _ = reference.ldmm_run(I0, I1, T, 3, sigma=1.0, step=0.01)
+    v = np.zeros((T, 3) + shape, np.float32)
+    eo = [oracle.ldmm_iterate(I0, I1, v, sigma=1.0, step=0.01)[0] for _ in range(3)]
+    assert np.abs(v - vr).max() <= 1e-5 * np.abs(vr).max()
+    assert np.allclose(eo, er, rtol=1e-5)
+
+
+def test_ldmm_adaptive_step_matches_reference(oracle, reference):
+    shape, T = (16, 14, 12), 4
+    I0, I1 = greedy_pair(shape, 3, n_blobs=4, umax=2.0)
+    _, _, sr = reference.ldmm_run(I0, I1, T, 1, sigma=0.1, step=0.005, adaptive=True,
+                                  max_pert=0.1)
+    v = np.zeros((T, 3) + shape, np.float32)
+    _, so = oracle.ldmm_iterate(I0, I1, v, sigma=0.1, step=0.005, update_step=True, max_pert=0.1)
+    assert abs(so - sr) <= 1e-5 * sr
