@@ -46,6 +46,7 @@ SIGNATURES = {
     "aw_compose_hv": ([_fp] * 9 + [_i] * 3 + [_d] * 3 + [_f, _i, _i, _fp], _i),
     "aw_compose_vh": ([_fp] * 9 + [_i] * 3 + [_d] * 3 + [_f, _i, _i, _fp], _i),
     "aw_splat": ([_fp] * 5 + [_i] * 3 + [_f, _fp], _i),
+    "aw_splat_static": ([_fp] * 5 + [_i] * 3 + [_f, _fp], _i),
     "aw_downsample": ([_fp, _i, _i, _i, _d, _d, _d, _fp, _i, _i, _i, _fp], _i),
     "aw_upsample_hfield": ([_fp] * 3 + [_i] * 3 + [_fp] * 3 + [_i] * 4 + [_fp], _i),
     "aw_fluid_create": ([_i] * 3 + [_d] * 3 + [_f] * 3 + [_fp], _i),

@@ -64,6 +64,10 @@ inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
 }  // namespace
 
+namespace aw {
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+}  // namespace aw
+
 struct aw_fluid_s {
   aw::FluidPlan plan;
 };

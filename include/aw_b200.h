@@ -102,6 +102,23 @@ int aw_upsample_hfield(const float *hx, const float *hy, const float *hz, int nx
                        float *ox, float *oy, float *oz, int mx, int my, int mz, int rescale,
                        void *stream);
 
+/* Scratch capacity of aw_splat_static, fixed when the library is built. */
+#define AW_SPLAT_STATIC_MAX_BYTES (8u << 20)
+
+/* aw_splat for callers that must not allocate device memory while they run
+ * (no counterpart in the reference): a host that owns all device memory
+ * through its own pool, or a latency-critical loop where an allocation may
+ * block or fail. Same result as aw_splat, bit for bit. The scratch is one
+ * fixed array of AW_SPLAT_STATIC_MAX_BYTES in the library's device memory
+ * (held on every device that loads the library until the process exits);
+ * grids whose scratch (about 12 bytes per voxel, e.g. up to 80^3) exceeds it
+ * are rejected with an error. The first call on each device looks up the
+ * array's device address, so make it before any stream capture. All calls
+ * share the one array: calls that overlap on the GPU (other streams, other
+ * host threads) race and must be serialised by the caller. */
+int aw_splat_static(const float *img, const float *hx, const float *hy, const float *hz,
+                    float *out, int nx, int ny, int nz, float background, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Fluid kernel. Replaces KernelInterfaceGPU / DiffOperGPU
  * (Algorithms/Common/KernelInterfaceGPU.h:20-43, Common/DiffOperGPU.cxx:32-205)
