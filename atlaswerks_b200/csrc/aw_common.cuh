@@ -56,6 +56,21 @@ AW_D float fadd(float a, float b) { return __fadd_rn(a, b); }
 AW_D float fsub(float a, float b) { return __fsub_rn(a, b); }
 AW_D float fdiv(float a, float b) { return __fdiv_rn(a, b); }
 
+// Atlas subjects on grids of their own: a deformation lives on the template
+// grid (n voxels per axis) and points into the subject's grid (m voxels per
+// axis) through the map of voxel centres of equal physical extent,
+// p -> (p + 0.5) * (m / n) - 0.5, in double. `on` is 0 when m == n, and the
+// sample point is then h itself, as in the reference's equal-grid atlas.
+struct AtlasMap {
+  int on;
+  double r[3];  // m / n per axis
+};
+AW_D void atlas_point(const AtlasMap &a, double &x, double &y, double &z) {
+  x = dsub(dmul(dadd(x, 0.5), a.r[0]), 0.5);
+  y = dsub(dmul(dadd(y, 0.5), a.r[1]), 0.5);
+  z = dsub(dmul(dadd(z, 0.5), a.r[2]), 0.5);
+}
+
 // floor as the reference computes it: truncate, then step down for
 // negative non-integers (Array3DUtils.txx:70-75)
 AW_D int ref_floor_d(double x) {
@@ -90,8 +105,9 @@ AW_D float trilerp_scalar(const float *__restrict__ a, const Dims d, double x, d
   float c[8];
   const bool inside = fx >= 0 && cx < d.nx && fy >= 0 && cy < d.ny && fz >= 0 && cz < d.nz;
   if (inside) {
-    const long b = d.idx(fx, fy, fz);
-    const long sy = d.nx, sz = (long)d.nx * d.ny;
+    // 32-bit offsets: every grid here has fewer than 2^31 voxels
+    const int b = (fz * d.ny + fy) * d.nx + fx;
+    const int sy = d.nx, sz = d.nx * d.ny;
     c[0] = __ldg(a + b);
     c[1] = __ldg(a + b + 1);
     c[2] = __ldg(a + b + sy + 1);
@@ -154,12 +170,37 @@ AW_D void trilerp_vector(const float *__restrict__ hx, const float *__restrict__
   const int Z[8] = {fz, fz, fz, fz, cz, cz, cz, cz};
   float cxv[8], cyv[8], czv[8];
   if (inside) {
+    // corner offsets from one 32-bit base (grids have < 2^31 voxels); CLAMP
+    // and WRAP corners are not a unit cube, so they index each corner
+    const int sy = d.nx, sz = d.nx * d.ny;
+    int off[8];
+    if (bgs == BG_WRAP || bgs == BG_CLAMP) {
+#pragma unroll
+      for (int c = 0; c < 8; ++c) off[c] = (Z[c] * d.ny + Y[c]) * d.nx + X[c];
+    } else {
+      const int b = (fz * d.ny + fy) * d.nx + fx;
+      off[0] = b;
+      off[1] = b + 1;
+      off[2] = b + sy + 1;
+      off[3] = b + sy;
+      off[4] = b + sy + sz;
+      off[5] = b + sy + sz + 1;
+      off[6] = b + sz + 1;
+      off[7] = b + sz;
+    }
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-      const long i = d.idx(X[c], Y[c], Z[c]);
-      cxv[c] = fmul(__ldg(hx + i), scale);
-      cyv[c] = fmul(__ldg(hy + i), scale);
-      czv[c] = fmul(__ldg(hz + i), scale);
+      cxv[c] = __ldg(hx + off[c]);
+      cyv[c] = __ldg(hy + off[c]);
+      czv[c] = __ldg(hz + off[c]);
+    }
+    if (scale != 1.0f) {
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        cxv[c] = fmul(cxv[c], scale);
+        cyv[c] = fmul(cyv[c], scale);
+        czv[c] = fmul(czv[c], scale);
+      }
     }
   } else if (bgs == BG_ID) {
     ox = x; oy = y; oz = z;

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/aw_b200.h"
+#include "atlas.cuh"
 #include "greedy.cuh"
 #include "interp.cuh"
 #include "ldmm.cuh"
@@ -87,6 +88,10 @@ struct aw_ldmm_s {
   cudaStream_t gstream = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   std::map<std::pair<const void *, const void *>, std::pair<const void *, cudaGraphExec_t>> graphs;
+};
+
+struct aw_atlas_s {
+  aw::AtlasCtx ctx;
 };
 
 struct aw_greedy_s {
@@ -451,21 +456,117 @@ int aw_greedy_profile(aw_greedy_t g, const float *I0, const float *I1, const flo
   return rc;
 }
 
-int aw_greedy_get_energies(aw_greedy_t g, double *out, int max_count, int *count) {
-  if (!g || !count) return fail("aw_greedy_get_energies: null pointer");
-  AW_CUDA(cudaDeviceSynchronize(), "aw_greedy_get_energies (pending work)");
+static int copy_energies(const aw::GreedyDevState &st, double *out, int max_count, int *count,
+                         const char *what) {
+  AW_CUDA(cudaDeviceSynchronize(), what);
   int n = 0;
-  AW_CUDA(cudaMemcpy(&n, g->ctx.st.count, sizeof(int), cudaMemcpyDeviceToHost),
-          "aw_greedy_get_energies");
-  const int cap = g->ctx.st.cap;
+  AW_CUDA(cudaMemcpy(&n, st.count, sizeof(int), cudaMemcpyDeviceToHost), what);
+  const int cap = st.cap;
   const int avail = n < cap ? n : cap;
   std::vector<double> ring(cap);
-  AW_CUDA(cudaMemcpy(ring.data(), g->ctx.st.energy, sizeof(double) * cap, cudaMemcpyDeviceToHost),
-          "aw_greedy_get_energies");
+  AW_CUDA(cudaMemcpy(ring.data(), st.energy, sizeof(double) * cap, cudaMemcpyDeviceToHost), what);
   const int m = (out && max_count < avail) ? max_count : avail;
   for (int i = 0; i < m && out; ++i) out[i] = ring[(n - avail + i) % cap];
   *count = avail;
   return 0;
+}
+
+int aw_greedy_get_energies(aw_greedy_t g, double *out, int max_count, int *count) {
+  if (!g || !count) return fail("aw_greedy_get_energies: null pointer");
+  return copy_energies(g->ctx.st, out, max_count, count, "aw_greedy_get_energies");
+}
+
+int aw_atlas_create(int nx, int ny, int nz, double spx, double spy, double spz, float alpha,
+                    float beta, float gamma, float max_pert, int n_subjects, aw_atlas_t *out) {
+  std::string why;
+  if (!out) return fail("aw_atlas_create: null handle pointer");
+  *out = nullptr;
+  if (!dims_ok(nx, ny, nz, why)) return fail("aw_atlas_create: " + why);
+  if (!spacing_ok(spx, spy, spz)) return fail("aw_atlas_create: spacing must be positive");
+  if (!(gamma > 0.0f) || alpha < 0.0f || beta < 0.0f)
+    return fail("aw_atlas_create: need gamma > 0, alpha >= 0, beta >= 0 (L must be SPD)");
+  if (!(max_pert > 0.0f)) return fail("aw_atlas_create: MaxPert must be positive");
+  if (n_subjects < 1) return fail("aw_atlas_create: need at least one subject");
+  aw_atlas_s *a = new (std::nothrow) aw_atlas_s;
+  if (!a) return fail("aw_atlas_create: out of host memory");
+  const int rc = aw::atlas_create(&a->ctx, nx, ny, nz, spx, spy, spz, alpha, beta, gamma,
+                                  max_pert, n_subjects);
+  if (rc) {
+    aw::atlas_destroy(&a->ctx);
+    delete a;
+    return fail(std::string("aw_atlas_create: ") +
+                (rc == 5 ? "stream/event/copy setup failed" : plan_error(rc)));
+  }
+  *out = a;
+  return 0;
+}
+
+int aw_atlas_destroy(aw_atlas_t a) {
+  if (!a) return 0;
+  aw::atlas_destroy(&a->ctx);
+  delete a;
+  return 0;
+}
+
+int aw_atlas_set_subject(aw_atlas_t a, int i, const float *img, int snx, int sny, int snz,
+                         float weight) {
+  if (!a || !img) return fail("aw_atlas_set_subject: null pointer");
+  if (i < 0 || i >= a->ctx.ns) return fail("aw_atlas_set_subject: subject index out of range");
+  if (snx < 2 || sny < 2 || snz < 2) return fail("aw_atlas_set_subject: every grid axis must be >= 2");
+  AW_CUDA(aw::atlas_set_subject(&a->ctx, i, img, aw::Dims{snx, sny, snz}, weight),
+          "aw_atlas_set_subject");
+  return 0;
+}
+
+int aw_atlas_field(aw_atlas_t a, int i, float **hx, float **hy, float **hz) {
+  if (!a || !hx || !hy || !hz) return fail("aw_atlas_field: null pointer");
+  if (i < 0 || i >= a->ctx.ns) return fail("aw_atlas_field: subject index out of range");
+  *hx = aw::atlas_field(&a->ctx, i, 0);
+  *hy = aw::atlas_field(&a->ctx, i, 1);
+  *hz = aw::atlas_field(&a->ctx, i, 2);
+  return 0;
+}
+
+int aw_atlas_mean_buffer(aw_atlas_t a, float **mean) {
+  if (!a || !mean) return fail("aw_atlas_mean_buffer: null pointer");
+  *mean = a->ctx.mean;
+  return 0;
+}
+
+static bool atlas_ready(aw_atlas_t a) {
+  for (int r : a->ctx.ready)
+    if (!r) return false;
+  return true;
+}
+
+int aw_atlas_compute_mean(aw_atlas_t a, void *stream) {
+  if (!a) return fail("aw_atlas_compute_mean: null handle");
+  if (!atlas_ready(a)) return fail("aw_atlas_compute_mean: a subject image is not set");
+  AW_CUDA(aw::atlas_mean(&a->ctx, S(stream)), "aw_atlas_compute_mean");
+  return 0;
+}
+
+int aw_atlas_iterate(aw_atlas_t a, int n_iters, int update_first, void *stream) {
+  if (!a) return fail("aw_atlas_iterate: null handle");
+  if (n_iters < 0) return fail("aw_atlas_iterate: negative iteration count");
+  if (!atlas_ready(a)) return fail("aw_atlas_iterate: a subject image is not set");
+  AW_CUDA(aw::atlas_iterate(&a->ctx, n_iters, update_first, S(stream)), "aw_atlas_iterate");
+  return 0;
+}
+
+int aw_atlas_get_step(aw_atlas_t a, int i, float *step) {
+  if (!a || !step) return fail("aw_atlas_get_step: null pointer");
+  if (i < 0 || i >= a->ctx.ns) return fail("aw_atlas_get_step: subject index out of range");
+  AW_CUDA(cudaDeviceSynchronize(), "aw_atlas_get_step (pending work)");
+  AW_CUDA(cudaMemcpy(step, a->ctx.subj[i].st.step, sizeof(float), cudaMemcpyDeviceToHost),
+          "aw_atlas_get_step");
+  return 0;
+}
+
+int aw_atlas_get_energies(aw_atlas_t a, int i, double *out, int max_count, int *count) {
+  if (!a || !count) return fail("aw_atlas_get_energies: null pointer");
+  if (i < 0 || i >= a->ctx.ns) return fail("aw_atlas_get_energies: subject index out of range");
+  return copy_energies(a->ctx.subj[i].st, out, max_count, count, "aw_atlas_get_energies");
 }
 
 int aw_ldmm_create(int nx, int ny, int nz, double spx, double spy, double spz, float alpha,

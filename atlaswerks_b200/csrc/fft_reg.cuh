@@ -5,9 +5,8 @@
 // the four-step split N = E x T:
 //   1. every lane takes a length-E DFT of its strided values x[t + T*j],
 //   2. multiplies by W_N^(t*k1),
-//   3. the T lanes exchange through a per-line shared-memory scratch
-//      (padded so neither the writes nor the reads conflict beyond the
-//      two wavefronts a 64-bit warp access needs),
+//   3. the T lanes exchange through N shared-memory slots of the line
+//      (XOR-swizzled so neither the writes nor the reads conflict),
 //   4. every lane takes E/T length-T DFTs.
 // Only __syncwarp separates the steps. On exit lane t holds
 //   v[i*T + k2] = X[(t + T*i) + E*k2],  i < E/T, k2 < T.
@@ -30,16 +29,6 @@ template <>
 struct LineCfg<128> { static constexpr int T = 8, E = 16; };
 template <>
 struct LineCfg<256> { static constexpr int T = 16, E = 16; };
-
-// scratch floats2 per line: holds both the exchange (E*(T+1)) and a
-// natural-order copy of the line (N); padded to 8 mod 16 so that
-// neighbouring lines of a warp fall on opposite bank halves
-template <int N>
-constexpr int line_scratch() {
-  constexpr int T = LineCfg<N>::T, E = LineCfg<N>::E;
-  constexpr int a = E * (T + 1) > N ? E * (T + 1) : N;
-  return ((a + 7) / 16) * 16 + 8;
-}
 
 template <int SIGN>
 AW_D void dft4r(float2 &a0, float2 &a1, float2 &a2, float2 &a3) {
@@ -103,23 +92,29 @@ struct DFT<SIGN, 16> {
 };
 
 // Four-step line FFT; see the file comment for the register mapping.
-// `scr` is this line's scratch (line_scratch<N>() float2), `t` the lane
-// index within the line.
-template <int N, int SIGN>
-AW_D void line_fft(float2 *v, int t, float2 *scr, const float2 *__restrict__ tw) {
+// `slot(m)` returns the address of exchange slot m (0 <= m < N), storage
+// that belongs to this line only: the line's own elements in a slab or tile
+// when the transform runs in place. Slot (a, b) of the E x T exchange matrix
+// is stored at m = a*T + (b ^ (a mod T)): the XOR keeps both the row-wise
+// writes and the column-wise reads on distinct banks. `t` is the lane within
+// the line. The lanes' inputs must already be in registers: the first write
+// to a slot comes after a __syncwarp.
+template <int N, int SIGN, class Slot>
+AW_D void line_fft(float2 *v, int t, const Slot &slot, const float2 *__restrict__ tw) {
   constexpr int T = LineCfg<N>::T, E = LineCfg<N>::E;
+  static_assert(E % T == 0, "line split");
   DFT<SIGN, E>::run(v);
 #pragma unroll
   for (int k1 = 1; k1 < E; ++k1) v[k1] = cmul(v[k1], twiddle<SIGN>(tw, t * k1));
   __syncwarp();
 #pragma unroll
-  for (int k1 = 0; k1 < E; ++k1) scr[k1 * (T + 1) + t] = v[k1];
+  for (int k1 = 0; k1 < E; ++k1) *slot(k1 * T + (t ^ (k1 & (T - 1)))) = v[k1];
   __syncwarp();
 #pragma unroll
   for (int i = 0; i < E / T; ++i) {
     float2 w[T];
 #pragma unroll
-    for (int s = 0; s < T; ++s) w[s] = scr[(t + T * i) * (T + 1) + s];
+    for (int s = 0; s < T; ++s) w[s] = *slot((t + T * i) * T + (s ^ t));
     DFT<SIGN, T>::run(w);
 #pragma unroll
     for (int k2 = 0; k2 < T; ++k2) v[i * T + k2] = w[k2];

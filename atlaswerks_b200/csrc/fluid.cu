@@ -8,6 +8,8 @@
 //   L_ij = beta*s_i*s_j,  c = (2cos(2 pi k/n) - 2)/sp^2,  s = sin(2 pi k/n)/sp
 // (LUT: DiffOper.cxx:590-639; Cholesky: DiffOper.cxx:1005-1083). Here the
 // 1/N scaling is folded into the per-wavenumber step.
+#include <cudaTypedefs.h>
+
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -230,6 +232,31 @@ __global__ void __launch_bounds__(256) k_fft_xy_inv(FluidPlan p, Dst dst) {
   }
 }
 
+// TMA descriptor of the spectrum for the z-pass: a 3D float tensor
+// {2*ny*nxh, nz, 3} read and written in boxes {2*Kq, nz, 1} = one 128-byte
+// row per kz, stored in shared memory with the 128-byte swizzle
+bool encode_spec_map(FluidPlan *p) {
+  static PFN_cuTensorMapEncodeTiled encode = nullptr;
+  if (!encode) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return false;
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(fn);
+  }
+  const cuuint64_t ncols = (cuuint64_t)p->d.ny * p->nxh;
+  const cuuint64_t dims[3] = {2 * ncols, (cuuint64_t)p->d.nz, 3};
+  const cuuint64_t strides[2] = {2 * ncols * sizeof(float), 2 * ncols * sizeof(float) * p->d.nz};
+  const cuuint32_t box[3] = {(cuuint32_t)(2 * p->fast_kq), (cuuint32_t)p->d.nz, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  if (box[0] * sizeof(float) != 128 || box[1] > 256 || strides[0] % 16) return false;
+  return encode(&p->spec_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, p->spec, dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <class K>
 cudaError_t set_smem(K kernel, size_t bytes) {
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -260,11 +287,9 @@ int fluid_plan_create(FluidPlan *p, int nx, int ny, int nz, double spx, double s
   p->device = dev;
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (fast_supported(nx) && fast_supported(ny) && fast_supported(nz)) {
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    p->fast_kq = fast_z_kq(*p, sms);
+    p->fast_kq = fast_z_cols();
     p->fast_smem_xy = fast_xy_smem(nx, ny);
-    p->fast_smem_z = fast_z_smem(nz, p->fast_kq);
+    p->fast_smem_z = fast_z_smem(nz);
     p->fast = p->fast_smem_xy <= (size_t)maxsm && p->fast_smem_z <= (size_t)maxsm;
   }
   if (!p->fast && (p->smem_xy > (size_t)maxsm || p->smem_z > (size_t)maxsm)) return 2;
@@ -280,6 +305,8 @@ int fluid_plan_create(FluidPlan *p, int nx, int ny, int nz, double spx, double s
   if (cudaMalloc(&p->tw, tw.size() * sizeof(float2)) != cudaSuccess) return 3;
   if (cudaMalloc(&p->lut, lut.size() * sizeof(float)) != cudaSuccess) return 3;
   if (cudaMalloc(&p->spec, sizeof(float2) * 3 * (size_t)nz * ny * p->nxh) != cudaSuccess) return 3;
+  if (cudaMalloc(&p->status, sizeof(int)) != cudaSuccess) return 3;
+  cudaMemset(p->status, 0, sizeof(int));
   cudaMemcpy(p->tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice);
   cudaMemcpy(p->lut, lut.data(), lut.size() * sizeof(float), cudaMemcpyHostToDevice);
   p->ax.tw = p->tw;
@@ -291,6 +318,7 @@ int fluid_plan_create(FluidPlan *p, int nx, int ny, int nz, double spx, double s
       set_smem(k_fft_xy_inv<DstAxpby>, p->smem_xy) != cudaSuccess ||
       set_smem(k_fft_z_solve, p->smem_z) != cudaSuccess)
     return 4;
+  if (p->fast) p->fast_tma = encode_spec_map(p);
   if (p->fast && fast_configure(*p) != cudaSuccess) return 4;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
@@ -299,6 +327,7 @@ void fluid_plan_destroy(FluidPlan *p) {
   if (p->tw) cudaFree(p->tw);
   if (p->lut) cudaFree(p->lut);
   if (p->spec) cudaFree(p->spec);
+  if (p->status) cudaFree(p->status);
   std::memset(p, 0, sizeof(*p));
 }
 

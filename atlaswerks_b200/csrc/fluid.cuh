@@ -16,6 +16,8 @@
 // trips instead of the six of a pass-per-axis transform.
 #pragma once
 
+#include <cuda.h>
+
 #include "aw_common.cuh"
 #include "fft_smem.cuh"
 
@@ -35,8 +37,11 @@ struct FluidPlan {
   int device;
   // register-FFT path (fluid_fast.cu): power-of-two axes
   int fast;
-  int fast_kq;
+  int fast_kq;               // (ky,kx) columns per z-pass CTA
   size_t fast_smem_xy, fast_smem_z;
+  int *status;               // device status word: bounded waits that timed out
+  int fast_tma;              // z-pass tiles moved by TMA tensor copies
+  CUtensorMap spec_map;      // spectrum as [3][nz][2*ny*nxh] floats, 128B swizzle
 };
 
 // --- producers for the forward pass ----------------------------------------

@@ -3,12 +3,24 @@
 //
 // Same three passes as fluid.cu (xy-forward, z-solve, xy-inverse) and the
 // same arithmetic definition; the layout of work differs:
-//  * xy kernels: one 512-thread CTA per (z-slab, component); x-lines are
-//    row pairs packed as one complex line; the kx = 0 and kx = nx/2 columns
-//    (real after the x-transform) are packed into one complex y-line, so a
-//    128 x 128 slab is exactly 64 x-lines + 64 y-lines.
-//  * z kernel: one CTA per Kq consecutive (ky,kx) columns, all three
-//    components, lines loaded straight from HBM into registers.
+//  * xy kernels: one 256-thread CTA per (z-slab, component) holding only the
+//    slab's half spectrum in shared memory (66.5 KB at 128 x 128, three
+//    CTAs per SM). x-lines are row pairs packed as one complex line; the
+//    kx = 0 and kx = nx/2 columns (real after the x-transform) are packed into
+//    one complex y-line, so a 128 x 128 slab is exactly 64 x-lines + 64
+//    y-lines. Every line's four-step exchange runs in place in the slab slots
+//    that line owns, so the CTA needs no scratch. Lines that share a
+//    half-warp are placed 8 banks apart, which with the exchange swizzle
+//    makes every shared-memory access conflict-free. The finished slab leaves
+//    (forward) or arrives (inverse) as one bulk copy.
+//  * z kernel: one CTA per 16 consecutive (ky,kx) columns, all three
+//    components. The [nz x 16] complex tiles arrive by TMA tensor copies in
+//    the 128-byte swizzled layout (one 128-byte row per kz), each z-line
+//    transforms in place in its tile column, the 3x3 solve runs in the
+//    tiles, and TMA tensor stores write them back.
+#include <cstdint>
+
+#include "bulk.cuh"
 #include "fft_reg.cuh"
 #include "fluid.cuh"
 #include "fluid_fast.cuh"
@@ -17,136 +29,179 @@ namespace aw {
 
 namespace {
 
-constexpr int kXYThreads = 512;
+constexpr int kXYThreads = 256;
 constexpr int kXYWarps = kXYThreads / 32;
+constexpr int kZq = 16;  // columns per z tile: one 128-byte row per kz
 
 template <int NX, int NY>
 struct XYShape {
   static constexpr int NXH = NX / 2 + 1;
   static constexpr int TX = LineCfg<NX>::T, EX = LineCfg<NX>::E;
   static constexpr int TY = LineCfg<NY>::T, EY = LineCfg<NY>::E;
-  static constexpr int LSX = line_scratch<NX>(), LSY = line_scratch<NY>();
-  static constexpr int LS = LSX > LSY ? LSX : LSY;
-  static constexpr int LPW = 32 / (TX < TY ? TX : TY);  // max lines per warp
-  static constexpr size_t smem() {
-    return sizeof(float2) * ((size_t)NY * NXH + (size_t)kXYWarps * LPW * LS);
+  static constexpr size_t smem() { return sizeof(float2) * (size_t)NY * NXH; }
+  // CTAs that fit one SM's shared memory, at most 3 (85 registers a thread)
+  static constexpr int ctas() {
+    return (int)((227u * 1024u) / (smem() + 1024u)) >= 3 ? 3
+           : (int)((227u * 1024u) / (smem() + 1024u)) >= 2 ? 2 : 1;
   }
 };
 
+// Row pair of x-line g. A row pair is 2*NXH = nx + 2 slots long (2 banks mod
+// 16), so the 16/T lines of a half-warp take pairs 8/(16/T) apart.
+template <int T>
+AW_D int xline_pair(int g) {
+  constexpr int H = 16 / T;
+  const int r = g & 7;
+  return (g & ~7) + (r % H) * (8 / H) + r / H;
+}
+
+// Column of y-line g (column 0 stands for the packed 0 | nx/2 line). Columns
+// are 1 bank apart (NXH = 1 mod 16), so the lines of a half-warp take
+// columns BC/(16/T) apart within blocks of BC.
+template <int T, int BC>
+AW_D int yline_col(int g) {
+  constexpr int H = (16 / T) < BC ? (16 / T) : BC;
+  const int r = g % BC;
+  return g - r + (r % H) * (BC / H) + r / H;
+}
+
 template <int NX, int NY, class Src>
-__global__ void __launch_bounds__(kXYThreads) k_xy_fwd_fast(FluidPlan p, Src src) {
+__global__ void __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
+    k_xy_fwd_fast(FluidPlan p, Src src) {
   using S = XYShape<NX, NY>;
   constexpr int NXH = S::NXH, TX = S::TX, EX = S::EX, TY = S::TY, EY = S::EY;
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(128) float2 sm[];
   float2 *C = sm;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float2 *wscr = C + NY * NXH + warp * S::LPW * S::LS;
   const Dims d = p.d;
   const int z = blockIdx.x, comp = blockIdx.y;
 
-  // ---- x: row pairs (y0, y1) as one complex line -------------------------
+  // ---- x: row pairs (y0, y0+1) as one complex line, exchanged in place ----
   {
-    constexpr int L = 32 / TX;
+    constexpr int L = 32 / TX, NLINES = NY / 2;
+    static_assert(NLINES % 8 == 0 && NLINES % L == 0, "x-lines fill whole warps");
+    constexpr int KU = (NXH + TX - 1) / TX;
     const int lw = lane / TX, t = lane % TX;
-    float2 *scr = wscr + lw * S::LS;
-    for (int base = warp * L; base < NY / 2; base += kXYWarps * L) {
-      const int pr = base + lw;
-      const bool act = pr < NY / 2;
-      const int y0 = 2 * (act ? pr : 0);
+    for (int base = warp * L; base < NLINES; base += kXYWarps * L) {
+      const int y0 = 2 * xline_pair<TX>(base + lw);
       float2 v[EX];
 #pragma unroll
       for (int j = 0; j < EX; ++j) {
         const int x = t + TX * j;
         v[j] = make_float2(src.value(comp, x, y0, z, d), src.value(comp, x, y0 + 1, z, d));
       }
-      line_fft<NX, -1>(v, t, scr, p.ax.tw);
+      float2 *row = C + y0 * NXH;
+      line_fft<NX, -1>(v, t, [row](int m) { return row + m; }, p.ax.tw);
 #pragma unroll
-      for (int r = 0; r < EX; ++r) scr[line_out_index<NX>(t, r)] = v[r];
+      for (int r = 0; r < EX; ++r) row[line_out_index<NX>(t, r)] = v[r];
       __syncwarp();
-      if (act) {
-        for (int k = t; k < NXH; k += TX) {
-          const float2 Z = scr[k], Zm = scr[(NX - k) & (NX - 1)];
-          C[y0 * NXH + k] = make_float2(0.5f * (Z.x + Zm.x), 0.5f * (Z.y - Zm.y));
-          C[(y0 + 1) * NXH + k] = make_float2(0.5f * (Z.y + Zm.y), -0.5f * (Z.x - Zm.x));
+      // two real rows from one complex transform:
+      // X0[k] = (Z[k] + conj Z[n-k]) / 2,  X1[k] = (Z[k] - conj Z[n-k]) / 2i
+      float2 Zk[KU], Zm[KU];
+#pragma unroll
+      for (int i = 0; i < KU; ++i) {
+        const int k = t + TX * i;
+        if (k < NXH) {
+          Zk[i] = row[k];
+          Zm[i] = row[(NX - k) & (NX - 1)];
         }
       }
       __syncwarp();
+#pragma unroll
+      for (int i = 0; i < KU; ++i) {
+        const int k = t + TX * i;
+        if (k < NXH) {
+          const float2 Z = Zk[i], M = Zm[i];
+          row[k] = make_float2(0.5f * (Z.x + M.x), 0.5f * (Z.y - M.y));
+          row[NXH + k] = make_float2(0.5f * (Z.y + M.y), -0.5f * (Z.x - M.x));
+        }
+      }
     }
   }
   __syncthreads();
 
   // ---- y: columns kx = 1..NX/2-1, plus the packed real columns 0 | NX/2 ---
   {
-    constexpr int L = 32 / TY;
+    constexpr int L = 32 / TY, NLINES = NX / 2, BC = NLINES >= 16 ? 16 : NLINES;
+    static_assert(NLINES % L == 0, "y-lines fill whole warps");
     const int lw = lane / TY, t = lane % TY;
-    float2 *scr = wscr + lw * S::LS;
-    constexpr int NL = NXH - 1;  // lines
-    for (int base = warp * L; base < NL; base += kXYWarps * L) {
-      const int l = base + lw;
-      const bool act = l < NL;
-      const bool packed = (l == 0);
-      const int kx = act ? l : 1;
+    for (int base = warp * L; base < NLINES; base += kXYWarps * L) {
+      const int l = yline_col<TY, BC>(base + lw);
+      const bool packed = l == 0;
+      float2 *col = C + l;
       float2 v[EY];
 #pragma unroll
       for (int j = 0; j < EY; ++j) {
         const int y = t + TY * j;
-        v[j] = packed ? make_float2(C[y * NXH].x, C[y * NXH + NX / 2].x) : C[y * NXH + kx];
+        v[j] = packed ? make_float2(C[y * NXH].x, C[y * NXH + NX / 2].x) : col[y * NXH];
       }
-      line_fft<NY, -1>(v, t, scr, p.ay.tw);
+      line_fft<NY, -1>(v, t, [col](int m) { return col + m * NXH; }, p.ay.tw);
+#pragma unroll
+      for (int r = 0; r < EY; ++r) col[line_out_index<NY>(t, r) * NXH] = v[r];
       if (packed) {
+        // split the packed line into the spectra of columns 0 and NX/2
+        const unsigned mask = (TY == 32 ? 0xffffffffu : ((1u << TY) - 1u)) << (lw * TY);
+        float2 Zm[EY];
+        __syncwarp(mask);
 #pragma unroll
-        for (int r = 0; r < EY; ++r) scr[line_out_index<NY>(t, r)] = v[r];
-      }
-      __syncwarp();
-      if (act && !packed) {
+        for (int i = 0; i < EY; ++i) {
+          const int k = t + TY * i;
+          v[i] = C[k * NXH];
+          Zm[i] = C[((NY - k) & (NY - 1)) * NXH];
+        }
+        __syncwarp(mask);
 #pragma unroll
-        for (int r = 0; r < EY; ++r) C[line_out_index<NY>(t, r) * NXH + kx] = v[r];
-      } else if (packed) {
-        for (int k = t; k < NY; k += TY) {
-          const float2 Z = scr[k], Zm = scr[(NY - k) & (NY - 1)];
-          C[k * NXH] = make_float2(0.5f * (Z.x + Zm.x), 0.5f * (Z.y - Zm.y));
-          C[k * NXH + NX / 2] = make_float2(0.5f * (Z.y + Zm.y), -0.5f * (Z.x - Zm.x));
+        for (int i = 0; i < EY; ++i) {
+          const int k = t + TY * i;
+          const float2 Z = v[i], M = Zm[i];
+          C[k * NXH] = make_float2(0.5f * (Z.x + M.x), 0.5f * (Z.y - M.y));
+          C[k * NXH + NX / 2] = make_float2(0.5f * (Z.y + M.y), -0.5f * (Z.x - M.x));
         }
       }
       __syncwarp();
     }
   }
-  __syncthreads();
 
-  // ---- store the slab: contiguous, 16-byte vectors ------------------------
-  const float4 *c4 = reinterpret_cast<const float4 *>(C);
-  float4 *o4 = reinterpret_cast<float4 *>(p.spec + ((long)comp * d.nz + z) * NY * NXH);
-  for (int i = threadIdx.x; i < NY * NXH / 2; i += kXYThreads) o4[i] = c4[i];
+  // ---- store the slab: one bulk copy shared -> HBM -----------------------
+  fence_async_smem();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bulk_store(p.spec + ((long)comp * d.nz + z) * NY * NXH, C,
+               (uint32_t)(sizeof(float2) * NY * NXH));
+    bulk_wait_read();
+  }
 }
 
 template <int NX, int NY, class Dst>
-__global__ void __launch_bounds__(kXYThreads) k_xy_inv_fast(FluidPlan p, Dst dst) {
+__global__ void __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
+    k_xy_inv_fast(FluidPlan p, Dst dst) {
   using S = XYShape<NX, NY>;
   constexpr int NXH = S::NXH, TX = S::TX, EX = S::EX, TY = S::TY, EY = S::EY;
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(128) float2 sm[];
+  __shared__ uint64_t mbar;
   float2 *C = sm;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float2 *wscr = C + NY * NXH + warp * S::LPW * S::LS;
   const Dims d = p.d;
   const int z = blockIdx.x, comp = blockIdx.y;
-  {
-    float4 *c4 = reinterpret_cast<float4 *>(C);
-    const float4 *i4 = reinterpret_cast<const float4 *>(p.spec + ((long)comp * d.nz + z) * NY * NXH);
-    for (int i = threadIdx.x; i < NY * NXH / 2; i += kXYThreads) c4[i] = i4[i];
+  // the spectrum slab, one bulk copy HBM -> shared
+  if (threadIdx.x == 0) {
+    const uint32_t bytes = (uint32_t)(sizeof(float2) * NY * NXH);
+    mbar_init(&mbar, 1);
+    mbar_expect_tx(&mbar, bytes);
+    bulk_load(C, p.spec + ((long)comp * d.nz + z) * NY * NXH, bytes, &mbar);
   }
   __syncthreads();
+  // a slab that never lands: the status word says so and the CTA leaves as one
+  if (__syncthreads_or(!mbar_wait(&mbar, 0, p.status))) return;
 
   // ---- inverse y on columns; packed real columns 0 | NX/2 -----------------
   {
-    constexpr int L = 32 / TY;
+    constexpr int L = 32 / TY, NLINES = NX / 2, BC = NLINES >= 16 ? 16 : NLINES;
     const int lw = lane / TY, t = lane % TY;
-    float2 *scr = wscr + lw * S::LS;
-    constexpr int NL = NXH - 1;
-    for (int base = warp * L; base < NL; base += kXYWarps * L) {
-      const int l = base + lw;
-      const bool act = l < NL;
-      const bool packed = (l == 0);
-      const int kx = act ? l : 1;
+    for (int base = warp * L; base < NLINES; base += kXYWarps * L) {
+      const int l = yline_col<TY, BC>(base + lw);
+      const bool packed = l == 0;
+      float2 *col = C + l;
       float2 v[EY];
 #pragma unroll
       for (int j = 0; j < EY; ++j) {
@@ -155,133 +210,178 @@ __global__ void __launch_bounds__(kXYThreads) k_xy_inv_fast(FluidPlan p, Dst dst
           const float2 a = C[y * NXH], b = C[y * NXH + NX / 2];
           v[j] = make_float2(a.x - b.y, a.y + b.x);  // a + i b
         } else {
-          v[j] = C[y * NXH + kx];
+          v[j] = col[y * NXH];
         }
       }
-      __syncwarp();
-      line_fft<NY, +1>(v, t, scr, p.ay.tw);
-      if (act) {
+      line_fft<NY, +1>(v, t, [col](int m) { return col + m * NXH; }, p.ay.tw);
 #pragma unroll
-        for (int r = 0; r < EY; ++r) {
-          const int y = line_out_index<NY>(t, r);
-          if (packed) {
-            // real parts of the two columns; c2r ignores their imaginary parts
-            C[y * NXH] = make_float2(v[r].x, 0.f);
-            C[y * NXH + NX / 2] = make_float2(v[r].y, 0.f);
-          } else {
-            C[y * NXH + kx] = v[r];
-          }
+      for (int r = 0; r < EY; ++r) {
+        const int y = line_out_index<NY>(t, r);
+        if (packed) {
+          // real parts of the two columns; c2r ignores their imaginary parts
+          C[y * NXH] = make_float2(v[r].x, 0.f);
+          C[y * NXH + NX / 2] = make_float2(v[r].y, 0.f);
+        } else {
+          col[y * NXH] = v[r];
         }
       }
-      __syncwarp();
     }
   }
   __syncthreads();
 
   // ---- inverse x: row pairs, Hermitian completion, real output ------------
   {
-    constexpr int L = 32 / TX;
+    constexpr int L = 32 / TX, NLINES = NY / 2;
     const int lw = lane / TX, t = lane % TX;
-    float2 *scr = wscr + lw * S::LS;
-    for (int base = warp * L; base < NY / 2; base += kXYWarps * L) {
-      const int pr = base + lw;
-      const bool act = pr < NY / 2;
-      const int y0 = 2 * (act ? pr : 0);
+    for (int base = warp * L; base < NLINES; base += kXYWarps * L) {
+      const int y0 = 2 * xline_pair<TX>(base + lw);
+      float2 *row = C + y0 * NXH;
       float2 v[EX];
 #pragma unroll
       for (int j = 0; j < EX; ++j) {
         const int k = t + TX * j;
         const bool upper = k > NX / 2;
         const int kk = upper ? NX - k : k;
-        float2 X0 = C[y0 * NXH + kk], X1 = C[(y0 + 1) * NXH + kk];
+        float2 X0 = row[kk], X1 = row[NXH + kk];
         if (kk == 0 || kk == NX / 2) { X0.y = 0.f; X1.y = 0.f; }
         if (upper) { X0.y = -X0.y; X1.y = -X1.y; }
         v[j] = make_float2(X0.x - X1.y, X0.y + X1.x);
       }
-      line_fft<NX, +1>(v, t, scr, p.ax.tw);
-      if (act) {
+      line_fft<NX, +1>(v, t, [row](int m) { return row + m; }, p.ax.tw);
 #pragma unroll
-        for (int r = 0; r < EX; ++r) {
-          const int x = line_out_index<NX>(t, r);
-          dst.store(comp, d.idx(x, y0, z), v[r].x);
-          dst.store(comp, d.idx(x, y0 + 1, z), v[r].y);
-        }
+      for (int r = 0; r < EX; ++r) {
+        const int x = line_out_index<NX>(t, r);
+        dst.store(comp, d.idx(x, y0, z), v[r].x);
+        dst.store(comp, d.idx(x, y0 + 1, z), v[r].y);
       }
     }
   }
 }
 
+// per-wavenumber solve of one (kx, ky, kz): the three components at b0p,
+// b1p, b2p (DiffOper.cxx:1005-1083 for the inverse, 1088-1116 for L)
+AW_D void solve_point(const FluidPlan &p, int kx, int ky, int kz, int inverse, float invN,
+                      float2 *b0p, float2 *b1p, float2 *b2p) {
+  const float *cwx = p.lut, *swx = cwx + p.d.nx, *cwy = swx + p.d.nx, *swy = cwy + p.d.ny,
+              *cwz = swy + p.d.ny, *swz = cwz + p.d.nz;
+  const float cx = __ldg(cwx + kx), cy = __ldg(cwy + ky), cz = __ldg(cwz + kz);
+  const float sx = __ldg(swx + kx), sy = __ldg(swy + ky), sz = __ldg(swz + kz);
+  const float lambda = -p.alpha * (cx + cy + cz) + p.gamma;
+  const float L00 = lambda - p.beta * cx, L11 = lambda - p.beta * cy, L22 = lambda - p.beta * cz;
+  const float L10 = p.beta * sx * sy, L20 = p.beta * sx * sz, L21 = p.beta * sy * sz;
+  float2 b0 = *b0p, b1 = *b1p, b2 = *b2p;
+  b0.x *= invN; b0.y *= invN; b1.x *= invN; b1.y *= invN; b2.x *= invN; b2.y *= invN;
+  float2 o0, o1, o2;
+  if (inverse) {
+    // Cholesky L = G G^T, then G y = b, G^T x = y (real matrix, complex rhs)
+    const float G00 = sqrtf(L00);
+    const float G10 = L10 / G00, G20 = L20 / G00;
+    const float G11 = sqrtf(L11 - G10 * G10);
+    const float G21 = (L21 - G20 * G10) / G11;
+    const float G22 = sqrtf(L22 - (G20 * G20 + G21 * G21));
+    float2 y0, y1, y2;
+    y0.x = b0.x / G00;                              y0.y = b0.y / G00;
+    y1.x = (b1.x - G10 * y0.x) / G11;               y1.y = (b1.y - G10 * y0.y) / G11;
+    y2.x = (b2.x - G20 * y0.x - G21 * y1.x) / G22;  y2.y = (b2.y - G20 * y0.y - G21 * y1.y) / G22;
+    o2.x = y2.x / G22;                              o2.y = y2.y / G22;
+    o1.x = (y1.x - G21 * o2.x) / G11;               o1.y = (y1.y - G21 * o2.y) / G11;
+    o0.x = (y0.x - G10 * o1.x - G20 * o2.x) / G00;  o0.y = (y0.y - G10 * o1.y - G20 * o2.y) / G00;
+  } else {
+    o0.x = L00 * b0.x + L10 * b1.x + L20 * b2.x;  o0.y = L00 * b0.y + L10 * b1.y + L20 * b2.y;
+    o1.x = L10 * b0.x + L11 * b1.x + L21 * b2.x;  o1.y = L10 * b0.y + L11 * b1.y + L21 * b2.y;
+    o2.x = L20 * b0.x + L21 * b1.x + L22 * b2.x;  o2.y = L20 * b0.y + L21 * b1.y + L22 * b2.y;
+  }
+  *b0p = o0;
+  *b1p = o1;
+  *b2p = o2;
+}
+
+// element (kz, q) of a [nz x 16] complex tile in the TMA 128-byte swizzle:
+// the 16-byte chunk q/2 of row kz sits at chunk (q/2) ^ (kz mod 8)
+AW_D int zt(int k, int q) { return k * kZq + (q ^ ((k & 7) << 1)); }
+
 template <int NZ>
-__global__ void __launch_bounds__(768) k_z_solve_fast(FluidPlan p, int inverse, int Kq) {
-  constexpr int T = LineCfg<NZ>::T, E = LineCfg<NZ>::E, LS = line_scratch<NZ>();
-  extern __shared__ float2 sm[];
-  const int nxh = p.nxh;
-  const long ncols = (long)p.d.ny * nxh;
-  const long j0 = (long)blockIdx.x * Kq;
-  const long plane = ncols;
-  const int line = threadIdx.x / T, t = threadIdx.x % T;  // line = c*Kq + q
-  const int c = line / Kq, q = line - c * Kq;
-  const bool act = (j0 + q) < ncols;
-  const long col = act ? j0 + q : j0;
-  float2 *S = sm + line * LS;
+constexpr int z_threads() { return 3 * kZq * LineCfg<NZ>::T; }
+
+// z-pass over one CTA's 16 columns; tiles TB[c] = [nz x 16] complex. With
+// TMA the tiles move by tensor copies (columns past the spectrum's end read
+// as zero and are not written back), else by coalesced plain copies.
+template <int NZ, bool TMA>
+__global__ void __launch_bounds__(z_threads<NZ>(), (NZ <= 128 ? 3 : 1))
+    k_z_solve_fast(FluidPlan p, const __grid_constant__ CUtensorMap tmap, int inverse) {
+  constexpr int T = LineCfg<NZ>::T, E = LineCfg<NZ>::E, TILE = NZ * kZq;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ uint64_t mbar[3];
+  // the swizzle pattern repeats every 1024 bytes: align the tiles to it
+  float2 *TB = reinterpret_cast<float2 *>(smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u));
+  const long ncols = (long)p.d.ny * p.nxh;
+  const long j0 = (long)blockIdx.x * kZq;
+  const int line = threadIdx.x / T, t = threadIdx.x % T;
+  const int c = line / kZq, q = line % kZq;
+  float2 *tile = TB + c * TILE;
+  bool ok = true;
+  if constexpr (TMA) {
+    if (threadIdx.x == 0) {
+      for (int cc = 0; cc < 3; ++cc) mbar_init(&mbar[cc], 1);
+      for (int cc = 0; cc < 3; ++cc) {
+        mbar_expect_tx(&mbar[cc], (uint32_t)(TILE * sizeof(float2)));
+        tma_load_3d(TB + cc * TILE, &tmap, (int)(2 * j0), 0, cc, &mbar[cc]);
+      }
+    }
+    __syncthreads();
+    // each component's lines start as soon as their own tile has landed
+    ok = mbar_wait(&mbar[c], 0, p.status);
+  } else {
+    for (int i = threadIdx.x; i < 3 * TILE; i += blockDim.x) {
+      const int qq = i % kZq, r = i / kZq;  // r = cc*NZ + kz
+      const int cc = r / NZ, kz = r - cc * NZ;
+      TB[cc * TILE + zt(kz, qq)] =
+          (j0 + qq < ncols) ? p.spec[(long)r * ncols + j0 + qq] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+  }
+
   float2 v[E];
 #pragma unroll
-  for (int j = 0; j < E; ++j) v[j] = p.spec[((long)c * NZ + t + T * j) * plane + col];
-  line_fft<NZ, -1>(v, t, S, p.az.tw);
+  for (int j = 0; j < E; ++j) v[j] = tile[zt(t + T * j, q)];
+  line_fft<NZ, -1>(v, t, [tile, q](int m) { return tile + zt(m, q); }, p.az.tw);
 #pragma unroll
-  for (int r = 0; r < E; ++r) S[line_out_index<NZ>(t, r)] = v[r];
-  __syncthreads();
-  // per-wavenumber solve (DiffOper.cxx:1005-1083) on all (q, kz) of the tile
-  {
-    const float *cwx = p.lut, *swx = cwx + p.d.nx, *cwy = swx + p.d.nx, *swy = cwy + p.d.ny,
-                *cwz = swy + p.d.ny, *swz = cwz + NZ;
-    const float invN = 1.0f / (float)p.d.n();
-    for (int i = threadIdx.x; i < Kq * NZ; i += blockDim.x) {
-      const int qq = i / NZ, kz = i - qq * NZ;
-      const long jj = j0 + qq;
-      if (jj >= ncols) continue;
-      const int ky = (int)(jj / nxh), kx = (int)(jj - (long)ky * nxh);
-      const float cx = __ldg(cwx + kx), cy = __ldg(cwy + ky), cz = __ldg(cwz + kz);
-      const float sx = __ldg(swx + kx), sy = __ldg(swy + ky), sz = __ldg(swz + kz);
-      const float lambda = -p.alpha * (cx + cy + cz) + p.gamma;
-      const float L00 = lambda - p.beta * cx, L11 = lambda - p.beta * cy, L22 = lambda - p.beta * cz;
-      const float L10 = p.beta * sx * sy, L20 = p.beta * sx * sz, L21 = p.beta * sy * sz;
-      float2 *s0 = sm + (0 * Kq + qq) * LS + kz, *s1 = sm + (1 * Kq + qq) * LS + kz,
-             *s2 = sm + (2 * Kq + qq) * LS + kz;
-      float2 b0 = *s0, b1 = *s1, b2 = *s2;
-      b0.x *= invN; b0.y *= invN; b1.x *= invN; b1.y *= invN; b2.x *= invN; b2.y *= invN;
-      float2 o0, o1, o2;
-      if (inverse) {
-        const float G00 = sqrtf(L00);
-        const float G10 = L10 / G00, G20 = L20 / G00;
-        const float G11 = sqrtf(L11 - G10 * G10);
-        const float G21 = (L21 - G20 * G10) / G11;
-        const float G22 = sqrtf(L22 - (G20 * G20 + G21 * G21));
-        float2 y0, y1, y2;
-        y0.x = b0.x / G00;                              y0.y = b0.y / G00;
-        y1.x = (b1.x - G10 * y0.x) / G11;               y1.y = (b1.y - G10 * y0.y) / G11;
-        y2.x = (b2.x - G20 * y0.x - G21 * y1.x) / G22;  y2.y = (b2.y - G20 * y0.y - G21 * y1.y) / G22;
-        o2.x = y2.x / G22;                              o2.y = y2.y / G22;
-        o1.x = (y1.x - G21 * o2.x) / G11;               o1.y = (y1.y - G21 * o2.y) / G11;
-        o0.x = (y0.x - G10 * o1.x - G20 * o2.x) / G00;  o0.y = (y0.y - G10 * o1.y - G20 * o2.y) / G00;
-      } else {
-        o0.x = L00 * b0.x + L10 * b1.x + L20 * b2.x;  o0.y = L00 * b0.y + L10 * b1.y + L20 * b2.y;
-        o1.x = L10 * b0.x + L11 * b1.x + L21 * b2.x;  o1.y = L10 * b0.y + L11 * b1.y + L21 * b2.y;
-        o2.x = L20 * b0.x + L21 * b1.x + L22 * b2.x;  o2.y = L20 * b0.y + L21 * b1.y + L22 * b2.y;
-      }
-      *s0 = o0;
-      *s1 = o1;
-      *s2 = o2;
-    }
+  for (int r = 0; r < E; ++r) tile[zt(line_out_index<NZ>(t, r), q)] = v[r];
+  if (__syncthreads_or(!ok)) return;  // a tile never landed: the status word says so
+
+  const float invN = 1.0f / (float)p.d.n();
+  const int nxh = p.nxh;
+  for (int i = threadIdx.x; i < TILE; i += blockDim.x) {
+    const int kz = i / kZq, qq = i % kZq;
+    const long jj = j0 + qq;
+    if (jj >= ncols) continue;
+    const int ky = (int)(jj / nxh), kx = (int)(jj - (long)ky * nxh);
+    const int e = zt(kz, qq);
+    solve_point(p, kx, ky, kz, inverse, invN, TB + e, TB + TILE + e, TB + 2 * TILE + e);
   }
   __syncthreads();
+
 #pragma unroll
-  for (int j = 0; j < E; ++j) v[j] = S[t + T * j];
-  line_fft<NZ, +1>(v, t, S, p.az.tw);
-  if (act) {
+  for (int j = 0; j < E; ++j) v[j] = tile[zt(t + T * j, q)];
+  line_fft<NZ, +1>(v, t, [tile, q](int m) { return tile + zt(m, q); }, p.az.tw);
 #pragma unroll
-    for (int r = 0; r < E; ++r)
-      p.spec[((long)c * NZ + line_out_index<NZ>(t, r)) * plane + col] = v[r];
+  for (int r = 0; r < E; ++r) tile[zt(line_out_index<NZ>(t, r), q)] = v[r];
+
+  if constexpr (TMA) {
+    fence_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int cc = 0; cc < 3; ++cc) tma_store_3d(&tmap, (int)(2 * j0), 0, cc, TB + cc * TILE);
+      bulk_commit();
+      bulk_wait_read();
+    }
+  } else {
+    __syncthreads();
+    for (int i = threadIdx.x; i < 3 * TILE; i += blockDim.x) {
+      const int qq = i % kZq, r = i / kZq;
+      const int cc = r / NZ, kz = r - cc * NZ;
+      if (j0 + qq < ncols) p.spec[(long)r * ncols + j0 + qq] = TB[cc * TILE + zt(kz, qq)];
+    }
   }
 }
 
@@ -310,48 +410,30 @@ size_t fast_xy_smem(int nx, int ny) {
   return r;
 }
 
-int fast_z_kq(const FluidPlan &p, int sms) {
-  // Enough columns per CTA that one wave covers the spectrum, in whole lines
-  // per warp, bounded by 768 threads.
-  const int T = (p.d.nz == 16 || p.d.nz == 32) ? 4 : (p.d.nz == 256 ? 16 : 8);
-  const int lpw = 32 / T;
-  const long ncols = (long)p.d.ny * p.nxh;
-  long kq = (ncols + 3L * sms - 1) / (3L * sms);
-  kq = ((kq + lpw - 1) / lpw) * lpw;
-  const long maxkq = (768 / T) / 3 / lpw * lpw;
-  if (kq > maxkq) kq = maxkq;
-  if (kq < lpw) kq = lpw;
-  return (int)kq;
-}
+int fast_z_cols() { return kZq; }
 
-size_t fast_z_smem(int nz, int kq) {
-  size_t r = 0;
-  dispatch_n(nz, [&](auto Z) { r = sizeof(float2) * 3 * (size_t)kq * line_scratch<decltype(Z)::value>(); });
-  return r;
-}
+size_t fast_z_smem(int nz) { return sizeof(float2) * 3 * (size_t)nz * kZq + 1024; }
 
 cudaError_t fast_configure(const FluidPlan &p) {
   cudaError_t e = cudaSuccess;
   const size_t sxy = fast_xy_smem(p.d.nx, p.d.ny);
+  auto set = [&](const void *k, size_t bytes) {
+    cudaError_t r = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (r != cudaSuccess) e = r;
+  };
   dispatch_n(p.d.nx, [&](auto X) {
     dispatch_n(p.d.ny, [&](auto Y) {
       constexpr int NX = decltype(X)::value, NY = decltype(Y)::value;
-      auto set = [&](const void *k) {
-        cudaError_t r = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sxy);
-        if (r != cudaSuccess) e = r;
-      };
-      set((const void *)k_xy_fwd_fast<NX, NY, SrcField>);
-      set((const void *)k_xy_fwd_fast<NX, NY, SrcForce>);
-      set((const void *)k_xy_inv_fast<NX, NY, DstField>);
-      set((const void *)k_xy_inv_fast<NX, NY, DstAxpby>);
+      set((const void *)k_xy_fwd_fast<NX, NY, SrcField>, sxy);
+      set((const void *)k_xy_fwd_fast<NX, NY, SrcForce>, sxy);
+      set((const void *)k_xy_inv_fast<NX, NY, DstField>, sxy);
+      set((const void *)k_xy_inv_fast<NX, NY, DstAxpby>, sxy);
     });
   });
   dispatch_n(p.d.nz, [&](auto Z) {
     constexpr int NZ = decltype(Z)::value;
-    cudaError_t r = cudaFuncSetAttribute((const void *)k_z_solve_fast<NZ>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)p.fast_smem_z);
-    if (r != cudaSuccess) e = r;
+    set((const void *)k_z_solve_fast<NZ, true>, p.fast_smem_z);
+    set((const void *)k_z_solve_fast<NZ, false>, p.fast_smem_z);
   });
   return e;
 }
@@ -380,11 +462,13 @@ cudaError_t fast_xy_inverse(const FluidPlan &p, const Dst &dst, cudaStream_t s) 
 
 cudaError_t fast_z_solve(const FluidPlan &p, int inverse, cudaStream_t s) {
   const long ncols = (long)p.d.ny * p.nxh;
-  const int grid = (int)((ncols + p.fast_kq - 1) / p.fast_kq);
+  const int grid = (int)((ncols + kZq - 1) / kZq);
   dispatch_n(p.d.nz, [&](auto Z) {
     constexpr int NZ = decltype(Z)::value;
-    constexpr int T = LineCfg<NZ>::T;
-    k_z_solve_fast<NZ><<<grid, 3 * p.fast_kq * T, p.fast_smem_z, s>>>(p, inverse, p.fast_kq);
+    if (p.fast_tma)
+      k_z_solve_fast<NZ, true><<<grid, z_threads<NZ>(), p.fast_smem_z, s>>>(p, p.spec_map, inverse);
+    else
+      k_z_solve_fast<NZ, false><<<grid, z_threads<NZ>(), p.fast_smem_z, s>>>(p, p.spec_map, inverse);
   });
   return cudaGetLastError();
 }

@@ -9,8 +9,8 @@ namespace aw {
 
 bool fast_supported(int n);
 size_t fast_xy_smem(int nx, int ny);
-int fast_z_kq(const FluidPlan &p, int sms);
-size_t fast_z_smem(int nz, int kq);
+int fast_z_cols();
+size_t fast_z_smem(int nz);
 cudaError_t fast_configure(const FluidPlan &p);
 template <class Src>
 cudaError_t fast_xy_forward(const FluidPlan &p, const Src &src, cudaStream_t s);

@@ -27,13 +27,17 @@ constexpr int kThreads = 256;
 
 // Rows per force-prep block: each block sums the energy of kPrepRows rows, so
 // the fixed-order final sum has few partials to read.
-constexpr int kPrepRows = 16;
+constexpr int kPrepRows = 2;
 
+// I0(h) and the energy partials. With AFFINE the subject image lives on its
+// own grid di and h is in template voxels: the sample point is the atlas map
+// of h (atlas_point, interp.cuh).
+template <bool AFFINE>
 __global__ void __launch_bounds__(kRowThreads)
     k_force_prep(const float *__restrict__ I0, const float *__restrict__ I1,
                  const float *__restrict__ hx, const float *__restrict__ hy,
                  const float *__restrict__ hz, float *__restrict__ idef, double *__restrict__ partials,
-                 Dims d) {
+                 Dims d, Dims di, AtlasMap am) {
   const int x = blockIdx.x * kRowThreads + threadIdx.x;
   const int z = blockIdx.z;
   double e = 0.0;
@@ -42,7 +46,9 @@ __global__ void __launch_bounds__(kRowThreads)
     const int y1 = min(y0 + kPrepRows, d.ny);
     for (int y = y0; y < y1; ++y) {
       const long i = ((long)z * d.ny + y) * d.nx + x;
-      const float v = trilerp_scalar(I0, d, (double)hx[i], (double)hy[i], (double)hz[i], 0.0f);
+      double px = (double)hx[i], py = (double)hy[i], pz = (double)hz[i];
+      if (AFFINE) atlas_point(am, px, py, pz);
+      const float v = trilerp_scalar(I0, AFFINE ? di : d, px, py, pz, 0.0f);
       idef[i] = v;
       const float r = -fsub(v, I1[i]);
       e += (double)r * (double)r;
@@ -66,27 +72,41 @@ inline dim3 prep_grid(const Dims &d) {
 }
 
 // Fixed-order reduction of the block partials, so the energy is bitwise
-// reproducible run to run.
-__global__ void __launch_bounds__(kThreads)
+// reproducible run to run: four independent thread-strided sums per thread,
+// combined in a fixed order, then the warp and block trees.
+constexpr int kFinalThreads = 1024;
+
+__global__ void __launch_bounds__(kFinalThreads)
     k_energy_final(const double *__restrict__ partials, int nparts, double scale,
                    GreedyDevState st, int auto_reduce) {
-  double t = 0.0;
-  for (int i = threadIdx.x; i < nparts; i += blockDim.x) t += partials[i];
-  __shared__ double ws[kThreads / 32];  // fixed order: thread-strided, then warp tree
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  const int step = 4 * kFinalThreads;
+  int i = threadIdx.x;
+  for (; i + 3 * kFinalThreads < nparts; i += step) {
+    a0 += partials[i];
+    a1 += partials[i + kFinalThreads];
+    a2 += partials[i + 2 * kFinalThreads];
+    a3 += partials[i + 3 * kFinalThreads];
+  }
+  for (; i < nparts; i += kFinalThreads) a0 += partials[i];
+  double t = (a0 + a1) + (a2 + a3);
+  __shared__ double ws[kFinalThreads / 32];
   t = warp_sum(t);
   if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = t;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int w = 0; w < kThreads / 32; ++w) s += ws[w];
-    const double e = s * scale;
-    const int k = *st.count;
-    if (auto_reduce && k > 0) {
-      const double prev = st.energy[(k - 1) % st.cap];
-      if ((float)e - (float)prev > 0.0f) *st.step = *st.step / 2.0f;
+  if (threadIdx.x < 32) {
+    double u = ws[threadIdx.x];
+    u = warp_sum(u);
+    if (threadIdx.x == 0) {
+      const double e = u * scale;
+      const int k = *st.count;
+      if (auto_reduce && k > 0) {
+        const double prev = st.energy[(k - 1) % st.cap];
+        if ((float)e - (float)prev > 0.0f) *st.step = *st.step / 2.0f;
+      }
+      st.energy[k % st.cap] = e;
+      *st.count = k + 1;
     }
-    st.energy[k % st.cap] = e;
-    *st.count = k + 1;
   }
 }
 
@@ -155,6 +175,7 @@ int greedy_create(GreedyCtx *g, int nx, int ny, int nz, double spx, double spy, 
   const int rc = fluid_plan_create(&g->plan, nx, ny, nz, spx, spy, spz, alpha, beta, gamma);
   if (rc) return rc;
   g->d = g->plan.d;
+  g->di = g->d;
   g->sp = g->plan.sp;
   g->max_pert = max_pert;
   const long n = g->d.n();
@@ -196,11 +217,16 @@ cudaError_t greedy_stage(GreedyCtx *g, int stage, const float *I0, const float *
   float *v[3] = {g->vbuf, g->vbuf + n, g->vbuf + 2 * n};
   switch (stage) {
     case kStageForcePrep:
-      k_force_prep<<<prep_grid(d), kRowThreads, 0, s>>>(I0, I1, h[0], h[1], h[2], g->idef, g->partials, d);
+      if (g->am.on)
+        k_force_prep<true><<<prep_grid(d), kRowThreads, 0, s>>>(I0, I1, h[0], h[1], h[2], g->idef,
+                                                                g->partials, d, g->di, g->am);
+      else
+        k_force_prep<false><<<prep_grid(d), kRowThreads, 0, s>>>(I0, I1, h[0], h[1], h[2], g->idef,
+                                                                 g->partials, d, d, g->am);
       return cudaGetLastError();
     case kStageEnergy: {
       const double spprod = g->sp.x * g->sp.y * g->sp.z;
-      k_energy_final<<<1, kThreads, 0, s>>>(g->partials, g->nparts, spprod, g->st, auto_reduce);
+      k_energy_final<<<1, kFinalThreads, 0, s>>>(g->partials, g->nparts, spprod, g->st, auto_reduce);
       return cudaGetLastError();
     }
     case kStageXYForward:

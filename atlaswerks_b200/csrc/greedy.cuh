@@ -16,6 +16,8 @@ struct GreedyDevState {
 struct GreedyCtx {
   FluidPlan plan;
   Dims d;
+  Dims di;          // grid of I0 (= d, except for atlas subjects on their own grid)
+  AtlasMap am;      // template voxel -> I0 voxel map when di != d (atlas_point)
   Spacing sp;
   float max_pert;
   float *idef;      // I0(h), N

@@ -184,6 +184,43 @@ int aw_greedy_profile(aw_greedy_t g, const float *I0, const float *I1, const flo
 int aw_greedy_get_energies(aw_greedy_t g, double *out, int max_count, int *count);
 
 /* ---------------------------------------------------------------------------
+ * Greedy atlas building over the subjects resident on one GPU. Replaces the
+ * per-GPU thread of GreedyAtlasBuilder (Algorithms/Greedy/GreedyAtlasBuilder.txx:
+ * 150-301, Algorithms/Common/AtlasThread.txx:97-181,
+ * Algorithms/Greedy/GreedyAtlasThreadGPU.cxx:161-194). Every subject's
+ * deformation h_i (template grid, identity at create) is owned by the handle;
+ * the mean template (template grid) is the I1 of every subject. A subject
+ * image may sit on its own grid: it is sampled at (h + 0.5) * m/n - 0.5 per
+ * axis (voxel centres of equal physical extent); with equal grids the
+ * iteration is the reference's. Across GPUs, shard the subjects, call
+ * aw_atlas_compute_mean on each, sum the mean buffers (one all-reduce) and
+ * continue: the weights are the global ones.
+ * ------------------------------------------------------------------------- */
+typedef struct aw_atlas_s *aw_atlas_t;
+
+/* template grid, spacing, DiffOper parameters, MaxPert, local subject count */
+int aw_atlas_create(int nx, int ny, int nz, double spx, double spy, double spz, float alpha,
+                    float beta, float gamma, float max_pert, int n_subjects, aw_atlas_t *out);
+int aw_atlas_destroy(aw_atlas_t a);
+/* GreedyAtlasDefDataGPU(I, mean, weight): subject i's image (device, the
+ * caller keeps it alive, grid snx x sny x snz) and its mean weight */
+int aw_atlas_set_subject(aw_atlas_t a, int i, const float *img, int snx, int sny, int snz,
+                         float weight);
+/* device pointers of subject i's deformation (template grid; read or write
+ * between calls, e.g. to resume from a checkpoint) and of the mean buffer */
+int aw_atlas_field(aw_atlas_t a, int i, float **hx, float **hy, float **hz);
+int aw_atlas_mean_buffer(aw_atlas_t a, float **mean);
+/* ComputeThreadMean: mean = sum_i w_i I_i(h_i), float, in subject order */
+int aw_atlas_compute_mean(aw_atlas_t a, void *stream);
+/* n_iters greedy iterations of every subject toward the current mean;
+ * update_first=1 recomputes each subject's step at the first one
+ * (BeginImageIteration at iteration 0). Graph-captured, no host sync. */
+int aw_atlas_iterate(aw_atlas_t a, int n_iters, int update_first, void *stream);
+/* subject i's step size and energy history (oldest first); synchronise */
+int aw_atlas_get_step(aw_atlas_t a, int i, float *step);
+int aw_atlas_get_energies(aw_atlas_t a, int i, double *out, int max_count, int *count);
+
+/* ---------------------------------------------------------------------------
  * LDMM iterator (relaxation, splatting gradient). Replaces LDMMIteratorGPU /
  * LDMMIteratorCPU::IterateNew (Algorithms/LDMM/LDMMIteratorGPU.cxx:159-293,
  * LDMMIteratorCPU.cxx:529-631). Velocity fields are one device buffer

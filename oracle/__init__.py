@@ -88,6 +88,7 @@ class Oracle:
         L.aw_oracle_greedy_iterate.restype = ctypes.c_double
         L.aw_oracle_max_norm.restype = ctypes.c_float
         L.aw_oracle_ldmm_iterate.restype = ctypes.c_double
+        L.aw_oracle_atlas_iterate.restype = ctypes.c_double
 
     # --- interpolation family -------------------------------------------------
     def apply(self, img, h, bg=0.0):
@@ -228,6 +229,56 @@ class Oracle:
                                           update_step=(it == 0), step=step)
             energies.append(e)
         return h, hinv, np.array(energies), step
+
+
+    # --- atlas ------------------------------------------------------------------
+    def apply_atlas(self, img, h):
+        """Subject image (own grid) sampled at the atlas map of h (template grid)."""
+        out = np.empty(h.shape[1:], np.float32)
+        mx, my, mz = _shape(img)
+        self.lib.aw_oracle_apply_atlas(_fp(img), _i(mx), _i(my), _i(mz), _fp(h[0]), _fp(h[1]),
+                                       _fp(h[2]), _fp(out), *_shape(h))
+        return out
+
+    def atlas_mean(self, imgs, hs, weights):
+        """GreedyAtlasThreadCPU::ComputeThreadMean over subjects in order."""
+        ns = len(imgs)
+        shape = hs[0].shape[1:]
+        mean = np.empty(shape, np.float32)
+        ip = (_f * ns)(*[_fp(a) for a in imgs])
+        dims = (ctypes.c_int * (3 * ns))(*[d for a in imgs for d in _shape(a)])
+        hp = (_f * (3 * ns))(*[_fp(h[c]) for h in hs for c in range(3)])
+        w = (ctypes.c_float * ns)(*weights)
+        self.lib.aw_oracle_atlas_mean(ip, dims, hp, w, _i(ns), _fp(mean), *_shape(hs[0]))
+        return mean
+
+    def atlas_iterate(self, img, mean, h, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01,
+                      gamma=0.001, max_pert=0.5, update_step=False, step=0.0):
+        st = ctypes.c_float(step)
+        mx, my, mz = _shape(img)
+        e = self.lib.aw_oracle_atlas_iterate(
+            _fp(img), _i(mx), _i(my), _i(mz), _fp(mean), _fp(h[0]), _fp(h[1]), _fp(h[2]),
+            *_shape(h), *map(_dbl, sp), _dbl(alpha), _dbl(beta), _dbl(gamma),
+            ctypes.c_float(max_pert), _i(int(update_step)), ctypes.byref(st))
+        return float(e), float(st.value)
+
+    def atlas_run(self, imgs, weights, shape, iters, mean_period=1, sp=(1.0, 1.0, 1.0),
+                  alpha=0.01, beta=0.01, gamma=0.001, max_pert=0.5):
+        """AtlasThread::AtlasThreadMain at one scale: mean, then per iteration
+        one greedy step of every subject toward the mean, the mean recomputed
+        after every mean_period-th iteration. Returns (mean, [h_i],
+        energies [iters, ns], steps)."""
+        hs = [identity(shape) for _ in imgs]
+        mean = self.atlas_mean(imgs, hs, weights)
+        steps = [0.0] * len(imgs)
+        en = np.zeros((iters, len(imgs)))
+        for it in range(iters):
+            for k, img in enumerate(imgs):
+                en[it, k], steps[k] = self.atlas_iterate(img, mean, hs[k], sp, alpha, beta, gamma,
+                                                         max_pert, it == 0, steps[k])
+            if (it + 1) % mean_period == 0:
+                mean = self.atlas_mean(imgs, hs, weights)
+        return mean, hs, en, steps
 
 
 _quiet_lock = threading.Lock()
@@ -381,3 +432,24 @@ class Reference:
                 ctypes.byref(st))
         self._check(rc)
         return v, en, float(st.value)
+
+    def atlas_run(self, imgs, weights, iters, mean_period=1, sp=(1.0, 1.0, 1.0), alpha=0.01,
+                  beta=0.01, gamma=0.001, max_pert=0.5):
+        """The reference's GreedyDeformationData / GreedyIteratorCPU driven
+        through the AtlasThreadMain loop (equal grids). Returns (mean, [h_i],
+        energies [iters, ns])."""
+        ns = len(imgs)
+        shape = imgs[0].shape
+        n = imgs[0].size
+        stack = np.ascontiguousarray(np.stack(imgs), np.float32)
+        w = (ctypes.c_float * ns)(*weights)
+        mean = np.empty(shape, np.float32)
+        h = np.empty((ns, 3) + shape, np.float32)
+        en = np.zeros((iters, ns), np.float64)
+        with quiet_stdout():
+            rc = self.lib.awref_atlas_run(
+                stack.ctypes.data_as(_f), _i(ns), w, *_shape(imgs[0]), *map(_dbl, sp), _i(iters),
+                ctypes.c_float(max_pert), _dbl(alpha), _dbl(beta), _dbl(gamma), _i(mean_period),
+                _fp(mean), h.ctypes.data_as(_f), _dp(en))
+        self._check(rc)
+        return mean, [h[k] for k in range(ns)], en

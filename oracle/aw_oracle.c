@@ -435,16 +435,17 @@ float aw_oracle_max_norm(const float *vx, const float *vy, const float *vz, long
  * energy spacing^3 * sum (I1 - I0(h))^2 of the incoming h, accumulated in
  * double (the reference accumulates in float).
  * ---------------------------------------------------------------------- */
-double aw_oracle_greedy_iterate(const float *I0, const float *I1, float *hx, float *hy, float *hz,
-                                float *hix, float *hiy, float *hiz, int nx, int ny, int nz,
-                                double spx, double spy, double spz, double alpha, double beta,
-                                double gamma, float max_pert, int update_step, float *step) {
+/* The iteration after I0(h): GreedyIteratorCPU::Iterate from the gradient
+ * on (Greedy/GreedyIteratorCPU.cxx:105-137). idef = I0(h). */
+static double greedy_iterate_idef(const float *idef, const float *I1, float *hx, float *hy,
+                                  float *hz, float *hix, float *hiy, float *hiz, int nx, int ny,
+                                  int nz, double spx, double spy, double spz, double alpha,
+                                  double beta, double gamma, float max_pert, int update_step,
+                                  float *step) {
   const long n = (long)nx * ny * nz;
-  float *idef = (float *)malloc(sizeof(float) * (size_t)n);
   float *f = (float *)malloc(sizeof(float) * (size_t)(3 * n));
   float *o = (float *)malloc(sizeof(float) * (size_t)(3 * n));
   float *fx = f, *fy = f + n, *fz = f + 2 * n;
-  aw_oracle_apply(I0, hx, hy, hz, idef, nx, ny, nz, 0.0f);
   aw_oracle_gradient(idef, fx, fy, fz, nx, ny, nz, spx, spy, spz, 0);
   double e = 0.0;
   for (long i = 0; i < n; ++i) {
@@ -475,10 +476,76 @@ double aw_oracle_greedy_iterate(const float *I0, const float *I1, float *hx, flo
     memcpy(hiy, o + n, sizeof(float) * (size_t)n);
     memcpy(hiz, o + 2 * n, sizeof(float) * (size_t)n);
   }
-  free(idef);
   free(f);
   free(o);
   return e;
+}
+
+double aw_oracle_greedy_iterate(const float *I0, const float *I1, float *hx, float *hy, float *hz,
+                                float *hix, float *hiy, float *hiz, int nx, int ny, int nz,
+                                double spx, double spy, double spz, double alpha, double beta,
+                                double gamma, float max_pert, int update_step, float *step) {
+  const long n = (long)nx * ny * nz;
+  float *idef = (float *)malloc(sizeof(float) * (size_t)n);
+  aw_oracle_apply(I0, hx, hy, hz, idef, nx, ny, nz, 0.0f);
+  const double e = greedy_iterate_idef(idef, I1, hx, hy, hz, hix, hiy, hiz, nx, ny, nz, spx, spy,
+                                       spz, alpha, beta, gamma, max_pert, update_step, step);
+  free(idef);
+  return e;
+}
+
+/* I(h) for an atlas subject on its own grid (mx, my, mz) with h on the
+ * template grid (nx, ny, nz): the sample point is (h + 0.5) * (m / n) - 0.5
+ * per axis in double; with equal grids it is h itself
+ * (HField3DUtils::apply, UtilitiesDataTypes/HField3DUtils.txx:734-752). */
+void aw_oracle_apply_atlas(const float *img, int mx, int my, int mz, const float *hx,
+                           const float *hy, const float *hz, float *out, int nx, int ny, int nz) {
+  const int same = mx == nx && my == ny && mz == nz;
+  const double rx = (double)mx / (double)nx, ry = (double)my / (double)ny,
+               rz = (double)mz / (double)nz;
+  const long n = (long)nx * ny * nz;
+  for (long i = 0; i < n; ++i) {
+    double px = (double)hx[i], py = (double)hy[i], pz = (double)hz[i];
+    if (!same) {
+      px = (px + 0.5) * rx - 0.5;
+      py = (py + 0.5) * ry - 0.5;
+      pz = (pz + 0.5) * rz - 0.5;
+    }
+    out[i] = trilerp_val(img, mx, my, mz, px, py, pz, 0.0f);
+  }
+}
+
+/* One greedy iteration of atlas subject (I0 on its own grid) toward the
+ * mean I1 (template grid): the iteration of AtlasThread::AtlasThreadMain
+ * (Common/AtlasThread.txx:137-152) for one image. */
+double aw_oracle_atlas_iterate(const float *I0, int mx, int my, int mz, const float *I1, float *hx,
+                               float *hy, float *hz, int nx, int ny, int nz, double spx,
+                               double spy, double spz, double alpha, double beta, double gamma,
+                               float max_pert, int update_step, float *step) {
+  const long n = (long)nx * ny * nz;
+  float *idef = (float *)malloc(sizeof(float) * (size_t)n);
+  aw_oracle_apply_atlas(I0, mx, my, mz, hx, hy, hz, idef, nx, ny, nz);
+  const double e = greedy_iterate_idef(idef, I1, hx, hy, hz, NULL, NULL, NULL, nx, ny, nz, spx,
+                                       spy, spz, alpha, beta, gamma, max_pert, update_step, step);
+  free(idef);
+  return e;
+}
+
+/* The thread mean of GreedyAtlasThreadCPU::ComputeThreadMean
+ * (Greedy/GreedyAtlasThreadCPU.cxx): mean = 0, then for each subject in
+ * order mean[j] += I_i(h_i)[j] * w_i in float. dims holds (mx, my, mz) per
+ * subject, h holds 3 pointers per subject. */
+void aw_oracle_atlas_mean(const float *const *imgs, const int *dims, const float *const *h,
+                          const float *w, int ns, float *mean, int nx, int ny, int nz) {
+  const long n = (long)nx * ny * nz;
+  float *d = (float *)malloc(sizeof(float) * (size_t)n);
+  for (long j = 0; j < n; ++j) mean[j] = 0.0f;
+  for (int k = 0; k < ns; ++k) {
+    aw_oracle_apply_atlas(imgs[k], dims[3 * k], dims[3 * k + 1], dims[3 * k + 2], h[3 * k],
+                          h[3 * k + 1], h[3 * k + 2], d, nx, ny, nz);
+    for (long j = 0; j < n; ++j) mean[j] += d[j] * w[k];
+  }
+  free(d);
 }
 
 void aw_oracle_identity(float *hx, float *hy, float *hz, int nx, int ny, int nz) {

@@ -51,6 +51,15 @@ double aw_oracle_greedy_iterate(const float *I0, const float *I1, float *hx, flo
                                 double spx, double spy, double spz, double alpha, double beta,
                                 double gamma, float max_pert, int update_step, float *step);
 
+void aw_oracle_apply_atlas(const float *img, int mx, int my, int mz, const float *hx,
+                           const float *hy, const float *hz, float *out, int nx, int ny, int nz);
+double aw_oracle_atlas_iterate(const float *I0, int mx, int my, int mz, const float *I1, float *hx,
+                               float *hy, float *hz, int nx, int ny, int nz, double spx,
+                               double spy, double spz, double alpha, double beta, double gamma,
+                               float max_pert, int update_step, float *step);
+void aw_oracle_atlas_mean(const float *const *imgs, const int *dims, const float *const *h,
+                          const float *w, int ns, float *mean, int nx, int ny, int nz);
+
 double aw_oracle_ldmm_iterate(const float *I0, const float *I1, float *v, int T, int nx, int ny,
                               int nz, double spx, double spy, double spz, double alpha,
                               double beta, double gamma, float sigma, float *step,

@@ -310,6 +310,79 @@ int awref_greedy_run(const float *i0, const float *i1, int nx, int ny, int nz, d
   GUARD_END
 }
 
+/* Greedy atlas on one node and one thread, one scale, equal grids: the loop
+ * of AtlasThread::AtlasThreadMain (Algorithms/Common/AtlasThread.txx:97-181)
+ * over the reference's GreedyDeformationData with I1 = the shared mean and
+ * ScaleI1 off (the set-up of GreedyAtlasDefDataCPU), one GreedyIteratorCPU
+ * for all subjects (Greedy/GreedyAtlasThreadCPU.cxx InitThread), the step
+ * recomputed at iteration 0 (BeginImageIteration), and the mean of
+ * GreedyAtlasThreadCPU::ComputeThreadMean via GetI0At1, recomputed after
+ * every `mean_period`-th iteration (1: after every iteration, as there).
+ * imgs: ns images back to back; h_out: ns x 3 planes; energies: iters x ns. */
+int awref_atlas_run(const float *imgs, int ns, const float *weights, int nx, int ny, int nz,
+                    double spx, double spy, double spz, int iters, float maxpert, double alpha,
+                    double beta, double gamma, int mean_period, float *mean_out, float *h_out,
+                    double *energies) {
+  GUARD_BEGIN
+  std::ostringstream xml;
+  xml.precision(17);
+  xml << "<GreedyWarpParameterFile><GreedyScaleLevel><ScaleLevel><DownsampleFactor val=\"1\"/>"
+      << "</ScaleLevel><GreedyIterator>" << diffoper_xml(alpha, beta, gamma)
+      << "<MaxPert val=\"" << maxpert << "\"/></GreedyIterator><NIterations val=\"" << iters
+      << "\"/></GreedyScaleLevel><AutoStepReduce val=\"false\"/></GreedyWarpParameterFile>";
+  GreedyParam param;
+  parse_into(param, xml.str());
+  SizeType size(nx, ny, nz);
+  SpacingType sp(spx, spy, spz);
+  OriginType origin(0, 0, 0);
+  const long n = (long)nx * ny * nz;
+  RealImage mean(size, origin, sp);
+  mean.fill(0.f);
+  std::vector<RealImage *> ims;
+  std::vector<GreedyDeformationData *> data;
+  for (int i = 0; i < ns; ++i) {
+    ims.push_back(new RealImage(size, origin, sp));
+    to_im(imgs + i * n, *ims.back());
+    data.push_back(new GreedyDeformationData(ims.back(), &mean, param));
+    data.back()->ScaleI1(false);
+  }
+  MultiscaleManager scaleManager(size, sp, origin, param);
+  scaleManager.SetScaleVectorFields(true);
+  GreedyIteratorCPU iterator(size, origin, sp, true);
+  for (auto *d : data) d->InitializeWarp();
+  scaleManager.SetScaleLevel(0);
+  iterator.SetScaleLevel(scaleManager, param.GetScaleLevel(0).Iterator());
+  for (auto *d : data) d->SetScaleLevel(scaleManager);
+  RealImage defIm(size, origin, sp);
+  auto thread_mean = [&]() {
+    mean.fill(0.0);
+    Real *avg = mean.getDataPointer();
+    for (int i = 0; i < ns; ++i) {
+      data[i]->GetI0At1(defIm);
+      const Real *im = defIm.getDataPointer();
+      for (long j = 0; j < n; ++j) avg[j] += im[j] * weights[i];
+    }
+  };
+  thread_mean();
+  for (int iter = 0; iter < iters; ++iter) {
+    for (int i = 0; i < ns; ++i) {
+      data[i]->SetCurIter(iter);
+      if (iter == 0) iterator.UpdateStepSizeNextIteration();
+      iterator.Iterate(*data[i]);
+      if (energies) energies[(long)iter * ns + i] = data[i]->GetEnergyHistory().LastEnergy()->GetEnergy();
+    }
+    if ((iter + 1) % mean_period == 0) thread_mean();
+  }
+  from_im(mean, mean_out);
+  for (int i = 0; i < ns; ++i) {
+    float *o = h_out + (long)i * 3 * n;
+    from_vf(data[i]->Def1To0(), o, o + n, o + 2 * n);
+  }
+  for (auto *d : data) delete d;
+  for (auto *im : ims) delete im;
+  GUARD_END
+}
+
 /* ImageUtils::gaussianDownsample (MultiscaleManager::DownsampleToLevel) */
 int awref_downsample(const float *in, int nx, int ny, int nz, double spx, double spy, double spz,
                      float *out, int mx, int my, int mz) {
