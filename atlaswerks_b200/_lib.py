@@ -61,6 +61,15 @@ SIGNATURES = {
     "aw_greedy_run": ([_fp] * 15 + [_i, _i, _fp], _i),
     "aw_greedy_profile": ([_fp] * 15 + [_i, _fp, _fp], _i),
     "aw_greedy_get_energies": ([_fp, _fp, _i, _fp], _i),
+    "aw_atlas_create": ([_i] * 3 + [_d] * 3 + [_f] * 4 + [_i, _fp], _i),
+    "aw_atlas_destroy": ([_fp], _i),
+    "aw_atlas_set_subject": ([_fp, _i, _fp, _i, _i, _i, _f], _i),
+    "aw_atlas_field": ([_fp, _i, _fp, _fp, _fp], _i),
+    "aw_atlas_mean_buffer": ([_fp, _fp], _i),
+    "aw_atlas_compute_mean": ([_fp, _fp], _i),
+    "aw_atlas_iterate": ([_fp, _i, _i, _fp], _i),
+    "aw_atlas_get_step": ([_fp, _i, _fp], _i),
+    "aw_atlas_get_energies": ([_fp, _i, _fp, _i, _fp], _i),
     "aw_ldmm_create": ([_i] * 3 + [_d] * 3 + [_f] * 3 + [_i, _f, _f, _fp], _i),
     "aw_ldmm_destroy": ([_fp], _i),
     "aw_ldmm_set_step": ([_fp, _f], _i),

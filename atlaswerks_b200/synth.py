@@ -84,12 +84,15 @@ def warp(img: np.ndarray, u: np.ndarray) -> np.ndarray:
 
 
 def greedy_pair(shape: Shape, seed: int, n_blobs: int = 8, umax: float = 3.0,
-                noise_sd: float = 0.0) -> Tuple[np.ndarray, np.ndarray]:
+                noise_sd: float = 0.0, sigma_range=(4.0, 10.0),
+                smooth_sigma: float = 8.0) -> Tuple[np.ndarray, np.ndarray]:
     """(I0 source, I1 target) for pair registration: I1 = I0 warped by a
-    smooth random displacement, plus optional Gaussian noise on both."""
+    smooth random displacement, plus optional Gaussian noise on both.
+    sigma_range / smooth_sigma shrink the blobs and the displacement
+    correlation length for grids much smaller than 64^3."""
     rng = rng_for(seed)
-    src = blobs(shape, n_blobs, rng)
-    u = smooth_displacement(shape, umax, rng)
+    src = blobs(shape, n_blobs, rng, sigma_range)
+    u = smooth_displacement(shape, umax, rng, smooth_sigma)
     tgt = warp(src, u)
     if noise_sd > 0:
         src = (src + rng.normal(0.0, noise_sd, shape)).astype(np.float32)

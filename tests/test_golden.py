@@ -1,0 +1,107 @@
+"""The oracle against the golden fixtures in tests/golden/ — outputs of the
+reference's own CPU code (compiled from its sources; tests/golden/
+make_golden.py made them). These run anywhere, without the reference tree.
+
+Tolerances: interpolation family, gradient, splat, downsample, upsample:
+bit-exact. Fluid operator: the oracle's FP64 solve vs the reference's FP32
+one, 1e-5 of the field's maximum (the FP64 golden to 1e-12). Greedy, LDMM
+and atlas runs: 1e-4 voxel (fields) and 1e-5 relative (energies), the FP32
+rounding of the reference's transforms carried through the iterations.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import identity
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+BG = ["partial_id", "id", "partial_zero", "zero", "clamp", "wrap"]
+
+
+def load(name):
+    return np.load(os.path.join(GOLDEN, name + ".npz"))
+
+
+def test_interpolation_family(oracle):
+    z = load("interp_9x13x11")
+    img, h, v, sp = z["img"], z["h"], z["v"], tuple(z["sp"])
+    assert np.array_equal(oracle.apply(img, h), z["apply"])
+    assert np.array_equal(oracle.gradient(img, sp, False), z["gradient"])
+    assert np.array_equal(oracle.gradient(img, sp, True), z["gradient_wrap"])
+    assert np.array_equal(oracle.splat(img, h), z["splat"])
+    for b, name in enumerate(BG):
+        assert np.array_equal(oracle.compose_hv(h, v, sp, 1, b), z["compose_hv_" + name]), name
+        assert np.array_equal(oracle.compose_hv(h, v, sp, -1, b), z["compose_hvinv_" + name]), name
+        assert np.array_equal(oracle.compose_vh(v, h, sp, -1, b), z["compose_vhinv_" + name]), name
+
+
+def test_fluid_operator(oracle):
+    z = load("fluid_16x12x20")
+    f, sp = z["f"], tuple(z["sp"])
+    # the reference holds alpha, beta, gamma as float (Real)
+    a, b, g = (float(np.float32(z[k])) for k in ("alpha", "beta", "gamma"))
+    inv = oracle.fluid(f, sp, a, b, g, True)
+    assert np.abs(inv - z["inverse"]).max() <= 1e-5 * np.abs(z["inverse"]).max()
+    fwd = oracle.fluid(f, sp, a, b, g, False)
+    assert np.abs(fwd - z["forward"]).max() <= 1e-5 * np.abs(z["forward"]).max()
+    inv64 = oracle.fluid_f64(f, sp, a, b, g, True)
+    assert np.abs(inv64 - z["inverse_f64"]).max() <= 1e-12 * np.abs(z["inverse_f64"]).max()
+
+
+def test_greedy_single_scale(oracle):
+    z = load("greedy_16")
+    h, hinv, en, step = oracle.greedy_run(z["I0"], z["I1"], len(z["energies"]), inverse=True)
+    assert np.abs(h - z["h"]).max() <= 1e-4
+    assert np.abs(hinv - z["hinv"]).max() <= 1e-4
+    assert np.allclose(en, z["energies"], rtol=1e-5)
+    assert abs(step - z["steps"][-1]) <= 1e-6 * z["steps"][-1]
+
+
+def test_greedy_two_scales(oracle):
+    z = load("greedy_24_two_scales")
+    h, _, en = oracle.greedy_warp(z["I0"], z["I1"], [(2, 10, 0.5), (1, 6, 0.5)])
+    assert np.abs(h - z["h"]).max() <= 1e-4
+    assert np.allclose(np.concatenate(en), z["energies"], rtol=1e-5)
+
+
+def test_multiscale_resampling(oracle):
+    z = load("downsample_16x20x24")
+    assert np.array_equal(oracle.downsample(z["img"], (12, 10, 8)), z["half"])
+    z = load("upsample_12x10x8")
+    assert np.array_equal(oracle.upsample_hfield(z["h"], (16, 20, 24), True), z["up"])
+    assert np.array_equal(oracle.upsample_hfield(z["h"], (16, 20, 24), False), z["up_norescale"])
+
+
+@pytest.mark.parametrize("adaptive", [False, True])
+def test_ldmm_iterate_new(oracle, adaptive):
+    z = load("ldmm_16_T4")
+    sfx = "_adaptive" if adaptive else ""
+    want_v, want_e = z["v" + sfx], z["energies" + sfx]
+    v = np.zeros_like(want_v)
+    step, en = 0.01, []
+    if adaptive:
+        # LDMMWarp: a step-size pass (v unchanged, no energy) before iteration 0
+        _, step = oracle.ldmm_iterate(z["I0"], z["I1"], v, sigma=1.0, step=step,
+                                      update_step=True, max_pert=0.2)
+    for it in range(len(want_e)):
+        e, step = oracle.ldmm_iterate(z["I0"], z["I1"], v, sigma=1.0, step=step)
+        en.append(e)
+    assert np.abs(v - want_v).max() <= 1e-4 * np.abs(want_v).max()
+    assert np.allclose(en, want_e, rtol=1e-5)
+    assert abs(step - float(z["step" + sfx])) <= 1e-6 * float(z["step" + sfx])
+
+
+@pytest.mark.parametrize("period", [1, 2])
+def test_atlas(oracle, period):
+    z = load("atlas_16x3")
+    imgs = [a for a in z["imgs"]]
+    mean, hs, en, _ = oracle.atlas_run(imgs, list(z["w"]), (16, 16, 16), 6, period)
+    assert np.abs(mean - z[f"mean_p{period}"]).max() <= 1e-5
+    assert np.abs(np.stack(hs) - z[f"h_p{period}"]).max() <= 1e-4
+    assert np.allclose(en, z[f"energies_p{period}"], rtol=1e-5)
+
+
+def test_identity_helper():
+    h = identity((2, 3, 4))
+    assert h.shape == (3, 2, 3, 4) and h[0, 1, 2, 3] == 3 and h[1, 1, 2, 3] == 2 and h[2, 1, 2, 3] == 1
