@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
 
 #define AW_HD __host__ __device__ __forceinline__
@@ -55,6 +56,28 @@ AW_D float fmul(float a, float b) { return __fmul_rn(a, b); }
 AW_D float fadd(float a, float b) { return __fadd_rn(a, b); }
 AW_D float fsub(float a, float b) { return __fsub_rn(a, b); }
 AW_D float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+
+// x / d as the reference divides (IEEE, round to nearest). When d is a power
+// of two the quotient is x scaled by an exact power of two, and x * (1/d)
+// is the same number: the multiply replaces the division sequence.
+struct DivD {
+  double d, r;
+  int p2;
+};
+struct DivF {
+  float d, r;
+  int p2;
+};
+inline bool host_is_pow2(double d) {
+  if (!(d > 0.0)) return false;
+  int e = 0;
+  const double m = frexp(d, &e);
+  return m == 0.5 && e > -1000 && e < 1000;
+}
+inline DivD make_div(double d) { return DivD{d, 1.0 / d, host_is_pow2(d) ? 1 : 0}; }
+inline DivF make_divf(float d) { return DivF{d, 1.0f / d, host_is_pow2((double)d) ? 1 : 0}; }
+AW_D double ddiv(double x, const DivD &q) { return q.p2 ? dmul(x, q.r) : __ddiv_rn(x, q.d); }
+AW_D float fdivq(float x, const DivF &q) { return q.p2 ? fmul(x, q.r) : fdiv(x, q.d); }
 
 // Atlas subjects on grids of their own: a deformation lives on the template
 // grid (n voxels per axis) and points into the subject's grid (m voxels per

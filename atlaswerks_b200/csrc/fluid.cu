@@ -341,7 +341,7 @@ cudaError_t fluid_forward_field(const FluidPlan &p, const float *fx, const float
 
 cudaError_t fluid_forward_force(const FluidPlan &p, const float *G, const float *A, int diff,
                                 cudaStream_t s) {
-  SrcForce src{G, A, diff, p.sp};
+  const SrcForce src = make_force(G, A, diff, p.sp);
   if (p.fast) return fast_xy_forward(p, src, s);
   k_fft_xy_fwd<SrcForce><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, src);
   return cudaGetLastError();

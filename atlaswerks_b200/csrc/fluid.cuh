@@ -62,31 +62,41 @@ struct SrcForce {
   const float *G;
   const float *A;
   int diff;
-  Spacing sp;
+  DivD c2[3], c1[3];  // 2 sp and sp per axis
   AW_D float value(int comp, int x, int y, int z, const Dims &d) const {
     const long i = d.idx(x, y, z);
     const float g0 = __ldg(G + i);
-    int lo, hi, pos, n;
+    int pos, n;
     long stride;
-    double s;
-    if (comp == 0) { pos = x; n = d.nx; stride = 1; s = sp.x; }
-    else if (comp == 1) { pos = y; n = d.ny; stride = d.nx; s = sp.y; }
-    else { pos = z; n = d.nz; stride = (long)d.nx * d.ny; s = sp.z; }
+    if (comp == 0) { pos = x; n = d.nx; stride = 1; }
+    else if (comp == 1) { pos = y; n = d.ny; stride = d.nx; }
+    else { pos = z; n = d.nz; stride = (long)d.nx * d.ny; }
     float grad;
     if (pos > 0 && pos < n - 1) {
-      lo = -1; hi = 1;
-      grad = __double2float_rn((double)fsub(__ldg(G + i + hi * stride), __ldg(G + i + lo * stride)) /
-                               (2.0 * s));
+      grad = __double2float_rn(ddiv((double)fsub(__ldg(G + i + stride), __ldg(G + i - stride)),
+                                    c2[comp]));
     } else if (pos == 0) {
-      grad = __double2float_rn((double)fsub(__ldg(G + i + stride), g0) / s);
+      grad = __double2float_rn(ddiv((double)fsub(__ldg(G + i + stride), g0), c1[comp]));
     } else {
-      grad = __double2float_rn((double)fsub(g0, __ldg(G + i - stride)) / s);
+      grad = __double2float_rn(ddiv((double)fsub(g0, __ldg(G + i - stride)), c1[comp]));
     }
     const float a = __ldg(A + i);
     const float m = diff ? -fsub(g0, a) : a;
     return fmul(grad, m);
   }
 };
+inline SrcForce make_force(const float *G, const float *A, int diff, const Spacing &sp) {
+  SrcForce f;
+  f.G = G;
+  f.A = A;
+  f.diff = diff;
+  const double s[3] = {sp.x, sp.y, sp.z};
+  for (int c = 0; c < 3; ++c) {
+    f.c2[c] = make_div(2.0 * s[c]);
+    f.c1[c] = make_div(s[c]);
+  }
+  return f;
+}
 
 // --- consumers for the inverse pass ----------------------------------------
 struct DstField {

@@ -273,19 +273,20 @@ AW_D void solve_point(const FluidPlan &p, int kx, int ky, int kz, int inverse, f
   b0.x *= invN; b0.y *= invN; b1.x *= invN; b1.y *= invN; b2.x *= invN; b2.y *= invN;
   float2 o0, o1, o2;
   if (inverse) {
-    // Cholesky L = G G^T, then G y = b, G^T x = y (real matrix, complex rhs)
-    const float G00 = sqrtf(L00);
-    const float G10 = L10 / G00, G20 = L20 / G00;
-    const float G11 = sqrtf(L11 - G10 * G10);
-    const float G21 = (L21 - G20 * G10) / G11;
-    const float G22 = sqrtf(L22 - (G20 * G20 + G21 * G21));
+    // Cholesky L = G G^T, then G y = b, G^T x = y (real matrix, complex
+    // rhs), dividing by the diagonal through its reciprocals
+    const float G00 = sqrtf(L00), i00 = 1.0f / G00;
+    const float G10 = L10 * i00, G20 = L20 * i00;
+    const float G11 = sqrtf(L11 - G10 * G10), i11 = 1.0f / G11;
+    const float G21 = (L21 - G20 * G10) * i11;
+    const float G22 = sqrtf(L22 - (G20 * G20 + G21 * G21)), i22 = 1.0f / G22;
     float2 y0, y1, y2;
-    y0.x = b0.x / G00;                              y0.y = b0.y / G00;
-    y1.x = (b1.x - G10 * y0.x) / G11;               y1.y = (b1.y - G10 * y0.y) / G11;
-    y2.x = (b2.x - G20 * y0.x - G21 * y1.x) / G22;  y2.y = (b2.y - G20 * y0.y - G21 * y1.y) / G22;
-    o2.x = y2.x / G22;                              o2.y = y2.y / G22;
-    o1.x = (y1.x - G21 * o2.x) / G11;               o1.y = (y1.y - G21 * o2.y) / G11;
-    o0.x = (y0.x - G10 * o1.x - G20 * o2.x) / G00;  o0.y = (y0.y - G10 * o1.y - G20 * o2.y) / G00;
+    y0.x = b0.x * i00;                              y0.y = b0.y * i00;
+    y1.x = (b1.x - G10 * y0.x) * i11;               y1.y = (b1.y - G10 * y0.y) * i11;
+    y2.x = (b2.x - G20 * y0.x - G21 * y1.x) * i22;  y2.y = (b2.y - G20 * y0.y - G21 * y1.y) * i22;
+    o2.x = y2.x * i22;                              o2.y = y2.y * i22;
+    o1.x = (y1.x - G21 * o2.x) * i11;               o1.y = (y1.y - G21 * o2.y) * i11;
+    o0.x = (y0.x - G10 * o1.x - G20 * o2.x) * i00;  o0.y = (y0.y - G10 * o1.y - G20 * o2.y) * i00;
   } else {
     o0.x = L00 * b0.x + L10 * b1.x + L20 * b2.x;  o0.y = L00 * b0.y + L10 * b1.y + L20 * b2.y;
     o1.x = L10 * b0.x + L11 * b1.x + L21 * b2.x;  o1.y = L10 * b0.y + L11 * b1.y + L21 * b2.y;

@@ -130,22 +130,25 @@ __global__ void k_set_step(const unsigned *__restrict__ maxbits, float max_pert,
 // composeHV(h, eps*v, PARTIAL_ID) and, when hinv is given,
 // composeVHInv(eps*v, hinv, PARTIAL_ZERO) — GreedyIteratorCPU::updateDeformation
 // (GreedyIteratorCPU.cxx:83-95), both from one read of v.
+// composeHV(h, eps*v, PARTIAL_ID) and, when hinv is given,
+// composeVHInv(eps*v, hinv, PARTIAL_ZERO) — GreedyIteratorCPU::updateDeformation
+// (GreedyIteratorCPU.cxx:83-95), both from one read of v. q[] divides by the
+// float spacing (a multiply when it is a power of two).
 __global__ void __launch_bounds__(kRowThreads)
     k_update(const float *__restrict__ hx, const float *__restrict__ hy, const float *__restrict__ hz,
              const float *__restrict__ vx, const float *__restrict__ vy, const float *__restrict__ vz,
              float *__restrict__ ox, float *__restrict__ oy, float *__restrict__ oz,
              const float *__restrict__ gx, const float *__restrict__ gy, const float *__restrict__ gz,
              float *__restrict__ qx, float *__restrict__ qy, float *__restrict__ qz, Dims d,
-             Spacing sp, const float *__restrict__ step_ptr) {
+             DivF q0, DivF q1, DivF q2, const float *__restrict__ step_ptr) {
   Voxel vox;
   if (!voxel_of(d, vox)) return;
   const long i = vox.i;
   const int x = vox.x, y = vox.y, z = vox.z;
   const float eps = *step_ptr;
-  const float sx = (float)sp.x, sy = (float)sp.y, sz = (float)sp.z;
-  const float px = fadd(__int2float_rn(x), fdiv(fmul(vx[i], eps), sx));
-  const float py = fadd(__int2float_rn(y), fdiv(fmul(vy[i], eps), sy));
-  const float pz = fadd(__int2float_rn(z), fdiv(fmul(vz[i], eps), sz));
+  const float px = fadd(__int2float_rn(x), fdivq(fmul(vx[i], eps), q0));
+  const float py = fadd(__int2float_rn(y), fdivq(fmul(vy[i], eps), q1));
+  const float pz = fadd(__int2float_rn(z), fdivq(fmul(vz[i], eps), q2));
   float rx, ry, rz;
   trilerp_vector(hx, hy, hz, d, px, py, pz, BG_PARTIAL_ID, 1.0f, rx, ry, rz);
   ox[i] = rx;
@@ -155,9 +158,10 @@ __global__ void __launch_bounds__(kRowThreads)
     const float g0 = gx[i], g1 = gy[i], g2 = gz[i];
     float a, b, c;
     trilerp_vector(vx, vy, vz, d, g0, g1, g2, BG_PARTIAL_ZERO, eps, a, b, c);
-    qx[i] = fadd(fdiv(a, -sx), g0);
-    qy[i] = fadd(fdiv(b, -sy), g1);
-    qz[i] = fadd(fdiv(c, -sz), g2);
+    // a / -s = -(a / s) exactly in round-to-nearest
+    qx[i] = fadd(-fdivq(a, q0), g0);
+    qy[i] = fadd(-fdivq(b, q1), g1);
+    qz[i] = fadd(-fdivq(c, q2), g2);
   }
 }
 
@@ -195,6 +199,10 @@ int greedy_create(GreedyCtx *g, int nx, int ny, int nz, double spx, double spy, 
   g->st.step = reinterpret_cast<float *>(g->scalars);
   g->st.count = reinterpret_cast<int *>(g->scalars + 4);
   g->maxbits = reinterpret_cast<unsigned *>(g->scalars + 8);
+  if (cudaStreamCreateWithFlags(&g->aux, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&g->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&g->ev_join, cudaEventDisableTiming) != cudaSuccess)
+    return 4;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
@@ -205,6 +213,9 @@ void greedy_destroy(GreedyCtx *g) {
   if (g->partials) cudaFree(g->partials);
   if (g->st.energy) cudaFree(g->st.energy);
   if (g->scalars) cudaFree(g->scalars);
+  if (g->aux) cudaStreamDestroy(g->aux);
+  if (g->ev_fork) cudaEventDestroy(g->ev_fork);
+  if (g->ev_join) cudaEventDestroy(g->ev_join);
   std::memset(g, 0, sizeof(*g));
 }
 
@@ -248,22 +259,30 @@ cudaError_t greedy_stage(GreedyCtx *g, int stage, const float *I0, const float *
           h[0], h[1], h[2], v[0], v[1], v[2], h_out[0], h_out[1], h_out[2],
           inv ? hinv[0] : nullptr, inv ? hinv[1] : nullptr, inv ? hinv[2] : nullptr,
           inv ? hinv_out[0] : nullptr, inv ? hinv_out[1] : nullptr, inv ? hinv_out[2] : nullptr,
-          d, g->sp, g->st.step);
+          d, make_divf((float)g->sp.x), make_divf((float)g->sp.y), make_divf((float)g->sp.z),
+          g->st.step);
       return cudaGetLastError();
     }
   }
   return cudaErrorInvalidValue;
 }
 
+// The energy sum runs on a side stream, concurrently with the transforms;
+// it joins before the step-size stage and the update, the two readers and
+// writers of the step it may reduce (AutoStepReduce).
 cudaError_t greedy_iterate(GreedyCtx *g, const float *I0, const float *I1, const float *const h[3],
                            float *const h_out[3], const float *const hinv[3],
                            float *const hinv_out[3], int update_step, int auto_reduce,
                            cudaStream_t s) {
   AW_TRY(greedy_stage(g, kStageForcePrep, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
-  AW_TRY(greedy_stage(g, kStageEnergy, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
+  AW_TRY(cudaEventRecord(g->ev_fork, s));
+  AW_TRY(cudaStreamWaitEvent(g->aux, g->ev_fork, 0));
+  AW_TRY(greedy_stage(g, kStageEnergy, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, g->aux));
+  AW_TRY(cudaEventRecord(g->ev_join, g->aux));
   AW_TRY(greedy_stage(g, kStageXYForward, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
   AW_TRY(greedy_stage(g, kStageZSolve, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
   AW_TRY(greedy_stage(g, kStageXYInverse, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
+  AW_TRY(cudaStreamWaitEvent(s, g->ev_join, 0));
   if (update_step)
     AW_TRY(greedy_stage(g, kStageMaxNorm, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
   return greedy_stage(g, kStageUpdate, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s);

@@ -25,6 +25,8 @@ struct GreedyCtx {
   double *partials; // per-block energy sums
   int nparts;
   int sms;
+  cudaStream_t aux;  // side stream of the energy sum
+  cudaEvent_t ev_fork, ev_join;
   char *scalars;    // step | count | maxbits
   unsigned *maxbits;
   GreedyDevState st;
