@@ -70,6 +70,7 @@ SIGNATURES = {
     "aw_atlas_iterate": ([_fp, _i, _i, _fp], _i),
     "aw_atlas_get_step": ([_fp, _i, _fp], _i),
     "aw_atlas_get_energies": ([_fp, _i, _fp, _i, _fp], _i),
+    "aw_ldmm_use_orig_gradient_calc": ([_fp, _i], _i),
     "aw_ldmm_create": ([_i] * 3 + [_d] * 3 + [_f] * 3 + [_i, _f, _f, _fp], _i),
     "aw_ldmm_destroy": ([_fp], _i),
     "aw_ldmm_set_step": ([_fp, _f], _i),

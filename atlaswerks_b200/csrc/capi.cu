@@ -613,6 +613,15 @@ int aw_ldmm_destroy(aw_ldmm_t l) {
   return 0;
 }
 
+int aw_ldmm_use_orig_gradient_calc(aw_ldmm_t l, int on) {
+  if (!l) return fail("aw_ldmm_use_orig_gradient_calc: null handle");
+  AW_CUDA(cudaDeviceSynchronize(), "aw_ldmm_use_orig_gradient_calc (pending work)");
+  if (aw::ldmm_set_orig(&l->ctx, on)) return fail("aw_ldmm_use_orig_gradient_calc: device allocation failed");
+  for (auto &kv : l->graphs) cudaGraphExecDestroy(kv.second.second);
+  l->graphs.clear();  // captured iterations belong to the other variant
+  return 0;
+}
+
 int aw_ldmm_set_step(aw_ldmm_t l, float step) {
   if (!l) return fail("aw_ldmm_set_step: null handle");
   AW_CUDA(cudaMemcpy(l->ctx.step, &step, sizeof(float), cudaMemcpyHostToDevice),

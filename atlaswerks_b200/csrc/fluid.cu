@@ -347,6 +347,14 @@ cudaError_t fluid_forward_force(const FluidPlan &p, const float *G, const float 
   return cudaGetLastError();
 }
 
+cudaError_t fluid_forward_force_jac(const FluidPlan &p, const float *G, const float *A,
+                                    const float *B, cudaStream_t s) {
+  const SrcForce src = make_force(G, A, 2, p.sp, B);
+  if (p.fast) return fast_xy_forward(p, src, s);
+  k_fft_xy_fwd<SrcForce><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, src);
+  return cudaGetLastError();
+}
+
 cudaError_t fluid_solve(const FluidPlan &p, int inverse, cudaStream_t s) {
   if (p.fast) return fast_z_solve(p, inverse, s);
   const long ncols = (long)p.d.ny * p.nxh;

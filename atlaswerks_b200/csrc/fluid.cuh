@@ -53,15 +53,18 @@ struct SrcField {
   }
 };
 
-// body force f_c = d/dc(G) * M, with M = A - G (greedy: G = I0(h), A = I1)
-// or M = A (LDMM: G = J0_{t-1}, A = splatted residual). The gradient is
+// body force f_c = d/dc(G) * M, with M = A - G (mode 1, greedy: G = I0(h),
+// A = I1), M = A (mode 0, LDMM IterateNew: G = J0_{t-1}, A = splatted
+// residual) or M = (G - A) * B (mode 2, LDMM IterateOrig: G = I0(h),
+// A = JT_t, B = JacDet_t; LDMMIteratorCPU.cxx:447-452). The gradient is
 // Array3DUtils::computeGradient with wrap = false (Array3DUtils.txx:783-900):
 // central differences / (2 sp), one-sided at the borders, the float
 // difference divided in double.
 struct SrcForce {
   const float *G;
   const float *A;
-  int diff;
+  const float *B;
+  int mode;
   DivD c2[3], c1[3];  // 2 sp and sp per axis
   AW_D float value(int comp, int x, int y, int z, const Dims &d) const {
     const long i = d.idx(x, y, z);
@@ -81,15 +84,17 @@ struct SrcForce {
       grad = __double2float_rn(ddiv((double)fsub(g0, __ldg(G + i - stride)), c1[comp]));
     }
     const float a = __ldg(A + i);
-    const float m = diff ? -fsub(g0, a) : a;
+    const float m = mode == 0 ? a : (mode == 1 ? -fsub(g0, a) : fmul(fsub(g0, a), __ldg(B + i)));
     return fmul(grad, m);
   }
 };
-inline SrcForce make_force(const float *G, const float *A, int diff, const Spacing &sp) {
+inline SrcForce make_force(const float *G, const float *A, int mode, const Spacing &sp,
+                           const float *B = nullptr) {
   SrcForce f;
   f.G = G;
   f.A = A;
-  f.diff = diff;
+  f.B = B;
+  f.mode = mode;
   const double s[3] = {sp.x, sp.y, sp.z};
   for (int c = 0; c < 3; ++c) {
     f.c2[c] = make_div(2.0 * s[c]);
@@ -129,6 +134,9 @@ cudaError_t fluid_forward_field(const FluidPlan &p, const float *fx, const float
                                 const float *fz, cudaStream_t s);
 cudaError_t fluid_forward_force(const FluidPlan &p, const float *G, const float *A, int diff,
                                 cudaStream_t s);
+// force (G - A) * B * grad G (mode 2)
+cudaError_t fluid_forward_force_jac(const FluidPlan &p, const float *G, const float *A,
+                                    const float *B, cudaStream_t s);
 cudaError_t fluid_solve(const FluidPlan &p, int inverse, cudaStream_t s);
 cudaError_t fluid_inverse_store(const FluidPlan &p, float *ox, float *oy, float *oz,
                                 cudaStream_t s);

@@ -34,7 +34,9 @@ __global__ void __launch_bounds__(kRowThreads)
 }
 
 // h_out(x) = h_in(x - v(x)/sp) [PARTIAL_ID]; J(x) = I0(h_out(x))
-// (composeHVInv + apply, LDMMIteratorCPU.cxx:549-554)
+// (composeHVInv + apply, LDMMIteratorCPU.cxx:549-554); with PLUS,
+// h_in(x + v(x)/sp) (composeHV, IterateOrig's backward sweep :397-405)
+template <bool PLUS>
 __global__ void __launch_bounds__(kRowThreads)
     k_forward_step(const float *__restrict__ hx, const float *__restrict__ hy,
                    const float *__restrict__ hz, const float *__restrict__ vx,
@@ -44,15 +46,81 @@ __global__ void __launch_bounds__(kRowThreads)
   Voxel vox;
   if (!voxel_of(d, vox)) return;
   const long i = vox.i;
-  const float px = fsub(__int2float_rn(vox.x), fdiv(vx[i], (float)sp.x));
-  const float py = fsub(__int2float_rn(vox.y), fdiv(vy[i], (float)sp.y));
-  const float pz = fsub(__int2float_rn(vox.z), fdiv(vz[i], (float)sp.z));
+  const float ux = fdiv(vx[i], (float)sp.x), uy = fdiv(vy[i], (float)sp.y),
+              uz = fdiv(vz[i], (float)sp.z);
+  const float px = PLUS ? fadd(__int2float_rn(vox.x), ux) : fsub(__int2float_rn(vox.x), ux);
+  const float py = PLUS ? fadd(__int2float_rn(vox.y), uy) : fsub(__int2float_rn(vox.y), uy);
+  const float pz = PLUS ? fadd(__int2float_rn(vox.z), uz) : fsub(__int2float_rn(vox.z), uz);
   float a, b, c;
   trilerp_vector(hx, hy, hz, d, px, py, pz, BG_PARTIAL_ID, 1.0f, a, b, c);
   ox[i] = a;
   oy[i] = b;
   oz[i] = c;
-  J[i] = trilerp_scalar(I0, d, (double)a, (double)b, (double)c, 0.0f);
+  if (J) J[i] = trilerp_scalar(I0, d, (double)a, (double)b, (double)c, 0.0f);
+}
+
+// float component c of IterateOrig's world-coordinate map x*sp + v
+// (setToIdentity, scale by the float spacing, pointwiseAdd v:
+// LDMMIteratorCPU.cxx:409-414)
+AW_D float world(const float *__restrict__ vc, long i, int coord, float spc) {
+  return fadd(fmul(__int2float_rn(coord), spc), __ldg(vc + i));
+}
+
+// d/d(axis) of component c of the world map at voxel (x,y,z): computeGradient
+// with wrap = false (Array3DUtils.txx:783-900), as SrcForce forms it
+AW_D float world_grad(const float *__restrict__ vc, int c, int axis, int x, int y, int z,
+                      const Dims &d, float spc, const DivD &c2, const DivD &c1) {
+  const int p[3] = {x, y, z};
+  const int n = axis == 0 ? d.nx : (axis == 1 ? d.ny : d.nz);
+  const long st = axis == 0 ? 1 : (axis == 1 ? (long)d.nx : (long)d.nx * d.ny);
+  const long i = d.idx(x, y, z);
+  const int pos = p[axis];
+  const int cc = p[c];  // the coordinate that component c adds to v
+  // the neighbours' own coordinate along c moves only when axis == c
+  const int dlo = (axis == c) ? -1 : 0, dhi = (axis == c) ? 1 : 0;
+  if (pos > 0 && pos < n - 1)
+    return __double2float_rn(ddiv((double)fsub(world(vc, i + st, cc + dhi, spc),
+                                                world(vc, i - st, cc + dlo, spc)), c2));
+  if (pos == 0)
+    return __double2float_rn(ddiv((double)fsub(world(vc, i + st, cc + dhi, spc),
+                                                world(vc, i, cc, spc)), c1));
+  return __double2float_rn(ddiv((double)fsub(world(vc, i, cc, spc),
+                                              world(vc, i - st, cc + dlo, spc)), c1));
+}
+
+// JacDet_t = (t < T-1 ? JacDet_{t+1}(x + v_t/sp) : 1) * |D(x*sp + v_t)|
+// (HField3DUtils::jacobian + applyU + pointwiseMultiplyBy,
+// LDMMIteratorCPU.cxx:416-427; the determinant of HField3DUtils.txx:2408-2419)
+__global__ void __launch_bounds__(kRowThreads)
+    k_jacdet(const float *__restrict__ vx, const float *__restrict__ vy,
+             const float *__restrict__ vz, const float *__restrict__ next,
+             float *__restrict__ out, Dims d, Spacing sp, DivD a2, DivD b2, DivD e2, DivD a1,
+             DivD b1, DivD e1) {
+  Voxel vox;
+  if (!voxel_of(d, vox)) return;
+  const int x = vox.x, y = vox.y, z = vox.z;
+  const float s[3] = {(float)sp.x, (float)sp.y, (float)sp.z};
+  const DivD c2[3] = {a2, b2, e2}, c1[3] = {a1, b1, e1};
+  const float *vc[3] = {vx, vy, vz};
+  float g[3][3];  // g[c][axis]
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) g[c][a] = world_grad(vc[c], c, a, x, y, z, d, s[c], c2[a], c1[a]);
+  const float t1 = fmul(g[0][0], fsub(fmul(g[1][1], g[2][2]), fmul(g[1][2], g[2][1])));
+  const float t2 = fmul(g[0][1], fsub(fmul(g[1][0], g[2][2]), fmul(g[1][2], g[2][0])));
+  const float t3 = fmul(g[0][2], fsub(fmul(g[1][0], g[2][1]), fmul(g[1][1], g[2][0])));
+  const float jac = fadd(fsub(t1, t2), t3);
+  const long i = vox.i;
+  if (next) {
+    // applyU: coord = v/sp + (x,y,z), default scalar background 0
+    const float px = fadd(fdiv(vx[i], s[0]), __int2float_rn(x));
+    const float py = fadd(fdiv(vy[i], s[1]), __int2float_rn(y));
+    const float pz = fadd(fdiv(vz[i], s[2]), __int2float_rn(z));
+    out[i] = fmul(trilerp_scalar(next, d, (double)px, (double)py, (double)pz, 0.0f), jac);
+  } else {
+    out[i] = jac;
+  }
 }
 
 __global__ void __launch_bounds__(kRowThreads)
@@ -161,14 +229,18 @@ int ldmm_create(LdmmCtx *c, int nx, int ny, int nz, double spx, double spy, doub
 void ldmm_destroy(LdmmCtx *c) {
   fluid_plan_destroy(&c->plan);
   void *ptrs[] = {c->J0, c->hbuf, c->diff, c->S, c->u, c->splat_scratch, c->partials, c->energy,
-                  c->scalars};
+                  c->scalars, c->JT, c->JD};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   std::memset(c, 0, sizeof(*c));
 }
 
+cudaError_t ldmm_iterate_orig(LdmmCtx *c, const float *I0, const float *I1, float *v,
+                              int update_step, cudaStream_t s);
+
 cudaError_t ldmm_iterate(LdmmCtx *c, const float *I0, const float *I1, float *v, int update_step,
                          cudaStream_t s) {
+  if (c->orig) return ldmm_iterate_orig(c, I0, I1, v, update_step, s);
   const Dims d = c->d;
   const long n = d.n();
   const int T = c->T;
@@ -180,7 +252,7 @@ cudaError_t ldmm_iterate(LdmmCtx *c, const float *I0, const float *I1, float *v,
   int cur = 0;
   for (int i = 0; i < T; ++i) {
     float *vi = v + (long)i * 3 * n;
-    k_forward_step<<<row_grid(d), kRowThreads, 0, s>>>(
+    k_forward_step<false><<<row_grid(d), kRowThreads, 0, s>>>(
         comp(H[cur], 0), comp(H[cur], 1), comp(H[cur], 2), comp(vi, 0), comp(vi, 1), comp(vi, 2),
         comp(H[1 - cur], 0), comp(H[1 - cur], 1), comp(H[1 - cur], 2), I0, c->J0 + (long)i * n,
         d, c->sp);
@@ -230,6 +302,85 @@ cudaError_t ldmm_iterate(LdmmCtx *c, const float *I0, const float *I1, float *v,
     AW_TRY(cudaGetLastError());
   }
   return cudaSuccess;
+}
+
+int ldmm_set_orig(LdmmCtx *c, int on) {
+  c->orig = on ? 1 : 0;
+  if (c->orig && !c->JT) {
+    const size_t bytes = sizeof(float) * (size_t)c->T * c->d.n();
+    if (cudaMalloc(&c->JT, bytes) != cudaSuccess || cudaMalloc(&c->JD, bytes) != cudaSuccess)
+      return 3;
+  }
+  return 0;
+}
+
+// LDMMIteratorCPU::IterateOrig (LDMM/LDMMIteratorCPU.cxx:377-527)
+cudaError_t ldmm_iterate_orig(LdmmCtx *c, const float *I0, const float *I1, float *v,
+                              int update_step, cudaStream_t s) {
+  const Dims d = c->d;
+  const long n = d.n();
+  const int T = c->T;
+  float *H[2] = {c->hbuf, c->hbuf + 3 * n};
+  auto comp = [&](float *base, int k) { return base + k * n; };
+  const DivD a2 = make_div(2.0 * c->sp.x), b2 = make_div(2.0 * c->sp.y), e2 = make_div(2.0 * c->sp.z);
+  const DivD a1 = make_div(c->sp.x), b1 = make_div(c->sp.y), e1 = make_div(c->sp.z);
+  // backward sweep: h <- h(x + v_t/sp), JT_t = I1(h), Jacobian transport
+  k_identity<<<row_grid(d), kRowThreads, 0, s>>>(comp(H[0], 0), comp(H[0], 1), comp(H[0], 2), d);
+  AW_TRY(cudaGetLastError());
+  int cur = 0;
+  for (int t = T - 1; t >= 0; --t) {
+    float *vt = v + (long)t * 3 * n;
+    k_forward_step<true><<<row_grid(d), kRowThreads, 0, s>>>(
+        comp(H[cur], 0), comp(H[cur], 1), comp(H[cur], 2), comp(vt, 0), comp(vt, 1), comp(vt, 2),
+        comp(H[1 - cur], 0), comp(H[1 - cur], 1), comp(H[1 - cur], 2), I1, c->JT + (long)t * n,
+        d, c->sp);
+    AW_TRY(cudaGetLastError());
+    cur = 1 - cur;
+    k_jacdet<<<row_grid(d), kRowThreads, 0, s>>>(comp(vt, 0), comp(vt, 1), comp(vt, 2),
+                                                 t == T - 1 ? nullptr : c->JD + (long)(t + 1) * n,
+                                                 c->JD + (long)t * n, d, c->sp, a2, b2, e2, a1, b1,
+                                                 e1);
+    AW_TRY(cudaGetLastError());
+  }
+  if (update_step) AW_TRY(cudaMemsetAsync(c->maxbits, 0, sizeof(unsigned), s));
+  // forward sweep: S = I0(h), force grad(S) * (S - JT_t) * JacDet_t, K, update,
+  // h <- h(x - v_t/sp) with the updated v_t, and S for the next t
+  k_identity<<<row_grid(d), kRowThreads, 0, s>>>(comp(H[0], 0), comp(H[0], 1), comp(H[0], 2), d);
+  AW_TRY(cudaGetLastError());
+  cur = 0;
+  float *Sb = c->S;
+  for (int t = 0; t < T; ++t) {
+    float *vt = v + (long)t * 3 * n;
+    const float *Sg = t == 0 ? I0 : Sb;
+    AW_TRY(fluid_forward_force_jac(c->plan, Sg, c->JT + (long)t * n, c->JD + (long)t * n, s));
+    AW_TRY(fluid_solve(c->plan, 1, s));
+    if (update_step) {
+      AW_TRY(fluid_inverse_store(c->plan, comp(c->u, 0), comp(c->u, 1), comp(c->u, 2), s));
+      int sms = 148;
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->plan.device);
+      k_max_disp<<<sms * 4, 256, 0, s>>>(comp(vt, 0), comp(vt, 1), comp(vt, 2), comp(c->u, 0),
+                                         comp(c->u, 1), comp(c->u, 2), n, c->sigma, c->maxbits);
+      AW_TRY(cudaGetLastError());
+    } else {
+      AW_TRY(fluid_inverse_axpby(c->plan, comp(vt, 0), comp(vt, 1), comp(vt, 2), c->step,
+                                 c->sigma, s));
+    }
+    k_forward_step<false><<<row_grid(d), kRowThreads, 0, s>>>(
+        comp(H[cur], 0), comp(H[cur], 1), comp(H[cur], 2), comp(vt, 0), comp(vt, 1), comp(vt, 2),
+        comp(H[1 - cur], 0), comp(H[1 - cur], 1), comp(H[1 - cur], 2), I0, Sb, d, c->sp);
+    AW_TRY(cudaGetLastError());
+    cur = 1 - cur;
+  }
+  if (update_step) {
+    k_step_from_max<<<1, 1, 0, s>>>(c->maxbits, c->max_pert, c->step);
+    return cudaGetLastError();
+  }
+  // image energy of the updated path: sp^3 * sum (I0(h) - I1)^2
+  k_residual<<<row_grid(d), kRowThreads, 0, s>>>(Sb, I1, c->diff, c->partials, d);
+  AW_TRY(cudaGetLastError());
+  const double spprod = c->sp.x * c->sp.y * c->sp.z;
+  k_record_energy<<<1, 256, 0, s>>>(c->partials, c->nparts, spprod, c->energy, c->count, c->cap);
+  return cudaGetLastError();
 }
 
 }  // namespace aw

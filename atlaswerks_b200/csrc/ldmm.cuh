@@ -28,13 +28,19 @@ struct LdmmCtx {
   unsigned *maxbits;
   double *energy;   // image-energy history ring
   int cap;
+  int orig;         // IterateOrig (Jacobian path) instead of IterateNew
+  float *JT;        // T x N: I1 pulled back to each time point (IterateOrig)
+  float *JD;        // T x N: transported Jacobian determinants (IterateOrig)
 };
 
 int ldmm_create(LdmmCtx *c, int nx, int ny, int nz, double spx, double spy, double spz,
                 float alpha, float beta, float gamma, int T, float sigma, float max_pert);
 void ldmm_destroy(LdmmCtx *c);
-// One IterateNew; v is [T][3][N]. update_step: compute the step from
-// max |2v - (2/sigma^2) K f| and leave v unchanged.
+// LDMMIteratorCPU's UseOrigGradientCalc: 1 selects IterateOrig (the
+// reference's default), 0 IterateNew; allocates the IterateOrig buffers
+int ldmm_set_orig(LdmmCtx *c, int on);
+// One iteration (IterateNew or IterateOrig); v is [T][3][N]. update_step:
+// compute the step from max |2v - (2/sigma^2) K f| and leave v unchanged.
 cudaError_t ldmm_iterate(LdmmCtx *c, const float *I0, const float *I1, float *v, int update_step,
                          cudaStream_t s);
 

@@ -62,6 +62,7 @@ class LDMMIteratorB200:
         self.T = int(n_time_steps)
         self._h = ctypes.c_void_p()
         self._update_step = False
+        self._orig = False
 
     def SetScaleLevel(self, size: Sequence[int], spacing: Sequence[float],
                       param: LDMMIteratorParam):
@@ -76,6 +77,15 @@ class LDMMIteratorB200:
                                         ctypes.byref(self._h)))
         self.param = param
         self.SetStepSize(param.StepSize)
+        if self._orig:
+            check(_lib.lib().aw_ldmm_use_orig_gradient_calc(self._h, 1))
+
+    def SetUseOrigGradientCalc(self, on: bool):
+        """LDMMIteratorCPU's mUseOrigGradientCalc: IterateOrig (Jacobian
+        transport) instead of IterateNew (splatting)."""
+        self._orig = bool(on)
+        if self._h:
+            check(_lib.lib().aw_ldmm_use_orig_gradient_calc(self._h, int(self._orig)))
 
     def UpdateStepSizeNextIteration(self):
         self._update_step = True
@@ -122,10 +132,12 @@ class LDMMIteratorB200:
 
 def ldmm_register(I0: torch.Tensor, I1: torch.Tensor, n_time_steps: int, n_iters: int,
                   spacing=(1.0, 1.0, 1.0), sigma=0.1, step=0.005, adaptive=False, max_pert=0.1,
-                  alpha=0.01, beta=0.01, gamma=0.001):
-    """LDMMWarp at one scale level (LDMM/LDMMWarp.txx:71-130)."""
+                  alpha=0.01, beta=0.01, gamma=0.001, orig_gradient=False):
+    """LDMMWarp at one scale level (LDMM/LDMMWarp.txx:71-130); orig_gradient
+    selects IterateOrig (the reference's default) over IterateNew."""
     nz, ny, nx = I0.shape
     it = LDMMIteratorB200((nx, ny, nz), spacing=spacing, n_time_steps=n_time_steps)
+    it.SetUseOrigGradientCalc(orig_gradient)
     p = LDMMIteratorParam(DiffOperParam(alpha, beta, gamma), sigma, step, adaptive, max_pert)
     it.SetScaleLevel((nx, ny, nz), spacing, p)
     data = LDMMDeformationDataB200(I0, I1, n_time_steps, spacing)

@@ -234,6 +234,11 @@ int aw_ldmm_create(int nx, int ny, int nz, double spx, double spy, double spz, f
                    float beta, float gamma, int n_time_steps, float sigma, float max_pert,
                    aw_ldmm_t *out);
 int aw_ldmm_destroy(aw_ldmm_t l);
+/* LDMMIteratorCPU's UseOrigGradientCalc (LDMM/LDMMIteratorCPU.cxx:33,
+ * 369-527): 1 = IterateOrig, the Jacobian-transport gradient (the
+ * reference's default), 0 = IterateNew, the splatting gradient (this
+ * handle's default). Allocates 2 T N floats for IterateOrig. */
+int aw_ldmm_use_orig_gradient_calc(aw_ldmm_t l, int on);
 /* LDMMDeformationData::StepSize(s) / StepSize(); get synchronises. */
 int aw_ldmm_set_step(aw_ldmm_t l, float step);
 int aw_ldmm_get_step(aw_ldmm_t l, float *step);

@@ -89,6 +89,7 @@ class Oracle:
         L.aw_oracle_max_norm.restype = ctypes.c_float
         L.aw_oracle_ldmm_iterate.restype = ctypes.c_double
         L.aw_oracle_atlas_iterate.restype = ctypes.c_double
+        L.aw_oracle_ldmm_iterate_orig.restype = ctypes.c_double
 
     # --- interpolation family -------------------------------------------------
     def apply(self, img, h, bg=0.0):
@@ -216,6 +217,25 @@ class Oracle:
                                             *_shape(I0), *map(_dbl, sp), _dbl(alpha), _dbl(beta),
                                             _dbl(gamma), ctypes.c_float(sigma), ctypes.byref(st),
                                             _i(int(update_step)), ctypes.c_float(max_pert))
+        return float(e), float(st.value)
+
+    def jacobian(self, v, sp=(1.0, 1.0, 1.0)):
+        """|D(x*sp + v)| (HField3DUtils::jacobian of IterateOrig's map)."""
+        out = np.empty(v.shape[1:], np.float32)
+        self.lib.aw_oracle_jacobian(_fp(v[0]), _fp(v[1]), _fp(v[2]), _fp(out), *_shape(v),
+                                    *map(_dbl, sp))
+        return out
+
+    def ldmm_iterate_orig(self, I0, I1, v, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01,
+                          gamma=0.001, sigma=0.1, step=0.005, update_step=False, max_pert=0.1):
+        """One LDMMIteratorCPU::IterateOrig; v updated in place. Returns
+        (image energy after the update, step)."""
+        assert v.dtype == np.float32 and v.flags.c_contiguous
+        st = ctypes.c_float(step)
+        e = self.lib.aw_oracle_ldmm_iterate_orig(
+            _fp(I0), _fp(I1), v.ctypes.data_as(_f), _i(v.shape[0]), *_shape(I0), *map(_dbl, sp),
+            _dbl(alpha), _dbl(beta), _dbl(gamma), ctypes.c_float(sigma), ctypes.byref(st),
+            _i(int(update_step)), ctypes.c_float(max_pert))
         return float(e), float(st.value)
 
     def greedy_run(self, I0, I1, iters, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01, gamma=0.001,

@@ -636,6 +636,138 @@ double aw_oracle_ldmm_iterate(const float *I0, const float *I1, float *v, int T,
   return e;
 }
 
+/* |D(x*sp + v)|: HField3DUtils::jacobian (UtilitiesDataTypes/HField3DUtils.txx:
+ * 2374-2420) of the world-coordinate map that LDMMIteratorCPU::IterateOrig
+ * forms (LDMM/LDMMIteratorCPU.cxx:409-417: identity scaled by the float
+ * spacing, plus v): float components, gradients by computeGradient
+ * (wrap = false), the determinant expanded along its first row in float. */
+void aw_oracle_jacobian(const float *vx, const float *vy, const float *vz, float *jac, int nx,
+                        int ny, int nz, double spx, double spy, double spz) {
+  const long n = (long)nx * ny * nz;
+  float *w = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *g = (float *)malloc(sizeof(float) * (size_t)(9 * n));
+  const float sx = (float)spx, sy = (float)spy, sz = (float)spz;
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const long i = IDX(x, y, z);
+        w[i] = (float)x * sx + vx[i];
+        w[n + i] = (float)y * sy + vy[i];
+        w[2 * n + i] = (float)z * sz + vz[i];
+      }
+  for (int c = 0; c < 3; ++c)
+    aw_oracle_gradient(w + c * n, g + 3 * c * n, g + (3 * c + 1) * n, g + (3 * c + 2) * n, nx, ny,
+                       nz, spx, spy, spz, 0);
+  for (long i = 0; i < n; ++i) {
+    const float ax = g[i], ay = g[n + i], az = g[2 * n + i];           /* grad h1 */
+    const float bx = g[3 * n + i], by = g[4 * n + i], bz = g[5 * n + i]; /* grad h2 */
+    const float cx = g[6 * n + i], cy = g[7 * n + i], cz = g[8 * n + i]; /* grad h3 */
+    const float t1 = ax * (by * cz - bz * cy);
+    const float t2 = ay * (bx * cz - bz * cx);
+    const float t3 = az * (bx * cy - by * cx);
+    jac[i] = t1 - t2 + t3;
+  }
+  free(w);
+  free(g);
+}
+
+/* ------------------------------------------------------------------------
+ * LDMM relaxation, LDMMIteratorCPU::IterateOrig (LDMM/LDMMIteratorCPU.cxx:
+ * 377-527): a backward sweep t = T-1..0 composing h <- h(x + v_t/sp)
+ * [PARTIAL_ID], JT_t = I1(h) and the Jacobian transport
+ * JacDet_t = JacDet_{t+1}(x + v_t/sp) * |D(x + v_t)| (applyU); then a
+ * forward sweep t = 0..T-1 with S = I0 (t = 0) or I0(h), the body force
+ * grad(S) * ((S - JT_t) * JacDet_t), K, the velocity update (or, with
+ * update_step, the max of |(-2/sigma^2) K f + 2 v_t|), and
+ * h <- h(x - v_t/sp) [PARTIAL_ID] with the updated v_t. Returns the image
+ * energy sp^3 * sum (I0(h) - I1)^2 after the sweep (0 with update_step).
+ * ---------------------------------------------------------------------- */
+double aw_oracle_ldmm_iterate_orig(const float *I0, const float *I1, float *v, int T, int nx,
+                                   int ny, int nz, double spx, double spy, double spz,
+                                   double alpha, double beta, double gamma, float sigma,
+                                   float *step, int update_step, float max_pert) {
+  const long n = (long)nx * ny * nz;
+  float *h = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *o = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *JT = (float *)malloc(sizeof(float) * (size_t)(T * n));
+  float *JD = (float *)malloc(sizeof(float) * (size_t)(T * n));
+  float *S = (float *)malloc(sizeof(float) * (size_t)n);
+  float *jac = (float *)malloc(sizeof(float) * (size_t)n);
+  float *f = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  aw_oracle_identity(h, h + n, h + 2 * n, nx, ny, nz);
+  for (int t = T - 1; t >= 0; --t) {
+    float *vt = v + (long)t * 3 * n;
+    aw_oracle_compose_hv(h, h + n, h + 2 * n, vt, vt + n, vt + 2 * n, o, o + n, o + 2 * n, nx, ny,
+                         nz, spx, spy, spz, 1, AW_BG_PARTIAL_ID);
+    memcpy(h, o, sizeof(float) * (size_t)(3 * n));
+    aw_oracle_apply(I1, h, h + n, h + 2 * n, JT + (long)t * n, nx, ny, nz, 0.0f);
+    aw_oracle_jacobian(vt, vt + n, vt + 2 * n, jac, nx, ny, nz, spx, spy, spz);
+    float *jd = JD + (long)t * n;
+    if (t == T - 1) {
+      memcpy(jd, jac, sizeof(float) * (size_t)n);
+    } else {
+      aw_oracle_apply_u(JD + (long)(t + 1) * n, vt, vt + n, vt + 2 * n, jd, nx, ny, nz, spx, spy,
+                        spz, 0.0f);
+      for (long k = 0; k < n; ++k) jd[k] *= jac[k];
+    }
+  }
+  const float vfac = 1.f - 2 * *step;
+  const float ufac = 2 * *step / (sigma * sigma);
+  float total_max = 0.f;
+  aw_oracle_identity(h, h + n, h + 2 * n, nx, ny, nz);
+  for (int t = 0; t < T; ++t) {
+    float *vt = v + (long)t * 3 * n;
+    if (t == 0)
+      memcpy(S, I0, sizeof(float) * (size_t)n);
+    else
+      aw_oracle_apply(I0, h, h + n, h + 2 * n, S, nx, ny, nz, 0.0f);
+    aw_oracle_gradient(S, f, f + n, f + 2 * n, nx, ny, nz, spx, spy, spz, 0);
+    const float *jt = JT + (long)t * n, *jd = JD + (long)t * n;
+    for (long k = 0; k < n; ++k) {
+      float m = S[k] - jt[k];
+      m = m * jd[k];
+      f[k] *= m;
+      f[n + k] *= m;
+      f[2 * n + k] *= m;
+    }
+    aw_oracle_fluid_apply(f, f + n, f + 2 * n, nx, ny, nz, spx, spy, spz, alpha, beta, gamma, 1);
+    if (update_step) {
+      const float b = -2.0f / (sigma * sigma);
+      for (long k = 0; k < n; ++k) {
+        const float x = b * f[k] + 2.0f * vt[k];
+        const float y = b * f[n + k] + 2.0f * vt[n + k];
+        const float zz = b * f[2 * n + k] + 2.0f * vt[2 * n + k];
+        const float len = (float)sqrt((double)(x * x + y * y + zz * zz));
+        if (len > total_max) total_max = len;
+      }
+    } else {
+      for (long k = 0; k < 3 * n; ++k) vt[k] = vfac * vt[k] + ufac * f[k];
+    }
+    aw_oracle_compose_hv(h, h + n, h + 2 * n, vt, vt + n, vt + 2 * n, o, o + n, o + 2 * n, nx, ny,
+                         nz, spx, spy, spz, -1, AW_BG_PARTIAL_ID);
+    memcpy(h, o, sizeof(float) * (size_t)(3 * n));
+  }
+  double e = 0.0;
+  if (update_step) {
+    *step = max_pert / total_max;
+  } else {
+    aw_oracle_apply(I0, h, h + n, h + 2 * n, S, nx, ny, nz, 0.0f);
+    for (long k = 0; k < n; ++k) {
+      const float r = S[k] - I1[k];
+      e += (double)r * (double)r;
+    }
+    e *= spx * spy * spz;
+  }
+  free(h);
+  free(o);
+  free(JT);
+  free(JD);
+  free(S);
+  free(jac);
+  free(f);
+  return e;
+}
+
 /* ------------------------------------------------------------------------
  * Multiscale (Algorithms/Common/MultiscaleManager.cxx:301-366).
  * ---------------------------------------------------------------------- */

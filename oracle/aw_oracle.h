@@ -65,6 +65,13 @@ double aw_oracle_ldmm_iterate(const float *I0, const float *I1, float *v, int T,
                               double beta, double gamma, float sigma, float *step,
                               int update_step, float max_pert);
 
+void aw_oracle_jacobian(const float *vx, const float *vy, const float *vz, float *jac, int nx,
+                        int ny, int nz, double spx, double spy, double spz);
+double aw_oracle_ldmm_iterate_orig(const float *I0, const float *I1, float *v, int T, int nx,
+                                   int ny, int nz, double spx, double spy, double spz,
+                                   double alpha, double beta, double gamma, float sigma,
+                                   float *step, int update_step, float max_pert);
+
 void aw_oracle_gauss_blur(const float *in, float *out, int nx, int ny, int nz, float sx, float sy,
                           float sz, int kx, int ky, int kz);
 void aw_oracle_downsample(const float *in, int nx, int ny, int nz, double spx, double spy,

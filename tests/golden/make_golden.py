@@ -88,6 +88,16 @@ def main():
     save("ldmm_16_T4", I0=I0, I1=I1, v=vv, energies=en, step=np.float32(stp), v_adaptive=va,
          energies_adaptive=ea, step_adaptive=np.float32(sa))
 
+    # LDMM IterateOrig (Jacobian transport, the reference's default), 16x14x12,
+    # T = 4, anisotropic spacing; fixed and adaptive steps
+    I0, I1 = small_pair((12, 14, 16), 10)
+    sp = (1.5, 0.75, 1.25)
+    vo, eo, so = ref.ldmm_run(I0, I1, 4, 6, sp=sp, sigma=1.0, step=0.01, use_new=False)
+    voa, eoa, soa = ref.ldmm_run(I0, I1, 4, 4, sp=sp, sigma=1.0, step=0.01, adaptive=True,
+                                 max_pert=0.2, use_new=False)
+    save("ldmm_orig_16x14x12_T4", I0=I0, I1=I1, sp=np.array(sp), v=vo, energies=eo,
+         step=np.float32(so), v_adaptive=voa, energies_adaptive=eoa, step_adaptive=np.float32(soa))
+
     # greedy atlas, equal grids 16^3, 3 subjects, mean every iteration and every 2nd
     imgs = atlas_subjects(3, 13, sizes=(16,), n_blobs=6, umax=2.0)
     w = np.array([0.25, 0.35, 0.4], np.float32)

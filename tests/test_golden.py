@@ -92,6 +92,25 @@ def test_ldmm_iterate_new(oracle, adaptive):
     assert abs(step - float(z["step" + sfx])) <= 1e-6 * float(z["step" + sfx])
 
 
+@pytest.mark.parametrize("adaptive", [False, True])
+def test_ldmm_iterate_orig(oracle, adaptive):
+    z = load("ldmm_orig_16x14x12_T4")
+    sfx = "_adaptive" if adaptive else ""
+    want_v, want_e, sp = z["v" + sfx], z["energies" + sfx], tuple(z["sp"])
+    v = np.zeros_like(want_v)
+    step, en = 0.01, []
+    if adaptive:
+        _, step = oracle.ldmm_iterate_orig(z["I0"], z["I1"], v, sp, sigma=1.0, step=step,
+                                           update_step=True, max_pert=0.2)
+    for it in range(len(want_e)):
+        e, step = oracle.ldmm_iterate_orig(z["I0"], z["I1"], v, sp, sigma=1.0, step=step)
+        en.append(e)
+    assert np.abs(v - want_v).max() <= 1e-5 * np.abs(want_v).max()
+    # the reference's energy: float sum of squares
+    assert np.allclose(en, want_e, rtol=1e-5)
+    assert abs(step - float(z["step" + sfx])) <= 1e-6 * float(z["step" + sfx])
+
+
 @pytest.mark.parametrize("period", [1, 2])
 def test_atlas(oracle, period):
     z = load("atlas_16x3")

@@ -105,6 +105,19 @@ def test_ldmm_iterate_new(adaptive):
     assert abs(step - float(z["step" + sfx])) <= 1e-5 * float(z["step" + sfx])
 
 
+@pytest.mark.parametrize("adaptive", [False, True])
+def test_ldmm_iterate_orig(adaptive):
+    z = load("ldmm_orig_16x14x12_T4")
+    sfx = "_adaptive" if adaptive else ""
+    want_v, want_e = z["v" + sfx], z["energies" + sfx]
+    v, en, step = ldmm_register(cu(z["I0"]), cu(z["I1"]), 4, len(want_e), tuple(z["sp"]),
+                                sigma=1.0, step=0.01, adaptive=adaptive, max_pert=0.2,
+                                orig_gradient=True)
+    assert np.abs(host(v) - want_v).max() <= 1e-3 * np.abs(want_v).max()
+    assert np.allclose(en, want_e, rtol=1e-4)
+    assert abs(step - float(z["step" + sfx])) <= 1e-5 * float(z["step" + sfx])
+
+
 @pytest.mark.parametrize("period", [1, 2])
 def test_atlas(period):
     z = load("atlas_16x3")

@@ -139,3 +139,47 @@ def test_ldmm_register_decreases_energy():
     V, e, _ = ldmm_register(cu(I0), cu(I1), 5, 20, sigma=1.0, step=0.01)
     assert len(e) == 20
     assert e[-1] < 0.7 * e[0]
+
+
+@pytest.mark.parametrize("shape,T,sp", [((16, 16, 16), 4, (1.0, 1.0, 1.0)),
+                                        ((12, 14, 16), 3, (1.5, 0.75, 1.25)),
+                                        ((32, 32, 32), 5, (1.0, 1.0, 1.0))])
+def test_ldmm_orig_iterations_vs_oracle(oracle, shape, T, sp):
+    """IterateOrig (Jacobian transport): same bar as IterateNew."""
+    I0, I1 = greedy_pair(shape, seed=31, n_blobs=5, umax=1.5, sigma_range=(1.5, 3.0),
+                         smooth_sigma=3.0)
+    sigma, step = 1.0, 0.01
+    nz, ny, nx = shape
+    it = LDMMIteratorB200((nx, ny, nz), spacing=sp, n_time_steps=T)
+    it.SetUseOrigGradientCalc(True)
+    it.SetScaleLevel((nx, ny, nz), sp, LDMMIteratorParam(DiffOperParam(), sigma, step, False, 0.1))
+    data = LDMMDeformationDataB200(cu(I0), cu(I1), T, sp)
+    v = np.zeros((T, 3) + shape, np.float32)
+    for k in range(3):
+        e_o, _ = oracle.ldmm_iterate_orig(I0, I1, v, sp, sigma=sigma, step=step)
+        it.Iterate(data)
+        got = host(data.V)
+        err = np.abs(got - v).max() / max(np.abs(v).max(), 1e-12)
+        assert err <= 1e-4, (k, err)
+        data.V.copy_(cu(v))
+        assert abs(it.Energies()[-1] - e_o) <= 1e-5 * e_o
+
+
+def test_ldmm_orig_adaptive_step_vs_oracle(oracle):
+    shape, T = (16, 16, 16), 3
+    I0, I1 = greedy_pair(shape, seed=32, n_blobs=5, umax=1.5, sigma_range=(1.5, 3.0),
+                         smooth_sigma=3.0)
+    nz, ny, nx = shape
+    it = LDMMIteratorB200((nx, ny, nz), n_time_steps=T)
+    it.SetUseOrigGradientCalc(True)
+    it.SetScaleLevel((nx, ny, nz), (1.0, 1.0, 1.0),
+                     LDMMIteratorParam(DiffOperParam(), 1.0, 0.01, True, 0.2))
+    data = LDMMDeformationDataB200(cu(I0), cu(I1), T)
+    data.V.normal_(0, 0.05, generator=torch.Generator(device="cuda").manual_seed(4))
+    v = host(data.V).copy()
+    _, step_o = oracle.ldmm_iterate_orig(I0, I1, v, sigma=1.0, step=0.01, update_step=True,
+                                         max_pert=0.2)
+    it.UpdateStepSizeNextIteration()
+    it.Iterate(data)
+    assert abs(it.StepSize() - step_o) <= 1e-4 * step_o
+    assert np.array_equal(host(data.V), v)

@@ -79,3 +79,22 @@ def test_ldmm_adaptive_step_matches_reference(oracle, reference):
     v = np.zeros((T, 3) + shape, np.float32)
     _, so = oracle.ldmm_iterate(I0, I1, v, sigma=0.1, step=0.005, update_step=True, max_pert=0.1)
     assert abs(so - sr) <= 1e-5 * sr
+
+
+def test_ldmm_orig_iterations_match_reference(oracle, reference):
+    """IterateOrig (Jacobian transport), anisotropic spacing, against the
+    reference's LDMMIteratorCPU with UseOrigGradientCalc."""
+    shape, T = (12, 14, 16), 4
+    I0, I1 = greedy_pair(shape, 3, n_blobs=4, umax=1.5, sigma_range=(1.5, 3.0), smooth_sigma=3.0)
+    sp = (1.5, 0.75, 1.25)
+    vr, er, _ = reference.ldmm_run(I0, I1, T, 3, sp=sp, sigma=1.0, step=0.01, use_new=False)
+    v = np.zeros((T, 3) + shape, np.float32)
+    eo = [oracle.ldmm_iterate_orig(I0, I1, v, sp, sigma=1.0, step=0.01)[0] for _ in range(3)]
+    assert np.abs(v - vr).max() <= 1e-5 * np.abs(vr).max()
+    assert np.allclose(eo, er, rtol=1e-5)
+
+
+def test_jacobian_of_identity_map_is_spacing_volume(oracle):
+    v = np.zeros((3, 6, 7, 8), np.float32)
+    jac = oracle.jacobian(v, (1.5, 0.75, 1.25))
+    assert np.allclose(jac, 1.0)  # d(x*sp)/dx / sp = 1 per axis
