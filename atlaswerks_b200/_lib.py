@@ -78,6 +78,21 @@ SIGNATURES = {
     "aw_ldmm_iterate": ([_fp] * 4 + [_i, _fp], _i),
     "aw_ldmm_run": ([_fp] * 4 + [_i, _i, _fp], _i),
     "aw_ldmm_get_energies": ([_fp, _fp, _i, _fp], _i),
+    "aw_nn_conv3d_fwd": ([_fp] + [_i] * 5 + [_fp, _fp, _i, _i, _i, _fp, _fp, _fp], _i),
+    "aw_nn_conv3d_dgrad": ([_fp] + [_i] * 5 + [_fp, _i, _i, _fp, _fp, _fp], _i),
+    "aw_nn_wgrad_scratch_floats": ([_i, _i, _i, _i], ctypes.c_size_t),
+    "aw_nn_conv3d_wgrad": ([_fp, _fp] + [_i] * 8 + [_fp, _fp, _fp], _i),
+    "aw_nn_bias_grad": ([_fp, ctypes.c_long, _i, _fp, _fp], _i),
+    "aw_nn_pool": ([_fp] + [_i] * 5 + [_fp, _i, _fp, _fp, _fp], _i),
+    "aw_nn_upsample": ([_fp] + [_i] * 5 + [_fp, _i, _i, _i, _fp], _i),
+    "aw_nn_slice": ([_fp, _i, _i, _fp, _i, _i, _i, ctypes.c_long, _i, _fp], _i),
+    "aw_nn_pack_pair": ([_fp, _fp, ctypes.c_long, _fp, _fp], _i),
+    "aw_nn_mse_scratch_doubles": ([ctypes.c_long], ctypes.c_size_t),
+    "aw_nn_mse": ([_fp, _fp, ctypes.c_long, _fp, _fp, _fp, _fp], _i),
+    "aw_nn_adam": ([_fp, _fp, _fp, _fp, ctypes.c_long, _f, _f, _f, _f, _i, _fp], _i),
+    "aw_nn_weights_bf16": ([_fp, _i, _i, _i, _fp, _fp, _fp], _i),
+    "aw_nn_displacement_to_h": ([_fp, _i, _i, _i, _fp, _fp, _fp, _fp], _i),
+    "aw_nn_status": ([_fp], _i),
 }
 
 

@@ -1,0 +1,690 @@
+// nn.cu — the learned warm start's network kernels: 3D convolutions as
+// implicit GEMMs on the 5th-generation tensor cores (tcgen05, BF16 x BF16
+// -> FP32 in TMEM), forward, data gradient and weight gradient, plus the
+// elementwise layers of the encoder-decoder (average pooling, nearest
+// upsampling, skip concatenation), the MSE loss and Adam.
+//
+// Activations are BF16, channels last: [B][D][H][W][C] with C a multiple of
+// 16. Weights are BF16 [Cout][taps][Cin] (K = taps * Cin contiguous per
+// output channel) with an FP32 master copy; taps is 27 (3x3x3, zero
+// padding) or 1.
+//
+// One GEMM kernel serves the three products. A CTA owns 128 rows of D and
+// all N columns (N = the output channels, 16..256): 128 threads gather the
+// A and B tiles of one 64-deep K step into shared memory (two stages), one
+// thread issues four K=16 MMAs per step into the TMEM accumulator and
+// commits them to the stage's mbarrier, and the four warps read their 32
+// TMEM lanes back for the fused epilogue.
+//   forward  D[voxel][co]  = sum_{tap,ci} X[voxel + off(tap)][ci] W[co][tap][ci]
+//   dgrad    D[voxel][ci]  = sum_{tap,co} dY[voxel - off(tap)][co] W[co][tap][ci]
+//   wgrad    D[(tap,ci)][co] = sum_voxel X[voxel + off(tap)][ci] dY[voxel][co]
+// (wgrad: K = voxels, split over CTAs; both of its operands are read
+// MN-major straight from the channels-last tensors).
+#include <cuda_bf16.h>
+
+#include <cstdint>
+
+#include "umma.cuh"
+
+namespace aw {
+
+namespace {
+
+constexpr int kGBM = 128;      // rows per CTA
+constexpr int kGBK = 64;       // K per stage
+constexpr int kGThreads = 128;
+constexpr int kAStage = kGBM * kGBK * 2;  // bytes
+
+typedef __nv_bfloat16 bf16;
+
+struct Vol {
+  int B, D, H, W;
+  AW_HD long voxels() const { return (long)B * D * H * W; }
+};
+
+AW_D void tap_offset(int tap, int ntaps, int &dz, int &dy, int &dx) {
+  if (ntaps == 1) {
+    dz = dy = dx = 0;
+  } else {
+    dz = tap / 9 - 1;
+    dy = (tap / 3) % 3 - 1;
+    dx = tap % 3 - 1;
+  }
+}
+
+// voxel index m -> (b, z, y, x)
+AW_D void voxel_coords(const Vol &v, long m, int &b, int &z, int &y, int &x) {
+  x = (int)(m % v.W);
+  long t = m / v.W;
+  y = (int)(t % v.H);
+  t /= v.H;
+  z = (int)(t % v.D);
+  b = (int)(t / v.D);
+}
+
+// source voxel of (b,z,y,x) shifted by sign * off(tap), or -1 outside
+AW_D long shifted(const Vol &v, int b, int z, int y, int x, int tap, int ntaps, int sign) {
+  int dz, dy, dx;
+  tap_offset(tap, ntaps, dz, dy, dx);
+  const int zz = z + sign * dz, yy = y + sign * dy, xx = x + sign * dx;
+  if (zz < 0 || zz >= v.D || yy < 0 || yy >= v.H || xx < 0 || xx >= v.W) return -1;
+  return (((long)b * v.D + zz) * v.H + yy) * v.W + xx;
+}
+
+AW_D uint32_t kmajor_off(int r, int j, int R) { return j * (R * 16) + (r >> 3) * 128 + (r & 7) * 16; }
+AW_D uint32_t mnmajor_off(int k, int c, int R) { return (k >> 3) * (R * 16) + c * 128 + (k & 7) * 16; }
+
+// ---- operand loaders: fill one stage (K in [k0, k0 + 64), zero past kend) --
+// A of forward / dgrad: rows = voxels, K = (tap, channel) of X shifted by
+// sign * off(tap); K-major (the 8 channels of one chunk are contiguous)
+struct LoadConvA {
+  const bf16 *x;
+  Vol v;
+  int C, ntaps, sign;
+  long M;
+  static constexpr int kMN = 0;
+  AW_D void fill(uint8_t *s, long m0, int k0, int kend) const {
+    const int r = threadIdx.x;  // one row per thread
+    const long m = m0 + r;
+    int b = 0, z = 0, y = 0, xx = 0;
+    if (m < M) voxel_coords(v, m, b, z, y, xx);
+#pragma unroll
+    for (int j = 0; j < kGBK / 8; ++j) {
+      const int k = k0 + 8 * j;
+      uint4 val = make_uint4(0, 0, 0, 0);
+      if (m < M && k < kend) {
+        const int tap = k / C, ci = k - tap * C;
+        const long src = shifted(v, b, z, y, xx, tap, ntaps, sign);
+        if (src >= 0) val = *reinterpret_cast<const uint4 *>(x + src * C + ci);
+      }
+      *reinterpret_cast<uint4 *>(s + kmajor_off(r, j, kGBM)) = val;
+    }
+  }
+};
+
+// B of forward / dgrad: rows = output columns n < N, K contiguous per row
+template <int BN>
+struct LoadRowsB {
+  const bf16 *w;  // [BN][K]
+  int K;
+  static constexpr int kMN = 0;
+  AW_D void fill(uint8_t *s, int k0, int kend) const {
+    for (int i = threadIdx.x; i < BN * (kGBK / 8); i += kGThreads) {
+      const int r = i / (kGBK / 8), j = i % (kGBK / 8);
+      const int k = k0 + 8 * j;
+      uint4 val = make_uint4(0, 0, 0, 0);
+      if (k < kend) val = *reinterpret_cast<const uint4 *>(w + (long)r * K + k);
+      *reinterpret_cast<uint4 *>(s + kmajor_off(r, j, BN)) = val;
+    }
+  }
+};
+
+// A of wgrad: rows = (tap, ci) < ntaps*C, K = voxels; MN-major: the 8
+// channels of a chunk are contiguous in X
+struct LoadWgradA {
+  const bf16 *x;
+  Vol v;
+  int C, ntaps;
+  int Mtot;  // ntaps * C
+  static constexpr int kMN = 1;
+  AW_D void fill(uint8_t *s, long m0, int k0, int kend) const {
+    for (int i = threadIdx.x; i < kGBK * (kGBM / 8); i += kGThreads) {
+      const int kk = i / (kGBM / 8), c = i % (kGBM / 8);
+      const int k = k0 + kk;
+      const int mn = (int)m0 + 8 * c;
+      uint4 val = make_uint4(0, 0, 0, 0);
+      if (k < kend && mn < Mtot) {
+        const int tap = mn / C, ci = mn - tap * C;
+        int b, z, y, xx;
+        voxel_coords(v, k, b, z, y, xx);
+        const long src = shifted(v, b, z, y, xx, tap, ntaps, 1);
+        if (src >= 0) val = *reinterpret_cast<const uint4 *>(x + src * C + ci);
+      }
+      *reinterpret_cast<uint4 *>(s + mnmajor_off(kk, c, kGBM)) = val;
+    }
+  }
+};
+
+// B of wgrad: rows = co < BN, K = voxels; MN-major (dY's channels contiguous)
+template <int BN>
+struct LoadWgradB {
+  const bf16 *dy;  // [voxels][BN]
+  static constexpr int kMN = 1;
+  AW_D void fill(uint8_t *s, int k0, int kend) const {
+    for (int i = threadIdx.x; i < kGBK * (BN / 8); i += kGThreads) {
+      const int kk = i / (BN / 8), c = i % (BN / 8);
+      const int k = k0 + kk;
+      uint4 val = make_uint4(0, 0, 0, 0);
+      if (k < kend) val = *reinterpret_cast<const uint4 *>(dy + (long)k * BN + 8 * c);
+      *reinterpret_cast<uint4 *>(s + mnmajor_off(kk, c, BN)) = val;
+    }
+  }
+};
+
+// ---- epilogues: row m, 16 columns from n0 ----------------------------------
+// forward: + bias, optional ReLU, BF16 out (or FP32 out)
+template <int BN>
+struct EpiAct {
+  const float *bias;
+  bf16 *out;
+  float *outf;
+  int relu;
+  long M;
+  AW_D void store(long m, int n0, const float (&v)[16]) const {
+    if (m >= M) return;
+    float r[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      float t = v[i] + (bias ? bias[n0 + i] : 0.0f);
+      r[i] = relu ? fmaxf(t, 0.0f) : t;
+    }
+    if (outf) {
+#pragma unroll
+      for (int i = 0; i < 16; i += 4)
+        *reinterpret_cast<float4 *>(outf + m * BN + n0 + i) = make_float4(r[i], r[i + 1], r[i + 2], r[i + 3]);
+    } else {
+      __align__(16) bf16 h[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) h[i] = __float2bfloat16_rn(r[i]);
+      uint4 *dst = reinterpret_cast<uint4 *>(out + m * BN + n0);
+      dst[0] = reinterpret_cast<const uint4 *>(h)[0];
+      dst[1] = reinterpret_cast<const uint4 *>(h)[1];
+    }
+  }
+};
+
+// dgrad: the gradient times the ReLU derivative of the layer input (its
+// post-activation value > 0), BF16 out
+template <int BN>
+struct EpiMask {
+  const bf16 *mask;  // [M][BN], or null
+  bf16 *out;
+  long M;
+  AW_D void store(long m, int n0, const float (&v)[16]) const {
+    if (m >= M) return;
+    __align__(16) bf16 h[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const bool on = !mask || __bfloat162float(mask[m * BN + n0 + i]) > 0.0f;
+      h[i] = __float2bfloat16_rn(on ? v[i] : 0.0f);
+    }
+    uint4 *dst = reinterpret_cast<uint4 *>(out + m * BN + n0);
+    dst[0] = reinterpret_cast<const uint4 *>(h)[0];
+    dst[1] = reinterpret_cast<const uint4 *>(h)[1];
+  }
+};
+
+// wgrad: FP32 partial of this K split, stored [split][co][(tap,ci)]
+template <int BN>
+struct EpiWgrad {
+  float *part;
+  int Mtot;
+  AW_D void store(long m, int n0, const float (&v)[16]) const {
+    if (m >= Mtot) return;
+    float *p = part + (long)blockIdx.y * BN * Mtot;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) p[(long)(n0 + i) * Mtot + m] = v[i];
+  }
+};
+
+template <int BN>
+constexpr int tmem_cols() {
+  return BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
+}
+template <int BN>
+constexpr size_t gemm_smem() {
+  return 1024 + 2 * (size_t)kAStage + 2 * (size_t)BN * kGBK * 2;
+}
+
+template <int BN, class LA, class LB, class EP>
+__global__ void __launch_bounds__(kGThreads)
+    k_umma_gemm(LA la, LB lb, EP ep, int K, int k_per_split, int *status) {
+  extern __shared__ __align__(1024) uint8_t smraw[];
+  __shared__ uint64_t mbar[2];
+  __shared__ uint32_t tbase;
+  uint8_t *base = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
+  uint8_t *sA[2] = {base, base + kAStage};
+  uint8_t *sB[2] = {base + 2 * kAStage, base + 2 * kAStage + BN * kGBK * 2};
+  constexpr int TC = tmem_cols<BN>();
+  constexpr uint32_t IDESC = umma_idesc_bf16(kGBM, BN, LA::kMN, LB::kMN);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const long m0 = (long)blockIdx.x * kGBM;
+  const int kbeg = blockIdx.y * k_per_split;
+  const int kend = min(K, kbeg + k_per_split);
+  const int nsteps = kend > kbeg ? (kend - kbeg + kGBK - 1) / kGBK : 0;
+
+  if (warp == 0) tmem_alloc(&tbase, TC);
+  if (tid == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tbase;
+
+  uint32_t phase[2] = {0u, 0u};
+  bool ok = true;
+  for (int s = 0; s < nsteps; ++s) {
+    const int st = s & 1;
+    if (s >= 2) {  // the MMAs that read this stage two steps ago are done
+      ok = mbar_wait(&mbar[st], phase[st], status) && ok;
+      phase[st] ^= 1u;
+    }
+    const int k0 = kbeg + s * kGBK;
+    la.fill(sA[st], m0, k0, kend);
+    lb.fill(sB[st], k0, kend);
+    fence_async_smem();  // the tensor core reads what the threads wrote
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t a0 = smem_u32(sA[st]), b0 = smem_u32(sB[st]);
+#pragma unroll
+      for (int kk = 0; kk < kGBK / 16; ++kk) {
+        const uint64_t da = umma_desc(a0 + kk * 2 * (kGBM * 16), kGBM * 16, 128);
+        const uint64_t db = umma_desc(b0 + kk * 2 * (BN * 16), BN * 16, 128);
+        umma_bf16(tmem, da, db, IDESC, (s > 0 || kk > 0) ? 1u : 0u);
+      }
+      umma_commit(&mbar[st]);
+    }
+  }
+  if (nsteps > 0) {
+    const int last = (nsteps - 1) & 1;
+    ok = mbar_wait(&mbar[last], phase[last], status) && ok;
+  }
+  tc_fence_after();
+  // epilogue: warp w owns TMEM lanes (rows) 32w .. 32w+31
+  const long m = m0 + 32 * warp + (tid & 31);
+#pragma unroll 1
+  for (int c = 0; c < BN / 16; ++c) {
+    float v[16];
+    tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(16 * c), v);
+    if (nsteps == 0 || !ok) {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) v[i] = 0.0f;
+    }
+    ep.store(m, 16 * c, v);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, TC);
+}
+
+template <int BN, class LA, class LB, class EP>
+cudaError_t launch_gemm(const LA &la, const LB &lb, const EP &ep, long M, int K, int splits,
+                        int k_per_split, int *status, cudaStream_t s) {
+  const size_t smem = gemm_smem<BN>();
+  auto kern = k_umma_gemm<BN, LA, LB, EP>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((unsigned)((M + kGBM - 1) / kGBM), (unsigned)splits);
+  kern<<<grid, kGThreads, smem, s>>>(la, lb, ep, K, k_per_split, status);
+  return cudaGetLastError();
+}
+
+template <class F>
+bool dispatch_bn(int n, F &&f) {
+  switch (n) {
+    case 16: f(std::integral_constant<int, 16>()); return true;
+    case 32: f(std::integral_constant<int, 32>()); return true;
+    case 48: f(std::integral_constant<int, 48>()); return true;
+    case 64: f(std::integral_constant<int, 64>()); return true;
+    case 96: f(std::integral_constant<int, 96>()); return true;
+    case 128: f(std::integral_constant<int, 128>()); return true;
+    case 192: f(std::integral_constant<int, 192>()); return true;
+    default: return false;
+  }
+}
+
+// ---- elementwise layers ------------------------------------------------------
+constexpr int kEw = 256;
+inline unsigned ew_grid(long n) { return (unsigned)((n + kEw - 1) / kEw); }
+
+// 2x2x2 average pooling, channels last; backward spreads dY / 8
+__global__ void k_pool_fwd(const bf16 *__restrict__ x, bf16 *__restrict__ y, Vol vo, int C) {
+  const long i = (long)blockIdx.x * kEw + threadIdx.x;  // over output voxels * C
+  if (i >= vo.voxels() * C) return;
+  const int c = (int)(i % C);
+  int b, z, yy, xx;
+  voxel_coords(vo, i / C, b, z, yy, xx);
+  const Vol vi{vo.B, 2 * vo.D, 2 * vo.H, 2 * vo.W};
+  float s = 0.0f;
+  for (int dz = 0; dz < 2; ++dz)
+    for (int dy = 0; dy < 2; ++dy)
+      for (int dx = 0; dx < 2; ++dx)
+        s += __bfloat162float(
+            x[((((long)b * vi.D + 2 * z + dz) * vi.H + 2 * yy + dy) * vi.W + 2 * xx + dx) * C + c]);
+  y[i] = __float2bfloat16_rn(0.125f * s);
+}
+// backward: dx = (dy / 8 + add) where mask > 0 (mask: the pooled
+// post-ReLU activation; add, mask may be null)
+__global__ void k_pool_bwd(const bf16 *__restrict__ dy, bf16 *__restrict__ dx, Vol vi, int C,
+                           const bf16 *__restrict__ add, const bf16 *__restrict__ mask) {
+  const long i = (long)blockIdx.x * kEw + threadIdx.x;  // over input voxels * C
+  if (i >= vi.voxels() * C) return;
+  const int c = (int)(i % C);
+  int b, z, y, x;
+  voxel_coords(vi, i / C, b, z, y, x);
+  const Vol vo{vi.B, vi.D / 2, vi.H / 2, vi.W / 2};
+  float g = 0.125f * __bfloat162float(dy[((((long)b * vo.D + z / 2) * vo.H + y / 2) * vo.W + x / 2) * C + c]);
+  if (add) g += __bfloat162float(add[i]);
+  if (mask && !(__bfloat162float(mask[i]) > 0.0f)) g = 0.0f;
+  dx[i] = __float2bfloat16_rn(g);
+}
+// nearest x2 upsampling into channels [c0, c0 + C) of a Ct-channel tensor;
+// backward sums the 8 children
+__global__ void k_up_fwd(const bf16 *__restrict__ x, bf16 *__restrict__ y, Vol vo, int C, int Ct,
+                         int c0) {
+  const long i = (long)blockIdx.x * kEw + threadIdx.x;  // over output voxels * C
+  if (i >= vo.voxels() * C) return;
+  const int c = (int)(i % C);
+  const long m = i / C;
+  int b, z, yy, xx;
+  voxel_coords(vo, m, b, z, yy, xx);
+  const Vol vi{vo.B, vo.D / 2, vo.H / 2, vo.W / 2};
+  y[m * Ct + c0 + c] = x[((((long)b * vi.D + z / 2) * vi.H + yy / 2) * vi.W + xx / 2) * C + c];
+}
+__global__ void k_up_bwd(const bf16 *__restrict__ dy, bf16 *__restrict__ dx, Vol vi, int C, int Ct,
+                         int c0) {
+  const long i = (long)blockIdx.x * kEw + threadIdx.x;  // over input (coarse) voxels * C
+  if (i >= vi.voxels() * C) return;
+  const int c = (int)(i % C);
+  int b, z, y, x;
+  voxel_coords(vi, i / C, b, z, y, x);
+  const Vol vo{vi.B, 2 * vi.D, 2 * vi.H, 2 * vi.W};
+  float s = 0.0f;
+  for (int dz = 0; dz < 2; ++dz)
+    for (int dyy = 0; dyy < 2; ++dyy)
+      for (int dxx = 0; dxx < 2; ++dxx)
+        s += __bfloat162float(
+            dy[((((long)b * vo.D + 2 * z + dz) * vo.H + 2 * y + dyy) * vo.W + 2 * x + dxx) * Ct + c0 + c]);
+  dx[i] = __float2bfloat16_rn(s);
+}
+// copy C channels into / out of channels [c0, c0 + C) of a Ct-channel tensor
+// (the skip half of a concatenation); out += when accumulate
+__global__ void k_slice(const bf16 *__restrict__ src, int Cs, int cs0, bf16 *__restrict__ dst,
+                        int Cd, int cd0, int C, long voxels, int accumulate) {
+  const long i = (long)blockIdx.x * kEw + threadIdx.x;
+  if (i >= voxels * C) return;
+  const long m = i / C;
+  const int c = (int)(i % C);
+  float v = __bfloat162float(src[m * Cs + cs0 + c]);
+  if (accumulate) v += __bfloat162float(dst[m * Cd + cd0 + c]);
+  dst[m * Cd + cd0 + c] = __float2bfloat16_rn(v);
+}
+
+// (I0, I1) planar float -> channels 0, 1 of a 16-channel BF16 tensor
+__global__ void k_pack_pair(const float *__restrict__ a, const float *__restrict__ b,
+                            bf16 *__restrict__ x, long voxels) {
+  const long m = (long)blockIdx.x * kEw + threadIdx.x;
+  if (m >= voxels) return;
+  __align__(16) bf16 h[16];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) h[c] = __float2bfloat16_rn(0.0f);
+  h[0] = __float2bfloat16_rn(a[m]);
+  h[1] = __float2bfloat16_rn(b[m]);
+  uint4 *d = reinterpret_cast<uint4 *>(x + m * 16);
+  d[0] = reinterpret_cast<const uint4 *>(h)[0];
+  d[1] = reinterpret_cast<const uint4 *>(h)[1];
+}
+
+// MSE over the first 3 of 16 prediction channels against a planar target:
+// block partial sums of squares and the BF16 gradient 2 (p - t) / (3 V)
+__global__ void k_mse(const float *__restrict__ pred, const float *__restrict__ tgt, long voxels,
+                      bf16 *__restrict__ grad, double *__restrict__ partials) {
+  const long m = (long)blockIdx.x * kEw + threadIdx.x;
+  double e = 0.0;
+  if (m < voxels) {
+    __align__(16) bf16 h[16];
+    const float scale = 2.0f / (3.0f * (float)voxels);
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      float g = 0.0f;
+      if (c < 3) {
+        const float d = pred[m * 16 + c] - tgt[c * voxels + m];
+        e += (double)d * d;
+        g = scale * d;
+      }
+      h[c] = __float2bfloat16_rn(g);
+    }
+    uint4 *dst = reinterpret_cast<uint4 *>(grad + m * 16);
+    dst[0] = reinterpret_cast<const uint4 *>(h)[0];
+    dst[1] = reinterpret_cast<const uint4 *>(h)[1];
+  }
+  __shared__ double ws[kEw / 32];
+  e = warp_sum(e);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = e;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kEw / 32; ++w) t += ws[w];
+    partials[blockIdx.x] = t;
+  }
+}
+__global__ void k_sum_partials(const double *__restrict__ p, int n, double scale,
+                               float *__restrict__ out) {
+  double t = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) t += p[i];
+  __shared__ double ws[32];
+  t = warp_sum(t);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) s += ws[w];
+    *out = (float)(s * scale);
+  }
+}
+
+// dW = sum over K splits of the partials [split][co][K]
+__global__ void k_reduce_splits(const float *__restrict__ part, int splits, long n,
+                                float *__restrict__ dw) {
+  const long i = (long)blockIdx.x * kEw + threadIdx.x;
+  if (i >= n) return;
+  float s = 0.0f;
+  for (int k = 0; k < splits; ++k) s += part[k * n + i];
+  dw[i] = s;
+}
+// bias gradient: column sums of dY [M][N], one block per column
+__global__ void k_bias_grad(const bf16 *__restrict__ dy, long M, int N, float *__restrict__ db) {
+  const int n = blockIdx.x;
+  float s = 0.0f;
+  for (long m = threadIdx.x; m < M; m += blockDim.x) s += __bfloat162float(dy[m * N + n]);
+  __shared__ float ws[32];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.0f;
+    for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) t += ws[w];
+    db[n] = t;
+  }
+}
+
+// Adam (Kingma & Ba 2015) on the FP32 masters
+__global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m1,
+                       float *__restrict__ m2, long n, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+  const long i = (long)blockIdx.x * kEw + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float a = b1 * m1[i] + (1.0f - b1) * gi;
+  const float b = b2 * m2[i] + (1.0f - b2) * gi * gi;
+  m1[i] = a;
+  m2[i] = b;
+  w[i] -= lr * (a / c1) / (sqrtf(b / c2) + eps);
+}
+// BF16 weights [co][tap][ci] and the dgrad copy [ci][tap][co]
+__global__ void k_weights_bf16(const float *__restrict__ w, int cout, int ntaps, int cin,
+                               bf16 *__restrict__ wb, bf16 *__restrict__ wt) {
+  const long i = (long)blockIdx.x * kEw + threadIdx.x;
+  const long n = (long)cout * ntaps * cin;
+  if (i >= n) return;
+  const int ci = (int)(i % cin);
+  const long r = i / cin;
+  const int tap = (int)(r % ntaps), co = (int)(r / ntaps);
+  const bf16 v = __float2bfloat16_rn(w[i]);
+  wb[i] = v;
+  if (wt) wt[((long)ci * ntaps + tap) * cout + co] = v;
+}
+
+// h = identity + the first 3 prediction channels (the warm start)
+__global__ void k_disp_to_h(const float *__restrict__ pred, Vol v, float *__restrict__ hx,
+                            float *__restrict__ hy, float *__restrict__ hz) {
+  const long m = (long)blockIdx.x * kEw + threadIdx.x;
+  if (m >= v.voxels()) return;
+  int b, z, y, x;
+  voxel_coords(v, m, b, z, y, x);
+  hx[m] = (float)x + pred[m * 16 + 0];
+  hy[m] = (float)y + pred[m * 16 + 1];
+  hz[m] = (float)z + pred[m * 16 + 2];
+}
+
+}  // namespace
+
+// ---- host entry points (called from capi.cu) ---------------------------------
+bool nn_channels_ok(int c) { return dispatch_bn(c, [](auto) {}); }
+
+cudaError_t nn_conv_fwd(const void *x, int B, int D, int H, int W, int cin, const void *w,
+                        const float *bias, int cout, int ntaps, int relu, void *out,
+                        float *outf, int *status, cudaStream_t s) {
+  const Vol v{B, D, H, W};
+  const long M = (long)B * D * H * W;
+  const int K = ntaps * cin;
+  cudaError_t e = cudaErrorInvalidValue;
+  dispatch_bn(cout, [&](auto BNc) {
+    constexpr int BN = decltype(BNc)::value;
+    LoadConvA la{static_cast<const bf16 *>(x), v, cin, ntaps, 1, M};
+    LoadRowsB<BN> lb{static_cast<const bf16 *>(w), K};
+    EpiAct<BN> ep{bias, static_cast<bf16 *>(out), outf, relu, M};
+    e = launch_gemm<BN>(la, lb, ep, M, K, 1, K, status, s);
+  });
+  return e;
+}
+
+cudaError_t nn_conv_dgrad(const void *dy, int B, int D, int H, int W, int cout, const void *wt,
+                          int cin, int ntaps, const void *mask, void *dx, int *status,
+                          cudaStream_t s) {
+  const Vol v{B, D, H, W};
+  const long M = (long)B * D * H * W;
+  const int K = ntaps * cout;
+  cudaError_t e = cudaErrorInvalidValue;
+  dispatch_bn(cin, [&](auto BNc) {
+    constexpr int BN = decltype(BNc)::value;
+    LoadConvA la{static_cast<const bf16 *>(dy), v, cout, ntaps, -1, M};
+    LoadRowsB<BN> lb{static_cast<const bf16 *>(wt), K};
+    EpiMask<BN> ep{static_cast<const bf16 *>(mask), static_cast<bf16 *>(dx), M};
+    e = launch_gemm<BN>(la, lb, ep, M, K, 1, K, status, s);
+  });
+  return e;
+}
+
+size_t nn_wgrad_part_floats(int cin, int cout, int ntaps, int splits) {
+  return (size_t)splits * cout * ntaps * cin;
+}
+
+cudaError_t nn_conv_wgrad(const void *x, const void *dy, int B, int D, int H, int W, int cin,
+                          int cout, int ntaps, int splits, float *part, float *dw, int *status,
+                          cudaStream_t s) {
+  const Vol v{B, D, H, W};
+  const long voxels = (long)B * D * H * W;
+  const int Mtot = ntaps * cin;
+  long per = (voxels + splits - 1) / splits;
+  per = ((per + kGBK - 1) / kGBK) * kGBK;
+  splits = (int)((voxels + per - 1) / per);
+  cudaError_t e = cudaErrorInvalidValue;
+  dispatch_bn(cout, [&](auto BNc) {
+    constexpr int BN = decltype(BNc)::value;
+    LoadWgradA la{static_cast<const bf16 *>(x), v, cin, ntaps, Mtot};
+    LoadWgradB<BN> lb{static_cast<const bf16 *>(dy)};
+    EpiWgrad<BN> ep{part, Mtot};
+    e = launch_gemm<BN>(la, lb, ep, Mtot, (int)voxels, splits, (int)per, status, s);
+  });
+  if (e != cudaSuccess) return e;
+  const long n = (long)cout * Mtot;
+  k_reduce_splits<<<ew_grid(n), kEw, 0, s>>>(part, splits, n, dw);
+  return cudaGetLastError();
+}
+
+cudaError_t nn_bias_grad(const void *dy, long M, int N, float *db, cudaStream_t s) {
+  k_bias_grad<<<N, 256, 0, s>>>(static_cast<const bf16 *>(dy), M, N, db);
+  return cudaGetLastError();
+}
+
+cudaError_t nn_pool(const void *in, int B, int D, int H, int W, int C, void *out, int backward,
+                    const void *add, const void *mask, cudaStream_t s) {
+  // forward: (D,H,W) is the input grid; backward: the input-gradient grid
+  if (!backward) {
+    const Vol vo{B, D / 2, H / 2, W / 2};
+    k_pool_fwd<<<ew_grid(vo.voxels() * C), kEw, 0, s>>>(static_cast<const bf16 *>(in),
+                                                        static_cast<bf16 *>(out), vo, C);
+  } else {
+    const Vol vi{B, D, H, W};
+    k_pool_bwd<<<ew_grid(vi.voxels() * C), kEw, 0, s>>>(static_cast<const bf16 *>(in),
+                                                        static_cast<bf16 *>(out), vi, C,
+                                                        static_cast<const bf16 *>(add),
+                                                        static_cast<const bf16 *>(mask));
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t nn_upsample(const void *in, int B, int D, int H, int W, int C, void *out, int Ct,
+                        int c0, int backward, cudaStream_t s) {
+  // (D,H,W) is the coarse grid in both directions
+  const Vol vc{B, D, H, W};
+  const Vol vf{B, 2 * D, 2 * H, 2 * W};
+  if (!backward)
+    k_up_fwd<<<ew_grid(vf.voxels() * C), kEw, 0, s>>>(static_cast<const bf16 *>(in),
+                                                      static_cast<bf16 *>(out), vf, C, Ct, c0);
+  else
+    k_up_bwd<<<ew_grid(vc.voxels() * C), kEw, 0, s>>>(static_cast<const bf16 *>(in),
+                                                      static_cast<bf16 *>(out), vc, C, Ct, c0);
+  return cudaGetLastError();
+}
+
+cudaError_t nn_slice(const void *src, int Cs, int cs0, void *dst, int Cd, int cd0, int C,
+                     long voxels, int accumulate, cudaStream_t s) {
+  k_slice<<<ew_grid(voxels * C), kEw, 0, s>>>(static_cast<const bf16 *>(src), Cs, cs0,
+                                               static_cast<bf16 *>(dst), Cd, cd0, C, voxels,
+                                               accumulate);
+  return cudaGetLastError();
+}
+
+cudaError_t nn_pack_pair(const float *a, const float *b, long voxels, void *x, cudaStream_t s) {
+  k_pack_pair<<<ew_grid(voxels), kEw, 0, s>>>(a, b, static_cast<bf16 *>(x), voxels);
+  return cudaGetLastError();
+}
+
+size_t nn_mse_partials(long voxels) { return ew_grid(voxels); }
+
+cudaError_t nn_mse(const float *pred, const float *tgt, long voxels, void *grad, double *partials,
+                   float *loss, cudaStream_t s) {
+  const unsigned g = ew_grid(voxels);
+  k_mse<<<g, kEw, 0, s>>>(pred, tgt, voxels, static_cast<bf16 *>(grad), partials);
+  k_sum_partials<<<1, 1024, 0, s>>>(partials, (int)g, 1.0 / (3.0 * (double)voxels), loss);
+  return cudaGetLastError();
+}
+
+cudaError_t nn_adam(float *w, const float *g, float *m1, float *m2, long n, float lr, float b1,
+                    float b2, float eps, int t, cudaStream_t s) {
+  const float c1 = 1.0f - powf(b1, (float)t), c2 = 1.0f - powf(b2, (float)t);
+  k_adam<<<ew_grid(n), kEw, 0, s>>>(w, g, m1, m2, n, lr, b1, b2, eps, c1, c2);
+  return cudaGetLastError();
+}
+
+cudaError_t nn_weights_bf16(const float *w, int cout, int ntaps, int cin, void *wb, void *wt,
+                            cudaStream_t s) {
+  const long n = (long)cout * ntaps * cin;
+  k_weights_bf16<<<ew_grid(n), kEw, 0, s>>>(w, cout, ntaps, cin, static_cast<bf16 *>(wb),
+                                            static_cast<bf16 *>(wt));
+  return cudaGetLastError();
+}
+
+cudaError_t nn_disp_to_h(const float *pred, int D, int H, int W, float *hx, float *hy, float *hz,
+                         cudaStream_t s) {
+  const Vol v{1, D, H, W};
+  k_disp_to_h<<<ew_grid(v.voxels()), kEw, 0, s>>>(pred, v, hx, hy, hz);
+  return cudaGetLastError();
+}
+
+}  // namespace aw

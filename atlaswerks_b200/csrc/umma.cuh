@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "aw_common.cuh"
 #include "bulk.cuh"
 
 namespace aw {

@@ -254,6 +254,64 @@ int aw_ldmm_run(aw_ldmm_t l, const float *I0, const float *I1, float *v, int n_i
 /* Image energies sp^3 * sum (I0(h_T) - I1)^2, oldest first; synchronises. */
 int aw_ldmm_get_energies(aw_ldmm_t l, double *out, int max_count, int *count);
 
+/* ---------------------------------------------------------------------------
+ * Learned warm start: the kernels of a 3D convolutional encoder-decoder
+ * (no counterpart in the reference; it predicts an initial deformation
+ * that the greedy iteration then refines). Convolutions run as implicit
+ * GEMMs on the tcgen05 tensor cores, BF16 operands, FP32 accumulation.
+ * Activations: BF16 [B][D][H][W][C], channels last, C a multiple of 16.
+ * Weights: BF16 [Cout][taps][Cin] (taps 27 = 3x3x3 zero-padded, or 1);
+ * the data gradient takes the transposed copy [Cin][taps][Cout] that
+ * aw_nn_weights_bf16 writes. Output channels: 16 32 48 64 96 128 192.
+ * ------------------------------------------------------------------------- */
+/* out = act(conv(x, w) + bias): BF16 out_bf16, or FP32 out_f32 when given */
+int aw_nn_conv3d_fwd(const void *x, int B, int D, int H, int W, int cin, const void *w,
+                     const float *bias, int cout, int ntaps, int relu, void *out_bf16,
+                     float *out_f32, void *stream);
+/* dx = conv^T(dy, w) times (mask > 0) (the ReLU derivative of the layer's
+ * input, which is a post-ReLU activation); mask NULL = no mask */
+int aw_nn_conv3d_dgrad(const void *dy, int B, int D, int H, int W, int cout, const void *wt,
+                       int cin, int ntaps, const void *mask, void *dx, void *stream);
+/* dw [Cout][taps][Cin] (FP32) = sum over voxels of dy x shifted x; the
+ * voxel sum is split over `splits` CTA columns whose partials go to
+ * scratch (aw_nn_wgrad_scratch_floats floats) and are summed in order */
+size_t aw_nn_wgrad_scratch_floats(int cin, int cout, int ntaps, int splits);
+int aw_nn_conv3d_wgrad(const void *x, const void *dy, int B, int D, int H, int W, int cin,
+                       int cout, int ntaps, int splits, float *scratch, float *dw, void *stream);
+/* db[c] = sum over the M voxels of dy[.][c] */
+int aw_nn_bias_grad(const void *dy, long M, int cout, float *db, void *stream);
+/* 2x2x2 average pooling of the (D,H,W) grid; backward (D,H,W = the fine
+ * grid) spreads dy/8, adds `add` and keeps it where mask > 0 (the pooled
+ * post-ReLU activation); add and mask may be NULL */
+int aw_nn_pool(const void *in, int B, int D, int H, int W, int C, void *out, int backward,
+               const void *add, const void *mask, void *stream);
+/* nearest x2 upsampling of the coarse (D,H,W) grid into channels
+ * [c0, c0+C) of a Ct-channel fine tensor; backward sums the 8 children */
+int aw_nn_upsample(const void *in, int B, int D, int H, int W, int C, void *out, int Ct, int c0,
+                   int backward, void *stream);
+/* copy (or add) C channels between channel slices of two tensors */
+int aw_nn_slice(const void *src, int Cs, int cs0, void *dst, int Cd, int cd0, int C, long voxels,
+                int accumulate, void *stream);
+/* (I0, I1) planar float -> channels 0, 1 of a 16-channel BF16 input */
+int aw_nn_pack_pair(const float *I0, const float *I1, long voxels, void *x, void *stream);
+/* loss = mean over voxels and 3 channels of (pred[.][c] - target[c][.])^2
+ * (pred FP32 [V][16], target planar [3][V]); grad BF16 [V][16] */
+size_t aw_nn_mse_scratch_doubles(long voxels);
+int aw_nn_mse(const float *pred, const float *target, long voxels, void *grad, double *scratch,
+              float *loss, void *stream);
+/* Adam on FP32 masters (step counts from 1) */
+int aw_nn_adam(float *w, const float *g, float *m1, float *m2, long n, float lr, float beta1,
+               float beta2, float eps, int step, void *stream);
+/* BF16 copies of FP32 weights: [Cout][taps][Cin] and (wt_bf16 non-NULL)
+ * the transposed [Cin][taps][Cout] */
+int aw_nn_weights_bf16(const float *w, int cout, int ntaps, int cin, void *w_bf16,
+                       void *wt_bf16, void *stream);
+/* h = identity + the predicted displacement (channels 0..2 of FP32 [V][16]) */
+int aw_nn_displacement_to_h(const float *pred, int D, int H, int W, float *hx, float *hy,
+                            float *hz, void *stream);
+/* 1 in *timed_out when a GEMM gave up a bounded wait since the last call */
+int aw_nn_status(int *timed_out);
+
 #ifdef __cplusplus
 }
 #endif
