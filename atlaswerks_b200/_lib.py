@@ -78,11 +78,15 @@ SIGNATURES = {
     "aw_ldmm_iterate": ([_fp] * 4 + [_i, _fp], _i),
     "aw_ldmm_run": ([_fp] * 4 + [_i, _i, _fp], _i),
     "aw_ldmm_get_energies": ([_fp, _fp, _i, _fp], _i),
-    "aw_nn_conv3d_fwd": ([_fp] + [_i] * 5 + [_fp, _fp, _i, _i, _i, _fp, _fp, _fp], _i),
-    "aw_nn_conv3d_dgrad": ([_fp] + [_i] * 5 + [_fp, _i, _i, _fp, _fp, _fp], _i),
+    "aw_nn_conv3d_scratch_floats": ([_i] * 7, ctypes.c_size_t),
+    "aw_nn_conv3d_fwd": ([_fp] + [_i] * 5 + [_fp, _fp, _i, _i, _i, _fp, _fp, _fp,
+                                           ctypes.c_size_t, _fp], _i),
+    "aw_nn_conv3d_dgrad": ([_fp] + [_i] * 5 + [_fp, _i, _i, _fp, _fp, _fp, ctypes.c_size_t,
+                                             _fp], _i),
     "aw_nn_wgrad_scratch_floats": ([_i, _i, _i, _i], ctypes.c_size_t),
     "aw_nn_conv3d_wgrad": ([_fp, _fp] + [_i] * 8 + [_fp, _fp, _fp], _i),
-    "aw_nn_bias_grad": ([_fp, ctypes.c_long, _i, _fp, _fp], _i),
+    "aw_nn_bias_scratch_floats": ([ctypes.c_long, _i], ctypes.c_size_t),
+    "aw_nn_bias_grad": ([_fp, ctypes.c_long, _i, _fp, _fp, _fp], _i),
     "aw_nn_pool": ([_fp] + [_i] * 5 + [_fp, _i, _fp, _fp, _fp], _i),
     "aw_nn_upsample": ([_fp] + [_i] * 5 + [_fp, _i, _i, _i, _fp], _i),
     "aw_nn_slice": ([_fp, _i, _i, _fp, _i, _i, _i, ctypes.c_long, _i, _fp], _i),

@@ -37,11 +37,29 @@ constexpr int kAStage = kGBM * kGBK * 2;  // bytes
 
 typedef __nv_bfloat16 bf16;
 
+// n / d for 0 <= n < 2^31 by multiply and shift (round-up method):
+// mul = floor(2^32 (2^l - d) / d) + 1, l = ceil(log2 d), q = (hi(n mul) + n) >> l
+struct FastDiv {
+  uint32_t d, mul, l;
+  AW_D uint32_t div(uint32_t n) const { return (__umulhi(n, mul) + n) >> l; }
+};
+inline FastDiv make_fastdiv(uint32_t d) {
+  uint32_t l = 0;
+  while ((1ull << l) < d) ++l;
+  const uint64_t mul = ((1ull << 32) * ((1ull << l) - d)) / d + 1;
+  return FastDiv{d, (uint32_t)mul, l};
+}
+
 struct Vol {
   int B, D, H, W;
+  FastDiv fw, fh, fd;
   AW_HD long voxels() const { return (long)B * D * H * W; }
 };
+inline Vol make_vol(int B, int D, int H, int W) {
+  return Vol{B, D, H, W, make_fastdiv(W), make_fastdiv(H), make_fastdiv(D)};
+}
 
+// tap -> (dz, dy, dx) offsets of a 3x3x3 stencil, packed as 3 x 2 bits (+1)
 AW_D void tap_offset(int tap, int ntaps, int &dz, int &dy, int &dx) {
   if (ntaps == 1) {
     dz = dy = dx = 0;
@@ -53,110 +71,172 @@ AW_D void tap_offset(int tap, int ntaps, int &dz, int &dy, int &dx) {
 }
 
 // voxel index m -> (b, z, y, x)
-AW_D void voxel_coords(const Vol &v, long m, int &b, int &z, int &y, int &x) {
-  x = (int)(m % v.W);
-  long t = m / v.W;
-  y = (int)(t % v.H);
-  t /= v.H;
-  z = (int)(t % v.D);
-  b = (int)(t / v.D);
-}
-
-// source voxel of (b,z,y,x) shifted by sign * off(tap), or -1 outside
-AW_D long shifted(const Vol &v, int b, int z, int y, int x, int tap, int ntaps, int sign) {
-  int dz, dy, dx;
-  tap_offset(tap, ntaps, dz, dy, dx);
-  const int zz = z + sign * dz, yy = y + sign * dy, xx = x + sign * dx;
-  if (zz < 0 || zz >= v.D || yy < 0 || yy >= v.H || xx < 0 || xx >= v.W) return -1;
-  return (((long)b * v.D + zz) * v.H + yy) * v.W + xx;
+AW_D void voxel_coords(const Vol &v, int m, int &b, int &z, int &y, int &x) {
+  const int q1 = (int)v.fw.div((uint32_t)m);
+  x = m - q1 * v.W;
+  const int q2 = (int)v.fh.div((uint32_t)q1);
+  y = q1 - q2 * v.H;
+  b = (int)v.fd.div((uint32_t)q2);
+  z = q2 - b * v.D;
 }
 
 AW_D uint32_t kmajor_off(int r, int j, int R) { return j * (R * 16) + (r >> 3) * 128 + (r & 7) * 16; }
 AW_D uint32_t mnmajor_off(int k, int c, int R) { return (k >> 3) * (R * 16) + c * 128 + (k & 7) * 16; }
 
-// ---- operand loaders: fill one stage (K in [k0, k0 + 64), zero past kend) --
+// ---- operand loaders ----------------------------------------------------------
+// Each loader moves this thread's 16-byte chunks of one 64-deep K step:
+// load() from global memory into registers (zero past kend or outside the
+// volume), store() into the stage's canonical layout. init() computes the
+// per-thread context once per CTA.
+
 // A of forward / dgrad: rows = voxels, K = (tap, channel) of X shifted by
-// sign * off(tap); K-major (the 8 channels of one chunk are contiguous)
+// sign * off(tap); K-major (the 8 channels of a chunk are contiguous).
+// Thread t owns row t of the tile.
 struct LoadConvA {
   const bf16 *x;
   Vol v;
   int C, ntaps, sign;
-  long M;
-  static constexpr int kMN = 0;
-  AW_D void fill(uint8_t *s, long m0, int k0, int kend) const {
-    const int r = threadIdx.x;  // one row per thread
-    const long m = m0 + r;
-    int b = 0, z = 0, y = 0, xx = 0;
-    if (m < M) voxel_coords(v, m, b, z, y, xx);
+  int M;
+  FastDiv fc;
+  static constexpr int kMN = 0, kChunks = kGBK / 8;
+  struct Ctx {
+    int m, b, z, y, xx;
+  };
+  AW_D Ctx init(long m0) const {
+    Ctx c;
+    c.m = (int)m0 + threadIdx.x;
+    c.b = c.z = c.y = c.xx = 0;
+    if (c.m < M) voxel_coords(v, c.m, c.b, c.z, c.y, c.xx);
+    return c;
+  }
+  AW_D void load(const Ctx &c, uint4 (&r)[kChunks], int k0, int kend) const {
+    int tap = (int)fc.div((uint32_t)k0);
+    int ci = k0 - tap * C;
 #pragma unroll
-    for (int j = 0; j < kGBK / 8; ++j) {
+    for (int j = 0; j < kChunks; ++j) {
       const int k = k0 + 8 * j;
       uint4 val = make_uint4(0, 0, 0, 0);
-      if (m < M && k < kend) {
-        const int tap = k / C, ci = k - tap * C;
-        const long src = shifted(v, b, z, y, xx, tap, ntaps, sign);
-        if (src >= 0) val = *reinterpret_cast<const uint4 *>(x + src * C + ci);
+      if (c.m < M && k < kend) {
+        int dz, dy, dx;
+        tap_offset(tap, ntaps, dz, dy, dx);
+        const int zz = c.z + sign * dz, yy = c.y + sign * dy, xs = c.xx + sign * dx;
+        if (zz >= 0 && zz < v.D && yy >= 0 && yy < v.H && xs >= 0 && xs < v.W) {
+          const int src = ((c.b * v.D + zz) * v.H + yy) * v.W + xs;
+          val = __ldg(reinterpret_cast<const uint4 *>(x + (long)src * C + ci));
+        }
       }
-      *reinterpret_cast<uint4 *>(s + kmajor_off(r, j, kGBM)) = val;
+      r[j] = val;
+      ci += 8;
+      if (ci == C) {
+        ci = 0;
+        ++tap;
+      }
     }
+  }
+  AW_D void store(uint8_t *s, const uint4 (&r)[kChunks]) const {
+#pragma unroll
+    for (int j = 0; j < kChunks; ++j)
+      *reinterpret_cast<uint4 *>(s + kmajor_off(threadIdx.x, j, kGBM)) = r[j];
   }
 };
 
-// B of forward / dgrad: rows = output columns n < N, K contiguous per row
+// B of forward / dgrad: rows = output columns n < N, K contiguous per row.
+// Chunk i = tid + 128 q: row i % BN, K chunk i / BN (consecutive threads
+// fill consecutive 16-byte slots of shared memory).
 template <int BN>
 struct LoadRowsB {
   const bf16 *w;  // [BN][K]
   int K;
-  static constexpr int kMN = 0;
-  AW_D void fill(uint8_t *s, int k0, int kend) const {
-    for (int i = threadIdx.x; i < BN * (kGBK / 8); i += kGThreads) {
-      const int r = i / (kGBK / 8), j = i % (kGBK / 8);
-      const int k = k0 + 8 * j;
-      uint4 val = make_uint4(0, 0, 0, 0);
-      if (k < kend) val = *reinterpret_cast<const uint4 *>(w + (long)r * K + k);
-      *reinterpret_cast<uint4 *>(s + kmajor_off(r, j, BN)) = val;
+  static constexpr int kMN = 0, kChunks = BN * (kGBK / 8) / kGThreads;
+  static_assert(BN * (kGBK / 8) % kGThreads == 0, "whole chunks per thread");
+  AW_D void load(uint4 (&r)[kChunks], int k0, int kend) const {
+#pragma unroll
+    for (int q = 0; q < kChunks; ++q) {
+      const int i = threadIdx.x + kGThreads * q;
+      const int row = i % BN, k = k0 + 8 * (i / BN);
+      r[q] = k < kend ? __ldg(reinterpret_cast<const uint4 *>(w + (long)row * K + k))
+                      : make_uint4(0, 0, 0, 0);
+    }
+  }
+  AW_D void store(uint8_t *s, const uint4 (&r)[kChunks]) const {
+#pragma unroll
+    for (int q = 0; q < kChunks; ++q) {
+      const int i = threadIdx.x + kGThreads * q;
+      *reinterpret_cast<uint4 *>(s + kmajor_off(i % BN, i / BN, BN)) = r[q];
     }
   }
 };
 
 // A of wgrad: rows = (tap, ci) < ntaps*C, K = voxels; MN-major: the 8
-// channels of a chunk are contiguous in X
+// channels of a chunk are contiguous in X. Thread t owns the channel chunk
+// c = (t / 8) % 16 (a fixed (tap, ci0) for the CTA) at voxels
+// k0 + t % 8 + 8j, so consecutive threads fill consecutive shared slots.
 struct LoadWgradA {
   const bf16 *x;
   Vol v;
   int C, ntaps;
   int Mtot;  // ntaps * C
-  static constexpr int kMN = 1;
-  AW_D void fill(uint8_t *s, long m0, int k0, int kend) const {
-    for (int i = threadIdx.x; i < kGBK * (kGBM / 8); i += kGThreads) {
-      const int kk = i / (kGBM / 8), c = i % (kGBM / 8);
-      const int k = k0 + kk;
-      const int mn = (int)m0 + 8 * c;
+  FastDiv fc;
+  static constexpr int kMN = 1, kChunks = kGBK / 8;
+  struct Ctx {
+    int ok, ci, dz, dy, dx;
+  };
+  AW_D Ctx init(long m0) const {
+    Ctx c;
+    const int mn = (int)m0 + 8 * ((threadIdx.x >> 3) & 15);
+    c.ok = mn < Mtot;
+    const int tap = c.ok ? (int)fc.div((uint32_t)mn) : 0;
+    c.ci = mn - tap * C;
+    tap_offset(tap, ntaps, c.dz, c.dy, c.dx);
+    return c;
+  }
+  AW_D void load(const Ctx &c, uint4 (&r)[kChunks], int k0, int kend) const {
+#pragma unroll
+    for (int j = 0; j < kChunks; ++j) {
+      const int k = k0 + (threadIdx.x & 7) + 8 * j;
       uint4 val = make_uint4(0, 0, 0, 0);
-      if (k < kend && mn < Mtot) {
-        const int tap = mn / C, ci = mn - tap * C;
+      if (c.ok && k < kend) {
         int b, z, y, xx;
         voxel_coords(v, k, b, z, y, xx);
-        const long src = shifted(v, b, z, y, xx, tap, ntaps, 1);
-        if (src >= 0) val = *reinterpret_cast<const uint4 *>(x + src * C + ci);
+        const int zz = z + c.dz, yy = y + c.dy, xs = xx + c.dx;
+        if (zz >= 0 && zz < v.D && yy >= 0 && yy < v.H && xs >= 0 && xs < v.W) {
+          const int src = ((b * v.D + zz) * v.H + yy) * v.W + xs;
+          val = __ldg(reinterpret_cast<const uint4 *>(x + (long)src * C + c.ci));
+        }
       }
-      *reinterpret_cast<uint4 *>(s + mnmajor_off(kk, c, kGBM)) = val;
+      r[j] = val;
     }
+  }
+  AW_D void store(uint8_t *s, const uint4 (&r)[kChunks]) const {
+#pragma unroll
+    for (int j = 0; j < kChunks; ++j)
+      *reinterpret_cast<uint4 *>(s + mnmajor_off((threadIdx.x & 7) + 8 * j,
+                                                 (threadIdx.x >> 3) & 15, kGBM)) = r[j];
   }
 };
 
-// B of wgrad: rows = co < BN, K = voxels; MN-major (dY's channels contiguous)
+// B of wgrad: rows = co < BN, K = voxels; MN-major (dY's channels
+// contiguous). Chunk i = tid + 128 q: voxel i / (BN/8), channel chunk i % (BN/8).
 template <int BN>
 struct LoadWgradB {
   const bf16 *dy;  // [voxels][BN]
-  static constexpr int kMN = 1;
-  AW_D void fill(uint8_t *s, int k0, int kend) const {
-    for (int i = threadIdx.x; i < kGBK * (BN / 8); i += kGThreads) {
+  static constexpr int kMN = 1, kChunks = kGBK * (BN / 8) / kGThreads;
+  static_assert(kGBK * (BN / 8) % kGThreads == 0, "whole chunks per thread");
+  AW_D void load(uint4 (&r)[kChunks], int k0, int kend) const {
+#pragma unroll
+    for (int q = 0; q < kChunks; ++q) {
+      const int i = threadIdx.x + kGThreads * q;
       const int kk = i / (BN / 8), c = i % (BN / 8);
       const int k = k0 + kk;
-      uint4 val = make_uint4(0, 0, 0, 0);
-      if (k < kend) val = *reinterpret_cast<const uint4 *>(dy + (long)k * BN + 8 * c);
-      *reinterpret_cast<uint4 *>(s + mnmajor_off(kk, c, BN)) = val;
+      r[q] = k < kend ? __ldg(reinterpret_cast<const uint4 *>(dy + (long)k * BN + 8 * c))
+                      : make_uint4(0, 0, 0, 0);
+    }
+  }
+  AW_D void store(uint8_t *s, const uint4 (&r)[kChunks]) const {
+#pragma unroll
+    for (int q = 0; q < kChunks; ++q) {
+      const int i = threadIdx.x + kGThreads * q;
+      *reinterpret_cast<uint4 *>(s + mnmajor_off(i / (BN / 8), i % (BN / 8), BN)) = r[q];
     }
   }
 };
@@ -214,6 +294,20 @@ struct EpiMask {
   }
 };
 
+// split K of forward / dgrad: FP32 partial of this split, [split][M][BN]
+template <int BN>
+struct EpiPartial {
+  float *part;
+  long M;
+  AW_D void store(long m, int n0, const float (&v)[16]) const {
+    if (m >= M) return;
+    float *p = part + ((long)blockIdx.y * M + m) * BN + n0;
+#pragma unroll
+    for (int i = 0; i < 16; i += 4)
+      *reinterpret_cast<float4 *>(p + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+  }
+};
+
 // wgrad: FP32 partial of this K split, stored [split][co][(tap,ci)]
 template <int BN>
 struct EpiWgrad {
@@ -265,15 +359,27 @@ __global__ void __launch_bounds__(kGThreads)
 
   uint32_t phase[2] = {0u, 0u};
   bool ok = true;
+  // registers carry the next step's chunks while the current one is stored
+  // and multiplied
+  const typename LA::Ctx ca = la.init(m0);
+  uint4 ra[LA::kChunks], rb[LB::kChunks];
+  if (nsteps > 0) {
+    la.load(ca, ra, kbeg, kend);
+    lb.load(rb, kbeg, kend);
+  }
   for (int s = 0; s < nsteps; ++s) {
     const int st = s & 1;
     if (s >= 2) {  // the MMAs that read this stage two steps ago are done
       ok = mbar_wait(&mbar[st], phase[st], status) && ok;
       phase[st] ^= 1u;
     }
-    const int k0 = kbeg + s * kGBK;
-    la.fill(sA[st], m0, k0, kend);
-    lb.fill(sB[st], k0, kend);
+    la.store(sA[st], ra);
+    lb.store(sB[st], rb);
+    if (s + 1 < nsteps) {
+      const int k1 = kbeg + (s + 1) * kGBK;
+      la.load(ca, ra, k1, kend);
+      lb.load(rb, k1, kend);
+    }
     fence_async_smem();  // the tensor core reads what the threads wrote
     __syncthreads();
     if (tid == 0) {
@@ -340,20 +446,39 @@ bool dispatch_bn(int n, F &&f) {
 constexpr int kEw = 256;
 inline unsigned ew_grid(long n) { return (unsigned)((n + kEw - 1) / kEw); }
 
+// the sum of split-K partials [splits][M][N] in split order, then the
+// forward epilogue (+ bias, ReLU, BF16 or FP32) or the dgrad one (mask)
+__global__ void k_splitk_finish(const float *__restrict__ part, int splits, long M, int N,
+                                const float *__restrict__ bias, int relu, bf16 *__restrict__ out,
+                                float *__restrict__ outf, const bf16 *__restrict__ mask) {
+  const long i = (long)blockIdx.x * kEw + threadIdx.x;
+  if (i >= M * N) return;
+  float t = 0.0f;
+  for (int k = 0; k < splits; ++k) t += part[k * M * N + i];
+  const int n = (int)(i % N);
+  if (bias) t += bias[n];
+  if (relu) t = fmaxf(t, 0.0f);
+  if (mask && !(__bfloat162float(mask[i]) > 0.0f)) t = 0.0f;
+  if (outf)
+    outf[i] = t;
+  else
+    out[i] = __float2bfloat16_rn(t);
+}
+
 // 2x2x2 average pooling, channels last; backward spreads dY / 8
 __global__ void k_pool_fwd(const bf16 *__restrict__ x, bf16 *__restrict__ y, Vol vo, int C) {
   const long i = (long)blockIdx.x * kEw + threadIdx.x;  // over output voxels * C
   if (i >= vo.voxels() * C) return;
   const int c = (int)(i % C);
   int b, z, yy, xx;
-  voxel_coords(vo, i / C, b, z, yy, xx);
-  const Vol vi{vo.B, 2 * vo.D, 2 * vo.H, 2 * vo.W};
+  voxel_coords(vo, (int)(i / C), b, z, yy, xx);
+  const int viD = 2 * vo.D, viH = 2 * vo.H, viW = 2 * vo.W;
   float s = 0.0f;
   for (int dz = 0; dz < 2; ++dz)
     for (int dy = 0; dy < 2; ++dy)
       for (int dx = 0; dx < 2; ++dx)
         s += __bfloat162float(
-            x[((((long)b * vi.D + 2 * z + dz) * vi.H + 2 * yy + dy) * vi.W + 2 * xx + dx) * C + c]);
+            x[((((long)b * viD + 2 * z + dz) * viH + 2 * yy + dy) * viW + 2 * xx + dx) * C + c]);
   y[i] = __float2bfloat16_rn(0.125f * s);
 }
 // backward: dx = (dy / 8 + add) where mask > 0 (mask: the pooled
@@ -364,7 +489,7 @@ __global__ void k_pool_bwd(const bf16 *__restrict__ dy, bf16 *__restrict__ dx, V
   if (i >= vi.voxels() * C) return;
   const int c = (int)(i % C);
   int b, z, y, x;
-  voxel_coords(vi, i / C, b, z, y, x);
+  voxel_coords(vi, (int)(i / C), b, z, y, x);
   const Vol vo{vi.B, vi.D / 2, vi.H / 2, vi.W / 2};
   float g = 0.125f * __bfloat162float(dy[((((long)b * vo.D + z / 2) * vo.H + y / 2) * vo.W + x / 2) * C + c]);
   if (add) g += __bfloat162float(add[i]);
@@ -380,7 +505,7 @@ __global__ void k_up_fwd(const bf16 *__restrict__ x, bf16 *__restrict__ y, Vol v
   const int c = (int)(i % C);
   const long m = i / C;
   int b, z, yy, xx;
-  voxel_coords(vo, m, b, z, yy, xx);
+  voxel_coords(vo, (int)m, b, z, yy, xx);
   const Vol vi{vo.B, vo.D / 2, vo.H / 2, vo.W / 2};
   y[m * Ct + c0 + c] = x[((((long)b * vi.D + z / 2) * vi.H + yy / 2) * vi.W + xx / 2) * C + c];
 }
@@ -390,7 +515,7 @@ __global__ void k_up_bwd(const bf16 *__restrict__ dy, bf16 *__restrict__ dx, Vol
   if (i >= vi.voxels() * C) return;
   const int c = (int)(i % C);
   int b, z, y, x;
-  voxel_coords(vi, i / C, b, z, y, x);
+  voxel_coords(vi, (int)(i / C), b, z, y, x);
   const Vol vo{vi.B, 2 * vi.D, 2 * vi.H, 2 * vi.W};
   float s = 0.0f;
   for (int dz = 0; dz < 2; ++dz)
@@ -485,18 +610,30 @@ __global__ void k_reduce_splits(const float *__restrict__ part, int splits, long
   for (int k = 0; k < splits; ++k) s += part[k * n + i];
   dw[i] = s;
 }
-// bias gradient: column sums of dY [M][N], one block per column
-__global__ void k_bias_grad(const bf16 *__restrict__ dy, long M, int N, float *__restrict__ db) {
-  const int n = blockIdx.x;
+// bias gradient: column sums of dY [M][N]; block b sums rows
+// [b*kBiasRows, (b+1)*kBiasRows) into part[b][N], then one block adds the
+// partials in block order
+constexpr int kBiasRows = 512;
+__global__ void k_bias_partial(const bf16 *__restrict__ dy, long M, int N, float *__restrict__ part) {
+  const int groups = kEw / N;
+  const int n = threadIdx.x % N, g = threadIdx.x / N;
+  const long r0 = (long)blockIdx.x * kBiasRows, r1 = min(M, r0 + kBiasRows);
   float s = 0.0f;
-  for (long m = threadIdx.x; m < M; m += blockDim.x) s += __bfloat162float(dy[m * N + n]);
-  __shared__ float ws[32];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  if (g < groups)
+    for (long m = r0 + g; m < r1; m += groups) s += __bfloat162float(dy[m * N + n]);
+  __shared__ float sh[kEw];
+  sh[threadIdx.x] = s;
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < N) {
     float t = 0.0f;
-    for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) t += ws[w];
+    for (int gg = 0; gg < groups; ++gg) t += sh[gg * N + threadIdx.x];
+    part[(long)blockIdx.x * N + threadIdx.x] = t;
+  }
+}
+__global__ void k_bias_final(const float *__restrict__ part, int nb, int N, float *__restrict__ db) {
+  for (int n = threadIdx.x; n < N; n += blockDim.x) {
+    float t = 0.0f;
+    for (int b = 0; b < nb; ++b) t += part[(long)b * N + n];
     db[n] = t;
   }
 }
@@ -534,7 +671,7 @@ __global__ void k_disp_to_h(const float *__restrict__ pred, Vol v, float *__rest
   const long m = (long)blockIdx.x * kEw + threadIdx.x;
   if (m >= v.voxels()) return;
   int b, z, y, x;
-  voxel_coords(v, m, b, z, y, x);
+  voxel_coords(v, (int)m, b, z, y, x);
   hx[m] = (float)x + pred[m * 16 + 0];
   hy[m] = (float)y + pred[m * 16 + 1];
   hz[m] = (float)z + pred[m * 16 + 2];
@@ -545,38 +682,82 @@ __global__ void k_disp_to_h(const float *__restrict__ pred, Vol v, float *__rest
 // ---- host entry points (called from capi.cu) ---------------------------------
 bool nn_channels_ok(int c) { return dispatch_bn(c, [](auto) {}); }
 
-cudaError_t nn_conv_fwd(const void *x, int B, int D, int H, int W, int cin, const void *w,
-                        const float *bias, int cout, int ntaps, int relu, void *out,
-                        float *outf, int *status, cudaStream_t s) {
-  const Vol v{B, D, H, W};
-  const long M = (long)B * D * H * W;
-  const int K = ntaps * cin;
+// K splits for a GEMM of `mtiles` row tiles and `ksteps` 64-deep steps:
+// about four CTAs per SM, at least two steps per split
+inline int choose_splits(long mtiles, int ksteps, int sms) {
+  const long target = 4L * sms;  // CTAs
+  if (mtiles * 2 > target) return 1;
+  long want = (target + mtiles - 1) / mtiles;
+  long maxs = ksteps / 2;
+  long sp = want < maxs ? want : maxs;
+  return sp < 1 ? 1 : (int)sp;
+}
+
+size_t nn_splitk_floats(long M, int N, int K) {
+  const int sp = choose_splits((M + kGBM - 1) / kGBM, (K + kGBK - 1) / kGBK, 148);
+  return sp > 1 ? (size_t)sp * M * N : 0;
+}
+
+// the conv GEMM of forward (sign +1) or dgrad (-1), split over K when the
+// row tiles alone cannot fill the GPU and the scratch allows
+template <class EPI_DIRECT>
+cudaError_t conv_gemm(const void *a, const Vol &v, int ca, int ntaps, int sign, const void *b,
+                      int N, long M, const float *bias, int relu, void *out, float *outf,
+                      const void *mask, float *scratch, size_t scratch_floats, int *status,
+                      cudaStream_t s) {
+  const int K = ntaps * ca;
+  int sms = 148;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long mtiles = (M + kGBM - 1) / kGBM;
+  const int ksteps = (K + kGBK - 1) / kGBK;
+  int splits = choose_splits(mtiles, ksteps, sms);
+  const int per = ((ksteps + splits - 1) / splits) * kGBK;
+  splits = (K + per - 1) / per;
+  if (splits > 1 && (!scratch || scratch_floats < (size_t)splits * M * N)) splits = 1;
   cudaError_t e = cudaErrorInvalidValue;
-  dispatch_bn(cout, [&](auto BNc) {
+  dispatch_bn(N, [&](auto BNc) {
     constexpr int BN = decltype(BNc)::value;
-    LoadConvA la{static_cast<const bf16 *>(x), v, cin, ntaps, 1, M};
-    LoadRowsB<BN> lb{static_cast<const bf16 *>(w), K};
-    EpiAct<BN> ep{bias, static_cast<bf16 *>(out), outf, relu, M};
-    e = launch_gemm<BN>(la, lb, ep, M, K, 1, K, status, s);
+    LoadConvA la{static_cast<const bf16 *>(a), v, ca, ntaps, sign, (int)M, make_fastdiv(ca)};
+    LoadRowsB<BN> lb{static_cast<const bf16 *>(b), K};
+    if (splits > 1) {
+      EpiPartial<BN> ep{scratch, M};
+      e = launch_gemm<BN>(la, lb, ep, M, K, splits, per, status, s);
+      if (e == cudaSuccess) {
+        k_splitk_finish<<<ew_grid(M * BN), kEw, 0, s>>>(
+            scratch, splits, M, BN, bias, relu, static_cast<bf16 *>(out), outf,
+            static_cast<const bf16 *>(mask));
+        e = cudaGetLastError();
+      }
+    } else if (EPI_DIRECT::kForward) {
+      EpiAct<BN> ep{bias, static_cast<bf16 *>(out), outf, relu, M};
+      e = launch_gemm<BN>(la, lb, ep, M, K, 1, K, status, s);
+    } else {
+      EpiMask<BN> ep{static_cast<const bf16 *>(mask), static_cast<bf16 *>(out), M};
+      e = launch_gemm<BN>(la, lb, ep, M, K, 1, K, status, s);
+    }
   });
   return e;
 }
+struct FwdTag { static constexpr bool kForward = true; };
+struct DgradTag { static constexpr bool kForward = false; };
+
+cudaError_t nn_conv_fwd(const void *x, int B, int D, int H, int W, int cin, const void *w,
+                        const float *bias, int cout, int ntaps, int relu, void *out,
+                        float *outf, float *scratch, size_t scratch_floats, int *status,
+                        cudaStream_t s) {
+  const long M = (long)B * D * H * W;
+  return conv_gemm<FwdTag>(x, make_vol(B, D, H, W), cin, ntaps, 1, w, cout, M, bias, relu, out,
+                           outf, nullptr, scratch, scratch_floats, status, s);
+}
 
 cudaError_t nn_conv_dgrad(const void *dy, int B, int D, int H, int W, int cout, const void *wt,
-                          int cin, int ntaps, const void *mask, void *dx, int *status,
-                          cudaStream_t s) {
-  const Vol v{B, D, H, W};
+                          int cin, int ntaps, const void *mask, void *dx, float *scratch,
+                          size_t scratch_floats, int *status, cudaStream_t s) {
   const long M = (long)B * D * H * W;
-  const int K = ntaps * cout;
-  cudaError_t e = cudaErrorInvalidValue;
-  dispatch_bn(cin, [&](auto BNc) {
-    constexpr int BN = decltype(BNc)::value;
-    LoadConvA la{static_cast<const bf16 *>(dy), v, cout, ntaps, -1, M};
-    LoadRowsB<BN> lb{static_cast<const bf16 *>(wt), K};
-    EpiMask<BN> ep{static_cast<const bf16 *>(mask), static_cast<bf16 *>(dx), M};
-    e = launch_gemm<BN>(la, lb, ep, M, K, 1, K, status, s);
-  });
-  return e;
+  return conv_gemm<DgradTag>(dy, make_vol(B, D, H, W), cout, ntaps, -1, wt, cin, M, nullptr, 0,
+                             dx, nullptr, mask, scratch, scratch_floats, status, s);
 }
 
 size_t nn_wgrad_part_floats(int cin, int cout, int ntaps, int splits) {
@@ -586,7 +767,7 @@ size_t nn_wgrad_part_floats(int cin, int cout, int ntaps, int splits) {
 cudaError_t nn_conv_wgrad(const void *x, const void *dy, int B, int D, int H, int W, int cin,
                           int cout, int ntaps, int splits, float *part, float *dw, int *status,
                           cudaStream_t s) {
-  const Vol v{B, D, H, W};
+  const Vol v = make_vol(B, D, H, W);
   const long voxels = (long)B * D * H * W;
   const int Mtot = ntaps * cin;
   long per = (voxels + splits - 1) / splits;
@@ -595,7 +776,7 @@ cudaError_t nn_conv_wgrad(const void *x, const void *dy, int B, int D, int H, in
   cudaError_t e = cudaErrorInvalidValue;
   dispatch_bn(cout, [&](auto BNc) {
     constexpr int BN = decltype(BNc)::value;
-    LoadWgradA la{static_cast<const bf16 *>(x), v, cin, ntaps, Mtot};
+    LoadWgradA la{static_cast<const bf16 *>(x), v, cin, ntaps, Mtot, make_fastdiv(cin)};
     LoadWgradB<BN> lb{static_cast<const bf16 *>(dy)};
     EpiWgrad<BN> ep{part, Mtot};
     e = launch_gemm<BN>(la, lb, ep, Mtot, (int)voxels, splits, (int)per, status, s);
@@ -606,8 +787,14 @@ cudaError_t nn_conv_wgrad(const void *x, const void *dy, int B, int D, int H, in
   return cudaGetLastError();
 }
 
-cudaError_t nn_bias_grad(const void *dy, long M, int N, float *db, cudaStream_t s) {
-  k_bias_grad<<<N, 256, 0, s>>>(static_cast<const bf16 *>(dy), M, N, db);
+size_t nn_bias_scratch_floats(long M, int N) {
+  return (size_t)((M + kBiasRows - 1) / kBiasRows) * N;
+}
+
+cudaError_t nn_bias_grad(const void *dy, long M, int N, float *scratch, float *db, cudaStream_t s) {
+  const int nb = (int)((M + kBiasRows - 1) / kBiasRows);
+  k_bias_partial<<<nb, kEw, 0, s>>>(static_cast<const bf16 *>(dy), M, N, scratch);
+  k_bias_final<<<1, 256, 0, s>>>(scratch, nb, N, db);
   return cudaGetLastError();
 }
 
@@ -615,11 +802,11 @@ cudaError_t nn_pool(const void *in, int B, int D, int H, int W, int C, void *out
                     const void *add, const void *mask, cudaStream_t s) {
   // forward: (D,H,W) is the input grid; backward: the input-gradient grid
   if (!backward) {
-    const Vol vo{B, D / 2, H / 2, W / 2};
+    const Vol vo = make_vol(B, D / 2, H / 2, W / 2);
     k_pool_fwd<<<ew_grid(vo.voxels() * C), kEw, 0, s>>>(static_cast<const bf16 *>(in),
                                                         static_cast<bf16 *>(out), vo, C);
   } else {
-    const Vol vi{B, D, H, W};
+    const Vol vi = make_vol(B, D, H, W);
     k_pool_bwd<<<ew_grid(vi.voxels() * C), kEw, 0, s>>>(static_cast<const bf16 *>(in),
                                                         static_cast<bf16 *>(out), vi, C,
                                                         static_cast<const bf16 *>(add),
@@ -631,8 +818,8 @@ cudaError_t nn_pool(const void *in, int B, int D, int H, int W, int C, void *out
 cudaError_t nn_upsample(const void *in, int B, int D, int H, int W, int C, void *out, int Ct,
                         int c0, int backward, cudaStream_t s) {
   // (D,H,W) is the coarse grid in both directions
-  const Vol vc{B, D, H, W};
-  const Vol vf{B, 2 * D, 2 * H, 2 * W};
+  const Vol vc = make_vol(B, D, H, W);
+  const Vol vf = make_vol(B, 2 * D, 2 * H, 2 * W);
   if (!backward)
     k_up_fwd<<<ew_grid(vf.voxels() * C), kEw, 0, s>>>(static_cast<const bf16 *>(in),
                                                       static_cast<bf16 *>(out), vf, C, Ct, c0);
@@ -682,7 +869,7 @@ cudaError_t nn_weights_bf16(const float *w, int cout, int ntaps, int cin, void *
 
 cudaError_t nn_disp_to_h(const float *pred, int D, int H, int W, float *hx, float *hy, float *hz,
                          cudaStream_t s) {
-  const Vol v{1, D, H, W};
+  const Vol v = make_vol(1, D, H, W);
   k_disp_to_h<<<ew_grid(v.voxels()), kEw, 0, s>>>(pred, v, hx, hy, hz);
   return cudaGetLastError();
 }

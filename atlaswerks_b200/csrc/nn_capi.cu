@@ -9,17 +9,19 @@
 
 namespace aw {
 bool nn_channels_ok(int c);
+size_t nn_splitk_floats(long M, int N, int K);
 cudaError_t nn_conv_fwd(const void *x, int B, int D, int H, int W, int cin, const void *w,
                         const float *bias, int cout, int ntaps, int relu, void *out, float *outf,
-                        int *status, cudaStream_t s);
+                        float *scratch, size_t scratch_floats, int *status, cudaStream_t s);
 cudaError_t nn_conv_dgrad(const void *dy, int B, int D, int H, int W, int cout, const void *wt,
-                          int cin, int ntaps, const void *mask, void *dx, int *status,
-                          cudaStream_t s);
+                          int cin, int ntaps, const void *mask, void *dx, float *scratch,
+                          size_t scratch_floats, int *status, cudaStream_t s);
 size_t nn_wgrad_part_floats(int cin, int cout, int ntaps, int splits);
 cudaError_t nn_conv_wgrad(const void *x, const void *dy, int B, int D, int H, int W, int cin,
                           int cout, int ntaps, int splits, float *part, float *dw, int *status,
                           cudaStream_t s);
-cudaError_t nn_bias_grad(const void *dy, long M, int N, float *db, cudaStream_t s);
+size_t nn_bias_scratch_floats(long M, int N);
+cudaError_t nn_bias_grad(const void *dy, long M, int N, float *scratch, float *db, cudaStream_t s);
 cudaError_t nn_pool(const void *in, int B, int D, int H, int W, int C, void *out, int backward,
                     const void *add, const void *mask, cudaStream_t s);
 cudaError_t nn_upsample(const void *in, int B, int D, int H, int W, int C, void *out, int Ct,
@@ -83,9 +85,18 @@ bool grid_ok(int B, int D, int H, int W) { return B >= 1 && D >= 1 && H >= 1 && 
 
 extern "C" {
 
+size_t aw_nn_conv3d_scratch_floats(int B, int D, int H, int W, int cin, int cout, int ntaps) {
+  // the larger of the forward (N = cout, K = taps cin) and dgrad (N = cin,
+  // K = taps cout) split-K partials
+  const long M = (long)B * D * H * W;
+  const size_t a = aw::nn_splitk_floats(M, cout, ntaps * cin);
+  const size_t b = aw::nn_splitk_floats(M, cin, ntaps * cout);
+  return a > b ? a : b;
+}
+
 int aw_nn_conv3d_fwd(const void *x, int B, int D, int H, int W, int cin, const void *w,
                      const float *bias, int cout, int ntaps, int relu, void *out_bf16,
-                     float *out_f32, void *stream) {
+                     float *out_f32, float *scratch, size_t scratch_floats, void *stream) {
   if (!x || !w || (!out_bf16 && !out_f32)) return nfail("aw_nn_conv3d_fwd: null pointer");
   if (!grid_ok(B, D, H, W)) return nfail("aw_nn_conv3d_fwd: empty grid");
   if (cin % 16 || cin <= 0) return nfail("aw_nn_conv3d_fwd: input channels must be a multiple of 16");
@@ -94,14 +105,15 @@ int aw_nn_conv3d_fwd(const void *x, int B, int D, int H, int W, int cin, const v
   if (ntaps != 27 && ntaps != 1) return nfail("aw_nn_conv3d_fwd: taps must be 27 (3x3x3) or 1");
   int *st = nullptr;
   if (int rc = status_word(&st)) return rc;
-  NN_CUDA(aw::nn_conv_fwd(x, B, D, H, W, cin, w, bias, cout, ntaps, relu, out_bf16, out_f32, st,
-                          S(stream)),
+  NN_CUDA(aw::nn_conv_fwd(x, B, D, H, W, cin, w, bias, cout, ntaps, relu, out_bf16, out_f32,
+                          scratch, scratch_floats, st, S(stream)),
           "aw_nn_conv3d_fwd");
   return 0;
 }
 
 int aw_nn_conv3d_dgrad(const void *dy, int B, int D, int H, int W, int cout, const void *wt,
-                       int cin, int ntaps, const void *mask, void *dx, void *stream) {
+                       int cin, int ntaps, const void *mask, void *dx, float *scratch,
+                       size_t scratch_floats, void *stream) {
   if (!dy || !wt || !dx) return nfail("aw_nn_conv3d_dgrad: null pointer");
   if (!grid_ok(B, D, H, W)) return nfail("aw_nn_conv3d_dgrad: empty grid");
   if (cout % 16 || cout <= 0) return nfail("aw_nn_conv3d_dgrad: output channels must be a multiple of 16");
@@ -110,7 +122,8 @@ int aw_nn_conv3d_dgrad(const void *dy, int B, int D, int H, int W, int cout, con
   if (ntaps != 27 && ntaps != 1) return nfail("aw_nn_conv3d_dgrad: taps must be 27 or 1");
   int *st = nullptr;
   if (int rc = status_word(&st)) return rc;
-  NN_CUDA(aw::nn_conv_dgrad(dy, B, D, H, W, cout, wt, cin, ntaps, mask, dx, st, S(stream)),
+  NN_CUDA(aw::nn_conv_dgrad(dy, B, D, H, W, cout, wt, cin, ntaps, mask, dx, scratch,
+                            scratch_floats, st, S(stream)),
           "aw_nn_conv3d_dgrad");
   return 0;
 }
@@ -136,9 +149,12 @@ int aw_nn_conv3d_wgrad(const void *x, const void *dy, int B, int D, int H, int W
   return 0;
 }
 
-int aw_nn_bias_grad(const void *dy, long M, int cout, float *db, void *stream) {
-  if (!dy || !db) return nfail("aw_nn_bias_grad: null pointer");
-  NN_CUDA(aw::nn_bias_grad(dy, M, cout, db, S(stream)), "aw_nn_bias_grad");
+size_t aw_nn_bias_scratch_floats(long M, int cout) { return aw::nn_bias_scratch_floats(M, cout); }
+
+int aw_nn_bias_grad(const void *dy, long M, int cout, float *scratch, float *db, void *stream) {
+  if (!dy || !db || !scratch) return nfail("aw_nn_bias_grad: null pointer");
+  if (cout < 1 || cout > 256) return nfail("aw_nn_bias_grad: 1..256 channels");
+  NN_CUDA(aw::nn_bias_grad(dy, M, cout, scratch, db, S(stream)), "aw_nn_bias_grad");
   return 0;
 }
 

@@ -113,13 +113,20 @@ class WarmStartNet:
         self.dout = bf(0, 16)
         L = _lib.lib()
         self.splits = {}
-        need = 0
+        need, cneed = 0, 0
         for name, ci, co, t in LAYERS:
             lvl = self._level_of(name)
-            s = max(1, min(64, self._vox(lvl) // 2048))
+            vox = self._vox(lvl)
+            # weight gradient: K = voxels split so that ~8 CTAs per SM run
+            mtiles = -(-t * ci // 128)
+            s = max(1, min(vox // 512, -(-1184 // mtiles)))
             self.splits[name] = s
             need = max(need, L.aw_nn_wgrad_scratch_floats(ci, co, t, s))
+            cneed = max(cneed, L.aw_nn_conv3d_scratch_floats(1, *self._grid(lvl), ci, co, t))
         self.wscratch = torch.zeros(int(need), device=self.dev)
+        self.cscratch = torch.zeros(max(1, int(cneed)), device=self.dev)
+        self.bscratch = torch.zeros(int(L.aw_nn_bias_scratch_floats(self._vox(0), 192)),
+                                    device=self.dev)
         self.mse_scratch = torch.zeros(int(L.aw_nn_mse_scratch_doubles(self._vox(0))),
                                        dtype=torch.float64, device=self.dev)
         self.loss = torch.zeros(1, device=self.dev)
@@ -140,7 +147,7 @@ class WarmStartNet:
         d, h, w = self._grid(lvl)
         check(_lib.lib().aw_nn_conv3d_fwd(_p(x), 1, d, h, w, ci, _p(self.wb[name]),
                                           _p(self.b[name]), co, t, int(relu), _p(out), _p(outf),
-                                          _stream()))
+                                          _p(self.cscratch), self.cscratch.numel(), _stream()))
 
     def _pool(self, src, lvl_fine, c, dst):
         d, h, w = self._grid(lvl_fine)
@@ -192,10 +199,11 @@ class WarmStartNet:
         L, s = _lib.lib(), _stream()
         check(L.aw_nn_conv3d_wgrad(_p(inp), _p(dy), 1, d, h, w, ci, co, t, self.splits[name],
                                    _p(self.wscratch), _p(self.gw[name]), s))
-        check(L.aw_nn_bias_grad(_p(dy), self._vox(lvl), co, _p(self.gb[name]), s))
+        check(L.aw_nn_bias_grad(_p(dy), self._vox(lvl), co, _p(self.bscratch), _p(self.gb[name]),
+                                s))
         if dx is not None:
             check(L.aw_nn_conv3d_dgrad(_p(dy), 1, d, h, w, co, _p(self.wt[name]), ci, t, _p(mask),
-                                       _p(dx), s))
+                                       _p(dx), _p(self.cscratch), self.cscratch.numel(), s))
 
     def _pool_bwd(self, dp, lvl_fine, c, add, mask, dst):
         d, h, w = self._grid(lvl_fine)
@@ -306,7 +314,7 @@ def solver_target(I0: torch.Tensor, I1: torch.Tensor, iters: int = 50,
 
 
 def refine(I0: torch.Tensor, I1: torch.Tensor, h0: torch.Tensor, target: float,
-           max_iters: int = 50, chunk: int = 5, max_pert: float = 0.5):
+           max_iters: int = 50, chunk: int = 5, max_pert: float = 0.5, it=None, data=None):
     """Greedy refinement from h0 until the iteration energy (the mismatch
     sum (I1 - I0(h))^2 of the deformation entering an iteration, recorded
     on the device) is <= target, in chunks of `chunk` graph-replayed
@@ -314,8 +322,8 @@ def refine(I0: torch.Tensor, I1: torch.Tensor, h0: torch.Tensor, target: float,
     energies, reached, fell); `fell` is False when a chunk did not lower the
     energy — the signal to fall back to the plain solve from the identity."""
     from .greedy import GreedyDeformationDataB200
-    it = _greedy(tuple(I0.shape), max_pert)
-    data = GreedyDeformationDataB200(I0, I1)
+    it = it or _greedy(tuple(I0.shape), max_pert)
+    data = data or GreedyDeformationDataB200(I0, I1)
     data.Def1To0().copy_(h0)
     done = 0
     en = np.zeros(0)
@@ -363,6 +371,9 @@ def evaluate(net: "WarmStartNet", pairs, plain_iters: int = 50, tol: float = 0.0
         shape = tuple(I0.shape)
         it = _greedy(shape, max_pert)
         data = GreedyDeformationDataB200(I0, I1)
+        # the warm path's handles exist before its clock starts, as the plain one's do
+        it_w, data_w = _greedy(shape, max_pert), GreedyDeformationDataB200(I0, I1)
+        it2, d2 = _greedy(shape, max_pert), GreedyDeformationDataB200(I0, I1)
         torch.cuda.synchronize()
         ev[0].record()
         it.Run(data, plain_iters, update_first=True)
@@ -372,11 +383,10 @@ def evaluate(net: "WarmStartNet", pairs, plain_iters: int = 50, tol: float = 0.0
         target = float(e_plain[-1]) * (1.0 + tol)
         ev[2].record()
         h0 = net.predict_h(I0, I1)
-        h, k, en, reached, fell = refine(I0, I1, h0, target, plain_iters, chunk, max_pert)
+        h, k, en, reached, fell = refine(I0, I1, h0, target, plain_iters, chunk, max_pert,
+                                         it_w, data_w)
         fallback = not fell
         if fallback:  # the warm start did not help: the plain solve, unassisted
-            it2 = _greedy(shape, max_pert)
-            d2 = GreedyDeformationDataB200(I0, I1)
             it2.Run(d2, plain_iters, update_first=True)
             k += plain_iters
         ev[3].record()
@@ -401,22 +411,33 @@ def train(net: "WarmStartNet", pairs, targets, epochs: int = 1, lr: float = 1e-3
         order = rng.permutation(len(pairs))
         for j, i in enumerate(order):
             I0, I1 = dev_pairs[i]
-            losses.append(net.train_step(I0, I1, targets[i], lr))
+            losses.append(net.train_step(I0, I1, targets[i], lr).clone())
             if log_every and (j + 1) % log_every == 0:
                 print(f"epoch {ep} step {j + 1} loss {float(losses[-1]):.5f}", flush=True)
     torch.cuda.synchronize()
-    return [float(l) for l in losses]
+    return [float(l) for l in torch.cat(losses).cpu()]
+
+
+def _bf16_bits(a: np.ndarray) -> np.ndarray:
+    b = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    return (((b + 0x7FFF + ((b >> 16) & 1)) >> 16) & 0xFFFF).astype(np.uint16)
 
 
 def save_weights(net: "WarmStartNet", path: str):
+    """Weights as BF16 bit patterns (what the convolutions compute with),
+    biases as float32."""
     st = net.state()
-    np.savez_compressed(path, **{f"w_{k}": v for k, v in st["w"].items()},
+    np.savez_compressed(path, **{f"w_{k}": _bf16_bits(v) for k, v in st["w"].items()},
                         **{f"b_{k}": v for k, v in st["b"].items()})
 
 
 def load_weights(net: "WarmStartNet", path: str):
     z = np.load(path)
-    net.load({"w": {k: z[f"w_{k}"] for k in net.w}, "b": {k: z[f"b_{k}"] for k in net.b}})
+    w = {}
+    for k in net.w:
+        a = z[f"w_{k}"]
+        w[k] = (a.astype(np.uint32) << 16).view(np.float32) if a.dtype == np.uint16 else a
+    net.load({"w": w, "b": {k: z[f"b_{k}"] for k in net.b}})
 
 
 def main(argv=None):

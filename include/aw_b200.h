@@ -264,22 +264,29 @@ int aw_ldmm_get_energies(aw_ldmm_t l, double *out, int max_count, int *count);
  * the data gradient takes the transposed copy [Cin][taps][Cout] that
  * aw_nn_weights_bf16 writes. Output channels: 16 32 48 64 96 128 192.
  * ------------------------------------------------------------------------- */
+/* Grids too small to fill the GPU with 128-voxel row tiles split K over
+ * CTAs; the FP32 partials go to `scratch` (at least
+ * aw_nn_conv3d_scratch_floats floats; NULL or smaller = no split). */
+size_t aw_nn_conv3d_scratch_floats(int B, int D, int H, int W, int cin, int cout, int ntaps);
 /* out = act(conv(x, w) + bias): BF16 out_bf16, or FP32 out_f32 when given */
 int aw_nn_conv3d_fwd(const void *x, int B, int D, int H, int W, int cin, const void *w,
                      const float *bias, int cout, int ntaps, int relu, void *out_bf16,
-                     float *out_f32, void *stream);
+                     float *out_f32, float *scratch, size_t scratch_floats, void *stream);
 /* dx = conv^T(dy, w) times (mask > 0) (the ReLU derivative of the layer's
  * input, which is a post-ReLU activation); mask NULL = no mask */
 int aw_nn_conv3d_dgrad(const void *dy, int B, int D, int H, int W, int cout, const void *wt,
-                       int cin, int ntaps, const void *mask, void *dx, void *stream);
+                       int cin, int ntaps, const void *mask, void *dx, float *scratch,
+                       size_t scratch_floats, void *stream);
 /* dw [Cout][taps][Cin] (FP32) = sum over voxels of dy x shifted x; the
  * voxel sum is split over `splits` CTA columns whose partials go to
  * scratch (aw_nn_wgrad_scratch_floats floats) and are summed in order */
 size_t aw_nn_wgrad_scratch_floats(int cin, int cout, int ntaps, int splits);
 int aw_nn_conv3d_wgrad(const void *x, const void *dy, int B, int D, int H, int W, int cin,
                        int cout, int ntaps, int splits, float *scratch, float *dw, void *stream);
-/* db[c] = sum over the M voxels of dy[.][c] */
-int aw_nn_bias_grad(const void *dy, long M, int cout, float *db, void *stream);
+/* db[c] = sum over the M voxels of dy[.][c], through block partials in
+ * scratch (aw_nn_bias_scratch_floats floats) added in order */
+size_t aw_nn_bias_scratch_floats(long M, int cout);
+int aw_nn_bias_grad(const void *dy, long M, int cout, float *scratch, float *db, void *stream);
 /* 2x2x2 average pooling of the (D,H,W) grid; backward (D,H,W = the fine
  * grid) spreads dy/8, adds `add` and keeps it where mask > 0 (the pooled
  * post-ReLU activation); add and mask may be NULL */

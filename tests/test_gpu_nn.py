@@ -39,9 +39,18 @@ def rel(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)
 
 
+def scratch_for(grid, cin, cout, taps, split):
+    """Split-K scratch (None: the direct, unsplit GEMM)."""
+    if not split:
+        return None, 0
+    n = int(_lib.lib().aw_nn_conv3d_scratch_floats(*grid, cin, cout, taps))
+    return torch.zeros(max(n, 1), device="cuda"), n
+
+
+@pytest.mark.parametrize("split", [False, True])
 @pytest.mark.parametrize("grid", [(1, 8, 8, 8), (1, 4, 6, 10), (2, 4, 8, 8)])
 @pytest.mark.parametrize("cin,cout,taps", CONFIGS)
-def test_conv_forward(grid, cin, cout, taps):
+def test_conv_forward(grid, cin, cout, taps, split):
     rng = np.random.default_rng(cin * 7 + cout + taps)
     B, D, H, W = grid
     x = O.bf16(rng.normal(0, 1, (B, D, H, W, cin)).astype(np.float32))
@@ -51,23 +60,26 @@ def test_conv_forward(grid, cin, cout, taps):
     # device copies held in names: a temporary's memory could be reused
     # by the next temporary before the kernel runs
     xd, wd, bd = bf(x), bf(w), torch.from_numpy(b).cuda()
+    sc, nsc = scratch_for(grid, cin, cout, taps, split)
+    scp = sc.data_ptr() if sc is not None else None
     outf = torch.zeros((B * D * H * W, cout), device="cuda")
     rc = _lib.lib().aw_nn_conv3d_fwd(xd.data_ptr(), B, D, H, W, cin, wd.data_ptr(), bd.data_ptr(),
-                                     cout, taps, 0, None, outf.data_ptr(), None)
+                                     cout, taps, 0, None, outf.data_ptr(), scp, nsc, None)
     assert rc == 0, _lib.lib().aw_last_error()
     got = f32(outf).reshape(want.shape)
     assert rel(got, want) <= 1e-3
     # BF16 output with ReLU
     outb = torch.zeros((B * D * H * W, cout), dtype=torch.bfloat16, device="cuda")
     rc = _lib.lib().aw_nn_conv3d_fwd(xd.data_ptr(), B, D, H, W, cin, wd.data_ptr(), bd.data_ptr(),
-                                     cout, taps, 1, outb.data_ptr(), None, None)
+                                     cout, taps, 1, outb.data_ptr(), None, scp, nsc, None)
     assert rc == 0
     assert rel(f32(outb).reshape(want.shape), np.maximum(want, 0)) <= 1e-2
 
 
+@pytest.mark.parametrize("split", [False, True])
 @pytest.mark.parametrize("grid", [(1, 8, 8, 8), (1, 4, 6, 10)])
 @pytest.mark.parametrize("cin,cout,taps", CONFIGS)
-def test_conv_dgrad(grid, cin, cout, taps):
+def test_conv_dgrad(grid, cin, cout, taps, split):
     rng = np.random.default_rng(cin + cout * 3 + taps)
     B, D, H, W = grid
     dy = O.bf16(rng.normal(0, 1, (B, D, H, W, cout)).astype(np.float32))
@@ -76,9 +88,11 @@ def test_conv_dgrad(grid, cin, cout, taps):
     want = O.conv_dgrad(dy, w, mask)
     wt = np.ascontiguousarray(w.transpose(2, 1, 0))
     dyd, wtd, md = bf(dy), bf(wt), bf(mask)
+    sc, nsc = scratch_for(grid, cin, cout, taps, split)
     dx = torch.zeros((B * D * H * W, cin), dtype=torch.bfloat16, device="cuda")
     rc = _lib.lib().aw_nn_conv3d_dgrad(dyd.data_ptr(), B, D, H, W, cout, wtd.data_ptr(), cin, taps,
-                                       md.data_ptr(), dx.data_ptr(), None)
+                                       md.data_ptr(), dx.data_ptr(),
+                                       sc.data_ptr() if sc is not None else None, nsc, None)
     assert rc == 0, _lib.lib().aw_last_error()
     assert rel(f32(dx).reshape(want.shape), want) <= 1e-2
 
