@@ -84,48 +84,72 @@ AW_D uint32_t kmajor_off(int r, int j, int R) { return j * (R * 16) + (r >> 3) *
 AW_D uint32_t mnmajor_off(int k, int c, int R) { return (k >> 3) * (R * 16) + c * 128 + (k & 7) * 16; }
 
 // ---- operand loaders ----------------------------------------------------------
-// Each loader moves this thread's 16-byte chunks of one 64-deep K step:
-// load() from global memory into registers (zero past kend or outside the
-// volume), store() into the stage's canonical layout. init() computes the
-// per-thread context once per CTA.
+// Each loader copies this thread's 16-byte chunks of one 64-deep K step
+// from global memory straight into the stage's canonical layout with
+// cp.async (zero-filled past kend or outside the volume; cached in L1, where
+// the 27 taps of neighbouring rows meet); init() computes the per-thread
+// context once per CTA.
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(smem_dst)),
+               "l"(gsrc), "r"(valid ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 // A of forward / dgrad: rows = voxels, K = (tap, channel) of X shifted by
 // sign * off(tap); K-major (the 8 channels of a chunk are contiguous).
-// Thread t owns row t of the tile.
+// Thread t owns row t of the tile; which taps stay inside the volume for
+// that voxel is a 27-bit mask, and the voxel-index offset of each tap a
+// table in shared memory, both made once per CTA.
 struct LoadConvA {
   const bf16 *x;
   Vol v;
   int C, ntaps, sign;
   int M;
   FastDiv fc;
-  static constexpr int kMN = 0, kChunks = kGBK / 8;
+  static constexpr int kMN = 0;
   struct Ctx {
-    int m, b, z, y, xx;
+    int m;
+    uint32_t vmask;
+    const int *toff;
   };
   AW_D Ctx init(long m0) const {
+    __shared__ int s_toff[27];
+    if (threadIdx.x < ntaps) {
+      int dz, dy, dx;
+      tap_offset(threadIdx.x, ntaps, dz, dy, dx);
+      s_toff[threadIdx.x] = sign * ((dz * v.H + dy) * v.W + dx);
+    }
     Ctx c;
     c.m = (int)m0 + threadIdx.x;
-    c.b = c.z = c.y = c.xx = 0;
-    if (c.m < M) voxel_coords(v, c.m, c.b, c.z, c.y, c.xx);
-    return c;
+    c.toff = s_toff;
+    c.vmask = 0;
+    if (c.m < M) {
+      int b, z, y, xx;
+      voxel_coords(v, c.m, b, z, y, xx);
+      for (int t = 0; t < ntaps; ++t) {
+        int dz, dy, dx;
+        tap_offset(t, ntaps, dz, dy, dx);
+        const int zz = z + sign * dz, yy = y + sign * dy, xs = xx + sign * dx;
+        if (zz >= 0 && zz < v.D && yy >= 0 && yy < v.H && xs >= 0 && xs < v.W) c.vmask |= 1u << t;
+      }
+    }
+    return c;  // the caller synchronises the CTA before the first issue()
   }
-  AW_D void load(const Ctx &c, uint4 (&r)[kChunks], int k0, int kend) const {
+  AW_D void issue(const Ctx &c, uint8_t *s, int k0, int kend) const {
     int tap = (int)fc.div((uint32_t)k0);
     int ci = k0 - tap * C;
 #pragma unroll
-    for (int j = 0; j < kChunks; ++j) {
-      const int k = k0 + 8 * j;
-      uint4 val = make_uint4(0, 0, 0, 0);
-      if (c.m < M && k < kend) {
-        int dz, dy, dx;
-        tap_offset(tap, ntaps, dz, dy, dx);
-        const int zz = c.z + sign * dz, yy = c.y + sign * dy, xs = c.xx + sign * dx;
-        if (zz >= 0 && zz < v.D && yy >= 0 && yy < v.H && xs >= 0 && xs < v.W) {
-          const int src = ((c.b * v.D + zz) * v.H + yy) * v.W + xs;
-          val = __ldg(reinterpret_cast<const uint4 *>(x + (long)src * C + ci));
-        }
-      }
-      r[j] = val;
+    for (int j = 0; j < kGBK / 8; ++j) {
+      const bool ok = ((c.vmask >> tap) & 1u) && (k0 + 8 * j < kend);
+      const bf16 *src = ok ? x + (long)(c.m + c.toff[tap]) * C + ci : x;
+      cp_async16(s + kmajor_off(threadIdx.x, j, kGBM), src, ok);
       ci += 8;
       if (ci == C) {
         ci = 0;
@@ -133,36 +157,26 @@ struct LoadConvA {
       }
     }
   }
-  AW_D void store(uint8_t *s, const uint4 (&r)[kChunks]) const {
-#pragma unroll
-    for (int j = 0; j < kChunks; ++j)
-      *reinterpret_cast<uint4 *>(s + kmajor_off(threadIdx.x, j, kGBM)) = r[j];
-  }
 };
 
 // B of forward / dgrad: rows = output columns n < N, K contiguous per row.
-// Chunk i = tid + 128 q: row i % BN, K chunk i / BN (consecutive threads
-// fill consecutive 16-byte slots of shared memory).
+// Chunk i = tid + 128 q: row i / 8, K chunk i % 8 (8 threads read one
+// row's 128 contiguous bytes).
 template <int BN>
 struct LoadRowsB {
   const bf16 *w;  // [BN][K]
   int K;
   static constexpr int kMN = 0, kChunks = BN * (kGBK / 8) / kGThreads;
   static_assert(BN * (kGBK / 8) % kGThreads == 0, "whole chunks per thread");
-  AW_D void load(uint4 (&r)[kChunks], int k0, int kend) const {
+  struct Ctx {};
+  AW_D Ctx init(long) const { return Ctx{}; }
+  AW_D void issue(const Ctx &, uint8_t *s, int k0, int kend) const {
 #pragma unroll
     for (int q = 0; q < kChunks; ++q) {
       const int i = threadIdx.x + kGThreads * q;
-      const int row = i % BN, k = k0 + 8 * (i / BN);
-      r[q] = k < kend ? __ldg(reinterpret_cast<const uint4 *>(w + (long)row * K + k))
-                      : make_uint4(0, 0, 0, 0);
-    }
-  }
-  AW_D void store(uint8_t *s, const uint4 (&r)[kChunks]) const {
-#pragma unroll
-    for (int q = 0; q < kChunks; ++q) {
-      const int i = threadIdx.x + kGThreads * q;
-      *reinterpret_cast<uint4 *>(s + kmajor_off(i % BN, i / BN, BN)) = r[q];
+      const int row = i >> 3, j = i & 7, k = k0 + 8 * j;
+      const bool ok = k < kend;
+      cp_async16(s + kmajor_off(row, j, BN), ok ? w + (long)row * K + k : w, ok);
     }
   }
 };
@@ -177,7 +191,7 @@ struct LoadWgradA {
   int C, ntaps;
   int Mtot;  // ntaps * C
   FastDiv fc;
-  static constexpr int kMN = 1, kChunks = kGBK / 8;
+  static constexpr int kMN = 1;
   struct Ctx {
     int ok, ci, dz, dy, dx;
   };
@@ -190,28 +204,37 @@ struct LoadWgradA {
     tap_offset(tap, ntaps, c.dz, c.dy, c.dx);
     return c;
   }
-  AW_D void load(const Ctx &c, uint4 (&r)[kChunks], int k0, int kend) const {
+  AW_D void issue(const Ctx &c, uint8_t *s, int k0, int kend) const {
+    // the voxel of the first chunk decoded once, then stepped by 8 along x
+    int k = k0 + (threadIdx.x & 7);
+    int b = 0, z = 0, y = 0, xx = 0;
+    if (k < kend) voxel_coords(v, k, b, z, y, xx);
 #pragma unroll
-    for (int j = 0; j < kChunks; ++j) {
-      const int k = k0 + (threadIdx.x & 7) + 8 * j;
-      uint4 val = make_uint4(0, 0, 0, 0);
+    for (int j = 0; j < kGBK / 8; ++j) {
+      const bf16 *src = x;
+      bool ok = false;
       if (c.ok && k < kend) {
-        int b, z, y, xx;
-        voxel_coords(v, k, b, z, y, xx);
         const int zz = z + c.dz, yy = y + c.dy, xs = xx + c.dx;
         if (zz >= 0 && zz < v.D && yy >= 0 && yy < v.H && xs >= 0 && xs < v.W) {
-          const int src = ((b * v.D + zz) * v.H + yy) * v.W + xs;
-          val = __ldg(reinterpret_cast<const uint4 *>(x + (long)src * C + c.ci));
+          src = x + (long)(((b * v.D + zz) * v.H + yy) * v.W + xs) * C + c.ci;
+          ok = true;
         }
       }
-      r[j] = val;
+      cp_async16(s + mnmajor_off((threadIdx.x & 7) + 8 * j, (threadIdx.x >> 3) & 15, kGBM), src,
+                 ok);
+      k += 8;
+      xx += 8;
+      while (xx >= v.W) {
+        xx -= v.W;
+        if (++y == v.H) {
+          y = 0;
+          if (++z == v.D) {
+            z = 0;
+            ++b;
+          }
+        }
+      }
     }
-  }
-  AW_D void store(uint8_t *s, const uint4 (&r)[kChunks]) const {
-#pragma unroll
-    for (int j = 0; j < kChunks; ++j)
-      *reinterpret_cast<uint4 *>(s + mnmajor_off((threadIdx.x & 7) + 8 * j,
-                                                 (threadIdx.x >> 3) & 15, kGBM)) = r[j];
   }
 };
 
@@ -222,21 +245,16 @@ struct LoadWgradB {
   const bf16 *dy;  // [voxels][BN]
   static constexpr int kMN = 1, kChunks = kGBK * (BN / 8) / kGThreads;
   static_assert(kGBK * (BN / 8) % kGThreads == 0, "whole chunks per thread");
-  AW_D void load(uint4 (&r)[kChunks], int k0, int kend) const {
+  struct Ctx {};
+  AW_D Ctx init(long) const { return Ctx{}; }
+  AW_D void issue(const Ctx &, uint8_t *s, int k0, int kend) const {
 #pragma unroll
     for (int q = 0; q < kChunks; ++q) {
       const int i = threadIdx.x + kGThreads * q;
       const int kk = i / (BN / 8), c = i % (BN / 8);
       const int k = k0 + kk;
-      r[q] = k < kend ? __ldg(reinterpret_cast<const uint4 *>(dy + (long)k * BN + 8 * c))
-                      : make_uint4(0, 0, 0, 0);
-    }
-  }
-  AW_D void store(uint8_t *s, const uint4 (&r)[kChunks]) const {
-#pragma unroll
-    for (int q = 0; q < kChunks; ++q) {
-      const int i = threadIdx.x + kGThreads * q;
-      *reinterpret_cast<uint4 *>(s + mnmajor_off(i / (BN / 8), i % (BN / 8), BN)) = r[q];
+      const bool ok = k < kend;
+      cp_async16(s + mnmajor_off(kk, c, BN), ok ? dy + (long)k * BN + 8 * c : dy, ok);
     }
   }
 };
@@ -325,20 +343,32 @@ template <int BN>
 constexpr int tmem_cols() {
   return BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
 }
+// pipeline depth: shared-memory stages of one K step each
+template <int BN>
+constexpr int gemm_stages() {
+  return 3;
+}
+template <int BN>
+constexpr size_t stage_bytes() {
+  return (size_t)kAStage + (size_t)BN * kGBK * 2;
+}
 template <int BN>
 constexpr size_t gemm_smem() {
-  return 1024 + 2 * (size_t)kAStage + 2 * (size_t)BN * kGBK * 2;
+  return 1024 + gemm_stages<BN>() * stage_bytes<BN>();
 }
 
+// One CTA: 128 rows x BN columns of D over K in [kbeg, kend). Stage s % S
+// of shared memory holds K step s; cp.async keeps S-1 steps in flight while
+// one thread issues the MMAs of the oldest, each step's MMAs committed to
+// the stage's mbarrier (phase = the step's use count of that stage).
 template <int BN, class LA, class LB, class EP>
 __global__ void __launch_bounds__(kGThreads)
     k_umma_gemm(LA la, LB lb, EP ep, int K, int k_per_split, int *status) {
+  constexpr int S = gemm_stages<BN>();
   extern __shared__ __align__(1024) uint8_t smraw[];
-  __shared__ uint64_t mbar[2];
+  __shared__ uint64_t mbar[S];
   __shared__ uint32_t tbase;
   uint8_t *base = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
-  uint8_t *sA[2] = {base, base + kAStage};
-  uint8_t *sB[2] = {base + 2 * kAStage, base + 2 * kAStage + BN * kGBK * 2};
   constexpr int TC = tmem_cols<BN>();
   constexpr uint32_t IDESC = umma_idesc_bf16(kGBM, BN, LA::kMN, LB::kMN);
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -346,45 +376,46 @@ __global__ void __launch_bounds__(kGThreads)
   const int kbeg = blockIdx.y * k_per_split;
   const int kend = min(K, kbeg + k_per_split);
   const int nsteps = kend > kbeg ? (kend - kbeg + kGBK - 1) / kGBK : 0;
+  auto sA = [&](int st) { return base + st * stage_bytes<BN>(); };
+  auto sB = [&](int st) { return base + st * stage_bytes<BN>() + kAStage; };
 
   if (warp == 0) tmem_alloc(&tbase, TC);
-  if (tid == 0) {
-    mbar_init(&mbar[0], 1);
-    mbar_init(&mbar[1], 1);
-  }
+  if (tid == 0)
+    for (int i = 0; i < S; ++i) mbar_init(&mbar[i], 1);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tbase;
 
-  uint32_t phase[2] = {0u, 0u};
-  bool ok = true;
-  // registers carry the next step's chunks while the current one is stored
-  // and multiplied
   const typename LA::Ctx ca = la.init(m0);
-  uint4 ra[LA::kChunks], rb[LB::kChunks];
-  if (nsteps > 0) {
-    la.load(ca, ra, kbeg, kend);
-    lb.load(rb, kbeg, kend);
+  const typename LB::Ctx cb = lb.init(m0);
+  __syncthreads();  // per-CTA loader tables
+  bool ok = true;
+  // steps 0 .. S-2 in flight before the loop; one commit group per step
+#pragma unroll
+  for (int p = 0; p < S - 1; ++p) {
+    if (p < nsteps) {
+      la.issue(ca, sA(p), kbeg + p * kGBK, kend);
+      lb.issue(cb, sB(p), kbeg + p * kGBK, kend);
+    }
+    cp_async_commit();
   }
   for (int s = 0; s < nsteps; ++s) {
-    const int st = s & 1;
-    if (s >= 2) {  // the MMAs that read this stage two steps ago are done
-      ok = mbar_wait(&mbar[st], phase[st], status) && ok;
-      phase[st] ^= 1u;
+    const int st = s % S;
+    const int nxt = s + S - 1;
+    if (nxt < nsteps) {
+      // stage nxt % S last held step s - 1: its MMAs must be done
+      if (s >= 1) ok = mbar_wait(&mbar[(s - 1) % S], ((s - 1) / S) & 1u, status) && ok;
+      la.issue(ca, sA(nxt % S), kbeg + nxt * kGBK, kend);
+      lb.issue(cb, sB(nxt % S), kbeg + nxt * kGBK, kend);
     }
-    la.store(sA[st], ra);
-    lb.store(sB[st], rb);
-    if (s + 1 < nsteps) {
-      const int k1 = kbeg + (s + 1) * kGBK;
-      la.load(ca, ra, k1, kend);
-      lb.load(rb, k1, kend);
-    }
-    fence_async_smem();  // the tensor core reads what the threads wrote
+    cp_async_commit();
+    cp_async_wait<S - 1>();  // this thread's copies of step s have landed
+    fence_async_smem();      // and are visible to the tensor core
     __syncthreads();
     if (tid == 0) {
       tc_fence_after();
-      const uint32_t a0 = smem_u32(sA[st]), b0 = smem_u32(sB[st]);
+      const uint32_t a0 = smem_u32(sA(st)), b0 = smem_u32(sB(st));
 #pragma unroll
       for (int kk = 0; kk < kGBK / 16; ++kk) {
         const uint64_t da = umma_desc(a0 + kk * 2 * (kGBM * 16), kGBM * 16, 128);
@@ -394,9 +425,10 @@ __global__ void __launch_bounds__(kGThreads)
       umma_commit(&mbar[st]);
     }
   }
+  cp_async_wait<0>();
   if (nsteps > 0) {
-    const int last = (nsteps - 1) & 1;
-    ok = mbar_wait(&mbar[last], phase[last], status) && ok;
+    const int last = nsteps - 1;
+    ok = mbar_wait(&mbar[last % S], (last / S) & 1u, status) && ok;
   }
   tc_fence_after();
   // epilogue: warp w owns TMEM lanes (rows) 32w .. 32w+31

@@ -314,30 +314,50 @@ def solver_target(I0: torch.Tensor, I1: torch.Tensor, iters: int = 50,
 
 
 def refine(I0: torch.Tensor, I1: torch.Tensor, h0: torch.Tensor, target: float,
-           max_iters: int = 50, chunk: int = 5, max_pert: float = 0.5, it=None, data=None):
+           max_iters: int = 50, chunk: int = 5, max_pert: float = 0.5, it=None, data=None,
+           step: Optional[float] = None, auto_reduce: bool = True):
     """Greedy refinement from h0 until the iteration energy (the mismatch
     sum (I1 - I0(h))^2 of the deformation entering an iteration, recorded
     on the device) is <= target, in chunks of `chunk` graph-replayed
-    iterations with the step set at the first. Returns (h, iterations,
-    energies, reached, fell); `fell` is False when a chunk did not lower the
-    energy — the signal to fall back to the plain solve from the identity."""
+    iterations. With `step` the iteration keeps that step size (the plain
+    solve's, from the identity); without it the step is set at the first
+    iteration from the warm start's own velocity. auto_reduce halves the
+    step whenever the energy rises (GreedyParam::AutoStepReduce), which
+    damps the oscillation of a step chosen from a small residual. Returns (h, iterations,
+    energies, reached, fell): `fell` is False when a chunk did not improve
+    on the best energy so far — the signal to fall back to the plain solve."""
     from .greedy import GreedyDeformationDataB200
     it = it or _greedy(tuple(I0.shape), max_pert)
     data = data or GreedyDeformationDataB200(I0, I1)
     data.Def1To0().copy_(h0)
+    if step is not None:
+        it.SetStepSize(step)
+    it.SetAutoStepReduce(auto_reduce)
     done = 0
     en = np.zeros(0)
+    best = np.inf
     while done < max_iters:
         k = min(chunk, max_iters - done)
-        it.Run(data, k, update_first=(done == 0))
+        it.Run(data, k, update_first=(done == 0 and step is None))
         done += k
-        en = it.Energies()
+        en = it.Energies()[-done:]
         hit = np.nonzero(en <= target)[0]
         if hit.size:
             return data.Def1To0(), int(hit[0]) + 1, en, True, True
-        if len(en) > k and not en[-1] < en[-k - 1]:
+        cmin = float(en[-k:].min())
+        if not cmin < best:
             return data.Def1To0(), done, en, False, False
+        best = cmin
     return data.Def1To0(), done, en, False, True
+
+
+def plain_step(I0: torch.Tensor, I1: torch.Tensor, it, data, max_pert: float = 0.5) -> float:
+    """The plain solve's step size: MaxPert / max |v| of the first iteration
+    from the identity (one iteration on scratch data)."""
+    from .device import identity
+    data.Def1To0().copy_(identity(tuple(I0.shape), I0.device))
+    it.Run(data, 1, update_first=True)
+    return it.StepSize()
 
 
 def make_pairs(seeds: Sequence[int], n: int, workers: int = 0):
@@ -355,12 +375,15 @@ def make_pairs(seeds: Sequence[int], n: int, workers: int = 0):
 
 
 def evaluate(net: "WarmStartNet", pairs, plain_iters: int = 50, tol: float = 0.01,
-             chunk: int = 5, max_pert: float = 0.5):
+             chunk: int = 5, max_pert: float = 0.5, policy: str = "own"):
     """Per pair: the plain solve from the identity for plain_iters
     iterations, then the warm start (network + refinement until the
     iteration energy is within (1 + tol) of the plain solve's last one,
     with the plain solve as fallback when a refinement chunk does not lower
-    the energy). Device times from CUDA events. Returns a list of dicts."""
+    the energy). policy "own": the refinement sets its step from the warm
+    start and halves it when the energy rises; "plain": it keeps the plain
+    solve's step from the identity (one extra iteration to find it).
+    Device times from CUDA events. Returns a list of dicts."""
     from .device import identity
     from .greedy import GreedyDeformationDataB200
     out = []
@@ -382,11 +405,15 @@ def evaluate(net: "WarmStartNet", pairs, plain_iters: int = 50, tol: float = 0.0
         e_plain = it.Energies()
         target = float(e_plain[-1]) * (1.0 + tol)
         ev[2].record()
+        eps = plain_step(I0, I1, it_w, data_w, max_pert) if policy == "plain" else None
         h0 = net.predict_h(I0, I1)
-        h, k, en, reached, fell = refine(I0, I1, h0, target, plain_iters, chunk, max_pert,
-                                         it_w, data_w)
-        fallback = not fell
-        if fallback:  # the warm start did not help: the plain solve, unassisted
+        # past half the plain iteration count the warm path cannot win: cap it there
+        h, k, en, reached, fell = refine(I0, I1, h0, target, plain_iters // 2, chunk, max_pert,
+                                         it_w, data_w, step=eps, auto_reduce=(policy == "own"))
+        if policy == "plain":
+            k += 1  # the step-size iteration
+        fallback = not reached
+        if fallback:  # the warm start did not get there: the plain solve, unassisted
             it2.Run(d2, plain_iters, update_first=True)
             k += plain_iters
         ev[3].record()
@@ -457,6 +484,7 @@ def main(argv=None):
     ap.add_argument("--save", default="", help="where to write the trained weights")
     ap.add_argument("--json", default="", help="where to write the evaluation summary")
     ap.add_argument("--workers", type=int, default=min(32, os.cpu_count() or 1))
+    ap.add_argument("--policy", default="own", choices=["own", "plain"])
     a = ap.parse_args(argv)
     t0 = time.time()
     eval_pairs = make_pairs(range(10_000_000, 10_000_000 + a.eval), a.n, a.workers)
@@ -479,7 +507,8 @@ def main(argv=None):
                         "loss_last": float(np.mean(losses[-50:]))})
         if a.save:
             save_weights(net, a.save)
-    res = evaluate(net, eval_pairs)
+    res = evaluate(net, eval_pairs, policy=a.policy)
+    summary["policy"] = a.policy
     pm = float(np.sum([r["plain_ms"] for r in res]))
     wm = float(np.sum([r["warm_ms"] for r in res]))
     summary.update({
