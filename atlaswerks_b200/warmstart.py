@@ -360,6 +360,38 @@ def plain_step(I0: torch.Tensor, I1: torch.Tensor, it, data, max_pert: float = 0
     return it.StepSize()
 
 
+def warm_h(net: "WarmStartNet", I0: torch.Tensor, I1: torch.Tensor) -> torch.Tensor:
+    """The warm-start deformation on the pair's grid. When the network's
+    grid is coarser, the pair is Gaussian-downsampled to it (the multiscale
+    downsampling of the greedy path), the network predicts there, and the
+    deformation is upsampled with its vectors rescaled — the network takes
+    the place of the coarse levels of a multiscale solve."""
+    from . import device as D
+    fine = tuple(I0.shape)
+    coarse = (net.D, net.H, net.W)
+    if fine == coarse:
+        return net.predict_h(I0, I1)
+    hc = net.predict_h(D.downsample(I0, coarse), D.downsample(I1, coarse))
+    return D.upsample_hfield(hc, fine, True)
+
+
+def coarse_training_set(seeds: Sequence[int], n: int, coarse: int, workers: int = 0,
+                        batch: int = 128, iters: int = 50):
+    """Training pairs of the n^3 generator, downsampled on the device to the
+    network's coarse^3 grid, with the plain solver's displacement there as
+    the target; generated in batches so the host holds one batch at a time."""
+    from . import device as D
+    out_pairs, out_targets = [], []
+    seeds = list(seeds)
+    for i in range(0, len(seeds), batch):
+        for a, b in make_pairs(seeds[i:i + batch], n, workers):
+            ca = D.downsample(torch.from_numpy(a).cuda(), (coarse,) * 3)
+            cb = D.downsample(torch.from_numpy(b).cuda(), (coarse,) * 3)
+            out_pairs.append((ca, cb))
+            out_targets.append(solver_target(ca, cb, iters))
+    return out_pairs, out_targets
+
+
 def make_pairs(seeds: Sequence[int], n: int, workers: int = 0):
     """(I0, I1) pairs of the pair-registration generator (8 blobs, smooth
     warp with max |u| = 3 voxels) on an n^3 grid, one per seed, generated in
@@ -406,7 +438,7 @@ def evaluate(net: "WarmStartNet", pairs, plain_iters: int = 50, tol: float = 0.0
         target = float(e_plain[-1]) * (1.0 + tol)
         ev[2].record()
         eps = plain_step(I0, I1, it_w, data_w, max_pert) if policy == "plain" else None
-        h0 = net.predict_h(I0, I1)
+        h0 = warm_h(net, I0, I1)
         # past half the plain iteration count the warm path cannot win: cap it there
         h, k, en, reached, fell = refine(I0, I1, h0, target, plain_iters // 2, chunk, max_pert,
                                          it_w, data_w, step=eps, auto_reduce=(policy == "own"))
@@ -433,7 +465,8 @@ def train(net: "WarmStartNet", pairs, targets, epochs: int = 1, lr: float = 1e-3
     Returns the per-step losses."""
     rng = np.random.default_rng(1234)
     losses = []
-    dev_pairs = [(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()) for a, b in pairs]
+    dev_pairs = [(a if torch.is_tensor(a) else torch.from_numpy(a).cuda(),
+                  b if torch.is_tensor(b) else torch.from_numpy(b).cuda()) for a, b in pairs]
     for ep in range(epochs):
         order = rng.permutation(len(pairs))
         for j, i in enumerate(order):
@@ -485,18 +518,26 @@ def main(argv=None):
     ap.add_argument("--json", default="", help="where to write the evaluation summary")
     ap.add_argument("--workers", type=int, default=min(32, os.cpu_count() or 1))
     ap.add_argument("--policy", default="own", choices=["own", "plain"])
+    ap.add_argument("--net", type=int, default=0,
+                    help="the network's grid (default: --n); smaller = predict on the "
+                         "downsampled pair and upsample the deformation")
     a = ap.parse_args(argv)
     t0 = time.time()
-    eval_pairs = make_pairs(range(10_000_000, 10_000_000 + a.eval), a.n, a.workers)
-    net = WarmStartNet((a.n, a.n, a.n))
-    summary = {"grid": a.n, "n_train": a.train, "n_eval": a.eval, "parameters": n_parameters()}
+    nn_grid = a.net or a.n
+    net = WarmStartNet((nn_grid,) * 3)
+    summary = {"grid": a.n, "net_grid": nn_grid, "n_train": a.train, "n_eval": a.eval,
+               "parameters": n_parameters()}
     if a.weights:
         load_weights(net, a.weights)
     else:
-        train_pairs = make_pairs(range(a.train), a.n, a.workers)
-        t1 = time.time()
-        targets = [solver_target(torch.from_numpy(p[0]).cuda(), torch.from_numpy(p[1]).cuda())
-                   for p in train_pairs]
+        if nn_grid == a.n:
+            train_pairs = make_pairs(range(a.train), a.n, a.workers)
+            t1 = time.time()
+            targets = [solver_target(torch.from_numpy(p[0]).cuda(),
+                                     torch.from_numpy(p[1]).cuda()) for p in train_pairs]
+        else:
+            t1 = time.time()
+            train_pairs, targets = coarse_training_set(range(a.train), a.n, nn_grid, a.workers)
         torch.cuda.synchronize()
         t2 = time.time()
         losses = train(net, train_pairs, targets, a.epochs, a.lr, log_every=500)
@@ -507,6 +548,8 @@ def main(argv=None):
                         "loss_last": float(np.mean(losses[-50:]))})
         if a.save:
             save_weights(net, a.save)
+        del train_pairs, targets
+    eval_pairs = make_pairs(range(10_000_000, 10_000_000 + a.eval), a.n, a.workers)
     res = evaluate(net, eval_pairs, policy=a.policy)
     summary["policy"] = a.policy
     pm = float(np.sum([r["plain_ms"] for r in res]))
