@@ -375,6 +375,40 @@ def warm_h(net: "WarmStartNet", I0: torch.Tensor, I1: torch.Tensor) -> torch.Ten
     return D.upsample_hfield(hc, fine, True)
 
 
+class WarmStartPredictor:
+    """warm_h for one pair grid as one CUDA graph replay: the pair is copied
+    into static buffers, and the downsampling, the 25 launches of the
+    network's forward pass, the displacement-to-h kernel and the
+    upsampling replay from a graph captured once (no per-layer host work).
+    The returned field is the predictor's own buffer, overwritten by the
+    next call; the weights are read at replay, so a predictor follows
+    later weight updates of its network."""
+
+    def __init__(self, net: "WarmStartNet", shape: Sequence[int]):
+        self.net = net
+        self.shape = tuple(int(s) for s in shape)
+        self.I0 = torch.zeros(self.shape, device=net.dev)
+        self.I1 = torch.zeros(self.shape, device=net.dev)
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):  # first launches (module loads, attributes) outside capture
+            warm_h(net, self.I0, self.I1)
+        torch.cuda.current_stream().wait_stream(side)
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.h = warm_h(net, self.I0, self.I1)
+        torch.cuda.synchronize()
+
+    def __call__(self, I0: torch.Tensor, I1: torch.Tensor) -> torch.Tensor:
+        if tuple(I0.shape) != self.shape or tuple(I1.shape) != self.shape:
+            raise ValueError(f"pair grid {tuple(I0.shape)} != predictor grid {self.shape}")
+        self.I0.copy_(I0)
+        self.I1.copy_(I1)
+        self.graph.replay()
+        return self.h
+
+
 def coarse_training_set(seeds: Sequence[int], n: int, coarse: int, workers: int = 0,
                         batch: int = 128, iters: int = 50):
     """Training pairs of the n^3 generator, downsampled on the device to the
@@ -407,7 +441,7 @@ def make_pairs(seeds: Sequence[int], n: int, workers: int = 0):
 
 
 def evaluate(net: "WarmStartNet", pairs, plain_iters: int = 50, tol: float = 0.01,
-             chunk: int = 5, max_pert: float = 0.5, policy: str = "own"):
+             chunk: int = 3, max_pert: float = 0.5, policy: str = "own"):
     """Per pair: the plain solve from the identity for plain_iters
     iterations, then the warm start (network + refinement until the
     iteration energy is within (1 + tol) of the plain solve's last one,
@@ -415,12 +449,17 @@ def evaluate(net: "WarmStartNet", pairs, plain_iters: int = 50, tol: float = 0.0
     the energy). policy "own": the refinement sets its step from the warm
     start and halves it when the energy rises; "plain": it keeps the plain
     solve's step from the identity (one extra iteration to find it).
-    Device times from CUDA events. Returns a list of dicts."""
-    from .device import identity
+    The network runs as one graph replay (WarmStartPredictor, built once
+    per grid before any clock starts). Device times from CUDA events;
+    warm_iters counts the iterations needed, warm_iters_run the ones
+    executed (whole chunks). Returns a list of dicts."""
     from .greedy import GreedyDeformationDataB200
     out = []
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    predictors: Dict[tuple, WarmStartPredictor] = {}
     for I0n, I1n in pairs:
+        if I0n.shape not in predictors:
+            predictors[I0n.shape] = WarmStartPredictor(net, I0n.shape)
         I0 = torch.from_numpy(I0n).cuda()
         I1 = torch.from_numpy(I1n).cuda()
         shape = tuple(I0.shape)
@@ -438,19 +477,24 @@ def evaluate(net: "WarmStartNet", pairs, plain_iters: int = 50, tol: float = 0.0
         target = float(e_plain[-1]) * (1.0 + tol)
         ev[2].record()
         eps = plain_step(I0, I1, it_w, data_w, max_pert) if policy == "plain" else None
-        h0 = warm_h(net, I0, I1)
+        h0 = predictors[I0n.shape](I0, I1)
+        ev[4].record()
         # past half the plain iteration count the warm path cannot win: cap it there
         h, k, en, reached, fell = refine(I0, I1, h0, target, plain_iters // 2, chunk, max_pert,
                                          it_w, data_w, step=eps, auto_reduce=(policy == "own"))
+        run = len(en)  # one recorded energy per executed iteration
         if policy == "plain":
             k += 1  # the step-size iteration
+            run += 1
         fallback = not reached
         if fallback:  # the warm start did not get there: the plain solve, unassisted
             it2.Run(d2, plain_iters, update_first=True)
             k += plain_iters
+            run += plain_iters
         ev[3].record()
         torch.cuda.synchronize()
         out.append({"plain_ms": ev[0].elapsed_time(ev[1]), "warm_ms": ev[2].elapsed_time(ev[3]),
+                    "predict_ms": ev[2].elapsed_time(ev[4]), "warm_iters_run": run,
                     "plain_iters": plain_iters, "warm_iters": int(k), "reached": bool(reached),
                     "fallback": bool(fallback), "plain_energy": float(e_plain[-1]),
                     "warm_start_energy": float(en[0]) if len(en) else float("nan"),
@@ -489,6 +533,23 @@ def save_weights(net: "WarmStartNet", path: str):
     st = net.state()
     np.savez_compressed(path, **{f"w_{k}": _bf16_bits(v) for k, v in st["w"].items()},
                         **{f"b_{k}": v for k, v in st["b"].items()})
+
+
+# committed trained weights: pair grid -> (file in atlaswerks_b200/data, network grid).
+# 64^3 pairs: the network at the pair's grid; 128^3 pairs: the network at 64^3
+# on the downsampled pair (warm_h), trained on 2000 pairs of the 128^3 generator.
+TRAINED = {64: ("warmstart_64.npz", 64), 128: ("warmstart_128.npz", 64)}
+
+
+def trained(grid: int) -> "WarmStartNet":
+    """The committed network for n^3 pairs (n in TRAINED), weights loaded."""
+    import os
+    if grid not in TRAINED:
+        raise ValueError(f"no trained weights for {grid}^3 pairs (have {sorted(TRAINED)})")
+    name, net_grid = TRAINED[grid]
+    net = WarmStartNet((net_grid,) * 3)
+    load_weights(net, os.path.join(os.path.dirname(__file__), "data", name))
+    return net
 
 
 def load_weights(net: "WarmStartNet", path: str):
@@ -550,6 +611,7 @@ def main(argv=None):
             save_weights(net, a.save)
         del train_pairs, targets
     eval_pairs = make_pairs(range(10_000_000, 10_000_000 + a.eval), a.n, a.workers)
+    evaluate(net, eval_pairs[:2], policy=a.policy)  # warm-up: module loads, pools, graphs
     res = evaluate(net, eval_pairs, policy=a.policy)
     summary["policy"] = a.policy
     pm = float(np.sum([r["plain_ms"] for r in res]))
@@ -559,6 +621,10 @@ def main(argv=None):
         "plain_pairs_per_s": 1000.0 * len(res) / pm, "warm_pairs_per_s": 1000.0 * len(res) / wm,
         "iters_plain_mean": float(np.mean([r["plain_iters"] for r in res])),
         "iters_warm_mean": float(np.mean([r["warm_iters"] for r in res])),
+        "iters_warm_run_mean": float(np.mean([r["warm_iters_run"] for r in res])),
+        "predict_ms_median": float(np.median([r["predict_ms"] for r in res])),
+        "warm_ms_median": float(np.median([r["warm_ms"] for r in res])),
+        "plain_ms_median": float(np.median([r["plain_ms"] for r in res])),
         "reached_fraction": float(np.mean([r["reached"] for r in res])),
         "fallback_fraction": float(np.mean([r["fallback"] for r in res])),
         "warm_start_energy_over_identity": float(np.median(

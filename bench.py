@@ -8,7 +8,9 @@ Workload (one "step"): every rank holds 4 independent 128^3 pairs resident
 in HBM (config-2 generator: 16 Gaussian blobs + N(0, 0.02^2) noise, smooth
 warp with max |u| = 6 voxels; alpha = beta = 0.01, gamma = 0.001,
 MaxPert 0.5) and runs 2 greedy iterations on each pair, so a step is 8
-iterations. The 4 pairs' working sets (~120 MB each) exceed the 126 MB L2,
+iterations; each pair's iterations run on its own stream (a batch of
+independent registrations, as an atlas or a registration service runs
+them). The 4 pairs' working sets (~120 MB each) exceed the 126 MB L2,
 so consecutive steps find none of their data in L2.
 
 Pair registrations are independent: with N GPUs every rank runs its own
@@ -142,10 +144,10 @@ def make_pair(seed):
 def config(extra=None):
     c = {"workload": f"greedy-fluid pair registration, {N}^3 float32, single scale "
                      f"(finest level of the 3-level config), {PAIRS} resident pairs x "
-                     f"{ITERS_PER_PAIR} iterations per step",
+                     f"{ITERS_PER_PAIR} iterations per step, one stream per pair",
          "grid": [N, N, N], "alpha": ALPHA, "beta": BETA, "gamma": GAMMA, "max_pert": MAX_PERT,
          "pairs_per_rank": PAIRS, "iterations_per_step_per_rank": PAIRS * ITERS_PER_PAIR,
-         "l2": "inputs larger than L2: 4 pairs x ~120 MB working set, round-robin",
+         "l2": "inputs larger than L2: 4 pairs x ~120 MB working set, concurrent",
          "inverse_field": False}
     if extra:
         c.update(extra)
@@ -241,10 +243,23 @@ def run_b200(args):
         iters.append(it)
         datas.append(d)
     stream = torch.cuda.current_stream()
+    # each pair runs on its own stream, so one pair's kernels fill the SMs
+    # that another pair's kernel leaves idle (tails, single-wave grids)
+    pair_streams = [torch.cuda.Stream() for _ in range(PAIRS)]
 
     def step():
-        for it, d in zip(iters, datas):
-            it.Run(d, ITERS_PER_PAIR, update_first=False)
+        fork = torch.cuda.Event()
+        fork.record(stream)
+        joins = []
+        for it, d, ps in zip(iters, datas, pair_streams):
+            ps.wait_event(fork)
+            with torch.cuda.stream(ps):
+                it.Run(d, ITERS_PER_PAIR, update_first=False)
+                j = torch.cuda.Event()
+                j.record(ps)
+            joins.append(j)
+        for j in joins:
+            stream.wait_event(j)
 
     for _ in range(max(args.warmup, 3)):
         step()
@@ -518,22 +533,22 @@ def run_ldmm(args):
 
 def run_warmstart(args):
     """Learned warm start + refinement against the plain GPU greedy solve on
-    held-out pairs (config-1 generator), with the committed trained weights."""
+    held-out pairs of the pair-registration generator, with the committed
+    trained weights (128^3 pairs: the network at 64^3 on the downsampled
+    pair). A step = one pair through both paths."""
     import numpy as np
     import torch
 
     from atlaswerks_b200 import warmstart as W
-    n = args.grid or 64
-    wpath = os.path.join(ROOT, "atlaswerks_b200", "data", "warmstart_64.npz")
-    if not os.path.exists(wpath):
-        print(json.dumps({"metric": "warm-start pairs/s", "unavailable":
-                          "no trained weights at atlaswerks_b200/data/warmstart_64.npz"}))
+    n = args.grid or 128
+    if n not in W.TRAINED:
+        print(json.dumps({"metric": f"{n}^3 warm-start registrations/s", "unavailable":
+                          f"no trained weights for {n}^3 pairs"}))
         return 0
     pairs = W.make_pairs(range(10_000_000, 10_000_000 + args.pairs), n,
                          min(32, os.cpu_count() or 1))
-    net = W.WarmStartNet((n, n, n))
-    W.load_weights(net, wpath)
-    W.evaluate(net, pairs[:2])  # warm-up (graph capture, caches)
+    net = W.trained(n)
+    W.evaluate(net, pairs[:2])  # warm-up (module loads, graph capture, pools)
     res = W.evaluate(net, pairs)
     pm = float(np.sum([r["plain_ms"] for r in res]))
     wm = float(np.sum([r["warm_ms"] for r in res]))
@@ -542,12 +557,16 @@ def run_warmstart(args):
         "value": 1000.0 * len(res) / wm, "unit": "pairs/s", "n_gpus": 1, "steps": len(res),
         "higher_is_better": True, "dtype": "bf16 network, f32 registration",
         "data": "synthetic held-out seeds (8 blobs, smooth warp max 3 voxels)",
-        "config": {"workload": "warm start (trained encoder-decoder) + greedy refinement with "
-                   "fallback vs plain greedy (50 iterations from the identity)", "grid": [n] * 3,
-                   "pairs": len(res)},
+        "config": {"workload": "warm start (trained encoder-decoder, one graph replay) + greedy "
+                   "refinement with fallback vs plain greedy (50 iterations from the identity)",
+                   "grid": [n] * 3, "network_grid": [net.D, net.H, net.W], "pairs": len(res)},
         "plain_pairs_per_s": 1000.0 * len(res) / pm, "wall_ratio_warm_over_plain": wm / pm,
+        "predict_ms_median": float(np.median([r["predict_ms"] for r in res])),
+        "warm_ms_median": float(np.median([r["warm_ms"] for r in res])),
+        "plain_ms_median": float(np.median([r["plain_ms"] for r in res])),
         "iters_plain_mean": float(np.mean([r["plain_iters"] for r in res])),
         "iters_warm_mean": float(np.mean([r["warm_iters"] for r in res])),
+        "iters_warm_run_mean": float(np.mean([r["warm_iters_run"] for r in res])),
         "reached_fraction": float(np.mean([r["reached"] for r in res])),
         "fallback_fraction": float(np.mean([r["fallback"] for r in res]))}))
     return 0
@@ -565,7 +584,7 @@ def main():
     ap.add_argument("--workload", default="greedy",
                     choices=["greedy", "atlas", "ldmm", "warmstart"],
                     help="the headline greedy line (default) or another hot-path row")
-    ap.add_argument("--grid", type=int, default=0, help="warmstart: grid size (64 or 128)")
+    ap.add_argument("--grid", type=int, default=0, help="warmstart: pair grid (64 or 128; default 128)")
     ap.add_argument("--pairs", type=int, default=32, help="warmstart: held-out pairs")
     args = ap.parse_args()
     if args.ncu_case:

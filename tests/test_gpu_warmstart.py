@@ -1,8 +1,10 @@
 """What the trained warm-start network gains over the plain greedy solve,
-on held-out seeded pairs of the pair-registration generator at 64^3, with
-the weights committed in atlaswerks_b200/data (trained on the GPU by the
-network's own kernels from the solver's displacements), and that training
-lowers the loss.
+on held-out seeded pairs of the pair-registration generator at 64^3 and
+128^3 (the latter predicted by the network at 64^3 on the downsampled
+pair), with the weights committed in atlaswerks_b200/data (trained on the
+GPU by the network's own kernels from the solver's displacements), that
+the graph-replayed predictor gives the eager path's field bit for bit,
+and that training lowers the loss.
 
 The bar: the predicted deformation removes most of the initial mismatch
 (median energy <= 20 % of the identity's), and the refinement reaches the
@@ -35,6 +37,31 @@ def test_trained_warm_start_beats_plain_solve():
     assert np.mean([r["warm_iters"] for r in reached]) <= 20
     # a fallback ends with the plain solve itself: never worse than it
     assert all(r["fallback"] or r["reached"] for r in res)
+
+
+def test_coarse_network_warm_start_at_128():
+    pairs = W.make_pairs(range(20_000_100, 20_000_104), 128, 0)
+    net = W.trained(128)
+    assert (net.D, net.H, net.W) == (64, 64, 64)
+    res = W.evaluate(net, pairs)
+    start = np.median([r["warm_start_energy"] / r["identity_energy"] for r in res])
+    assert start <= 0.2
+    assert sum(r["reached"] for r in res) >= 3
+    assert np.mean([r["warm_iters_run"] for r in res if r["reached"]]) <= 10
+    assert not net.timed_out()
+
+
+def test_graph_predictor_matches_eager_path():
+    I0, I1 = (torch.from_numpy(a).cuda() for a in W.make_pairs([20_000_200], 128, 0)[0])
+    net = W.trained(128)
+    eager = W.warm_h(net, I0, I1).clone()
+    pred = W.WarmStartPredictor(net, (128, 128, 128))
+    got = pred(I0, I1)
+    torch.cuda.synchronize()
+    assert torch.equal(got, eager)
+    # a second pair through the same graph
+    J0, J1 = (torch.from_numpy(a).cuda() for a in W.make_pairs([20_000_201], 128, 0)[0])
+    assert torch.equal(pred(J0, J1).clone(), W.warm_h(net, J0, J1))
 
 
 def test_training_lowers_the_loss():
