@@ -96,12 +96,18 @@ AW_D void atlas_point(const AtlasMap &a, double &x, double &y, double &z) {
 
 // floor as the reference computes it: truncate, then step down for
 // negative non-integers (Array3DUtils.txx:70-75)
+// Positions are clamped to [-2^30, 2^30] first (NaN to -2^30): the same
+// floor for every position a grid can hold, and for huge, infinite or NaN
+// positions a cell far outside every grid, so fx + 1 cannot overflow and
+// the callers' inside/outside tests never pass an out-of-range corner.
 AW_D int ref_floor_d(double x) {
+  x = fmin(fmax(x, -0x1p30), 0x1p30);
   int f = __double2int_rz(x);
   if (x < 0.0 && x != (double)f) --f;
   return f;
 }
 AW_D int ref_floor_f(float x) {
+  x = fminf(fmaxf(x, -0x1p30f), 0x1p30f);
   int f = __float2int_rz(x);
   if (x < 0.0f && x != __int2float_rn(f)) --f;
   return f;

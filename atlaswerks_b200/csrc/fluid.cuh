@@ -51,6 +51,14 @@ struct SrcField {
   AW_D float value(int comp, int x, int y, int z, const Dims &d) const {
     return __ldg(c[comp] + d.idx(x, y, z));
   }
+  // rows y0 and y0+1 of slab z at x = t + TX*j, j < E, as (row y0, row y0+1)
+  template <int E, int TX>
+  AW_D void row_pair(int comp, int t, int y0, int z, const Dims &d, float2 *v) const {
+    const float *r0 = (comp == 0 ? c[0] : comp == 1 ? c[1] : c[2]) + d.idx(t, y0, z);
+    const float *r1 = r0 + d.nx;
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = make_float2(__ldg(r0 + TX * j), __ldg(r1 + TX * j));
+  }
 };
 
 // body force f_c = d/dc(G) * M, with M = A - G (mode 1, greedy: G = I0(h),
@@ -66,6 +74,19 @@ struct SrcForce {
   const float *B;
   int mode;
   DivD c2[3], c1[3];  // 2 sp and sp per axis
+  // All six divisors are powers of two whose reciprocals are normal floats:
+  // the difference times the float reciprocal is then the same float as the
+  // double quotient rounded (both are the exact product, rounded once to
+  // nearest), so the gradient needs no double arithmetic.
+  int fexact;
+  float r2[3], r1[3];
+  AW_D float grad(float diff, int comp, bool interior) const {
+    if (fexact) return fmul(diff, interior ? r2[comp] : r1[comp]);
+    return __double2float_rn(ddiv((double)diff, interior ? c2[comp] : c1[comp]));
+  }
+  AW_D float mismatch(float g0, float a, const float *b) const {
+    return mode == 0 ? a : (mode == 1 ? -fsub(g0, a) : fmul(fsub(g0, a), __ldg(b)));
+  }
   AW_D float value(int comp, int x, int y, int z, const Dims &d) const {
     const long i = d.idx(x, y, z);
     const float g0 = __ldg(G + i);
@@ -74,18 +95,66 @@ struct SrcForce {
     if (comp == 0) { pos = x; n = d.nx; stride = 1; }
     else if (comp == 1) { pos = y; n = d.ny; stride = d.nx; }
     else { pos = z; n = d.nz; stride = (long)d.nx * d.ny; }
-    float grad;
+    float g;
     if (pos > 0 && pos < n - 1) {
-      grad = __double2float_rn(ddiv((double)fsub(__ldg(G + i + stride), __ldg(G + i - stride)),
-                                    c2[comp]));
+      g = grad(fsub(__ldg(G + i + stride), __ldg(G + i - stride)), comp, true);
     } else if (pos == 0) {
-      grad = __double2float_rn(ddiv((double)fsub(__ldg(G + i + stride), g0), c1[comp]));
+      g = grad(fsub(__ldg(G + i + stride), g0), comp, false);
     } else {
-      grad = __double2float_rn(ddiv((double)fsub(g0, __ldg(G + i - stride)), c1[comp]));
+      g = grad(fsub(g0, __ldg(G + i - stride)), comp, false);
     }
-    const float a = __ldg(A + i);
-    const float m = mode == 0 ? a : (mode == 1 ? -fsub(g0, a) : fmul(fsub(g0, a), __ldg(B + i)));
-    return fmul(grad, m);
+    return fmul(g, mismatch(g0, __ldg(A + i), B + i));
+  }
+  // Rows y0 and y0+1 of slab z at x = t + TX*j, j < E, as (row y0, row
+  // y0+1): the same values as value(), from row pointers formed once and one
+  // code path per component. Needs nx, ny, nz >= 3 and an even ny.
+  template <int E, int TX>
+  AW_D void row_pair(int comp, int t, int y0, int z, const Dims &d, float2 *v) const {
+    const long i0 = d.idx(t, y0, z);
+    const int nx = d.nx;
+    const float *g0p = G + i0, *g1p = g0p + nx, *a0p = A + i0, *b0p = B + i0;
+    if (comp == 0) {
+#pragma unroll
+      for (int j = 0; j < E; ++j) {
+        const int x = t + TX * j;
+        const int lo = x > 0 ? -1 : 0, hi = x < nx - 1 ? 1 : 0;
+        const bool in = lo != 0 && hi != 0;
+        const int o = TX * j;
+        const float g0 = __ldg(g0p + o), g1 = __ldg(g1p + o);
+        const float d0 = fsub(__ldg(g0p + o + hi), __ldg(g0p + o + lo));
+        const float d1 = fsub(__ldg(g1p + o + hi), __ldg(g1p + o + lo));
+        v[j] = make_float2(fmul(grad(d0, 0, in), mismatch(g0, __ldg(a0p + o), b0p + o)),
+                           fmul(grad(d1, 0, in), mismatch(g1, __ldg(a0p + o + nx), b0p + o + nx)));
+      }
+    } else if (comp == 1) {
+      // y0 - 1 (or y0 at the first row) and y0 + 2 (or y0 + 1 at the last)
+      const int lo = y0 > 0 ? -nx : 0, hi = y0 + 2 < d.ny ? 2 * nx : nx;
+      const bool in0 = y0 > 0, in1 = y0 + 2 < d.ny;
+#pragma unroll
+      for (int j = 0; j < E; ++j) {
+        const int o = TX * j;
+        const float g0 = __ldg(g0p + o), g1 = __ldg(g1p + o);
+        // row y0: G[y0+1] - G[y0-1], or G[1] - G[0] (lo = 0);
+        // row y0+1: G[y0+2] - G[y0], or G[ny-1] - G[ny-2] (hi = nx)
+        const float d0 = fsub(g1, __ldg(g0p + o + lo));
+        const float d1 = fsub(__ldg(g0p + o + hi), g0);
+        v[j] = make_float2(fmul(grad(d0, 1, in0), mismatch(g0, __ldg(a0p + o), b0p + o)),
+                           fmul(grad(d1, 1, in1), mismatch(g1, __ldg(a0p + o + nx), b0p + o + nx)));
+      }
+    } else {
+      const long sl = (long)nx * d.ny;
+      const long lo = z > 0 ? -sl : 0, hi = z < d.nz - 1 ? sl : 0;
+      const bool in = z > 0 && z < d.nz - 1;
+#pragma unroll
+      for (int j = 0; j < E; ++j) {
+        const int o = TX * j;
+        const float g0 = __ldg(g0p + o), g1 = __ldg(g1p + o);
+        const float d0 = fsub(__ldg(g0p + o + hi), __ldg(g0p + o + lo));
+        const float d1 = fsub(__ldg(g1p + o + hi), __ldg(g1p + o + lo));
+        v[j] = make_float2(fmul(grad(d0, 2, in), mismatch(g0, __ldg(a0p + o), b0p + o)),
+                           fmul(grad(d1, 2, in), mismatch(g1, __ldg(a0p + o + nx), b0p + o + nx)));
+      }
+    }
   }
 };
 inline SrcForce make_force(const float *G, const float *A, int mode, const Spacing &sp,
@@ -96,9 +165,15 @@ inline SrcForce make_force(const float *G, const float *A, int mode, const Spaci
   f.B = B;
   f.mode = mode;
   const double s[3] = {sp.x, sp.y, sp.z};
+  f.fexact = 1;
   for (int c = 0; c < 3; ++c) {
     f.c2[c] = make_div(2.0 * s[c]);
     f.c1[c] = make_div(s[c]);
+    f.r2[c] = (float)f.c2[c].r;
+    f.r1[c] = (float)f.c1[c].r;
+    // a power of two whose reciprocal is a float (well inside the normal range)
+    for (const DivD *q : {&f.c2[c], &f.c1[c]})
+      if (!q->p2 || !(q->r >= 0x1p-100 && q->r <= 0x1p+100)) f.fexact = 0;
   }
   return f;
 }

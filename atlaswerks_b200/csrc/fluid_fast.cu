@@ -85,11 +85,7 @@ __global__ void __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
     for (int base = warp * L; base < NLINES; base += kXYWarps * L) {
       const int y0 = 2 * xline_pair<TX>(base + lw);
       float2 v[EX];
-#pragma unroll
-      for (int j = 0; j < EX; ++j) {
-        const int x = t + TX * j;
-        v[j] = make_float2(src.value(comp, x, y0, z, d), src.value(comp, x, y0 + 1, z, d));
-      }
+      src.template row_pair<EX, TX>(comp, t, y0, z, d, v);
       float2 *row = C + y0 * NXH;
       line_fft<NX, -1>(v, t, [row](int m) { return row + m; }, p.ax.tw);
 #pragma unroll

@@ -11,6 +11,11 @@
 //  * hToVelocity, HField3DUtils::resampleNew with CLAMP and rescaled vectors,
 //    velocityToH (UtilitiesDataTypes/HField3DUtils.txx:57-110, 1816-1881).
 #include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "multiscale.cuh"
@@ -124,10 +129,53 @@ void gauss_rows(float sigma, int size, std::vector<float> &rows) {
 }  // namespace
 
 size_t downsample_scratch_bytes(const Dims &din) {
-  // two blur buffers + three filter tables of at most (2*ceil(sqrt(n/2))+1)^2
-  const size_t fl = 3 * 64 * 64;
-  return sizeof(float) * (2 * (size_t)din.n() + fl);
+  // two blur buffers
+  return sizeof(float) * 2 * (size_t)din.n();
 }
+
+namespace {
+
+// The Gaussian tables live in device memory for the life of the process,
+// one per (device, sigma, half-width), uploaded by the first call that
+// needs them. A later call issues no host copy, so a stream capture of the
+// downsampling (a CUDA graph) replays without host data. A table missing
+// while the stream is being captured is an error: the first call must run
+// outside the capture.
+std::mutex g_gauss_mu;
+std::map<std::tuple<int, uint32_t, int>, float *> g_gauss;
+
+cudaError_t gauss_table(float sigma, int K, cudaStream_t s, const float **table) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  uint32_t bits;
+  std::memcpy(&bits, &sigma, sizeof(bits));
+  const auto key = std::make_tuple(dev, bits, K);
+  std::lock_guard<std::mutex> lock(g_gauss_mu);
+  auto it = g_gauss.find(key);
+  if (it != g_gauss.end()) {
+    *table = it->second;
+    return cudaSuccess;
+  }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if ((e = cudaStreamIsCapturing(s, &cs)) != cudaSuccess) return e;
+  if (cs != cudaStreamCaptureStatusNone) return cudaErrorStreamCaptureUnsupported;
+  std::vector<float> rows;
+  gauss_rows(sigma, K, rows);
+  float *t = nullptr;
+  if ((e = cudaMalloc(&t, rows.size() * sizeof(float))) != cudaSuccess) return e;
+  e = cudaMemcpyAsync(t, rows.data(), rows.size() * sizeof(float), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // rows outlives the copy
+  if (e != cudaSuccess) {
+    cudaFree(t);
+    return e;
+  }
+  g_gauss[key] = t;
+  *table = t;
+  return cudaSuccess;
+}
+
+}  // namespace
 
 cudaError_t downsample(const float *in, Dims din, Spacing sin, float *out, Dims dout,
                        void *scratch, cudaStream_t s) {
@@ -136,7 +184,6 @@ cudaError_t downsample(const float *in, Dims din, Spacing sin, float *out, Dims 
   const int n[3] = {din.nx, din.ny, din.nz};
   float *b1 = static_cast<float *>(scratch);
   float *b2 = b1 + din.n();
-  float *tab = b2 + din.n();
   const float *src = in;
   float *dst[3] = {b1, b2, b1};
   for (int a = 0; a < 3; ++a) {
@@ -144,13 +191,8 @@ cudaError_t downsample(const float *in, Dims din, Spacing sin, float *out, Dims 
     int K = 2 * (int)std::ceil(sg);
     if (K > n[a] / 2 - 1) K = n[a] / 2 - 1;
     if (K < 0) K = 0;
-    if ((K + 1) * (K + 1) > 64 * 64) return cudaErrorInvalidValue;
-    std::vector<float> rows;
-    gauss_rows((float)sg, K, rows);
-    float *t = tab + a * 64 * 64;
-    // from pageable memory: the call returns once the table has been staged
-    cudaError_t e = cudaMemcpyAsync(t, rows.data(), rows.size() * sizeof(float),
-                                    cudaMemcpyHostToDevice, s);
+    const float *t = nullptr;
+    cudaError_t e = gauss_table((float)sg, K, s, &t);
     if (e != cudaSuccess) return e;
     k_gauss_axis<<<row_grid(din), kRowThreads, 0, s>>>(src, dst[a], din, a, K, t);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -190,3 +190,67 @@ def test_greedy_deterministic():
     r2 = greedy_register(cu(I0), cu(I1), 10)
     assert torch.equal(r1[0], r2[0])
     assert np.array_equal(r1[2], r2[2])
+
+
+# NaN, infinite and huge positions (a diverged or untrained deformation):
+# every kernel treats them as far outside the volume and reads nothing out
+# of range. Voxels whose positions are finite keep their exact values.
+_BAD = np.array([np.nan, np.inf, -np.inf, 1e30, -1e30, 3e9, -3e9, 2.2e9], np.float32)
+
+
+def _plant(field, rng, count=64):
+    """A copy of field with `count` entries of every component replaced by
+    the values of _BAD; returns (copy, mask of the voxels touched)."""
+    out = field.copy()
+    n = field[0].size
+    mask = np.zeros(n, bool)
+    for c in range(3):
+        idx = rng.choice(n, count, replace=False)
+        out[c].reshape(-1)[idx] = _BAD[rng.integers(0, len(_BAD), count)]
+        mask[idx] = True
+    return out, mask.reshape(field.shape[1:])
+
+
+def test_nonfinite_positions_apply_splat(oracle):
+    shape = (12, 11, 10)
+    rng = np.random.default_rng(11)
+    img = rng.random(shape, dtype=np.float32)
+    h = identity(shape) + rng.normal(0, 2.0, (3,) + shape).astype(np.float32)
+    bad, mask = _plant(h, rng)
+    got = host(D.apply(cu(img), cu(bad), 0.5))
+    assert np.array_equal(got[~mask], oracle.apply(img, h, 0.5)[~mask])
+    # the splat skips sources outside the grown volume: the same sum as with
+    # those sources moved far outside
+    far = h.copy()
+    for c in range(3):
+        far[c][mask] = -1.0e4
+    assert np.array_equal(host(D.splat(cu(img), cu(bad))), oracle.splat(img, far))
+
+
+@pytest.mark.parametrize("bg", range(6))
+def test_nonfinite_velocity_compose(oracle, bg):
+    shape, sp = (12, 11, 10), (1.0, 1.3, 0.8)
+    rng = np.random.default_rng(12)
+    g = identity(shape) + rng.normal(0, 1.5, (3,) + shape).astype(np.float32)
+    v = rng.normal(0, 1.5, (3,) + shape).astype(np.float32)
+    bad, mask = _plant(v, rng)
+    got = host(D.compose_hv(cu(g), cu(bad), sp, 1.0, 1, bg))
+    want = oracle.compose_hv(g, v, sp, 1, bg)
+    assert np.array_equal(got[:, ~mask], want[:, ~mask])
+
+
+def test_nonfinite_deformation_iterates_without_fault():
+    """A greedy iteration from a deformation holding NaN / inf / huge
+    entries completes; the energy it records is not finite."""
+    shape = (32, 32, 32)
+    I0, I1 = greedy_pair(shape, seed=6)
+    rng = np.random.default_rng(13)
+    bad, _ = _plant(identity(shape), rng)
+    it = GreedyIteratorB200(shape)
+    it.SetScaleLevel(shape, (1.0, 1.0, 1.0), GreedyIteratorParam(DiffOperParam(0.01, 0.01, 0.001),
+                                                                  0.5))
+    d = GreedyDeformationDataB200(cu(I0), cu(I1))
+    d.Def1To0().copy_(cu(bad))
+    it.Run(d, 3, update_first=True)
+    torch.cuda.synchronize()
+    assert not np.isfinite(it.Energies()[0])
