@@ -79,6 +79,8 @@ SIGNATURES = {
     "aw_ldmm_run": ([_fp] * 4 + [_i, _i, _fp], _i),
     "aw_ldmm_get_energies": ([_fp, _fp, _i, _fp], _i),
     "aw_nn_conv3d_scratch_floats": ([_i] * 7, ctypes.c_size_t),
+    "aw_nn_conv3d_direct_planes": ([_i] * 7, _i),
+    "aw_nn_set_gemm_only": ([_i], None),
     "aw_nn_conv3d_fwd": ([_fp] + [_i] * 5 + [_fp, _fp, _i, _i, _i, _fp, _fp, _fp,
                                            ctypes.c_size_t, _fp], _i),
     "aw_nn_conv3d_dgrad": ([_fp] + [_i] * 5 + [_fp, _i, _i, _fp, _fp, _fp, ctypes.c_size_t,

@@ -86,6 +86,18 @@ __device__ __forceinline__ void tma_load_3d(void *smem_dst, const void *tmap, in
       : "memory");
 }
 
+// 5D tensor tile load (no multicast): coordinates innermost first; a box
+// reaching outside the tensor reads zeros there (the innermost coordinate
+// must stay a multiple of 16 bytes; the others may be negative)
+__device__ __forceinline__ void tma_load_5d(void *smem_dst, const void *tmap, int c0, int c1, int c2,
+                                            int c3, int c4, uint64_t *mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(smem_dst)),
+      "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(mbar))
+      : "memory");
+}
+
 // 3D tensor tile store; out-of-bounds box elements are not written
 __device__ __forceinline__ void tma_store_3d(const void *tmap, int x, int y, int z,
                                              const void *smem_src) {

@@ -20,8 +20,11 @@
 //   wgrad    D[(tap,ci)][co] = sum_voxel X[voxel + off(tap)][ci] dY[voxel][co]
 // (wgrad: K = voxels, split over CTAs; both of its operands are read
 // MN-major straight from the channels-last tensors).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "umma.cuh"
@@ -709,9 +712,259 @@ __global__ void k_disp_to_h(const float *__restrict__ pred, Vol v, float *__rest
   hz[m] = (float)z + pred[m * 16 + 2];
 }
 
+// ---- direct 3x3x3 convolution from a TMA-staged halo tile ------------------
+// For the wide, shallow layers (16-48 channels) the im2col gather of the
+// GEMM above costs ten times the tensor and HBM work. Here a CTA owns an
+// output tile of 8 (x) x 16 (y) voxels x ZT planes of one batch item; the
+// input box it needs — CIN/8 chunks of 8 channels, each [ZT+2][18][10]
+// cells of 16 bytes — arrives by TMA tensor loads, zero-filled outside the
+// volume. Row r = x + 8y of a 128-row MMA tile is voxel (x, y), so for tap
+// (dz, dy, dx) and plane zz the A operand is that box shifted by
+// (dx, dy, zz + dz): core matrix i (row group y = i) starts at cell
+// (dx, i + dy, zz + dz), 160 bytes apart, its 8 rows (x) 16 bytes apart in
+// one contiguous 128-byte run, and the two 8-channel chunks of a K = 16
+// step one region apart. One MMA per (plane, tap, 16 input channels), no
+// operand copy at all; the weights sit in shared memory in the canonical
+// K-major layout; each plane accumulates in its own COUT TMEM columns.
+// Small shared footprint, one tile per CTA, several CTAs per SM: the TMA
+// loads, MMAs and epilogues of co-resident CTAs overlap. (A persistent
+// double-buffered variant measured slower here: with N = 16 the MMAs are
+// bound by reading the 4 KB A operand from shared memory, and fewer
+// resident CTAs left that bandwidth idle between tiles.)
+template <int CIN, int COUT, int ZT>
+struct DirectCfg {
+  static constexpr int NCH = CIN / 8;
+  static constexpr int CELLS = 10 * 18 * (ZT + 2);
+  static constexpr int BOX_BYTES = CELLS * 16;
+  static constexpr int REGION = (BOX_BYTES + 127) / 128 * 128;
+  static constexpr int IN_BYTES = NCH * REGION;
+  static constexpr int W_BYTES = 27 * CIN * COUT * 2;  // a multiple of 128
+  static constexpr int COLS = ZT * COUT;
+  static constexpr int TMEM_COLS = COLS <= 32 ? 32 : COLS <= 64 ? 64 : COLS <= 128 ? 128 : 256;
+  static constexpr size_t smem() { return 1024 + (size_t)IN_BYTES + W_BYTES; }
+  static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COLS <= 256, "direct conv shape");
+};
+
+template <int CIN, int COUT, int ZT>
+__global__ void __launch_bounds__(128)
+    k_conv_direct(const __grid_constant__ CUtensorMap tmap, const bf16 *__restrict__ w,
+                  const float *__restrict__ bias, int relu, bf16 *__restrict__ out,
+                  float *__restrict__ outf, int D, int H, int W, int *status) {
+  using C = DirectCfg<CIN, COUT, ZT>;
+  extern __shared__ __align__(1024) uint8_t smraw[];
+  __shared__ uint64_t mbar[2];  // 0: input box landed, 1: MMAs done
+  __shared__ uint32_t tbase;
+  __shared__ int s_ok;
+  uint8_t *base = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
+  uint8_t *sW = base, *sIn = base + C::W_BYTES;
+  constexpr uint32_t IDESC = umma_idesc_bf16(128, COUT, 0, 0);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  // tile coordinates: x fastest, then y, z, batch
+  const int tx = W / 8, ty = H / 16, tz = D / ZT;
+  int t = blockIdx.x;
+  const int x0 = (t % tx) * 8;
+  t /= tx;
+  const int y0 = (t % ty) * 16;
+  t /= ty;
+  const int z0 = (t % tz) * ZT;
+  const int b = t / tz;
+
+  if (warp == 0) tmem_alloc(&tbase, C::TMEM_COLS);
+  if (tid == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tbase;
+  if (tid == 0) {
+    mbar_expect_tx(&mbar[0], (uint32_t)(C::NCH * C::BOX_BYTES));
+#pragma unroll 1
+    for (int j = 0; j < C::NCH; ++j)
+      tma_load_5d(sIn + j * C::REGION, &tmap, 8 * j, x0 - 1, y0 - 1, z0 - 1, b, &mbar[0]);
+  }
+  // weights [COUT][27][CIN] -> chunk (tap, j, n) at ((tap*NCH + j)*(COUT/8) + n/8)*128 +
+  // (n%8)*16 = 16 c for c = (tap*NCH + j)*COUT + n: consecutive threads, consecutive chunks
+#pragma unroll 1
+  for (int c = tid; c < COUT * 27 * C::NCH; c += 128) {
+    const int n = c % COUT, r = c / COUT;
+    const int j = r % C::NCH, tap = r / C::NCH;
+    const uint4 val = __ldg(reinterpret_cast<const uint4 *>(w + ((long)n * 27 + tap) * CIN + 8 * j));
+    *reinterpret_cast<uint4 *>(sW + 16 * c) = val;
+  }
+  fence_async_smem();
+  __syncthreads();
+  if (tid == 0) {
+    s_ok = mbar_wait(&mbar[0], 0, status) ? 1 : 0;
+    if (s_ok) {
+      tc_fence_after();
+      const uint32_t a0 = smem_u32(sIn), b0 = smem_u32(sW);
+#pragma unroll 1
+      for (int zz = 0; zz < ZT; ++zz) {
+#pragma unroll 1
+        for (int tap = 0; tap < 27; ++tap) {
+          const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
+          const uint32_t cell = (uint32_t)((((zz + dz) * 18 + dy) * 10 + dx) * 16);
+#pragma unroll
+          for (int jp = 0; jp < C::NCH / 2; ++jp) {
+            const uint64_t da = umma_desc(a0 + 2 * jp * C::REGION + cell, C::REGION, 160);
+            const uint64_t db =
+                umma_desc(b0 + (tap * C::NCH + 2 * jp) * (COUT / 8) * 128, COUT * 16, 128);
+            umma_bf16(tmem + (uint32_t)(zz * COUT), da, db, IDESC, (tap | jp) ? 1u : 0u);
+          }
+        }
+      }
+      umma_commit(&mbar[1]);
+    }
+  }
+  __syncthreads();
+  const bool ok = s_ok && mbar_wait(&mbar[1], 0, status);
+  tc_fence_after();
+  // epilogue: warp w owns TMEM lanes 32w .. 32w+31 = rows r = x + 8y
+  const int r = 32 * warp + (tid & 31);
+  const int x = x0 + (r & 7), y = y0 + (r >> 3);
+#pragma unroll 1
+  for (int zz = 0; zz < ZT; ++zz) {
+    const long m = (((long)b * D + z0 + zz) * H + y) * W + x;
+#pragma unroll
+    for (int g = 0; g < COUT / 16; ++g) {
+      float v[16];
+      tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(zz * COUT + 16 * g), v);
+      float o[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const float tv = ok ? v[i] + (bias ? bias[16 * g + i] : 0.0f) : 0.0f;
+        o[i] = relu ? fmaxf(tv, 0.0f) : tv;
+      }
+      if (outf) {
+#pragma unroll
+        for (int i = 0; i < 16; i += 4)
+          *reinterpret_cast<float4 *>(outf + m * COUT + 16 * g + i) =
+              make_float4(o[i], o[i + 1], o[i + 2], o[i + 3]);
+      } else {
+        __align__(16) bf16 h[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) h[i] = __float2bfloat16_rn(o[i]);
+        uint4 *dst = reinterpret_cast<uint4 *>(out + m * COUT + 16 * g);
+        dst[0] = reinterpret_cast<const uint4 *>(h)[0];
+        dst[1] = reinterpret_cast<const uint4 *>(h)[1];
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, C::TMEM_COLS);
+}
+
+PFN_cuTensorMapEncodeTiled tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled encode = nullptr;
+  if (!encode) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess && fn)
+      encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(fn);
+  }
+  return encode;
+}
+
+template <int CIN, int COUT, int ZT>
+cudaError_t launch_direct(const void *x, int B, int D, int H, int W, const void *w,
+                          const float *bias, int relu, void *out, float *outf, int *status,
+                          cudaStream_t s) {
+  using C = DirectCfg<CIN, COUT, ZT>;
+  PFN_cuTensorMapEncodeTiled encode = tensor_map_encoder();
+  if (!encode) return cudaErrorNotSupported;
+  CUtensorMap tmap;
+  const cuuint64_t dims[5] = {(cuuint64_t)CIN, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)D,
+                              (cuuint64_t)B};
+  const cuuint64_t strides[4] = {(cuuint64_t)CIN * 2, (cuuint64_t)W * CIN * 2,
+                                 (cuuint64_t)H * W * CIN * 2, (cuuint64_t)D * H * W * CIN * 2};
+  const cuuint32_t box[5] = {8, 10, 18, (cuuint32_t)(ZT + 2), 1};
+  const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  if (reinterpret_cast<uintptr_t>(x) % 16 || reinterpret_cast<uintptr_t>(w) % 16 ||
+      encode(&tmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void *>(x), dims, strides, box,
+             estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return cudaErrorNotSupported;
+  auto kern = k_conv_direct<CIN, COUT, ZT>;
+  cudaError_t e =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem());
+  if (e != cudaSuccess) return e;
+  const unsigned grid = (unsigned)((long)B * (D / ZT) * (H / 16) * (W / 8));
+  kern<<<grid, 128, C::smem(), s>>>(tmap, static_cast<const bf16 *>(w), bias, relu,
+                                     static_cast<bf16 *>(out), outf, D, H, W, status);
+  return cudaGetLastError();
+}
+
+template <int CIN, int COUT>
+size_t direct_smem(int zt) {
+  return zt == 4 ? DirectCfg<CIN, COUT, 4>::smem()
+                 : zt == 2 ? DirectCfg<CIN, COUT, 2>::smem() : DirectCfg<CIN, COUT, 1>::smem();
+}
+
+// planes per tile for the direct kernel (0: the GEMM path): the deepest tile
+// whose grid still gives two CTAs per SM, else the shallowest (the most
+// CTAs), within two CTAs' shared memory per SM
+int direct_planes(int cin, int cout, int ntaps, int B, int D, int H, int W, int sms) {
+  // the input box (10 x 18 x (planes + 2) voxels) stays within the tensor's extents
+  if (ntaps != 27 || W % 8 || H % 16 || W < 16 || H < 32 || B < 1 || D < 3) return 0;
+  size_t (*smem)(int) = nullptr;
+  if (cin == 16 && cout == 16) smem = direct_smem<16, 16>;
+  else if (cin == 48 && cout == 16) smem = direct_smem<48, 16>;
+  else if (cin == 16 && cout == 32) smem = direct_smem<16, 32>;
+  else if (cin == 32 && cout == 32) smem = direct_smem<32, 32>;
+  if (!smem) return 0;
+  int shallowest = 0;
+  for (int zt : {4, 2, 1}) {
+    if (D % zt || D < zt + 2 || smem(zt) > 113u * 1024u) continue;
+    shallowest = zt;
+    if ((long)B * (D / zt) * (H / 16) * (W / 8) >= 2L * sms) return zt;
+  }
+  return shallowest;
+}
+
+template <int CIN, int COUT>
+cudaError_t direct_zt(int zt, const void *x, int B, int D, int H, int W, const void *w,
+                      const float *bias, int relu, void *out, float *outf, int *status,
+                      cudaStream_t s) {
+  if (zt == 4) return launch_direct<CIN, COUT, 4>(x, B, D, H, W, w, bias, relu, out, outf, status, s);
+  if (zt == 2) return launch_direct<CIN, COUT, 2>(x, B, D, H, W, w, bias, relu, out, outf, status, s);
+  return launch_direct<CIN, COUT, 1>(x, B, D, H, W, w, bias, relu, out, outf, status, s);
+}
+
+cudaError_t conv_direct(int zt, const void *x, int B, int D, int H, int W, int cin, const void *w,
+                        const float *bias, int cout, int relu, void *out, float *outf,
+                        int *status, cudaStream_t s) {
+  if (cin == 16 && cout == 16)
+    return direct_zt<16, 16>(zt, x, B, D, H, W, w, bias, relu, out, outf, status, s);
+  if (cin == 48 && cout == 16)
+    return direct_zt<48, 16>(zt, x, B, D, H, W, w, bias, relu, out, outf, status, s);
+  if (cin == 16 && cout == 32)
+    return direct_zt<16, 32>(zt, x, B, D, H, W, w, bias, relu, out, outf, status, s);
+  if (cin == 32 && cout == 32)
+    return direct_zt<32, 32>(zt, x, B, D, H, W, w, bias, relu, out, outf, status, s);
+  return cudaErrorInvalidValue;
+}
+
 }  // namespace
 
 // ---- host entry points (called from capi.cu) ---------------------------------
+// 1: every forward convolution on the implicit-GEMM kernel (the direct
+// kernel off), for comparing the two paths; process-wide
+static int g_gemm_only = 0;
+void nn_set_gemm_only(int on) { g_gemm_only = on ? 1 : 0; }
+
+int nn_conv_direct_planes(int B, int D, int H, int W, int cin, int cout, int ntaps) {
+  if (g_gemm_only) return 0;
+  int sms = 148, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return direct_planes(cin, cout, ntaps, B, D, H, W, sms);
+}
+
 bool nn_channels_ok(int c) { return dispatch_bn(c, [](auto) {}); }
 
 // K splits for a GEMM of `mtiles` row tiles and `ksteps` 64-deep steps:
@@ -780,6 +1033,13 @@ cudaError_t nn_conv_fwd(const void *x, int B, int D, int H, int W, int cin, cons
                         float *outf, float *scratch, size_t scratch_floats, int *status,
                         cudaStream_t s) {
   const long M = (long)B * D * H * W;
+  const int zt = nn_conv_direct_planes(B, D, H, W, cin, cout, ntaps);
+  if (zt > 0) {
+    // cudaErrorNotSupported: no tensor map for this tensor (nothing launched)
+    const cudaError_t e =
+        conv_direct(zt, x, B, D, H, W, cin, w, bias, cout, relu, out, outf, status, s);
+    if (e != cudaErrorNotSupported) return e;
+  }
   return conv_gemm<FwdTag>(x, make_vol(B, D, H, W), cin, ntaps, 1, w, cout, M, bias, relu, out,
                            outf, nullptr, scratch, scratch_floats, status, s);
 }

@@ -10,6 +10,8 @@
 namespace aw {
 bool nn_channels_ok(int c);
 size_t nn_splitk_floats(long M, int N, int K);
+int nn_conv_direct_planes(int B, int D, int H, int W, int cin, int cout, int ntaps);
+void nn_set_gemm_only(int on);
 cudaError_t nn_conv_fwd(const void *x, int B, int D, int H, int W, int cin, const void *w,
                         const float *bias, int cout, int ntaps, int relu, void *out, float *outf,
                         float *scratch, size_t scratch_floats, int *status, cudaStream_t s);
@@ -92,6 +94,13 @@ size_t aw_nn_conv3d_scratch_floats(int B, int D, int H, int W, int cin, int cout
   const size_t a = aw::nn_splitk_floats(M, cout, ntaps * cin);
   const size_t b = aw::nn_splitk_floats(M, cin, ntaps * cout);
   return a > b ? a : b;
+}
+
+void aw_nn_set_gemm_only(int on) { aw::nn_set_gemm_only(on); }
+
+int aw_nn_conv3d_direct_planes(int B, int D, int H, int W, int cin, int cout, int ntaps) {
+  if (!grid_ok(B, D, H, W)) return 0;
+  return aw::nn_conv_direct_planes(B, D, H, W, cin, cout, ntaps);
 }
 
 int aw_nn_conv3d_fwd(const void *x, int B, int D, int H, int W, int cin, const void *w,

@@ -268,6 +268,15 @@ int aw_ldmm_get_energies(aw_ldmm_t l, double *out, int max_count, int *count);
  * CTAs; the FP32 partials go to `scratch` (at least
  * aw_nn_conv3d_scratch_floats floats; NULL or smaller = no split). */
 size_t aw_nn_conv3d_scratch_floats(int B, int D, int H, int W, int cin, int cout, int ntaps);
+/* Planes per tile of the direct (TMA halo tile + shifted-descriptor MMA)
+ * kernel that aw_nn_conv3d_fwd uses for this shape: 3x3x3 taps, W % 8 == 0,
+ * H % 16 == 0, (cin, cout) in {(16,16), (48,16), (16,32), (32,32)};
+ * 0 = the implicit-GEMM kernel. Needs a current CUDA device. */
+int aw_nn_conv3d_direct_planes(int B, int D, int H, int W, int cin, int cout, int ntaps);
+/* on = 1: every forward convolution takes the implicit-GEMM kernel (the
+ * direct kernel off, process-wide), to compare the two paths; 0 restores
+ * the shape-based choice */
+void aw_nn_set_gemm_only(int on);
 /* out = act(conv(x, w) + bias): BF16 out_bf16, or FP32 out_f32 when given */
 int aw_nn_conv3d_fwd(const void *x, int B, int D, int H, int W, int cin, const void *w,
                      const float *bias, int cout, int ntaps, int relu, void *out_bf16,

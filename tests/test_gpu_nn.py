@@ -76,6 +76,50 @@ def test_conv_forward(grid, cin, cout, taps, split):
     assert rel(f32(outb).reshape(want.shape), np.maximum(want, 0)) <= 1e-2
 
 
+# shapes that take the direct kernel (TMA halo tile + shifted-descriptor
+# MMAs), with 1, 2 and 4 output planes per tile
+DIRECT = [(16, 16), (48, 16), (16, 32), (32, 32)]
+DIRECT_GRIDS = [(1, 8, 32, 16), (2, 6, 32, 24), (1, 32, 64, 64), (1, 64, 64, 64)]
+
+
+@pytest.mark.parametrize("grid", DIRECT_GRIDS)
+@pytest.mark.parametrize("cin,cout", DIRECT)
+def test_conv_forward_direct(grid, cin, cout):
+    L = _lib.lib()
+    B, D, H, W = grid
+    planes = L.aw_nn_conv3d_direct_planes(B, D, H, W, cin, cout, 27)
+    assert planes in (1, 2, 4)
+    rng = np.random.default_rng(cin * 3 + cout + D)
+    x = O.bf16(rng.normal(0, 1, (B, D, H, W, cin)).astype(np.float32))
+    w = O.bf16(rng.normal(0, 0.1, (cout, 27, cin)).astype(np.float32))
+    b = rng.normal(0, 0.1, cout).astype(np.float32)
+    want = O.conv_fwd(x, w, b, relu=False)
+    xd, wd, bd = bf(x), bf(w), torch.from_numpy(b).cuda()
+    outf = torch.zeros((B * D * H * W, cout), device="cuda")
+    rc = L.aw_nn_conv3d_fwd(xd.data_ptr(), B, D, H, W, cin, wd.data_ptr(), bd.data_ptr(), cout, 27,
+                            0, None, outf.data_ptr(), None, 0, None)
+    assert rc == 0, L.aw_last_error()
+    assert rel(f32(outf).reshape(want.shape), want) <= 1e-3
+    outb = torch.zeros((B * D * H * W, cout), dtype=torch.bfloat16, device="cuda")
+    rc = L.aw_nn_conv3d_fwd(xd.data_ptr(), B, D, H, W, cin, wd.data_ptr(), bd.data_ptr(), cout, 27,
+                            1, outb.data_ptr(), None, None, 0, None)
+    assert rc == 0
+    assert rel(f32(outb).reshape(want.shape), np.maximum(want, 0)) <= 1e-2
+
+
+def test_direct_plane_choice():
+    """The dispatcher's tile depth: 4 planes for the 64^3 16-channel layers,
+    2 for the 48-channel one (shared memory), 1 on small grids, and the
+    GEMM path (0) where the box would not fit or the channels are other."""
+    L = _lib.lib()
+    assert L.aw_nn_conv3d_direct_planes(1, 64, 64, 64, 16, 16, 27) == 4
+    assert L.aw_nn_conv3d_direct_planes(1, 64, 64, 64, 48, 16, 27) == 2
+    assert L.aw_nn_conv3d_direct_planes(1, 32, 32, 32, 16, 32, 27) == 1
+    assert L.aw_nn_conv3d_direct_planes(1, 16, 16, 16, 16, 16, 27) == 0
+    assert L.aw_nn_conv3d_direct_planes(1, 64, 64, 64, 96, 32, 27) == 0
+    assert L.aw_nn_conv3d_direct_planes(1, 64, 64, 64, 16, 16, 1) == 0
+
+
 @pytest.mark.parametrize("split", [False, True])
 @pytest.mark.parametrize("grid", [(1, 8, 8, 8), (1, 4, 6, 10)])
 @pytest.mark.parametrize("cin,cout,taps", CONFIGS)
@@ -146,7 +190,8 @@ def test_elementwise_layers():
 
 def test_network_gradients_match_oracle():
     """Forward and backward of the whole encoder-decoder at 16^3."""
-    shape = (16, 16, 16)
+    n = 16
+    shape = (n, n, n)
     net = WarmStartNet(shape, seed=5)
     # a head large enough that its gradient reaches every layer
     rng = np.random.default_rng(6)
@@ -162,7 +207,7 @@ def test_network_gradients_match_oracle():
                        {k: v.cpu().numpy() for k, v in net.b.items()})
     want = ref.forward(x).reshape(-1, 16)
     assert np.linalg.norm(out - want) <= 2e-2 * np.linalg.norm(want)
-    dout = O.bf16(rng.normal(0, 1e-3, (16 ** 3, 16)).astype(np.float32))
+    dout = O.bf16(rng.normal(0, 1e-3, (n ** 3, 16)).astype(np.float32))
     doutd = bf(dout)
     net.backward(doutd)
     g = ref.backward(dout.reshape((1,) + shape + (16,)).astype(np.float64))
@@ -173,6 +218,47 @@ def test_network_gradients_match_oracle():
         assert np.linalg.norm(gw - rw) <= 5e-2 * np.linalg.norm(rw), name
         assert np.linalg.norm(gb - rb) <= 5e-2 * max(np.linalg.norm(rb), 1e-12), name
     assert not net.timed_out()
+
+
+def test_network_direct_path_32():
+    """At 32^3 the level-0 convolutions take the direct kernel. Its forward
+    output agrees with the oracle and with the all-GEMM path; the weight
+    gradients point the oracle's way (BF16 activations and gradients
+    through 15 layers at 32^3 leave 4-16 % relative noise on either path,
+    so the check is the cosine, >= 0.97 per layer)."""
+    L = _lib.lib()
+    shape = (32, 32, 32)
+    assert L.aw_nn_conv3d_direct_planes(1, 32, 32, 32, 16, 16, 27) > 0
+    rng = np.random.default_rng(7)
+    I0 = rng.random(shape, dtype=np.float32)
+    I1 = rng.random(shape, dtype=np.float32)
+    dout = O.bf16(rng.normal(0, 1e-3, (32 ** 3, 16)).astype(np.float32))
+    doutd = bf(dout)
+    outs, grads = [], []
+    try:
+        for gemm_only in (0, 1):
+            L.aw_nn_set_gemm_only(gemm_only)
+            net = WarmStartNet(shape, seed=5)
+            net.w["head"].copy_(torch.from_numpy(
+                np.random.default_rng(6).normal(0, 0.2, (16, 1, 16)).astype(np.float32)))
+            net.refresh_bf16()
+            outs.append(f32(net.forward(torch.from_numpy(I0).cuda(), torch.from_numpy(I1).cuda())))
+            net.backward(doutd)
+            grads.append({k: f32(net.gw[k]) for k, *_ in LAYERS})
+    finally:
+        L.aw_nn_set_gemm_only(0)
+    x = np.zeros((1,) + shape + (16,), np.float32)
+    x[..., 0], x[..., 1] = O.bf16(I0), O.bf16(I1)
+    layers = [(n, ci, co, t, n != "head") for n, ci, co, t in LAYERS]
+    ref = O.UNetOracle(layers, {k: v.cpu().numpy() for k, v in net.w.items()},
+                       {k: v.cpu().numpy() for k, v in net.b.items()})
+    want = ref.forward(x).reshape(-1, 16)
+    assert np.linalg.norm(outs[0] - want) <= 1e-2 * np.linalg.norm(want)
+    assert np.linalg.norm(outs[0] - outs[1]) <= 1e-2 * np.linalg.norm(want)
+    g = ref.backward(dout.reshape((1,) + shape + (16,)).astype(np.float64))
+    for name, *_ in LAYERS:
+        a, r = grads[0][name].ravel(), g[name][0].ravel()
+        assert a @ r >= 0.97 * np.linalg.norm(a) * np.linalg.norm(r), name
 
 
 def test_parameter_count():
