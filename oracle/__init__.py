@@ -238,6 +238,64 @@ class Oracle:
             _i(int(update_step)), ctypes.c_float(max_pert))
         return float(e), float(st.value)
 
+    def ldmm_i1_at_0(self, I1, v, sp=(1.0, 1.0, 1.0), jacdet=True):
+        """LDMMDeformationData::GetI1At0 and LDMMIteratorCPU::ComputeJacDet
+        for velocities v [T,3,nz,ny,nx]. Returns (image, JacDet or None)."""
+        v = np.ascontiguousarray(v, np.float32)
+        img = np.empty(I1.shape, np.float32)
+        jd = np.empty(I1.shape, np.float32) if jacdet else None
+        self.lib.aw_oracle_ldmm_i1_at_0(_fp(I1), v.ctypes.data_as(_f), _i(v.shape[0]),
+                                        *_shape(I1), *map(_dbl, sp), _fp(img),
+                                        _fp(jd) if jd is not None else None)
+        return img, jd
+
+    def ldmm_atlas_mean_sums(self, imgs, vs, weights, sp=(1.0, 1.0, 1.0), jacobian_scale=True):
+        """One node's sums of LDMMAtlasThreadCPU::ComputeThreadMean: (sum w
+        I1At0 JacDet, sum w JacDet) with JacobianScale, else (sum w I1At0,
+        None); float32, subjects added in order (one thread per image)."""
+        acc = np.zeros(imgs[0].shape, np.float32)
+        jsum = np.zeros(imgs[0].shape, np.float32) if jacobian_scale else None
+        for img, v, w in zip(imgs, vs, weights):
+            d, jd = self.ldmm_i1_at_0(img, v, sp, jacdet=jacobian_scale)
+            w = np.float32(w)
+            if jacobian_scale:
+                acc += (d * jd) * w
+                jsum += jd * w
+            else:
+                acc += d * w
+        return acc, jsum
+
+    def ldmm_atlas_run(self, imgs, weights, T, iters, sp=(1.0, 1.0, 1.0), sigma=0.1, step=0.005,
+                       adaptive=False, max_pert=0.1, alpha=0.01, beta=0.01, gamma=0.001,
+                       use_new=True, jacobian_scale=True):
+        """LDMM relaxation atlas, the AtlasThreadMain loop (Algorithms/Common/
+        AtlasThread.txx:97-181) with LDMMAtlasThreadCPU's hooks
+        (LDMM/LDMMAtlasThreadCPU.cxx:146-264): mean from v = 0, then per
+        iteration every subject's LDMM iteration toward the mean (the
+        step-size pass first at iteration 0 when adaptive) and the mean
+        again, sum w I1At0 JacDet / sum w JacDet (LDMMAtlasBuilder.txx:
+        274-335). Returns (mean, [v_i], image energies [iters, ns])."""
+        ns = len(imgs)
+        vs = [np.zeros((T, 3) + imgs[0].shape, np.float32) for _ in range(ns)]
+        steps = [float(step)] * ns
+        it = self.ldmm_iterate if use_new else self.ldmm_iterate_orig
+        kw = dict(sp=sp, alpha=alpha, beta=beta, gamma=gamma, sigma=sigma)
+
+        def mean_of():
+            acc, jsum = self.ldmm_atlas_mean_sums(imgs, vs, weights, sp, jacobian_scale)
+            return acc / jsum if jacobian_scale else acc
+
+        mean = mean_of()
+        en = np.zeros((iters, ns))
+        for k in range(iters):
+            for i in range(ns):
+                if k == 0 and adaptive:
+                    _, steps[i] = it(mean, imgs[i], vs[i], step=steps[i], update_step=True,
+                                     max_pert=max_pert, **kw)
+                en[k, i], _ = it(mean, imgs[i], vs[i], step=steps[i], **kw)
+            mean = mean_of()
+        return mean, vs, en
+
     def greedy_run(self, I0, I1, iters, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01, gamma=0.001,
                    max_pert=0.5, inverse=False):
         """Single-scale greedy registration from the identity."""
@@ -452,6 +510,39 @@ class Reference:
                 ctypes.byref(st))
         self._check(rc)
         return v, en, float(st.value)
+
+    def ldmm_i1_at_0(self, I1, v, sp=(1.0, 1.0, 1.0)):
+        """The reference's GetI1At0 and ComputeJacDet for velocities v."""
+        v = np.ascontiguousarray(v, np.float32)
+        img = np.empty(I1.shape, np.float32)
+        jd = np.empty(I1.shape, np.float32)
+        with quiet_stdout():
+            rc = self.lib.awref_ldmm_i1_at_0(_fp(I1), v.ctypes.data_as(_f), *_shape(I1),
+                                             *map(_dbl, sp), _i(v.shape[0]), _fp(img), _fp(jd))
+        self._check(rc)
+        return img, jd
+
+    def ldmm_atlas_run(self, imgs, weights, T, iters, sp=(1.0, 1.0, 1.0), sigma=0.1, step=0.005,
+                       adaptive=False, max_pert=0.1, alpha=0.01, beta=0.01, gamma=0.001,
+                       use_new=True, jacobian_scale=True):
+        """The reference's LDMMDeformationData / LDMMIteratorCPU driven through
+        the AtlasThreadMain loop with the LDMM atlas thread's mean. Returns
+        (mean, [v_i], image energies [iters, ns])."""
+        ns = len(imgs)
+        n = imgs[0].size
+        stack = np.ascontiguousarray(np.stack(imgs), np.float32)
+        w = (ctypes.c_float * ns)(*weights)
+        mean = np.empty(imgs[0].shape, np.float32)
+        v = np.zeros((ns, T, 3) + imgs[0].shape, np.float32)
+        en = np.zeros((iters, ns), np.float64)
+        with quiet_stdout():
+            rc = self.lib.awref_ldmm_atlas_run(
+                stack.ctypes.data_as(_f), _i(ns), w, *_shape(imgs[0]), *map(_dbl, sp), _i(T),
+                _i(iters), ctypes.c_float(sigma), ctypes.c_float(step), _i(int(adaptive)),
+                ctypes.c_float(max_pert), _dbl(alpha), _dbl(beta), _dbl(gamma), _i(int(use_new)),
+                _i(int(jacobian_scale)), _fp(mean), v.ctypes.data_as(_f), _dp(en))
+        self._check(rc)
+        return mean, [v[k] for k in range(ns)], en
 
     def atlas_run(self, imgs, weights, iters, mean_period=1, sp=(1.0, 1.0, 1.0), alpha=0.01,
                   beta=0.01, gamma=0.001, max_pert=0.5):

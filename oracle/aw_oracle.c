@@ -769,6 +769,46 @@ double aw_oracle_ldmm_iterate_orig(const float *I0, const float *I1, float *v, i
 }
 
 /* ------------------------------------------------------------------------
+ * LDMM atlas pieces. GetI1At0: I1 pulled back to time 0 through
+ * h_{0->1} = (((id)(x + v_{T-1}/sp)) ... )(x + v_0/sp), composeHV with
+ * PARTIAL_ID from t = T-1 down to 0, then apply with background 0
+ * (LDMMDeformationData::GetDefTTo1 / GetI1AtT, LDMM/LDMMDeformationData.cxx:
+ * 255-265, 325-336). ComputeJacDet: JacDet = |D(x*sp + v_0)| *
+ * (|D(x*sp + v_1)| * (...)(x + v_1/sp))(x + v_0/sp), the transport of
+ * LDMMIteratorCPU::ComputeJacDet (LDMM/LDMMIteratorCPU.cxx:309-340).
+ * jd may be NULL.
+ * ---------------------------------------------------------------------- */
+void aw_oracle_ldmm_i1_at_0(const float *I1, const float *v, int T, int nx, int ny, int nz,
+                            double spx, double spy, double spz, float *img, float *jd) {
+  const long n = (long)nx * ny * nz;
+  float *h = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *o = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *jac = (float *)malloc(sizeof(float) * (size_t)n);
+  float *tmp = (float *)malloc(sizeof(float) * (size_t)n);
+  aw_oracle_identity(h, h + n, h + 2 * n, nx, ny, nz);
+  for (int t = T - 1; t >= 0; --t) {
+    const float *vt = v + (long)t * 3 * n;
+    aw_oracle_compose_hv(h, h + n, h + 2 * n, vt, vt + n, vt + 2 * n, o, o + n, o + 2 * n, nx, ny,
+                         nz, spx, spy, spz, 1, AW_BG_PARTIAL_ID);
+    memcpy(h, o, sizeof(float) * (size_t)(3 * n));
+    if (jd) {
+      aw_oracle_jacobian(vt, vt + n, vt + 2 * n, jac, nx, ny, nz, spx, spy, spz);
+      if (t == T - 1) {
+        memcpy(jd, jac, sizeof(float) * (size_t)n);
+      } else {
+        aw_oracle_apply_u(jd, vt, vt + n, vt + 2 * n, tmp, nx, ny, nz, spx, spy, spz, 0.0f);
+        for (long k = 0; k < n; ++k) jd[k] = tmp[k] * jac[k];
+      }
+    }
+  }
+  aw_oracle_apply(I1, h, h + n, h + 2 * n, img, nx, ny, nz, 0.0f);
+  free(h);
+  free(o);
+  free(jac);
+  free(tmp);
+}
+
+/* ------------------------------------------------------------------------
  * Multiscale (Algorithms/Common/MultiscaleManager.cxx:301-366).
  * ---------------------------------------------------------------------- */
 

@@ -71,6 +71,9 @@ double aw_oracle_ldmm_iterate_orig(const float *I0, const float *I1, float *v, i
                                    int ny, int nz, double spx, double spy, double spz,
                                    double alpha, double beta, double gamma, float sigma,
                                    float *step, int update_step, float max_pert);
+/* GetI1At0 (I1 pulled back through the velocities) and ComputeJacDet */
+void aw_oracle_ldmm_i1_at_0(const float *I1, const float *v, int T, int nx, int ny, int nz,
+                            double spx, double spy, double spz, float *img, float *jd);
 
 void aw_oracle_gauss_blur(const float *in, float *out, int nx, int ny, int nz, float sx, float sy,
                           float sz, int kx, int ky, int kz);

@@ -476,4 +476,157 @@ int awref_ldmm_run(const float *i0, const float *i1, int nx, int ny, int nz, dou
   GUARD_END
 }
 
+/*
+ * LDMMDeformationData::GetI1At0 and LDMMIteratorCPU::ComputeJacDet for
+ * given velocities v [T][3][N] (jd may be NULL).
+ */
+int awref_ldmm_i1_at_0(const float *i1, const float *v, int nx, int ny, int nz, double spx,
+                       double spy, double spz, int T, float *img, float *jd) {
+  GUARD_BEGIN
+  std::ostringstream xml;
+  xml << "<LDMMWarpParameterFile><LDMMScaleLevel><ScaleLevel><DownsampleFactor val=\"1\"/>"
+      << "</ScaleLevel><LDMMIterator>" << diffoper_xml(0.01, 0.01, 0.001)
+      << "</LDMMIterator><NIterations val=\"1\"/></LDMMScaleLevel><NTimeSteps val=\"" << T
+      << "\"/></LDMMWarpParameterFile>";
+  LDMMParam param;
+  parse_into(param, xml.str());
+  SizeType size(nx, ny, nz);
+  SpacingType sp(spx, spy, spz);
+  OriginType origin(0, 0, 0);
+  RealImage I0(size, origin, sp), I1(size, origin, sp);
+  to_im(i1, I0);
+  to_im(i1, I1);
+  MultiscaleManager scaleManager(size, sp, origin, param);
+  scaleManager.SetScaleVectorFields(false);
+  LDMMDeformationData data(&I0, &I1, param);
+  LDMMIteratorNewCPU iterator(size, origin, sp, T, false, false);
+  const long n = (long)nx * ny * nz;
+  data.InitializeWarp();
+  scaleManager.SetScaleLevel(0);
+  iterator.SetScaleLevel(scaleManager, param.GetScaleLevel(0).Iterator());
+  data.SetScaleLevel(scaleManager);
+  for (int t = 0; t < T; ++t)
+    to_vf(v + t * 3 * n, v + t * 3 * n + n, v + t * 3 * n + 2 * n, data.v(t));
+  RealImage def(size, origin, sp);
+  data.GetI1At0(def);
+  from_im(def, img);
+  if (jd) {
+    RealImage jac(size, origin, sp);
+    iterator.ComputeJacDet(data.v(), &jac);
+    from_im(jac, jd);
+  }
+  GUARD_END
+}
+
+/*
+ * LDMM relaxation atlas: the AtlasThreadMain loop (Algorithms/Common/
+ * AtlasThread.txx:97-181) with the LDMM thread's hooks
+ * (LDMM/LDMMAtlasThreadCPU.cxx): every subject is an LDMMDeformationData
+ * with I0 = the shared mean (not rescaled, as LDMMAtlasDefDataCPU) and I1 =
+ * its image, one LDMMIteratorCPU per subject (one thread per image, the
+ * default); BeginImageIteration's step-size pass at iteration 0; the mean
+ * after every iteration from GetI1At0 and ComputeJacDet
+ * (ComputeThreadMean, :207-264, JacobianScale: sum w I1At0 JacDet /
+ * sum w JacDet, LDMMAtlasBuilder.txx:274-335), thread sums added in
+ * subject order. mean out; v out as [ns][T][3][N]; energies[iter][i] = the
+ * image term of each subject's last iteration.
+ */
+int awref_ldmm_atlas_run(const float *imgs, int ns, const float *weights, int nx, int ny, int nz,
+                         double spx, double spy, double spz, int T, int iters, float sigma,
+                         float step, int adaptive, float max_pert, double alpha, double beta,
+                         double gamma, int use_new, int jacobian_scale, float *mean_out,
+                         float *v_out, double *energies) {
+  GUARD_BEGIN
+  std::ostringstream xml;
+  xml.precision(17);
+  xml << "<LDMMWarpParameterFile><LDMMScaleLevel><ScaleLevel><DownsampleFactor val=\"1\"/>"
+      << "</ScaleLevel><LDMMIterator>" << diffoper_xml(alpha, beta, gamma) << "<Sigma val=\""
+      << sigma << "\"/><StepSize val=\"" << step << "\"/><UseAdaptiveStepSize val=\""
+      << (adaptive ? "true" : "false") << "\"/><MaxPert val=\"" << max_pert
+      << "\"/></LDMMIterator><NIterations val=\"" << iters
+      << "\"/></LDMMScaleLevel><NTimeSteps val=\"" << T
+      << "\"/><AutoStepReduce val=\"false\"/></LDMMWarpParameterFile>";
+  LDMMParam param;
+  parse_into(param, xml.str());
+  SizeType size(nx, ny, nz);
+  SpacingType sp(spx, spy, spz);
+  OriginType origin(0, 0, 0);
+  const long n = (long)nx * ny * nz;
+  RealImage mean(size, origin, sp);
+  std::vector<RealImage *> I(ns);
+  std::vector<LDMMDeformationData *> data(ns);
+  std::vector<LDMMIteratorNewCPU *> it(ns);
+  MultiscaleManager scaleManager(size, sp, origin, param);
+  scaleManager.SetScaleVectorFields(false);
+  scaleManager.SetScaleLevel(0);
+  const LDMMScaleLevelParam &lp = param.GetScaleLevel(0);
+  for (int i = 0; i < ns; ++i) {
+    I[i] = new RealImage(size, origin, sp);
+    to_im(imgs + i * n, *I[i]);
+    data[i] = new LDMMDeformationData(&mean, I[i], param);
+    data[i]->ScaleI0(false);
+    it[i] = new LDMMIteratorNewCPU(size, origin, sp, T, true, use_new != 0);
+    data[i]->InitializeWarp();
+    it[i]->SetScaleLevel(scaleManager, lp.Iterator());
+    data[i]->SetScaleLevel(scaleManager);
+    data[i]->StepSize(lp.Iterator().StepSize());
+  }
+  RealImage def(size, origin, sp), jac(size, origin, sp), jsum(size, origin, sp);
+  auto compute_mean = [&]() {
+    RealImage acc(size, origin, sp);
+    acc.fill(0.0);
+    jsum.fill(0.0);
+    for (int i = 0; i < ns; ++i) {
+      RealImage tm(size, origin, sp), tj(size, origin, sp);  // the image's thread sums
+      tm.fill(0.0);
+      tj.fill(0.0);
+      data[i]->GetI1At0(def);
+      it[i]->ComputeJacDet(data[i]->v(), &jac);
+      const Real w = weights[i];
+      Real *pm = tm.getDataPointer(), *pj = tj.getDataPointer();
+      const Real *pd = def.getDataPointer(), *pc = jac.getDataPointer();
+      for (long j = 0; j < n; ++j) {
+        if (jacobian_scale) {
+          pm[j] += pd[j] * pc[j] * w;
+          pj[j] += pc[j] * w;
+        } else {
+          pm[j] += pd[j] * w;
+        }
+      }
+      acc.pointwiseAdd(tm);
+      jsum.pointwiseAdd(tj);
+    }
+    if (jacobian_scale) acc.pointwiseDivideBy(jsum);
+    mean = acc;
+  };
+  compute_mean();
+  for (int iter = 0; iter < iters; ++iter) {
+    for (int i = 0; i < ns; ++i) {
+      data[i]->SetCurIter(iter);
+      if (iter == 0 && lp.Iterator().UseAdaptiveStepSize()) {
+        it[i]->UpdateStepSizeNextIteration();
+        it[i]->Iterate(*data[i]);
+      }
+      it[i]->Iterate(*data[i]);
+      if (energies) {
+        LDMMEnergy *e = dynamic_cast<LDMMEnergy *>(data[i]->GetEnergyHistory().LastEnergy());
+        energies[iter * ns + i] = e ? (double)e->ImageEnergy() * sigma * sigma : 0.0;
+      }
+    }
+    compute_mean();
+  }
+  from_im(mean, mean_out);
+  for (int i = 0; i < ns; ++i)
+    for (int t = 0; t < T; ++t) {
+      float *vt = v_out + ((long)i * T + t) * 3 * n;
+      from_vf(data[i]->v(t), vt, vt + n, vt + 2 * n);
+    }
+  for (int i = 0; i < ns; ++i) {
+    delete it[i];
+    delete data[i];
+    delete I[i];
+  }
+  GUARD_END
+}
+
 }  // extern "C"

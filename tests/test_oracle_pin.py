@@ -98,3 +98,41 @@ def test_jacobian_of_identity_map_is_spacing_volume(oracle):
     v = np.zeros((3, 6, 7, 8), np.float32)
     jac = oracle.jacobian(v, (1.5, 0.75, 1.25))
     assert np.allclose(jac, 1.0)  # d(x*sp)/dx / sp = 1 per axis
+
+
+def test_ldmm_i1_at_0_matches_reference(oracle, reference):
+    """GetI1At0 and ComputeJacDet for nonzero velocities (from three LDMM
+    iterations), anisotropic spacing: the restatement against the
+    reference's LDMMDeformationData / LDMMIteratorCPU."""
+    shape, T = (12, 14, 16), 4
+    sp = (1.5, 0.75, 1.25)
+    I0, I1 = greedy_pair(shape, 5, n_blobs=4, umax=1.5, sigma_range=(1.5, 3.0), smooth_sigma=3.0)
+    v, _, _ = reference.ldmm_run(I0, I1, T, 3, sp=sp, sigma=1.0, step=0.01)
+    img_r, jd_r = reference.ldmm_i1_at_0(I1, v, sp)
+    img_o, jd_o = oracle.ldmm_i1_at_0(I1, v, sp)
+    assert np.array_equal(img_o, img_r)
+    assert np.array_equal(jd_o, jd_r)
+    assert np.abs(jd_o - 1.0).max() > 1e-3  # the velocities are not trivial
+
+
+@pytest.mark.parametrize("use_new,jacobian_scale,adaptive", [(True, True, False),
+                                                              (False, True, True),
+                                                              (True, False, False)])
+def test_ldmm_atlas_matches_reference(oracle, reference, use_new, jacobian_scale, adaptive):
+    """Three subjects, three atlas iterations of LDMM relaxation (IterateNew
+    or IterateOrig, with or without JacobianScale, fixed or adaptive step):
+    the restated loop against the reference's classes driven through the
+    AtlasThreadMain loop."""
+    shape, T = (12, 12, 12), 3
+    imgs = [greedy_pair(shape, 40 + k, n_blobs=4, umax=1.5, sigma_range=(1.5, 3.0),
+                        smooth_sigma=3.0)[1] for k in range(3)]
+    w = [0.5, 0.3, 0.2]
+    kw = dict(sigma=1.0, step=0.01, adaptive=adaptive, max_pert=0.2, use_new=use_new,
+              jacobian_scale=jacobian_scale)
+    mr, vr, er = reference.ldmm_atlas_run(imgs, w, T, 3, **kw)
+    mo, vo, eo = oracle.ldmm_atlas_run(imgs, w, T, 3, **kw)
+    assert np.abs(mo - mr).max() <= 1e-5 * np.abs(mr).max()
+    for a, b in zip(vo, vr):
+        assert np.abs(a - b).max() <= 1e-4 * max(np.abs(b).max(), 1e-12)
+    assert np.allclose(eo, er, rtol=1e-4)
+    assert np.abs(vr[0]).max() > 0
