@@ -682,6 +682,31 @@ int aw_ldmm_run(aw_ldmm_t l, const float *I0, const float *I1, float *v, int n_i
   return 0;
 }
 
+int aw_ldmm_i1_at_0(aw_ldmm_t l, const float *I1, const float *v, float *img, float *jacdet,
+                    void *stream) {
+  if (!l || !I1 || !v || !img) return fail("aw_ldmm_i1_at_0: null pointer");
+  AW_CUDA(aw::ldmm_i1_at_0(&l->ctx, I1, v, img, jacdet, S(stream)), "aw_ldmm_i1_at_0");
+  return 0;
+}
+
+int aw_ldmm_atlas_accumulate(float *acc, float *jacsum, const float *img, const float *jacdet,
+                             float weight, long n, void *stream) {
+  if (!acc || !img || (jacdet && !jacsum)) return fail("aw_ldmm_atlas_accumulate: null pointer");
+  if (n < 0) return fail("aw_ldmm_atlas_accumulate: negative size");
+  if (n == 0) return 0;
+  AW_CUDA(aw::ldmm_atlas_accumulate(acc, jacsum, img, jacdet, weight, n, S(stream)),
+          "aw_ldmm_atlas_accumulate");
+  return 0;
+}
+
+int aw_ldmm_atlas_normalize(float *acc, const float *jacsum, long n, void *stream) {
+  if (!acc || !jacsum) return fail("aw_ldmm_atlas_normalize: null pointer");
+  if (n < 0) return fail("aw_ldmm_atlas_normalize: negative size");
+  if (n == 0) return 0;
+  AW_CUDA(aw::ldmm_atlas_normalize(acc, jacsum, n, S(stream)), "aw_ldmm_atlas_normalize");
+  return 0;
+}
+
 int aw_ldmm_get_energies(aw_ldmm_t l, double *out, int max_count, int *count) {
   if (!l || !count) return fail("aw_ldmm_get_energies: null pointer");
   AW_CUDA(cudaDeviceSynchronize(), "aw_ldmm_get_energies (pending work)");

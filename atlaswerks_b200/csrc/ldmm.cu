@@ -304,6 +304,78 @@ cudaError_t ldmm_iterate(LdmmCtx *c, const float *I0, const float *I1, float *v,
   return cudaSuccess;
 }
 
+// LDMMDeformationData::GetI1At0 (LDMM/LDMMDeformationData.cxx:255-265,
+// 325-336: h_{0->1} by composeHV [PARTIAL_ID] from t = T-1 down to 0, then
+// apply with background 0) and LDMMIteratorCPU::ComputeJacDet
+// (LDMMIteratorCPU.cxx:309-340), the same backward sweep as IterateOrig's.
+// The Jacobian ping-pongs between jd and the context's splat buffer so that
+// t = 0 lands in jd; jd may be null.
+cudaError_t ldmm_i1_at_0(LdmmCtx *c, const float *I1, const float *v, float *img, float *jd,
+                         cudaStream_t s) {
+  const Dims d = c->d;
+  const long n = d.n();
+  const int T = c->T;
+  float *H[2] = {c->hbuf, c->hbuf + 3 * n};
+  auto comp = [&](float *base, int k) { return base + k * n; };
+  auto vcomp = [&](const float *base, int k) { return base + k * n; };
+  const DivD a2 = make_div(2.0 * c->sp.x), b2 = make_div(2.0 * c->sp.y), e2 = make_div(2.0 * c->sp.z);
+  const DivD a1 = make_div(c->sp.x), b1 = make_div(c->sp.y), e1 = make_div(c->sp.z);
+  auto jbuf = [&](int t) { return (t % 2 == 0) ? jd : c->S; };
+  k_identity<<<row_grid(d), kRowThreads, 0, s>>>(comp(H[0], 0), comp(H[0], 1), comp(H[0], 2), d);
+  AW_TRY(cudaGetLastError());
+  int cur = 0;
+  for (int t = T - 1; t >= 0; --t) {
+    const float *vt = v + (long)t * 3 * n;
+    k_forward_step<true><<<row_grid(d), kRowThreads, 0, s>>>(
+        comp(H[cur], 0), comp(H[cur], 1), comp(H[cur], 2), vcomp(vt, 0), vcomp(vt, 1),
+        vcomp(vt, 2), comp(H[1 - cur], 0), comp(H[1 - cur], 1), comp(H[1 - cur], 2), I1,
+        t == 0 ? img : nullptr, d, c->sp);
+    AW_TRY(cudaGetLastError());
+    cur = 1 - cur;
+    if (jd) {
+      k_jacdet<<<row_grid(d), kRowThreads, 0, s>>>(vcomp(vt, 0), vcomp(vt, 1), vcomp(vt, 2),
+                                                   t == T - 1 ? nullptr : jbuf(t + 1), jbuf(t),
+                                                   d, c->sp, a2, b2, e2, a1, b1, e1);
+      AW_TRY(cudaGetLastError());
+    }
+  }
+  return cudaSuccess;
+}
+
+namespace {
+// LDMMAtlasThreadCPU::ComputeThreadMean's sums (LDMM/LDMMAtlasThreadCPU.cxx:
+// 243-252), float in the reference's order: acc += (img * jd) * w and
+// jsum += jd * w with JacobianScale (jd given), else acc += img * w
+__global__ void k_atlas_accumulate(float *__restrict__ acc, float *__restrict__ jsum,
+                                   const float *__restrict__ img, const float *__restrict__ jd,
+                                   float w, long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (jd) {
+    acc[i] = fadd(acc[i], fmul(fmul(img[i], jd[i]), w));
+    jsum[i] = fadd(jsum[i], fmul(jd[i], w));
+  } else {
+    acc[i] = fadd(acc[i], fmul(img[i], w));
+  }
+}
+// mean = acc / jsum (RealImage::pointwiseDivideBy, LDMMAtlasBuilder.txx:332-334)
+__global__ void k_atlas_normalize(float *__restrict__ acc, const float *__restrict__ jsum, long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) acc[i] = fdiv(acc[i], jsum[i]);
+}
+}  // namespace
+
+cudaError_t ldmm_atlas_accumulate(float *acc, float *jsum, const float *img, const float *jd,
+                                  float w, long n, cudaStream_t s) {
+  k_atlas_accumulate<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(acc, jsum, img, jd, w, n);
+  return cudaGetLastError();
+}
+
+cudaError_t ldmm_atlas_normalize(float *acc, const float *jsum, long n, cudaStream_t s) {
+  k_atlas_normalize<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(acc, jsum, n);
+  return cudaGetLastError();
+}
+
 int ldmm_set_orig(LdmmCtx *c, int on) {
   c->orig = on ? 1 : 0;
   if (c->orig && !c->JT) {

@@ -39,6 +39,11 @@ void ldmm_destroy(LdmmCtx *c);
 // LDMMIteratorCPU's UseOrigGradientCalc: 1 selects IterateOrig (the
 // reference's default), 0 IterateNew; allocates the IterateOrig buffers
 int ldmm_set_orig(LdmmCtx *c, int on);
+cudaError_t ldmm_i1_at_0(LdmmCtx *c, const float *I1, const float *v, float *img, float *jd,
+                         cudaStream_t s);
+cudaError_t ldmm_atlas_accumulate(float *acc, float *jsum, const float *img, const float *jd,
+                                  float w, long n, cudaStream_t s);
+cudaError_t ldmm_atlas_normalize(float *acc, const float *jsum, long n, cudaStream_t s);
 // One iteration (IterateNew or IterateOrig); v is [T][3][N]. update_step:
 // compute the step from max |2v - (2/sigma^2) K f| and leave v unchanged.
 cudaError_t ldmm_iterate(LdmmCtx *c, const float *I0, const float *I1, float *v, int update_step,

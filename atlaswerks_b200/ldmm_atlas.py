@@ -1,0 +1,191 @@
+"""Host-side mirror of the reference's LDMM relaxation atlas builder.
+
+``LDMMAtlasBuilderB200`` follows LDMMAtlasBuilder (Algorithms/LDMM/
+LDMMAtlasBuilder.h, .txx:20-335) and the per-thread hooks of
+LDMMAtlasThreadCPU / LDMMAtlasThreadGPU inside AtlasThread::AtlasThreadMain
+(Algorithms/Common/AtlasThread.txx:97-181):
+
+* every subject i is an LDMM registration whose I0 is the shared mean
+  template (not rescaled: LDMMAtlasDefDataCPU, LDMMAtlasThreadCPU.cxx:41-53)
+  and whose I1 is the subject's image, with T velocity fields of its own;
+* the mean starts from v = 0 (the weighted mean of the subjects) and, after
+  every iteration of all subjects (BeginImageIteration's step-size pass
+  first at iteration 0 with UseAdaptiveStepSize), becomes
+  sum_i w_i I1_i(h_i,0->1) |D h_i| / sum_i w_i |D h_i| (JacobianScale, the
+  default) or sum_i w_i I1_i(h_i,0->1): GetI1At0 and ComputeJacDet per
+  subject (LDMMAtlasThreadCPU::ComputeThreadMean, .cxx:207-264), the sums of
+  all threads and nodes, then the division (LDMMAtlasBuilder::ComputeMean,
+  .txx:274-335);
+* with several processes (one per GPU), rank r owns subjects
+  {i : i mod world == r}; each rank forms its two partial sums and two
+  all-reduces (sum) over the process group complete them, the exchange of
+  LDMMAtlasBuilder::SumAcrossNodes (.txx:236-269, MPI_Allreduce there).
+
+Not built: ComputeMedian / TrimmedMeanSize re-weighting, UsePerVoxelMedian,
+the PCA step, multiscale (one scale level per BuildAtlas call).
+
+The per-rank work runs in libaw_b200.so (``aw_ldmm_*``) through
+``CudaLDMMAtlasEngine``; the builder only sequences it and the collectives.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check
+from .atlas import local_subjects
+from .device import _check_image, _stream
+from .ldmm import LDMMDeformationDataB200, LDMMIteratorB200, LDMMIteratorParam
+
+
+@dataclass
+class LDMMAtlasParam:
+    """LDMMAtlasParam (Algorithms/LDMM/LDMMAtlasParam.h:26-147) at one scale
+    level: the iterator, NTimeSteps, NIterations, JacobianScale, and the
+    gradient variant (IterateOrig with UseOrigGradientCalc)."""
+    Iterator: LDMMIteratorParam = field(default_factory=LDMMIteratorParam)
+    NTimeSteps: int = 5
+    NIterations: int = 50
+    JacobianScale: bool = True
+    UseOrigGradientCalc: bool = False
+
+
+class CudaLDMMAtlasEngine:
+    """The subjects of one rank on its GPU: one LDMM handle per subject (the
+    reference runs one thread, hence one iterator, per image), the shared
+    mean they read as I0, and the two sums of the mean."""
+
+    def __init__(self, size: Sequence[int], spacing: Sequence[float], param: LDMMAtlasParam,
+                 images: Sequence[torch.Tensor], weights: Sequence[float]):
+        nx, ny, nz = size
+        self.shape = (nz, ny, nx)
+        self.param = param
+        self.w = [float(x) for x in weights]
+        self.n = nx * ny * nz
+        self.mean = torch.zeros(self.shape, device="cuda")
+        self.acc = torch.zeros(self.shape, device="cuda")
+        self.jsum = torch.zeros(self.shape, device="cuda")
+        self._img = torch.zeros(self.shape, device="cuda")
+        self._jd = torch.zeros(self.shape, device="cuda")
+        self.images = list(images)
+        self.its: List[LDMMIteratorB200] = []
+        self.data: List[LDMMDeformationDataB200] = []
+        for i, img in enumerate(self.images):
+            _check_image(img, f"image {i}")
+            if tuple(img.shape) != self.shape:
+                raise ValueError("LDMM atlas subjects must be on the template grid")
+            it = LDMMIteratorB200(size, spacing=spacing, n_time_steps=param.NTimeSteps)
+            it.SetUseOrigGradientCalc(param.UseOrigGradientCalc)
+            it.SetScaleLevel(size, spacing, param.Iterator)
+            self.its.append(it)
+            self.data.append(LDMMDeformationDataB200(self.mean, img, param.NTimeSteps, spacing))
+
+    def mean_sums(self):
+        """This rank's (sum w I1At0 JacDet, sum w JacDet), or (sum w I1At0,
+        None) without JacobianScale, in subject order."""
+        L, s = _lib.lib(), _stream()
+        js = self.param.JacobianScale
+        self.acc.zero_()
+        self.jsum.zero_()
+        for it, d, w in zip(self.its, self.data, self.w):
+            check(L.aw_ldmm_i1_at_0(it._h, d.I1.data_ptr(), d.V.data_ptr(), self._img.data_ptr(),
+                                    self._jd.data_ptr() if js else None, s))
+            check(L.aw_ldmm_atlas_accumulate(self.acc.data_ptr(), self.jsum.data_ptr(),
+                                             self._img.data_ptr(),
+                                             self._jd.data_ptr() if js else None, w, self.n, s))
+        return self.acc, (self.jsum if js else None)
+
+    def set_mean(self, acc: torch.Tensor, jsum: Optional[torch.Tensor]) -> torch.Tensor:
+        """The new mean from the (all-reduced) sums, into the I0 every
+        subject's iterations read."""
+        if jsum is not None:
+            check(_lib.lib().aw_ldmm_atlas_normalize(acc.data_ptr(), jsum.data_ptr(), self.n,
+                                                     _stream()))
+        self.mean.copy_(acc)
+        return self.mean
+
+    def iterate(self, first: bool) -> None:
+        adaptive = first and self.param.Iterator.UseAdaptiveStepSize
+        for it, d in zip(self.its, self.data):
+            it.Run(d, 1, adaptive_first=adaptive)
+
+    def velocities(self, i: int) -> torch.Tensor:
+        return self.data[i].V
+
+    def step(self, i: int) -> float:
+        return self.its[i].StepSize()
+
+    def energies(self, i: int) -> np.ndarray:
+        return self.its[i].Energies()
+
+
+class LDMMAtlasBuilderB200:
+    """LDMMAtlasBuilder over the subjects of this rank (one scale level).
+
+    images / weights are the GLOBAL lists (only the local images need to be
+    real tensors); weights default to 1/N. ``group`` is a torch.distributed
+    process group (None: one process). ``engine_factory(size, spacing,
+    param, images, weights)`` builds the per-rank engine (default
+    CudaLDMMAtlasEngine).
+    """
+
+    def __init__(self, images: Sequence[Optional[torch.Tensor]], size: Sequence[int],
+                 param: LDMMAtlasParam, spacing=(1.0, 1.0, 1.0),
+                 weights: Optional[Sequence[float]] = None, group=None, engine_factory=None):
+        self.n_total = len(images)
+        if self.n_total < 1:
+            raise ValueError("an atlas needs at least one image")
+        if weights is None:
+            weights = [1.0 / self.n_total] * self.n_total
+        if len(weights) != self.n_total:
+            raise ValueError("one weight per image")
+        self.param = param
+        self.group = group
+        if group is not None:
+            import torch.distributed as dist
+            self.rank, self.world = dist.get_rank(group), dist.get_world_size(group)
+        else:
+            self.rank, self.world = 0, 1
+        self.local = local_subjects(self.n_total, self.rank, self.world)
+        if not self.local:
+            raise ValueError(f"rank {self.rank} owns no subject: use at most {self.n_total} ranks")
+        factory = engine_factory or CudaLDMMAtlasEngine
+        self.engine = factory(tuple(size), tuple(float(s) for s in spacing), param,
+                              [images[i] for i in self.local], [weights[i] for i in self.local])
+        self.mean = None
+
+    def _update_mean(self):
+        acc, jsum = self.engine.mean_sums()
+        if self.group is not None and self.world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(acc, op=dist.ReduceOp.SUM, group=self.group)
+            if jsum is not None:
+                dist.all_reduce(jsum, op=dist.ReduceOp.SUM, group=self.group)
+        self.mean = self.engine.set_mean(acc, jsum)
+
+    def BuildAtlas(self):
+        """The AtlasThreadMain loop at one scale level: the mean, then per
+        iteration every subject's LDMM iteration and the mean again."""
+        self._update_mean()
+        for k in range(self.param.NIterations):
+            self.engine.iterate(first=(k == 0))
+            self._update_mean()
+        return self.mean
+
+    def GetMeanImage(self) -> torch.Tensor:
+        return self.mean
+
+    def GetVelocities(self, i: int) -> torch.Tensor:
+        """v [T, 3, nz, ny, nx] of global subject i (local to this rank)."""
+        return self.engine.velocities(self.local.index(i))
+
+    def GetStepSize(self, i: int) -> float:
+        return self.engine.step(self.local.index(i))
+
+    def GetEnergies(self, i: int) -> np.ndarray:
+        return self.engine.energies(self.local.index(i))

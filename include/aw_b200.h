@@ -254,6 +254,28 @@ int aw_ldmm_run(aw_ldmm_t l, const float *I0, const float *I1, float *v, int n_i
 /* Image energies sp^3 * sum (I0(h_T) - I1)^2, oldest first; synchronises. */
 int aw_ldmm_get_energies(aw_ldmm_t l, double *out, int max_count, int *count);
 
+/* LDMM relaxation atlas (LDMMAtlasBuilder / LDMMAtlasThreadCPU,
+ * Algorithms/LDMM/LDMMAtlasThreadCPU.cxx:207-264, LDMMAtlasBuilder.txx:274-335).
+ * Every subject is an aw_ldmm_t whose I0 is the shared mean and I1 its image;
+ * after the subjects' iterations the caller forms
+ *   mean = sum_i w_i I1_i(h_{0->1}) JacDet_i / sum_i w_i JacDet_i
+ * (JacobianScale), or sum_i w_i I1_i(h_{0->1}), from these three calls
+ * (across processes: sum acc and jacsum, e.g. one all-reduce each, before
+ * normalising).
+ *
+ * aw_ldmm_i1_at_0: LDMMDeformationData::GetI1At0 (I1 pulled back to time 0
+ * through v) into img and LDMMIteratorCPU::ComputeJacDet into jacdet (NULL:
+ * skipped); v is [T][3][N] of the handle's grid. Uses the handle's scratch:
+ * not concurrent with its iterations. */
+int aw_ldmm_i1_at_0(aw_ldmm_t l, const float *I1, const float *v, float *img, float *jacdet,
+                    void *stream);
+/* acc += (img * jacdet) * weight and jacsum += jacdet * weight (float, in
+ * that order), or acc += img * weight when jacdet is NULL; n voxels */
+int aw_ldmm_atlas_accumulate(float *acc, float *jacsum, const float *img, const float *jacdet,
+                             float weight, long n, void *stream);
+/* acc /= jacsum (float division), n voxels */
+int aw_ldmm_atlas_normalize(float *acc, const float *jacsum, long n, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Learned warm start: the kernels of a 3D convolutional encoder-decoder
  * (no counterpart in the reference; it predicts an initial deformation
