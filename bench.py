@@ -531,6 +531,53 @@ def run_ldmm(args):
     return 0
 
 
+def run_ldmm_atlas(args):
+    """LDMM relaxation atlas: 4 subjects at 128^3, T = 5 time steps,
+    IterateNew, sigma 1, fixed step 0.01, JacobianScale mean after every
+    iteration; a step = one atlas iteration (every subject's LDMM iteration,
+    then GetI1At0 + ComputeJacDet of every subject and the mean)."""
+    import torch
+
+    from atlaswerks_b200.greedy import DiffOperParam
+    from atlaswerks_b200.ldmm import LDMMIteratorParam
+    from atlaswerks_b200.ldmm_atlas import LDMMAtlasBuilderB200, LDMMAtlasParam
+    from atlaswerks_b200.synth import greedy_pair
+    ns, T = 4, 5
+    imgs = [torch.from_numpy(greedy_pair((N, N, N), 300 + k, 8, 3.0)[1]).cuda() for k in range(ns)]
+    param = LDMMAtlasParam(LDMMIteratorParam(DiffOperParam(ALPHA, BETA, GAMMA), 1.0, 0.01, False,
+                                             0.1), NTimeSteps=T, NIterations=1,
+                           JacobianScale=True)
+    b = LDMMAtlasBuilderB200(imgs, (N, N, N), param)
+    b._update_mean()
+    stream = torch.cuda.current_stream()
+
+    def step():
+        b.engine.iterate(first=False)
+        b._update_mean()
+
+    ms, clocks = _timed(step, args.steps, args.warmup, stream)
+    value = args.steps / (ms / 1000.0)
+    peak, kind = peaks()
+    # per subject: the LDMM iteration (176 N per time step) and the mean's
+    # backward sweep (compose 36 N + Jacobian transport 20 N per time step,
+    # the pulled-back image 4 N, the two sums 20 N)
+    b_iter = ns * (176 * T + 56 * T + 24) * N ** 3
+    gbs = b_iter * value / 1e9
+    print(json.dumps({
+        "metric": "128^3 LDMM atlas iterations/s (4 subjects, T=5)", "value": value,
+        "unit": "atlas-iters/s", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded blobs + smooth warp)",
+        "config": {"workload": "LDMM relaxation atlas (IterateNew, JacobianScale), 4 subjects "
+                   "128^3, 5 time steps, sigma 1, step 0.01, mean every iteration",
+                   "grid": [N, N, N], "subjects": ns, "time_steps": T},
+        "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                     "frac": gbs / peak, "traffic": None,
+                     "algorithmic_bytes_per_atlas_iteration": b_iter},
+        "clocks": clocks}))
+    return 0
+
+
 def run_warmstart(args):
     """Learned warm start + refinement against the plain GPU greedy solve on
     held-out pairs of the pair-registration generator, with the committed
@@ -582,7 +629,7 @@ def main():
     ap.add_argument("--ncu-case", action="store_true",
                     help="run a short untimed 128^3 workload for ncu captures")
     ap.add_argument("--workload", default="greedy",
-                    choices=["greedy", "atlas", "ldmm", "warmstart"],
+                    choices=["greedy", "atlas", "ldmm", "ldmm_atlas", "warmstart"],
                     help="the headline greedy line (default) or another hot-path row")
     ap.add_argument("--grid", type=int, default=0, help="warmstart: pair grid (64 or 128; default 128)")
     ap.add_argument("--pairs", type=int, default=32, help="warmstart: held-out pairs")
@@ -592,8 +639,8 @@ def main():
     if args.workload != "greedy" and args.impl == "b200":
         import torch
         torch.cuda.set_device(0)
-        return {"atlas": run_atlas, "ldmm": run_ldmm, "warmstart": run_warmstart}[
-            args.workload](args)
+        return {"atlas": run_atlas, "ldmm": run_ldmm, "ldmm_atlas": run_ldmm_atlas,
+                "warmstart": run_warmstart}[args.workload](args)
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)

@@ -90,6 +90,7 @@ class Oracle:
         L.aw_oracle_ldmm_iterate.restype = ctypes.c_double
         L.aw_oracle_atlas_iterate.restype = ctypes.c_double
         L.aw_oracle_ldmm_iterate_orig.restype = ctypes.c_double
+        L.aw_oracle_ldmm_shoot_iterate.restype = ctypes.c_double
 
     # --- interpolation family -------------------------------------------------
     def apply(self, img, h, bg=0.0):
@@ -237,6 +238,19 @@ class Oracle:
             _dbl(alpha), _dbl(beta), _dbl(gamma), ctypes.c_float(sigma), ctypes.byref(st),
             _i(int(update_step)), ctypes.c_float(max_pert))
         return float(e), float(st.value)
+
+    def ldmm_shoot_iterate(self, I0, I1, alpha0, T, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01,
+                           gamma=0.001, sigma=0.1, step=0.005):
+        """One LDMMShootingIteratorCPU::Iterate; alpha0 [nz,ny,nx] updated in
+        place. Returns (image energy, phi0T, phiT0)."""
+        assert alpha0.dtype == np.float32 and alpha0.flags.c_contiguous
+        p0 = np.empty((3,) + I0.shape, np.float32)
+        p1 = np.empty((3,) + I0.shape, np.float32)
+        e = self.lib.aw_oracle_ldmm_shoot_iterate(
+            _fp(I0), _fp(I1), _fp(alpha0), p0.ctypes.data_as(_f), p1.ctypes.data_as(_f), _i(T),
+            *_shape(I0), *map(_dbl, sp), _dbl(alpha), _dbl(beta), _dbl(gamma),
+            ctypes.c_float(sigma), ctypes.c_float(step))
+        return float(e), p0, p1
 
     def ldmm_i1_at_0(self, I1, v, sp=(1.0, 1.0, 1.0), jacdet=True):
         """LDMMDeformationData::GetI1At0 and LDMMIteratorCPU::ComputeJacDet
@@ -521,6 +535,23 @@ class Reference:
                                              *map(_dbl, sp), _i(v.shape[0]), _fp(img), _fp(jd))
         self._check(rc)
         return img, jd
+
+    def shoot_run(self, I0, I1, T, iters, sp=(1.0, 1.0, 1.0), sigma=0.1, step=0.005, alpha=0.01,
+                  beta=0.01, gamma=0.001):
+        """The reference's LDMMShootingDefData / LDMMShootingIteratorCPU for
+        `iters` iterations from alpha0 = 0. Returns (alpha0, phi0T, phiT0,
+        image energies)."""
+        a0 = np.empty(I0.shape, np.float32)
+        p0 = np.empty((3,) + I0.shape, np.float32)
+        p1 = np.empty((3,) + I0.shape, np.float32)
+        en = np.zeros(iters, np.float64)
+        with quiet_stdout():
+            rc = self.lib.awref_shoot_run(
+                _fp(I0), _fp(I1), *_shape(I0), *map(_dbl, sp), _i(T), _i(iters),
+                ctypes.c_float(sigma), ctypes.c_float(step), _dbl(alpha), _dbl(beta), _dbl(gamma),
+                _fp(a0), p0.ctypes.data_as(_f), p1.ctypes.data_as(_f), _dp(en))
+        self._check(rc)
+        return a0, p0, p1, en
 
     def ldmm_atlas_run(self, imgs, weights, T, iters, sp=(1.0, 1.0, 1.0), sigma=0.1, step=0.005,
                        adaptive=False, max_pert=0.1, alpha=0.01, beta=0.01, gamma=0.001,

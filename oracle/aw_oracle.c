@@ -809,6 +809,79 @@ void aw_oracle_ldmm_i1_at_0(const float *I1, const float *v, int T, int nx, int 
 }
 
 /* ------------------------------------------------------------------------
+ * LDMM geodesic shooting from the initial momentum alpha0,
+ * LDMMShootingIteratorCPU::Iterate (LDMM/LDMMShootingIteratorCPU.cxx:
+ * 199-304): phi0T = phiT0 = id, alphaT = alpha0, v = K(grad(I0) alphaT);
+ * for t = 1..T-1: phi0T = composeVH(v, phi0T) [PARTIAL_ZERO],
+ * alphaT = forwardApply(alpha0, phi0T), phiT0 = composeHVInv(phiT0, v)
+ * [PARTIAL_ID], I = I0(phiT0), v = K(grad(I) alphaT); then both maps take
+ * the last v, diff = I0(phiT0) - I1, alphaT = forwardApply(diff, phiT0) and
+ * alpha0 <- (1 - step) alpha0 + (step / sigma^2) alphaT. Returns the image
+ * energy sp^3 sum diff^2 (the velocity terms of LDMMEnergy are not formed).
+ * ---------------------------------------------------------------------- */
+double aw_oracle_ldmm_shoot_iterate(const float *I0, const float *I1, float *alpha0, float *phi0T,
+                                    float *phiT0, int T, int nx, int ny, int nz, double spx,
+                                    double spy, double spz, double alpha, double beta,
+                                    double gamma, float sigma, float step) {
+  const long n = (long)nx * ny * nz;
+  float *v = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *o = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *aT = (float *)malloc(sizeof(float) * (size_t)n);
+  float *I = (float *)malloc(sizeof(float) * (size_t)n);
+  float *p0 = phi0T, *p1 = phiT0;
+  aw_oracle_identity(p0, p0 + n, p0 + 2 * n, nx, ny, nz);
+  aw_oracle_identity(p1, p1 + n, p1 + 2 * n, nx, ny, nz);
+  memcpy(aT, alpha0, sizeof(float) * (size_t)n);
+  /* v = K(grad(G) * alphaT) */
+#define AW_SHOOT_VELOCITY(G)                                                                  \
+  do {                                                                                        \
+    aw_oracle_gradient((G), v, v + n, v + 2 * n, nx, ny, nz, spx, spy, spz, 0);               \
+    for (long k = 0; k < n; ++k) {                                                            \
+      v[k] *= aT[k];                                                                          \
+      v[n + k] *= aT[k];                                                                      \
+      v[2 * n + k] *= aT[k];                                                                  \
+    }                                                                                         \
+    aw_oracle_fluid_apply(v, v + n, v + 2 * n, nx, ny, nz, spx, spy, spz, alpha, beta, gamma, \
+                          1);                                                                 \
+  } while (0)
+  AW_SHOOT_VELOCITY(I0);
+  for (int t = 1; t < T; ++t) {
+    aw_oracle_compose_vh(v, v + n, v + 2 * n, p0, p0 + n, p0 + 2 * n, o, o + n, o + 2 * n, nx, ny,
+                         nz, spx, spy, spz, 1, AW_BG_PARTIAL_ZERO);
+    memcpy(p0, o, sizeof(float) * (size_t)(3 * n));
+    aw_oracle_splat(alpha0, p0, p0 + n, p0 + 2 * n, aT, nx, ny, nz, 0.0f);
+    aw_oracle_compose_hv(p1, p1 + n, p1 + 2 * n, v, v + n, v + 2 * n, o, o + n, o + 2 * n, nx, ny,
+                         nz, spx, spy, spz, -1, AW_BG_PARTIAL_ID);
+    memcpy(p1, o, sizeof(float) * (size_t)(3 * n));
+    aw_oracle_apply(I0, p1, p1 + n, p1 + 2 * n, I, nx, ny, nz, 0.0f);
+    AW_SHOOT_VELOCITY(I);
+  }
+#undef AW_SHOOT_VELOCITY
+  aw_oracle_compose_hv(p1, p1 + n, p1 + 2 * n, v, v + n, v + 2 * n, o, o + n, o + 2 * n, nx, ny,
+                       nz, spx, spy, spz, -1, AW_BG_PARTIAL_ID);
+  memcpy(p1, o, sizeof(float) * (size_t)(3 * n));
+  aw_oracle_compose_vh(v, v + n, v + 2 * n, p0, p0 + n, p0 + 2 * n, o, o + n, o + 2 * n, nx, ny,
+                       nz, spx, spy, spz, 1, AW_BG_PARTIAL_ZERO);
+  memcpy(p0, o, sizeof(float) * (size_t)(3 * n));
+  aw_oracle_apply(I0, p1, p1 + n, p1 + 2 * n, I, nx, ny, nz, 0.0f);
+  double e = 0.0;
+  for (long k = 0; k < n; ++k) {
+    I[k] = I[k] - I1[k];
+    e += (double)I[k] * (double)I[k];
+  }
+  e *= spx * spy * spz;
+  aw_oracle_splat(I, p1, p1 + n, p1 + 2 * n, aT, nx, ny, nz, 0.0f);
+  const float vfac = (float)(1.0 - (double)step);
+  const float ufac = step / (sigma * sigma);
+  for (long k = 0; k < n; ++k) alpha0[k] = vfac * alpha0[k] + ufac * aT[k];
+  free(v);
+  free(o);
+  free(aT);
+  free(I);
+  return e;
+}
+
+/* ------------------------------------------------------------------------
  * Multiscale (Algorithms/Common/MultiscaleManager.cxx:301-366).
  * ---------------------------------------------------------------------- */
 

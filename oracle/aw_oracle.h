@@ -74,6 +74,11 @@ double aw_oracle_ldmm_iterate_orig(const float *I0, const float *I1, float *v, i
 /* GetI1At0 (I1 pulled back through the velocities) and ComputeJacDet */
 void aw_oracle_ldmm_i1_at_0(const float *I1, const float *v, int T, int nx, int ny, int nz,
                             double spx, double spy, double spz, float *img, float *jd);
+/* LDMMShootingIteratorCPU::Iterate: alpha0, phi0T, phiT0 updated in place */
+double aw_oracle_ldmm_shoot_iterate(const float *I0, const float *I1, float *alpha0, float *phi0T,
+                                    float *phiT0, int T, int nx, int ny, int nz, double spx,
+                                    double spy, double spz, double alpha, double beta,
+                                    double gamma, float sigma, float step);
 
 void aw_oracle_gauss_blur(const float *in, float *out, int nx, int ny, int nz, float sx, float sy,
                           float sz, int kx, int ky, int kz);

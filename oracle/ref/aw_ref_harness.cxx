@@ -29,6 +29,8 @@
 #include "LDMMEnergy.h"
 #include "LDMMIteratorCPU.h"
 #include "LDMMParam.h"
+#include "LDMMShootingDefData.h"
+#include "LDMMShootingIteratorCPU.h"
 #include "MultiscaleManager.h"
 #include "tinyxml.h"
 
@@ -626,6 +628,59 @@ int awref_ldmm_atlas_run(const float *imgs, int ns, const float *weights, int nx
     delete data[i];
     delete I[i];
   }
+  GUARD_END
+}
+
+/*
+ * LDMM geodesic shooting: LDMMShootingDefData + LDMMShootingIteratorCPU at
+ * one scale level, `iters` iterations from alpha0 = 0. Writes alpha0, phi0T,
+ * phiT0 ([3][N] each) and the image term of each iteration's energy.
+ */
+int awref_shoot_run(const float *i0, const float *i1, int nx, int ny, int nz, double spx,
+                    double spy, double spz, int T, int iters, float sigma, float step, double alpha,
+                    double beta, double gamma, float *alpha0, float *phi0T, float *phiT0,
+                    double *energies) {
+  GUARD_BEGIN
+  std::ostringstream xml;
+  xml.precision(17);
+  xml << "<LDMMWarpParameterFile><LDMMScaleLevel><ScaleLevel><DownsampleFactor val=\"1\"/>"
+      << "</ScaleLevel><LDMMIterator>" << diffoper_xml(alpha, beta, gamma) << "<Sigma val=\""
+      << sigma << "\"/><StepSize val=\"" << step
+      << "\"/><UseAdaptiveStepSize val=\"false\"/></LDMMIterator><NIterations val=\"" << iters
+      << "\"/></LDMMScaleLevel><NTimeSteps val=\"" << T
+      << "\"/><AutoStepReduce val=\"false\"/></LDMMWarpParameterFile>";
+  LDMMParam param;
+  parse_into(param, xml.str());
+  SizeType size(nx, ny, nz);
+  SpacingType sp(spx, spy, spz);
+  OriginType origin(0, 0, 0);
+  RealImage I0(size, origin, sp), I1(size, origin, sp);
+  to_im(i0, I0);
+  to_im(i1, I1);
+  MultiscaleManager scaleManager(size, sp, origin, param);
+  scaleManager.SetScaleVectorFields(false);
+  LDMMShootingDefData data(&I0, &I1, param);
+  LDMMShootingIteratorCPU iterator(size, origin, sp, T, true);
+  const long n = (long)nx * ny * nz;
+  data.InitializeWarp();
+  scaleManager.SetScaleLevel(0);
+  const LDMMScaleLevelParam &lp = param.GetScaleLevel(0);
+  iterator.SetScaleLevel(scaleManager, lp.Iterator());
+  // the const overload: LDMMShootingDefData.h declares a non-const one that
+  // has no definition
+  data.SetScaleLevel(static_cast<const MultiscaleManager &>(scaleManager));
+  data.StepSize(lp.Iterator().StepSize());
+  for (int iter = 0; iter < iters; ++iter) {
+    data.SetCurIter(iter);
+    iterator.Iterate(data);
+    if (energies) {
+      LDMMEnergy *e = dynamic_cast<LDMMEnergy *>(data.GetEnergyHistory().LastEnergy());
+      energies[iter] = e ? (double)e->ImageEnergy() * sigma * sigma : 0.0;
+    }
+  }
+  from_im(data.Alpha0(), alpha0);
+  from_vf(data.Phi0T(), phi0T, phi0T + n, phi0T + 2 * n);
+  from_vf(data.PhiT0(), phiT0, phiT0 + n, phiT0 + 2 * n);
   GUARD_END
 }
 

@@ -136,3 +136,23 @@ def test_ldmm_atlas_matches_reference(oracle, reference, use_new, jacobian_scale
         assert np.abs(a - b).max() <= 1e-4 * max(np.abs(b).max(), 1e-12)
     assert np.allclose(eo, er, rtol=1e-4)
     assert np.abs(vr[0]).max() > 0
+
+
+@pytest.mark.parametrize("sp", [(1.0, 1.0, 1.0), (1.5, 0.75, 1.25)])
+def test_ldmm_shooting_matches_reference(oracle, reference, sp):
+    """Geodesic shooting from the initial momentum, four iterations from
+    alpha0 = 0: the restatement against LDMMShootingIteratorCPU."""
+    shape, T, iters = (12, 14, 16), 4, 4
+    I0, I1 = greedy_pair(shape, 7, n_blobs=4, umax=1.5, sigma_range=(1.5, 3.0), smooth_sigma=3.0)
+    a_r, p0_r, p1_r, e_r = reference.shoot_run(I0, I1, T, iters, sp=sp, sigma=1.0, step=0.05)
+    a = np.zeros(shape, np.float32)
+    e_o = []
+    for _ in range(iters):
+        e, p0, p1 = oracle.ldmm_shoot_iterate(I0, I1, a, T, sp, sigma=1.0, step=0.05)
+        e_o.append(e)
+    # the oracle's FP64 fluid solve vs the reference's FP32 one
+    assert np.abs(a - a_r).max() <= 1e-5 * np.abs(a_r).max()
+    assert np.abs(p0 - p0_r).max() <= 1e-4
+    assert np.abs(p1 - p1_r).max() <= 1e-4
+    assert np.allclose(e_o, e_r, rtol=1e-5)
+    assert e_r[-1] < e_r[0]  # the shooting lowers the mismatch
