@@ -79,6 +79,7 @@ SIGNATURES = {
     "aw_ldmm_run": ([_fp] * 4 + [_i, _i, _fp], _i),
     "aw_ldmm_get_energies": ([_fp, _fp, _i, _fp], _i),
     "aw_ldmm_i1_at_0": ([_fp] * 6, _i),
+    "aw_ldmm_shoot_iterate": ([_fp] * 7, _i),
     "aw_ldmm_atlas_accumulate": ([_fp] * 4 + [ctypes.c_float, ctypes.c_long, _fp], _i),
     "aw_ldmm_atlas_normalize": ([_fp, _fp, ctypes.c_long, _fp], _i),
     "aw_nn_conv3d_scratch_floats": ([_i] * 7, ctypes.c_size_t),

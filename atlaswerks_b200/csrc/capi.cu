@@ -707,6 +707,15 @@ int aw_ldmm_atlas_normalize(float *acc, const float *jacsum, long n, void *strea
   return 0;
 }
 
+int aw_ldmm_shoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *alpha0,
+                          float *phi0T, float *phiT0, void *stream) {
+  if (!l || !I0 || !I1 || !alpha0 || !phi0T || !phiT0)
+    return fail("aw_ldmm_shoot_iterate: null pointer");
+  AW_CUDA(aw::ldmm_shoot_iterate(&l->ctx, I0, I1, alpha0, phi0T, phiT0, S(stream)),
+          "aw_ldmm_shoot_iterate");
+  return 0;
+}
+
 int aw_ldmm_get_energies(aw_ldmm_t l, double *out, int max_count, int *count) {
   if (!l || !count) return fail("aw_ldmm_get_energies: null pointer");
   AW_CUDA(cudaDeviceSynchronize(), "aw_ldmm_get_energies (pending work)");

@@ -204,6 +204,7 @@ __global__ void __launch_bounds__(256) k_fft_xy_inv(FluidPlan p, Dst dst) {
   }
   const int npairs = (ny + 1) >> 1;
   const bool even = (nx & 1) == 0;
+  const auto out = dst.bind(comp);
   for (int p0 = 0; p0 < npairs; p0 += P) {
     const int pb = min(P, npairs - p0);
     // Z[k] = X0[k] + i X1[k] over the Hermitian completion; the imaginary
@@ -225,8 +226,8 @@ __global__ void __launch_bounds__(256) k_fft_xy_inv(FluidPlan p, Dst dst) {
       const int b = t / nx, x = t - b * nx;
       const int y0 = 2 * (p0 + b), y1 = y0 + 1;
       const float2 v = R[b * nx + x];
-      dst.store(comp, d.idx(x, y0, z), v.x);
-      if (y1 < ny) dst.store(comp, d.idx(x, y1, z), v.y);
+      out.store(d.idx(x, y0, z), v.x);
+      if (y1 < ny) out.store(d.idx(x, y1, z), v.y);
     }
     __syncthreads();
   }

@@ -179,24 +179,39 @@ inline SrcForce make_force(const float *G, const float *A, int mode, const Spaci
 }
 
 // --- consumers for the inverse pass ----------------------------------------
+// A kernel stores component `comp` through dst.bind(comp): the component's
+// pointer picked once (no indexed parameter array) and any per-launch
+// factors formed once.
+struct DstFieldBound {
+  float *c;
+  AW_D void store(long i, float v) const { c[i] = v; }
+};
 struct DstField {
   float *c[3];
-  AW_D void store(int comp, long i, float v) const { c[comp][i] = v; }
+  AW_D DstFieldBound bind(int comp) const {
+    return DstFieldBound{comp == 0 ? c[0] : comp == 1 ? c[1] : c[2]};
+  }
 };
 
 // LDMM velocity update v = vfac * v + ufac * u (LDMMIteratorCPU::updateVelocity,
 // LDMM/LDMMIteratorCPU.cxx:177-190) with vfac = 1 - 2*eps and
 // ufac = 2*eps / sigma^2 formed from the device-resident step eps, float
 // arithmetic in the reference's order (LDMMIteratorCPU.cxx:606-609).
+struct DstAxpbyBound {
+  float *c;
+  float vfac, ufac;
+  AW_D void store(long i, float u) const { c[i] = fadd(fmul(vfac, c[i]), fmul(ufac, u)); }
+};
 struct DstAxpby {
   float *c[3];
   const float *step;
   float sigma;
-  AW_D void store(int comp, long i, float u) const {
+  // the step read once per thread, the two factors formed once
+  AW_D DstAxpbyBound bind(int comp) const {
     const float eps = *step;
     const float vfac = fsub(1.0f, fmul(2.0f, eps));
     const float ufac = fdiv(fmul(2.0f, eps), fmul(sigma, sigma));
-    c[comp][i] = fadd(fmul(vfac, c[comp][i]), fmul(ufac, u));
+    return DstAxpbyBound{comp == 0 ? c[0] : comp == 1 ? c[1] : c[2], vfac, ufac};
   }
 };
 

@@ -227,6 +227,7 @@ __global__ void __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
 
   // ---- inverse x: row pairs, Hermitian completion, real output ------------
   {
+    const auto out = dst.bind(comp);
     constexpr int L = 32 / TX, NLINES = NY / 2;
     const int lw = lane / TX, t = lane % TX;
     for (int base = warp * L; base < NLINES; base += kXYWarps * L) {
@@ -247,8 +248,8 @@ __global__ void __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
 #pragma unroll
       for (int r = 0; r < EX; ++r) {
         const int x = line_out_index<NX>(t, r);
-        dst.store(comp, d.idx(x, y0, z), v[r].x);
-        dst.store(comp, d.idx(x, y0 + 1, z), v[r].y);
+        out.store(d.idx(x, y0, z), v[r].x);
+        out.store(d.idx(x, y0 + 1, z), v[r].y);
       }
     }
   }

@@ -376,6 +376,86 @@ cudaError_t ldmm_atlas_normalize(float *acc, const float *jsum, long n, cudaStre
   return cudaGetLastError();
 }
 
+namespace {
+// alpha0 <- (1 - eps) alpha0 + (eps / sigma^2) alphaT, float, with
+// 1 - eps formed in double as the reference's `Real vFac = 1.0 - StepSize()`
+// (LDMMShootingIteratorCPU.cxx:287-297)
+__global__ void k_shoot_alpha(float *__restrict__ a0, const float *__restrict__ aT,
+                              const float *__restrict__ step, float sigma, long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float eps = *step;
+  const float vfac = __double2float_rn(1.0 - (double)eps);
+  const float ufac = fdiv(eps, fmul(sigma, sigma));
+  a0[i] = fadd(fmul(vfac, a0[i]), fmul(ufac, aT[i]));
+}
+}  // namespace
+
+// LDMMShootingIteratorCPU::Iterate (LDMM/LDMMShootingIteratorCPU.cxx:199-304):
+// geodesic shooting from the initial momentum alpha0 — v = K(grad(I) alphaT)
+// with I = I0(phiT0), alphaT = forwardApply(alpha0, phi0T), the two maps
+// advanced by composeVH [PARTIAL_ZERO] and composeHVInv [PARTIAL_ID] — then
+// the residual pulled back by splatting and the momentum update. The maps
+// ping-pong between the caller's buffers and the context's two vector
+// scratch fields; v lives in the context's u, alphaT in its splat buffer,
+// I0(phiT0) in J0[0]. Records the image energy sp^3 sum (I0(phiT0) - I1)^2.
+cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, float *alpha0,
+                               float *phi0T, float *phiT0, cudaStream_t s) {
+  const Dims d = c->d;
+  const long n = d.n();
+  const int T = c->T;
+  float *A[2] = {phi0T, c->hbuf}, *B[2] = {phiT0, c->hbuf + 3 * n};
+  int ca = 0, cb = 0;
+  auto comp = [&](float *base, int k) { return base + k * n; };
+  float *v = c->u, *aT = c->S, *I = c->J0;
+  auto velocity = [&](const float *G) -> cudaError_t {
+    AW_TRY(fluid_forward_force(c->plan, G, aT, 0, s));
+    AW_TRY(fluid_solve(c->plan, 1, s));
+    return fluid_inverse_store(c->plan, comp(v, 0), comp(v, 1), comp(v, 2), s);
+  };
+  auto advance_phi0T = [&]() -> cudaError_t {  // phi0T = composeVH(v, phi0T)
+    const float *vv[3] = {comp(v, 0), comp(v, 1), comp(v, 2)};
+    const float *hh[3] = {comp(A[ca], 0), comp(A[ca], 1), comp(A[ca], 2)};
+    float *oo[3] = {comp(A[1 - ca], 0), comp(A[1 - ca], 1), comp(A[1 - ca], 2)};
+    AW_TRY(launch_compose_vh(vv, hh, oo, d, c->sp, 1, BG_PARTIAL_ZERO, nullptr, 1.0f, s));
+    ca = 1 - ca;
+    return cudaSuccess;
+  };
+  auto advance_phiT0 = [&]() -> cudaError_t {  // phiT0 = composeHVInv(phiT0, v), I = I0(phiT0)
+    k_forward_step<false><<<row_grid(d), kRowThreads, 0, s>>>(
+        comp(B[cb], 0), comp(B[cb], 1), comp(B[cb], 2), comp(v, 0), comp(v, 1), comp(v, 2),
+        comp(B[1 - cb], 0), comp(B[1 - cb], 1), comp(B[1 - cb], 2), I0, I, d, c->sp);
+    cb = 1 - cb;
+    return cudaGetLastError();
+  };
+  k_identity<<<row_grid(d), kRowThreads, 0, s>>>(comp(phi0T, 0), comp(phi0T, 1), comp(phi0T, 2), d);
+  AW_TRY(cudaGetLastError());
+  k_identity<<<row_grid(d), kRowThreads, 0, s>>>(comp(phiT0, 0), comp(phiT0, 1), comp(phiT0, 2), d);
+  AW_TRY(cudaGetLastError());
+  AW_TRY(cudaMemcpyAsync(aT, alpha0, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+  AW_TRY(velocity(I0));
+  for (int t = 1; t < T; ++t) {
+    AW_TRY(advance_phi0T());
+    AW_TRY(splat(c->sw, alpha0, comp(A[ca], 0), comp(A[ca], 1), comp(A[ca], 2), aT, 0.0f, s));
+    AW_TRY(advance_phiT0());
+    AW_TRY(velocity(I));
+  }
+  AW_TRY(advance_phiT0());
+  AW_TRY(advance_phi0T());
+  k_residual<<<row_grid(d), kRowThreads, 0, s>>>(I, I1, c->diff, c->partials, d);
+  AW_TRY(cudaGetLastError());
+  AW_TRY(splat(c->sw, c->diff, comp(B[cb], 0), comp(B[cb], 1), comp(B[cb], 2), aT, 0.0f, s));
+  k_shoot_alpha<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(alpha0, aT, c->step, c->sigma, n);
+  AW_TRY(cudaGetLastError());
+  const double spprod = c->sp.x * c->sp.y * c->sp.z;
+  k_record_energy<<<1, 256, 0, s>>>(c->partials, c->nparts, spprod, c->energy, c->count, c->cap);
+  AW_TRY(cudaGetLastError());
+  // the maps end in the caller's buffers
+  if (ca) AW_TRY(cudaMemcpyAsync(phi0T, A[1], sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
+  if (cb) AW_TRY(cudaMemcpyAsync(phiT0, B[1], sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
+  return cudaSuccess;
+}
+
 int ldmm_set_orig(LdmmCtx *c, int on) {
   c->orig = on ? 1 : 0;
   if (c->orig && !c->JT) {

@@ -44,6 +44,8 @@ cudaError_t ldmm_i1_at_0(LdmmCtx *c, const float *I1, const float *v, float *img
 cudaError_t ldmm_atlas_accumulate(float *acc, float *jsum, const float *img, const float *jd,
                                   float w, long n, cudaStream_t s);
 cudaError_t ldmm_atlas_normalize(float *acc, const float *jsum, long n, cudaStream_t s);
+cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, float *alpha0,
+                               float *phi0T, float *phiT0, cudaStream_t s);
 // One iteration (IterateNew or IterateOrig); v is [T][3][N]. update_step:
 // compute the step from max |2v - (2/sigma^2) K f| and leave v unchanged.
 cudaError_t ldmm_iterate(LdmmCtx *c, const float *I0, const float *I1, float *v, int update_step,

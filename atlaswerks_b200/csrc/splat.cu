@@ -182,7 +182,11 @@ AW_D float corner_weight(float px, float py, float pz, int cx, int cy, int cz) {
   return __double2float_rn(dmul(dmul(ax, ay), az));
 }
 
-// every destination merges its eight candidate buckets in source order
+// every destination merges its eight candidate buckets in source order (the
+// order forwardApply adds them). Buckets (dx = 1, dx = 0) of one (dy, dz) are
+// adjacent: three offsets bound both. (Fetching all candidates up front and
+// merging them in registers measured slower: the 16-way selection costs
+// more issue slots than the dependent loads it saves.)
 __global__ void __launch_bounds__(kRowThreads)
     k_gather(const float *__restrict__ img, const float *__restrict__ hx,
              const float *__restrict__ hy, const float *__restrict__ hz, Dims d,
@@ -195,19 +199,26 @@ __global__ void __launch_bounds__(kRowThreads)
   // bucket k = (dz, dy, dx) bits; source in bucket b contributes corner
   // (dx, dy, dz) to this voxel
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const int dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
-    const long b = (long)(v.z - dz + 1) * sz + (long)(v.y - dy + 1) * sy + (v.x - dx + 1);
-    pos[k] = offsets[b];
-    end[k] = offsets[b + 1];
-    cur[k] = pos[k] < end[k] ? order[pos[k]] : INT_MAX;
+  for (int r = 0; r < 4; ++r) {
+    const int dy = r & 1, dz = r >> 1;
+    const long b1 = (long)(v.z - dz + 1) * sz + (long)(v.y - dy + 1) * sy + v.x;  // dx = 1
+    const int o0 = __ldg(offsets + b1), o1 = __ldg(offsets + b1 + 1), o2 = __ldg(offsets + b1 + 2);
+    pos[2 * r + 1] = o0;
+    end[2 * r + 1] = o1;
+    pos[2 * r] = o1;
+    end[2 * r] = o2;
   }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) cur[k] = pos[k] < end[k] ? order[pos[k]] : INT_MAX;
   float acc = bg;
   while (true) {
     int m = INT_MAX, sel = -1;
 #pragma unroll
     for (int k = 0; k < 8; ++k)
-      if (cur[k] < m) { m = cur[k]; sel = k; }
+      if (cur[k] < m) {
+        m = cur[k];
+        sel = k;
+      }
     if (sel < 0) break;
     const float px = hx[m], py = hy[m], pz = hz[m];
     const float w = corner_weight(px, py, pz, sel & 1, (sel >> 1) & 1, (sel >> 2) & 1);

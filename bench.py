@@ -292,12 +292,12 @@ def run_b200(args):
     peak, peak_kind = peaks()
     it0, d0 = iters[0], datas[0]
     h, ho = d0.Def1To0(), d0._next()[0]
-    ms7 = (ctypes.c_float * 7)()
+    ms_stage = (ctypes.c_float * len(STAGE_NAMES))()
     z = [None, None, None]
     _lib.check(_lib.lib().aw_greedy_profile(
         it0._h, d0.I0.data_ptr(), d0.I1.data_ptr(), *[t.data_ptr() for t in h],
-        *[t.data_ptr() for t in ho], *z, *z, 20, stream.cuda_stream, ms7))
-    stage_ms = {n: float(ms7[i]) for i, n in enumerate(STAGE_NAMES)}
+        *[t.data_ptr() for t in ho], *z, *z, 20, stream.cuda_stream, ms_stage))
+    stage_ms = {n: float(ms_stage[i]) for i, n in enumerate(STAGE_NAMES)}
     per_iter_stages = [n for n in STAGE_NAMES if n != "max_norm"]
     dom = max(per_iter_stages, key=lambda n: stage_ms[n])
     nvox = N ** 3
@@ -376,7 +376,9 @@ def run_b200(args):
                          f"(GreedyIteratorCPU{'' if kind == 'reference' else ' port'}; FFT = "
                          f"FP64 shim, not FFTW)"}
 
-    launches_per_iter = 6
+    # six launches per iteration: force-prep, energy, xy-forward, z-solve,
+    # xy-inverse, update
+    launches = 6 * per_rank_iters
     line = {"metric": "128^3 fluid iters/s", "value": value, "unit": "iters/s",
             "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -384,7 +386,7 @@ def run_b200(args):
             "data": "synthetic (seeded Gaussian blobs + smooth random warp, no dataset)",
             "config": config(), "roofline": roofline,
             "iteration_roofline": iteration_roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": launches_per_iter * per_rank_iters,
+            "gpu_launches": launches,
             "clocks": clk.summary()}
     if dist:
         dist.barrier()
@@ -396,8 +398,19 @@ def run_b200(args):
 
 def run_ncu_case(args):
     """A short, untimed workload for ncu captures: one 128^3 pair, a step
-    update, then `--steps` iterations through the graph path."""
+    update, then `--steps` iterations through the graph path (with
+    --workload ldmm: `--steps` LDMM IterateNew iterations at 128^3, T = 10,
+    sigma 1, step 0.01)."""
     import torch
+    if args.workload == "ldmm":
+        from atlaswerks_b200.ldmm import ldmm_register
+        from atlaswerks_b200.synth import greedy_pair
+        I0, I1 = greedy_pair((N, N, N), 7, 8, 3.0)
+        ldmm_register(torch.from_numpy(I0).cuda(), torch.from_numpy(I1).cuda(), 10, args.steps,
+                      sigma=1.0, step=0.01)
+        torch.cuda.synchronize()
+        print(json.dumps({"ncu_case": "ldmm 128^3 T=10", "iterations": args.steps}))
+        return 0
 
     from atlaswerks_b200.greedy import (DiffOperParam, GreedyDeformationDataB200,
                                         GreedyIteratorB200, GreedyIteratorParam)

@@ -254,6 +254,16 @@ int aw_ldmm_run(aw_ldmm_t l, const float *I0, const float *I1, float *v, int n_i
 /* Image energies sp^3 * sum (I0(h_T) - I1)^2, oldest first; synchronises. */
 int aw_ldmm_get_energies(aw_ldmm_t l, double *out, int max_count, int *count);
 
+/* LDMM geodesic shooting (LDMMShootingIteratorCPU / GPU::Iterate,
+ * Algorithms/LDMM/LDMMShootingIteratorCPU.cxx:199-304) on an LDMM handle (its
+ * T, sigma, step size and kernel): shoots from the initial momentum alpha0
+ * (a scalar image, updated in place to (1 - step) alpha0 + (step/sigma^2)
+ * times the splatted residual) and leaves phi0T and phiT0 ([3][N] each, the
+ * maps LDMMShootingDefData::Phi0T / PhiT0) in the caller's buffers; records
+ * the image energy (aw_ldmm_get_energies). */
+int aw_ldmm_shoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *alpha0,
+                          float *phi0T, float *phiT0, void *stream);
+
 /* LDMM relaxation atlas (LDMMAtlasBuilder / LDMMAtlasThreadCPU,
  * Algorithms/LDMM/LDMMAtlasThreadCPU.cxx:207-264, LDMMAtlasBuilder.txx:274-335).
  * Every subject is an aw_ldmm_t whose I0 is the shared mean and I1 its image;
