@@ -24,12 +24,16 @@ namespace aw {
 
 namespace {
 
-// one axis of the separable blur; rows = (K+1) x (K+1) filter table
+// one axis of the separable blur; rows = (K+1) x (K+1) filter table. KT > 0
+// fixes K at compile time, so the interior taps' loads are all issued before
+// the first add (same arithmetic, same order); KT = 0 takes K at run time.
+template <int KT>
 __global__ void __launch_bounds__(kRowThreads)
-    k_gauss_axis(const float *__restrict__ in, float *__restrict__ out, Dims d, int axis, int K,
+    k_gauss_axis(const float *__restrict__ in, float *__restrict__ out, Dims d, int axis, int Kr,
                  const float *__restrict__ rows) {
   Voxel v;
   if (!voxel_of(d, v)) return;
+  const int K = KT > 0 ? KT : Kr;
   const int pos = axis == 0 ? v.x : (axis == 1 ? v.y : v.z);
   const int n = axis == 0 ? d.nx : (axis == 1 ? d.ny : d.nz);
   const long st = axis == 0 ? 1 : (axis == 1 ? (long)d.nx : (long)d.nx * d.ny);
@@ -37,8 +41,21 @@ __global__ void __launch_bounds__(kRowThreads)
   float o;
   if (pos >= K && pos < n - K) {
     const float *f = rows;
-    o = fmul(in[i], f[0]);
-    for (int k = 1; k <= K; ++k) o = fadd(o, fmul(fadd(in[i - k * st], in[i + k * st]), f[k]));
+    if (KT > 0) {
+      float lo[KT > 0 ? KT : 1], hi[KT > 0 ? KT : 1], fk[KT > 0 ? KT : 1];
+#pragma unroll
+      for (int k = 1; k <= KT; ++k) {
+        lo[k - 1] = __ldg(in + i - k * st);
+        hi[k - 1] = __ldg(in + i + k * st);
+        fk[k - 1] = __ldg(f + k);
+      }
+      o = fmul(__ldg(in + i), __ldg(f));
+#pragma unroll
+      for (int k = 1; k <= KT; ++k) o = fadd(o, fmul(fadd(lo[k - 1], hi[k - 1]), fk[k - 1]));
+    } else {
+      o = fmul(in[i], f[0]);
+      for (int k = 1; k <= K; ++k) o = fadd(o, fmul(fadd(in[i - k * st], in[i + k * st]), f[k]));
+    }
   } else if (pos < K) {
     const int x = pos;
     const float *f = rows + (K - x) * (K + 1);
@@ -194,7 +211,13 @@ cudaError_t downsample(const float *in, Dims din, Spacing sin, float *out, Dims 
     const float *t = nullptr;
     cudaError_t e = gauss_table((float)sg, K, s, &t);
     if (e != cudaSuccess) return e;
-    k_gauss_axis<<<row_grid(din), kRowThreads, 0, s>>>(src, dst[a], din, a, K, t);
+    switch (K) {
+      case 1: k_gauss_axis<1><<<row_grid(din), kRowThreads, 0, s>>>(src, dst[a], din, a, K, t); break;
+      case 2: k_gauss_axis<2><<<row_grid(din), kRowThreads, 0, s>>>(src, dst[a], din, a, K, t); break;
+      case 3: k_gauss_axis<3><<<row_grid(din), kRowThreads, 0, s>>>(src, dst[a], din, a, K, t); break;
+      case 4: k_gauss_axis<4><<<row_grid(din), kRowThreads, 0, s>>>(src, dst[a], din, a, K, t); break;
+      default: k_gauss_axis<0><<<row_grid(din), kRowThreads, 0, s>>>(src, dst[a], din, a, K, t);
+    }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     src = dst[a];
   }
