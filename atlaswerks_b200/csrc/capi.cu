@@ -318,6 +318,15 @@ int aw_greedy_set_auto_step_reduce(aw_greedy_t g, int on) {
   return 0;
 }
 
+int aw_greedy_set_staged_update(aw_greedy_t g, int on) {
+  if (!g) return fail("aw_greedy_set_staged_update: null handle");
+  AW_CUDA(cudaDeviceSynchronize(), "aw_greedy_set_staged_update (pending work)");
+  g->ctx.no_staged_update = on ? 0 : 1;
+  for (auto &kv : g->graphs) cudaGraphExecDestroy(kv.second);
+  g->graphs.clear();  // captured iterations hold the other update kernel
+  return 0;
+}
+
 int aw_greedy_iterate(aw_greedy_t g, const float *I0, const float *I1, const float *hx,
                       const float *hy, const float *hz, float *ox, float *oy, float *oz,
                       const float *hix, const float *hiy, const float *hiz, float *hiox,

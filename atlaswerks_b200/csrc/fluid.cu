@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "fluid.cuh"
+#include "tma_host.cuh"
 #include "fluid_fast.cuh"
 
 namespace aw {
@@ -237,16 +238,8 @@ __global__ void __launch_bounds__(256) k_fft_xy_inv(FluidPlan p, Dst dst) {
 // {2*ny*nxh, nz, 3} read and written in boxes {2*Kq, nz, 1} = one 128-byte
 // row per kz, stored in shared memory with the 128-byte swizzle
 bool encode_spec_map(FluidPlan *p) {
-  static PFN_cuTensorMapEncodeTiled encode = nullptr;
-  if (!encode) {
-    void *fn = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
-            cudaSuccess ||
-        q != cudaDriverEntryPointSuccess || !fn)
-      return false;
-    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(fn);
-  }
+  const PFN_cuTensorMapEncodeTiled encode = tensor_map_encoder();
+  if (!encode) return false;
   const cuuint64_t ncols = (cuuint64_t)p->d.ny * p->nxh;
   const cuuint64_t dims[3] = {2 * ncols, (cuuint64_t)p->d.nz, 3};
   const cuuint64_t strides[2] = {2 * ncols * sizeof(float), 2 * ncols * sizeof(float) * p->d.nz};

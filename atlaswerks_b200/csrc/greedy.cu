@@ -15,9 +15,12 @@
 // GreedyWarp.txx:99), a max|v| reduction and eps = MaxPert / max|v| computed
 // on the device (GreedyIteratorCPU.cxx:125-131).
 #include <cstring>
+#include <map>
 
+#include "bulk.cuh"
 #include "greedy.cuh"
 #include "interp.cuh"
+#include "tma_host.cuh"
 
 namespace aw {
 
@@ -134,35 +137,163 @@ __global__ void k_set_step(const unsigned *__restrict__ maxbits, float max_pert,
 // composeVHInv(eps*v, hinv, PARTIAL_ZERO) — GreedyIteratorCPU::updateDeformation
 // (GreedyIteratorCPU.cxx:83-95), both from one read of v. q[] divides by the
 // float spacing (a multiply when it is a power of two).
+struct UpdateArgs {
+  const float *hx, *hy, *hz, *vx, *vy, *vz;
+  float *ox, *oy, *oz;
+  const float *gx, *gy, *gz;  // hinv (null: no inverse)
+  float *qx, *qy, *qz;        // hinv'
+  DivF q0, q1, q2;
+};
+
 __global__ void __launch_bounds__(kRowThreads)
-    k_update(const float *__restrict__ hx, const float *__restrict__ hy, const float *__restrict__ hz,
-             const float *__restrict__ vx, const float *__restrict__ vy, const float *__restrict__ vz,
-             float *__restrict__ ox, float *__restrict__ oy, float *__restrict__ oz,
-             const float *__restrict__ gx, const float *__restrict__ gy, const float *__restrict__ gz,
-             float *__restrict__ qx, float *__restrict__ qy, float *__restrict__ qz, Dims d,
-             DivF q0, DivF q1, DivF q2, const float *__restrict__ step_ptr) {
+    k_update(UpdateArgs a, Dims d, const float *__restrict__ step_ptr) {
   Voxel vox;
   if (!voxel_of(d, vox)) return;
   const long i = vox.i;
   const int x = vox.x, y = vox.y, z = vox.z;
   const float eps = *step_ptr;
-  const float px = fadd(__int2float_rn(x), fdivq(fmul(vx[i], eps), q0));
-  const float py = fadd(__int2float_rn(y), fdivq(fmul(vy[i], eps), q1));
-  const float pz = fadd(__int2float_rn(z), fdivq(fmul(vz[i], eps), q2));
+  const float px = fadd(__int2float_rn(x), fdivq(fmul(a.vx[i], eps), a.q0));
+  const float py = fadd(__int2float_rn(y), fdivq(fmul(a.vy[i], eps), a.q1));
+  const float pz = fadd(__int2float_rn(z), fdivq(fmul(a.vz[i], eps), a.q2));
   float rx, ry, rz;
-  trilerp_vector(hx, hy, hz, d, px, py, pz, BG_PARTIAL_ID, 1.0f, rx, ry, rz);
-  ox[i] = rx;
-  oy[i] = ry;
-  oz[i] = rz;
-  if (gx) {
-    const float g0 = gx[i], g1 = gy[i], g2 = gz[i];
-    float a, b, c;
-    trilerp_vector(vx, vy, vz, d, g0, g1, g2, BG_PARTIAL_ZERO, eps, a, b, c);
-    // a / -s = -(a / s) exactly in round-to-nearest
-    qx[i] = fadd(-fdivq(a, q0), g0);
-    qy[i] = fadd(-fdivq(b, q1), g1);
-    qz[i] = fadd(-fdivq(c, q2), g2);
+  trilerp_vector(a.hx, a.hy, a.hz, d, px, py, pz, BG_PARTIAL_ID, 1.0f, rx, ry, rz);
+  a.ox[i] = rx;
+  a.oy[i] = ry;
+  a.oz[i] = rz;
+  if (a.gx) {
+    const float g0 = a.gx[i], g1 = a.gy[i], g2 = a.gz[i];
+    float b0, b1, b2;
+    trilerp_vector(a.vx, a.vy, a.vz, d, g0, g1, g2, BG_PARTIAL_ZERO, eps, b0, b1, b2);
+    // b / -s = -(b / s) exactly in round-to-nearest
+    a.qx[i] = fadd(-fdivq(b0, a.q0), g0);
+    a.qy[i] = fadd(-fdivq(b1, a.q1), g1);
+    a.qz[i] = fadd(-fdivq(b2, a.q2), g2);
   }
+}
+
+// The update with h staged in shared memory. The step keeps eps*v/sp within
+// MaxPert of a voxel at the iteration that sets it, so the eight corners a
+// voxel reads lie within one voxel of it: a CTA owns a 32 x 8 x 4 tile and
+// the three components of h over the tile plus a one-voxel halo arrive by
+// TMA tensor loads (x from x0 - 4, so the box starts on a 16-byte boundary:
+// 40 x 10 x 6 floats each). Corners inside the volume and the box are read
+// from shared memory with trilerp_vector's own arithmetic (corner order,
+// double weights, lerp tree); any other voxel (a corner outside the volume,
+// a larger step) takes trilerp_vector from global memory. No inverse field.
+constexpr int kUTX = 32, kUTY = 8, kUTZ = 4;
+constexpr int kUBX = 40, kUBY = kUTY + 2, kUBZ = kUTZ + 2;
+constexpr int kUBox = kUBX * kUBY * kUBZ;  // floats per component (9600 B)
+
+struct HMaps {
+  CUtensorMap m[3];
+};
+
+__global__ void __launch_bounds__(kUTX * kUTY, 4)
+    k_update_tiled(const __grid_constant__ HMaps maps, UpdateArgs a, Dims d,
+                   const float *__restrict__ step_ptr, int *status) {
+  __shared__ __align__(128) float sh[3][kUBox];
+  __shared__ uint64_t mbar;
+  const int tx = (d.nx + kUTX - 1) / kUTX, ty = (d.ny + kUTY - 1) / kUTY;
+  int t = blockIdx.x;
+  const int x0 = (t % tx) * kUTX;
+  t /= tx;
+  const int y0 = (t % ty) * kUTY;
+  const int z0 = (t / ty) * kUTZ;
+  const int bx0 = x0 - 4, by0 = y0 - 1, bz0 = z0 - 1;
+  if (threadIdx.x == 0) {
+    mbar_init(&mbar, 1);
+    mbar_expect_tx(&mbar, (uint32_t)(3 * kUBox * sizeof(float)));
+    for (int c = 0; c < 3; ++c) tma_load_3d(sh[c], &maps.m[c], bx0, by0, bz0, &mbar);
+  }
+  __syncthreads();
+  const int x = x0 + (threadIdx.x % kUTX), y = y0 + (threadIdx.x / kUTX);
+  const bool col = x < d.nx && y < d.ny;
+  // v of the thread's four voxels first: independent of the staged h, so
+  // these loads overlap the tile's arrival
+  const float eps = *step_ptr;
+  float vx4[kUTZ], vy4[kUTZ], vz4[kUTZ];
+#pragma unroll
+  for (int zz = 0; zz < kUTZ; ++zz) {
+    const long i = d.idx(x, y, z0 + zz);
+    const bool ok = col && z0 + zz < d.nz;
+    vx4[zz] = ok ? __ldg(a.vx + i) : 0.0f;
+    vy4[zz] = ok ? __ldg(a.vy + i) : 0.0f;
+    vz4[zz] = ok ? __ldg(a.vz + i) : 0.0f;
+  }
+  const bool staged = mbar_wait(&mbar, 0, status);
+  if (!col) return;
+#pragma unroll
+  for (int zz = 0; zz < kUTZ; ++zz) {
+    const int z = z0 + zz;
+    if (z >= d.nz) break;
+    const long i = d.idx(x, y, z);
+    const float px = fadd(__int2float_rn(x), fdivq(fmul(vx4[zz], eps), a.q0));
+    const float py = fadd(__int2float_rn(y), fdivq(fmul(vy4[zz], eps), a.q1));
+    const float pz = fadd(__int2float_rn(z), fdivq(fmul(vz4[zz], eps), a.q2));
+    const int fx = ref_floor_f(px), fy = ref_floor_f(py), fz = ref_floor_f(pz);
+    const bool fast = staged && fx >= 0 && fx + 1 < d.nx && fy >= 0 && fy + 1 < d.ny &&
+                      fz >= 0 && fz + 1 < d.nz && fx >= bx0 && fx + 1 < bx0 + kUBX &&
+                      fy >= by0 && fy + 1 < by0 + kUBY && fz >= bz0 && fz + 1 < bz0 + kUBZ;
+    float rx, ry, rz;
+    if (fast) {
+      const double tt = (double)fsub(px, __int2float_rn(fx));
+      const double uu = (double)fsub(py, __int2float_rn(fy));
+      const double vv = (double)fsub(pz, __int2float_rn(fz));
+      const double omt = dsub(1.0, tt), omu = dsub(1.0, uu), omv = dsub(1.0, vv);
+      const int b = ((fz - bz0) * kUBY + (fy - by0)) * kUBX + (fx - bx0);
+      constexpr int sy = kUBX, sz = kUBX * kUBY;
+      const int off[8] = {b, b + 1, b + sy + 1, b + sy, b + sy + sz, b + sy + sz + 1, b + sz + 1,
+                          b + sz};
+      float cx[8], cy[8], cz[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        cx[c] = sh[0][off[c]];
+        cy[c] = sh[1][off[c]];
+        cz[c] = sh[2][off[c]];
+      }
+      rx = __double2float_rn(lerp_tree(cx, tt, uu, vv, omt, omu, omv));
+      ry = __double2float_rn(lerp_tree(cy, tt, uu, vv, omt, omu, omv));
+      rz = __double2float_rn(lerp_tree(cz, tt, uu, vv, omt, omu, omv));
+    } else {
+      trilerp_vector(a.hx, a.hy, a.hz, d, px, py, pz, BG_PARTIAL_ID, 1.0f, rx, ry, rz);
+    }
+    a.ox[i] = rx;
+    a.oy[i] = ry;
+    a.oz[i] = rz;
+  }
+}
+
+// tensor maps of h planes, one per (pointer, grid), encoded on first use
+struct HMapCache {
+  std::map<std::pair<const float *, long>, CUtensorMap> maps;
+};
+
+bool h_map(GreedyCtx *g, const float *p, CUtensorMap *out) {
+  if (!g->hmaps) return false;
+  auto *cache = static_cast<HMapCache *>(g->hmaps);
+  const Dims d = g->d;
+  const long key2 = ((long)d.nz * 4096 + d.ny) * 4096 + d.nx;
+  auto it = cache->maps.find({p, key2});
+  if (it != cache->maps.end()) {
+    *out = it->second;
+    return true;
+  }
+  const PFN_cuTensorMapEncodeTiled encode = tensor_map_encoder();
+  if (!encode || reinterpret_cast<uintptr_t>(p) % 16 || d.nx % 4 || d.nx < kUBX || d.ny < kUBY ||
+      d.nz < kUBZ)
+    return false;
+  CUtensorMap m;
+  const cuuint64_t dims[3] = {(cuuint64_t)d.nx, (cuuint64_t)d.ny, (cuuint64_t)d.nz};
+  const cuuint64_t strides[2] = {(cuuint64_t)d.nx * 4, (cuuint64_t)d.nx * d.ny * 4};
+  const cuuint32_t box[3] = {kUBX, kUBY, kUBZ};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  if (encode(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(p), dims, strides, box,
+             estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  cache->maps[{p, key2}] = m;
+  *out = m;
+  return true;
 }
 
 #define AW_TRY(x)                         \
@@ -199,6 +330,7 @@ int greedy_create(GreedyCtx *g, int nx, int ny, int nz, double spx, double spy, 
   g->st.step = reinterpret_cast<float *>(g->scalars);
   g->st.count = reinterpret_cast<int *>(g->scalars + 4);
   g->maxbits = reinterpret_cast<unsigned *>(g->scalars + 8);
+  g->hmaps = new HMapCache();
   if (cudaStreamCreateWithFlags(&g->aux, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&g->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&g->ev_join, cudaEventDisableTiming) != cudaSuccess)
@@ -216,6 +348,7 @@ void greedy_destroy(GreedyCtx *g) {
   if (g->aux) cudaStreamDestroy(g->aux);
   if (g->ev_fork) cudaEventDestroy(g->ev_fork);
   if (g->ev_join) cudaEventDestroy(g->ev_join);
+  delete static_cast<HMapCache *>(g->hmaps);
   std::memset(g, 0, sizeof(*g));
 }
 
@@ -255,12 +388,21 @@ cudaError_t greedy_stage(GreedyCtx *g, int stage, const float *I0, const float *
     }
     case kStageUpdate: {
       const bool inv = hinv && hinv[0] && hinv_out && hinv_out[0];
-      k_update<<<row_grid(d), kRowThreads, 0, s>>>(
-          h[0], h[1], h[2], v[0], v[1], v[2], h_out[0], h_out[1], h_out[2],
-          inv ? hinv[0] : nullptr, inv ? hinv[1] : nullptr, inv ? hinv[2] : nullptr,
-          inv ? hinv_out[0] : nullptr, inv ? hinv_out[1] : nullptr, inv ? hinv_out[2] : nullptr,
-          d, make_divf((float)g->sp.x), make_divf((float)g->sp.y), make_divf((float)g->sp.z),
-          g->st.step);
+      const UpdateArgs a{h[0], h[1], h[2], v[0], v[1], v[2], h_out[0], h_out[1], h_out[2],
+                         inv ? hinv[0] : nullptr, inv ? hinv[1] : nullptr,
+                         inv ? hinv[2] : nullptr, inv ? hinv_out[0] : nullptr,
+                         inv ? hinv_out[1] : nullptr, inv ? hinv_out[2] : nullptr,
+                         make_divf((float)g->sp.x), make_divf((float)g->sp.y),
+                         make_divf((float)g->sp.z)};
+      HMaps maps;
+      if (!inv && !g->no_staged_update && h_map(g, h[0], &maps.m[0]) && h_map(g, h[1], &maps.m[1]) &&
+          h_map(g, h[2], &maps.m[2])) {
+        const unsigned tiles = (unsigned)(((d.nx + kUTX - 1) / kUTX) * ((d.ny + kUTY - 1) / kUTY) *
+                                          ((d.nz + kUTZ - 1) / kUTZ));
+        k_update_tiled<<<tiles, kUTX * kUTY, 0, s>>>(maps, a, d, g->st.step, g->plan.status);
+      } else {
+        k_update<<<row_grid(d), kRowThreads, 0, s>>>(a, d, g->st.step);
+      }
       return cudaGetLastError();
     }
   }

@@ -30,6 +30,8 @@ struct GreedyCtx {
   char *scalars;    // step | count | maxbits
   unsigned *maxbits;
   GreedyDevState st;
+  void *hmaps;      // host cache of the h planes' tensor maps (greedy.cu)
+  int no_staged_update;  // 1: the update gathers h from global memory only
 };
 
 // stages of one iteration, in launch order

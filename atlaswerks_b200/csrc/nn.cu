@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <cstdint>
 
+#include "tma_host.cuh"
 #include "umma.cuh"
 
 namespace aw {
@@ -944,18 +945,6 @@ __global__ void __launch_bounds__(128)
   if (warp == 0) tmem_dealloc(tmem, C::TMEM_COLS);
 }
 
-PFN_cuTensorMapEncodeTiled tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled encode = nullptr;
-  if (!encode) {
-    void *fn = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess && fn)
-      encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(fn);
-  }
-  return encode;
-}
 
 template <int CIN, int COUT, int ZT>
 cudaError_t launch_direct(const void *x, int B, int D, int H, int W, const void *w,

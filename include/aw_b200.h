@@ -151,6 +151,11 @@ int aw_greedy_set_step(aw_greedy_t g, float step);
 int aw_greedy_get_step(aw_greedy_t g, float *step);
 /* GreedyParam::AutoStepReduce (Greedy/GreedyParam.h:61-65); off by default. */
 int aw_greedy_set_auto_step_reduce(aw_greedy_t g, int on);
+/* on = 1 (default): the update stages h over each tile (plus a one-voxel
+ * halo) in shared memory by TMA where the grid allows (nx % 4 == 0, nx >= 40,
+ * ny >= 10, nz >= 6, no inverse field); 0: every gather from global memory.
+ * Both give the same bits; the switch exists to compare them. */
+int aw_greedy_set_staged_update(aw_greedy_t g, int on);
 
 /* One Iterate(): reads h (and hinv when non-NULL), writes the updated fields
  * to h_out / hinv_out (distinct buffers). update_step=1 recomputes the step
