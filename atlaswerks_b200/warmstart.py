@@ -536,9 +536,11 @@ def save_weights(net: "WarmStartNet", path: str):
 
 
 # committed trained weights: pair grid -> (file in atlaswerks_b200/data, network grid).
-# 64^3 pairs: the network at the pair's grid; 128^3 pairs: the network at 64^3
-# on the downsampled pair (warm_h), trained on 2000 pairs of the 128^3 generator.
-TRAINED = {64: ("warmstart_64.npz", 64), 128: ("warmstart_128.npz", 64)}
+# The network runs at half the pair's grid on the downsampled pair (warm_h),
+# trained on 2000 pairs of the pair generator at the pair's grid with the
+# solver's displacements at the network's grid as targets.
+# (warmstart_64.npz: the network at 64^3 on 64^3 pairs, the native-grid variant.)
+TRAINED = {64: ("warmstart_64_net32.npz", 32), 128: ("warmstart_128.npz", 64)}
 
 
 def trained(grid: int) -> "WarmStartNet":

@@ -607,7 +607,7 @@ def run_ldmm_atlas(args):
 def run_warmstart(args):
     """Learned warm start + refinement against the plain GPU greedy solve on
     held-out pairs of the pair-registration generator, with the committed
-    trained weights (128^3 pairs: the network at 64^3 on the downsampled
+    trained weights (the network at half the pair's grid on the downsampled
     pair). A step = one pair through both paths."""
     import numpy as np
     import torch

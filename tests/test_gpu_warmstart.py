@@ -39,6 +39,16 @@ def test_trained_warm_start_beats_plain_solve():
     assert all(r["fallback"] or r["reached"] for r in res)
 
 
+def test_coarse_network_warm_start_at_64():
+    pairs = W.make_pairs(range(20_000_300, 20_000_308), 64, 0)
+    net = W.trained(64)
+    assert (net.D, net.H, net.W) == (32, 32, 32)
+    res = W.evaluate(net, pairs)
+    assert sum(r["reached"] for r in res) >= 7
+    assert np.mean([r["warm_iters_run"] for r in res if r["reached"]]) <= 10
+    assert all(r["fallback"] or r["reached"] for r in res)
+
+
 def test_coarse_network_warm_start_at_128():
     pairs = W.make_pairs(range(20_000_100, 20_000_104), 128, 0)
     net = W.trained(128)
