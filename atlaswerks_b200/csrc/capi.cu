@@ -248,6 +248,31 @@ int aw_fluid_apply(aw_fluid_t k, float *vx, float *vy, float *vz, int inverse, v
   return 0;
 }
 
+int aw_fluid_get_shapes(aw_fluid_t k, int *shapes) {
+  if (!k || !shapes) return fail("aw_fluid_get_shapes: null pointer");
+  const int tunable = aw::fluid_get_shapes(k->plan, shapes, shapes + 1, shapes + 2);
+  if (!tunable) shapes[0] = shapes[1] = shapes[2] = 0;
+  return 0;
+}
+
+int aw_fluid_set_shapes(aw_fluid_t k, int pairs, int cols, int zcols) {
+  if (!k) return fail("aw_fluid_set_shapes: null handle");
+  AW_CUDA(cudaDeviceSynchronize(), "aw_fluid_set_shapes (pending work)");
+  const cudaError_t e = aw::fluid_set_shapes(&k->plan, pairs, cols, zcols);
+  if (e == cudaErrorNotSupported)
+    return fail("aw_fluid_set_shapes: power-of-two grids use fixed register-FFT shapes");
+  if (e == cudaErrorInvalidValue)
+    return fail("aw_fluid_set_shapes: shapes out of range or beyond shared memory");
+  AW_CUDA(e, "aw_fluid_set_shapes");
+  return 0;
+}
+
+int aw_fluid_autotune(aw_fluid_t k, void *stream) {
+  if (!k) return fail("aw_fluid_autotune: null handle");
+  AW_CUDA(aw::fluid_autotune(&k->plan, S(stream)), "aw_fluid_autotune");
+  return 0;
+}
+
 int aw_fluid_destroy(aw_fluid_t k) {
   if (!k) return 0;
   aw::fluid_plan_destroy(&k->plan);

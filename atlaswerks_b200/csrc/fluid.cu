@@ -12,6 +12,9 @@
 
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "fluid.cuh"
@@ -251,12 +254,154 @@ bool encode_spec_map(FluidPlan *p) {
                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// The shared-memory limit is an attribute of the kernel, shared by every
+// plan on the device: only ever raise it, so a plan created later with a
+// smaller footprint cannot invalidate the launches of a larger one.
+std::mutex g_smem_mu;
+std::map<std::pair<const void *, int>, size_t> g_smem;
+
 template <class K>
 cudaError_t set_smem(K kernel, size_t bytes) {
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(g_smem_mu);
+  size_t &cur = g_smem[{reinterpret_cast<const void *>(kernel), dev}];
+  if (bytes <= cur) return cudaSuccess;
+  const cudaError_t e =
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) cur = bytes;
+  return e;
 }
 
+// Shapes of the shared-memory (any-size) path: x-line pairs and y-columns per
+// batch of the xy kernels, (ky,kx) columns per CTA of the z kernel, and the
+// shared memory they need.
+void generic_shapes(FluidPlan *p, int P, int Q, int K) {
+  const int nx = p->d.nx, ny = p->d.ny, nz = p->d.nz;
+  p->pairs_per_batch = P;
+  p->cols_per_batch = Q;
+  p->zcols_per_cta = K;
+  const size_t ws = std::max((size_t)P * nx, (size_t)Q * ny);
+  p->smem_xy = sizeof(float2) * ((size_t)ny * p->nxh + 2 * ws);
+  p->smem_z = sizeof(float2) * (size_t)(2 * 3 * K * nz);
+}
+
+cudaError_t generic_configure(const FluidPlan &p) {
+  cudaError_t e;
+  if ((e = set_smem(k_fft_xy_fwd<SrcField>, p.smem_xy)) != cudaSuccess) return e;
+  if ((e = set_smem(k_fft_xy_fwd<SrcForce>, p.smem_xy)) != cudaSuccess) return e;
+  if ((e = set_smem(k_fft_xy_inv<DstField>, p.smem_xy)) != cudaSuccess) return e;
+  if ((e = set_smem(k_fft_xy_inv<DstAxpby>, p.smem_xy)) != cudaSuccess) return e;
+  return set_smem(k_fft_z_solve, p.smem_z);
+}
+
+// autotuned shapes per (grid, device), kept for the life of the process
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, std::tuple<int, int, int>> g_tuned;
+
 }  // namespace
+
+int fluid_get_shapes(const FluidPlan &p, int *P, int *Q, int *K) {
+  *P = p.pairs_per_batch;
+  *Q = p.cols_per_batch;
+  *K = p.zcols_per_cta;
+  return p.fast ? 0 : 1;
+}
+
+cudaError_t fluid_set_shapes(FluidPlan *p, int P, int Q, int K) {
+  const int npairs = (p->d.ny + 1) / 2;
+  if (p->fast) return cudaErrorNotSupported;
+  if (P < 1 || P > npairs || Q < 1 || Q > p->nxh || K < 1 || K > 64) return cudaErrorInvalidValue;
+  FluidPlan t = *p;
+  generic_shapes(&t, P, Q, K);
+  int maxsm = 0;
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device);
+  if (t.smem_xy > (size_t)maxsm || t.smem_z > (size_t)maxsm) return cudaErrorInvalidValue;
+  const cudaError_t e = generic_configure(t);
+  if (e == cudaSuccess) *p = t;
+  return e;
+}
+
+// The shared-memory path's autotuner: every combination of half, the
+// heuristic and twice the heuristic line pairs and columns per batch is
+// timed on the forward + inverse xy pass, then 2..32 columns per z CTA on
+// the z pass (alternating L^-1 and L so the spectrum keeps its scale), each
+// the mean of three launches after one untimed, on a zero field (the
+// arithmetic is the same for every shape; only the distribution of lines
+// over CTAs changes). The choice is kept per grid and device.
+cudaError_t fluid_autotune(FluidPlan *p, cudaStream_t s) {
+  if (p->fast) return cudaSuccess;
+  const auto key = std::make_tuple(p->d.nx, p->d.ny, p->d.nz, p->device);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end())
+      return fluid_set_shapes(p, std::get<0>(it->second), std::get<1>(it->second),
+                              std::get<2>(it->second));
+  }
+  const long n = p->d.n();
+  float *f = nullptr;
+  cudaError_t e = cudaMalloc(&f, sizeof(float) * 3 * n);
+  if (e != cudaSuccess) return e;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  auto timed = [&](auto &&fn, float *ms) -> cudaError_t {
+    cudaError_t r = fn();
+    if (r != cudaSuccess) return r;
+    cudaEventRecord(e0, s);
+    for (int i = 0; i < 3 && r == cudaSuccess; ++i) r = fn();
+    cudaEventRecord(e1, s);
+    if (r == cudaSuccess) r = cudaEventSynchronize(e1);
+    if (r == cudaSuccess) r = cudaEventElapsedTime(ms, e0, e1);
+    return r;
+  };
+  float *c[3] = {f, f + n, f + 2 * n};
+  const int P0 = p->pairs_per_batch, Q0 = p->cols_per_batch, K0 = p->zcols_per_cta;
+  int bestP = P0, bestQ = Q0, bestK = K0;
+  float best = 1e30f;
+  if ((e = cudaMemsetAsync(f, 0, sizeof(float) * 3 * n, s)) == cudaSuccess) {
+    for (int P : {P0 / 2, P0, 2 * P0})
+      for (int Q : {Q0 / 2, Q0, 2 * Q0}) {
+        if (fluid_set_shapes(p, P, Q, K0) != cudaSuccess) continue;
+        float ms = 0.f;
+        if ((e = timed([&]() {
+               cudaError_t r = fluid_forward_field(*p, c[0], c[1], c[2], s);
+               return r == cudaSuccess ? fluid_inverse_store(*p, c[0], c[1], c[2], s) : r;
+             }, &ms)) != cudaSuccess)
+          break;
+        if (ms < best) {
+          best = ms;
+          bestP = P;
+          bestQ = Q;
+        }
+      }
+  }
+  if (e == cudaSuccess) {
+    best = 1e30f;
+    int flip = 0;
+    for (int K : {2, 4, 8, 16, 32}) {
+      if (fluid_set_shapes(p, bestP, bestQ, K) != cudaSuccess) continue;
+      float ms = 0.f;
+      if ((e = timed([&]() { return fluid_solve(*p, (flip++ & 1) ? 0 : 1, s); }, &ms)) !=
+          cudaSuccess)
+        break;
+      if (ms < best) {
+        best = ms;
+        bestK = K;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(f);
+  if (e != cudaSuccess) return e;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tuned[key] = std::make_tuple(bestP, bestQ, bestK);
+  }
+  return fluid_set_shapes(p, bestP, bestQ, bestK);
+}
 
 int fluid_plan_create(FluidPlan *p, int nx, int ny, int nz, double spx, double spy, double spz,
                       float alpha, float beta, float gamma) {
@@ -270,12 +415,9 @@ int fluid_plan_create(FluidPlan *p, int nx, int ny, int nz, double spx, double s
   p->nxh = nx / 2 + 1;
   if (!factorize(nx, p->ax) || !factorize(ny, p->ay) || !factorize(nz, p->az)) return 1;
   const int npairs = (ny + 1) / 2;
-  p->pairs_per_batch = std::max(1, std::min(npairs, (2048 + nx - 1) / nx));
-  p->cols_per_batch = std::max(1, std::min(p->nxh, (2048 + ny - 1) / ny));
-  p->zcols_per_cta = std::max(1, std::min(16, 3072 / (3 * nz)));
-  const size_t ws = std::max((size_t)p->pairs_per_batch * nx, (size_t)p->cols_per_batch * ny);
-  p->smem_xy = sizeof(float2) * ((size_t)ny * p->nxh + 2 * ws);
-  p->smem_z = sizeof(float2) * (size_t)(2 * 3 * p->zcols_per_cta * nz);
+  generic_shapes(p, std::max(1, std::min(npairs, (2048 + nx - 1) / nx)),
+                 std::max(1, std::min(p->nxh, (2048 + ny - 1) / ny)),
+                 std::max(1, std::min(16, 3072 / (3 * nz))));
   int dev = 0, maxsm = 0;
   cudaGetDevice(&dev);
   p->device = dev;
@@ -306,14 +448,10 @@ int fluid_plan_create(FluidPlan *p, int nx, int ny, int nz, double spx, double s
   p->ax.tw = p->tw;
   p->ay.tw = p->tw + nx;
   p->az.tw = p->tw + nx + ny;
-  if (set_smem(k_fft_xy_fwd<SrcField>, p->smem_xy) != cudaSuccess ||
-      set_smem(k_fft_xy_fwd<SrcForce>, p->smem_xy) != cudaSuccess ||
-      set_smem(k_fft_xy_inv<DstField>, p->smem_xy) != cudaSuccess ||
-      set_smem(k_fft_xy_inv<DstAxpby>, p->smem_xy) != cudaSuccess ||
-      set_smem(k_fft_z_solve, p->smem_z) != cudaSuccess)
-    return 4;
+  if (generic_configure(*p) != cudaSuccess) return 4;
   if (p->fast) p->fast_tma = encode_spec_map(p);
   if (p->fast && fast_configure(*p) != cudaSuccess) return 4;
+  if (!p->fast && fluid_autotune(p, 0) != cudaSuccess) return 4;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 

@@ -228,6 +228,11 @@ cudaError_t fluid_forward_force(const FluidPlan &p, const float *G, const float 
 cudaError_t fluid_forward_force_jac(const FluidPlan &p, const float *G, const float *A,
                                     const float *B, cudaStream_t s);
 cudaError_t fluid_solve(const FluidPlan &p, int inverse, cudaStream_t s);
+// shapes of the shared-memory (any-size) path; fluid_get_shapes returns 0 on
+// the register path, whose shapes are fixed
+int fluid_get_shapes(const FluidPlan &p, int *P, int *Q, int *K);
+cudaError_t fluid_set_shapes(FluidPlan *p, int P, int Q, int K);
+cudaError_t fluid_autotune(FluidPlan *p, cudaStream_t s);
 cudaError_t fluid_inverse_store(const FluidPlan &p, float *ox, float *oy, float *oz,
                                 cudaStream_t s);
 cudaError_t fluid_inverse_axpby(const FluidPlan &p, float *vx, float *vy, float *vz,

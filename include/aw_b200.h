@@ -133,6 +133,16 @@ int aw_fluid_create(int nx, int ny, int nz, double spx, double spy, double spz, 
  * ApplyOperator (v <- L v). */
 int aw_fluid_apply(aw_fluid_t k, float *vx, float *vy, float *vz, int inverse, void *stream);
 int aw_fluid_destroy(aw_fluid_t k);
+/* Launch shapes of the shared-memory FFT path (grids with an axis that is
+ * not a power of two in [16, 256]): x-line pairs per batch, y-columns per
+ * batch, (ky,kx) columns per z-pass CTA. The plan autotunes them when it is
+ * created (each candidate timed on the device; the choice is kept per grid
+ * and device for the process); aw_fluid_autotune re-runs the tuning,
+ * aw_fluid_set_shapes overrides it. Results do not depend on the shapes.
+ * aw_fluid_get_shapes writes zeros on the register-FFT path (fixed shapes). */
+int aw_fluid_get_shapes(aw_fluid_t k, int *shapes /* [3] */);
+int aw_fluid_set_shapes(aw_fluid_t k, int pairs, int cols, int zcols);
+int aw_fluid_autotune(aw_fluid_t k, void *stream);
 
 /* ---------------------------------------------------------------------------
  * Greedy iterator. Replaces GreedyIteratorGPU / GreedyIteratorCPU

@@ -278,3 +278,38 @@ def test_staged_update_equals_global_gathers(shape, sp, max_pert):
     assert np.array_equal(out[0][0], out[1][0])
     assert np.array_equal(out[0][1], out[1][1])
     assert np.abs(out[0][0] - identity(shape)).max() > 0.5
+
+
+@pytest.mark.parametrize("shape", [(36, 31, 32), (48, 40, 44), (96, 80, 72)])
+def test_fluid_shapes_autotuned_and_result_independent(shape):
+    """The shared-memory FFT path picks its launch shapes by timing at plan
+    creation; every legal shape gives the same bits, the register path
+    reports fixed shapes, and a rejected shape leaves the plan unchanged."""
+    import ctypes
+    from atlaswerks_b200 import _lib
+    L = _lib.lib()
+    rng = np.random.default_rng(21)
+    v = rng.normal(0, 1, (3,) + shape).astype(np.float32)
+    op = DiffOperB200()
+    op.SetSize(shape[::-1], (1.0, 1.3, 0.8), DiffOperParam(0.01, 0.01, 0.001))
+    sh = (ctypes.c_int * 3)()
+    _lib.check(L.aw_fluid_get_shapes(op._h, sh))
+    tuned = tuple(sh)
+    assert all(x >= 1 for x in tuned)
+    ref = host(op.ApplyInverseOperator(cu(v)))
+    for P, Q, K in [(1, 1, 1), (2, 3, 4), (tuned[0], tuned[1], 16)]:
+        _lib.check(L.aw_fluid_set_shapes(op._h, P, Q, K))
+        assert np.array_equal(host(op.ApplyInverseOperator(cu(v))), ref), (P, Q, K)
+    assert L.aw_fluid_set_shapes(op._h, 0, 1, 1) != 0
+    _lib.check(L.aw_fluid_get_shapes(op._h, sh))
+    assert tuple(sh) == (tuned[0], tuned[1], 16)
+    # a second plan of the grid reuses the tuned shapes
+    op2 = DiffOperB200()
+    op2.SetSize(shape[::-1], (1.0, 1.3, 0.8), DiffOperParam(0.01, 0.01, 0.001))
+    _lib.check(L.aw_fluid_get_shapes(op2._h, sh))
+    assert tuple(sh) == tuned
+    # power-of-two grids: fixed register-FFT shapes
+    op3 = DiffOperB200()
+    op3.SetSize((32, 32, 32), (1.0, 1.0, 1.0), DiffOperParam(0.01, 0.01, 0.001))
+    _lib.check(L.aw_fluid_get_shapes(op3._h, sh))
+    assert tuple(sh) == (0, 0, 0)
