@@ -61,6 +61,7 @@ SIGNATURES = {
     "aw_greedy_get_step": ([_fp, _fp], _i),
     "aw_greedy_set_auto_step_reduce": ([_fp, _i], _i),
     "aw_greedy_set_staged_update": ([_fp, _i], _i),
+    "aw_greedy_update_tile": ([_fp, _i, _fp], _i),
     "aw_greedy_iterate": ([_fp] * 15 + [_i, _fp], _i),
     "aw_greedy_run": ([_fp] * 15 + [_i, _i, _fp], _i),
     "aw_greedy_profile": ([_fp] * 15 + [_i, _fp, _fp], _i),

@@ -352,6 +352,20 @@ int aw_greedy_set_staged_update(aw_greedy_t g, int on) {
   return 0;
 }
 
+int aw_greedy_update_tile(aw_greedy_t g, int set, int *tile) {
+  if (!g || !tile) return fail("aw_greedy_update_tile: null pointer");
+  if (set) {
+    if (*tile < 0 || *tile >= 4) return fail("aw_greedy_update_tile: tile index must be 0..3");
+    AW_CUDA(cudaDeviceSynchronize(), "aw_greedy_update_tile (pending work)");
+    g->ctx.utile = *tile;
+    for (auto &kv : g->graphs) cudaGraphExecDestroy(kv.second);
+    g->graphs.clear();  // captured iterations hold the other tile's kernel
+  } else {
+    *tile = g->ctx.utile;
+  }
+  return 0;
+}
+
 int aw_greedy_iterate(aw_greedy_t g, const float *I0, const float *I1, const float *hx,
                       const float *hy, const float *hz, float *ox, float *oy, float *oz,
                       const float *hix, const float *hiy, const float *hiz, float *hiox,

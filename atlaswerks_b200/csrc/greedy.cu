@@ -16,6 +16,8 @@
 // on the device (GreedyIteratorCPU.cxx:125-131).
 #include <cstring>
 #include <map>
+#include <mutex>
+#include <tuple>
 
 #include "bulk.cuh"
 #include "greedy.cuh"
@@ -171,26 +173,50 @@ __global__ void __launch_bounds__(kRowThreads)
   }
 }
 
+// tuning input: h = identity, v = 0.4 in every component
+__global__ void __launch_bounds__(kRowThreads)
+    k_fill_identity_shift(float *__restrict__ hx, float *__restrict__ hy, float *__restrict__ hz,
+                          float *__restrict__ v, Dims d) {
+  Voxel p;
+  if (!voxel_of(d, p)) return;
+  const long n = d.n();
+  hx[p.i] = (float)p.x;
+  hy[p.i] = (float)p.y;
+  hz[p.i] = (float)p.z;
+  v[p.i] = 0.4f;
+  v[n + p.i] = 0.4f;
+  v[2 * n + p.i] = 0.4f;
+}
+
 // The update with h staged in shared memory. The step keeps eps*v/sp within
 // MaxPert of a voxel at the iteration that sets it, so the eight corners a
-// voxel reads lie within one voxel of it: a CTA owns a 32 x 8 x 4 tile and
+// voxel reads lie within one voxel of it: a CTA owns a 32 x TY x TZ tile and
 // the three components of h over the tile plus a one-voxel halo arrive by
 // TMA tensor loads (x from x0 - 4, so the box starts on a 16-byte boundary:
-// 40 x 10 x 6 floats each). Corners inside the volume and the box are read
-// from shared memory with trilerp_vector's own arithmetic (corner order,
-// double weights, lerp tree); any other voxel (a corner outside the volume,
-// a larger step) takes trilerp_vector from global memory. No inverse field.
-constexpr int kUTX = 32, kUTY = 8, kUTZ = 4;
-constexpr int kUBX = 40, kUBY = kUTY + 2, kUBZ = kUTZ + 2;
-constexpr int kUBox = kUBX * kUBY * kUBZ;  // floats per component (9600 B)
+// 40 x (TY+2) x (TZ+2) floats each). Corners inside the volume and the box
+// are read from shared memory with trilerp_vector's own arithmetic (corner
+// order, double weights, lerp tree); any other voxel (a corner outside the
+// volume, a larger step) takes trilerp_vector from global memory. No inverse
+// field. The tile shape is chosen per grid by timing (tune_update_tile).
+constexpr int kUTX = 32, kUBX = 40;
+template <int TY, int TZ>
+struct UTile {
+  static constexpr int BY = TY + 2, BZ = TZ + 2, BOX = kUBX * BY * BZ;
+};
+// candidate tile shapes (TY, TZ); index 0 is the default
+constexpr int kNumTiles = 4;
+constexpr int kTileTY[kNumTiles] = {8, 4, 8, 16}, kTileTZ[kNumTiles] = {4, 8, 8, 2};
 
 struct HMaps {
   CUtensorMap m[3];
 };
 
-__global__ void __launch_bounds__(kUTX * kUTY, 4)
+template <int TY, int TZ>
+__global__ void __launch_bounds__(kUTX * TY, 1024 / (kUTX * TY))
     k_update_tiled(const __grid_constant__ HMaps maps, UpdateArgs a, Dims d,
                    const float *__restrict__ step_ptr, int *status) {
+  using U = UTile<TY, TZ>;
+  constexpr int kUTY = TY, kUTZ = TZ, kUBY = U::BY, kUBZ = U::BZ, kUBox = U::BOX;
   __shared__ __align__(128) float sh[3][kUBox];
   __shared__ uint64_t mbar;
   const int tx = (d.nx + kUTX - 1) / kUTX, ty = (d.ny + kUTY - 1) / kUTY;
@@ -268,11 +294,12 @@ struct HMapCache {
   std::map<std::pair<const float *, long>, CUtensorMap> maps;
 };
 
-bool h_map(GreedyCtx *g, const float *p, CUtensorMap *out) {
+bool h_map(GreedyCtx *g, const float *p, int tile, CUtensorMap *out) {
   if (!g->hmaps) return false;
   auto *cache = static_cast<HMapCache *>(g->hmaps);
   const Dims d = g->d;
-  const long key2 = ((long)d.nz * 4096 + d.ny) * 4096 + d.nx;
+  const int kUBY = kTileTY[tile] + 2, kUBZ = kTileTZ[tile] + 2;
+  const long key2 = (((long)d.nz * 4096 + d.ny) * 4096 + d.nx) * kNumTiles + tile;
   auto it = cache->maps.find({p, key2});
   if (it != cache->maps.end()) {
     *out = it->second;
@@ -294,6 +321,103 @@ bool h_map(GreedyCtx *g, const float *p, CUtensorMap *out) {
   cache->maps[{p, key2}] = m;
   *out = m;
   return true;
+}
+
+template <int TY, int TZ>
+void launch_tiled(const HMaps &maps, const UpdateArgs &a, const Dims &d, const float *step,
+                  int *status, cudaStream_t s) {
+  const unsigned tiles = (unsigned)(((d.nx + kUTX - 1) / kUTX) * ((d.ny + TY - 1) / TY) *
+                                    ((d.nz + TZ - 1) / TZ));
+  k_update_tiled<TY, TZ><<<tiles, kUTX * TY, 0, s>>>(maps, a, d, step, status);
+}
+
+// the staged update with tile shape `tile`; false when h cannot be staged
+// (grid or alignment), so the caller takes the global-gather kernel
+bool launch_update_tiled(GreedyCtx *g, int tile, const UpdateArgs &a, const float *const h[3],
+                         cudaStream_t s) {
+  HMaps maps;
+  for (int c = 0; c < 3; ++c)
+    if (!h_map(g, h[c], tile, &maps.m[c])) return false;
+  const Dims d = g->d;
+  int *st = g->plan.status;
+  switch (tile) {
+    case 0: launch_tiled<8, 4>(maps, a, d, g->st.step, st, s); break;
+    case 1: launch_tiled<4, 8>(maps, a, d, g->st.step, st, s); break;
+    case 2: launch_tiled<8, 8>(maps, a, d, g->st.step, st, s); break;
+    default: launch_tiled<16, 2>(maps, a, d, g->st.step, st, s); break;
+  }
+  return true;
+}
+
+// tuned tile per (grid, device), kept for the process
+std::mutex g_tile_mu;
+std::map<std::tuple<int, int, int, int>, int> g_tile;
+
+// Times every tile shape on an update of the identity by a field of 0.4
+// voxel (all staged reads, the common case), 3 launches after 1 untimed
+// each, and keeps the fastest; a grid the staged kernel cannot take keeps 0.
+void tune_update_tile(GreedyCtx *g) {
+  g->utile = 0;
+  const Dims d = g->d;
+  const auto key = std::make_tuple(d.nx, d.ny, d.nz, g->plan.device);
+  {
+    std::lock_guard<std::mutex> lock(g_tile_mu);
+    auto it = g_tile.find(key);
+    if (it != g_tile.end()) {
+      g->utile = it->second;
+      return;
+    }
+  }
+  const long n = d.n();
+  float *buf = nullptr;
+  float *step = nullptr;
+  if (cudaMalloc(&buf, sizeof(float) * 6 * n) != cudaSuccess) return;
+  if (cudaMalloc(&step, sizeof(float)) != cudaSuccess) {
+    cudaFree(buf);
+    return;
+  }
+  const float one = 1.0f;
+  cudaMemcpy(step, &one, sizeof(float), cudaMemcpyHostToDevice);
+  float *h[3] = {buf, buf + n, buf + 2 * n}, *o[3] = {buf + 3 * n, buf + 4 * n, buf + 5 * n};
+  k_fill_identity_shift<<<row_grid(d), kRowThreads>>>(h[0], h[1], h[2], g->vbuf, d);
+  const UpdateArgs a{h[0], h[1], h[2], g->vbuf, g->vbuf + n, g->vbuf + 2 * n, o[0], o[1], o[2],
+                     nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                     make_divf((float)g->sp.x), make_divf((float)g->sp.y),
+                     make_divf((float)g->sp.z)};
+  const float *hc[3] = {h[0], h[1], h[2]};
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int pick = 0;
+  bool any = false;
+  float *saved_step = g->st.step;
+  g->st.step = step;
+  for (int tile = 0; tile < kNumTiles; ++tile) {
+    if (!launch_update_tiled(g, tile, a, hc, 0)) break;
+    any = true;
+    cudaEventRecord(e0, 0);
+    for (int r = 0; r < 3; ++r) launch_update_tiled(g, tile, a, hc, 0);
+    cudaEventRecord(e1, 0);
+    float ms = 0.f;
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+      break;
+    if (ms < best) {
+      best = ms;
+      pick = tile;
+    }
+  }
+  g->st.step = saved_step;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(step);
+  cudaFree(buf);
+  // the tensor maps of the scratch planes go with them
+  static_cast<HMapCache *>(g->hmaps)->maps.clear();
+  if (cudaGetLastError() != cudaSuccess || !any) return;
+  g->utile = pick;
+  std::lock_guard<std::mutex> lock(g_tile_mu);
+  g_tile[key] = pick;
 }
 
 #define AW_TRY(x)                         \
@@ -335,6 +459,8 @@ int greedy_create(GreedyCtx *g, int nx, int ny, int nz, double spx, double spy, 
       cudaEventCreateWithFlags(&g->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&g->ev_join, cudaEventDisableTiming) != cudaSuccess)
     return 4;
+  if (cudaGetLastError() != cudaSuccess) return 4;
+  tune_update_tile(g);
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
@@ -394,15 +520,8 @@ cudaError_t greedy_stage(GreedyCtx *g, int stage, const float *I0, const float *
                          inv ? hinv_out[1] : nullptr, inv ? hinv_out[2] : nullptr,
                          make_divf((float)g->sp.x), make_divf((float)g->sp.y),
                          make_divf((float)g->sp.z)};
-      HMaps maps;
-      if (!inv && !g->no_staged_update && h_map(g, h[0], &maps.m[0]) && h_map(g, h[1], &maps.m[1]) &&
-          h_map(g, h[2], &maps.m[2])) {
-        const unsigned tiles = (unsigned)(((d.nx + kUTX - 1) / kUTX) * ((d.ny + kUTY - 1) / kUTY) *
-                                          ((d.nz + kUTZ - 1) / kUTZ));
-        k_update_tiled<<<tiles, kUTX * kUTY, 0, s>>>(maps, a, d, g->st.step, g->plan.status);
-      } else {
+      if (inv || g->no_staged_update || !launch_update_tiled(g, g->utile, a, h, s))
         k_update<<<row_grid(d), kRowThreads, 0, s>>>(a, d, g->st.step);
-      }
       return cudaGetLastError();
     }
   }

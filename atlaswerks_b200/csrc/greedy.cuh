@@ -32,6 +32,7 @@ struct GreedyCtx {
   GreedyDevState st;
   void *hmaps;      // host cache of the h planes' tensor maps (greedy.cu)
   int no_staged_update;  // 1: the update gathers h from global memory only
+  int utile;             // tile shape of the staged update (greedy.cu)
 };
 
 // stages of one iteration, in launch order

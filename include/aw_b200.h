@@ -166,6 +166,11 @@ int aw_greedy_set_auto_step_reduce(aw_greedy_t g, int on);
  * ny >= 10, nz >= 6, no inverse field); 0: every gather from global memory.
  * Both give the same bits; the switch exists to compare them. */
 int aw_greedy_set_staged_update(aw_greedy_t g, int on);
+/* Tile shape of the staged update (x 32 voxels; index 0: 8 x 4 in y x z,
+ * 1: 4 x 8, 2: 8 x 8, 3: 16 x 2), chosen when the handle is created by
+ * timing each on the device (kept per grid and device for the process).
+ * set = 0 reads it into *tile, set = 1 overrides it with *tile. */
+int aw_greedy_update_tile(aw_greedy_t g, int set, int *tile);
 
 /* One Iterate(): reads h (and hinv when non-NULL), writes the updated fields
  * to h_out / hinv_out (distinct buffers). update_step=1 recomputes the step

@@ -260,23 +260,30 @@ def test_nonfinite_deformation_iterates_without_fault():
                                                ((40, 37, 52), (1.25, 0.8, 1.0), 3.0),
                                                ((64, 64, 64), (1.0, 1.0, 1.0), 0.5)])
 def test_staged_update_equals_global_gathers(shape, sp, max_pert):
-    """The update with h staged in shared memory by TMA against the one that
-    gathers every corner from global memory: bit-identical fields and
-    energies after several iterations, on grids with partial edge tiles and
-    a step large enough (MaxPert 3) that many corners leave the staged box."""
+    """The update with h staged in shared memory by TMA, in each of its four
+    tile shapes, against the one that gathers every corner from global
+    memory: bit-identical fields and energies after several iterations, on
+    grids with partial edge tiles and a step large enough (MaxPert 3) that
+    many corners leave the staged box."""
     from atlaswerks_b200 import _lib
     I0, I1 = greedy_pair(shape, seed=12)
+    import ctypes
+    L = _lib.lib()
     out = []
-    for staged in (1, 0):
+    # the global-gather kernel, then every staged tile shape
+    for staged, tile in [(0, 0), (1, 0), (1, 1), (1, 2), (1, 3)]:
         it = GreedyIteratorB200(shape[::-1], spacing=sp)
         it.SetScaleLevel(shape[::-1], sp, GreedyIteratorParam(DiffOperParam(0.01, 0.01, 0.001),
                                                                max_pert))
-        _lib.check(_lib.lib().aw_greedy_set_staged_update(it._h, staged))
+        _lib.check(L.aw_greedy_set_staged_update(it._h, staged))
+        t = ctypes.c_int(tile)
+        _lib.check(L.aw_greedy_update_tile(it._h, 1, ctypes.byref(t)))
         d = GreedyDeformationDataB200(cu(I0), cu(I1), spacing=sp)
         it.Run(d, 5, update_first=True)
         out.append((host(d.Def1To0()).copy(), it.Energies()))
-    assert np.array_equal(out[0][0], out[1][0])
-    assert np.array_equal(out[0][1], out[1][1])
+    for h, e in out[1:]:
+        assert np.array_equal(h, out[0][0])
+        assert np.array_equal(e, out[0][1])
     assert np.abs(out[0][0] - identity(shape)).max() > 0.5
 
 
