@@ -14,6 +14,8 @@
 // plus, at a step-size update (iteration 0 of a scale level,
 // GreedyWarp.txx:99), a max|v| reduction and eps = MaxPert / max|v| computed
 // on the device (GreedyIteratorCPU.cxx:125-131).
+#include <algorithm>
+#include <climits>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -291,36 +293,41 @@ __global__ void __launch_bounds__(kUTX * TY, 1024 / (kUTX * TY))
 
 // tensor maps of h planes, one per (pointer, grid), encoded on first use
 struct HMapCache {
-  std::map<std::pair<const float *, long>, CUtensorMap> maps;
+  // (plane, nx, ny, nz, box x, box y, box z) -> map
+  std::map<std::tuple<const float *, int, int, int, int, int, int>, CUtensorMap> maps;
 };
 
-bool h_map(GreedyCtx *g, const float *p, int tile, CUtensorMap *out) {
+// tensor map of one float plane of the handle's grid with a bx x by x bz box
+bool plane_map(GreedyCtx *g, const float *p, int bx, int by, int bz, CUtensorMap *out) {
   if (!g->hmaps) return false;
   auto *cache = static_cast<HMapCache *>(g->hmaps);
   const Dims d = g->d;
-  const int kUBY = kTileTY[tile] + 2, kUBZ = kTileTZ[tile] + 2;
-  const long key2 = (((long)d.nz * 4096 + d.ny) * 4096 + d.nx) * kNumTiles + tile;
-  auto it = cache->maps.find({p, key2});
+  const auto key = std::make_tuple(p, d.nx, d.ny, d.nz, bx, by, bz);
+  auto it = cache->maps.find(key);
   if (it != cache->maps.end()) {
     *out = it->second;
     return true;
   }
   const PFN_cuTensorMapEncodeTiled encode = tensor_map_encoder();
-  if (!encode || reinterpret_cast<uintptr_t>(p) % 16 || d.nx % 4 || d.nx < kUBX || d.ny < kUBY ||
-      d.nz < kUBZ)
+  if (!encode || reinterpret_cast<uintptr_t>(p) % 16 || d.nx % 4 || d.nx < bx || d.ny < by ||
+      d.nz < bz)
     return false;
   CUtensorMap m;
   const cuuint64_t dims[3] = {(cuuint64_t)d.nx, (cuuint64_t)d.ny, (cuuint64_t)d.nz};
   const cuuint64_t strides[2] = {(cuuint64_t)d.nx * 4, (cuuint64_t)d.nx * d.ny * 4};
-  const cuuint32_t box[3] = {kUBX, kUBY, kUBZ};
+  const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz};
   const cuuint32_t estr[3] = {1, 1, 1};
   if (encode(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(p), dims, strides, box,
              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return false;
-  cache->maps[{p, key2}] = m;
+  cache->maps[key] = m;
   *out = m;
   return true;
+}
+
+bool h_map(GreedyCtx *g, const float *p, int tile, CUtensorMap *out) {
+  return plane_map(g, p, kUBX, kTileTY[tile] + 2, kTileTZ[tile] + 2, out);
 }
 
 template <int TY, int TZ>
@@ -486,17 +493,23 @@ cudaError_t greedy_stage(GreedyCtx *g, int stage, const float *I0, const float *
   const long n = d.n();
   float *v[3] = {g->vbuf, g->vbuf + n, g->vbuf + 2 * n};
   switch (stage) {
-    case kStageForcePrep:
+    case kStageForcePrep: {
+      // (staging the box of I0 a tile's h points into measured slower here:
+      // the h load, the block's range reduction and the box's arrival run
+      // one after another, against eight L2-resident gathers per voxel)
+      const dim3 pg = prep_grid(d);
       if (g->am.on)
-        k_force_prep<true><<<prep_grid(d), kRowThreads, 0, s>>>(I0, I1, h[0], h[1], h[2], g->idef,
-                                                                g->partials, d, g->di, g->am);
+        k_force_prep<true><<<pg, kRowThreads, 0, s>>>(I0, I1, h[0], h[1], h[2], g->idef,
+                                                      g->partials, d, g->di, g->am);
       else
-        k_force_prep<false><<<prep_grid(d), kRowThreads, 0, s>>>(I0, I1, h[0], h[1], h[2], g->idef,
-                                                                 g->partials, d, d, g->am);
+        k_force_prep<false><<<pg, kRowThreads, 0, s>>>(I0, I1, h[0], h[1], h[2], g->idef,
+                                                       g->partials, d, d, g->am);
       return cudaGetLastError();
+    }
     case kStageEnergy: {
       const double spprod = g->sp.x * g->sp.y * g->sp.z;
-      k_energy_final<<<1, kFinalThreads, 0, s>>>(g->partials, g->nparts, spprod, g->st, auto_reduce);
+      k_energy_final<<<1, kFinalThreads, 0, s>>>(g->partials, g->nparts, spprod, g->st,
+                                                 auto_reduce);
       return cudaGetLastError();
     }
     case kStageXYForward:
