@@ -378,8 +378,14 @@ void tune_update_tile(GreedyCtx *g) {
   const long n = d.n();
   float *buf = nullptr;
   float *step = nullptr;
-  if (cudaMalloc(&buf, sizeof(float) * 6 * n) != cudaSuccess) return;
+  // no room for the tuning scratch: keep the default shape (and clear the
+  // allocation error, which is not the handle's)
+  if (cudaMalloc(&buf, sizeof(float) * 6 * n) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
   if (cudaMalloc(&step, sizeof(float)) != cudaSuccess) {
+    cudaGetLastError();
     cudaFree(buf);
     return;
   }
