@@ -48,6 +48,7 @@ SIGNATURES = {
     "aw_splat": ([_fp] * 5 + [_i] * 3 + [_f, _fp], _i),
     "aw_splat_static": ([_fp] * 5 + [_i] * 3 + [_f, _fp], _i),
     "aw_downsample": ([_fp, _i, _i, _i, _d, _d, _d, _fp, _i, _i, _i, _fp], _i),
+    "aw_resample_image": ([_fp, _i, _i, _i, _d, _d, _d, _fp, _i, _i, _i, _d, _d, _d, _fp], _i),
     "aw_upsample_hfield": ([_fp] * 3 + [_i] * 3 + [_fp] * 3 + [_i] * 4 + [_fp], _i),
     "aw_fluid_create": ([_i] * 3 + [_d] * 3 + [_f] * 3 + [_fp], _i),
     "aw_fluid_apply": ([_fp] * 4 + [_i, _fp], _i),
@@ -85,6 +86,9 @@ SIGNATURES = {
     "aw_ldmm_get_energies": ([_fp, _fp, _i, _fp], _i),
     "aw_ldmm_i1_at_0": ([_fp] * 6, _i),
     "aw_ldmm_shoot_iterate": ([_fp] * 7, _i),
+    "aw_ldmm_adshoot_iterate": ([_fp] * 7, _i),
+    "aw_ldmm_adshoot_final_maps": ([_fp] * 4, _i),
+    "aw_ldmm_get_vec_energies": ([_fp, _fp, _i, _fp], _i),
     "aw_ldmm_atlas_accumulate": ([_fp] * 4 + [ctypes.c_float, ctypes.c_long, _fp], _i),
     "aw_ldmm_atlas_normalize": ([_fp, _fp, ctypes.c_long, _fp], _i),
     "aw_nn_conv3d_scratch_floats": ([_i] * 7, ctypes.c_size_t),

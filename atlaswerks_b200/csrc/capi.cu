@@ -199,6 +199,20 @@ int aw_downsample(const float *in, int nx, int ny, int nz, double spx, double sp
   return 0;
 }
 
+int aw_resample_image(const float *in, int nx, int ny, int nz, double sx, double sy, double sz,
+                      float *out, int mx, int my, int mz, double tx, double ty, double tz,
+                      void *stream) {
+  if (!in || !out) return fail("aw_resample_image: null pointer");
+  if (nx < 1 || ny < 1 || nz < 1 || mx < 1 || my < 1 || mz < 1)
+    return fail("aw_resample_image: empty grid");
+  if (!spacing_ok(sx, sy, sz) || !spacing_ok(tx, ty, tz))
+    return fail("aw_resample_image: spacing must be positive");
+  AW_CUDA(aw::resample_image(in, aw::Dims{nx, ny, nz}, aw::Spacing{sx, sy, sz}, out,
+                             aw::Dims{mx, my, mz}, aw::Spacing{tx, ty, tz}, S(stream)),
+          "aw_resample_image");
+  return 0;
+}
+
 int aw_upsample_hfield(const float *hx, const float *hy, const float *hz, int nx, int ny, int nz,
                        float *ox, float *oy, float *oz, int mx, int my, int mz, int rescale,
                        void *stream) {
@@ -764,21 +778,55 @@ int aw_ldmm_shoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *
   return 0;
 }
 
-int aw_ldmm_get_energies(aw_ldmm_t l, double *out, int max_count, int *count) {
-  if (!l || !count) return fail("aw_ldmm_get_energies: null pointer");
-  AW_CUDA(cudaDeviceSynchronize(), "aw_ldmm_get_energies (pending work)");
+int aw_ldmm_adshoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *alpha0,
+                            float *phi0T, float *phiT0, void *stream) {
+  if (!l || !I0 || !I1 || !alpha0 || !phi0T || !phiT0)
+    return fail("aw_ldmm_adshoot_iterate: null pointer");
+  if (aw::ldmm_adshoot_prepare(&l->ctx))
+    return fail("aw_ldmm_adshoot_iterate: device allocation failed");
+  AW_CUDA(aw::ldmm_adshoot_iterate(&l->ctx, I0, I1, alpha0, phi0T, phiT0, S(stream)),
+          "aw_ldmm_adshoot_iterate");
+  return 0;
+}
+
+int aw_ldmm_adshoot_final_maps(aw_ldmm_t l, float *phi0T, float *phiT0, void *stream) {
+  if (!l || !phi0T || !phiT0) return fail("aw_ldmm_adshoot_final_maps: null pointer");
+  if (!l->ctx.adV) return fail("aw_ldmm_adshoot_final_maps: no adjoint shooting iteration yet");
+  AW_CUDA(aw::ldmm_adshoot_final_maps(&l->ctx, phi0T, phiT0, S(stream)),
+          "aw_ldmm_adshoot_final_maps");
+  return 0;
+}
+
+namespace {
+// the last min(count, cap) entries of a device ring, oldest first
+int read_ring(aw_ldmm_t l, const double *ring_dev, double *out, int max_count, int *count,
+              const char *who) {
+  AW_CUDA(cudaDeviceSynchronize(), who);
   int n = 0;
-  AW_CUDA(cudaMemcpy(&n, l->ctx.count, sizeof(int), cudaMemcpyDeviceToHost),
-          "aw_ldmm_get_energies");
+  AW_CUDA(cudaMemcpy(&n, l->ctx.count, sizeof(int), cudaMemcpyDeviceToHost), who);
   const int cap = l->ctx.cap;
   const int avail = n < cap ? n : cap;
   std::vector<double> ring(cap);
-  AW_CUDA(cudaMemcpy(ring.data(), l->ctx.energy, sizeof(double) * cap, cudaMemcpyDeviceToHost),
-          "aw_ldmm_get_energies");
+  AW_CUDA(cudaMemcpy(ring.data(), ring_dev, sizeof(double) * cap, cudaMemcpyDeviceToHost), who);
   const int m = (out && max_count < avail) ? max_count : avail;
   for (int i = 0; i < m && out; ++i) out[i] = ring[(n - avail + i) % cap];
   *count = avail;
   return 0;
+}
+}  // namespace
+
+int aw_ldmm_get_vec_energies(aw_ldmm_t l, double *out, int max_count, int *count) {
+  if (!l || !count) return fail("aw_ldmm_get_vec_energies: null pointer");
+  if (!l->ctx.venergy) {
+    *count = 0;
+    return 0;
+  }
+  return read_ring(l, l->ctx.venergy, out, max_count, count, "aw_ldmm_get_vec_energies");
+}
+
+int aw_ldmm_get_energies(aw_ldmm_t l, double *out, int max_count, int *count) {
+  if (!l || !count) return fail("aw_ldmm_get_energies: null pointer");
+  return read_ring(l, l->ctx.energy, out, max_count, count, "aw_ldmm_get_energies");
 }
 
 }  // extern "C"

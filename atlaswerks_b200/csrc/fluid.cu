@@ -292,6 +292,7 @@ cudaError_t generic_configure(const FluidPlan &p) {
   if ((e = set_smem(k_fft_xy_fwd<SrcForce>, p.smem_xy)) != cudaSuccess) return e;
   if ((e = set_smem(k_fft_xy_inv<DstField>, p.smem_xy)) != cudaSuccess) return e;
   if ((e = set_smem(k_fft_xy_inv<DstAxpby>, p.smem_xy)) != cudaSuccess) return e;
+  if ((e = set_smem(k_fft_xy_inv<DstNeg>, p.smem_xy)) != cudaSuccess) return e;
   return set_smem(k_fft_z_solve, p.smem_z);
 }
 
@@ -503,6 +504,14 @@ cudaError_t fluid_inverse_store(const FluidPlan &p, float *ox, float *oy, float 
   DstField dst{{ox, oy, oz}};
   if (p.fast) return fast_xy_inverse(p, dst, s);
   k_fft_xy_inv<DstField><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, dst);
+  return cudaGetLastError();
+}
+
+cudaError_t fluid_inverse_store_neg(const FluidPlan &p, float *ox, float *oy, float *oz,
+                                    cudaStream_t s) {
+  DstNeg dst{{ox, oy, oz}};
+  if (p.fast) return fast_xy_inverse(p, dst, s);
+  k_fft_xy_inv<DstNeg><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, dst);
   return cudaGetLastError();
 }
 

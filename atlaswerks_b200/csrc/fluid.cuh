@@ -193,6 +193,19 @@ struct DstField {
   }
 };
 
+// -K f: the shooting velocities (LDMMAdShootingIteratorCPU.cxx:256-261,
+// 291-296 scale K f by -1, an exact sign flip)
+struct DstNegBound {
+  float *c;
+  AW_D void store(long i, float v) const { c[i] = -v; }
+};
+struct DstNeg {
+  float *c[3];
+  AW_D DstNegBound bind(int comp) const {
+    return DstNegBound{comp == 0 ? c[0] : comp == 1 ? c[1] : c[2]};
+  }
+};
+
 // LDMM velocity update v = vfac * v + ufac * u (LDMMIteratorCPU::updateVelocity,
 // LDMM/LDMMIteratorCPU.cxx:177-190) with vfac = 1 - 2*eps and
 // ufac = 2*eps / sigma^2 formed from the device-resident step eps, float
@@ -235,6 +248,8 @@ cudaError_t fluid_set_shapes(FluidPlan *p, int P, int Q, int K);
 cudaError_t fluid_autotune(FluidPlan *p, cudaStream_t s);
 cudaError_t fluid_inverse_store(const FluidPlan &p, float *ox, float *oy, float *oz,
                                 cudaStream_t s);
+cudaError_t fluid_inverse_store_neg(const FluidPlan &p, float *ox, float *oy, float *oz,
+                                    cudaStream_t s);
 cudaError_t fluid_inverse_axpby(const FluidPlan &p, float *vx, float *vy, float *vz,
                                 const float *step, float sigma, cudaStream_t s);
 

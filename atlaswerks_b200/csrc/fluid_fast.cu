@@ -426,6 +426,7 @@ cudaError_t fast_configure(const FluidPlan &p) {
       set((const void *)k_xy_fwd_fast<NX, NY, SrcForce>, sxy);
       set((const void *)k_xy_inv_fast<NX, NY, DstField>, sxy);
       set((const void *)k_xy_inv_fast<NX, NY, DstAxpby>, sxy);
+      set((const void *)k_xy_inv_fast<NX, NY, DstNeg>, sxy);
     });
   });
   dispatch_n(p.d.nz, [&](auto Z) {
@@ -475,5 +476,6 @@ template cudaError_t fast_xy_forward<SrcField>(const FluidPlan &, const SrcField
 template cudaError_t fast_xy_forward<SrcForce>(const FluidPlan &, const SrcForce &, cudaStream_t);
 template cudaError_t fast_xy_inverse<DstField>(const FluidPlan &, const DstField &, cudaStream_t);
 template cudaError_t fast_xy_inverse<DstAxpby>(const FluidPlan &, const DstAxpby &, cudaStream_t);
+template cudaError_t fast_xy_inverse<DstNeg>(const FluidPlan &, const DstNeg &, cudaStream_t);
 
 }  // namespace aw

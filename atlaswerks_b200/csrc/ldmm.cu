@@ -145,9 +145,12 @@ __global__ void __launch_bounds__(kRowThreads)
   }
 }
 
+// energy[count % cap] = scale * sum(partials); advance: count += 1 (the
+// image energy, recorded last in an iteration)
 __global__ void __launch_bounds__(256)
     k_record_energy(const double *__restrict__ partials, int nparts, double scale,
-                    double *__restrict__ energy, int *__restrict__ count, int cap) {
+                    double *__restrict__ energy, int *__restrict__ count, int cap,
+                    int advance = 1) {
   double t = 0.0;
   for (int i = threadIdx.x; i < nparts; i += blockDim.x) t += partials[i];
   __shared__ double ws[8];
@@ -159,7 +162,7 @@ __global__ void __launch_bounds__(256)
     for (int w = 0; w < 8; ++w) s += ws[w];
     const int k = *count;
     energy[k % cap] = s * scale;
-    *count = k + 1;
+    if (advance) *count = k + 1;
   }
 }
 
@@ -185,6 +188,171 @@ __global__ void __launch_bounds__(256)
 __global__ void k_step_from_max(const unsigned *__restrict__ maxbits, float max_pert,
                                 float *__restrict__ step) {
   *step = fdiv(max_pert, __uint_as_float(*maxbits));
+}
+
+// ---- adjoint shooting (LDMMAdShootingIteratorCPU.cxx:237-453) ----------
+
+// central (2 sp) and one-sided (sp) divisors per axis of computeGradient
+struct GradDiv {
+  DivD c2[3], c1[3];
+};
+
+GradDiv grad_div(const Spacing &sp) {
+  return GradDiv{{make_div(2.0 * sp.x), make_div(2.0 * sp.y), make_div(2.0 * sp.z)},
+                 {make_div(sp.x), make_div(sp.y), make_div(sp.z)}};
+}
+
+// along axis c of voxel v: the offset to the two samples computeGradient
+// (wrap = false, Array3DUtils.txx:783-900) differences, and whether the
+// voxel is interior (central difference) or on a face (one-sided)
+struct GradTaps {
+  long lo, hi;
+  bool in;
+};
+AW_D GradTaps grad_taps(int c, const Voxel &v, const Dims &d) {
+  const int pos = c == 0 ? v.x : (c == 1 ? v.y : v.z);
+  const int n = c == 0 ? d.nx : (c == 1 ? d.ny : d.nz);
+  const long st = c == 0 ? 1 : (c == 1 ? (long)d.nx : (long)d.nx * d.ny);
+  return GradTaps{pos > 0 ? -st : 0, pos < n - 1 ? st : 0, pos > 0 && pos < n - 1};
+}
+AW_D float grad_of(float diff, int c, const GradTaps &t, const GradDiv &g) {
+  return __double2float_rn(ddiv((double)diff, t.in ? g.c2[c] : g.c1[c]));
+}
+// component c of computeGradient(a) at voxel v
+AW_D float ref_grad(const float *__restrict__ a, int c, const Voxel &v, const Dims &d,
+                    const GradDiv &g) {
+  const GradTaps t = grad_taps(c, v, d);
+  return grad_of(fsub(__ldg(a + v.i + t.hi), __ldg(a + v.i + t.lo)), c, t, g);
+}
+
+// f = grad(alphaHat) * alpha_t - grad(I_t) * IHat, component-wise in float
+// (backwardAdIntegration, LDMMAdShootingIteratorCPU.cxx:384-392)
+__global__ void __launch_bounds__(kRowThreads)
+    k_ad_force(const float *__restrict__ aHat, const float *__restrict__ aT,
+               const float *__restrict__ IT, const float *__restrict__ IHat, float *__restrict__ fx,
+               float *__restrict__ fy, float *__restrict__ fz, Dims d, GradDiv g) {
+  Voxel v;
+  if (!voxel_of(d, v)) return;
+  const float at = __ldg(aT + v.i), ih = __ldg(IHat + v.i);
+  float *const f[3] = {fx, fy, fz};
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    f[c][v.i] = fsub(fmul(ref_grad(aHat, c, v, d, g), at), fmul(ref_grad(IT, c, v, d, g), ih));
+}
+
+// dot = grad(I_t) . vhat (Vector3D::dot in float, x first) and
+// div = div(alpha_t * vhat) (HField3DUtils::divergence, wrap = false: the
+// products formed in float at each tap, the partials summed in float)
+// (LDMMAdShootingIteratorCPU.cxx:398-417)
+__global__ void __launch_bounds__(kRowThreads)
+    k_ad_dot_div(const float *__restrict__ IT, const float *__restrict__ vx,
+                 const float *__restrict__ vy, const float *__restrict__ vz,
+                 const float *__restrict__ aT, float *__restrict__ dot, float *__restrict__ div,
+                 Dims d, GradDiv g) {
+  Voxel v;
+  if (!voxel_of(d, v)) return;
+  const float *const vc[3] = {vx, vy, vz};
+  float dp = 0.0f, dv = 0.0f;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float gi = ref_grad(IT, c, v, d, g);
+    const float p = fmul(gi, __ldg(vc[c] + v.i));
+    dp = c == 0 ? p : fadd(dp, p);
+    const GradTaps t = grad_taps(c, v, d);
+    const float hi = fmul(__ldg(vc[c] + v.i + t.hi), __ldg(aT + v.i + t.hi));
+    const float lo = fmul(__ldg(vc[c] + v.i + t.lo), __ldg(aT + v.i + t.lo));
+    const float part = grad_of(fsub(hi, lo), c, t, g);
+    dv = c == 0 ? part : fadd(dv, part);
+  }
+  dot[v.i] = dp;
+  div[v.i] = dv;
+}
+
+// out = src(h) with background 0 (HField3DUtils::apply); sub: out -= src(h)
+template <bool SUB>
+__global__ void __launch_bounds__(kRowThreads)
+    k_ad_pull(const float *__restrict__ src, const float *__restrict__ hx,
+              const float *__restrict__ hy, const float *__restrict__ hz, float *__restrict__ out,
+              Dims d) {
+  Voxel v;
+  if (!voxel_of(d, v)) return;
+  const float r = trilerp_scalar(src, d, (double)__ldg(hx + v.i), (double)__ldg(hy + v.i),
+                                 (double)__ldg(hz + v.i), 0.0f);
+  out[v.i] = SUB ? fsub(out[v.i], r) : r;
+}
+
+__global__ void __launch_bounds__(256) k_ad_add(float *__restrict__ a, const float *__restrict__ b,
+                                                long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = fadd(a[i], b[i]);
+}
+
+// IHat = (I1 - I0(phiT0)) * (1 / sigma^2) and the image-energy partials of
+// (I0(phiT0) - I1)^2 (LDMMAdShootingIteratorCPU.cxx:313-316, 338-342)
+__global__ void __launch_bounds__(kRowThreads)
+    k_ad_residual(const float *__restrict__ J, const float *__restrict__ I1, float inv,
+                  float *__restrict__ ihat, double *__restrict__ partials, Dims d) {
+  Voxel v;
+  double e = 0.0;
+  if (voxel_of(d, v)) {
+    const float j = J[v.i], i1 = I1[v.i];
+    ihat[v.i] = fmul(fsub(i1, j), inv);
+    const float r = fsub(j, i1);
+    e = (double)r * (double)r;
+  }
+  __shared__ double ws[kRowThreads / 32];
+  e = warp_sum(e);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = e;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = threadIdx.x < kRowThreads / 32 ? ws[threadIdx.x] : 0.0;
+    t = warp_sum(t);
+    if (threadIdx.x == 0)
+      partials[((long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// partials of sum_c sum_x (L v0)_c v0_c (HField3DUtils::l2DotProd), float
+// products summed in double
+__global__ void __launch_bounds__(kRowThreads)
+    k_ad_vdot(const float *__restrict__ u, const float *__restrict__ v0,
+              double *__restrict__ partials, Dims d) {
+  Voxel v;
+  double e = 0.0;
+  if (voxel_of(d, v)) {
+    const long n = d.n();
+#pragma unroll
+    for (int c = 0; c < 3; ++c) e += (double)fmul(u[c * n + v.i], v0[c * n + v.i]);
+  }
+  __shared__ double ws[kRowThreads / 32];
+  e = warp_sum(e);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = e;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = threadIdx.x < kRowThreads / 32 ? ws[threadIdx.x] : 0.0;
+    t = warp_sum(t);
+    if (threadIdx.x == 0)
+      partials[((long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// alpha0 -= step * (-(grad(I0) . v0) - alphaTilde), float in the
+// reference's order (LDMMAdShootingIteratorCPU.cxx:421-430)
+__global__ void __launch_bounds__(kRowThreads)
+    k_ad_alpha(const float *__restrict__ I0, const float *__restrict__ v0,
+               const float *__restrict__ aTil, const float *__restrict__ step,
+               float *__restrict__ alpha0, Dims d, GradDiv g) {
+  Voxel v;
+  if (!voxel_of(d, v)) return;
+  const long n = d.n();
+  float dp = 0.0f;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float p = fmul(ref_grad(I0, c, v, d, g), __ldg(v0 + c * n + v.i));
+    dp = c == 0 ? p : fadd(dp, p);
+  }
+  const float gr = fmul(fsub(fmul(dp, -1.0f), aTil[v.i]), *step);
+  alpha0[v.i] = fsub(alpha0[v.i], gr);
 }
 
 #define AW_TRY(x)                     \
@@ -228,8 +396,9 @@ int ldmm_create(LdmmCtx *c, int nx, int ny, int nz, double spx, double spy, doub
 
 void ldmm_destroy(LdmmCtx *c) {
   fluid_plan_destroy(&c->plan);
-  void *ptrs[] = {c->J0, c->hbuf, c->diff, c->S, c->u, c->splat_scratch, c->partials, c->energy,
-                  c->scalars, c->JT, c->JD};
+  void *ptrs[] = {c->J0,     c->hbuf,   c->diff, c->S,   c->u,   c->splat_scratch,
+                  c->partials, c->energy, c->scalars, c->JT, c->JD, c->adV,
+                  c->adP,    c->adA,    c->adI,  c->venergy};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   std::memset(c, 0, sizeof(*c));
@@ -454,6 +623,158 @@ cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, flo
   if (ca) AW_TRY(cudaMemcpyAsync(phi0T, A[1], sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
   if (cb) AW_TRY(cudaMemcpyAsync(phiT0, B[1], sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
   return cudaSuccess;
+}
+
+int ldmm_adshoot_prepare(LdmmCtx *c) {
+  if (c->adV) return 0;
+  const size_t n = (size_t)c->d.n(), T = (size_t)c->T;
+  if (cudaMalloc(&c->adV, sizeof(float) * T * 3 * n) != cudaSuccess ||
+      cudaMalloc(&c->adP, sizeof(float) * 2 * (T + 1) * 3 * n) != cudaSuccess ||
+      cudaMalloc(&c->adA, sizeof(float) * T * n) != cudaSuccess ||
+      cudaMalloc(&c->adI, sizeof(float) * 6 * n) != cudaSuccess ||
+      cudaMalloc(&c->venergy, sizeof(double) * c->cap) != cudaSuccess) {
+    cudaGetLastError();
+    void *ptrs[] = {c->adV, c->adP, c->adA, c->adI, c->venergy};
+    for (void *p : ptrs)
+      if (p) cudaFree(p);
+    c->adV = c->adP = c->adA = c->adI = nullptr;
+    c->venergy = nullptr;
+    return 3;
+  }
+  // entries of iterations of the other kinds read as 0
+  return cudaMemset(c->venergy, 0, sizeof(double) * c->cap) == cudaSuccess ? 0 : 3;
+}
+
+// LDMMAdShootingIteratorCPU::Iterate (LDMM/LDMMAdShootingIteratorCPU.cxx:
+// 237-323) and backwardAdIntegration (:325-431).
+//
+//   shoot     v_0 = -K(grad(I0) alpha0); for t = 1..T-1:
+//               phi0T_t = composeVH(v_{t-1}, phi0T_{t-1})   [PARTIAL_ZERO]
+//               alpha_t = splat(alpha0, phi0T_t)
+//               phiT0_t = composeHVInv(phiT0_{t-1}, v_{t-1}) [PARTIAL_ID],
+//               I_t = I0(phiT0_t)                 (one fused kernel)
+//               v_t = -K(grad(I_t) alpha_t)       (force fused into the FFT)
+//             then the maps, I_T and alpha_T at t = T
+//   energies  image sp^3 sum (I_T - I1)^2, vector <L v0, v0>
+//   adjoint   IHat = (I1 - I_T)/sigma^2, ITilde = splat(IHat, phiT0_T),
+//             alphaTilde = 0; for i = T-1..0 at t = i+1:
+//               alphaHat = alphaTilde(phiT0_t), IHat = splat(ITilde, phi0T_t)
+//               vhat = K(grad(alphaHat) alpha_t - grad(I_t) IHat)
+//               alphaTilde -= (grad(I_t) . vhat)(phi0T_t)
+//               ITilde += splat(div(alpha_t vhat), phiT0_t)
+//   update    alpha0 -= step (-(grad(I0) . v_0) - alphaTilde)
+//
+// The reference recomposes phi0T_t / phiT0_t from the identity at every
+// backward step (O(T^2) compositions) and recomputes I_t and alpha_t; the
+// same operations in the same order produce the same values, so here the
+// shooting keeps every map, I_t and alpha_t resident in HBM and the
+// backward sweep reads them back.
+cudaError_t ldmm_adshoot_iterate(LdmmCtx *c, const float *I0, const float *I1, float *alpha0,
+                                 float *phi0T, float *phiT0, cudaStream_t s) {
+  if (!c->adV) return cudaErrorNotReady;
+  const Dims d = c->d;
+  const long n = d.n();
+  const int T = c->T;
+  const GradDiv g = grad_div(c->sp);
+  const dim3 grid = row_grid(d);
+  const unsigned flat = (unsigned)((n + 255) / 256);
+  auto V = [&](int t) { return c->adV + (long)t * 3 * n; };
+  auto P0 = [&](int t) { return c->adP + (long)t * 3 * n; };
+  auto P1 = [&](int t) { return c->adP + (long)(T + 1 + t) * 3 * n; };
+  auto A = [&](int t) { return c->adA + (long)(t - 1) * n; };  // alpha_t, t >= 1
+  auto I = [&](int t) { return c->J0 + (long)(t - 1) * n; };   // I_t, t >= 1
+  float *aHat = c->adI, *IHat = aHat + n, *aTil = IHat + n, *ITil = aTil + n, *s1 = ITil + n,
+        *s2 = s1 + n;
+  auto comp = [&](float *base, int k) { return base + k * n; };
+  auto velocity = [&](const float *G, const float *At, int t) -> cudaError_t {
+    AW_TRY(fluid_forward_force(c->plan, G, At, 0, s));
+    AW_TRY(fluid_solve(c->plan, 1, s));
+    return fluid_inverse_store_neg(c->plan, comp(V(t), 0), comp(V(t), 1), comp(V(t), 2), s);
+  };
+  auto advance = [&](int t) -> cudaError_t {  // maps, I_t and alpha_t at t from t-1
+    const float *vv[3] = {comp(V(t - 1), 0), comp(V(t - 1), 1), comp(V(t - 1), 2)};
+    const float *hh[3] = {comp(P0(t - 1), 0), comp(P0(t - 1), 1), comp(P0(t - 1), 2)};
+    float *oo[3] = {comp(P0(t), 0), comp(P0(t), 1), comp(P0(t), 2)};
+    AW_TRY(launch_compose_vh(vv, hh, oo, d, c->sp, 1, BG_PARTIAL_ZERO, nullptr, 1.0f, s));
+    AW_TRY(splat(c->sw, alpha0, oo[0], oo[1], oo[2], A(t), 0.0f, s));
+    k_forward_step<false><<<grid, kRowThreads, 0, s>>>(
+        comp(P1(t - 1), 0), comp(P1(t - 1), 1), comp(P1(t - 1), 2), vv[0], vv[1], vv[2],
+        comp(P1(t), 0), comp(P1(t), 1), comp(P1(t), 2), I0, I(t), d, c->sp);
+    return cudaGetLastError();
+  };
+
+  // shooting
+  k_identity<<<grid, kRowThreads, 0, s>>>(comp(P0(0), 0), comp(P0(0), 1), comp(P0(0), 2), d);
+  AW_TRY(cudaGetLastError());
+  k_identity<<<grid, kRowThreads, 0, s>>>(comp(P1(0), 0), comp(P1(0), 1), comp(P1(0), 2), d);
+  AW_TRY(cudaGetLastError());
+  AW_TRY(velocity(I0, alpha0, 0));
+  for (int t = 1; t < T; ++t) {
+    AW_TRY(advance(t));
+    AW_TRY(velocity(I(t), A(t), t));
+  }
+  AW_TRY(advance(T));
+
+  // energies: <L v0, v0> (recorded without advancing the count), then the image term
+  const double spprod = c->sp.x * c->sp.y * c->sp.z;
+  AW_TRY(fluid_forward_field(c->plan, comp(V(0), 0), comp(V(0), 1), comp(V(0), 2), s));
+  AW_TRY(fluid_solve(c->plan, 0, s));
+  AW_TRY(fluid_inverse_store(c->plan, comp(c->u, 0), comp(c->u, 1), comp(c->u, 2), s));
+  k_ad_vdot<<<grid, kRowThreads, 0, s>>>(c->u, V(0), c->partials, d);
+  AW_TRY(cudaGetLastError());
+  k_record_energy<<<1, 256, 0, s>>>(c->partials, c->nparts, spprod, c->venergy, c->count, c->cap,
+                                    0);
+  AW_TRY(cudaGetLastError());
+  const float inv = 1.0f / (c->sigma * c->sigma);
+  k_ad_residual<<<grid, kRowThreads, 0, s>>>(I(T), I1, inv, IHat, c->partials, d);
+  AW_TRY(cudaGetLastError());
+  k_record_energy<<<1, 256, 0, s>>>(c->partials, c->nparts, spprod, c->energy, c->count, c->cap,
+                                    1);
+  AW_TRY(cudaGetLastError());
+
+  // backward integration of the adjoint equations
+  AW_TRY(splat(c->sw, IHat, comp(P1(T), 0), comp(P1(T), 1), comp(P1(T), 2), ITil, 0.0f, s));
+  AW_TRY(cudaMemsetAsync(aTil, 0, sizeof(float) * n, s));
+  for (int i = T - 1; i >= 0; --i) {
+    const int t = i + 1;
+    float *p0[3] = {comp(P0(t), 0), comp(P0(t), 1), comp(P0(t), 2)};
+    float *p1[3] = {comp(P1(t), 0), comp(P1(t), 1), comp(P1(t), 2)};
+    k_ad_pull<false><<<grid, kRowThreads, 0, s>>>(aTil, p1[0], p1[1], p1[2], aHat, d);
+    AW_TRY(cudaGetLastError());
+    AW_TRY(splat(c->sw, ITil, p0[0], p0[1], p0[2], IHat, 0.0f, s));
+    k_ad_force<<<grid, kRowThreads, 0, s>>>(aHat, A(t), I(t), IHat, comp(c->u, 0), comp(c->u, 1),
+                                            comp(c->u, 2), d, g);
+    AW_TRY(cudaGetLastError());
+    AW_TRY(fluid_forward_field(c->plan, comp(c->u, 0), comp(c->u, 1), comp(c->u, 2), s));
+    AW_TRY(fluid_solve(c->plan, 1, s));
+    AW_TRY(fluid_inverse_store(c->plan, comp(c->u, 0), comp(c->u, 1), comp(c->u, 2), s));
+    k_ad_dot_div<<<grid, kRowThreads, 0, s>>>(I(t), comp(c->u, 0), comp(c->u, 1), comp(c->u, 2),
+                                              A(t), s1, s2, d, g);
+    AW_TRY(cudaGetLastError());
+    k_ad_pull<true><<<grid, kRowThreads, 0, s>>>(s1, p0[0], p0[1], p0[2], aTil, d);
+    AW_TRY(cudaGetLastError());
+    AW_TRY(splat(c->sw, s2, p1[0], p1[1], p1[2], s1, 0.0f, s));
+    k_ad_add<<<flat, 256, 0, s>>>(ITil, s1, n);
+    AW_TRY(cudaGetLastError());
+  }
+  k_ad_alpha<<<grid, kRowThreads, 0, s>>>(I0, V(0), aTil, c->step, alpha0, d, g);
+  AW_TRY(cudaGetLastError());
+  // the data's maps end at t_1, where the reference's backward sweep leaves them
+  AW_TRY(cudaMemcpyAsync(phi0T, P0(1), sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
+  return cudaMemcpyAsync(phiT0, P1(1), sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s);
+}
+
+// finalUpdatePhi0T / finalUpdatePhiT0 (LDMMAdShootingIteratorCPU.cxx:433-453)
+// compose the maps from the identity through the last Iterate's velocities:
+// the maps at t = T that Iterate kept
+cudaError_t ldmm_adshoot_final_maps(LdmmCtx *c, float *phi0T, float *phiT0, cudaStream_t s) {
+  if (!c->adV) return cudaErrorNotReady;
+  const long n = c->d.n();
+  const int T = c->T;
+  AW_TRY(cudaMemcpyAsync(phi0T, c->adP + (long)T * 3 * n, sizeof(float) * 3 * n,
+                         cudaMemcpyDeviceToDevice, s));
+  return cudaMemcpyAsync(phiT0, c->adP + (long)(2 * T + 1) * 3 * n, sizeof(float) * 3 * n,
+                         cudaMemcpyDeviceToDevice, s);
 }
 
 int ldmm_set_orig(LdmmCtx *c, int on) {

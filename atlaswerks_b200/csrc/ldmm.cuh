@@ -31,6 +31,12 @@ struct LdmmCtx {
   int orig;         // IterateOrig (Jacobian path) instead of IterateNew
   float *JT;        // T x N: I1 pulled back to each time point (IterateOrig)
   float *JD;        // T x N: transported Jacobian determinants (IterateOrig)
+  // adjoint shooting (allocated by ldmm_adshoot_prepare)
+  float *adV;       // T x 3N: the shot velocities v_0 .. v_{T-1}
+  float *adP;       // 2 x (T+1) x 3N: phi0T then phiT0 at t = 0 .. T
+  float *adA;       // T x N: alpha_t = splat(alpha0, phi0T_t), t = 1 .. T
+  float *adI;       // 6N: alphaHat, IHat, alphaTilde, ITilde and two scratch images
+  double *venergy;  // <L v0, v0> history ring, indexed like energy
 };
 
 int ldmm_create(LdmmCtx *c, int nx, int ny, int nz, double spx, double spy, double spz,
@@ -46,6 +52,13 @@ cudaError_t ldmm_atlas_accumulate(float *acc, float *jsum, const float *img, con
 cudaError_t ldmm_atlas_normalize(float *acc, const float *jsum, long n, cudaStream_t s);
 cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, float *alpha0,
                                float *phi0T, float *phiT0, cudaStream_t s);
+// LDMMAdShootingIteratorCPU (LDMM/LDMMAdShootingIteratorCPU.cxx): the
+// buffers (returns 3 when an allocation fails), one Iterate, and the final
+// maps of finalUpdatePhi0T / finalUpdatePhiT0 from the last Iterate
+int ldmm_adshoot_prepare(LdmmCtx *c);
+cudaError_t ldmm_adshoot_iterate(LdmmCtx *c, const float *I0, const float *I1, float *alpha0,
+                                 float *phi0T, float *phiT0, cudaStream_t s);
+cudaError_t ldmm_adshoot_final_maps(LdmmCtx *c, float *phi0T, float *phiT0, cudaStream_t s);
 // One iteration (IterateNew or IterateOrig); v is [T][3][N]. update_step:
 // compute the step from max |2v - (2/sigma^2) K f| and leave v unchanged.
 cudaError_t ldmm_iterate(LdmmCtx *c, const float *I0, const float *I1, float *v, int update_step,

@@ -124,6 +124,52 @@ __global__ void __launch_bounds__(kRowThreads)
   oz[p.i] = fadd(__int2float_rn(p.z), c);
 }
 
+// ImageUtils::resampleNew with BACKGROUND_STRATEGY_CLAMP and linear
+// interpolation (UtilitiesDataTypes/ImageUtils.txx:306-349,
+// Array3DUtils::trilerp, Array3DUtils.txx:63-210), origin 0: destination
+// voxel x samples the source at (x dsp + (dsp - ssp)/2) / ssp, the weights
+// formed from the unclamped floor, the corners clamped into the grid.
+__global__ void __launch_bounds__(kRowThreads)
+    k_resample_image(const float *__restrict__ in, Dims din, double ssx, double ssy, double ssz,
+                     float *__restrict__ out, Dims dout, double dsx, double dsy, double dsz) {
+  Voxel p;
+  if (!voxel_of(dout, p)) return;
+  const double pos[3] = {
+      __ddiv_rn(dadd(dmul(dsx, (double)p.x), __ddiv_rn(dsub(dsx, ssx), 2.0)), ssx),
+      __ddiv_rn(dadd(dmul(dsy, (double)p.y), __ddiv_rn(dsub(dsy, ssy), 2.0)), ssy),
+      __ddiv_rn(dadd(dmul(dsz, (double)p.z), __ddiv_rn(dsub(dsz, ssz), 2.0)), ssz)};
+  const int size[3] = {din.nx, din.ny, din.nz};
+  int f[3], c[3];
+  double w[3], omw[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    f[a] = ref_floor_d(pos[a]);
+    c[a] = f[a] + 1;
+    w[a] = dsub(pos[a], (double)f[a]);
+    omw[a] = dsub(1.0, w[a]);
+    // the reference's clamp, then (for positions past the last cell plus
+    // one, which the reference reads out of bounds) into the grid
+    if (f[a] < 0) {
+      f[a] = 0;
+      if (c[a] < 0) c[a] = 0;
+    }
+    if (c[a] >= size[a]) {
+      c[a] = size[a] - 1;
+      if (f[a] > size[a] - 1) f[a] = size[a] - 1;
+    }
+  }
+  float v[8];
+  v[0] = __ldg(in + din.idx(f[0], f[1], f[2]));
+  v[1] = __ldg(in + din.idx(c[0], f[1], f[2]));
+  v[2] = __ldg(in + din.idx(c[0], c[1], f[2]));
+  v[3] = __ldg(in + din.idx(f[0], c[1], f[2]));
+  v[4] = __ldg(in + din.idx(f[0], c[1], c[2]));
+  v[5] = __ldg(in + din.idx(c[0], c[1], c[2]));
+  v[6] = __ldg(in + din.idx(c[0], f[1], c[2]));
+  v[7] = __ldg(in + din.idx(f[0], f[1], c[2]));
+  out[p.i] = __double2float_rn(lerp_tree(v, w[0], w[1], w[2], omw[0], omw[1], omw[2]));
+}
+
 // GaussianFilter3D::filter_generate_gauss_full, float arithmetic as there
 void gauss_rows(float sigma, int size, std::vector<float> &rows) {
   rows.assign((size_t)(size + 1) * (size + 1), 0.0f);
@@ -225,6 +271,13 @@ cudaError_t downsample(const float *in, Dims din, Spacing sin, float *out, Dims 
   // sin * (nin / nout) (gaussianDownsample)
   const Spacing sout{sin.x * f[0], sin.y * f[1], sin.z * f[2]};
   k_resample_down<<<row_grid(dout), kRowThreads, 0, s>>>(src, din, out, dout, sin, sout);
+  return cudaGetLastError();
+}
+
+cudaError_t resample_image(const float *in, Dims din, Spacing sin, float *out, Dims dout,
+                           Spacing sout, cudaStream_t s) {
+  k_resample_image<<<row_grid(dout), kRowThreads, 0, s>>>(in, din, sin.x, sin.y, sin.z, out, dout,
+                                                         sout.x, sout.y, sout.z);
   return cudaGetLastError();
 }
 

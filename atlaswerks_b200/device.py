@@ -112,6 +112,17 @@ def downsample(img: torch.Tensor, new_shape, spacing=(1.0, 1.0, 1.0)) -> torch.T
     return out
 
 
+def resample_image(img: torch.Tensor, new_shape, spacing, new_spacing) -> torch.Tensor:
+    """ImageUtils::resampleNew (clamped linear, origin 0) onto new_shape =
+    (nz, ny, nx) with new_spacing: MultiscaleManager's image upsampling."""
+    _check_image(img, "img")
+    out = torch.empty(tuple(new_shape), device=img.device, dtype=torch.float32)
+    mz, my, mx = new_shape
+    check(_lib.lib().aw_resample_image(_p(img), *_dims(img), *map(float, spacing), _p(out), mx,
+                                       my, mz, *map(float, new_spacing), _stream()))
+    return out
+
+
 def upsample_hfield(h: torch.Tensor, new_shape, rescale: bool = True) -> torch.Tensor:
     """hToVelocity + resampleNew(CLAMP) + velocityToH to new_shape."""
     _check_field(h, "h")

@@ -10,21 +10,34 @@
   geodesic from alpha0 over T time steps, pull the residual back by
   splatting and update alpha0 (LDMMShootingIteratorCPU.cxx:199-304).
 
-The iteration runs in libaw_b200.so (``aw_ldmm_shoot_iterate`` on an LDMM
-handle, which holds T, sigma, the step size and the fluid kernel). The
-energy history holds the image term sp^3 sum (I0(phiT0) - I1)^2; the
-velocity terms LDMMEnergy adds are not formed.
+* ``LDMMAdShootingIteratorB200`` — LDMMAdShootingIteratorCPU / GPU
+  (LDMM/LDMMAdShootingIteratorCPU.cxx:237-453): shoots the geodesic keeping
+  every time point, integrates the adjoint equations backward and takes the
+  gradient step on alpha0; ``finalUpdatePhi0T`` / ``finalUpdatePhiT0``.
+* ``LDMMAdShootingWarpB200`` — LDMMWarpAd<LDMMAdShootingIterator*>: the
+  RunWarp scale loop (LDMM/LDMMWarp.txx:72-133) with LDMMShootingDefData's
+  scale change (alpha0 resampled, images Gaussian-downsampled:
+  LDMMShootingDefData.cxx:133-176) and FinishWarp's final maps
+  (LDMMWarpAd.txx:37-42).
+
+The iterations run in libaw_b200.so (``aw_ldmm_shoot_iterate`` /
+``aw_ldmm_adshoot_iterate`` on an LDMM handle, which holds T, sigma, the
+step size and the fluid kernel). The energy history holds the image term
+sp^3 sum (I0(phiT0) - I1)^2; the adjoint iterator also records the vector
+term <L v0, v0> (``VecEnergies``).
 """
 from __future__ import annotations
 
 import ctypes
-from typing import Sequence
+from dataclasses import dataclass
+from typing import List, Sequence
 
 import numpy as np
 import torch
 
 from . import _lib
 from ._lib import check
+from . import device as D
 from .device import _check_image, _stream, apply, identity
 from .ldmm import LDMMIteratorParam
 
@@ -120,3 +133,110 @@ def shoot_register(I0: torch.Tensor, I1: torch.Tensor, n_time_steps: int, n_iter
     for _ in range(n_iters):
         it.Iterate(data)
     return data, it.Energies()
+
+
+class LDMMAdShootingIteratorB200(LDMMShootingIteratorB200):
+    """LDMMAdShootingIteratorCPU / GPU (LDMM/LDMMAdShootingIteratorCPU.h):
+    the same handle and scale-level set-up as the momentum-shooting
+    iterator, the adjoint Iterate."""
+
+    def Iterate(self, data: LDMMShootingDefDataB200):
+        check(_lib.lib().aw_ldmm_adshoot_iterate(self._h, data.I0.data_ptr(), data.I1.data_ptr(),
+                                                 data.Alpha0.data_ptr(), data.Phi0T.data_ptr(),
+                                                 data.PhiT0.data_ptr(), _stream()))
+
+    def _final(self, data: LDMMShootingDefDataB200, which: int):
+        other = torch.empty_like(data.Phi0T)
+        p0, p1 = (data.Phi0T, other) if which == 0 else (other, data.PhiT0)
+        check(_lib.lib().aw_ldmm_adshoot_final_maps(self._h, p0.data_ptr(), p1.data_ptr(),
+                                                    _stream()))
+
+    def finalUpdatePhi0T(self, data: LDMMShootingDefDataB200):
+        """Phi0T composed from the identity through the last iteration's v_t."""
+        self._final(data, 0)
+
+    def finalUpdatePhiT0(self, data: LDMMShootingDefDataB200):
+        """PhiT0 composed from the identity through the last iteration's v_t."""
+        self._final(data, 1)
+
+    def VecEnergies(self) -> np.ndarray:
+        """<L v0, v0> per iteration (LDMMEnergy::VecStepEnergy(0))."""
+        n = ctypes.c_int()
+        check(_lib.lib().aw_ldmm_get_vec_energies(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros(max(n.value, 1), np.float64)
+        check(_lib.lib().aw_ldmm_get_vec_energies(self._h, out.ctypes.data, n.value,
+                                                  ctypes.byref(n)))
+        return out[: n.value]
+
+
+@dataclass
+class LDMMShootingScaleLevel:
+    """One LDMMScaleLevel of an adjoint-shooting warp: downsample factor,
+    iterations, fixed step size (UseAdaptiveStepSize is false for shooting)."""
+    DownsampleFactor: int
+    NIterations: int
+    StepSize: float
+
+
+class LDMMAdShootingWarpB200:
+    """LDMMWarpAd<LDMMAdShootingIteratorB200>::RunWarp over the scale levels,
+    coarsest first: at the first level alpha0 = 0; at each later one alpha0
+    is resampled onto the finer grid (MultiscaleManager::UpsampleToLevel, the
+    images' resampleNew) and the images are Gaussian-downsampled from the
+    originals except at factor 1. FinishWarp leaves the final maps."""
+
+    def __init__(self, I0: torch.Tensor, I1: torch.Tensor,
+                 levels: Sequence[LDMMShootingScaleLevel], n_time_steps: int = 5,
+                 spacing=(1.0, 1.0, 1.0), sigma: float = 1.0, kernel=None):
+        from .greedy import DiffOperParam
+        _check_image(I0, "I0")
+        _check_image(I1, "I1")
+        self.I0, self.I1 = I0, I1
+        self.T = int(n_time_steps)
+        self.spacing = tuple(float(s) for s in spacing)
+        self.levels = sorted(levels, key=lambda l: -l.DownsampleFactor)
+        if len({l.DownsampleFactor for l in self.levels}) != len(self.levels):
+            raise ValueError("cannot add multiple scale levels with the same downsample factor")
+        self.sigma = float(sigma)
+        self.kernel = kernel or DiffOperParam()
+        self.energies: List[np.ndarray] = []
+        self.vec_energies: List[np.ndarray] = []
+        self.data = None
+
+    def RunWarp(self) -> LDMMShootingDefDataB200:
+        from .multiscale import level_geometry
+        shape = tuple(self.I0.shape)
+        alpha0, prev_sp = None, None
+        for li, lev in enumerate(self.levels):
+            size, sp = level_geometry(shape, self.spacing, lev.DownsampleFactor)
+            if size == shape:
+                I0, I1 = self.I0, self.I1
+            else:
+                I0 = D.downsample(self.I0, size, self.spacing)
+                I1 = D.downsample(self.I1, size, self.spacing)
+            data = LDMMShootingDefDataB200(I0, I1, sp)
+            if li > 0:
+                data.Alpha0.copy_(D.resample_image(alpha0, size, prev_sp, sp))
+            it = LDMMAdShootingIteratorB200((size[2], size[1], size[0]), spacing=sp,
+                                            n_time_steps=self.T)
+            it.SetScaleLevel((size[2], size[1], size[0]), sp,
+                             LDMMIteratorParam(self.kernel, self.sigma, lev.StepSize, False))
+            for _ in range(lev.NIterations):
+                it.Iterate(data)
+            self.energies.append(it.Energies())
+            self.vec_energies.append(it.VecEnergies())
+            alpha0, prev_sp = data.Alpha0, sp
+        it.finalUpdatePhi0T(data)
+        it.finalUpdatePhiT0(data)
+        self.data = data
+        return data
+
+    def GetDefImage(self) -> torch.Tensor:
+        """I0 carried to time 1 (LDMMWarp::GetDefImage -> GetI0At1)."""
+        return self.data.GetI0At1()
+
+    def GetInvDefImage(self) -> torch.Tensor:
+        return self.data.GetI1At0()
+
+    def GetAlpha0(self) -> torch.Tensor:
+        return self.data.Alpha0

@@ -102,6 +102,17 @@ int aw_upsample_hfield(const float *hx, const float *hy, const float *hz, int nx
                        float *ox, float *oy, float *oz, int mx, int my, int mz, int rescale,
                        void *stream);
 
+/* Image resampling onto another grid: ImageUtils::resampleNew
+ * (UtilitiesDataTypes/ImageUtils.txx:306-349) with clamped linear
+ * interpolation, origin 0, (sx, sy, sz) the input spacing and (tx, ty, tz)
+ * the output spacing — MultiscaleManager::UpsampleToLevel for images
+ * (Algorithms/Common/MultiscaleManager.cxx:301-323), which
+ * LDMMShootingDefData::SetScaleLevel applies to Alpha0
+ * (Algorithms/LDMM/LDMMShootingDefData.cxx:166-168). */
+int aw_resample_image(const float *in, int nx, int ny, int nz, double sx, double sy, double sz,
+                      float *out, int mx, int my, int mz, double tx, double ty, double tz,
+                      void *stream);
+
 /* Scratch capacity of aw_splat_static, fixed when the library is built. */
 #define AW_SPLAT_STATIC_MAX_BYTES (8u << 20)
 
@@ -283,6 +294,27 @@ int aw_ldmm_get_energies(aw_ldmm_t l, double *out, int max_count, int *count);
  * the image energy (aw_ldmm_get_energies). */
 int aw_ldmm_shoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *alpha0,
                           float *phi0T, float *phiT0, void *stream);
+
+/* LDMM adjoint geodesic shooting (LDMMAdShootingIteratorCPU::Iterate and
+ * backwardAdIntegration, Algorithms/LDMM/LDMMAdShootingIteratorCPU.cxx:
+ * 237-431; GPU twin LDMMAdShootingIteratorGPU) on an LDMM handle (its T,
+ * sigma, step size and kernel): shoots the geodesic from alpha0 keeping
+ * every velocity, map, deformed image and momentum image of the T time
+ * points in device memory (allocated at the first call), integrates the
+ * adjoint equations backward and takes the gradient step
+ * alpha0 -= step * (-(grad I0 . v0) - alphaTilde). phi0T / phiT0 end at
+ * time t_1, as the reference's iteration leaves LDMMShootingDefData's maps.
+ * Records the image energy sp^3 sum (I0(phiT0) - I1)^2 (aw_ldmm_get_energies)
+ * and <L v0, v0> (aw_ldmm_get_vec_energies). */
+int aw_ldmm_adshoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *alpha0,
+                            float *phi0T, float *phiT0, void *stream);
+/* LDMMWarpAd::FinishWarp's finalUpdatePhi0T / finalUpdatePhiT0
+ * (LDMMAdShootingIteratorCPU.cxx:433-453, LDMMWarpAd.txx:37-42): the maps
+ * from time 0 to 1 and back composed through the last iteration's velocities. */
+int aw_ldmm_adshoot_final_maps(aw_ldmm_t l, float *phi0T, float *phiT0, void *stream);
+/* Vector energies <L v0, v0> sp^3 of the adjoint shooting iterations, oldest
+ * first (LDMMEnergy::VecStepEnergy(0)); synchronises. */
+int aw_ldmm_get_vec_energies(aw_ldmm_t l, double *out, int max_count, int *count);
 
 /* LDMM relaxation atlas (LDMMAtlasBuilder / LDMMAtlasThreadCPU,
  * Algorithms/LDMM/LDMMAtlasThreadCPU.cxx:207-264, LDMMAtlasBuilder.txx:274-335).

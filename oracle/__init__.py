@@ -91,6 +91,7 @@ class Oracle:
         L.aw_oracle_atlas_iterate.restype = ctypes.c_double
         L.aw_oracle_ldmm_iterate_orig.restype = ctypes.c_double
         L.aw_oracle_ldmm_shoot_iterate.restype = ctypes.c_double
+        L.aw_oracle_ldmm_adshoot_iterate.restype = ctypes.c_double
 
     # --- interpolation family -------------------------------------------------
     def apply(self, img, h, bg=0.0):
@@ -251,6 +252,79 @@ class Oracle:
             *_shape(I0), *map(_dbl, sp), _dbl(alpha), _dbl(beta), _dbl(gamma),
             ctypes.c_float(sigma), ctypes.c_float(step))
         return float(e), p0, p1
+
+    def ldmm_adshoot_iterate(self, I0, I1, alpha0, T, sp=(1.0, 1.0, 1.0), alpha=0.01,
+                             beta=0.01, gamma=0.001, sigma=0.1, step=0.005):
+        """One LDMMAdShootingIteratorCPU::Iterate (shooting, then the backward
+        adjoint integration); alpha0 [nz,ny,nx] updated in place. Returns
+        (image energy, vector energy <L v0, v0>, V [T,3,...], phi0T, phiT0),
+        the maps as the iteration leaves them (at time t_1)."""
+        assert alpha0.dtype == np.float32 and alpha0.flags.c_contiguous
+        p0 = np.empty((3,) + I0.shape, np.float32)
+        p1 = np.empty((3,) + I0.shape, np.float32)
+        V = np.empty((T, 3) + I0.shape, np.float32)
+        ev = ctypes.c_double()
+        e = self.lib.aw_oracle_ldmm_adshoot_iterate(
+            _fp(I0), _fp(I1), _fp(alpha0), p0.ctypes.data_as(_f), p1.ctypes.data_as(_f),
+            V.ctypes.data_as(_f), _i(T), *_shape(I0), *map(_dbl, sp), _dbl(alpha), _dbl(beta),
+            _dbl(gamma), ctypes.c_float(sigma), ctypes.c_float(step), ctypes.byref(ev))
+        return float(e), float(ev.value), V, p0, p1
+
+    def adshoot_final_maps(self, V, sp=(1.0, 1.0, 1.0)):
+        """finalUpdatePhi0T / finalUpdatePhiT0 (LDMMAdShootingIteratorCPU.cxx:
+        433-453): the maps composed from identity through every stored v_t."""
+        shape = V.shape[2:]
+        p0, p1 = identity(shape), identity(shape)
+        for t in range(V.shape[0]):
+            p0 = self.compose_vh(V[t], p0, sp, direction=1, bg=BG_PARTIAL_ZERO)
+            p1 = self.compose_hv(p1, V[t], sp, direction=-1, bg=BG_PARTIAL_ID)
+        return p0, p1
+
+    def resample_image(self, img, new_shape, src_sp, dst_sp):
+        """ImageUtils::resampleNew with clamped linear interpolation (the
+        MultiscaleManager's image upsampling), origin 0."""
+        out = np.empty(new_shape, np.float32)
+        mz, my, mx = new_shape
+        self.lib.aw_oracle_resample_image(_fp(np.ascontiguousarray(img, np.float32)), *_shape(img),
+                                          *map(_dbl, src_sp), _fp(out), _i(mx), _i(my), _i(mz),
+                                          *map(_dbl, dst_sp))
+        return out
+
+    def adshoot_warp(self, I0, I1, T, levels, sp=(1.0, 1.0, 1.0), sigma=1.0, alpha=0.01,
+                     beta=0.01, gamma=0.001):
+        """LDMMWarpAd::RunWarp (Algorithms/LDMM/LDMMWarp.txx:72-133,
+        LDMMWarpAd.txx:37-42) over levels = [(factor, iters, step)], coarsest
+        first after sorting: images Gaussian-downsampled per level, alpha0
+        from zero at the first level and resampled (resampleNew) to each next
+        one, final maps from the last shooting. Returns (alpha0, phi0T,
+        phiT0, [(image energies, vector energies)] per level)."""
+        levels = sorted(levels, key=lambda l: -l[0])
+        shape = I0.shape
+        a0 = None
+        prev_sp = None
+        V = None
+        hist = []
+        for li, (f, iters, step) in enumerate(levels):
+            size = tuple(n // f for n in shape)
+            lsp = tuple(float(np.float32(s) * np.float32(f)) for s in sp)
+            if size == tuple(shape):
+                a, b = I0, I1
+            else:
+                a, b = self.downsample(I0, size, sp), self.downsample(I1, size, sp)
+            if li == 0:
+                a0 = np.zeros(size, np.float32)
+            else:
+                a0 = self.resample_image(a0, size, prev_sp, lsp)
+            prev_sp = lsp
+            ei, ev = [], []
+            for _ in range(iters):
+                e, v, V, _, _ = self.ldmm_adshoot_iterate(a, b, a0, T, lsp, alpha, beta, gamma,
+                                                          sigma, step)
+                ei.append(e)
+                ev.append(v)
+            hist.append((np.array(ei), np.array(ev)))
+        p0, p1 = self.adshoot_final_maps(V, prev_sp)
+        return a0, p0, p1, hist
 
     def ldmm_i1_at_0(self, I1, v, sp=(1.0, 1.0, 1.0), jacdet=True):
         """LDMMDeformationData::GetI1At0 and LDMMIteratorCPU::ComputeJacDet
@@ -552,6 +626,30 @@ class Reference:
                 _fp(a0), p0.ctypes.data_as(_f), p1.ctypes.data_as(_f), _dp(en))
         self._check(rc)
         return a0, p0, p1, en
+
+    def adshoot_run(self, I0, I1, T, levels, sp=(1.0, 1.0, 1.0), sigma=1.0, alpha=0.01,
+                    beta=0.01, gamma=0.001):
+        """The reference's LDMMShootingDefData / LDMMAdShootingIteratorCPU
+        through the LDMMWarpAd scale loop; levels = [(factor, iters, step)]
+        in parameter-file order. Returns (alpha0, phi0T, phiT0, image
+        energies, vector energies), the maps from FinishWarp."""
+        ns = len(levels)
+        fa = (ctypes.c_int * ns)(*[l[0] for l in levels])
+        it = (ctypes.c_int * ns)(*[l[1] for l in levels])
+        st = (ctypes.c_float * ns)(*[l[2] for l in levels])
+        a0 = np.empty(I0.shape, np.float32)
+        p0 = np.empty((3,) + I0.shape, np.float32)
+        p1 = np.empty((3,) + I0.shape, np.float32)
+        total = int(sum(l[1] for l in levels))
+        ei = np.zeros(total, np.float64)
+        ev = np.zeros(total, np.float64)
+        with quiet_stdout():
+            rc = self.lib.awref_adshoot_run(
+                _fp(I0), _fp(I1), *_shape(I0), *map(_dbl, sp), _i(T), _i(ns), fa, it, st,
+                ctypes.c_float(sigma), _dbl(alpha), _dbl(beta), _dbl(gamma), _fp(a0),
+                p0.ctypes.data_as(_f), p1.ctypes.data_as(_f), _dp(ei), _dp(ev))
+        self._check(rc)
+        return a0, p0, p1, ei, ev
 
     def ldmm_atlas_run(self, imgs, weights, T, iters, sp=(1.0, 1.0, 1.0), sigma=0.1, step=0.005,
                        adaptive=False, max_pert=0.1, alpha=0.01, beta=0.01, gamma=0.001,

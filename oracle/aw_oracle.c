@@ -882,6 +882,233 @@ double aw_oracle_ldmm_shoot_iterate(const float *I0, const float *I1, float *alp
 }
 
 /* ------------------------------------------------------------------------
+ * Adjoint geodesic shooting: LDMMAdShootingIteratorCPU::Iterate
+ * (Algorithms/LDMM/LDMMAdShootingIteratorCPU.cxx:237-323) and
+ * backwardAdIntegration (:325-431).
+ * ---------------------------------------------------------------------- */
+
+/* HField3DUtils::divergence with wrap = false (UtilitiesDataTypes/
+ * HField3DUtils.txx:2306-2349): d wx/dx + d wy/dy + d wz/dz, each partial
+ * from computeGradient of one component, summed in float */
+static void divergence(const float *w, float *out, float *g, int nx, int ny, int nz, double spx,
+                       double spy, double spz) {
+  const long n = (long)nx * ny * nz;
+  float *t1 = g, *t2 = g + n, *t3 = g + 2 * n;
+  float *scratch = (float *)malloc(sizeof(float) * (size_t)(2 * n));
+  /* only the diagonal partials are used: the others land in scratch */
+  aw_oracle_gradient(w, t1, scratch, scratch + n, nx, ny, nz, spx, spy, spz, 0);
+  aw_oracle_gradient(w + n, scratch, t2, scratch + n, nx, ny, nz, spx, spy, spz, 0);
+  aw_oracle_gradient(w + 2 * n, scratch, scratch + n, t3, nx, ny, nz, spx, spy, spz, 0);
+  for (long k = 0; k < n; ++k) out[k] = t1[k] + t2[k] + t3[k];
+  free(scratch);
+}
+
+/* Vector3D::dot in float, x first (HField3DUtils::pointwiseL2DotProd,
+ * HField3DUtils.txx:204-221) */
+static void dot3(const float *a, const float *b, float *out, long n) {
+  for (long k = 0; k < n; ++k) out[k] = a[k] * b[k] + a[n + k] * b[n + k] + a[2 * n + k] * b[2 * n + k];
+}
+
+/* w (3 planes) *= s, component-wise (Array3D<Vector3D>::pointwiseMultiplyBy) */
+static void scale3(float *w, const float *s, long n) {
+  for (long k = 0; k < n; ++k) {
+    w[k] *= s[k];
+    w[n + k] *= s[k];
+    w[2 * n + k] *= s[k];
+  }
+}
+
+double aw_oracle_ldmm_adshoot_iterate(const float *I0, const float *I1, float *alpha0,
+                                      float *phi0T, float *phiT0, float *V, int T, int nx, int ny,
+                                      int nz, double spx, double spy, double spz, double alpha,
+                                      double beta, double gamma, float sigma, float step,
+                                      double *vec_energy) {
+  const long n = (long)nx * ny * nz;
+  const size_t f1 = sizeof(float) * (size_t)n, f3 = 3 * f1;
+  float *o = (float *)malloc(f3), *w = (float *)malloc(f3), *w2 = (float *)malloc(f3);
+  float *aT = (float *)malloc(f1), *I = (float *)malloc(f1), *IHat = (float *)malloc(f1);
+  float *aHat = (float *)malloc(f1), *IT = (float *)malloc(f1), *aTil = (float *)malloc(f1);
+  float *ITil = (float *)malloc(f1), *s1 = (float *)malloc(f1), *s2 = (float *)malloc(f1);
+  float *p0 = phi0T, *p1 = phiT0;
+#define AD_V(t) (V + (long)(t) * 3 * n)
+  /* phi0T = composeVH(v, phi0T) [PARTIAL_ZERO]; phiT0 = composeHVInv(phiT0, v) [PARTIAL_ID] */
+#define AD_ADVANCE_P0(v)                                                                       \
+  do {                                                                                         \
+    aw_oracle_compose_vh((v), (v) + n, (v) + 2 * n, p0, p0 + n, p0 + 2 * n, o, o + n, o + 2 * n, \
+                         nx, ny, nz, spx, spy, spz, 1, AW_BG_PARTIAL_ZERO);                    \
+    memcpy(p0, o, f3);                                                                         \
+  } while (0)
+#define AD_ADVANCE_P1(v)                                                                       \
+  do {                                                                                         \
+    aw_oracle_compose_hv(p1, p1 + n, p1 + 2 * n, (v), (v) + n, (v) + 2 * n, o, o + n, o + 2 * n, \
+                         nx, ny, nz, spx, spy, spz, -1, AW_BG_PARTIAL_ID);                     \
+    memcpy(p1, o, f3);                                                                         \
+  } while (0)
+  /* v_t = -K(grad(G) * alpha_t) */
+#define AD_VELOCITY(G, t)                                                                      \
+  do {                                                                                         \
+    float *vt = AD_V(t);                                                                       \
+    aw_oracle_gradient((G), vt, vt + n, vt + 2 * n, nx, ny, nz, spx, spy, spz, 0);             \
+    scale3(vt, aT, n);                                                                         \
+    aw_oracle_fluid_apply(vt, vt + n, vt + 2 * n, nx, ny, nz, spx, spy, spz, alpha, beta,      \
+                          gamma, 1);                                                           \
+    for (long k = 0; k < 3 * n; ++k) vt[k] = vt[k] * -1.0f;                                    \
+  } while (0)
+
+  /* part 1: shooting, every v_t kept (Iterate, .cxx:245-322) */
+  aw_oracle_identity(p0, p0 + n, p0 + 2 * n, nx, ny, nz);
+  aw_oracle_identity(p1, p1 + n, p1 + 2 * n, nx, ny, nz);
+  memcpy(aT, alpha0, f1);
+  AD_VELOCITY(I0, 0);
+  for (int t = 1; t < T; ++t) {
+    AD_ADVANCE_P0(AD_V(t - 1));
+    aw_oracle_splat(alpha0, p0, p0 + n, p0 + 2 * n, aT, nx, ny, nz, 0.0f);
+    AD_ADVANCE_P1(AD_V(t - 1));
+    aw_oracle_apply(I0, p1, p1 + n, p1 + 2 * n, I, nx, ny, nz, 0.0f);
+    AD_VELOCITY(I, t);
+  }
+  AD_ADVANCE_P1(AD_V(T - 1));
+  AD_ADVANCE_P0(AD_V(T - 1));
+  /* <L v0, v0>: float products and float sums per component
+   * (HField3DUtils::l2DotProd, HField3DUtils.txx:190-200) */
+  memcpy(w, AD_V(0), f3);
+  aw_oracle_fluid_apply(w, w + n, w + 2 * n, nx, ny, nz, spx, spy, spz, alpha, beta, gamma, 0);
+  {
+    const float *v0 = AD_V(0);
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+    for (long k = 0; k < n; ++k) {
+      sx += w[k] * v0[k];
+      sy += w[n + k] * v0[n + k];
+      sz += w[2 * n + k] * v0[2 * n + k];
+    }
+    if (vec_energy) *vec_energy = (double)(float)(spx * spy * spz * (double)(sx + sy + sz));
+  }
+  aw_oracle_apply(I0, p1, p1 + n, p1 + 2 * n, I, nx, ny, nz, 0.0f);
+  double e = 0.0;
+  for (long k = 0; k < n; ++k) {
+    const float r = I[k] - I1[k];
+    e += (double)r * (double)r;
+  }
+  e *= spx * spy * spz;
+
+  /* part 2: backward integration of the adjoint equations
+   * (backwardAdIntegration, .cxx:325-431) */
+  memset(aTil, 0, f1);
+  {
+    const float inv = 1.0f / (sigma * sigma);
+    for (long k = 0; k < n; ++k) IHat[k] = (I1[k] - I[k]) * inv;
+  }
+  aw_oracle_splat(IHat, p1, p1 + n, p1 + 2 * n, ITil, nx, ny, nz, 0.0f);
+  for (int i = T - 1; i >= 0; --i) {
+    if (i != T - 1) {
+      aw_oracle_identity(p0, p0 + n, p0 + 2 * n, nx, ny, nz);
+      aw_oracle_identity(p1, p1 + n, p1 + 2 * n, nx, ny, nz);
+      for (int j = 1; j <= i + 1; ++j) {
+        AD_ADVANCE_P0(AD_V(j - 1));
+        AD_ADVANCE_P1(AD_V(j - 1));
+      }
+    }
+    aw_oracle_apply(I0, p1, p1 + n, p1 + 2 * n, IT, nx, ny, nz, 0.0f);
+    aw_oracle_splat(alpha0, p0, p0 + n, p0 + 2 * n, aT, nx, ny, nz, 0.0f);
+    aw_oracle_apply(aTil, p1, p1 + n, p1 + 2 * n, aHat, nx, ny, nz, 0.0f);
+    aw_oracle_splat(ITil, p0, p0 + n, p0 + 2 * n, IHat, nx, ny, nz, 0.0f);
+    /* vhat = K(grad(aHat) * aT - grad(IT) * IHat) */
+    aw_oracle_gradient(aHat, w, w + n, w + 2 * n, nx, ny, nz, spx, spy, spz, 0);
+    aw_oracle_gradient(IT, w2, w2 + n, w2 + 2 * n, nx, ny, nz, spx, spy, spz, 0);
+    scale3(w, aT, n);
+    scale3(w2, IHat, n);
+    for (long k = 0; k < 3 * n; ++k) w[k] = w[k] - w2[k];
+    aw_oracle_fluid_apply(w, w + n, w + 2 * n, nx, ny, nz, spx, spy, spz, alpha, beta, gamma, 1);
+    /* aTilde -= (grad(IT) . vhat)(phi0T) */
+    aw_oracle_gradient(IT, w2, w2 + n, w2 + 2 * n, nx, ny, nz, spx, spy, spz, 0);
+    dot3(w2, w, s1, n);
+    aw_oracle_apply(s1, p0, p0 + n, p0 + 2 * n, s2, nx, ny, nz, 0.0f);
+    for (long k = 0; k < n; ++k) aTil[k] = aTil[k] - s2[k];
+    /* ITilde += splat(div(aT vhat), phiT0) */
+    scale3(w, aT, n);
+    divergence(w, s1, w2, nx, ny, nz, spx, spy, spz);
+    aw_oracle_splat(s1, p1, p1 + n, p1 + 2 * n, s2, nx, ny, nz, 0.0f);
+    for (long k = 0; k < n; ++k) ITil[k] = ITil[k] + s2[k];
+  }
+  /* alpha0 -= step * (-(grad(I0) . v0) - aTilde) */
+  aw_oracle_gradient(I0, w, w + n, w + 2 * n, nx, ny, nz, spx, spy, spz, 0);
+  dot3(w, AD_V(0), s1, n);
+  for (long k = 0; k < n; ++k) {
+    float g = s1[k] * -1.0f;
+    g = g - aTil[k];
+    g = g * step;
+    alpha0[k] = alpha0[k] - g;
+  }
+#undef AD_V
+#undef AD_ADVANCE_P0
+#undef AD_ADVANCE_P1
+#undef AD_VELOCITY
+  free(o);
+  free(w);
+  free(w2);
+  free(aT);
+  free(I);
+  free(IHat);
+  free(aHat);
+  free(IT);
+  free(aTil);
+  free(ITil);
+  free(s1);
+  free(s2);
+  return e;
+}
+
+/* ImageUtils::resampleNew (UtilitiesDataTypes/ImageUtils.txx:306-349) with
+ * the default BACKGROUND_STRATEGY_CLAMP / linear interpolation
+ * (Array3DUtils::trilerp, Array3DUtils.txx:63-210), origin 0: destination
+ * voxel x samples the source at ((x*dsp + (dsp - ssp)/2) / ssp). The
+ * reference keeps a floor equal to the size (a position at or beyond the
+ * last cell plus one); such a corner is clamped here as well — the
+ * multiscale upsampling never reaches it. */
+static float trilerp_clamp(const float *a, int nx, int ny, int nz, double x, double y, double z) {
+  int fx = (int)x, fy = (int)y, fz = (int)z;
+  if (x < 0 && x != (int)x) --fx;
+  if (y < 0 && y != (int)y) --fy;
+  if (z < 0 && z != (int)z) --fz;
+  int cx = fx + 1, cy = fy + 1, cz = fz + 1;
+  const double t = x - fx, u = y - fy, v = z - fz;
+  const double omt = 1.0 - t, omu = 1.0 - u, omv = 1.0 - v;
+#define AD_CLAMP(f, c, s)           \
+  do {                              \
+    if (f < 0) {                    \
+      f = 0;                        \
+      if (c < 0) c = 0;             \
+    }                               \
+    if (c >= s) {                   \
+      c = s - 1;                    \
+      if (f > s - 1) f = s - 1;     \
+    }                               \
+  } while (0)
+  AD_CLAMP(fx, cx, nx);
+  AD_CLAMP(fy, cy, ny);
+  AD_CLAMP(fz, cz, nz);
+#undef AD_CLAMP
+  const float v0 = a[IDX(fx, fy, fz)], v1 = a[IDX(cx, fy, fz)], v2 = a[IDX(cx, cy, fz)],
+              v3 = a[IDX(fx, cy, fz)], v4 = a[IDX(fx, cy, cz)], v5 = a[IDX(cx, cy, cz)],
+              v6 = a[IDX(cx, fy, cz)], v7 = a[IDX(fx, fy, cz)];
+  return (float)(omt * (omu * (v0 * omv + v7 * v) + u * (v3 * omv + v4 * v)) +
+                 t * (omu * (v1 * omv + v6 * v) + u * (v2 * omv + v5 * v)));
+}
+
+void aw_oracle_resample_image(const float *in, int nx, int ny, int nz, double ssx, double ssy,
+                              double ssz, float *out, int mx, int my, int mz, double dsx,
+                              double dsy, double dsz) {
+  const double ox = (dsx - ssx) / 2.0, oy = (dsy - ssy) / 2.0, oz = (dsz - ssz) / 2.0;
+  for (int z = 0; z < mz; ++z)
+    for (int y = 0; y < my; ++y)
+      for (int x = 0; x < mx; ++x) {
+        const double wx = dsx * x + 0.0 + ox, wy = dsy * y + 0.0 + oy, wz = dsz * z + 0.0 + oz;
+        out[((long)z * my + y) * mx + x] =
+            trilerp_clamp(in, nx, ny, nz, (wx - 0.0) / ssx, (wy - 0.0) / ssy, (wz - 0.0) / ssz);
+      }
+}
+
+/* ------------------------------------------------------------------------
  * Multiscale (Algorithms/Common/MultiscaleManager.cxx:301-366).
  * ---------------------------------------------------------------------- */
 

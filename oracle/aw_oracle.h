@@ -80,6 +80,20 @@ double aw_oracle_ldmm_shoot_iterate(const float *I0, const float *I1, float *alp
                                     double spy, double spz, double alpha, double beta,
                                     double gamma, float sigma, float step);
 
+/* LDMMAdShootingIteratorCPU::Iterate + backwardAdIntegration: alpha0
+ * updated in place; V (T x 3N) receives the shot velocities; phi0T / phiT0
+ * are left at time t_1 as the reference leaves them. Returns the image
+ * energy sp^3 sum (I0(phiT0) - I1)^2; *vec_energy = <L v0, v0>. */
+double aw_oracle_ldmm_adshoot_iterate(const float *I0, const float *I1, float *alpha0,
+                                      float *phi0T, float *phiT0, float *V, int T, int nx, int ny,
+                                      int nz, double spx, double spy, double spz, double alpha,
+                                      double beta, double gamma, float sigma, float step,
+                                      double *vec_energy);
+/* ImageUtils::resampleNew, clamp background, linear (origin 0) */
+void aw_oracle_resample_image(const float *in, int nx, int ny, int nz, double ssx, double ssy,
+                              double ssz, float *out, int mx, int my, int mz, double dsx,
+                              double dsy, double dsz);
+
 void aw_oracle_gauss_blur(const float *in, float *out, int nx, int ny, int nz, float sx, float sy,
                           float sz, int kx, int ky, int kz);
 void aw_oracle_downsample(const float *in, int nx, int ny, int nz, double spx, double spy,

@@ -25,6 +25,7 @@
 #include "GreedyParam.h"
 #include "HField3DUtils.h"
 #include "ImageUtils.h"
+#include "LDMMAdShootingIteratorCPU.h"
 #include "LDMMDeformationData.h"
 #include "LDMMEnergy.h"
 #include "LDMMIteratorCPU.h"
@@ -678,6 +679,64 @@ int awref_shoot_run(const float *i0, const float *i1, int nx, int ny, int nz, do
       energies[iter] = e ? (double)e->ImageEnergy() * sigma * sigma : 0.0;
     }
   }
+  from_im(data.Alpha0(), alpha0);
+  from_vf(data.Phi0T(), phi0T, phi0T + n, phi0T + 2 * n);
+  from_vf(data.PhiT0(), phiT0, phiT0 + n, phiT0 + 2 * n);
+  GUARD_END
+}
+
+// LDMMWarpAd<LDMMAdShootingIteratorCPU>::RunWarp (LDMM/LDMMWarp.txx:72-133
+// with LDMMWarpAd.txx:37-42): every scale level in the given order (the
+// parameter file's; the MultiscaleManager sorts them), fixed step per level,
+// then FinishWarp's final maps. energies: per iteration the raw image term
+// and <L v0, v0>.
+int awref_adshoot_run(const float *i0, const float *i1, int nx, int ny, int nz, double spx,
+                      double spy, double spz, int T, int nscales, const int *factors,
+                      const int *iters, const float *steps, float sigma, double alpha,
+                      double beta, double gamma, float *alpha0, float *phi0T, float *phiT0,
+                      double *img_energy, double *vec_energy) {
+  GUARD_BEGIN
+  std::ostringstream xml;
+  xml.precision(17);
+  xml << "<LDMMWarpParameterFile>";
+  for (int s = 0; s < nscales; ++s)
+    xml << "<LDMMScaleLevel><ScaleLevel><DownsampleFactor val=\"" << factors[s]
+        << "\"/></ScaleLevel><LDMMIterator>" << diffoper_xml(alpha, beta, gamma)
+        << "<Sigma val=\"" << sigma << "\"/><StepSize val=\"" << steps[s]
+        << "\"/><UseAdaptiveStepSize val=\"false\"/></LDMMIterator><NIterations val=\""
+        << iters[s] << "\"/></LDMMScaleLevel>";
+  xml << "<NTimeSteps val=\"" << T << "\"/><AutoStepReduce val=\"false\"/></LDMMWarpParameterFile>";
+  LDMMParam param;
+  parse_into(param, xml.str());
+  SizeType size(nx, ny, nz);
+  SpacingType sp(spx, spy, spz);
+  OriginType origin(0, 0, 0);
+  RealImage I0(size, origin, sp), I1(size, origin, sp);
+  to_im(i0, I0);
+  to_im(i1, I1);
+  MultiscaleManager scaleManager(size, sp, origin, param);
+  scaleManager.SetScaleVectorFields(false);
+  LDMMShootingDefData data(&I0, &I1, param);
+  LDMMAdShootingIteratorCPU iterator(size, origin, sp, T, true);
+  const long n = (long)nx * ny * nz;
+  data.InitializeWarp();
+  int e = 0;
+  for (unsigned level = 0; level < param.GetNumberOfScaleLevels(); ++level) {
+    scaleManager.SetScaleLevel(level);
+    const LDMMScaleLevelParam &lp = param.GetScaleLevel(level);
+    iterator.SetScaleLevel(scaleManager, lp.Iterator());
+    data.SetScaleLevel(static_cast<const MultiscaleManager &>(scaleManager));
+    data.StepSize(lp.Iterator().StepSize());
+    for (unsigned iter = 0; iter < lp.NIterations(); ++iter, ++e) {
+      data.SetCurIter(iter);
+      iterator.Iterate(data);
+      LDMMEnergy *en = dynamic_cast<LDMMEnergy *>(data.GetEnergyHistory().LastEnergy());
+      if (img_energy) img_energy[e] = en ? (double)en->ImageEnergy() * sigma * sigma : 0.0;
+      if (vec_energy) vec_energy[e] = en ? (double)en->VecStepEnergy(0) : 0.0;
+    }
+  }
+  iterator.finalUpdatePhi0T(data);
+  iterator.finalUpdatePhiT0(data);
   from_im(data.Alpha0(), alpha0);
   from_vf(data.Phi0T(), phi0T, phi0T + n, phi0T + 2 * n);
   from_vf(data.PhiT0(), phiT0, phiT0 + n, phiT0 + 2 * n);

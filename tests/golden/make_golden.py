@@ -8,7 +8,8 @@ compressed .npz files, so the parity tests can check both the oracle and
 the CUDA path against reference outputs on machines without the reference
 tree. Run from the repository root:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            (every fixture)
+    python tests/golden/make_golden.py adshoot    (the adjoint-shooting ones)
 
 Every case is deterministic (seeded numpy generators); re-running rewrites
 identical files.
@@ -20,9 +21,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+sys.path.insert(0, os.path.dirname(HERE))
 
 from atlaswerks_b200.synth import atlas_subjects, bullseye, greedy_pair  # noqa: E402
 from oracle import REF_SO, Reference, build_reference, identity  # noqa: E402
+from metaimage import read_mha, read_nhdr, rescale_intensities  # noqa: E402
 
 BG = ["partial_id", "id", "partial_zero", "zero", "clamp", "wrap"]
 
@@ -106,6 +109,34 @@ def main():
     save("atlas_16x3", imgs=np.stack(imgs), w=w, mean_p1=m1, h_p1=np.stack(h1), energies_p1=e1,
          mean_p2=m2, h_p2=np.stack(h2), energies_p2=e2)
 
+    adshoot_cases(ref)
+
+
+def adshoot_cases(ref):
+    """LDMM adjoint shooting: a small single-scale run, and the reference's
+    own regression (Testing/Applications/LDMM/LDMMAdShootingWarp: the
+    bullseye pair rescaled to [0, 1], scale factors 2 then 1 with 100
+    iterations each at steps 0.0005 / 0.0002, T = 5, sigma 1, alpha = beta =
+    0.01, gamma = 0.001) with its Baseline deformed image."""
+    I0, I1 = small_pair((12, 14, 16), 11)
+    sp = (1.5, 0.75, 1.25)
+    a0, p0, p1, ei, ev = ref.adshoot_run(I0, I1, 4, [(1, 5, 0.0002)], sp, sigma=1.0)
+    save("adshoot_16x14x12_T4", I0=I0, I1=I1, sp=np.array(sp), alpha0=a0, phi0T=p0, phiT0=p1,
+         img_energy=ei, vec_energy=ev)
+    root = "/root/reference/Testing"
+    B0, bsp = read_nhdr(f"{root}/Data/Input/Bullseyes/BullseyeTestBlur00.nhdr")
+    B1, _ = read_nhdr(f"{root}/Data/Input/Bullseyes/BullseyeTestBlur01.nhdr")
+    base, _ = read_mha(f"{root}/Applications/LDMM/LDMMAdShootingWarp/Baseline/"
+                       "LDMMAdShootingWarpBullseyeTestBlur00_to_BullseyeTestBlur01DefImage.mha")
+    B0, B1 = rescale_intensities(B0), rescale_intensities(B1)
+    levels = [(1, 100, 0.0002), (2, 100, 0.0005)]
+    a0, _, p1, ei, ev = ref.adshoot_run(B0, B1, 5, levels, bsp, sigma=1.0)
+    save("adshoot_bullseye", I0=B0, I1=B1, sp=np.array(bsp), baseline_def_image=base,
+         alpha0=a0, phiT0=p1, img_energy=ei, vec_energy=ev)
+
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["adshoot"]:
+        adshoot_cases(Reference())
+    else:
+        main()

@@ -41,3 +41,12 @@ def read_nhdr(path):
     raw = os.path.join(os.path.dirname(path), hdr["data file"])
     arr = np.fromfile(raw, dtype="<f4").reshape(dims[2], dims[1], dims[0])
     return arr.astype(np.float32), sp
+
+
+def rescale_intensities(a):
+    """The ImagePreprocessor's intensity window to [0, 1]
+    (Array3DUtils::rescaleElements): (a - min) * (1 / (max - min)), the
+    difference in float, the product in double."""
+    mn, mx = float(a.min()), float(a.max())
+    scale = (1.0 - 0.0) / (mx - mn)
+    return ((a - np.float32(mn)).astype(np.float64) * scale).astype(np.float32)

@@ -124,3 +124,63 @@ def test_atlas(oracle, period):
 def test_identity_helper():
     h = identity((2, 3, 4))
     assert h.shape == (3, 2, 3, 4) and h[0, 1, 2, 3] == 3 and h[1, 1, 2, 3] == 2 and h[2, 1, 2, 3] == 1
+
+
+def test_adshoot_single_scale(oracle):
+    """LDMM adjoint shooting, 5 iterations at 12x14x16, T = 4, anisotropic
+    spacing: the oracle's Iterate and final maps against the reference's
+    LDMMAdShootingIteratorCPU through the LDMMWarpAd loop."""
+    g = load("adshoot_16x14x12_T4")
+    sp = tuple(g["sp"])
+    a = np.zeros(g["I0"].shape, np.float32)
+    ei, ev = [], []
+    for _ in range(5):
+        e, v, V, _, _ = oracle.ldmm_adshoot_iterate(g["I0"], g["I1"], a, 4, sp, sigma=1.0,
+                                                    step=0.0002)
+        ei.append(e)
+        ev.append(v)
+    p0, p1 = oracle.adshoot_final_maps(V, sp)
+    assert np.abs(a - g["alpha0"]).max() <= 1e-5 * np.abs(g["alpha0"]).max()
+    assert np.abs(p0 - g["phi0T"]).max() <= 1e-4
+    assert np.abs(p1 - g["phiT0"]).max() <= 1e-4
+    assert np.allclose(ei, g["img_energy"], rtol=1e-5)
+    assert np.allclose(ev, g["vec_energy"], rtol=1e-5, atol=1e-9)
+    assert ei[-1] < 0.5 * ei[0]
+
+
+def test_adshoot_bullseye_fixture_is_the_reference_regression(oracle):
+    """The fixture's reference-build result reproduces the reference's own
+    regression baseline (LDMMAdShootingWarp Baseline DefImage) by the
+    regression's criterion, L1 sum below 1.0 (AtlasWerksTestUtils.py:
+    122-168)."""
+    g = load("adshoot_bullseye")
+    err = float(np.abs(oracle.apply(g["I0"], g["phiT0"]) - g["baseline_def_image"]).sum())
+    assert err < 1.0, err
+    assert err < 0.02, err  # measured 0.0040
+
+
+def test_resample_image_is_clamped_trilinear(oracle):
+    """resampleNew of a linear ramp onto a grid twice as fine reproduces the
+    ramp inside and clamps to the edge values outside."""
+    src = np.fromfunction(lambda z, y, x: x + 2 * y + 3 * z, (5, 6, 7), dtype=np.float32)
+    out = oracle.resample_image(src, (10, 12, 14), (2.0, 2.0, 2.0), (1.0, 1.0, 1.0))
+    z, y, x = np.meshgrid(*[np.clip(np.arange(n) / 2.0 - 0.25, 0, m - 1)
+                            for n, m in ((10, 5), (12, 6), (14, 7))], indexing="ij")
+    assert np.abs(out - (x + 2 * y + 3 * z)).max() < 1e-5
+
+
+def test_adshoot_bullseye_regression(oracle):
+    """The oracle's LDMMWarpAd loop on the reference's regression pair
+    (factors 2 then 1, 100 iterations each, T = 5): the deformed image
+    against the reference's Baseline by the regression's criterion, alpha0
+    against the reference build's (about a minute on one core)."""
+    g = load("adshoot_bullseye")
+    sp = tuple(float(s) for s in g["sp"])
+    a, _, p1, hist = oracle.adshoot_warp(g["I0"], g["I1"], 5, [(1, 100, 0.0002), (2, 100, 0.0005)],
+                                         sp, sigma=1.0)
+    err = float(np.abs(oracle.apply(g["I0"], p1) - g["baseline_def_image"]).sum())
+    assert err < 1.0, err
+    assert err < 0.02, err  # measured 0.0041
+    assert np.abs(a - g["alpha0"]).max() <= 1e-5 * np.abs(g["alpha0"]).max()
+    # the reference keeps the image energy as a float: 3e-5 relative
+    assert np.allclose(np.concatenate([h[0] for h in hist]), g["img_energy"], rtol=3e-5)

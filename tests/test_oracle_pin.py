@@ -156,3 +156,44 @@ def test_ldmm_shooting_matches_reference(oracle, reference, sp):
     assert np.abs(p1 - p1_r).max() <= 1e-4
     assert np.allclose(e_o, e_r, rtol=1e-5)
     assert e_r[-1] < e_r[0]  # the shooting lowers the mismatch
+
+
+@pytest.mark.parametrize("sp", [(1.0, 1.0, 1.0), (1.5, 0.75, 1.25)])
+def test_ldmm_adjoint_shooting_matches_reference(oracle, reference, sp):
+    """Adjoint geodesic shooting, four iterations from alpha0 = 0: the
+    restatement of Iterate + backwardAdIntegration and of the final maps
+    against LDMMAdShootingIteratorCPU."""
+    shape, T, iters = (12, 14, 16), 4, 4
+    I0, I1 = greedy_pair(shape, 7, n_blobs=4, umax=1.5, sigma_range=(1.5, 3.0), smooth_sigma=3.0)
+    a_r, p0_r, p1_r, ei_r, ev_r = reference.adshoot_run(I0, I1, T, [(1, iters, 0.0005)], sp,
+                                                        sigma=1.0)
+    a = np.zeros(shape, np.float32)
+    ei, ev = [], []
+    for _ in range(iters):
+        e, v, V, _, _ = oracle.ldmm_adshoot_iterate(I0, I1, a, T, sp, sigma=1.0, step=0.0005)
+        ei.append(e)
+        ev.append(v)
+    p0, p1 = oracle.adshoot_final_maps(V, sp)
+    # the oracle's FP64 fluid solve vs the reference's FP32 one
+    assert np.abs(a - a_r).max() <= 1e-5 * np.abs(a_r).max()
+    assert np.abs(p0 - p0_r).max() <= 1e-4
+    assert np.abs(p1 - p1_r).max() <= 1e-4
+    assert np.allclose(ei, ei_r, rtol=1e-5)
+    assert np.allclose(ev, ev_r, rtol=1e-5, atol=1e-9)
+    assert ei_r[-1] < ei_r[0]
+
+
+def test_ldmm_adjoint_shooting_two_scales_matches_reference(oracle, reference):
+    """The LDMMWarpAd scale loop at 20x18x24, factors 2 then 1: downsampled
+    images, alpha0 resampled by resampleNew at the scale change."""
+    shape = (24, 18, 20)
+    sp = (1.0, 1.25, 0.8)
+    I0, I1 = greedy_pair(shape, 12, n_blobs=6, umax=1.5, sigma_range=(2.0, 3.0), smooth_sigma=3.0)
+    levels = [(1, 3, 0.0002), (2, 4, 0.0005)]
+    a_r, p0_r, p1_r, ei_r, ev_r = reference.adshoot_run(I0, I1, 3, levels, sp, sigma=1.0)
+    a, p0, p1, hist = oracle.adshoot_warp(I0, I1, 3, levels, sp, sigma=1.0)
+    assert np.abs(a - a_r).max() <= 1e-5 * np.abs(a_r).max()
+    assert np.abs(p0 - p0_r).max() <= 1e-4
+    assert np.abs(p1 - p1_r).max() <= 1e-4
+    ei = np.concatenate([h[0] for h in hist])
+    assert np.allclose(ei, ei_r, rtol=1e-5)

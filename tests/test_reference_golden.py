@@ -12,17 +12,13 @@ import os
 import numpy as np
 import pytest
 
-from metaimage import read_mha, read_nhdr
+from metaimage import read_mha, read_nhdr, rescale_intensities
 
 REF = "/root/reference/Testing"
 pytestmark = pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
 
 
-def _rescale(a):
-    """ImagePreprocessor intensity window to [0, 1] (Array3DUtils::rescaleElements)."""
-    mn, mx = float(a.min()), float(a.max())
-    scale = (1.0 - 0.0) / (mx - mn)
-    return ((a - np.float32(mn)).astype(np.float64) * scale).astype(np.float32)
+_rescale = rescale_intensities
 
 
 def _inputs():
