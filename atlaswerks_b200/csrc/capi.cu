@@ -782,6 +782,9 @@ int aw_ldmm_adshoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float
                             float *phi0T, float *phiT0, void *stream) {
   if (!l || !I0 || !I1 || !alpha0 || !phi0T || !phiT0)
     return fail("aw_ldmm_adshoot_iterate: null pointer");
+  if (l->ctx.T + 1 > aw::kMaxAdSorts)
+    return fail("aw_ldmm_adshoot_iterate: at most " + std::to_string(aw::kMaxAdSorts - 1) +
+                " time steps");
   if (aw::ldmm_adshoot_prepare(&l->ctx))
     return fail("aw_ldmm_adshoot_iterate: device allocation failed");
   AW_CUDA(aw::ldmm_adshoot_iterate(&l->ctx, I0, I1, alpha0, phi0T, phiT0, S(stream)),

@@ -398,7 +398,7 @@ void ldmm_destroy(LdmmCtx *c) {
   fluid_plan_destroy(&c->plan);
   void *ptrs[] = {c->J0,     c->hbuf,   c->diff, c->S,   c->u,   c->splat_scratch,
                   c->partials, c->energy, c->scalars, c->JT, c->JD, c->adV,
-                  c->adP,    c->adA,    c->adI,  c->venergy};
+                  c->adP,    c->adA,    c->adI,  c->venergy, c->adSortMem};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   std::memset(c, 0, sizeof(*c));
@@ -628,19 +628,25 @@ cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, flo
 int ldmm_adshoot_prepare(LdmmCtx *c) {
   if (c->adV) return 0;
   const size_t n = (size_t)c->d.n(), T = (size_t)c->T;
+  const size_t sort_bytes = (splat_scratch_bytes(c->d) + 255) & ~size_t(255);
+  if (c->T + 1 > kMaxAdSorts) return 3;
   if (cudaMalloc(&c->adV, sizeof(float) * T * 3 * n) != cudaSuccess ||
       cudaMalloc(&c->adP, sizeof(float) * 2 * (T + 1) * 3 * n) != cudaSuccess ||
       cudaMalloc(&c->adA, sizeof(float) * T * n) != cudaSuccess ||
       cudaMalloc(&c->adI, sizeof(float) * 6 * n) != cudaSuccess ||
-      cudaMalloc(&c->venergy, sizeof(double) * c->cap) != cudaSuccess) {
+      cudaMalloc(&c->venergy, sizeof(double) * c->cap) != cudaSuccess ||
+      cudaMalloc(&c->adSortMem, sort_bytes * (T + 1)) != cudaSuccess) {
     cudaGetLastError();
-    void *ptrs[] = {c->adV, c->adP, c->adA, c->adI, c->venergy};
+    void *ptrs[] = {c->adV, c->adP, c->adA, c->adI, c->venergy, c->adSortMem};
     for (void *p : ptrs)
       if (p) cudaFree(p);
     c->adV = c->adP = c->adA = c->adI = nullptr;
     c->venergy = nullptr;
+    c->adSortMem = nullptr;
     return 3;
   }
+  for (size_t k = 0; k <= T; ++k)
+    splat_work_bind(&c->adSort[k], c->d, static_cast<char *>(c->adSortMem) + k * sort_bytes);
   // entries of iterations of the other kinds read as 0
   return cudaMemset(c->venergy, 0, sizeof(double) * c->cap) == cudaSuccess ? 0 : 3;
 }
@@ -668,7 +674,9 @@ int ldmm_adshoot_prepare(LdmmCtx *c) {
 // backward step (O(T^2) compositions) and recomputes I_t and alpha_t; the
 // same operations in the same order produce the same values, so here the
 // shooting keeps every map, I_t and alpha_t resident in HBM and the
-// backward sweep reads them back.
+// backward sweep reads them back. The bucket sort of each phi0T_t (and of
+// phiT0_T) is kept too: the backward sweep splats by those maps again and
+// needs only the ordered sums.
 cudaError_t ldmm_adshoot_iterate(LdmmCtx *c, const float *I0, const float *I1, float *alpha0,
                                  float *phi0T, float *phiT0, cudaStream_t s) {
   if (!c->adV) return cudaErrorNotReady;
@@ -696,7 +704,8 @@ cudaError_t ldmm_adshoot_iterate(LdmmCtx *c, const float *I0, const float *I1, f
     const float *hh[3] = {comp(P0(t - 1), 0), comp(P0(t - 1), 1), comp(P0(t - 1), 2)};
     float *oo[3] = {comp(P0(t), 0), comp(P0(t), 1), comp(P0(t), 2)};
     AW_TRY(launch_compose_vh(vv, hh, oo, d, c->sp, 1, BG_PARTIAL_ZERO, nullptr, 1.0f, s));
-    AW_TRY(splat(c->sw, alpha0, oo[0], oo[1], oo[2], A(t), 0.0f, s));
+    AW_TRY(splat_sort(c->adSort[t], oo[0], oo[1], oo[2], s));
+    AW_TRY(splat_gather(c->adSort[t], alpha0, oo[0], oo[1], oo[2], A(t), 0.0f, s));
     k_forward_step<false><<<grid, kRowThreads, 0, s>>>(
         comp(P1(t - 1), 0), comp(P1(t - 1), 1), comp(P1(t - 1), 2), vv[0], vv[1], vv[2],
         comp(P1(t), 0), comp(P1(t), 1), comp(P1(t), 2), I0, I(t), d, c->sp);
@@ -733,7 +742,9 @@ cudaError_t ldmm_adshoot_iterate(LdmmCtx *c, const float *I0, const float *I1, f
   AW_TRY(cudaGetLastError());
 
   // backward integration of the adjoint equations
-  AW_TRY(splat(c->sw, IHat, comp(P1(T), 0), comp(P1(T), 1), comp(P1(T), 2), ITil, 0.0f, s));
+  AW_TRY(splat_sort(c->adSort[0], comp(P1(T), 0), comp(P1(T), 1), comp(P1(T), 2), s));
+  AW_TRY(splat_gather(c->adSort[0], IHat, comp(P1(T), 0), comp(P1(T), 1), comp(P1(T), 2), ITil,
+                      0.0f, s));
   AW_TRY(cudaMemsetAsync(aTil, 0, sizeof(float) * n, s));
   for (int i = T - 1; i >= 0; --i) {
     const int t = i + 1;
@@ -741,7 +752,7 @@ cudaError_t ldmm_adshoot_iterate(LdmmCtx *c, const float *I0, const float *I1, f
     float *p1[3] = {comp(P1(t), 0), comp(P1(t), 1), comp(P1(t), 2)};
     k_ad_pull<false><<<grid, kRowThreads, 0, s>>>(aTil, p1[0], p1[1], p1[2], aHat, d);
     AW_TRY(cudaGetLastError());
-    AW_TRY(splat(c->sw, ITil, p0[0], p0[1], p0[2], IHat, 0.0f, s));
+    AW_TRY(splat_gather(c->adSort[t], ITil, p0[0], p0[1], p0[2], IHat, 0.0f, s));
     k_ad_force<<<grid, kRowThreads, 0, s>>>(aHat, A(t), I(t), IHat, comp(c->u, 0), comp(c->u, 1),
                                             comp(c->u, 2), d, g);
     AW_TRY(cudaGetLastError());
@@ -753,7 +764,10 @@ cudaError_t ldmm_adshoot_iterate(LdmmCtx *c, const float *I0, const float *I1, f
     AW_TRY(cudaGetLastError());
     k_ad_pull<true><<<grid, kRowThreads, 0, s>>>(s1, p0[0], p0[1], p0[2], aTil, d);
     AW_TRY(cudaGetLastError());
-    AW_TRY(splat(c->sw, s2, p1[0], p1[1], p1[2], s1, 0.0f, s));
+    if (t == T)
+      AW_TRY(splat_gather(c->adSort[0], s2, p1[0], p1[1], p1[2], s1, 0.0f, s));
+    else
+      AW_TRY(splat(c->sw, s2, p1[0], p1[1], p1[2], s1, 0.0f, s));
     k_ad_add<<<flat, 256, 0, s>>>(ITil, s1, n);
     AW_TRY(cudaGetLastError());
   }

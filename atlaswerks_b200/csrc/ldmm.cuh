@@ -6,6 +6,9 @@
 
 namespace aw {
 
+// time steps whose splat sorts the adjoint shooting keeps (T + 1 sets)
+constexpr int kMaxAdSorts = 65;
+
 struct LdmmCtx {
   FluidPlan plan;
   Dims d;
@@ -37,6 +40,8 @@ struct LdmmCtx {
   float *adA;       // T x N: alpha_t = splat(alpha0, phi0T_t), t = 1 .. T
   float *adI;       // 6N: alphaHat, IHat, alphaTilde, ITilde and two scratch images
   double *venergy;  // <L v0, v0> history ring, indexed like energy
+  void *adSortMem;  // T + 1 splat scratch sets
+  SplatWork adSort[kMaxAdSorts];  // the sorts by phi0T_t (t = 1..T) and by phiT0_T (slot 0)
 };
 
 int ldmm_create(LdmmCtx *c, int nx, int ny, int nz, double spx, double spy, double spz,

@@ -184,9 +184,18 @@ AW_D float corner_weight(float px, float py, float pz, int cx, int cy, int cz) {
 
 // every destination merges its eight candidate buckets in source order (the
 // order forwardApply adds them). Buckets (dx = 1, dx = 0) of one (dy, dz) are
-// adjacent: three offsets bound both. (Fetching all candidates up front and
-// merging them in registers measured slower: the 16-way selection costs
-// more issue slots than the dependent loads it saves.)
+// adjacent: three offsets bound both.
+//
+// Fast path: the bucket of corner (dx, dy, dz) is the cell v - (dx, dy, dz),
+// so its sources usually precede those of every corner with a smaller
+// dx + 2 dy + 4 dz. The four (dy, dz) ranges are walked in that order
+// (dz = 1 first, then dy = 1; dx = 1 before dx = 0 inside each); when every
+// source index exceeds the one before it, this walk is the merged order and
+// the sum is complete. A source out of order (a folding or strongly
+// compressing map) sends the destination to the general eight-way merge,
+// which starts the sum again. (Fetching all candidates up front and merging
+// them in registers measured slower: the 16-way selection costs more issue
+// slots than the dependent loads it saves.)
 __global__ void __launch_bounds__(kRowThreads)
     k_gather(const float *__restrict__ img, const float *__restrict__ hx,
              const float *__restrict__ hy, const float *__restrict__ hz, Dims d,
@@ -208,9 +217,30 @@ __global__ void __launch_bounds__(kRowThreads)
     pos[2 * r] = o1;
     end[2 * r] = o2;
   }
+  float acc = bg;
+  int prev = -1;
+  bool ordered = true;
+#pragma unroll
+  for (int r = 3; r >= 0; --r) {
+    const int dy = r & 1, dz = r >> 1;
+    for (int p = pos[2 * r + 1]; ordered && p < end[2 * r]; ++p) {
+      const int m = __ldg(order + p);
+      if (m <= prev) {
+        ordered = false;
+        break;
+      }
+      prev = m;
+      const float w = corner_weight(hx[m], hy[m], hz[m], p < end[2 * r + 1] ? 1 : 0, dy, dz);
+      acc = fadd(acc, fmul(w, img[m]));
+    }
+  }
+  if (ordered) {
+    out[v.i] = acc;
+    return;
+  }
 #pragma unroll
   for (int k = 0; k < 8; ++k) cur[k] = pos[k] < end[k] ? order[pos[k]] : INT_MAX;
-  float acc = bg;
+  acc = bg;
   while (true) {
     int m = INT_MAX, sel = -1;
 #pragma unroll
@@ -257,8 +287,8 @@ void splat_work_bind(SplatWork *w, const Dims &d, void *scratch) {
   w->blocksums = reinterpret_cast<int *>(p);
 }
 
-cudaError_t splat(const SplatWork &w, const float *img, const float *hx, const float *hy,
-                  const float *hz, float *out, float bg, cudaStream_t s) {
+cudaError_t splat_sort(const SplatWork &w, const float *hx, const float *hy, const float *hz,
+                       cudaStream_t s) {
   const Dims d = w.d;
   cudaError_t e;
   if ((e = cudaMemsetAsync(w.offsets, 0, sizeof(int) * (w.next + 1), s)) != cudaSuccess) return e;
@@ -269,8 +299,20 @@ cudaError_t splat(const SplatWork &w, const float *img, const float *hx, const f
   k_scan_apply<<<w.nblocks, kScanThreads, 0, s>>>(w.offsets, w.next, w.blocksums);
   k_scatter<<<row_grid(d), kRowThreads, 0, s>>>(hx, hy, hz, d, w.offsets, w.cursor, w.order);
   k_bucket_sort<<<(int)((w.next + 255) / 256), 256, 0, s>>>(w.offsets, w.order, w.next);
+  return cudaGetLastError();
+}
+
+cudaError_t splat_gather(const SplatWork &w, const float *img, const float *hx, const float *hy,
+                         const float *hz, float *out, float bg, cudaStream_t s) {
+  const Dims d = w.d;
   k_gather<<<row_grid(d), kRowThreads, 0, s>>>(img, hx, hy, hz, d, w.offsets, w.order, out, bg);
   return cudaGetLastError();
+}
+
+cudaError_t splat(const SplatWork &w, const float *img, const float *hx, const float *hy,
+                  const float *hz, float *out, float bg, cudaStream_t s) {
+  const cudaError_t e = splat_sort(w, hx, hy, hz, s);
+  return e != cudaSuccess ? e : splat_gather(w, img, hx, hy, hz, out, bg, s);
 }
 
 }  // namespace aw

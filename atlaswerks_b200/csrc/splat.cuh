@@ -37,5 +37,12 @@ void splat_work_bind(SplatWork *w, const Dims &d, void *scratch);
 // out = splat of img by h (three planes), background bg; stream-ordered
 cudaError_t splat(const SplatWork &w, const float *img, const float *hx, const float *hy,
                   const float *hz, float *out, float bg, cudaStream_t s);
+// the two halves of splat(): the bucket sort of the sources by h, kept in w,
+// and the ordered per-destination sums of img, which any number of images
+// splatted by the same h can share
+cudaError_t splat_sort(const SplatWork &w, const float *hx, const float *hy, const float *hz,
+                       cudaStream_t s);
+cudaError_t splat_gather(const SplatWork &w, const float *img, const float *hx, const float *hy,
+                         const float *hz, float *out, float bg, cudaStream_t s);
 
 }  // namespace aw

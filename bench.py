@@ -413,7 +413,8 @@ def run_ncu_case(args):
     """A short, untimed workload for ncu captures: one 128^3 pair, a step
     update, then `--steps` iterations through the graph path (with
     --workload ldmm: `--steps` LDMM IterateNew iterations at 128^3, T = 10,
-    sigma 1, step 0.01)."""
+    sigma 1, step 0.01; with --workload adshoot: `--steps` adjoint shooting
+    iterations at 128^3, T = 5, sigma 1, step 0.0002)."""
     import torch
     if args.workload == "ldmm":
         from atlaswerks_b200.ldmm import ldmm_register
@@ -423,6 +424,21 @@ def run_ncu_case(args):
                       sigma=1.0, step=0.01)
         torch.cuda.synchronize()
         print(json.dumps({"ncu_case": "ldmm 128^3 T=10", "iterations": args.steps}))
+        return 0
+    if args.workload == "adshoot":
+        from atlaswerks_b200.greedy import DiffOperParam
+        from atlaswerks_b200.ldmm import LDMMIteratorParam
+        from atlaswerks_b200.shooting import LDMMAdShootingIteratorB200, LDMMShootingDefDataB200
+        from atlaswerks_b200.synth import greedy_pair
+        I0, I1 = greedy_pair((N, N, N), 7, 8, 3.0)
+        it = LDMMAdShootingIteratorB200((N, N, N), n_time_steps=5)
+        it.SetScaleLevel((N, N, N), (1.0, 1.0, 1.0),
+                         LDMMIteratorParam(DiffOperParam(ALPHA, BETA, GAMMA), 1.0, 0.0002, False))
+        data = LDMMShootingDefDataB200(torch.from_numpy(I0).cuda(), torch.from_numpy(I1).cuda())
+        for _ in range(args.steps):
+            it.Iterate(data)
+        torch.cuda.synchronize()
+        print(json.dumps({"ncu_case": "adshoot 128^3 T=5", "iterations": args.steps}))
         return 0
 
     from atlaswerks_b200.greedy import (DiffOperParam, GreedyDeformationDataB200,
@@ -557,6 +573,45 @@ def run_ldmm(args):
     return 0
 
 
+def run_adshoot(args):
+    """LDMM adjoint geodesic shooting (LDMMAdShootingIterator) at 128^3 with
+    T = 5 time steps, sigma 1, fixed step 0.0002 (the fine level of the
+    reference's LDMMAdShootingWarp regression); a step = one iteration
+    (shooting, backward adjoint sweep, alpha0 update)."""
+    import torch
+
+    from atlaswerks_b200.greedy import DiffOperParam
+    from atlaswerks_b200.ldmm import LDMMIteratorParam
+    from atlaswerks_b200.shooting import LDMMAdShootingIteratorB200, LDMMShootingDefDataB200
+    from atlaswerks_b200.synth import greedy_pair
+    T = 5
+    I0, I1 = greedy_pair((N, N, N), 7, 8, 3.0)
+    it = LDMMAdShootingIteratorB200((N, N, N), n_time_steps=T)
+    it.SetScaleLevel((N, N, N), (1.0, 1.0, 1.0),
+                     LDMMIteratorParam(DiffOperParam(ALPHA, BETA, GAMMA), 1.0, 0.0002, False))
+    data = LDMMShootingDefDataB200(torch.from_numpy(I0).cuda(), torch.from_numpy(I1).cuda())
+    stream = torch.cuda.current_stream()
+    ms, clocks = _timed(lambda: it.Iterate(data), args.steps, args.warmup, stream)
+    value = args.steps / (ms / 1000.0)
+    peak, kind = peaks()
+    # per voxel: T x (advance 100 + velocity 20 + 4S) + T x backward step (176 + 4S)
+    # + energies, the first adjoint splat, the alpha0 update and the map copies (160 + 4S)
+    b_iter = (T * (296 + 8 * SPEC) + 160 + 4 * SPEC) * N ** 3
+    gbs = b_iter * value / 1e9
+    print(json.dumps({
+        "metric": "128^3 adjoint shooting iterations/s (T=5)", "value": value, "unit": "iters/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded blobs + smooth warp)",
+        "config": {"workload": "LDMM adjoint shooting (LDMMAdShootingIterator), 128^3, 5 time "
+                   "steps, sigma 1, step 0.0002", "grid": [N, N, N], "time_steps": T},
+        "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                     "frac": gbs / peak, "traffic": None,
+                     "algorithmic_bytes_per_iteration": b_iter},
+        "clocks": clocks}))
+    return 0
+
+
 def run_ldmm_atlas(args):
     """LDMM relaxation atlas: 4 subjects at 128^3, T = 5 time steps,
     IterateNew, sigma 1, fixed step 0.01, JacobianScale mean after every
@@ -655,7 +710,7 @@ def main():
     ap.add_argument("--ncu-case", action="store_true",
                     help="run a short untimed 128^3 workload for ncu captures")
     ap.add_argument("--workload", default="greedy",
-                    choices=["greedy", "atlas", "ldmm", "ldmm_atlas", "warmstart"],
+                    choices=["greedy", "atlas", "ldmm", "ldmm_atlas", "warmstart", "adshoot"],
                     help="the headline greedy line (default) or another hot-path row")
     ap.add_argument("--grid", type=int, default=0, help="warmstart: pair grid (64 or 128; default 128)")
     ap.add_argument("--pairs", type=int, default=32, help="warmstart: held-out pairs")
@@ -666,7 +721,7 @@ def main():
         import torch
         torch.cuda.set_device(0)
         return {"atlas": run_atlas, "ldmm": run_ldmm, "ldmm_atlas": run_ldmm_atlas,
-                "warmstart": run_warmstart}[args.workload](args)
+                "warmstart": run_warmstart, "adshoot": run_adshoot}[args.workload](args)
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)
