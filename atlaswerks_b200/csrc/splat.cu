@@ -182,6 +182,25 @@ AW_D float corner_weight(float px, float py, float pz, int cx, int cy, int cz) {
   return __double2float_rn(dmul(dmul(ax, ay), az));
 }
 
+// the eight corner weights (index dx + 2 dy + 4 dz) of the source at every
+// sorted position, once per sort: the gathers of every image splatted by
+// the same h read them instead of the source's h and the weight arithmetic
+__global__ void __launch_bounds__(256)
+    k_weights(const float *__restrict__ hx, const float *__restrict__ hy,
+              const float *__restrict__ hz, const int *__restrict__ order,
+              const int *__restrict__ total, long n, float *__restrict__ wts) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n || p >= (long)__ldg(total)) return;
+  const int m = __ldg(order + p);
+  const float px = __ldg(hx + m), py = __ldg(hy + m), pz = __ldg(hz + m);
+  float w[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) w[k] = corner_weight(px, py, pz, k & 1, (k >> 1) & 1, (k >> 2) & 1);
+  float4 *o = reinterpret_cast<float4 *>(wts + p * 8);
+  o[0] = make_float4(w[0], w[1], w[2], w[3]);
+  o[1] = make_float4(w[4], w[5], w[6], w[7]);
+}
+
 // every destination merges its eight candidate buckets in source order (the
 // order forwardApply adds them). Buckets (dx = 1, dx = 0) of one (dy, dz) are
 // adjacent: three offsets bound both.
@@ -196,11 +215,12 @@ AW_D float corner_weight(float px, float py, float pz, int cx, int cy, int cz) {
 // which starts the sum again. (Fetching all candidates up front and merging
 // them in registers measured slower: the 16-way selection costs more issue
 // slots than the dependent loads it saves.)
+template <bool PRE>
 __global__ void __launch_bounds__(kRowThreads)
     k_gather(const float *__restrict__ img, const float *__restrict__ hx,
              const float *__restrict__ hy, const float *__restrict__ hz, Dims d,
              const int *__restrict__ offsets, const int *__restrict__ order,
-             float *__restrict__ out, float bg) {
+             const float *__restrict__ wts, float *__restrict__ out, float bg) {
   Voxel v;
   if (!voxel_of(d, v)) return;
   int pos[8], end[8], cur[8];
@@ -230,7 +250,9 @@ __global__ void __launch_bounds__(kRowThreads)
         break;
       }
       prev = m;
-      const float w = corner_weight(hx[m], hy[m], hz[m], p < end[2 * r + 1] ? 1 : 0, dy, dz);
+      const int dx = p < end[2 * r + 1] ? 1 : 0;
+      const float w = PRE ? __ldg(wts + (long)p * 8 + (dx + 2 * dy + 4 * dz))
+                          : corner_weight(hx[m], hy[m], hz[m], dx, dy, dz);
       acc = fadd(acc, fmul(w, img[m]));
     }
   }
@@ -250,8 +272,13 @@ __global__ void __launch_bounds__(kRowThreads)
         sel = k;
       }
     if (sel < 0) break;
-    const float px = hx[m], py = hy[m], pz = hz[m];
-    const float w = corner_weight(px, py, pz, sel & 1, (sel >> 1) & 1, (sel >> 2) & 1);
+    int at = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (k == sel) at = pos[k];
+    const float w = PRE ? __ldg(wts + (long)at * 8 + sel)
+                        : corner_weight(hx[m], hy[m], hz[m], sel & 1, (sel >> 1) & 1,
+                                        (sel >> 2) & 1);
     acc = fadd(acc, fmul(w, img[m]));
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
@@ -266,14 +293,15 @@ __global__ void __launch_bounds__(kRowThreads)
 
 }  // namespace
 
-size_t splat_scratch_bytes(const Dims &d) {
+size_t splat_scratch_bytes(const Dims &d, bool weights) {
   const long next = (long)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
   const long nb = (next + kScanBlock - 1) / kScanBlock;
   return align256(sizeof(int) * (next + 1)) + align256(sizeof(int) * next) +
-         align256(sizeof(int) * d.n()) + align256(sizeof(int) * nb);
+         align256(sizeof(int) * d.n()) + align256(sizeof(int) * nb) +
+         (weights ? align256(sizeof(float) * 8 * d.n()) : 0);
 }
 
-void splat_work_bind(SplatWork *w, const Dims &d, void *scratch) {
+void splat_work_bind(SplatWork *w, const Dims &d, void *scratch, bool weights) {
   char *p = static_cast<char *>(scratch);
   w->d = d;
   w->next = (long)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
@@ -285,6 +313,8 @@ void splat_work_bind(SplatWork *w, const Dims &d, void *scratch) {
   w->order = reinterpret_cast<int *>(p);
   p += align256(sizeof(int) * d.n());
   w->blocksums = reinterpret_cast<int *>(p);
+  p += align256(sizeof(int) * w->nblocks);
+  w->wts = weights ? reinterpret_cast<float *>(p) : nullptr;
 }
 
 cudaError_t splat_sort(const SplatWork &w, const float *hx, const float *hy, const float *hz,
@@ -299,13 +329,21 @@ cudaError_t splat_sort(const SplatWork &w, const float *hx, const float *hy, con
   k_scan_apply<<<w.nblocks, kScanThreads, 0, s>>>(w.offsets, w.next, w.blocksums);
   k_scatter<<<row_grid(d), kRowThreads, 0, s>>>(hx, hy, hz, d, w.offsets, w.cursor, w.order);
   k_bucket_sort<<<(int)((w.next + 255) / 256), 256, 0, s>>>(w.offsets, w.order, w.next);
+  if (w.wts)
+    k_weights<<<(unsigned)((d.n() + 255) / 256), 256, 0, s>>>(hx, hy, hz, w.order,
+                                                              w.offsets + w.next, d.n(), w.wts);
   return cudaGetLastError();
 }
 
 cudaError_t splat_gather(const SplatWork &w, const float *img, const float *hx, const float *hy,
                          const float *hz, float *out, float bg, cudaStream_t s) {
   const Dims d = w.d;
-  k_gather<<<row_grid(d), kRowThreads, 0, s>>>(img, hx, hy, hz, d, w.offsets, w.order, out, bg);
+  if (w.wts)
+    k_gather<true><<<row_grid(d), kRowThreads, 0, s>>>(img, hx, hy, hz, d, w.offsets, w.order,
+                                                       w.wts, out, bg);
+  else
+    k_gather<false><<<row_grid(d), kRowThreads, 0, s>>>(img, hx, hy, hz, d, w.offsets, w.order,
+                                                        nullptr, out, bg);
   return cudaGetLastError();
 }
 

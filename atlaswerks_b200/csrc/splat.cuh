@@ -27,12 +27,14 @@ struct SplatWork {
   int *order;       // n: source indices grouped by bucket
   int *blocksums;   // scan partials
   int nblocks;
+  float *wts;       // 8n or null: the corner weights of the source at each sorted position
 };
 
-// bytes of device scratch one splat of grid d needs
-size_t splat_scratch_bytes(const Dims &d);
+// bytes of device scratch one splat of grid d needs; weights: room for the
+// corner weights the sort can precompute (32 bytes per voxel)
+size_t splat_scratch_bytes(const Dims &d, bool weights = true);
 // lays out a SplatWork inside caller-provided device memory (256-aligned)
-void splat_work_bind(SplatWork *w, const Dims &d, void *scratch);
+void splat_work_bind(SplatWork *w, const Dims &d, void *scratch, bool weights = true);
 
 // out = splat of img by h (three planes), background bg; stream-ordered
 cudaError_t splat(const SplatWork &w, const float *img, const float *hx, const float *hy,

@@ -61,7 +61,7 @@ int aw_splat_static(const float *img, const float *hx, const float *hy, const fl
   if (!img || !hx || !hy || !hz || !out) return fail_static("aw_splat_static: null pointer");
   if (nx < 1 || ny < 1 || nz < 1) return fail_static("aw_splat_static: empty grid");
   const aw::Dims d{nx, ny, nz};
-  const size_t need = aw::splat_scratch_bytes(d);
+  const size_t need = aw::splat_scratch_bytes(d, false);
   if (need > (size_t)AW_SPLAT_STATIC_MAX_BYTES)
     return fail_static("aw_splat_static: grid needs " + std::to_string(need) +
                        " bytes of scratch, more than the fixed " +
@@ -70,7 +70,7 @@ int aw_splat_static(const float *img, const float *hx, const float *hy, const fl
   void *scratch = nullptr;
   if (scratch_address(&scratch)) return 1;
   aw::SplatWork w;
-  aw::splat_work_bind(&w, d, scratch);
+  aw::splat_work_bind(&w, d, scratch, false);
   // aw::splat zeroes the bucket counters itself; nothing from the previous
   // call's contents is read before it is rewritten
   const cudaError_t e =
