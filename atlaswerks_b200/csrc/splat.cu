@@ -147,23 +147,6 @@ __global__ void __launch_bounds__(kRowThreads)
   order[pos] = (int)v.i;
 }
 
-// insertion sort of each bucket by source index (buckets are short)
-__global__ void __launch_bounds__(256)
-    k_bucket_sort(const int *__restrict__ offsets, int *__restrict__ order, long next) {
-  const long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= next) return;
-  const int s = offsets[b], e = offsets[b + 1];
-  for (int i = s + 1; i < e; ++i) {
-    const int key = order[i];
-    int j = i - 1;
-    while (j >= s && order[j] > key) {
-      order[j + 1] = order[j];
-      --j;
-    }
-    order[j + 1] = key;
-  }
-}
-
 // weight of corner (cx, cy, cz) of a source at p, rounded to float as
 // forwardApply writes it (HField3DUtils.txx:1116-1123): the product runs left
 // to right, in double once a (1.0 - r) factor has entered it and in float
@@ -182,23 +165,38 @@ AW_D float corner_weight(float px, float py, float pz, int cx, int cy, int cz) {
   return __double2float_rn(dmul(dmul(ax, ay), az));
 }
 
-// the eight corner weights (index dx + 2 dy + 4 dz) of the source at every
-// sorted position, once per sort: the gathers of every image splatted by
-// the same h read them instead of the source's h and the weight arithmetic
+// insertion sort of each bucket by source index (buckets are short); with
+// wts, then the eight corner weights (index dx + 2 dy + 4 dz) of the source
+// at every position of the bucket, once per sort: the gathers of every image
+// splatted by the same h read them instead of the source's h and the weight
+// arithmetic
 __global__ void __launch_bounds__(256)
-    k_weights(const float *__restrict__ hx, const float *__restrict__ hy,
-              const float *__restrict__ hz, const int *__restrict__ order,
-              const int *__restrict__ total, long n, float *__restrict__ wts) {
-  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n || p >= (long)__ldg(total)) return;
-  const int m = __ldg(order + p);
-  const float px = __ldg(hx + m), py = __ldg(hy + m), pz = __ldg(hz + m);
-  float w[8];
+    k_bucket_sort(const int *__restrict__ offsets, int *__restrict__ order, long next,
+                  const float *__restrict__ hx, const float *__restrict__ hy,
+                  const float *__restrict__ hz, float *__restrict__ wts) {
+  const long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= next) return;
+  const int s = offsets[b], e = offsets[b + 1];
+  for (int i = s + 1; i < e; ++i) {
+    const int key = order[i];
+    int j = i - 1;
+    while (j >= s && order[j] > key) {
+      order[j + 1] = order[j];
+      --j;
+    }
+    order[j + 1] = key;
+  }
+  if (!wts) return;
+  for (int i = s; i < e; ++i) {
+    const int m = order[i];
+    const float px = __ldg(hx + m), py = __ldg(hy + m), pz = __ldg(hz + m);
+    float w[8];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) w[k] = corner_weight(px, py, pz, k & 1, (k >> 1) & 1, (k >> 2) & 1);
-  float4 *o = reinterpret_cast<float4 *>(wts + p * 8);
-  o[0] = make_float4(w[0], w[1], w[2], w[3]);
-  o[1] = make_float4(w[4], w[5], w[6], w[7]);
+    for (int k = 0; k < 8; ++k) w[k] = corner_weight(px, py, pz, k & 1, (k >> 1) & 1, (k >> 2) & 1);
+    float4 *o = reinterpret_cast<float4 *>(wts + (long)i * 8);
+    o[0] = make_float4(w[0], w[1], w[2], w[3]);
+    o[1] = make_float4(w[4], w[5], w[6], w[7]);
+  }
 }
 
 // every destination merges its eight candidate buckets in source order (the
@@ -328,10 +326,8 @@ cudaError_t splat_sort(const SplatWork &w, const float *hx, const float *hy, con
   k_scan_blocksums<<<1, kScanThreads, 0, s>>>(w.blocksums, w.nblocks);
   k_scan_apply<<<w.nblocks, kScanThreads, 0, s>>>(w.offsets, w.next, w.blocksums);
   k_scatter<<<row_grid(d), kRowThreads, 0, s>>>(hx, hy, hz, d, w.offsets, w.cursor, w.order);
-  k_bucket_sort<<<(int)((w.next + 255) / 256), 256, 0, s>>>(w.offsets, w.order, w.next);
-  if (w.wts)
-    k_weights<<<(unsigned)((d.n() + 255) / 256), 256, 0, s>>>(hx, hy, hz, w.order,
-                                                              w.offsets + w.next, d.n(), w.wts);
+  k_bucket_sort<<<(int)((w.next + 255) / 256), 256, 0, s>>>(w.offsets, w.order, w.next, hx, hy,
+                                                            hz, w.wts);
   return cudaGetLastError();
 }
 
