@@ -773,6 +773,8 @@ int aw_ldmm_shoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *
                           float *phi0T, float *phiT0, void *stream) {
   if (!l || !I0 || !I1 || !alpha0 || !phi0T || !phiT0)
     return fail("aw_ldmm_shoot_iterate: null pointer");
+  if (aw::ldmm_shoot_prepare(&l->ctx))
+    return fail("aw_ldmm_shoot_iterate: device allocation failed");
   AW_CUDA(aw::ldmm_shoot_iterate(&l->ctx, I0, I1, alpha0, phi0T, phiT0, S(stream)),
           "aw_ldmm_shoot_iterate");
   return 0;
@@ -820,10 +822,6 @@ int read_ring(aw_ldmm_t l, const double *ring_dev, double *out, int max_count, i
 
 int aw_ldmm_get_vec_energies(aw_ldmm_t l, double *out, int max_count, int *count) {
   if (!l || !count) return fail("aw_ldmm_get_vec_energies: null pointer");
-  if (!l->ctx.venergy) {
-    *count = 0;
-    return 0;
-  }
   return read_ring(l, l->ctx.venergy, out, max_count, count, "aw_ldmm_get_vec_energies");
 }
 

@@ -145,12 +145,12 @@ __global__ void __launch_bounds__(kRowThreads)
   }
 }
 
-// energy[count % cap] = scale * sum(partials); advance: count += 1 (the
-// image energy, recorded last in an iteration)
+// energy[count % cap] = scale * sum(partials) (add: +=); advance: count += 1
+// (the image energy, recorded last in an iteration)
 __global__ void __launch_bounds__(256)
     k_record_energy(const double *__restrict__ partials, int nparts, double scale,
                     double *__restrict__ energy, int *__restrict__ count, int cap,
-                    int advance = 1) {
+                    int advance = 1, int add = 0) {
   double t = 0.0;
   for (int i = threadIdx.x; i < nparts; i += blockDim.x) t += partials[i];
   __shared__ double ws[8];
@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(256)
     double s = 0.0;
     for (int w = 0; w < 8; ++w) s += ws[w];
     const int k = *count;
-    energy[k % cap] = s * scale;
+    energy[k % cap] = add ? energy[k % cap] + s * scale : s * scale;
     if (advance) *count = k + 1;
   }
 }
@@ -385,6 +385,8 @@ int ldmm_create(LdmmCtx *c, int nx, int ny, int nz, double spx, double spy, doub
   if (cudaMalloc(&c->splat_scratch, splat_scratch_bytes(c->d)) != cudaSuccess) return 3;
   if (cudaMalloc(&c->partials, sizeof(double) * c->nparts) != cudaSuccess) return 3;
   if (cudaMalloc(&c->energy, sizeof(double) * c->cap) != cudaSuccess) return 3;
+  if (cudaMalloc(&c->venergy, sizeof(double) * c->cap) != cudaSuccess) return 3;
+  cudaMemset(c->venergy, 0, sizeof(double) * c->cap);
   if (cudaMalloc(&c->scalars, 64) != cudaSuccess) return 3;
   cudaMemset(c->scalars, 0, 64);
   c->step = reinterpret_cast<float *>(c->scalars);
@@ -398,7 +400,7 @@ void ldmm_destroy(LdmmCtx *c) {
   fluid_plan_destroy(&c->plan);
   void *ptrs[] = {c->J0,     c->hbuf,   c->diff, c->S,   c->u,   c->splat_scratch,
                   c->partials, c->energy, c->scalars, c->JT, c->JD, c->adV,
-                  c->adP,    c->adA,    c->adI,  c->venergy, c->adSortMem};
+                  c->adP,    c->adA,    c->adI,  c->venergy, c->adSortMem, c->lv};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   std::memset(c, 0, sizeof(*c));
@@ -570,6 +572,7 @@ __global__ void k_shoot_alpha(float *__restrict__ a0, const float *__restrict__ 
 // I0(phiT0) in J0[0]. Records the image energy sp^3 sum (I0(phiT0) - I1)^2.
 cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, float *alpha0,
                                float *phi0T, float *phiT0, cudaStream_t s) {
+  if (!c->lv) return cudaErrorNotReady;
   const Dims d = c->d;
   const long n = d.n();
   const int T = c->T;
@@ -577,10 +580,22 @@ cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, flo
   int ca = 0, cb = 0;
   auto comp = [&](float *base, int k) { return base + k * n; };
   float *v = c->u, *aT = c->S, *I = c->J0;
+  const double spprod = c->sp.x * c->sp.y * c->sp.z;
+  int vt = 0;  // velocities formed so far
+  // v = K(grad(G) alpha_t), then its step energy <L v, v> added to this
+  // iteration's vector energy (LDMMShootingIteratorCPU.cxx:216-221, 257-262)
   auto velocity = [&](const float *G) -> cudaError_t {
     AW_TRY(fluid_forward_force(c->plan, G, aT, 0, s));
     AW_TRY(fluid_solve(c->plan, 1, s));
-    return fluid_inverse_store(c->plan, comp(v, 0), comp(v, 1), comp(v, 2), s);
+    AW_TRY(fluid_inverse_store(c->plan, comp(v, 0), comp(v, 1), comp(v, 2), s));
+    AW_TRY(fluid_forward_field(c->plan, comp(v, 0), comp(v, 1), comp(v, 2), s));
+    AW_TRY(fluid_solve(c->plan, 0, s));
+    AW_TRY(fluid_inverse_store(c->plan, comp(c->lv, 0), comp(c->lv, 1), comp(c->lv, 2), s));
+    k_ad_vdot<<<row_grid(d), kRowThreads, 0, s>>>(c->lv, v, c->partials, d);
+    AW_TRY(cudaGetLastError());
+    k_record_energy<<<1, 256, 0, s>>>(c->partials, c->nparts, spprod, c->venergy, c->count,
+                                      c->cap, 0, vt++ > 0);
+    return cudaGetLastError();
   };
   auto advance_phi0T = [&]() -> cudaError_t {  // phi0T = composeVH(v, phi0T)
     const float *vv[3] = {comp(v, 0), comp(v, 1), comp(v, 2)};
@@ -616,7 +631,6 @@ cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, flo
   AW_TRY(splat(c->sw, c->diff, comp(B[cb], 0), comp(B[cb], 1), comp(B[cb], 2), aT, 0.0f, s));
   k_shoot_alpha<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(alpha0, aT, c->step, c->sigma, n);
   AW_TRY(cudaGetLastError());
-  const double spprod = c->sp.x * c->sp.y * c->sp.z;
   k_record_energy<<<1, 256, 0, s>>>(c->partials, c->nparts, spprod, c->energy, c->count, c->cap);
   AW_TRY(cudaGetLastError());
   // the maps end in the caller's buffers
@@ -634,21 +648,28 @@ int ldmm_adshoot_prepare(LdmmCtx *c) {
       cudaMalloc(&c->adP, sizeof(float) * 2 * (T + 1) * 3 * n) != cudaSuccess ||
       cudaMalloc(&c->adA, sizeof(float) * T * n) != cudaSuccess ||
       cudaMalloc(&c->adI, sizeof(float) * 6 * n) != cudaSuccess ||
-      cudaMalloc(&c->venergy, sizeof(double) * c->cap) != cudaSuccess ||
       cudaMalloc(&c->adSortMem, sort_bytes * (T + 1)) != cudaSuccess) {
     cudaGetLastError();
-    void *ptrs[] = {c->adV, c->adP, c->adA, c->adI, c->venergy, c->adSortMem};
+    void *ptrs[] = {c->adV, c->adP, c->adA, c->adI, c->adSortMem};
     for (void *p : ptrs)
       if (p) cudaFree(p);
     c->adV = c->adP = c->adA = c->adI = nullptr;
-    c->venergy = nullptr;
     c->adSortMem = nullptr;
     return 3;
   }
   for (size_t k = 0; k <= T; ++k)
     splat_work_bind(&c->adSort[k], c->d, static_cast<char *>(c->adSortMem) + k * sort_bytes);
-  // entries of iterations of the other kinds read as 0
-  return cudaMemset(c->venergy, 0, sizeof(double) * c->cap) == cudaSuccess ? 0 : 3;
+  return 0;
+}
+
+int ldmm_shoot_prepare(LdmmCtx *c) {
+  if (c->lv) return 0;
+  if (cudaMalloc(&c->lv, sizeof(float) * 3 * (size_t)c->d.n()) != cudaSuccess) {
+    cudaGetLastError();
+    c->lv = nullptr;
+    return 3;
+  }
+  return 0;
 }
 
 // LDMMAdShootingIteratorCPU::Iterate (LDMM/LDMMAdShootingIteratorCPU.cxx:

@@ -39,8 +39,9 @@ struct LdmmCtx {
   float *adP;       // 2 x (T+1) x 3N: phi0T then phiT0 at t = 0 .. T
   float *adA;       // T x N: alpha_t = splat(alpha0, phi0T_t), t = 1 .. T
   float *adI;       // 6N: alphaHat, IHat, alphaTilde, ITilde and two scratch images
-  double *venergy;  // <L v0, v0> history ring, indexed like energy
+  double *venergy;  // vector-energy history ring, indexed like energy
   void *adSortMem;  // T + 1 splat scratch sets
+  float *lv;        // 3N: L v_t for the momentum shooting's vector energy
   SplatWork adSort[kMaxAdSorts];  // the sorts by phi0T_t (t = 1..T) and by phiT0_T (slot 0)
 };
 
@@ -55,6 +56,8 @@ cudaError_t ldmm_i1_at_0(LdmmCtx *c, const float *I1, const float *v, float *img
 cudaError_t ldmm_atlas_accumulate(float *acc, float *jsum, const float *img, const float *jd,
                                   float w, long n, cudaStream_t s);
 cudaError_t ldmm_atlas_normalize(float *acc, const float *jsum, long n, cudaStream_t s);
+// the momentum shooting's scratch (returns 3 when the allocation fails)
+int ldmm_shoot_prepare(LdmmCtx *c);
 cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, float *alpha0,
                                float *phi0T, float *phiT0, cudaStream_t s);
 // LDMMAdShootingIteratorCPU (LDMM/LDMMAdShootingIteratorCPU.cxx): the

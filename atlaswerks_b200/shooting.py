@@ -23,8 +23,9 @@
 The iterations run in libaw_b200.so (``aw_ldmm_shoot_iterate`` /
 ``aw_ldmm_adshoot_iterate`` on an LDMM handle, which holds T, sigma, the
 step size and the fluid kernel). The energy history holds the image term
-sp^3 sum (I0(phiT0) - I1)^2; the adjoint iterator also records the vector
-term <L v0, v0> (``VecEnergies``).
+sp^3 sum (I0(phiT0) - I1)^2 (``Energies``) and the vector term
+(``VecEnergies``): sum_t <L v_t, v_t> for the momentum shooting, <L v0, v0>
+for the adjoint shooting — the step energies LDMMEnergy holds.
 """
 from __future__ import annotations
 
@@ -108,6 +109,16 @@ class LDMMShootingIteratorB200:
                                               ctypes.byref(n)))
         return out[: n.value]
 
+    def VecEnergies(self) -> np.ndarray:
+        """The vector term per iteration: the sum over t of LDMMEnergy's step
+        energies <L v_t, v_t> (only v0's for the adjoint iterator)."""
+        n = ctypes.c_int()
+        check(_lib.lib().aw_ldmm_get_vec_energies(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros(max(n.value, 1), np.float64)
+        check(_lib.lib().aw_ldmm_get_vec_energies(self._h, out.ctypes.data, n.value,
+                                                  ctypes.byref(n)))
+        return out[: n.value]
+
     def _free(self):
         if self._h:
             _lib.lib().aw_ldmm_destroy(self._h)
@@ -159,14 +170,6 @@ class LDMMAdShootingIteratorB200(LDMMShootingIteratorB200):
         """PhiT0 composed from the identity through the last iteration's v_t."""
         self._final(data, 1)
 
-    def VecEnergies(self) -> np.ndarray:
-        """<L v0, v0> per iteration (LDMMEnergy::VecStepEnergy(0))."""
-        n = ctypes.c_int()
-        check(_lib.lib().aw_ldmm_get_vec_energies(self._h, None, 0, ctypes.byref(n)))
-        out = np.zeros(max(n.value, 1), np.float64)
-        check(_lib.lib().aw_ldmm_get_vec_energies(self._h, out.ctypes.data, n.value,
-                                                  ctypes.byref(n)))
-        return out[: n.value]
 
 
 @dataclass

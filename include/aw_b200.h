@@ -291,7 +291,8 @@ int aw_ldmm_get_energies(aw_ldmm_t l, double *out, int max_count, int *count);
  * (a scalar image, updated in place to (1 - step) alpha0 + (step/sigma^2)
  * times the splatted residual) and leaves phi0T and phiT0 ([3][N] each, the
  * maps LDMMShootingDefData::Phi0T / PhiT0) in the caller's buffers; records
- * the image energy (aw_ldmm_get_energies). */
+ * the image energy (aw_ldmm_get_energies) and the sum over t of the step
+ * energies <L v_t, v_t> (aw_ldmm_get_vec_energies). */
 int aw_ldmm_shoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *alpha0,
                           float *phi0T, float *phiT0, void *stream);
 
@@ -312,8 +313,10 @@ int aw_ldmm_adshoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float
  * (LDMMAdShootingIteratorCPU.cxx:433-453, LDMMWarpAd.txx:37-42): the maps
  * from time 0 to 1 and back composed through the last iteration's velocities. */
 int aw_ldmm_adshoot_final_maps(aw_ldmm_t l, float *phi0T, float *phiT0, void *stream);
-/* Vector energies <L v0, v0> sp^3 of the adjoint shooting iterations, oldest
- * first (LDMMEnergy::VecStepEnergy(0)); synchronises. */
+/* Vector energies of the shooting iterations, oldest first: the sum over
+ * the time steps of LDMMEnergy::VecStepEnergy(t), i.e. sum_t <L v_t, v_t> sp^3
+ * for aw_ldmm_shoot_iterate and <L v0, v0> sp^3 for aw_ldmm_adshoot_iterate
+ * (0 for the relaxation iterations); synchronises. */
 int aw_ldmm_get_vec_energies(aw_ldmm_t l, double *out, int max_count, int *count);
 
 /* LDMM relaxation atlas (LDMMAtlasBuilder / LDMMAtlasThreadCPU,

@@ -241,17 +241,19 @@ class Oracle:
         return float(e), float(st.value)
 
     def ldmm_shoot_iterate(self, I0, I1, alpha0, T, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01,
-                           gamma=0.001, sigma=0.1, step=0.005):
+                           gamma=0.001, sigma=0.1, step=0.005, vec=False):
         """One LDMMShootingIteratorCPU::Iterate; alpha0 [nz,ny,nx] updated in
-        place. Returns (image energy, phi0T, phiT0)."""
+        place. Returns (image energy, phi0T, phiT0), with vec=True (image
+        energy, sum over t of <L v_t, v_t>, phi0T, phiT0)."""
         assert alpha0.dtype == np.float32 and alpha0.flags.c_contiguous
         p0 = np.empty((3,) + I0.shape, np.float32)
         p1 = np.empty((3,) + I0.shape, np.float32)
+        ev = ctypes.c_double()
         e = self.lib.aw_oracle_ldmm_shoot_iterate(
             _fp(I0), _fp(I1), _fp(alpha0), p0.ctypes.data_as(_f), p1.ctypes.data_as(_f), _i(T),
             *_shape(I0), *map(_dbl, sp), _dbl(alpha), _dbl(beta), _dbl(gamma),
-            ctypes.c_float(sigma), ctypes.c_float(step))
-        return float(e), p0, p1
+            ctypes.c_float(sigma), ctypes.c_float(step), ctypes.byref(ev) if vec else None)
+        return (float(e), float(ev.value), p0, p1) if vec else (float(e), p0, p1)
 
     def ldmm_adshoot_iterate(self, I0, I1, alpha0, T, sp=(1.0, 1.0, 1.0), alpha=0.01,
                              beta=0.01, gamma=0.001, sigma=0.1, step=0.005):
@@ -611,21 +613,23 @@ class Reference:
         return img, jd
 
     def shoot_run(self, I0, I1, T, iters, sp=(1.0, 1.0, 1.0), sigma=0.1, step=0.005, alpha=0.01,
-                  beta=0.01, gamma=0.001):
+                  beta=0.01, gamma=0.001, vec=False):
         """The reference's LDMMShootingDefData / LDMMShootingIteratorCPU for
         `iters` iterations from alpha0 = 0. Returns (alpha0, phi0T, phiT0,
-        image energies)."""
+        image energies), with vec=True also the per-iteration sums over t of
+        the step energies <L v_t, v_t>."""
         a0 = np.empty(I0.shape, np.float32)
         p0 = np.empty((3,) + I0.shape, np.float32)
         p1 = np.empty((3,) + I0.shape, np.float32)
         en = np.zeros(iters, np.float64)
+        ev = np.zeros(iters, np.float64)
         with quiet_stdout():
             rc = self.lib.awref_shoot_run(
                 _fp(I0), _fp(I1), *_shape(I0), *map(_dbl, sp), _i(T), _i(iters),
                 ctypes.c_float(sigma), ctypes.c_float(step), _dbl(alpha), _dbl(beta), _dbl(gamma),
-                _fp(a0), p0.ctypes.data_as(_f), p1.ctypes.data_as(_f), _dp(en))
+                _fp(a0), p0.ctypes.data_as(_f), p1.ctypes.data_as(_f), _dp(en), _dp(ev))
         self._check(rc)
-        return a0, p0, p1, en
+        return (a0, p0, p1, en, ev) if vec else (a0, p0, p1, en)
 
     def adshoot_run(self, I0, I1, T, levels, sp=(1.0, 1.0, 1.0), sigma=1.0, alpha=0.01,
                     beta=0.01, gamma=0.001):

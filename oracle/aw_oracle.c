@@ -819,10 +819,28 @@ void aw_oracle_ldmm_i1_at_0(const float *I1, const float *v, int T, int nx, int 
  * alpha0 <- (1 - step) alpha0 + (step / sigma^2) alphaT. Returns the image
  * energy sp^3 sum diff^2 (the velocity terms of LDMMEnergy are not formed).
  * ---------------------------------------------------------------------- */
+/* <L v, v> sp^3 as HField3DUtils::l2DotProd forms it (HField3DUtils.txx:
+ * 190-200): float products, a float sum per component, the three sums
+ * added in float, times the spacing product, kept as a float (Real) */
+static double l_energy(const float *v, float *scratch, int nx, int ny, int nz, double spx,
+                       double spy, double spz, double alpha, double beta, double gamma) {
+  const long n = (long)nx * ny * nz;
+  memcpy(scratch, v, sizeof(float) * (size_t)(3 * n));
+  aw_oracle_fluid_apply(scratch, scratch + n, scratch + 2 * n, nx, ny, nz, spx, spy, spz, alpha,
+                        beta, gamma, 0);
+  float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+  for (long k = 0; k < n; ++k) {
+    sx += scratch[k] * v[k];
+    sy += scratch[n + k] * v[n + k];
+    sz += scratch[2 * n + k] * v[2 * n + k];
+  }
+  return (double)(float)(spx * spy * spz * (double)(sx + sy + sz));
+}
+
 double aw_oracle_ldmm_shoot_iterate(const float *I0, const float *I1, float *alpha0, float *phi0T,
                                     float *phiT0, int T, int nx, int ny, int nz, double spx,
                                     double spy, double spz, double alpha, double beta,
-                                    double gamma, float sigma, float step) {
+                                    double gamma, float sigma, float step, double *vec_energy) {
   const long n = (long)nx * ny * nz;
   float *v = (float *)malloc(sizeof(float) * (size_t)(3 * n));
   float *o = (float *)malloc(sizeof(float) * (size_t)(3 * n));
@@ -845,7 +863,10 @@ double aw_oracle_ldmm_shoot_iterate(const float *I0, const float *I1, float *alp
                           1);                                                                 \
   } while (0)
   AW_SHOOT_VELOCITY(I0);
+  /* sum over t of the step energies <L v_t, v_t> (.cxx:216-221, 257-262) */
+  double ev = 0.0;
   for (int t = 1; t < T; ++t) {
+    if (vec_energy) ev += l_energy(v, o, nx, ny, nz, spx, spy, spz, alpha, beta, gamma);
     aw_oracle_compose_vh(v, v + n, v + 2 * n, p0, p0 + n, p0 + 2 * n, o, o + n, o + 2 * n, nx, ny,
                          nz, spx, spy, spz, 1, AW_BG_PARTIAL_ZERO);
     memcpy(p0, o, sizeof(float) * (size_t)(3 * n));
@@ -857,6 +878,7 @@ double aw_oracle_ldmm_shoot_iterate(const float *I0, const float *I1, float *alp
     AW_SHOOT_VELOCITY(I);
   }
 #undef AW_SHOOT_VELOCITY
+  if (vec_energy) *vec_energy = ev + l_energy(v, o, nx, ny, nz, spx, spy, spz, alpha, beta, gamma);
   aw_oracle_compose_hv(p1, p1 + n, p1 + 2 * n, v, v + n, v + 2 * n, o, o + n, o + 2 * n, nx, ny,
                        nz, spx, spy, spz, -1, AW_BG_PARTIAL_ID);
   memcpy(p1, o, sizeof(float) * (size_t)(3 * n));
@@ -969,20 +991,8 @@ double aw_oracle_ldmm_adshoot_iterate(const float *I0, const float *I1, float *a
   }
   AD_ADVANCE_P1(AD_V(T - 1));
   AD_ADVANCE_P0(AD_V(T - 1));
-  /* <L v0, v0>: float products and float sums per component
-   * (HField3DUtils::l2DotProd, HField3DUtils.txx:190-200) */
-  memcpy(w, AD_V(0), f3);
-  aw_oracle_fluid_apply(w, w + n, w + 2 * n, nx, ny, nz, spx, spy, spz, alpha, beta, gamma, 0);
-  {
-    const float *v0 = AD_V(0);
-    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
-    for (long k = 0; k < n; ++k) {
-      sx += w[k] * v0[k];
-      sy += w[n + k] * v0[n + k];
-      sz += w[2 * n + k] * v0[2 * n + k];
-    }
-    if (vec_energy) *vec_energy = (double)(float)(spx * spy * spz * (double)(sx + sy + sz));
-  }
+  /* <L v0, v0> (.cxx:305-311) */
+  if (vec_energy) *vec_energy = l_energy(AD_V(0), w, nx, ny, nz, spx, spy, spz, alpha, beta, gamma);
   aw_oracle_apply(I0, p1, p1 + n, p1 + 2 * n, I, nx, ny, nz, 0.0f);
   double e = 0.0;
   for (long k = 0; k < n; ++k) {

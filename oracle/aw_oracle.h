@@ -74,11 +74,13 @@ double aw_oracle_ldmm_iterate_orig(const float *I0, const float *I1, float *v, i
 /* GetI1At0 (I1 pulled back through the velocities) and ComputeJacDet */
 void aw_oracle_ldmm_i1_at_0(const float *I1, const float *v, int T, int nx, int ny, int nz,
                             double spx, double spy, double spz, float *img, float *jd);
-/* LDMMShootingIteratorCPU::Iterate: alpha0, phi0T, phiT0 updated in place */
+/* LDMMShootingIteratorCPU::Iterate: alpha0, phi0T, phiT0 updated in place;
+ * returns the image energy; *vec_energy (if not null) = sum over t of the
+ * step energies <L v_t, v_t> */
 double aw_oracle_ldmm_shoot_iterate(const float *I0, const float *I1, float *alpha0, float *phi0T,
                                     float *phiT0, int T, int nx, int ny, int nz, double spx,
                                     double spy, double spz, double alpha, double beta,
-                                    double gamma, float sigma, float step);
+                                    double gamma, float sigma, float step, double *vec_energy);
 
 /* LDMMAdShootingIteratorCPU::Iterate + backwardAdIntegration: alpha0
  * updated in place; V (T x 3N) receives the shot velocities; phi0T / phiT0

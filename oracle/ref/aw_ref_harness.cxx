@@ -640,7 +640,7 @@ int awref_ldmm_atlas_run(const float *imgs, int ns, const float *weights, int nx
 int awref_shoot_run(const float *i0, const float *i1, int nx, int ny, int nz, double spx,
                     double spy, double spz, int T, int iters, float sigma, float step, double alpha,
                     double beta, double gamma, float *alpha0, float *phi0T, float *phiT0,
-                    double *energies) {
+                    double *energies, double *vec_energies) {
   GUARD_BEGIN
   std::ostringstream xml;
   xml.precision(17);
@@ -677,6 +677,12 @@ int awref_shoot_run(const float *i0, const float *i1, int nx, int ny, int nz, do
     if (energies) {
       LDMMEnergy *e = dynamic_cast<LDMMEnergy *>(data.GetEnergyHistory().LastEnergy());
       energies[iter] = e ? (double)e->ImageEnergy() * sigma * sigma : 0.0;
+    }
+    if (vec_energies) {
+      LDMMEnergy *e = dynamic_cast<LDMMEnergy *>(data.GetEnergyHistory().LastEnergy());
+      double sum = 0.0;
+      for (int t = 0; e && t < T; ++t) sum += (double)e->VecStepEnergy(t);
+      vec_energies[iter] = sum;
     }
   }
   from_im(data.Alpha0(), alpha0);

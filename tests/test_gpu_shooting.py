@@ -4,7 +4,7 @@ LDMMShootingIteratorCPU::Iterate (itself pinned against the reference in
 tests/test_oracle_pin.py).
 
 Tolerances (four iterations): alpha0 within 1e-4 of max |alpha0|, the
-maps within 1e-3 voxel, image energies 1e-4 relative — the fluid solve
+maps within 1e-3 voxel, image and vector energies 1e-4 relative — the fluid solve
 is FP32 on the device and FP64 in the oracle; interpolation, composition
 and splatting are bit-exact operations.
 """
@@ -35,16 +35,28 @@ def test_shooting_vs_oracle(oracle, shape, sp, T):
     iters = 4
     I0, I1 = greedy_pair(shape, 7, n_blobs=4, umax=1.5, sigma_range=(1.5, 3.0), smooth_sigma=3.0)
     a = np.zeros(shape, np.float32)
-    e_o = []
+    e_o, ev_o = [], []
     for _ in range(iters):
-        e, p0, p1 = oracle.ldmm_shoot_iterate(I0, I1, a, T, sp, sigma=1.0, step=0.05)
+        e, ev, p0, p1 = oracle.ldmm_shoot_iterate(I0, I1, a, T, sp, sigma=1.0, step=0.05,
+                                                  vec=True)
         e_o.append(e)
-    data, e_g = shoot_register(cu(I0), cu(I1), T, iters, sp, sigma=1.0, step=0.05)
+        ev_o.append(ev)
+    from atlaswerks_b200.shooting import LDMMShootingIteratorB200
+    from atlaswerks_b200.ldmm import LDMMIteratorParam
+    from atlaswerks_b200.greedy import DiffOperParam
+    it = LDMMShootingIteratorB200(shape[::-1], spacing=sp, n_time_steps=T)
+    it.SetScaleLevel(shape[::-1], sp, LDMMIteratorParam(DiffOperParam(), 1.0, 0.05, False))
+    from atlaswerks_b200.shooting import LDMMShootingDefDataB200
+    data = LDMMShootingDefDataB200(cu(I0), cu(I1), sp)
+    for _ in range(iters):
+        it.Iterate(data)
     ag = host(data.Alpha0)
     assert np.abs(ag - a).max() <= 1e-4 * np.abs(a).max()
     assert np.abs(host(data.Phi0T) - p0).max() <= 1e-3
     assert np.abs(host(data.PhiT0) - p1).max() <= 1e-3
-    assert np.allclose(e_g, e_o, rtol=1e-4)
+    assert np.allclose(it.Energies(), e_o, rtol=1e-4)
+    # sum over t of <L v_t, v_t>: double sums here, float sums in the oracle
+    assert np.allclose(it.VecEnergies(), ev_o, rtol=1e-4)
     assert e_o[-1] < e_o[0]
 
 

@@ -144,12 +144,17 @@ def test_ldmm_shooting_matches_reference(oracle, reference, sp):
     alpha0 = 0: the restatement against LDMMShootingIteratorCPU."""
     shape, T, iters = (12, 14, 16), 4, 4
     I0, I1 = greedy_pair(shape, 7, n_blobs=4, umax=1.5, sigma_range=(1.5, 3.0), smooth_sigma=3.0)
-    a_r, p0_r, p1_r, e_r = reference.shoot_run(I0, I1, T, iters, sp=sp, sigma=1.0, step=0.05)
+    a_r, p0_r, p1_r, e_r, ev_r = reference.shoot_run(I0, I1, T, iters, sp=sp, sigma=1.0,
+                                                     step=0.05, vec=True)
     a = np.zeros(shape, np.float32)
-    e_o = []
+    e_o, ev_o = [], []
     for _ in range(iters):
-        e, p0, p1 = oracle.ldmm_shoot_iterate(I0, I1, a, T, sp, sigma=1.0, step=0.05)
+        e, ev, p0, p1 = oracle.ldmm_shoot_iterate(I0, I1, a, T, sp, sigma=1.0, step=0.05,
+                                                  vec=True)
         e_o.append(e)
+        ev_o.append(ev)
+    # the vector energies: sum over t of <L v_t, v_t> (LDMMEnergy's step energies)
+    assert np.allclose(ev_o, ev_r, rtol=1e-5, atol=1e-9)
     # the oracle's FP64 fluid solve vs the reference's FP32 one
     assert np.abs(a - a_r).max() <= 1e-5 * np.abs(a_r).max()
     assert np.abs(p0 - p0_r).max() <= 1e-4
