@@ -147,19 +147,30 @@ __global__ void __launch_bounds__(kRowThreads)
 
 // energy[count % cap] = scale * sum(partials) (add: +=); advance: count += 1
 // (the image energy, recorded last in an iteration)
-__global__ void __launch_bounds__(256)
+// one block of kRecThreads; four independent partial sums per thread keep
+// four loads in flight (a fixed order: the same sum on every run)
+constexpr int kRecThreads = 1024;
+__global__ void __launch_bounds__(kRecThreads)
     k_record_energy(const double *__restrict__ partials, int nparts, double scale,
                     double *__restrict__ energy, int *__restrict__ count, int cap,
                     int advance = 1, int add = 0) {
-  double t = 0.0;
-  for (int i = threadIdx.x; i < nparts; i += blockDim.x) t += partials[i];
-  __shared__ double ws[8];
+  double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+  int i = threadIdx.x;
+  for (; i + 3 * kRecThreads < nparts; i += 4 * kRecThreads) {
+    t0 += __ldg(partials + i);
+    t1 += __ldg(partials + i + kRecThreads);
+    t2 += __ldg(partials + i + 2 * kRecThreads);
+    t3 += __ldg(partials + i + 3 * kRecThreads);
+  }
+  for (; i < nparts; i += kRecThreads) t0 += __ldg(partials + i);
+  double t = (t0 + t1) + (t2 + t3);
+  __shared__ double ws[kRecThreads / 32];
   t = warp_sum(t);
   if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = t;
   __syncthreads();
   if (threadIdx.x == 0) {
     double s = 0.0;
-    for (int w = 0; w < 8; ++w) s += ws[w];
+    for (int w = 0; w < kRecThreads / 32; ++w) s += ws[w];
     const int k = *count;
     energy[k % cap] = add ? energy[k % cap] + s * scale : s * scale;
     if (advance) *count = k + 1;
@@ -435,8 +446,8 @@ cudaError_t ldmm_iterate(LdmmCtx *c, const float *I0, const float *I1, float *v,
   AW_TRY(cudaGetLastError());
   if (!update_step) {
     const double spprod = c->sp.x * c->sp.y * c->sp.z;
-    k_record_energy<<<1, 256, 0, s>>>(c->partials, c->nparts, spprod, c->energy, c->count,
-                                      c->cap);
+    k_record_energy<<<1, kRecThreads, 0, s>>>(c->partials, c->nparts, spprod, c->energy,
+                                              c->count, c->cap);
     AW_TRY(cudaGetLastError());
   } else {
     AW_TRY(cudaMemsetAsync(c->maxbits, 0, sizeof(unsigned), s));
@@ -593,8 +604,8 @@ cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, flo
     AW_TRY(fluid_inverse_store(c->plan, comp(c->lv, 0), comp(c->lv, 1), comp(c->lv, 2), s));
     k_ad_vdot<<<row_grid(d), kRowThreads, 0, s>>>(c->lv, v, c->partials, d);
     AW_TRY(cudaGetLastError());
-    k_record_energy<<<1, 256, 0, s>>>(c->partials, c->nparts, spprod, c->venergy, c->count,
-                                      c->cap, 0, vt++ > 0);
+    k_record_energy<<<1, kRecThreads, 0, s>>>(c->partials, c->nparts, spprod, c->venergy,
+                                              c->count, c->cap, 0, vt++ > 0);
     return cudaGetLastError();
   };
   auto advance_phi0T = [&]() -> cudaError_t {  // phi0T = composeVH(v, phi0T)
@@ -631,7 +642,8 @@ cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, flo
   AW_TRY(splat(c->sw, c->diff, comp(B[cb], 0), comp(B[cb], 1), comp(B[cb], 2), aT, 0.0f, s));
   k_shoot_alpha<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(alpha0, aT, c->step, c->sigma, n);
   AW_TRY(cudaGetLastError());
-  k_record_energy<<<1, 256, 0, s>>>(c->partials, c->nparts, spprod, c->energy, c->count, c->cap);
+  k_record_energy<<<1, kRecThreads, 0, s>>>(c->partials, c->nparts, spprod, c->energy,
+                                            c->count, c->cap);
   AW_TRY(cudaGetLastError());
   // the maps end in the caller's buffers
   if (ca) AW_TRY(cudaMemcpyAsync(phi0T, A[1], sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
@@ -752,14 +764,14 @@ cudaError_t ldmm_adshoot_iterate(LdmmCtx *c, const float *I0, const float *I1, f
   AW_TRY(fluid_inverse_store(c->plan, comp(c->u, 0), comp(c->u, 1), comp(c->u, 2), s));
   k_ad_vdot<<<grid, kRowThreads, 0, s>>>(c->u, V(0), c->partials, d);
   AW_TRY(cudaGetLastError());
-  k_record_energy<<<1, 256, 0, s>>>(c->partials, c->nparts, spprod, c->venergy, c->count, c->cap,
-                                    0);
+  k_record_energy<<<1, kRecThreads, 0, s>>>(c->partials, c->nparts, spprod, c->venergy,
+                                            c->count, c->cap, 0);
   AW_TRY(cudaGetLastError());
   const float inv = 1.0f / (c->sigma * c->sigma);
   k_ad_residual<<<grid, kRowThreads, 0, s>>>(I(T), I1, inv, IHat, c->partials, d);
   AW_TRY(cudaGetLastError());
-  k_record_energy<<<1, 256, 0, s>>>(c->partials, c->nparts, spprod, c->energy, c->count, c->cap,
-                                    1);
+  k_record_energy<<<1, kRecThreads, 0, s>>>(c->partials, c->nparts, spprod, c->energy,
+                                            c->count, c->cap, 1);
   AW_TRY(cudaGetLastError());
 
   // backward integration of the adjoint equations
@@ -887,7 +899,8 @@ cudaError_t ldmm_iterate_orig(LdmmCtx *c, const float *I0, const float *I1, floa
   k_residual<<<row_grid(d), kRowThreads, 0, s>>>(Sb, I1, c->diff, c->partials, d);
   AW_TRY(cudaGetLastError());
   const double spprod = c->sp.x * c->sp.y * c->sp.z;
-  k_record_energy<<<1, 256, 0, s>>>(c->partials, c->nparts, spprod, c->energy, c->count, c->cap);
+  k_record_energy<<<1, kRecThreads, 0, s>>>(c->partials, c->nparts, spprod, c->energy,
+                                            c->count, c->cap);
   return cudaGetLastError();
 }
 
