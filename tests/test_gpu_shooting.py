@@ -176,3 +176,21 @@ def test_resample_image_vs_oracle(oracle, src_shape, dst_shape, ssp, dsp):
     dsp = tuple(float(np.float32(s)) for s in dsp)
     out = host(D.resample_image(cu(src), dst_shape, ssp, dsp))
     assert np.array_equal(out, oracle.resample_image(src, dst_shape, ssp, dsp))
+
+
+def test_adjoint_final_maps_before_any_iteration_fails_loudly():
+    """finalUpdatePhi0T has nothing to compose before the first Iterate: the
+    C ABI returns an error (raised by the host mirror) instead of copying
+    unset buffers."""
+    shape = (16, 16, 16)
+    I0, I1 = greedy_pair(shape, 7, n_blobs=4, umax=1.5, sigma_range=(1.5, 3.0), smooth_sigma=3.0)
+    it = LDMMAdShootingIteratorB200(shape[::-1], n_time_steps=3)
+    it.SetScaleLevel(shape[::-1], (1.0, 1.0, 1.0),
+                     LDMMIteratorParam(DiffOperParam(), 1.0, 0.0005, False))
+    data = LDMMShootingDefDataB200(cu(I0), cu(I1))
+    with pytest.raises(Exception, match="no adjoint shooting iteration"):
+        it.finalUpdatePhi0T(data)
+    it.Iterate(data)
+    it.finalUpdatePhi0T(data)
+    torch.cuda.synchronize()
+    assert len(it.Energies()) == 1 and len(it.VecEnergies()) == 1
