@@ -56,7 +56,7 @@ STAGE_BYTES = {
     "max_norm": 12,
     "update": 12 + 12 + 12,              # v, h gather (once), h' write
 }
-B_ITER = 92  # bytes/voxel of the fully fused 3-pass iteration (the survey's B_greedy)
+B_ITER = 92  # bytes/voxel of the fully fused 3-pass greedy iteration (each stream once)
 
 
 def peaks():
