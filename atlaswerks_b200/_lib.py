@@ -62,6 +62,14 @@ SIGNATURES = {
     "aw_greedy_get_step": ([_fp, _fp], _i),
     "aw_greedy_set_auto_step_reduce": ([_fp, _i], _i),
     "aw_greedy_set_staged_update": ([_fp, _i], _i),
+    "aw_greedy_last_energy": ([_fp, _fp], _i),
+    "aw_identity": ([_fp, _fp, _fp, _i, _i, _i, _fp], _i),
+    "aw_warmstart_param_floats": ([], ctypes.c_size_t),
+    "aw_warmstart_create": ([_i] * 6 + [_fp, ctypes.c_size_t, ctypes.c_float, _fp], _i),
+    "aw_warmstart_destroy": ([_fp], _i),
+    "aw_warmstart_predict": ([_fp] * 7, _i),
+    "aw_warmstart_register": ([_fp, _fp, _fp, ctypes.c_double, _i, _i, _i] + [_fp] * 6, _i),
+    "aw_greedy_set_fused_update": ([_fp, _i], _i),
     "aw_greedy_update_tile": ([_fp, _i, _fp], _i),
     "aw_greedy_iterate": ([_fp] * 15 + [_i, _fp], _i),
     "aw_greedy_run": ([_fp] * 15 + [_i, _i, _fp], _i),
@@ -82,6 +90,7 @@ SIGNATURES = {
     "aw_ldmm_set_step": ([_fp, _f], _i),
     "aw_ldmm_get_step": ([_fp, _fp], _i),
     "aw_ldmm_iterate": ([_fp] * 4 + [_i, _fp], _i),
+    "aw_ldmm_alphas": ([_fp, _fp, _fp, _fp, _fp, _fp], _i),
     "aw_ldmm_run": ([_fp] * 4 + [_i, _i, _fp], _i),
     "aw_ldmm_get_energies": ([_fp, _fp, _i, _fp], _i),
     "aw_ldmm_i1_at_0": ([_fp] * 6, _i),

@@ -199,6 +199,13 @@ int aw_downsample(const float *in, int nx, int ny, int nz, double spx, double sp
   return 0;
 }
 
+int aw_identity(float *hx, float *hy, float *hz, int nx, int ny, int nz, void *stream) {
+  if (!hx || !hy || !hz) return fail("aw_identity: null pointer");
+  if (nx < 1 || ny < 1 || nz < 1) return fail("aw_identity: empty grid");
+  AW_CUDA(aw::identity_field(hx, hy, hz, aw::Dims{nx, ny, nz}, S(stream)), "aw_identity");
+  return 0;
+}
+
 int aw_resample_image(const float *in, int nx, int ny, int nz, double sx, double sy, double sz,
                       float *out, int mx, int my, int mz, double tx, double ty, double tz,
                       void *stream) {
@@ -366,6 +373,15 @@ int aw_greedy_set_staged_update(aw_greedy_t g, int on) {
   return 0;
 }
 
+int aw_greedy_set_fused_update(aw_greedy_t g, int on) {
+  if (!g) return fail("aw_greedy_set_fused_update: null handle");
+  AW_CUDA(cudaDeviceSynchronize(), "aw_greedy_set_fused_update (pending work)");
+  g->ctx.no_fused_update = on ? 0 : 1;
+  for (auto &kv : g->graphs) cudaGraphExecDestroy(kv.second);
+  g->graphs.clear();  // captured iterations hold the other inverse/update kernels
+  return 0;
+}
+
 int aw_greedy_update_tile(aw_greedy_t g, int set, int *tile) {
   if (!g || !tile) return fail("aw_greedy_update_tile: null pointer");
   if (set) {
@@ -530,6 +546,18 @@ static int copy_energies(const aw::GreedyDevState &st, double *out, int max_coun
   const int m = (out && max_count < avail) ? max_count : avail;
   for (int i = 0; i < m && out; ++i) out[i] = ring[(n - avail + i) % cap];
   *count = avail;
+  return 0;
+}
+
+int aw_greedy_last_energy(aw_greedy_t g, double *energy) {
+  if (!g || !energy) return fail("aw_greedy_last_energy: null pointer");
+  const aw::GreedyDevState &st = g->ctx.st;
+  int n = 0;
+  // cudaMemcpy on the legacy stream waits for the iteration that records it
+  AW_CUDA(cudaMemcpy(&n, st.count, sizeof(int), cudaMemcpyDeviceToHost), "aw_greedy_last_energy");
+  if (n < 1) return fail("aw_greedy_last_energy: no energy recorded yet");
+  AW_CUDA(cudaMemcpy(energy, st.energy + (n - 1) % st.cap, sizeof(double), cudaMemcpyDeviceToHost),
+          "aw_greedy_last_energy");
   return 0;
 }
 
@@ -704,6 +732,17 @@ int aw_ldmm_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *v, int
   if (!l) return fail("aw_ldmm_iterate: null handle");
   if (!I0 || !I1 || !v) return fail("aw_ldmm_iterate: null pointer");
   AW_CUDA(aw::ldmm_iterate(&l->ctx, I0, I1, v, update_step, S(stream)), "aw_ldmm_iterate");
+  return 0;
+}
+
+int aw_ldmm_alphas(aw_ldmm_t l, const float *I0, const float *I1, const float *v, float *alphas,
+                   void *stream) {
+  if (!l) return fail("aw_ldmm_alphas: null handle");
+  if (!I0 || !I1 || !v || !alphas) return fail("aw_ldmm_alphas: null pointer");
+  if (l->ctx.orig)
+    return fail("aw_ldmm_alphas: the alphas come from the splatting gradient (IterateNew); "
+                "switch aw_ldmm_use_orig_gradient_calc off");
+  AW_CUDA(aw::ldmm_alphas(&l->ctx, I0, I1, v, alphas, S(stream)), "aw_ldmm_alphas");
   return 0;
 }
 

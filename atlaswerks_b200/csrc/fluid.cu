@@ -507,6 +507,11 @@ cudaError_t fluid_inverse_store(const FluidPlan &p, float *ox, float *oy, float 
   return cudaGetLastError();
 }
 
+cudaError_t fluid_inverse_compose(const FluidPlan &p, const ComposeArgs &a, cudaStream_t s) {
+  if (!p.fast) return cudaErrorNotSupported;
+  return fast_xy_inverse_compose(p, a, s);
+}
+
 cudaError_t fluid_inverse_store_neg(const FluidPlan &p, float *ox, float *oy, float *oz,
                                     cudaStream_t s) {
   DstNeg dst{{ox, oy, oz}};

@@ -228,6 +228,16 @@ struct DstAxpby {
   }
 };
 
+// The greedy update h'(x) = h(x + eps v(x)/sp) the inverse pass can apply
+// itself (fluid_inverse_compose): h in, h' out, the device-resident step,
+// the spacing divisors.
+struct ComposeArgs {
+  const float *hx, *hy, *hz;
+  float *ox, *oy, *oz;
+  const float *step;
+  DivF q0, q1, q2;
+};
+
 // host API (fluid.cu)
 int fluid_plan_create(FluidPlan *p, int nx, int ny, int nz, double spx, double spy, double spz,
                       float alpha, float beta, float gamma);
@@ -250,6 +260,10 @@ cudaError_t fluid_inverse_store(const FluidPlan &p, float *ox, float *oy, float 
                                 cudaStream_t s);
 cudaError_t fluid_inverse_store_neg(const FluidPlan &p, float *ox, float *oy, float *oz,
                                     cudaStream_t s);
+// v = K f never leaves the chip: h' = h(x + eps v/sp) from the inverse pass
+// itself (power-of-two grids: the register-FFT path); cudaErrorNotSupported
+// on other grids, where the caller stores v and updates separately
+cudaError_t fluid_inverse_compose(const FluidPlan &p, const ComposeArgs &a, cudaStream_t s);
 cudaError_t fluid_inverse_axpby(const FluidPlan &p, float *vx, float *vy, float *vz,
                                 const float *step, float sigma, cudaStream_t s);
 

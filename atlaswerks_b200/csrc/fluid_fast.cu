@@ -18,6 +18,7 @@
 //    the 128-byte swizzled layout (one 128-byte row per kz), each z-line
 //    transforms in place in its tile column, the 3x3 solve runs in the
 //    tiles, and TMA tensor stores write them back.
+#include <cooperative_groups.h>
 #include <cstdint>
 
 #include "bulk.cuh"
@@ -26,6 +27,8 @@
 #include "fluid_fast.cuh"
 
 namespace aw {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -168,91 +171,164 @@ __global__ void __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
   }
 }
 
+// Inverse y-transform of every column of the slab in shared memory, the
+// packed real columns 0 | NX/2 included.
+template <int NX, int NY>
+AW_D void inv_y_pass(float2 *C, const FluidPlan &p, int warp, int lane) {
+  using S = XYShape<NX, NY>;
+  constexpr int NXH = S::NXH, TY = S::TY, EY = S::EY;
+  constexpr int L = 32 / TY, NLINES = NX / 2, BC = NLINES >= 16 ? 16 : NLINES;
+  const int lw = lane / TY, t = lane % TY;
+  for (int base = warp * L; base < NLINES; base += kXYWarps * L) {
+    const int l = yline_col<TY, BC>(base + lw);
+    const bool packed = l == 0;
+    float2 *col = C + l;
+    float2 v[EY];
+#pragma unroll
+    for (int j = 0; j < EY; ++j) {
+      const int y = t + TY * j;
+      if (packed) {
+        const float2 a = C[y * NXH], b = C[y * NXH + NX / 2];
+        v[j] = make_float2(a.x - b.y, a.y + b.x);  // a + i b
+      } else {
+        v[j] = col[y * NXH];
+      }
+    }
+    line_fft<NY, +1>(v, t, [col](int m) { return col + m * NXH; }, p.ay.tw);
+#pragma unroll
+    for (int r = 0; r < EY; ++r) {
+      const int y = line_out_index<NY>(t, r);
+      if (packed) {
+        // real parts of the two columns; c2r ignores their imaginary parts
+        C[y * NXH] = make_float2(v[r].x, 0.f);
+        C[y * NXH + NX / 2] = make_float2(v[r].y, 0.f);
+      } else {
+        col[y * NXH] = v[r];
+      }
+    }
+  }
+}
+
+// Inverse x-transform (complex to real) of every row pair with Hermitian
+// completion; out(x, y, value) receives each real output. A row pair's lines
+// read and write only that pair's own slots, which hold 2 * NXH >= NX + 2
+// floats per row: an output may go back into its own row's slots once the
+// line's transform has returned (line_fft ends on a warp barrier).
+template <int NX, int NY, class Out>
+AW_D void inv_x_pass(float2 *C, const FluidPlan &p, int warp, int lane, const Out &out) {
+  using S = XYShape<NX, NY>;
+  constexpr int NXH = S::NXH, TX = S::TX, EX = S::EX;
+  constexpr int L = 32 / TX, NLINES = NY / 2;
+  const int lw = lane / TX, t = lane % TX;
+  for (int base = warp * L; base < NLINES; base += kXYWarps * L) {
+    const int y0 = 2 * xline_pair<TX>(base + lw);
+    float2 *row = C + y0 * NXH;
+    float2 v[EX];
+#pragma unroll
+    for (int j = 0; j < EX; ++j) {
+      const int k = t + TX * j;
+      const bool upper = k > NX / 2;
+      const int kk = upper ? NX - k : k;
+      float2 X0 = row[kk], X1 = row[NXH + kk];
+      if (kk == 0 || kk == NX / 2) { X0.y = 0.f; X1.y = 0.f; }
+      if (upper) { X0.y = -X0.y; X1.y = -X1.y; }
+      v[j] = make_float2(X0.x - X1.y, X0.y + X1.x);
+    }
+    line_fft<NX, +1>(v, t, [row](int m) { return row + m; }, p.ax.tw);
+#pragma unroll
+    for (int r = 0; r < EX; ++r) {
+      const int x = line_out_index<NX>(t, r);
+      out(x, y0, v[r].x);
+      out(x, y0 + 1, v[r].y);
+    }
+  }
+}
+
+// the slab of (z, comp), one bulk copy HBM -> shared; false (status word
+// set) when it never lands
+template <int NX, int NY>
+AW_D bool load_slab(float2 *C, uint64_t *mbar, const FluidPlan &p, int z, int comp) {
+  using S = XYShape<NX, NY>;
+  if (threadIdx.x == 0) {
+    const uint32_t bytes = (uint32_t)(sizeof(float2) * NY * S::NXH);
+    mbar_init(mbar, 1);
+    mbar_expect_tx(mbar, bytes);
+    bulk_load(C, p.spec + ((long)comp * p.d.nz + z) * NY * S::NXH, bytes, mbar);
+  }
+  __syncthreads();
+  return !__syncthreads_or(!mbar_wait(mbar, 0, p.status));
+}
+
 template <int NX, int NY, class Dst>
 __global__ void __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
     k_xy_inv_fast(FluidPlan p, Dst dst) {
-  using S = XYShape<NX, NY>;
-  constexpr int NXH = S::NXH, TX = S::TX, EX = S::EX, TY = S::TY, EY = S::EY;
   extern __shared__ __align__(128) float2 sm[];
   __shared__ uint64_t mbar;
   float2 *C = sm;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const Dims d = p.d;
   const int z = blockIdx.x, comp = blockIdx.y;
-  // the spectrum slab, one bulk copy HBM -> shared
-  if (threadIdx.x == 0) {
-    const uint32_t bytes = (uint32_t)(sizeof(float2) * NY * NXH);
-    mbar_init(&mbar, 1);
-    mbar_expect_tx(&mbar, bytes);
-    bulk_load(C, p.spec + ((long)comp * d.nz + z) * NY * NXH, bytes, &mbar);
-  }
-  __syncthreads();
   // a slab that never lands: the status word says so and the CTA leaves as one
-  if (__syncthreads_or(!mbar_wait(&mbar, 0, p.status))) return;
-
-  // ---- inverse y on columns; packed real columns 0 | NX/2 -----------------
-  {
-    constexpr int L = 32 / TY, NLINES = NX / 2, BC = NLINES >= 16 ? 16 : NLINES;
-    const int lw = lane / TY, t = lane % TY;
-    for (int base = warp * L; base < NLINES; base += kXYWarps * L) {
-      const int l = yline_col<TY, BC>(base + lw);
-      const bool packed = l == 0;
-      float2 *col = C + l;
-      float2 v[EY];
-#pragma unroll
-      for (int j = 0; j < EY; ++j) {
-        const int y = t + TY * j;
-        if (packed) {
-          const float2 a = C[y * NXH], b = C[y * NXH + NX / 2];
-          v[j] = make_float2(a.x - b.y, a.y + b.x);  // a + i b
-        } else {
-          v[j] = col[y * NXH];
-        }
-      }
-      line_fft<NY, +1>(v, t, [col](int m) { return col + m * NXH; }, p.ay.tw);
-#pragma unroll
-      for (int r = 0; r < EY; ++r) {
-        const int y = line_out_index<NY>(t, r);
-        if (packed) {
-          // real parts of the two columns; c2r ignores their imaginary parts
-          C[y * NXH] = make_float2(v[r].x, 0.f);
-          C[y * NXH + NX / 2] = make_float2(v[r].y, 0.f);
-        } else {
-          col[y * NXH] = v[r];
-        }
-      }
-    }
-  }
+  if (!load_slab<NX, NY>(C, &mbar, p, z, comp)) return;
+  inv_y_pass<NX, NY>(C, p, warp, lane);
   __syncthreads();
+  const auto o = dst.bind(comp);
+  inv_x_pass<NX, NY>(C, p, warp, lane,
+                     [&](int x, int y, float v) { o.store(d.idx(x, y, z), v); });
+}
 
-  // ---- inverse x: row pairs, Hermitian completion, real output ------------
-  {
-    const auto out = dst.bind(comp);
-    constexpr int L = 32 / TX, NLINES = NY / 2;
-    const int lw = lane / TX, t = lane % TX;
-    for (int base = warp * L; base < NLINES; base += kXYWarps * L) {
-      const int y0 = 2 * xline_pair<TX>(base + lw);
-      float2 *row = C + y0 * NXH;
-      float2 v[EX];
-#pragma unroll
-      for (int j = 0; j < EX; ++j) {
-        const int k = t + TX * j;
-        const bool upper = k > NX / 2;
-        const int kk = upper ? NX - k : k;
-        float2 X0 = row[kk], X1 = row[NXH + kk];
-        if (kk == 0 || kk == NX / 2) { X0.y = 0.f; X1.y = 0.f; }
-        if (upper) { X0.y = -X0.y; X1.y = -X1.y; }
-        v[j] = make_float2(X0.x - X1.y, X0.y + X1.x);
-      }
-      line_fft<NX, +1>(v, t, [row](int m) { return row + m; }, p.ax.tw);
-#pragma unroll
-      for (int r = 0; r < EX; ++r) {
-        const int x = line_out_index<NX>(t, r);
-        out.store(d.idx(x, y0, z), v[r].x);
-        out.store(d.idx(x, y0 + 1, z), v[r].y);
-      }
+// The inverse transform fused with the greedy update h'(x) = h(x + eps v(x)/sp)
+// (composeHV with PARTIAL_ID, HField3DUtils.txx:436-455, as k_update in
+// greedy.cu computes it). The three CTAs of a cluster hold the three
+// components of one z-slab: each transforms its component and keeps v in
+// its own shared memory, then each updates a third of the slab's rows,
+// reading the three components of v there through distributed shared
+// memory, so v never goes to HBM.
+template <int NX, int NY>
+__global__ void __cluster_dims__(1, 3, 1) __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
+    k_xy_inv_compose(FluidPlan p, ComposeArgs a) {
+  using S = XYShape<NX, NY>;
+  constexpr int NXH = S::NXH;
+  extern __shared__ __align__(128) float2 sm[];
+  __shared__ uint64_t mbar;
+  float2 *C = sm;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const Dims d = p.d;
+  const int z = blockIdx.x, comp = blockIdx.y;
+  cg::cluster_group cluster = cg::this_cluster();
+  // a slab that never lands: the status word says so; the CTA still takes
+  // part in both cluster barriers, so its partners never wait for it
+  const bool ok = load_slab<NX, NY>(C, &mbar, p, z, comp);
+  if (ok) {
+    inv_y_pass<NX, NY>(C, p, warp, lane);
+    __syncthreads();
+    inv_x_pass<NX, NY>(C, p, warp, lane, [C](int x, int y, float v) {
+      reinterpret_cast<float *>(C + y * NXH)[x] = v;
+    });
+  }
+  cluster.sync();  // all three components of v are in the cluster's shared memory
+  if (ok) {
+    const float *V0 = reinterpret_cast<const float *>(cluster.map_shared_rank(C, 0));
+    const float *V1 = reinterpret_cast<const float *>(cluster.map_shared_rank(C, 1));
+    const float *V2 = reinterpret_cast<const float *>(cluster.map_shared_rank(C, 2));
+    const float eps = *a.step;
+    constexpr int RPI = kXYThreads / NX;  // rows per pass
+    const int x = threadIdx.x % NX;
+    for (int y = comp + 3 * (threadIdx.x / NX); y < NY; y += 3 * RPI) {
+      const int e = y * 2 * NXH + x;
+      const float vx = V0[e], vy = V1[e], vz = V2[e];
+      const float px = fadd(__int2float_rn(x), fdivq(fmul(vx, eps), a.q0));
+      const float py = fadd(__int2float_rn(y), fdivq(fmul(vy, eps), a.q1));
+      const float pz = fadd(__int2float_rn(z), fdivq(fmul(vz, eps), a.q2));
+      float rx, ry, rz;
+      trilerp_vector(a.hx, a.hy, a.hz, d, px, py, pz, BG_PARTIAL_ID, 1.0f, rx, ry, rz);
+      const long i = d.idx(x, y, z);
+      a.ox[i] = rx;
+      a.oy[i] = ry;
+      a.oz[i] = rz;
     }
   }
+  cluster.sync();  // no CTA leaves while a partner may still read its v
 }
 
 // per-wavenumber solve of one (kx, ky, kz): the three components at b0p,
@@ -427,6 +503,7 @@ cudaError_t fast_configure(const FluidPlan &p) {
       set((const void *)k_xy_inv_fast<NX, NY, DstField>, sxy);
       set((const void *)k_xy_inv_fast<NX, NY, DstAxpby>, sxy);
       set((const void *)k_xy_inv_fast<NX, NY, DstNeg>, sxy);
+      set((const void *)k_xy_inv_compose<NX, NY>, sxy);
     });
   });
   dispatch_n(p.d.nz, [&](auto Z) {
@@ -454,6 +531,16 @@ cudaError_t fast_xy_inverse(const FluidPlan &p, const Dst &dst, cudaStream_t s) 
     dispatch_n(p.d.ny, [&](auto Y) {
       constexpr int NX = decltype(X)::value, NY = decltype(Y)::value;
       k_xy_inv_fast<NX, NY, Dst><<<dim3(p.d.nz, 3), kXYThreads, p.fast_smem_xy, s>>>(p, dst);
+    });
+  });
+  return cudaGetLastError();
+}
+
+cudaError_t fast_xy_inverse_compose(const FluidPlan &p, const ComposeArgs &a, cudaStream_t s) {
+  dispatch_n(p.d.nx, [&](auto X) {
+    dispatch_n(p.d.ny, [&](auto Y) {
+      constexpr int NX = decltype(X)::value, NY = decltype(Y)::value;
+      k_xy_inv_compose<NX, NY><<<dim3(p.d.nz, 3), kXYThreads, p.fast_smem_xy, s>>>(p, a);
     });
   });
   return cudaGetLastError();

@@ -16,6 +16,7 @@ template <class Src>
 cudaError_t fast_xy_forward(const FluidPlan &p, const Src &src, cudaStream_t s);
 template <class Dst>
 cudaError_t fast_xy_inverse(const FluidPlan &p, const Dst &dst, cudaStream_t s);
+cudaError_t fast_xy_inverse_compose(const FluidPlan &p, const ComposeArgs &a, cudaStream_t s);
 cudaError_t fast_z_solve(const FluidPlan &p, int inverse, cudaStream_t s);
 
 }  // namespace aw

@@ -543,6 +543,19 @@ cudaError_t greedy_stage(GreedyCtx *g, int stage, const float *I0, const float *
         k_update<<<row_grid(d), kRowThreads, 0, s>>>(a, d, g->st.step);
       return cudaGetLastError();
     }
+    case kStageInvCompose: {
+      // grids the fused kernel does not take run the two stages it replaces
+      if (!g->plan.fast) {
+        AW_TRY(greedy_stage(g, kStageXYInverse, I0, I1, h, h_out, hinv, hinv_out, auto_reduce,
+                            solve_inverse, s));
+        return greedy_stage(g, kStageUpdate, I0, I1, h, h_out, nullptr, nullptr, auto_reduce,
+                            solve_inverse, s);
+      }
+      const ComposeArgs a{h[0], h[1], h[2], h_out[0], h_out[1], h_out[2], g->st.step,
+                          make_divf((float)g->sp.x), make_divf((float)g->sp.y),
+                          make_divf((float)g->sp.z)};
+      return fluid_inverse_compose(g->plan, a, s);
+    }
   }
   return cudaErrorInvalidValue;
 }
@@ -550,10 +563,18 @@ cudaError_t greedy_stage(GreedyCtx *g, int stage, const float *I0, const float *
 // The energy sum runs on a side stream, concurrently with the transforms;
 // it joins before the step-size stage and the update, the two readers and
 // writers of the step it may reduce (AutoStepReduce).
+//
+// Without a step-size update or an inverse field, on the register-FFT path,
+// the inverse transform and the update are one kernel (kStageInvCompose):
+// v = K f stays in shared memory. The step update needs max |v| over the
+// whole field before any voxel moves, and the inverse field gathers v at
+// h^-1(x) anywhere in the volume, so those iterations store v.
 cudaError_t greedy_iterate(GreedyCtx *g, const float *I0, const float *I1, const float *const h[3],
                            float *const h_out[3], const float *const hinv[3],
                            float *const hinv_out[3], int update_step, int auto_reduce,
                            cudaStream_t s) {
+  const bool inv = hinv && hinv[0] && hinv_out && hinv_out[0];
+  const bool fuse = !update_step && !inv && !g->no_fused_update && g->plan.fast;
   AW_TRY(greedy_stage(g, kStageForcePrep, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
   AW_TRY(cudaEventRecord(g->ev_fork, s));
   AW_TRY(cudaStreamWaitEvent(g->aux, g->ev_fork, 0));
@@ -561,6 +582,11 @@ cudaError_t greedy_iterate(GreedyCtx *g, const float *I0, const float *I1, const
   AW_TRY(cudaEventRecord(g->ev_join, g->aux));
   AW_TRY(greedy_stage(g, kStageXYForward, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
   AW_TRY(greedy_stage(g, kStageZSolve, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
+  if (fuse) {
+    AW_TRY(cudaStreamWaitEvent(s, g->ev_join, 0));
+    return greedy_stage(g, kStageInvCompose, I0, I1, h, h_out, nullptr, nullptr, auto_reduce, 1,
+                        s);
+  }
   AW_TRY(greedy_stage(g, kStageXYInverse, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
   AW_TRY(cudaStreamWaitEvent(s, g->ev_join, 0));
   if (update_step)

@@ -32,6 +32,7 @@ struct GreedyCtx {
   GreedyDevState st;
   void *hmaps;      // host cache of the h planes' tensor maps (greedy.cu)
   int no_staged_update;  // 1: the update gathers h from global memory only
+  int no_fused_update;   // 1: v goes to HBM and a separate kernel updates h
   int utile;             // tile shape of the staged update (greedy.cu)
 };
 
@@ -44,7 +45,8 @@ enum GreedyStage {
   kStageXYInverse = 4,
   kStageMaxNorm = 5,
   kStageUpdate = 6,
-  kNumStages = 7
+  kStageInvCompose = 7,  // xy-inverse and update in one kernel (v stays on chip)
+  kNumStages = 8
 };
 
 int greedy_create(GreedyCtx *g, int nx, int ny, int nz, double spx, double spy, double spz,

@@ -420,24 +420,33 @@ void ldmm_destroy(LdmmCtx *c) {
 cudaError_t ldmm_iterate_orig(LdmmCtx *c, const float *I0, const float *I1, float *v,
                               int update_step, cudaStream_t s);
 
-cudaError_t ldmm_iterate(LdmmCtx *c, const float *I0, const float *I1, float *v, int update_step,
-                         cudaStream_t s) {
-  if (c->orig) return ldmm_iterate_orig(c, I0, I1, v, update_step, s);
+cudaError_t identity_field(float *hx, float *hy, float *hz, Dims d, cudaStream_t s) {
+  k_identity<<<row_grid(d), kRowThreads, 0, s>>>(hx, hy, hz, d);
+  return cudaGetLastError();
+}
+
+namespace {
+// IterateNew's forward integration (J0_t = I0 at the composed map of every
+// time point) and the residual J0_{T-1} - I1 with its energy partials; the
+// energy is recorded unless the step is being recomputed
+// (LDMMIteratorCPU.cxx:543-556, 616-627)
+cudaError_t ldmm_forward(LdmmCtx *c, const float *I0, const float *I1, const float *v,
+                         int update_step, cudaStream_t s) {
   const Dims d = c->d;
   const long n = d.n();
   const int T = c->T;
   float *H[2] = {c->hbuf, c->hbuf + 3 * n};
   auto comp = [&](float *base, int k) { return base + k * n; };
-  // forward integration
+  auto vcomp = [&](const float *base, int k) { return base + k * n; };
   k_identity<<<row_grid(d), kRowThreads, 0, s>>>(comp(H[0], 0), comp(H[0], 1), comp(H[0], 2), d);
   AW_TRY(cudaGetLastError());
   int cur = 0;
   for (int i = 0; i < T; ++i) {
-    float *vi = v + (long)i * 3 * n;
+    const float *vi = v + (long)i * 3 * n;
     k_forward_step<false><<<row_grid(d), kRowThreads, 0, s>>>(
-        comp(H[cur], 0), comp(H[cur], 1), comp(H[cur], 2), comp(vi, 0), comp(vi, 1), comp(vi, 2),
-        comp(H[1 - cur], 0), comp(H[1 - cur], 1), comp(H[1 - cur], 2), I0, c->J0 + (long)i * n,
-        d, c->sp);
+        comp(H[cur], 0), comp(H[cur], 1), comp(H[cur], 2), vcomp(vi, 0), vcomp(vi, 1),
+        vcomp(vi, 2), comp(H[1 - cur], 0), comp(H[1 - cur], 1), comp(H[1 - cur], 2), I0,
+        c->J0 + (long)i * n, d, c->sp);
     AW_TRY(cudaGetLastError());
     cur = 1 - cur;
   }
@@ -449,9 +458,60 @@ cudaError_t ldmm_iterate(LdmmCtx *c, const float *I0, const float *I1, float *v,
     k_record_energy<<<1, kRecThreads, 0, s>>>(c->partials, c->nparts, spprod, c->energy,
                                               c->count, c->cap);
     AW_TRY(cudaGetLastError());
-  } else {
-    AW_TRY(cudaMemsetAsync(c->maxbits, 0, sizeof(unsigned), s));
   }
+  return cudaSuccess;
+}
+
+// alpha_t = splat / sigma^2 in float, the factor (float)(1.0 / (sigma*sigma))
+// as Array3D::scale receives it (LDMMIteratorCPU.cxx:583-585)
+__global__ void __launch_bounds__(256)
+    k_scale_to(float *__restrict__ dst, const float *__restrict__ src, float f, long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = fmul(src[i], f);
+}
+}  // namespace
+
+// IterateNew with computeAlphasOnly (LDMMIteratorCPU.cxx:529-631): the
+// forward integration, the residual and its energy, then the backward sweep
+// of composeVHInv and splats, each splat scaled by 1/sigma^2 into
+// alphas[t]; v is left as it is.
+cudaError_t ldmm_alphas(LdmmCtx *c, const float *I0, const float *I1, const float *v,
+                        float *alphas, cudaStream_t s) {
+  const Dims d = c->d;
+  const long n = d.n();
+  const int T = c->T;
+  AW_TRY(ldmm_forward(c, I0, I1, v, 0, s));
+  float *H[2] = {c->hbuf, c->hbuf + 3 * n};
+  auto comp = [&](float *base, int k) { return base + k * n; };
+  k_identity<<<row_grid(d), kRowThreads, 0, s>>>(comp(H[0], 0), comp(H[0], 1), comp(H[0], 2), d);
+  AW_TRY(cudaGetLastError());
+  const float f = (float)(1.0 / (double)(c->sigma * c->sigma));
+  int cur = 0;
+  for (int t = T - 1; t >= 0; --t) {
+    const float *vt = v + (long)t * 3 * n;
+    const float *vv[3] = {vt, vt + n, vt + 2 * n};
+    const float *hh[3] = {comp(H[cur], 0), comp(H[cur], 1), comp(H[cur], 2)};
+    float *oo[3] = {comp(H[1 - cur], 0), comp(H[1 - cur], 1), comp(H[1 - cur], 2)};
+    AW_TRY(launch_compose_vh(vv, hh, oo, d, c->sp, -1, BG_PARTIAL_ZERO, nullptr, 1.0f, s));
+    cur = 1 - cur;
+    AW_TRY(splat(c->sw, c->diff, comp(H[cur], 0), comp(H[cur], 1), comp(H[cur], 2), c->S, 0.0f, s));
+    k_scale_to<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(alphas + (long)t * n, c->S, f, n);
+    AW_TRY(cudaGetLastError());
+  }
+  return cudaSuccess;
+}
+
+cudaError_t ldmm_iterate(LdmmCtx *c, const float *I0, const float *I1, float *v, int update_step,
+                         cudaStream_t s) {
+  if (c->orig) return ldmm_iterate_orig(c, I0, I1, v, update_step, s);
+  const Dims d = c->d;
+  const long n = d.n();
+  const int T = c->T;
+  float *H[2] = {c->hbuf, c->hbuf + 3 * n};
+  auto comp = [&](float *base, int k) { return base + k * n; };
+  AW_TRY(ldmm_forward(c, I0, I1, v, update_step, s));
+  if (update_step) AW_TRY(cudaMemsetAsync(c->maxbits, 0, sizeof(unsigned), s));
+  int cur = 0;
   // backward sweep
   k_identity<<<row_grid(d), kRowThreads, 0, s>>>(comp(H[0], 0), comp(H[0], 1), comp(H[0], 2), d);
   AW_TRY(cudaGetLastError());

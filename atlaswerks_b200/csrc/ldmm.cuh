@@ -69,6 +69,11 @@ cudaError_t ldmm_adshoot_iterate(LdmmCtx *c, const float *I0, const float *I1, f
 cudaError_t ldmm_adshoot_final_maps(LdmmCtx *c, float *phi0T, float *phiT0, cudaStream_t s);
 // One iteration (IterateNew or IterateOrig); v is [T][3][N]. update_step:
 // compute the step from max |2v - (2/sigma^2) K f| and leave v unchanged.
+// h(x) = x (HField3DUtils::setToIdentity), three planes of grid d
+cudaError_t identity_field(float *hx, float *hy, float *hz, Dims d, cudaStream_t s);
+// IterateNew's alphas only: alphas[t] = splat of the residual to t / sigma^2
+cudaError_t ldmm_alphas(LdmmCtx *c, const float *I0, const float *I1, const float *v,
+                        float *alphas, cudaStream_t s);
 cudaError_t ldmm_iterate(LdmmCtx *c, const float *I0, const float *I1, float *v, int update_step,
                          cudaStream_t s);
 

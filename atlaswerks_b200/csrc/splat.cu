@@ -165,37 +165,165 @@ AW_D float corner_weight(float px, float py, float pz, int cx, int cy, int cz) {
   return __double2float_rn(dmul(dmul(ax, ay), az));
 }
 
-// insertion sort of each bucket by source index (buckets are short); with
-// wts, then the eight corner weights (index dx + 2 dy + 4 dz) of the source
-// at every position of the bucket, once per sort: the gathers of every image
-// splatted by the same h read them instead of the source's h and the weight
-// arithmetic
-__global__ void __launch_bounds__(256)
-    k_bucket_sort(const int *__restrict__ offsets, int *__restrict__ order, long next,
-                  const float *__restrict__ hx, const float *__restrict__ hy,
-                  const float *__restrict__ hz, float *__restrict__ wts) {
-  const long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= next) return;
-  const int s = offsets[b], e = offsets[b + 1];
-  for (int i = s + 1; i < e; ++i) {
-    const int key = order[i];
-    int j = i - 1;
-    while (j >= s && order[j] > key) {
-      order[j + 1] = order[j];
-      --j;
-    }
-    order[j + 1] = key;
-  }
-  if (!wts) return;
-  for (int i = s; i < e; ++i) {
-    const int m = order[i];
-    const float px = __ldg(hx + m), py = __ldg(hy + m), pz = __ldg(hz + m);
-    float w[8];
+// the eight corner weights (index dx + 2 dy + 4 dz) of the source at sorted
+// position i
+AW_D void store_weights(const int *__restrict__ order, int i, const float *__restrict__ hx,
+                        const float *__restrict__ hy, const float *__restrict__ hz,
+                        float *__restrict__ wts) {
+  const int m = order[i];
+  const float px = __ldg(hx + m), py = __ldg(hy + m), pz = __ldg(hz + m);
+  float w[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) w[k] = corner_weight(px, py, pz, k & 1, (k >> 1) & 1, (k >> 2) & 1);
-    float4 *o = reinterpret_cast<float4 *>(wts + (long)i * 8);
-    o[0] = make_float4(w[0], w[1], w[2], w[3]);
-    o[1] = make_float4(w[4], w[5], w[6], w[7]);
+  for (int k = 0; k < 8; ++k) w[k] = corner_weight(px, py, pz, k & 1, (k >> 1) & 1, (k >> 2) & 1);
+  float4 *o = reinterpret_cast<float4 *>(wts + (long)i * 8);
+  o[0] = make_float4(w[0], w[1], w[2], w[3]);
+  o[1] = make_float4(w[4], w[5], w[6], w[7]);
+}
+
+// Buckets of up to kSmallBucket sources are insertion-sorted by one thread
+// (at most k(k-1)/2 moves); longer ones, which only a strongly compressing
+// or collapsed map produces, by the whole CTA with a stable radix sort.
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSmallBucket = 64;
+
+struct SortShared {
+  int large[kSortThreads];         // block-local indices of the long buckets
+  int nlarge;
+  int base[256];                   // running digit offsets within the segment
+  int wc[kSortWarps][256];         // per-warp digit counts of one 256-key tile
+  int red[2][kSortWarps];
+};
+
+// Stable LSD radix sort of the distinct source indices order[s, e) by the
+// whole CTA, 8 bits a pass over the keys' range, ping-ponging through
+// tmp[s, e). Every key's position comes from counts (no atomic order), so
+// the result is the ascending order whatever the input order; the work is
+// O(k) per pass and at most four passes.
+AW_D void block_radix_sort(int *__restrict__ order, int *__restrict__ tmp, int s, int e,
+                           SortShared &sh) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int mn = INT_MAX, mx = INT_MIN;
+  for (int i = s + tid; i < e; i += kSortThreads) {
+    const int k = order[i];
+    mn = min(mn, k);
+    mx = max(mx, k);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  if (lane == 0) {
+    sh.red[0][warp] = mn;
+    sh.red[1][warp] = mx;
+  }
+  __syncthreads();
+  mn = sh.red[0][0];
+  mx = sh.red[1][0];
+  for (int w = 1; w < kSortWarps; ++w) {
+    mn = min(mn, sh.red[0][w]);
+    mx = max(mx, sh.red[1][w]);
+  }
+  __syncthreads();
+  const unsigned range = (unsigned)mx - (unsigned)mn;
+  const int passes = range ? (32 - __clz((int)range) + 7) / 8 : 0;
+  int *src = order, *dst = tmp;
+  const unsigned lt = (1u << lane) - 1u;
+  for (int p = 0; p < passes; ++p) {
+    const int shift = 8 * p;
+    sh.base[tid] = 0;
+    __syncthreads();
+    for (int i = s + tid; i < e; i += kSortThreads)
+      atomicAdd(&sh.base[(((unsigned)src[i] - (unsigned)mn) >> shift) & 255u], 1);
+    __syncthreads();
+    {  // exclusive scan of the 256 digit counts, one per thread
+      const int c = sh.base[tid];
+      int incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (lane == 31) sh.red[0][warp] = incl;
+      __syncthreads();
+      int off = 0;
+      for (int w = 0; w < warp; ++w) off += sh.red[0][w];
+      sh.base[tid] = off + incl - c;
+      __syncthreads();
+    }
+    for (int t0 = s; t0 < e; t0 += kSortThreads) {
+      const int i = t0 + tid;
+      const bool valid = i < e;
+      const int key = valid ? src[i] : 0;
+      const int dg = valid ? (int)((((unsigned)key - (unsigned)mn) >> shift) & 255u) : 256;
+#pragma unroll
+      for (int w = 0; w < kSortWarps; ++w) sh.wc[w][tid] = 0;
+      __syncthreads();
+      const unsigned peers = __match_any_sync(0xffffffffu, dg);
+      if (valid && (__ffs(peers) - 1) == lane) sh.wc[warp][dg] = __popc(peers);
+      __syncthreads();
+      if (valid) {
+        int pre = sh.base[dg];
+        for (int w = 0; w < warp; ++w) pre += sh.wc[w][dg];
+        dst[s + pre + __popc(peers & lt)] = key;
+      }
+      __syncthreads();
+      int add = 0;
+#pragma unroll
+      for (int w = 0; w < kSortWarps; ++w) add += sh.wc[w][tid];
+      sh.base[tid] += add;
+      __syncthreads();
+    }
+    int *t = src;
+    src = dst;
+    dst = t;
+  }
+  if (src != order) {
+    for (int i = s + tid; i < e; i += kSortThreads) order[i] = src[i];
+  }
+  __syncthreads();
+}
+
+// Sorts every bucket by source index; with wts, then writes the eight corner
+// weights of the source at every sorted position, once per sort: the gathers
+// of every image splatted by the same h read them instead of the source's h
+// and the weight arithmetic. One CTA per 256 buckets; tmp (the scatter's
+// cursors, dead by now) holds at least n ints.
+__global__ void __launch_bounds__(kSortThreads)
+    k_bucket_sort(const int *__restrict__ offsets, int *__restrict__ order, int *__restrict__ tmp,
+                  long next, const float *__restrict__ hx, const float *__restrict__ hy,
+                  const float *__restrict__ hz, float *__restrict__ wts) {
+  __shared__ SortShared sh;
+  if (threadIdx.x == 0) sh.nlarge = 0;
+  __syncthreads();
+  const long b = (long)blockIdx.x * kSortThreads + threadIdx.x;
+  if (b < next) {
+    const int s = offsets[b], e = offsets[b + 1];
+    if (e - s <= kSmallBucket) {
+      for (int i = s + 1; i < e; ++i) {
+        const int key = order[i];
+        int j = i - 1;
+        while (j >= s && order[j] > key) {
+          order[j + 1] = order[j];
+          --j;
+        }
+        order[j + 1] = key;
+      }
+      if (wts)
+        for (int i = s; i < e; ++i) store_weights(order, i, hx, hy, hz, wts);
+    } else {
+      sh.large[atomicAdd(&sh.nlarge, 1)] = threadIdx.x;
+    }
+  }
+  __syncthreads();
+  const int nl = sh.nlarge;
+  for (int q = 0; q < nl; ++q) {
+    const long bb = (long)blockIdx.x * kSortThreads + sh.large[q];
+    const int s = offsets[bb], e = offsets[bb + 1];
+    block_radix_sort(order, tmp, s, e, sh);
+    if (wts)
+      for (int i = s + threadIdx.x; i < e; i += kSortThreads) store_weights(order, i, hx, hy, hz, wts);
   }
 }
 
@@ -326,8 +454,8 @@ cudaError_t splat_sort(const SplatWork &w, const float *hx, const float *hy, con
   k_scan_blocksums<<<1, kScanThreads, 0, s>>>(w.blocksums, w.nblocks);
   k_scan_apply<<<w.nblocks, kScanThreads, 0, s>>>(w.offsets, w.next, w.blocksums);
   k_scatter<<<row_grid(d), kRowThreads, 0, s>>>(hx, hy, hz, d, w.offsets, w.cursor, w.order);
-  k_bucket_sort<<<(int)((w.next + 255) / 256), 256, 0, s>>>(w.offsets, w.order, w.next, hx, hy,
-                                                            hz, w.wts);
+  k_bucket_sort<<<(int)((w.next + kSortThreads - 1) / kSortThreads), kSortThreads, 0, s>>>(
+      w.offsets, w.order, w.cursor, w.next, hx, hy, hz, w.wts);
   return cudaGetLastError();
 }
 

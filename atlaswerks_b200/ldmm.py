@@ -63,6 +63,8 @@ class LDMMIteratorB200:
         self._h = ctypes.c_void_p()
         self._update_step = False
         self._orig = False
+        self._alphas = None
+        self._alphas_valid = False
 
     def SetScaleLevel(self, size: Sequence[int], spacing: Sequence[float],
                       param: LDMMIteratorParam):
@@ -98,12 +100,32 @@ class LDMMIteratorB200:
         check(_lib.lib().aw_ldmm_get_step(self._h, ctypes.byref(s)))
         return float(s.value)
 
-    def Iterate(self, data: LDMMDeformationDataB200):
+    def Iterate(self, data: LDMMDeformationDataB200, computeAlphasOnly: bool = False):
+        """One iteration; with computeAlphasOnly the velocities stay as they
+        are and GetAlpha(t) returns the splatted residual at t over sigma^2
+        (LDMMIteratorGPU::Iterate(defData, computeAlphasOnly))."""
         if data.T != self.T:
             raise ValueError("data has a different number of time steps")
+        if computeAlphasOnly:
+            if self._alphas is None or self._alphas.shape[1:] != data.I0.shape:
+                self._alphas = torch.empty((self.T,) + tuple(data.I0.shape),
+                                           device=data.I0.device)
+            check(_lib.lib().aw_ldmm_alphas(self._h, data.I0.data_ptr(), data.I1.data_ptr(),
+                                            data.V.data_ptr(), self._alphas.data_ptr(),
+                                            _stream()))
+            self._alphas_valid = True
+            return
         check(_lib.lib().aw_ldmm_iterate(self._h, data.I0.data_ptr(), data.I1.data_ptr(),
                                          data.V.data_ptr(), int(self._update_step), _stream()))
         self._update_step = False
+        self._alphas_valid = False
+
+    def GetAlpha(self, t: int) -> torch.Tensor:
+        """alpha_t of the last Iterate(data, computeAlphasOnly=True); valid
+        until the next Iterate without it."""
+        if not self._alphas_valid:
+            raise RuntimeError("call Iterate(data, computeAlphasOnly=True) first")
+        return self._alphas[t]
 
     def Run(self, data: LDMMDeformationDataB200, n_iters: int, adaptive_first: bool = False):
         check(_lib.lib().aw_ldmm_run(self._h, data.I0.data_ptr(), data.I1.data_ptr(),

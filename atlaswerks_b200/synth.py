@@ -117,17 +117,20 @@ def bullseye(shape: Shape, radii: Sequence[float], center=None) -> np.ndarray:
 
 
 def atlas_subjects(n_subjects: int, seed: int, sizes=(96, 112, 128, 144, 160),
-                   n_blobs: int = 24, umax: float = 5.0):
+                   n_blobs: int = 24, umax: float = 5.0, grids=None):
     """Uneven-grid atlas inputs: a common blob template, sampled on each
     subject's grid (normalised coordinates), warped by its own smooth
-    displacement and scaled by U(0.9, 1.1)."""
+    displacement and scaled by U(0.9, 1.1). Each axis is drawn from `sizes`
+    unless `grids` gives every subject's (nx, ny, nz)."""
     rng = rng_for(seed)
     # template blob parameters in normalised [0,1]^3 coordinates
     params = [(rng.uniform(0.15, 0.85, 3), rng.uniform(0.03, 0.07), rng.uniform(0.3, 1.0))
               for _ in range(n_blobs)]
     subjects = []
-    for _ in range(n_subjects):
+    for k in range(n_subjects):
         nx, ny, nz = (int(rng.choice(sizes)) for _ in range(3))
+        if grids is not None:
+            nx, ny, nz = grids[k]
         z, y, x = np.meshgrid((np.arange(nz) + 0.5) / nz, (np.arange(ny) + 0.5) / ny,
                               (np.arange(nx) + 0.5) / nx, indexing="ij")
         img = np.zeros((nz, ny, nx), np.float64)

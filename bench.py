@@ -46,7 +46,7 @@ E2E_ITERS = 25  # the 128^3 level of the 3-level multiscale config
 # traffic of that kernel's function; spectrum = 3 complex64 x (nx/2+1)/nx)
 SPEC = 3 * 8 * (N // 2 + 1) / N  # bytes/voxel of the 3-channel half spectrum
 STAGE_NAMES = ["force_prep", "energy", "xy_forward_fft", "z_solve", "xy_inverse_fft",
-               "max_norm", "update"]
+               "max_norm", "update", "xy_inverse_update"]
 STAGE_BYTES = {
     "force_prep": 12 + 4 + 4 + 4,        # h, I1, I0 gather (once), I0(h) write
     "energy": 0,
@@ -55,8 +55,10 @@ STAGE_BYTES = {
     "xy_inverse_fft": SPEC + 12,         # spectrum read, v write
     "max_norm": 12,
     "update": 12 + 12 + 12,              # v, h gather (once), h' write
+    "xy_inverse_update": SPEC + 12 + 12,  # spectrum read, h gather (once), h' write
 }
 B_ITER = 92  # bytes/voxel of the fully fused 3-pass greedy iteration (each stream once)
+B_ITER_INV = B_ITER + 36  # with h^-1: its read and write, v gathered at h^-1
 
 
 def peaks():
@@ -120,19 +122,27 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference_iteration_rate(I0, I1, iters=2):
-    """Reference CPU (oracle/_ref) or, without it, the oracle port: 128^3
-    greedy iterations on one host thread. Returns (iters/s, kind)."""
-    import numpy as np  # noqa: F401
-    from oracle import REF_SO, Oracle, Reference
+def cpu_reference_iteration_rate(I0, I1, iters=4):
+    """Reference CPU (oracle/_ref) or, without it, the oracle port: steady-
+    state 128^3 greedy iterations on one host thread, after the handle and
+    iteration 0 (step update) are built untimed. Returns (iters/s, kind)."""
+    from oracle import REF_SO, Oracle, Reference, identity
     if os.path.exists(REF_SO):
         ref = Reference()
+        h = ref.greedy_open(I0, I1, max_pert=MAX_PERT, alpha=ALPHA, beta=BETA, gamma=GAMMA)
         t = time.perf_counter()
-        ref.greedy_run(I0, I1, [1], [iters], [MAX_PERT], alpha=ALPHA, beta=BETA, gamma=GAMMA)
-        return iters / (time.perf_counter() - t), "reference"
+        ref.greedy_iterate(h, iters)
+        dt = time.perf_counter() - t
+        ref.greedy_close(h)
+        return iters / dt, "reference"
     o = Oracle()
+    h = identity(I0.shape)
+    _, st = o.greedy_iterate(I0, I1, h, None, max_pert=MAX_PERT, alpha=ALPHA, beta=BETA,
+                             gamma=GAMMA, update_step=True)
     t = time.perf_counter()
-    o.greedy_run(I0, I1, iters, max_pert=MAX_PERT, alpha=ALPHA, beta=BETA, gamma=GAMMA)
+    for _ in range(iters):
+        o.greedy_iterate(I0, I1, h, None, max_pert=MAX_PERT, alpha=ALPHA, beta=BETA, gamma=GAMMA,
+                         step=st)
     return iters / (time.perf_counter() - t), "port"
 
 
@@ -155,55 +165,81 @@ def config(extra=None):
 
 
 def run_reference(args):
-    """CPU reference arm: all host threads (one 128^3 pair each, capped at 32
-    for memory), the reference's GreedyIteratorCPU through oracle/_ref."""
+    """CPU reference arm: the reference's GreedyIteratorCPU (oracle/_ref) on
+    all host threads, one 128^3 pair each (capped at 32 for memory). Each
+    thread builds its data object, iterator and FFT plans and runs iteration
+    0 (the step update) before the timed region; a step is one further
+    steady-state iteration of every thread's pair, the GPU arm's unit of
+    work. --warmup steps run untimed first, as in the GPU arm."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from oracle import REF_SO, Oracle, Reference
+    from oracle import REF_SO, Oracle, Reference, identity
     kind = "reference" if os.path.exists(REF_SO) else "port"
     cores = max(1, min(os.cpu_count() or 1, 32))
     pairs = [make_pair(1000 + t) for t in range(cores)]
+    if kind == "reference":
+        ref = Reference()
+        handles = [None] * cores
 
-    def worker(t, n_iters, out):
-        I0, I1 = pairs[t]
-        if kind == "reference":
-            Reference().greedy_run(I0, I1, [1], [n_iters], [MAX_PERT], alpha=ALPHA, beta=BETA,
-                                   gamma=GAMMA)
-        else:
-            Oracle().greedy_run(I0, I1, n_iters, max_pert=MAX_PERT, alpha=ALPHA, beta=BETA,
-                                gamma=GAMMA)
-        out[t] = n_iters
+        def opener(t):
+            handles[t] = ref.greedy_open(*pairs[t], max_pert=MAX_PERT, alpha=ALPHA, beta=BETA,
+                                         gamma=GAMMA)
 
-    def one_step():
-        out = [0] * cores
-        th = [threading.Thread(target=worker, args=(t, 1, out)) for t in range(cores)]
+        def worker(t):
+            ref.greedy_iterate(handles[t], 1)
+    else:
+        o = Oracle()
+        state = [None] * cores
+
+        def opener(t):
+            I0, I1 = pairs[t]
+            h = identity(I0.shape)
+            _, st = o.greedy_iterate(I0, I1, h, None, max_pert=MAX_PERT, alpha=ALPHA, beta=BETA,
+                                     gamma=GAMMA, update_step=True)
+            state[t] = (h, st)
+
+        def worker(t):
+            I0, I1 = pairs[t]
+            h, st = state[t]
+            o.greedy_iterate(I0, I1, h, None, max_pert=MAX_PERT, alpha=ALPHA, beta=BETA,
+                             gamma=GAMMA, step=st)
+
+    def parallel(fn):
+        th = [threading.Thread(target=fn, args=(t,)) for t in range(cores)]
         for x in th:
             x.start()
         for x in th:
             x.join()
-        return sum(out)
 
-    for _ in range(min(args.warmup, 1)):
-        one_step()
+    parallel(opener)
+    warmup = max(args.warmup, 3)
+    for _ in range(warmup):
+        parallel(worker)
     t = time.perf_counter()
-    done = 0
     for _ in range(args.steps):
-        done += one_step()
+        parallel(worker)
     dt = time.perf_counter() - t
-    value = done / dt
+    if kind == "reference":
+        for h in handles:
+            ref.greedy_close(h)
+    value = args.steps * cores / dt
     line = {"metric": "128^3 fluid iters/s", "value": value, "unit": "iters/s",
             "impl": "reference", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
-            "steps": args.steps, "warmup": min(args.warmup, 1),
+            "steps": args.steps, "warmup": warmup,
             "ms_per_step": 1000 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded blobs + smooth warp)",
             "config": config({"pairs_per_rank": cores, "iterations_per_step_per_rank": cores,
                               "workload": f"greedy-fluid pair registration, {N}^3 float32, one "
-                                          f"iteration of one pair per host thread per step"}),
+                                          f"steady-state iteration of one pair per host thread "
+                                          f"per step (handles built and iteration 0 run before "
+                                          f"the timed region)"}),
+            "fft": "the reference's DiffOper over an FP64 FFTW-API shim: FFTW is not installed, "
+                   "so single-precision FFTW would be faster than this arm",
             "cpu_baseline": {"value": value, "unit": "iters/s", "cores": cores, "kind": kind,
-                             "sample": f"{args.steps} steps x {cores} threads x 1 iteration of "
-                                       f"a {N}^3 pair (GreedyIteratorCPU; FFT = FP64 shim, "
-                                       f"not FFTW)"},
+                             "sample": f"{args.steps} steps x {cores} threads x 1 steady-state "
+                                       f"iteration of a {N}^3 pair (GreedyIteratorCPU; FFT = "
+                                       f"FP64 shim, not FFTW)"},
             "e2e": {"value": value, "unit": "iters/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -288,6 +324,49 @@ def run_b200(args):
     ms_per_step = ms / args.steps
     ms_per_iter = ms / per_rank_iters
 
+    # --- the same iterations maintaining the inverse field h^-1 too (the
+    # reference's default: WriteInvDefField, GreedyWarpParam.h:31): 36 more
+    # algorithmic bytes per voxel (h^-1 read, v gathered at h^-1, h^-1' write)
+    inv_datas = []
+    for it, (I0h, I1h) in zip(iters, host_pairs):
+        di = GreedyDeformationDataB200(torch.from_numpy(I0h).cuda(), torch.from_numpy(I1h).cuda(),
+                                       compute_inverse=True)
+        it.Run(di, 1, update_first=True)
+        inv_datas.append(di)
+
+    def inv_step():
+        fork = torch.cuda.Event()
+        fork.record(stream)
+        joins = []
+        for it, d, ps in zip(iters, inv_datas, pair_streams):
+            ps.wait_event(fork)
+            with torch.cuda.stream(ps):
+                it.Run(d, ITERS_PER_PAIR, update_first=False)
+                j = torch.cuda.Event()
+                j.record(ps)
+            joins.append(j)
+        for j in joins:
+            stream.wait_event(j)
+
+    for _ in range(3):
+        inv_step()
+    torch.cuda.synchronize()
+    inv_steps = max(args.steps // 2, 5)
+    i0 = torch.cuda.Event(enable_timing=True)
+    i1 = torch.cuda.Event(enable_timing=True)
+    i0.record(stream)
+    for _ in range(inv_steps):
+        inv_step()
+    i1.record(stream)
+    torch.cuda.synchronize()
+    inv_ms = i0.elapsed_time(i1)
+    if dist:
+        t = torch.tensor([inv_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        inv_ms = float(t.item())
+    inv_value = world * inv_steps * PAIRS * ITERS_PER_PAIR / (inv_ms / 1000.0)
+    del inv_datas
+
     # --- per-kernel roofline (pair 0, each stage timed alone with events) ---
     peak, peak_kind = peaks()
     it0, d0 = iters[0], datas[0]
@@ -298,7 +377,9 @@ def run_b200(args):
         it0._h, d0.I0.data_ptr(), d0.I1.data_ptr(), *[t.data_ptr() for t in h],
         *[t.data_ptr() for t in ho], *z, *z, 20, stream.cuda_stream, ms_stage))
     stage_ms = {n: float(ms_stage[i]) for i, n in enumerate(STAGE_NAMES)}
-    per_iter_stages = [n for n in STAGE_NAMES if n != "max_norm"]
+    # a steady-state iteration (no step update, no inverse field): the
+    # inverse transform and the update run as one kernel
+    per_iter_stages = ["force_prep", "energy", "xy_forward_fft", "z_solve", "xy_inverse_update"]
     dom = max(per_iter_stages, key=lambda n: stage_ms[n])
     nvox = N ** 3
     dom_bytes = STAGE_BYTES[dom] * nvox
@@ -316,6 +397,12 @@ def run_b200(args):
     iteration_roofline = {"bytes_per_iteration": B_ITER * nvox, "achieved": iter_gbs,
                           "peak": peak, "unit": "GB/s", "frac": iter_gbs / peak,
                           "stage_ms": stage_ms}
+    inv_gbs = B_ITER_INV * nvox * (inv_value / world) / 1e9
+    inverse_field = {"value": inv_value, "unit": "iters/s", "steps": inv_steps,
+                     "bytes_per_iteration": B_ITER_INV * nvox, "achieved": inv_gbs,
+                     "peak": peak, "frac": inv_gbs / peak,
+                     "workload": "the same pairs and iterations, h^-1 updated too "
+                                 "(composeVHInv, PARTIAL_ZERO)"}
 
     # --- end to end through the public API with host buffers ---
     # a step registers PAIRS pairs from pinned host memory, each on its own
@@ -383,22 +470,23 @@ def run_b200(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, kind = cpu_reference_iteration_rate(*host_pairs[0], iters=2)
+        rate, kind = cpu_reference_iteration_rate(*host_pairs[0], iters=4)
         cpu = {"value": rate, "unit": "iters/s", "cores": 1, "kind": kind,
-               "sample": f"2 greedy iterations of one {N}^3 pair on 1 host thread "
+               "sample": f"4 steady-state greedy iterations of one {N}^3 pair on 1 host thread "
                          f"(GreedyIteratorCPU{'' if kind == 'reference' else ' port'}; FFT = "
                          f"FP64 shim, not FFTW)"}
 
-    # six launches per iteration: force-prep, energy, xy-forward, z-solve,
-    # xy-inverse, update
-    launches = 6 * per_rank_iters
+    # five launches per steady-state iteration: force-prep, energy,
+    # xy-forward, z-solve, xy-inverse fused with the update
+    launches = 5 * per_rank_iters
     line = {"metric": "128^3 fluid iters/s", "value": value, "unit": "iters/s",
             "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded Gaussian blobs + smooth random warp, no dataset)",
             "config": config(), "roofline": roofline,
-            "iteration_roofline": iteration_roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "iteration_roofline": iteration_roofline, "inverse_field": inverse_field,
+            "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk.summary()}
     if dist:
@@ -490,25 +578,45 @@ def _atlas_subject(args):
 
 def run_atlas(args):
     """32 subjects, per-axis sizes in {96,...,160}, template 128^3, mean
-    every 10 iterations; a step = 10 iterations of every subject + the mean."""
+    every 10 iterations; a step = 10 iterations of every subject + the mean.
+    With N ranks (one per GPU), rank r owns subjects i mod N = r and the mean
+    is one NCCL all-reduce of the ranks' weighted sums per update (strong
+    scaling: the 32 subjects are the whole job)."""
     import multiprocessing as mp
 
-    import numpy as np
     import torch
 
-    from atlaswerks_b200.atlas import GreedyAtlasBuilderB200, GreedyAtlasParam
+    from atlaswerks_b200.atlas import GreedyAtlasBuilderB200, GreedyAtlasParam, local_subjects
     from atlaswerks_b200.greedy import DiffOperParam
     from atlaswerks_b200.synth import rng_for
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
     ns, T, period = 32, 128, 10
     rng = rng_for(4)
     params = [(rng.uniform(0.15, 0.85, 3), rng.uniform(0.03, 0.07), rng.uniform(0.3, 1.0))
               for _ in range(24)]
     sizes = [tuple(int(rng.choice([96, 112, 128, 144, 160])) for _ in range(3)) for _ in range(ns)]
+    mine = local_subjects(ns, rank, world)
+    # subject images are generated before the first CUDA call (spawned pool)
     with mp.get_context("spawn").Pool(min(32, os.cpu_count() or 1)) as pool:
-        imgs = pool.map(_atlas_subject, [(100 + i, params, sizes[i]) for i in range(ns)])
-    dev = [torch.from_numpy(a).cuda() for a in imgs]
+        imgs = pool.map(_atlas_subject, [(100 + i, params, sizes[i]) for i in mine])
+    torch.cuda.set_device(local)
+    dist = None
+    group = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        group = dist.group.WORLD
+    dev = [None] * ns
+    for i, a in zip(mine, imgs):
+        dev[i] = torch.from_numpy(a).cuda()
     b = GreedyAtlasBuilderB200(dev, (T, T, T), GreedyAtlasParam(DiffOperParam(ALPHA, BETA, GAMMA),
-                                                                 MAX_PERT, 100, period))
+                                                                 MAX_PERT, 100, period),
+                               group=group)
     b._update_mean()
     b.engine.iterate(2, True)
     stream = torch.cuda.current_stream()
@@ -517,24 +625,51 @@ def run_atlas(args):
         b.engine.iterate(period, False)
         b._update_mean()
 
-    ms, clocks = _timed(step, args.steps, args.warmup, stream)
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        s0.record(stream)
+        for _ in range(args.steps):
+            step()
+        s1.record(stream)
+        torch.cuda.synchronize()
+    ms = s0.elapsed_time(s1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    clocks = clk.summary()
     subj_iters = ns * period * args.steps
     value = subj_iters / (ms / 1000.0)
     peak, kind = peaks()
     gbs = B_ITER * T ** 3 * subj_iters / (ms / 1000.0) / 1e9
-    print(json.dumps({
+    line = {
         "metric": "atlas subject-iterations/s (template 128^3)", "value": value,
-        "unit": "subject-iters/s", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
-        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (24-blob template, per-subject "
-        "smooth warp max 5, intensity scale U(0.9,1.1))",
+        "unit": "subject-iters/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (24-blob template, per-subject smooth warp max 5, intensity scale "
+                "U(0.9,1.1))",
         "config": {"workload": "greedy atlas, 32 subjects of uneven grids {96..160}^3, deformations "
                    "on a 128^3 template grid, mean every 10 iterations", "subjects": ns,
-                   "subject_sizes": sizes, "template": [T, T, T], "mean_period": period},
-        "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
-                     "frac": gbs / peak, "traffic": None,
+                   "subject_sizes": sizes, "template": [T, T, T], "mean_period": period,
+                   "parallelism": f"subjects sharded over {world} rank(s), one all-reduce of the "
+                                  f"weighted sum per mean update"},
+        "roofline": {"bound": "hbm", "achieved": gbs / world, "peak": peak, "unit": "GB/s",
+                     "frac": gbs / world / peak, "traffic": None, "per": "GPU",
                      "algorithmic_bytes_per_subject_iteration": B_ITER * T ** 3},
-        "gpu_launches": (6 * period * ns + 1) * args.steps, "clocks": clocks}))
+        "gpu_launches": (6 * period * len(mine) + 1) * args.steps, "clocks": clocks}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
     return 0
 
 
@@ -700,6 +835,19 @@ def run_warmstart(args):
     return 0
 
 
+def _launch_ranks(n):
+    """--gpus n > 1 without a launcher: run this same command as n ranks,
+    one per GPU, through torch.distributed.run on 127.0.0.1."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port),
+           os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -715,15 +863,26 @@ def main():
     ap.add_argument("--grid", type=int, default=0, help="warmstart: pair grid (64 or 128; default 128)")
     ap.add_argument("--pairs", type=int, default=32, help="warmstart: held-out pairs")
     args = ap.parse_args()
+    if "WORLD_SIZE" in os.environ:
+        if int(os.environ["WORLD_SIZE"]) != args.gpus:
+            print(f"bench.py: --gpus {args.gpus} but the launcher started "
+                  f"{os.environ['WORLD_SIZE']} ranks", file=sys.stderr)
+            return 2
+    elif args.gpus > 1:
+        return _launch_ranks(args.gpus)
     if args.ncu_case:
         return run_ncu_case(args)
-    if args.workload != "greedy" and args.impl == "b200":
-        import torch
-        torch.cuda.set_device(0)
-        return {"atlas": run_atlas, "ldmm": run_ldmm, "ldmm_atlas": run_ldmm_atlas,
-                "warmstart": run_warmstart, "adshoot": run_adshoot}[args.workload](args)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "atlas":
+        return run_atlas(args)
+    if args.workload != "greedy":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0  # the other rows are single-GPU measurements
+        import torch
+        torch.cuda.set_device(0)
+        return {"ldmm": run_ldmm, "ldmm_atlas": run_ldmm_atlas, "warmstart": run_warmstart,
+                "adshoot": run_adshoot}[args.workload](args)
     return run_b200(args)
 
 

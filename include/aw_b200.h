@@ -85,6 +85,10 @@ int aw_compose_vh(const float *vx, const float *vy, const float *vz, const float
 int aw_splat(const float *img, const float *hx, const float *hy, const float *hz, float *out,
              int nx, int ny, int nz, float background, void *stream);
 
+/* h(x) = x on an nx x ny x nz grid, three planes
+ * (HField3DUtils::setToIdentity, UtilitiesDataTypes/HField3DUtils.txx:26-45). */
+int aw_identity(float *hx, float *hy, float *hz, int nx, int ny, int nz, void *stream);
+
 /* Gaussian downsampling of an image to a coarser grid (out: mx*my*mz):
  * ImageUtils::gaussianDownsample (UtilitiesDataTypes/ImageUtils.txx:259-298),
  * sigma = sqrt(n/m / 2) per axis, as MultiscaleManager::DownsampleToLevel
@@ -177,6 +181,13 @@ int aw_greedy_set_auto_step_reduce(aw_greedy_t g, int on);
  * ny >= 10, nz >= 6, no inverse field); 0: every gather from global memory.
  * Both give the same bits; the switch exists to compare them. */
 int aw_greedy_set_staged_update(aw_greedy_t g, int on);
+/* on = 1 (default): an iteration without a step-size update or an inverse
+ * field, on a grid of power-of-two axes, runs the inverse transform and the
+ * update h' = h(x + eps v/sp) as one kernel, so v = K f never goes to HBM
+ * (the stages GreedyIteratorGPU::Iterate runs as cplFFT inverse and
+ * composeHV, Greedy/GreedyIteratorGPU.cxx:120-134); 0: v is stored and the
+ * update is a kernel of its own. Both give the same bits. */
+int aw_greedy_set_fused_update(aw_greedy_t g, int on);
 /* Tile shape of the staged update (x 32 voxels; index 0: 8 x 4 in y x z,
  * 1: 4 x 8, 2: 8 x 8, 3: 16 x 2), chosen when the handle is created by
  * timing each on the device (kept per grid and device for the process).
@@ -203,9 +214,10 @@ int aw_greedy_run(aw_greedy_t g, const float *I0, const float *I1, float *hx, fl
 
 /* Per-kernel device time of one iteration: each stage (0 force-prep,
  * 1 energy, 2 xy-forward FFT, 3 z-solve, 4 xy-inverse FFT, 5 max-norm,
- * 6 update) is launched `reps` times back to back between CUDA events on
- * `stream`; ms_out[7] receives the mean milliseconds per launch. Leaves h_out
- * holding one iteration's result; records extra energies. Synchronises. */
+ * 6 update, 7 xy-inverse FFT fused with the update) is launched `reps` times
+ * back to back between CUDA events on `stream`; ms_out[8] receives the mean
+ * milliseconds per launch. Leaves h_out holding one iteration's result;
+ * records extra energies. Synchronises. */
 int aw_greedy_profile(aw_greedy_t g, const float *I0, const float *I1, const float *hx,
                       const float *hy, const float *hz, float *ox, float *oy, float *oz,
                       const float *hix, const float *hiy, const float *hiz, float *hiox,
@@ -213,6 +225,10 @@ int aw_greedy_profile(aw_greedy_t g, const float *I0, const float *I1, const flo
 
 /* Copies the energy history (oldest first) to host; synchronises. */
 int aw_greedy_get_energies(aw_greedy_t g, double *out, int max_count, int *count);
+/* The most recent energy only (GreedyDeformationData's LastEnergy, what
+ * GreedyIteratorGPU::Iterate adds to the data object in debug mode); waits
+ * for work queued on the legacy default stream. Error before any iteration. */
+int aw_greedy_last_energy(aw_greedy_t g, double *energy);
 
 /* ---------------------------------------------------------------------------
  * Greedy atlas building over the subjects resident on one GPU. Replaces the
@@ -278,6 +294,14 @@ int aw_ldmm_get_step(aw_ldmm_t l, float *step);
  * (UseAdaptiveStepSize, LDMM/LDMMWarp.txx:99-104). */
 int aw_ldmm_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *v, int update_step,
                     void *stream);
+/* LDMMIteratorCPU/GPU::Iterate(data, computeAlphasOnly = true) then GetAlpha(t)
+ * (LDMM/LDMMIteratorCPU.cxx:529-631, LDMMIteratorGPU.h:84-90): the forward
+ * integration and residual of IterateNew (its image energy recorded), then
+ * the backward sweep of composeVHInv and splats; alphas[t] (T x N floats) =
+ * splat of the residual to time t, times (float)(1 / sigma^2). v is not
+ * changed. IterateNew only (error with the Jacobian-transport gradient). */
+int aw_ldmm_alphas(aw_ldmm_t l, const float *I0, const float *I1, const float *v, float *alphas,
+                   void *stream);
 /* n_iters iterations replayed from a captured CUDA graph; adaptive_first=1
  * runs the step-size pass before the first iteration. */
 int aw_ldmm_run(aw_ldmm_t l, const float *I0, const float *I1, float *v, int n_iters,
@@ -414,6 +438,45 @@ int aw_nn_displacement_to_h(const float *pred, int D, int H, int W, float *hx, f
                             float *hz, void *stream);
 /* 1 in *timed_out when a GEMM gave up a bounded wait since the last call */
 int aw_nn_status(int *timed_out);
+
+/* ---------------------------------------------------------------------------
+ * The warm start as one handle (no counterpart in the reference): the
+ * trained encoder-decoder predicts a deformation for a pair, and the greedy
+ * iteration refines it, with the plain greedy solve from the identity as the
+ * fallback. The network runs on its own grid (axes multiples of 8, at most
+ * the pair's): the pair is Gaussian-downsampled to it (aw_downsample's
+ * filter) and the predicted deformation upsampled back with its vectors
+ * rescaled (aw_upsample_hfield). Unit spacing; fluid parameters alpha =
+ * beta = 0.01, gamma = 0.001.
+ * Parameters: host FP32, per layer in network order (e0a e0b e1a e1b e2a e2b
+ * e3a e3b d2a d2b d1a d1b d0a d0b head) the weights [Cout][taps][Cin] then
+ * the Cout biases; aw_warmstart_param_floats() of them in all. */
+size_t aw_warmstart_param_floats(void);
+typedef struct aw_warmstart_s *aw_warmstart_t;
+int aw_warmstart_create(int nx, int ny, int nz, int net_nx, int net_ny, int net_nz,
+                        const float *params, size_t n_params, float max_pert,
+                        aw_warmstart_t *out);
+int aw_warmstart_destroy(aw_warmstart_t w);
+/* h = the predicted deformation of the pair (device, pair grid). The
+ * prediction (downsampling, the network's 25 launches, upsampling) runs as
+ * one CUDA graph on the handle's stream, captured at the first call and
+ * again whenever the five pointers change; ordered after `stream`'s work
+ * and before its later work. */
+int aw_warmstart_predict(aw_warmstart_t w, const float *I0, const float *I1, float *hx, float *hy,
+                         float *hz, void *stream);
+/* Registration with the warm start: predict, then greedy iterations from
+ * the prediction (the step set at the first from its own velocity and
+ * halved whenever the energy rises) in chunks of `chunk`, until an
+ * iteration's energy sp^3 sum (I1 - I0(h))^2 is <= target_energy. A chunk
+ * that does not lower the best energy so far, or max_refine_iters without
+ * reaching the target, falls back to the plain solve from the identity for
+ * plain_iters iterations. h receives the result; *iters_run the iterations
+ * executed, *fell_back 1 when the fallback ran. Reads the energies back
+ * after every chunk (synchronises). */
+int aw_warmstart_register(aw_warmstart_t w, const float *I0, const float *I1,
+                          double target_energy, int max_refine_iters, int chunk, int plain_iters,
+                          float *hx, float *hy, float *hz, int *iters_run, int *fell_back,
+                          void *stream);
 
 #ifdef __cplusplus
 }

@@ -13,6 +13,8 @@
  * libaw_b200.so. All arithmetic runs in the library; this class forwards
  * the data object's device pointers and keeps the data object in step:
  * Def1To0 / Def0To1 updated in place, the step size, the energy record.
+ * The library's calls take the default stream (NULL), the stream the
+ * reference's GPU path uses.
  */
 #ifndef AW_B200_GREEDY_ITERATOR_HPP
 #define AW_B200_GREEDY_ITERATOR_HPP
@@ -65,15 +67,32 @@ class GreedyIteratorB200 : public DeformationIteratorInterface {
                            mCurSpacing.z, k->Alpha(), k->Beta(), k->Gamma(), param.MaxPert(),
                            &mHandle),
           "SetScaleLevel");
+    mStepKnown = false;  // a new handle starts from step 0
   }
 
   void UpdateStepSizeNextIteration() { mUpdateStep = true; }
 
-  /* GreedyIteratorGPU::Iterate */
+  /* GreedyIteratorGPU::Iterate. Everything is queued on the default stream
+   * without a host synchronisation, except where the data object needs a
+   * host value: the step after a step-size update, and the energy when the
+   * iterator was built with debug = true (as GreedyIteratorGPU computes the
+   * energy only then). The step goes to the device only when the data
+   * object's differs from the last one written or read. The library writes
+   * h' to this iterator's scratch (the update reads h around every voxel, so
+   * it cannot run in place) and an asynchronous device copy puts it back
+   * into the data object's planes, which may lie apart.
+   * Difference from the reference: GreedyDeformationData::AddEnergy halves
+   * the step when AutoStepReduce is set and the energy rose; the reference
+   * adds the energy before its update, this binding after it, so the halved
+   * step takes effect one iteration later. */
   void Iterate(DeformationDataInterface &deformationData) {
     GreedyDeformationDataGPU &data = dynamic_cast<GreedyDeformationDataGPU &>(deformationData);
     const size_t n = (size_t)mCurSize.x * mCurSize.y * mCurSize.z;
-    check(aw_greedy_set_step(mHandle, data.StepSize()), "Iterate (step)");
+    if (!mStepKnown || data.StepSize() != mStep) {
+      check(aw_greedy_set_step(mHandle, data.StepSize()), "Iterate (step)");
+      mStep = data.StepSize();
+      mStepKnown = true;
+    }
     cplVector3DArray &h = data.dDef1To0();
     float *s = mScratch, *si = mScratch + 3 * n;
     const bool inv = data.ComputeInverseHField();
@@ -83,21 +102,20 @@ class GreedyIteratorB200 : public DeformationIteratorInterface {
                             inv ? si : nullptr, inv ? si + n : nullptr, inv ? si + 2 * n : nullptr,
                             mUpdateStep ? 1 : 0, nullptr),
           "Iterate");
-    mUpdateStep = false;
-    // back into the data object's own buffers (its x, y, z may be apart)
     copy3(s, n, h);
     if (inv) copy3(si, n, *hi);
-    float step = 0.f;
-    check(aw_greedy_get_step(mHandle, &step), "Iterate (step)");
-    data.StepSize(step);
+    if (mUpdateStep) {
+      float step = 0.f;
+      check(aw_greedy_get_step(mHandle, &step), "Iterate (step)");
+      data.StepSize(step);
+      mStep = step;
+    }
+    mUpdateStep = false;
     if (mDebug) {
-      int count = 0;
-      check(aw_greedy_get_energies(mHandle, nullptr, 0, &count), "Iterate (energy)");
-      std::vector<double> all(count > 0 ? count : 1);
-      int got = 0;
-      check(aw_greedy_get_energies(mHandle, all.data(), count, &got), "Iterate (energy)");
+      double e = 0.0;
+      check(aw_greedy_last_energy(mHandle, &e), "Iterate (energy)");
       Energy energy;
-      energy.SetEnergy(got > 0 ? (Real)all[got - 1] : (Real)0);
+      energy.SetEnergy((Real)e);
       data.AddEnergy(energy);
     }
   }
@@ -108,10 +126,11 @@ class GreedyIteratorB200 : public DeformationIteratorInterface {
       throw AtlasWerksException(__FILE__, __LINE__,
                                 std::string("libaw_b200 ") + what + ": " + aw_last_error());
   }
+  /* stream-ordered device copies on the default stream, no host wait */
   static void copy3(const float *src, size_t n, cplVector3DArray &dst) {
     float *d[3] = {dst.x, dst.y, dst.z};
     for (int c = 0; c < 3; ++c)
-      if (cudaMemcpy(d[c], src + c * n, n * sizeof(float), cudaMemcpyDeviceToDevice) !=
+      if (cudaMemcpyAsync(d[c], src + c * n, n * sizeof(float), cudaMemcpyDeviceToDevice, 0) !=
           cudaSuccess)
         throw AtlasWerksException(__FILE__, __LINE__, "GreedyIteratorB200: field copy");
   }
@@ -119,6 +138,8 @@ class GreedyIteratorB200 : public DeformationIteratorInterface {
   aw_greedy_t mHandle = nullptr;
   float *mScratch = nullptr;
   bool mUpdateStep = false;
+  bool mStepKnown = false;  // mStep mirrors the device step
+  float mStep = 0.f;
   bool mDebug;
 };
 

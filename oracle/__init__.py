@@ -56,9 +56,16 @@ def build_oracle() -> None:
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-def build_reference(ref_root: str = "/root/reference") -> bool:
+def reference_root() -> str:
+    """Root of the reference source tree: $AW_REFERENCE_ROOT when set, else
+    the read-only checkout this build was developed against."""
+    return os.environ.get("AW_REFERENCE_ROOT", "/root/reference")
+
+
+def build_reference(ref_root: Optional[str] = None) -> bool:
     """Compile the reference CPU path into _ref/libawref.so when the
     reference tree is present. Returns True when the library exists."""
+    ref_root = ref_root or reference_root()
     if os.path.isdir(ref_root):
         subprocess.run(["make", "-s", "-j8", "-C", os.path.join(HERE, "ref"), f"REF={ref_root}"],
                        check=True)
@@ -220,6 +227,18 @@ class Oracle:
                                             _dbl(gamma), ctypes.c_float(sigma), ctypes.byref(st),
                                             _i(int(update_step)), ctypes.c_float(max_pert))
         return float(e), float(st.value)
+
+    def ldmm_alphas(self, I0, I1, v, sp=(1.0, 1.0, 1.0), sigma=0.1):
+        """IterateNew with computeAlphasOnly: alpha_t [T,nz,ny,nx]; returns
+        (alphas, image energy)."""
+        v = np.ascontiguousarray(v, np.float32)
+        T = v.shape[0]
+        out = np.empty((T,) + I0.shape, np.float32)
+        self.lib.aw_oracle_ldmm_alphas.restype = ctypes.c_double
+        e = self.lib.aw_oracle_ldmm_alphas(_fp(I0), _fp(I1), v.ctypes.data_as(_f), _i(T),
+                                           *_shape(I0), *map(_dbl, sp), ctypes.c_float(sigma),
+                                           out.ctypes.data_as(_f))
+        return out, float(e)
 
     def jacobian(self, v, sp=(1.0, 1.0, 1.0)):
         """|D(x*sp + v)| (HField3DUtils::jacobian of IterateOrig's map)."""
@@ -555,6 +574,28 @@ class Reference:
                                              *map(_dbl, sp), _dbl(alpha), _dbl(beta),
                                              _dbl(gamma), _i(int(inverse))))
         return o
+
+    def greedy_open(self, I0, I1, max_pert=0.5, alpha=0.01, beta=0.01, gamma=0.001,
+                    inverse=False):
+        """A single-scale GreedyIteratorCPU registration kept open (unit
+        spacing): builds the data object, iterator and FFT plans and runs
+        iteration 0 (the step update). Returns a handle for greedy_iterate."""
+        self.lib.awref_greedy_open.restype = ctypes.c_void_p
+        with quiet_stdout():
+            h = self.lib.awref_greedy_open(_fp(I0), _fp(I1), *_shape(I0), ctypes.c_float(max_pert),
+                                           _dbl(alpha), _dbl(beta), _dbl(gamma), _i(int(inverse)))
+        if not h:
+            raise RuntimeError(self.lib.awref_last_error().decode())
+        return ctypes.c_void_p(h)
+
+    def greedy_iterate(self, handle, n_iters=1) -> float:
+        """n_iters further GreedyIteratorCPU::Iterate calls; returns the last energy."""
+        e = ctypes.c_double()
+        self._check(self.lib.awref_greedy_iterate(handle, _i(n_iters), ctypes.byref(e)))
+        return float(e.value)
+
+    def greedy_close(self, handle):
+        self.lib.awref_greedy_close(handle)
 
     def greedy_run(self, I0, I1, factors: Sequence[int], iters: Sequence[int],
                    max_pert: Sequence[float], sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01,

@@ -636,6 +636,51 @@ double aw_oracle_ldmm_iterate(const float *I0, const float *I1, float *v, int T,
   return e;
 }
 
+/* LDMMIteratorCPU::IterateNew with computeAlphasOnly (LDMM/LDMMIteratorCPU.cxx:
+ * 543-586): the forward deformed images, the residual J0_{T-1} - I1, then per
+ * t from T-1 down: h = composeVHInv(v_t, h) [PARTIAL_ZERO], the residual
+ * splatted by h (forwardApply, normalize off) and scaled by
+ * (float)(1.0 / (sigma*sigma)) into alphas[t]. Returns the image energy. */
+double aw_oracle_ldmm_alphas(const float *I0, const float *I1, const float *v, int T, int nx,
+                             int ny, int nz, double spx, double spy, double spz, float sigma,
+                             float *alphas) {
+  const long n = (long)nx * ny * nz;
+  float *h = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *o = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *J = (float *)malloc(sizeof(float) * (size_t)n);
+  float *diff = (float *)malloc(sizeof(float) * (size_t)n);
+  aw_oracle_identity(h, h + n, h + 2 * n, nx, ny, nz);
+  for (int i = 0; i < T; ++i) {
+    const float *vi = v + (long)i * 3 * n;
+    aw_oracle_compose_hv(h, h + n, h + 2 * n, vi, vi + n, vi + 2 * n, o, o + n, o + 2 * n, nx, ny,
+                         nz, spx, spy, spz, -1, AW_BG_PARTIAL_ID);
+    memcpy(h, o, sizeof(float) * (size_t)(3 * n));
+  }
+  aw_oracle_apply(I0, h, h + n, h + 2 * n, J, nx, ny, nz, 0.0f);
+  double e = 0.0;
+  for (long k = 0; k < n; ++k) {
+    diff[k] = J[k] - I1[k];
+    e += (double)diff[k] * (double)diff[k];
+  }
+  e *= spx * spy * spz;
+  const float f = (float)(1.0 / (sigma * sigma));
+  aw_oracle_identity(h, h + n, h + 2 * n, nx, ny, nz);
+  for (int t = T - 1; t >= 0; --t) {
+    const float *vt = v + (long)t * 3 * n;
+    aw_oracle_compose_vh(vt, vt + n, vt + 2 * n, h, h + n, h + 2 * n, o, o + n, o + 2 * n, nx, ny,
+                         nz, spx, spy, spz, -1, AW_BG_PARTIAL_ZERO);
+    memcpy(h, o, sizeof(float) * (size_t)(3 * n));
+    float *a = alphas + (long)t * n;
+    aw_oracle_splat(diff, h, h + n, h + 2 * n, a, nx, ny, nz, 0.0f);
+    for (long k = 0; k < n; ++k) a[k] = a[k] * f;
+  }
+  free(h);
+  free(o);
+  free(J);
+  free(diff);
+  return e;
+}
+
 /* |D(x*sp + v)|: HField3DUtils::jacobian (UtilitiesDataTypes/HField3DUtils.txx:
  * 2374-2420) of the world-coordinate map that LDMMIteratorCPU::IterateOrig
  * forms (LDMM/LDMMIteratorCPU.cxx:409-417: identity scaled by the float

@@ -60,6 +60,9 @@ double aw_oracle_atlas_iterate(const float *I0, int mx, int my, int mz, const fl
 void aw_oracle_atlas_mean(const float *const *imgs, const int *dims, const float *const *h,
                           const float *w, int ns, float *mean, int nx, int ny, int nz);
 
+double aw_oracle_ldmm_alphas(const float *I0, const float *I1, const float *v, int T, int nx,
+                             int ny, int nz, double spx, double spy, double spz, float sigma,
+                             float *alphas);
 double aw_oracle_ldmm_iterate(const float *I0, const float *I1, float *v, int T, int nx, int ny,
                               int nz, double spx, double spy, double spz, double alpha,
                               double beta, double gamma, float sigma, float *step,

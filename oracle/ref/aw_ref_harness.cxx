@@ -313,6 +313,80 @@ int awref_greedy_run(const float *i0, const float *i1, int nx, int ny, int nz, d
   GUARD_END
 }
 
+/* A single-scale greedy registration kept open across calls, so a caller can
+ * time steady-state GreedyIteratorCPU::Iterate calls on one data object,
+ * iterator, DiffOper and FFT plan: awref_greedy_open builds them and runs
+ * iteration 0 (the step-size update of GreedyWarp.txx:99), awref_greedy_iterate
+ * runs further iterations at that step, awref_greedy_close frees it all. */
+struct AwRefGreedy {
+  GreedyParam param;
+  RealImage I0, I1;
+  MultiscaleManager *sm = nullptr;
+  GreedyDeformationData *data = nullptr;
+  GreedyIteratorCPU *it = nullptr;
+  unsigned iter = 0;
+  AwRefGreedy(const SizeType &size, const OriginType &o, const SpacingType &sp)
+      : I0(size, o, sp), I1(size, o, sp) {}
+  ~AwRefGreedy() {
+    delete it;
+    delete data;
+    delete sm;
+  }
+};
+
+void *awref_greedy_open(const float *i0, const float *i1, int nx, int ny, int nz, float maxpert,
+                        double alpha, double beta, double gamma, int compute_inverse) {
+  AwRefGreedy *g = nullptr;
+  try {
+    std::ostringstream xml;
+    xml.precision(17);
+    xml << "<GreedyWarpParameterFile><GreedyScaleLevel><ScaleLevel><DownsampleFactor val=\"1\"/>"
+        << "</ScaleLevel><GreedyIterator>" << diffoper_xml(alpha, beta, gamma)
+        << "<MaxPert val=\"" << maxpert << "\"/></GreedyIterator><NIterations val=\"1000000\"/>"
+        << "</GreedyScaleLevel><AutoStepReduce val=\"false\"/></GreedyWarpParameterFile>";
+    SizeType size(nx, ny, nz);
+    SpacingType sp(1.0, 1.0, 1.0);
+    OriginType origin(0, 0, 0);
+    g = new AwRefGreedy(size, origin, sp);
+    parse_into(g->param, xml.str());
+    to_im(i0, g->I0);
+    to_im(i1, g->I1);
+    g->sm = new MultiscaleManager(size, sp, origin, g->param);
+    g->sm->SetScaleVectorFields(true);
+    g->data = new GreedyDeformationData(&g->I0, &g->I1, g->param);
+    g->data->ComputeInverseHField(compute_inverse != 0);
+    g->it = new GreedyIteratorCPU(size, origin, sp, true);
+    g->data->InitializeWarp();
+    g->sm->SetScaleLevel(0);
+    g->it->SetScaleLevel(*g->sm, g->param.GetScaleLevel(0).Iterator());
+    g->data->SetScaleLevel(*g->sm);
+    g->data->SetCurIter(0);
+    g->it->UpdateStepSizeNextIteration();
+    g->it->Iterate(*g->data);
+    g->iter = 1;
+    return g;
+  } catch (const std::exception &e) {
+    g_err = e.what();
+  } catch (...) {
+    g_err = "unknown exception";
+  }
+  delete g;
+  return nullptr;
+}
+
+int awref_greedy_iterate(void *handle, int n_iters, double *last_energy) {
+  GUARD_BEGIN
+  AwRefGreedy *g = static_cast<AwRefGreedy *>(handle);
+  for (int k = 0; k < n_iters; ++k) {
+    g->data->SetCurIter(g->iter++);
+    g->it->Iterate(*g->data);
+  }
+  if (last_energy) *last_energy = g->data->GetEnergyHistory().LastEnergy()->GetEnergy();
+  GUARD_END
+}
+
+void awref_greedy_close(void *handle) { delete static_cast<AwRefGreedy *>(handle); }
+
 /* Greedy atlas on one node and one thread, one scale, equal grids: the loop
  * of AtlasThread::AtlasThreadMain (Algorithms/Common/AtlasThread.txx:97-181)
  * over the reference's GreedyDeformationData with I1 = the shared mean and

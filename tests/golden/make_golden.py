@@ -24,7 +24,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 sys.path.insert(0, os.path.dirname(HERE))
 
 from atlaswerks_b200.synth import atlas_subjects, bullseye, greedy_pair  # noqa: E402
-from oracle import REF_SO, Reference, build_reference, identity  # noqa: E402
+from oracle import REF_SO, Reference, build_reference, identity, reference_root  # noqa: E402
 from metaimage import read_mha, read_nhdr, rescale_intensities  # noqa: E402
 
 BG = ["partial_id", "id", "partial_zero", "zero", "clamp", "wrap"]
@@ -123,7 +123,7 @@ def adshoot_cases(ref):
     a0, p0, p1, ei, ev = ref.adshoot_run(I0, I1, 4, [(1, 5, 0.0002)], sp, sigma=1.0)
     save("adshoot_16x14x12_T4", I0=I0, I1=I1, sp=np.array(sp), alpha0=a0, phi0T=p0, phiT0=p1,
          img_energy=ei, vec_energy=ev)
-    root = "/root/reference/Testing"
+    root = os.path.join(reference_root(), "Testing")
     B0, bsp = read_nhdr(f"{root}/Data/Input/Bullseyes/BullseyeTestBlur00.nhdr")
     B1, _ = read_nhdr(f"{root}/Data/Input/Bullseyes/BullseyeTestBlur01.nhdr")
     base, _ = read_mha(f"{root}/Applications/LDMM/LDMMAdShootingWarp/Baseline/"

@@ -287,6 +287,37 @@ def test_staged_update_equals_global_gathers(shape, sp, max_pert):
     assert np.abs(out[0][0] - identity(shape)).max() > 0.5
 
 
+@pytest.mark.parametrize("shape,sp,max_pert", [((64, 64, 64), (1.0, 1.0, 1.0), 0.5),
+                                               ((16, 32, 128), (2.0, 1.3, 0.8), 3.0),
+                                               ((128, 128, 128), (1.0, 1.0, 1.0), 0.5),
+                                               ((32, 16, 16), (1.0, 1.0, 1.0), 2.0)])
+def test_fused_update_equals_separate_kernels(shape, sp, max_pert):
+    """The inverse transform fused with the update (v kept in the shared
+    memory of a three-CTA cluster) against v stored to HBM and the update
+    as a kernel of its own: bit-identical fields and energies, with large
+    steps that send corners outside the volume and with anisotropic spacing."""
+    from atlaswerks_b200 import _lib
+    I0, I1 = greedy_pair(shape, seed=13)
+    L = _lib.lib()
+    out = []
+    for fused in (0, 1):
+        it = GreedyIteratorB200(shape[::-1], spacing=sp)
+        it.SetScaleLevel(shape[::-1], sp, GreedyIteratorParam(DiffOperParam(0.01, 0.01, 0.001),
+                                                               max_pert))
+        _lib.check(L.aw_greedy_set_fused_update(it._h, fused))
+        d = GreedyDeformationDataB200(cu(I0), cu(I1), spacing=sp)
+        it.Run(d, 6, update_first=True)
+        d2 = GreedyDeformationDataB200(cu(I0), cu(I1), spacing=sp)
+        it.UpdateStepSizeNextIteration()
+        for _ in range(3):
+            it.Iterate(d2)
+        out.append((host(d.Def1To0()).copy(), it.Energies(), host(d2.Def1To0()).copy()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][2], out[1][2])
+    assert np.abs(out[0][0] - identity(shape)).max() > 0.1
+
+
 @pytest.mark.parametrize("shape", [(36, 31, 32), (48, 40, 44), (96, 80, 72)])
 def test_fluid_shapes_autotuned_and_result_independent(shape):
     """The shared-memory FFT path picks its launch shapes by timing at plan

@@ -56,6 +56,24 @@ def test_splat_compressing_map(oracle):
     assert np.array_equal(got, want)
 
 
+@pytest.mark.parametrize("shape,scale,shift", [
+    ((32, 32, 32), 0.0, 5.3),     # collapsed: every source in one cell (32768 sources)
+    ((32, 32, 32), 0.0, -0.5),    # collapsed onto the cell (-1, 0) of every axis
+    ((16, 16, 16), 0.2, 5.3),     # about 125 sources a cell: the CTA-wide sort
+    ((32, 32, 32), 0.1, 3.3),     # about 1000 sources a cell, many long buckets
+    ((24, 20, 28), 0.05, 1.1)])   # ragged grid, a few thousand sources a cell
+def test_splat_collapsing_maps(oracle, shape, scale, shift):
+    """Long buckets: bit-exact against forwardApply's source-order sums."""
+    rng = np.random.default_rng(15)
+    img = rng.random(shape, dtype=np.float32)
+    h = (identity(shape) * np.float32(scale) + np.float32(shift)).astype(np.float32)
+    want = oracle.splat(img, h)
+    got = host(D.splat(cu(img), cu(h)))
+    assert np.array_equal(got, want)
+    again = host(D.splat(cu(img), cu(h)))
+    assert np.array_equal(got, again)
+
+
 def test_splat_deterministic_and_adjoint():
     shape = (64, 64, 64)
     rng = np.random.default_rng(13)
@@ -102,6 +120,31 @@ def test_ldmm_iterations_vs_oracle(oracle, shape, T):
         assert err <= 1e-4, (k, err)
         data.V.copy_(cu(v))  # re-sync to the oracle's state
         assert abs(it.Energies()[-1] - e_o) <= 1e-5 * e_o
+
+
+@pytest.mark.parametrize("shape,T,sp", [((16, 16, 16), 4, (1.0, 1.0, 1.0)),
+                                        ((20, 18, 16), 3, (1.5, 0.75, 1.25))])
+def test_ldmm_alphas_vs_oracle(oracle, shape, T, sp):
+    """Iterate(computeAlphasOnly) + GetAlpha: bit-exact against the oracle's
+    restatement (compose, apply, splat and one float scale per voxel), v
+    unchanged, the image energy recorded."""
+    I0, I1 = greedy_pair(shape, seed=25, n_blobs=4, umax=2.0)
+    rng = np.random.default_rng(26)
+    v = rng.normal(0, 0.3, (T, 3) + shape).astype(np.float32)
+    nz, ny, nx = shape
+    it = LDMMIteratorB200((nx, ny, nz), spacing=sp, n_time_steps=T)
+    it.SetScaleLevel((nx, ny, nz), sp, LDMMIteratorParam(DiffOperParam(), 0.1, 0.005, False, 0.1))
+    data = LDMMDeformationDataB200(cu(I0), cu(I1), T)
+    data.V.copy_(cu(v))
+    it.Iterate(data, computeAlphasOnly=True)
+    want, e = oracle.ldmm_alphas(I0, I1, v, sp, sigma=0.1)
+    for t in range(T):
+        assert np.array_equal(host(it.GetAlpha(t)), want[t]), t
+    assert np.array_equal(host(data.V), v)
+    assert abs(it.Energies()[-1] - e) <= 1e-12 * e
+    it.Iterate(data)
+    with pytest.raises(RuntimeError):
+        it.GetAlpha(0)
 
 
 def test_ldmm_adaptive_step_vs_oracle(oracle):

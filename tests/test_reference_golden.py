@@ -13,8 +13,9 @@ import numpy as np
 import pytest
 
 from metaimage import read_mha, read_nhdr, rescale_intensities
+from oracle import reference_root
 
-REF = "/root/reference/Testing"
+REF = os.path.join(reference_root(), "Testing")
 pytestmark = pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
 
 

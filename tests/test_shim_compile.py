@@ -9,7 +9,9 @@ import subprocess
 
 import pytest
 
-REF = "/root/reference"
+from oracle import reference_root
+
+REF = reference_root()
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 TU = r"""
