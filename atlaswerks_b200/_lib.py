@@ -46,6 +46,7 @@ SIGNATURES = {
     "aw_compose_hv": ([_fp] * 9 + [_i] * 3 + [_d] * 3 + [_f, _i, _i, _fp], _i),
     "aw_compose_vh": ([_fp] * 9 + [_i] * 3 + [_d] * 3 + [_f, _i, _i, _fp], _i),
     "aw_splat": ([_fp] * 5 + [_i] * 3 + [_f, _fp], _i),
+    "aw_splat_static_fits": ([_i, _i, _i], _i),
     "aw_splat_static": ([_fp] * 5 + [_i] * 3 + [_f, _fp], _i),
     "aw_downsample": ([_fp, _i, _i, _i, _d, _d, _d, _fp, _i, _i, _i, _fp], _i),
     "aw_resample_image": ([_fp, _i, _i, _i, _d, _d, _d, _fp, _i, _i, _i, _d, _d, _d, _fp], _i),
@@ -69,6 +70,7 @@ SIGNATURES = {
     "aw_warmstart_destroy": ([_fp], _i),
     "aw_warmstart_predict": ([_fp] * 7, _i),
     "aw_warmstart_register": ([_fp, _fp, _fp, ctypes.c_double, _i, _i, _i] + [_fp] * 6, _i),
+    "aw_greedy_set_fast_interpolation": ([_fp, _i], _i),
     "aw_greedy_set_fused_update": ([_fp, _i], _i),
     "aw_greedy_update_tile": ([_fp, _i, _fp], _i),
     "aw_greedy_iterate": ([_fp] * 15 + [_i, _fp], _i),

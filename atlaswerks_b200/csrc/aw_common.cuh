@@ -123,14 +123,27 @@ AW_D double lerp_tree(const float c[8], double t, double u, double v, double omt
   return dadd(a, b);
 }
 
+// The same tree in float with fused multiply-adds, a + t (b - a) per lerp
+// (x first, then y, then z): the fast-interpolation mode. Not bit-identical
+// to the double tree; the difference is a few float ulps of the result.
+AW_D float lerpf(float a, float b, float t) { return fmaf(t, b - a, a); }
+AW_D float lerp_tree_f(const float c[8], float t, float u, float v) {
+  const float x00 = lerpf(c[0], c[1], t), x10 = lerpf(c[3], c[2], t);
+  const float x01 = lerpf(c[7], c[6], t), x11 = lerpf(c[4], c[5], t);
+  return lerpf(lerpf(x00, x10, u), lerpf(x01, x11, u), v);
+}
+
 // Scalar trilinear sample, background value per out-of-volume corner
 // (Array3DUtils::trilerp<T, BACKGROUND_STRATEGY_VAL>, Array3DUtils.txx:59-232).
+// FAST: the float tree (lerp_tree_f) on float fractions.
+template <bool FAST = false>
 AW_D float trilerp_scalar(const float *__restrict__ a, const Dims d, double x, double y, double z,
                           float bg) {
   const int fx = ref_floor_d(x), fy = ref_floor_d(y), fz = ref_floor_d(z);
   const int cx = fx + 1, cy = fy + 1, cz = fz + 1;
   const double t = dsub(x, (double)fx), u = dsub(y, (double)fy), v = dsub(z, (double)fz);
-  const double omt = dsub(1.0, t), omu = dsub(1.0, u), omv = dsub(1.0, v);
+  const double omt = FAST ? 0.0 : dsub(1.0, t), omu = FAST ? 0.0 : dsub(1.0, u),
+               omv = FAST ? 0.0 : dsub(1.0, v);
   float c[8];
   const bool inside = fx >= 0 && cx < d.nx && fy >= 0 && cy < d.ny && fz >= 0 && cz < d.nz;
   if (inside) {
@@ -157,6 +170,7 @@ AW_D float trilerp_scalar(const float *__restrict__ a, const Dims d, double x, d
     c[6] = (cxi && fyi && czi) ? __ldg(a + d.idx(cx, fy, cz)) : bg;
     c[7] = (fxi && fyi && czi) ? __ldg(a + d.idx(fx, fy, cz)) : bg;
   }
+  if (FAST) return lerp_tree_f(c, (float)t, (float)u, (float)v);
   return __double2float_rn(lerp_tree(c, t, u, v, omt, omu, omv));
 }
 
@@ -170,16 +184,19 @@ AW_D int safe_mod(int r, int m) {
 // fractional part formed in float, weights and sums in double. `scale`
 // multiplies each fetched corner value in float first (it reproduces
 // interpolating a field that the reference scaled in place beforehand);
-// pass 1.0f for none.
+// pass 1.0f for none. FAST: the float tree (lerp_tree_f).
+template <bool FAST = false>
 AW_D void trilerp_vector(const float *__restrict__ hx, const float *__restrict__ hy,
                          const float *__restrict__ hz, const Dims d, float x, float y, float z,
                          int bgs, float scale, float &ox, float &oy, float &oz) {
   int fx = ref_floor_f(x), fy = ref_floor_f(y), fz = ref_floor_f(z);
   int cx = fx + 1, cy = fy + 1, cz = fz + 1;
-  const double t = (double)fsub(x, __int2float_rn(fx));
-  const double u = (double)fsub(y, __int2float_rn(fy));
-  const double v = (double)fsub(z, __int2float_rn(fz));
-  const double omt = dsub(1.0, t), omu = dsub(1.0, u), omv = dsub(1.0, v);
+  const float tf = fsub(x, __int2float_rn(fx));
+  const float uf = fsub(y, __int2float_rn(fy));
+  const float vf = fsub(z, __int2float_rn(fz));
+  const double t = (double)tf, u = (double)uf, v = (double)vf;
+  const double omt = FAST ? 0.0 : dsub(1.0, t), omu = FAST ? 0.0 : dsub(1.0, u),
+               omv = FAST ? 0.0 : dsub(1.0, v);
   bool inside = true;
   if (bgs == BG_WRAP) {
     fx = safe_mod(fx, d.nx); fy = safe_mod(fy, d.ny); fz = safe_mod(fz, d.nz);
@@ -255,6 +272,12 @@ AW_D void trilerp_vector(const float *__restrict__ hx, const float *__restrict__
         cxv[c] = 0.f; cyv[c] = 0.f; czv[c] = 0.f;
       }
     }
+  }
+  if (FAST) {
+    ox = lerp_tree_f(cxv, tf, uf, vf);
+    oy = lerp_tree_f(cyv, tf, uf, vf);
+    oz = lerp_tree_f(czv, tf, uf, vf);
+    return;
   }
   ox = __double2float_rn(lerp_tree(cxv, t, u, v, omt, omu, omv));
   oy = __double2float_rn(lerp_tree(cyv, t, u, v, omt, omu, omv));

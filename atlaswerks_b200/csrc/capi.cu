@@ -382,6 +382,15 @@ int aw_greedy_set_fused_update(aw_greedy_t g, int on) {
   return 0;
 }
 
+int aw_greedy_set_fast_interpolation(aw_greedy_t g, int on) {
+  if (!g) return fail("aw_greedy_set_fast_interpolation: null handle");
+  AW_CUDA(cudaDeviceSynchronize(), "aw_greedy_set_fast_interpolation (pending work)");
+  g->ctx.fast_interp = on ? 1 : 0;
+  for (auto &kv : g->graphs) cudaGraphExecDestroy(kv.second);
+  g->graphs.clear();  // captured iterations hold the other kernels
+  return 0;
+}
+
 int aw_greedy_update_tile(aw_greedy_t g, int set, int *tile) {
   if (!g || !tile) return fail("aw_greedy_update_tile: null pointer");
   if (set) {
@@ -437,21 +446,40 @@ int aw_greedy_run(aw_greedy_t g, const float *I0, const float *I1, float *hx, fl
   float *AI[3] = {hix, hiy, hiz}, *BI[3] = {six, siy, siz};
   int done = 0;
   bool in_a = true;
-  auto one = [&](int upd) -> cudaError_t {
+  // Iterations without a step update end in the fused kernel, which can
+  // prepare the next iteration (I0(h') and its energy partials) so that the
+  // next one starts without a force-preparation kernel. Only inside this
+  // call: the first iteration always prepares itself, the last prepares
+  // nothing (the caller may change h between calls).
+  const bool ahead = aw::greedy_can_prep_ahead(&g->ctx, inv);
+  bool have = false;
+  auto one = [&](int upd, bool next) -> cudaError_t {
     float **src = in_a ? A : B, **dst = in_a ? B : A;
     float **isrc = in_a ? AI : BI, **idst = in_a ? BI : AI;
     const float *cs[3] = {src[0], src[1], src[2]}, *ci[3] = {isrc[0], isrc[1], isrc[2]};
+    const bool prep = next && ahead && !upd;
     cudaError_t e = aw::greedy_iterate(&g->ctx, I0, I1, cs, dst, inv ? ci : nullptr,
-                                       inv ? idst : nullptr, upd, g->auto_reduce, s);
+                                       inv ? idst : nullptr, upd, g->auto_reduce, s, have ? 1 : 0,
+                                       prep ? 1 : 0);
+    have = prep;
     in_a = !in_a;
     return e;
   };
   if (update_first) {
-    AW_CUDA(one(1), "aw_greedy_run (first iteration)");
+    AW_CUDA(one(1, false), "aw_greedy_run (first iteration)");
     ++done;
   }
-  // replay a captured pair of iterations (src->dst->src) as often as possible
-  const int pairs = (n_iters - done) / 2;
+  // the captured pair runs with the next iteration prepared on entry (when
+  // the handle prepares ahead): one lead-in iteration prepares the first
+  // replay, and one tail iteration follows the last
+  const int lead = (ahead && n_iters - done >= 3) ? 1 : 0;
+  if (lead) {
+    AW_CUDA(one(0, true), "aw_greedy_run (lead-in iteration)");
+    ++done;
+  }
+  // replay a captured pair of iterations (src->dst->src) as often as possible,
+  // keeping one iteration back for the tail when preparing ahead
+  const int pairs = (n_iters - done - lead) / 2;
   if (pairs > 0) {
     GraphKey key;
     std::memset(&key, 0, sizeof(key));
@@ -460,16 +488,17 @@ int aw_greedy_run(aw_greedy_t g, const float *I0, const float *I1, float *hx, fl
     const void *ptrs[14] = {I0,      I1,      src[0],  src[1],  src[2],  dst[0],  dst[1],
                             dst[2],  isrc[0], isrc[1], isrc[2], idst[0], idst[1], idst[2]};
     for (int i = 0; i < 14; ++i) key.p[i] = ptrs[i];
-    key.n = 2;
+    key.n = 2 + (lead ? 16 : 0);  // the prepared-on-entry pair is a different graph
     auto it = g->graphs.find(key);
     cudaGraphExec_t exec = nullptr;
     if (it == g->graphs.end()) {
       cudaGraph_t graph;
       AW_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "aw_greedy_run (capture)");
-      const bool start = in_a;
-      cudaError_t e1 = one(0), e2 = one(0);
+      const bool start = in_a, have0 = have;
+      cudaError_t e1 = one(0, lead != 0), e2 = one(0, lead != 0);
       cudaError_t ec = cudaStreamEndCapture(s, &graph);
       in_a = start;
+      have = have0;
       if (e1 != cudaSuccess) return cuda_fail(e1, "aw_greedy_run (captured iteration)");
       if (e2 != cudaSuccess) return cuda_fail(e2, "aw_greedy_run (captured iteration)");
       if (ec != cudaSuccess) return cuda_fail(ec, "aw_greedy_run (end capture)");
@@ -480,10 +509,10 @@ int aw_greedy_run(aw_greedy_t g, const float *I0, const float *I1, float *hx, fl
       exec = it->second;
     }
     for (int p = 0; p < pairs; ++p) AW_CUDA(cudaGraphLaunch(exec, s), "aw_greedy_run (launch)");
-    done += 2 * pairs;
+    done += 2 * pairs;  // the graph ends where it began: in_a and `have` as on entry
   }
-  if (done < n_iters) {
-    AW_CUDA(one(0), "aw_greedy_run (last iteration)");
+  while (done < n_iters) {
+    AW_CUDA(one(0, done + 1 < n_iters), "aw_greedy_run (remaining iteration)");
     ++done;
   }
   if (!in_a) {  // final field is in the scratch buffers: bring it home

@@ -10,12 +10,25 @@
 //   4. every lane takes E/T length-T DFTs.
 // Only __syncwarp separates the steps. On exit lane t holds
 //   v[i*T + k2] = X[(t + T*i) + E*k2],  i < E/T, k2 < T.
-// Twiddles come from the host-computed float table W_N^m (forward sign).
+// Twiddles come from the host-computed float table W_N^m (forward sign),
+// read from global memory or from a copy in shared memory (SmemTw).
 #pragma once
 
 #include "fft_smem.cuh"
 
 namespace aw {
+
+// A twiddle table the calling CTA copied into shared memory (the line
+// transforms read it instead of the global table: shorter latency, no L1
+// traffic competing with the producers' loads)
+struct SmemTw {
+  const float2 *p;
+};
+template <int SIGN>
+AW_D float2 twiddle(const SmemTw &tw, int m) {
+  const float2 w = tw.p[m];
+  return SIGN < 0 ? w : make_float2(w.x, -w.y);
+}
 
 template <int N>
 struct LineCfg;
@@ -99,8 +112,8 @@ struct DFT<SIGN, 16> {
 // writes and the column-wise reads on distinct banks. `t` is the lane within
 // the line. The lanes' inputs must already be in registers: the first write
 // to a slot comes after a __syncwarp.
-template <int N, int SIGN, class Slot>
-AW_D void line_fft(float2 *v, int t, const Slot &slot, const float2 *__restrict__ tw) {
+template <int N, int SIGN, class Slot, class Tw>
+AW_D void line_fft(float2 *v, int t, const Slot &slot, const Tw &tw) {
   constexpr int T = LineCfg<N>::T, E = LineCfg<N>::E;
   static_assert(E % T == 0, "line split");
   DFT<SIGN, E>::run(v);

@@ -107,24 +107,45 @@ struct SrcForce {
   }
   // Rows y0 and y0+1 of slab z at x = t + TX*j, j < E, as (row y0, row
   // y0+1): the same values as value(), from row pointers formed once and one
-  // code path per component. Needs nx, ny, nz >= 3 and an even ny.
+  // code path per component. Needs nx, ny, nz >= 3, an even ny, TX * E = nx
+  // and the TX lanes of a line consecutive within a warp, every lane of the
+  // warp calling it (the x neighbours come by shuffles).
   template <int E, int TX>
   AW_D void row_pair(int comp, int t, int y0, int z, const Dims &d, float2 *v) const {
     const long i0 = d.idx(t, y0, z);
     const int nx = d.nx;
     const float *g0p = G + i0, *g1p = g0p + nx, *a0p = A + i0, *b0p = B + i0;
     if (comp == 0) {
+      // the line covers the row (TX * E = nx): x +- 1 is held by the
+      // neighbouring lane at the same j, or by the line's first / last lane
+      // at j +- 1, so the neighbours come by shuffles instead of loads
+      float r0[E], r1[E];
 #pragma unroll
       for (int j = 0; j < E; ++j) {
+        r0[j] = __ldg(g0p + TX * j);
+        r1[j] = __ldg(g1p + TX * j);
+      }
+      const unsigned full = 0xffffffffu;
+      const int up = (t + 1) & (TX - 1), dn = (t - 1) & (TX - 1);
+#pragma unroll
+      for (int j = 0; j < E; ++j) {
+        const int jn = j + 1 < E ? j + 1 : j, jp = j > 0 ? j - 1 : j;
+        const float n0 = __shfl_sync(full, r0[j], up, TX), n1 = __shfl_sync(full, r1[j], up, TX);
+        const float w0 = __shfl_sync(full, r0[jn], 0, TX), w1 = __shfl_sync(full, r1[jn], 0, TX);
+        const float p0 = __shfl_sync(full, r0[j], dn, TX), p1 = __shfl_sync(full, r1[j], dn, TX);
+        const float q0 = __shfl_sync(full, r0[jp], TX - 1, TX),
+                    q1 = __shfl_sync(full, r1[jp], TX - 1, TX);
         const int x = t + TX * j;
-        const int lo = x > 0 ? -1 : 0, hi = x < nx - 1 ? 1 : 0;
-        const bool in = lo != 0 && hi != 0;
+        const bool first = x == 0, last = x == nx - 1, in = !first && !last;
+        // G[x + hi] and G[x + lo], hi = 0 at the last voxel, lo = 0 at the first
+        const float h0 = last ? r0[j] : (t == TX - 1 ? w0 : n0);
+        const float h1 = last ? r1[j] : (t == TX - 1 ? w1 : n1);
+        const float l0 = first ? r0[j] : (t == 0 ? q0 : p0);
+        const float l1 = first ? r1[j] : (t == 0 ? q1 : p1);
         const int o = TX * j;
-        const float g0 = __ldg(g0p + o), g1 = __ldg(g1p + o);
-        const float d0 = fsub(__ldg(g0p + o + hi), __ldg(g0p + o + lo));
-        const float d1 = fsub(__ldg(g1p + o + hi), __ldg(g1p + o + lo));
-        v[j] = make_float2(fmul(grad(d0, 0, in), mismatch(g0, __ldg(a0p + o), b0p + o)),
-                           fmul(grad(d1, 0, in), mismatch(g1, __ldg(a0p + o + nx), b0p + o + nx)));
+        v[j] = make_float2(fmul(grad(fsub(h0, l0), 0, in), mismatch(r0[j], __ldg(a0p + o), b0p + o)),
+                           fmul(grad(fsub(h1, l1), 0, in),
+                                mismatch(r1[j], __ldg(a0p + o + nx), b0p + o + nx)));
       }
     } else if (comp == 1) {
       // y0 - 1 (or y0 at the first row) and y0 + 2 (or y0 + 1 at the last)
@@ -228,6 +249,25 @@ struct DstAxpby {
   }
 };
 
+// The energy of an iteration, sp^3 sum (I1 - I0(h))^2 (GreedyIteratorCPU.cxx:
+// 113-121), is summed in two fixed stages: each warp of 32 consecutive x of a
+// row writes the double sum of its voxels' terms (a shuffle tree), then one
+// block sums the partials in a fixed order. The force preparation and the
+// fused inverse-and-update kernel (which prepares the next iteration) write
+// the same partials, so the energy does not depend on which one ran.
+AW_HD long energy_partials(const Dims &d) { return (long)d.nz * d.ny * ((d.nx + 31) / 32); }
+AW_D double energy_term(float idef, float i1) {
+  const float r = -fsub(idef, i1);
+  return (double)r * (double)r;
+}
+// every lane of the warp calls it with its voxel's term (0 outside the grid)
+AW_D void energy_partial(double e, int x, int y, int z, const Dims &d, double *partials) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+  const int nw = (d.nx + 31) / 32, w = x >> 5;
+  if ((threadIdx.x & 31) == 0 && w < nw) partials[((long)z * d.ny + y) * nw + w] = e;
+}
+
 // The greedy update h'(x) = h(x + eps v(x)/sp) the inverse pass can apply
 // itself (fluid_inverse_compose): h in, h' out, the device-resident step,
 // the spacing divisors.
@@ -236,6 +276,12 @@ struct ComposeArgs {
   float *ox, *oy, *oz;
   const float *step;
   DivF q0, q1, q2;
+  int fast;  // 1: float-tree interpolation (trilerp_vector<true>)
+  // non-null: also prepare the next iteration from h' (the force
+  // preparation's I0(h') into idef and its energy partials)
+  const float *I0, *I1;
+  float *idef;
+  double *partials;
 };
 
 // host API (fluid.cu)

@@ -41,7 +41,8 @@ struct XYShape {
   static constexpr int NXH = NX / 2 + 1;
   static constexpr int TX = LineCfg<NX>::T, EX = LineCfg<NX>::E;
   static constexpr int TY = LineCfg<NY>::T, EY = LineCfg<NY>::E;
-  static constexpr size_t smem() { return sizeof(float2) * (size_t)NY * NXH; }
+  // the slab, then copies of the x and y twiddle tables
+  static constexpr size_t smem() { return sizeof(float2) * ((size_t)NY * NXH + NX + NY); }
   // CTAs that fit one SM's shared memory, at most 3 (85 registers a thread)
   static constexpr int ctas() {
     return (int)((227u * 1024u) / (smem() + 1024u)) >= 3 ? 3
@@ -68,6 +69,16 @@ AW_D int yline_col(int g) {
   return g - r + (r % H) * (BC / H) + r / H;
 }
 
+// the x and y twiddle tables into shared memory after the slab; the
+// caller's next __syncthreads makes them visible
+template <int NX, int NY>
+AW_D SmemTw copy_twiddles(float2 *sm, const FluidPlan &p) {
+  float2 *tw = sm + (size_t)NY * XYShape<NX, NY>::NXH;
+  for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = __ldg(p.ax.tw + i);
+  for (int i = threadIdx.x; i < NY; i += blockDim.x) tw[NX + i] = __ldg(p.ay.tw + i);
+  return SmemTw{tw};
+}
+
 template <int NX, int NY, class Src>
 __global__ void __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
     k_xy_fwd_fast(FluidPlan p, Src src) {
@@ -78,6 +89,9 @@ __global__ void __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const Dims d = p.d;
   const int z = blockIdx.x, comp = blockIdx.y;
+  const SmemTw twx = copy_twiddles<NX, NY>(sm, p);
+  const SmemTw twy{twx.p + NX};
+  __syncthreads();
 
   // ---- x: row pairs (y0, y0+1) as one complex line, exchanged in place ----
   {
@@ -90,7 +104,7 @@ __global__ void __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
       float2 v[EX];
       src.template row_pair<EX, TX>(comp, t, y0, z, d, v);
       float2 *row = C + y0 * NXH;
-      line_fft<NX, -1>(v, t, [row](int m) { return row + m; }, p.ax.tw);
+      line_fft<NX, -1>(v, t, [row](int m) { return row + m; }, twx);
 #pragma unroll
       for (int r = 0; r < EX; ++r) row[line_out_index<NX>(t, r)] = v[r];
       __syncwarp();
@@ -134,7 +148,7 @@ __global__ void __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
         const int y = t + TY * j;
         v[j] = packed ? make_float2(C[y * NXH].x, C[y * NXH + NX / 2].x) : col[y * NXH];
       }
-      line_fft<NY, -1>(v, t, [col](int m) { return col + m * NXH; }, p.ay.tw);
+      line_fft<NY, -1>(v, t, [col](int m) { return col + m * NXH; }, twy);
 #pragma unroll
       for (int r = 0; r < EY; ++r) col[line_out_index<NY>(t, r) * NXH] = v[r];
       if (packed) {
@@ -174,7 +188,7 @@ __global__ void __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
 // Inverse y-transform of every column of the slab in shared memory, the
 // packed real columns 0 | NX/2 included.
 template <int NX, int NY>
-AW_D void inv_y_pass(float2 *C, const FluidPlan &p, int warp, int lane) {
+AW_D void inv_y_pass(float2 *C, const SmemTw &tw, int warp, int lane) {
   using S = XYShape<NX, NY>;
   constexpr int NXH = S::NXH, TY = S::TY, EY = S::EY;
   constexpr int L = 32 / TY, NLINES = NX / 2, BC = NLINES >= 16 ? 16 : NLINES;
@@ -194,7 +208,7 @@ AW_D void inv_y_pass(float2 *C, const FluidPlan &p, int warp, int lane) {
         v[j] = col[y * NXH];
       }
     }
-    line_fft<NY, +1>(v, t, [col](int m) { return col + m * NXH; }, p.ay.tw);
+    line_fft<NY, +1>(v, t, [col](int m) { return col + m * NXH; }, tw);
 #pragma unroll
     for (int r = 0; r < EY; ++r) {
       const int y = line_out_index<NY>(t, r);
@@ -215,7 +229,7 @@ AW_D void inv_y_pass(float2 *C, const FluidPlan &p, int warp, int lane) {
 // floats per row: an output may go back into its own row's slots once the
 // line's transform has returned (line_fft ends on a warp barrier).
 template <int NX, int NY, class Out>
-AW_D void inv_x_pass(float2 *C, const FluidPlan &p, int warp, int lane, const Out &out) {
+AW_D void inv_x_pass(float2 *C, const SmemTw &tw, int warp, int lane, const Out &out) {
   using S = XYShape<NX, NY>;
   constexpr int NXH = S::NXH, TX = S::TX, EX = S::EX;
   constexpr int L = 32 / TX, NLINES = NY / 2;
@@ -234,7 +248,7 @@ AW_D void inv_x_pass(float2 *C, const FluidPlan &p, int warp, int lane, const Ou
       if (upper) { X0.y = -X0.y; X1.y = -X1.y; }
       v[j] = make_float2(X0.x - X1.y, X0.y + X1.x);
     }
-    line_fft<NX, +1>(v, t, [row](int m) { return row + m; }, p.ax.tw);
+    line_fft<NX, +1>(v, t, [row](int m) { return row + m; }, tw);
 #pragma unroll
     for (int r = 0; r < EX; ++r) {
       const int x = line_out_index<NX>(t, r);
@@ -268,12 +282,14 @@ __global__ void __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const Dims d = p.d;
   const int z = blockIdx.x, comp = blockIdx.y;
+  const SmemTw twx = copy_twiddles<NX, NY>(sm, p);
+  const SmemTw twy{twx.p + NX};
   // a slab that never lands: the status word says so and the CTA leaves as one
   if (!load_slab<NX, NY>(C, &mbar, p, z, comp)) return;
-  inv_y_pass<NX, NY>(C, p, warp, lane);
+  inv_y_pass<NX, NY>(C, twy, warp, lane);
   __syncthreads();
   const auto o = dst.bind(comp);
-  inv_x_pass<NX, NY>(C, p, warp, lane,
+  inv_x_pass<NX, NY>(C, twx, warp, lane,
                      [&](int x, int y, float v) { o.store(d.idx(x, y, z), v); });
 }
 
@@ -284,7 +300,7 @@ __global__ void __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
 // its own shared memory, then each updates a third of the slab's rows,
 // reading the three components of v there through distributed shared
 // memory, so v never goes to HBM.
-template <int NX, int NY>
+template <int NX, int NY, bool FAST, bool PREP>
 __global__ void __cluster_dims__(1, 3, 1) __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
     k_xy_inv_compose(FluidPlan p, ComposeArgs a) {
   using S = XYShape<NX, NY>;
@@ -296,13 +312,15 @@ __global__ void __cluster_dims__(1, 3, 1) __launch_bounds__(kXYThreads, (XYShape
   const Dims d = p.d;
   const int z = blockIdx.x, comp = blockIdx.y;
   cg::cluster_group cluster = cg::this_cluster();
+  const SmemTw twx = copy_twiddles<NX, NY>(sm, p);
+  const SmemTw twy{twx.p + NX};
   // a slab that never lands: the status word says so; the CTA still takes
   // part in both cluster barriers, so its partners never wait for it
   const bool ok = load_slab<NX, NY>(C, &mbar, p, z, comp);
   if (ok) {
-    inv_y_pass<NX, NY>(C, p, warp, lane);
+    inv_y_pass<NX, NY>(C, twy, warp, lane);
     __syncthreads();
-    inv_x_pass<NX, NY>(C, p, warp, lane, [C](int x, int y, float v) {
+    inv_x_pass<NX, NY>(C, twx, warp, lane, [C](int x, int y, float v) {
       reinterpret_cast<float *>(C + y * NXH)[x] = v;
     });
   }
@@ -314,6 +332,7 @@ __global__ void __cluster_dims__(1, 3, 1) __launch_bounds__(kXYThreads, (XYShape
     const float eps = *a.step;
     constexpr int RPI = kXYThreads / NX;  // rows per pass
     const int x = threadIdx.x % NX;
+#pragma unroll 2
     for (int y = comp + 3 * (threadIdx.x / NX); y < NY; y += 3 * RPI) {
       const int e = y * 2 * NXH + x;
       const float vx = V0[e], vy = V1[e], vz = V2[e];
@@ -321,11 +340,19 @@ __global__ void __cluster_dims__(1, 3, 1) __launch_bounds__(kXYThreads, (XYShape
       const float py = fadd(__int2float_rn(y), fdivq(fmul(vy, eps), a.q1));
       const float pz = fadd(__int2float_rn(z), fdivq(fmul(vz, eps), a.q2));
       float rx, ry, rz;
-      trilerp_vector(a.hx, a.hy, a.hz, d, px, py, pz, BG_PARTIAL_ID, 1.0f, rx, ry, rz);
+      trilerp_vector<FAST>(a.hx, a.hy, a.hz, d, px, py, pz, BG_PARTIAL_ID, 1.0f, rx, ry, rz);
       const long i = d.idx(x, y, z);
       a.ox[i] = rx;
       a.oy[i] = ry;
       a.oz[i] = rz;
+      if (PREP) {
+        // the next iteration's force preparation at this voxel, from h' in
+        // registers: I0(h') and its energy term (k_force_prep's arithmetic);
+        // a warp holds 32 consecutive x of one row (NX >= 32)
+        const float w = trilerp_scalar<FAST>(a.I0, d, (double)rx, (double)ry, (double)rz, 0.0f);
+        a.idef[i] = w;
+        energy_partial(energy_term(w, __ldg(a.I1 + i)), x, y, z, d, a.partials);
+      }
     }
   }
   cluster.sync();  // no CTA leaves while a partner may still read its v
@@ -388,6 +415,10 @@ __global__ void __launch_bounds__(z_threads<NZ>(), (NZ <= 128 ? 3 : 1))
   __shared__ uint64_t mbar[3];
   // the swizzle pattern repeats every 1024 bytes: align the tiles to it
   float2 *TB = reinterpret_cast<float2 *>(smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u));
+  // the z twiddle table after the three tiles (visible after the first barrier)
+  float2 *twz = TB + 3 * TILE;
+  for (int i = threadIdx.x; i < NZ; i += blockDim.x) twz[i] = __ldg(p.az.tw + i);
+  const SmemTw tw{twz};
   const long ncols = (long)p.d.ny * p.nxh;
   const long j0 = (long)blockIdx.x * kZq;
   const int line = threadIdx.x / T, t = threadIdx.x % T;
@@ -418,7 +449,7 @@ __global__ void __launch_bounds__(z_threads<NZ>(), (NZ <= 128 ? 3 : 1))
   float2 v[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) v[j] = tile[zt(t + T * j, q)];
-  line_fft<NZ, -1>(v, t, [tile, q](int m) { return tile + zt(m, q); }, p.az.tw);
+  line_fft<NZ, -1>(v, t, [tile, q](int m) { return tile + zt(m, q); }, tw);
 #pragma unroll
   for (int r = 0; r < E; ++r) tile[zt(line_out_index<NZ>(t, r), q)] = v[r];
   if (__syncthreads_or(!ok)) return;  // a tile never landed: the status word says so
@@ -437,7 +468,7 @@ __global__ void __launch_bounds__(z_threads<NZ>(), (NZ <= 128 ? 3 : 1))
 
 #pragma unroll
   for (int j = 0; j < E; ++j) v[j] = tile[zt(t + T * j, q)];
-  line_fft<NZ, +1>(v, t, [tile, q](int m) { return tile + zt(m, q); }, p.az.tw);
+  line_fft<NZ, +1>(v, t, [tile, q](int m) { return tile + zt(m, q); }, tw);
 #pragma unroll
   for (int r = 0; r < E; ++r) tile[zt(line_out_index<NZ>(t, r), q)] = v[r];
 
@@ -486,7 +517,7 @@ size_t fast_xy_smem(int nx, int ny) {
 
 int fast_z_cols() { return kZq; }
 
-size_t fast_z_smem(int nz) { return sizeof(float2) * 3 * (size_t)nz * kZq + 1024; }
+size_t fast_z_smem(int nz) { return sizeof(float2) * (3 * (size_t)nz * kZq + nz) + 1024; }
 
 cudaError_t fast_configure(const FluidPlan &p) {
   cudaError_t e = cudaSuccess;
@@ -503,7 +534,10 @@ cudaError_t fast_configure(const FluidPlan &p) {
       set((const void *)k_xy_inv_fast<NX, NY, DstField>, sxy);
       set((const void *)k_xy_inv_fast<NX, NY, DstAxpby>, sxy);
       set((const void *)k_xy_inv_fast<NX, NY, DstNeg>, sxy);
-      set((const void *)k_xy_inv_compose<NX, NY>, sxy);
+      set((const void *)k_xy_inv_compose<NX, NY, false, false>, sxy);
+      set((const void *)k_xy_inv_compose<NX, NY, true, false>, sxy);
+      set((const void *)k_xy_inv_compose<NX, NY, false, true>, sxy);
+      set((const void *)k_xy_inv_compose<NX, NY, true, true>, sxy);
     });
   });
   dispatch_n(p.d.nz, [&](auto Z) {
@@ -540,7 +574,16 @@ cudaError_t fast_xy_inverse_compose(const FluidPlan &p, const ComposeArgs &a, cu
   dispatch_n(p.d.nx, [&](auto X) {
     dispatch_n(p.d.ny, [&](auto Y) {
       constexpr int NX = decltype(X)::value, NY = decltype(Y)::value;
-      k_xy_inv_compose<NX, NY><<<dim3(p.d.nz, 3), kXYThreads, p.fast_smem_xy, s>>>(p, a);
+      const dim3 grid(p.d.nz, 3);
+      const bool prep = a.idef != nullptr && NX >= 32;
+      if (a.fast && prep)
+        k_xy_inv_compose<NX, NY, true, true><<<grid, kXYThreads, p.fast_smem_xy, s>>>(p, a);
+      else if (a.fast)
+        k_xy_inv_compose<NX, NY, true, false><<<grid, kXYThreads, p.fast_smem_xy, s>>>(p, a);
+      else if (prep)
+        k_xy_inv_compose<NX, NY, false, true><<<grid, kXYThreads, p.fast_smem_xy, s>>>(p, a);
+      else
+        k_xy_inv_compose<NX, NY, false, false><<<grid, kXYThreads, p.fast_smem_xy, s>>>(p, a);
     });
   });
   return cudaGetLastError();

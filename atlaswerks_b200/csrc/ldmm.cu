@@ -323,17 +323,22 @@ __global__ void __launch_bounds__(kRowThreads)
   }
 }
 
-// partials of sum_c sum_x (L v0)_c v0_c (HField3DUtils::l2DotProd), float
-// products summed in double
+// partials of <L v, v> for v = sign * K f without applying L: L K f = f,
+// so it is sum_c sum_x (sign f_c) v_c with the body force f = grad(G) A
+// formed again on the fly as the forward transform formed it (SrcForce);
+// float products summed in double, as HField3DUtils::l2DotProd sums
+// (L v)_c v_c. Equal to the explicit L v route up to the transforms' float
+// rounding.
 __global__ void __launch_bounds__(kRowThreads)
-    k_ad_vdot(const float *__restrict__ u, const float *__restrict__ v0,
-              double *__restrict__ partials, Dims d) {
-  Voxel v;
+    k_force_vdot(SrcForce f, const float *__restrict__ v, float sign,
+                 double *__restrict__ partials, Dims d) {
+  Voxel p;
   double e = 0.0;
-  if (voxel_of(d, v)) {
+  if (voxel_of(d, p)) {
     const long n = d.n();
 #pragma unroll
-    for (int c = 0; c < 3; ++c) e += (double)fmul(u[c * n + v.i], v0[c * n + v.i]);
+    for (int c = 0; c < 3; ++c)
+      e += (double)fmul(sign * f.value(c, p.x, p.y, p.z, d), v[c * n + p.i]);
   }
   __shared__ double ws[kRowThreads / 32];
   e = warp_sum(e);
@@ -411,7 +416,7 @@ void ldmm_destroy(LdmmCtx *c) {
   fluid_plan_destroy(&c->plan);
   void *ptrs[] = {c->J0,     c->hbuf,   c->diff, c->S,   c->u,   c->splat_scratch,
                   c->partials, c->energy, c->scalars, c->JT, c->JD, c->adV,
-                  c->adP,    c->adA,    c->adI,  c->venergy, c->adSortMem, c->lv};
+                  c->adP,    c->adA,    c->adI,  c->venergy, c->adSortMem};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   std::memset(c, 0, sizeof(*c));
@@ -643,7 +648,6 @@ __global__ void k_shoot_alpha(float *__restrict__ a0, const float *__restrict__ 
 // I0(phiT0) in J0[0]. Records the image energy sp^3 sum (I0(phiT0) - I1)^2.
 cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, float *alpha0,
                                float *phi0T, float *phiT0, cudaStream_t s) {
-  if (!c->lv) return cudaErrorNotReady;
   const Dims d = c->d;
   const long n = d.n();
   const int T = c->T;
@@ -654,15 +658,14 @@ cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, flo
   const double spprod = c->sp.x * c->sp.y * c->sp.z;
   int vt = 0;  // velocities formed so far
   // v = K(grad(G) alpha_t), then its step energy <L v, v> added to this
-  // iteration's vector energy (LDMMShootingIteratorCPU.cxx:216-221, 257-262)
+  // iteration's vector energy (LDMMShootingIteratorCPU.cxx:216-221, 257-262),
+  // as <f, v> (k_force_vdot): no second transform
   auto velocity = [&](const float *G) -> cudaError_t {
     AW_TRY(fluid_forward_force(c->plan, G, aT, 0, s));
     AW_TRY(fluid_solve(c->plan, 1, s));
     AW_TRY(fluid_inverse_store(c->plan, comp(v, 0), comp(v, 1), comp(v, 2), s));
-    AW_TRY(fluid_forward_field(c->plan, comp(v, 0), comp(v, 1), comp(v, 2), s));
-    AW_TRY(fluid_solve(c->plan, 0, s));
-    AW_TRY(fluid_inverse_store(c->plan, comp(c->lv, 0), comp(c->lv, 1), comp(c->lv, 2), s));
-    k_ad_vdot<<<row_grid(d), kRowThreads, 0, s>>>(c->lv, v, c->partials, d);
+    k_force_vdot<<<row_grid(d), kRowThreads, 0, s>>>(make_force(G, aT, 0, c->sp), v, 1.0f,
+                                                      c->partials, d);
     AW_TRY(cudaGetLastError());
     k_record_energy<<<1, kRecThreads, 0, s>>>(c->partials, c->nparts, spprod, c->venergy,
                                               c->count, c->cap, 0, vt++ > 0);
@@ -734,15 +737,8 @@ int ldmm_adshoot_prepare(LdmmCtx *c) {
   return 0;
 }
 
-int ldmm_shoot_prepare(LdmmCtx *c) {
-  if (c->lv) return 0;
-  if (cudaMalloc(&c->lv, sizeof(float) * 3 * (size_t)c->d.n()) != cudaSuccess) {
-    cudaGetLastError();
-    c->lv = nullptr;
-    return 3;
-  }
-  return 0;
-}
+// the momentum shooting needs no device memory beyond the handle's own
+int ldmm_shoot_prepare(LdmmCtx *) { return 0; }
 
 // LDMMAdShootingIteratorCPU::Iterate (LDMM/LDMMAdShootingIteratorCPU.cxx:
 // 237-323) and backwardAdIntegration (:325-431).
@@ -817,12 +813,12 @@ cudaError_t ldmm_adshoot_iterate(LdmmCtx *c, const float *I0, const float *I1, f
   }
   AW_TRY(advance(T));
 
-  // energies: <L v0, v0> (recorded without advancing the count), then the image term
+  // energies: <L v0, v0> (recorded without advancing the count), then the
+  // image term; v0 = -K f0 with f0 = grad(I0) alpha0, so L v0 = -f0 and the
+  // product is formed from the force again (k_force_vdot), no second transform
   const double spprod = c->sp.x * c->sp.y * c->sp.z;
-  AW_TRY(fluid_forward_field(c->plan, comp(V(0), 0), comp(V(0), 1), comp(V(0), 2), s));
-  AW_TRY(fluid_solve(c->plan, 0, s));
-  AW_TRY(fluid_inverse_store(c->plan, comp(c->u, 0), comp(c->u, 1), comp(c->u, 2), s));
-  k_ad_vdot<<<grid, kRowThreads, 0, s>>>(c->u, V(0), c->partials, d);
+  k_force_vdot<<<grid, kRowThreads, 0, s>>>(make_force(I0, alpha0, 0, c->sp), V(0), -1.0f,
+                                             c->partials, d);
   AW_TRY(cudaGetLastError());
   k_record_energy<<<1, kRecThreads, 0, s>>>(c->partials, c->nparts, spprod, c->venergy,
                                             c->count, c->cap, 0);

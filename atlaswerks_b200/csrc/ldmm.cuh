@@ -41,7 +41,6 @@ struct LdmmCtx {
   float *adI;       // 6N: alphaHat, IHat, alphaTilde, ITilde and two scratch images
   double *venergy;  // vector-energy history ring, indexed like energy
   void *adSortMem;  // T + 1 splat scratch sets
-  float *lv;        // 3N: L v_t for the momentum shooting's vector energy
   SplatWork adSort[kMaxAdSorts];  // the sorts by phi0T_t (t = 1..T) and by phiT0_T (slot 0)
 };
 

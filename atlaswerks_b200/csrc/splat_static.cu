@@ -56,6 +56,14 @@ int scratch_address(void **out) {
 
 extern "C" {
 
+int aw_splat_static_fits(int nx, int ny, int nz) {
+  if (nx < 1 || ny < 1 || nz < 1) return 0;
+  return aw::splat_scratch_bytes(aw::Dims{nx, ny, nz}, false) <=
+                 (size_t)AW_SPLAT_STATIC_MAX_BYTES
+             ? 1
+             : 0;
+}
+
 int aw_splat_static(const float *img, const float *hx, const float *hy, const float *hz,
                     float *out, int nx, int ny, int nz, float background, void *stream) {
   if (!img || !hx || !hy || !hz || !out) return fail_static("aw_splat_static: null pointer");

@@ -171,6 +171,11 @@ class GreedyIteratorB200:
     def UpdateStepSizeNextIteration(self):
         self._update_step = True
 
+    def SetFastInterpolation(self, on: bool):
+        """Float fused-multiply-add interpolation in the force preparation
+        and the fused update (a few float ulps from the bit-exact path)."""
+        check(_lib.lib().aw_greedy_set_fast_interpolation(self._h, int(on)))
+
     def SetAutoStepReduce(self, on: bool):
         check(_lib.lib().aw_greedy_set_auto_step_reduce(self._h, int(on)))
 

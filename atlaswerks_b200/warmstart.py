@@ -440,8 +440,27 @@ def make_pairs(seeds: Sequence[int], n: int, workers: int = 0):
         return pool.starmap(greedy_pair, args, chunksize=max(1, len(args) // (4 * workers)))
 
 
+# the multiscale schedule of the 3-level pair-registration config:
+# (downsample factor, iterations, MaxPert), coarse to fine
+MULTISCALE = [(4, 100, 0.5), (2, 50, 0.5), (1, 25, 0.5)]
+
+
+def _multiscale(I0: torch.Tensor, I1: torch.Tensor):
+    """The plain multiscale solve (GreedyWarp over MULTISCALE) with its
+    iterators built (prepare), ready to run."""
+    from .multiscale import GreedyWarpB200, ScaleLevel
+    return GreedyWarpB200(I0, I1, [ScaleLevel(f, n, m) for f, n, m in MULTISCALE]).prepare()
+
+
+def _plain_multiscale(w):
+    """Runs a prepared multiscale solve from the identity; returns (h,
+    energies of the finest level)."""
+    h, _ = w.RunWarp()
+    return h, np.asarray(w.energies[-1])
+
+
 def evaluate(net: "WarmStartNet", pairs, plain_iters: int = 50, tol: float = 0.01,
-             chunk: int = 3, max_pert: float = 0.5, policy: str = "own"):
+             chunk: int = 3, max_pert: float = 0.5, policy: str = "own", plain: str = "single"):
     """Per pair: the plain solve from the identity for plain_iters
     iterations, then the warm start (network + refinement until the
     iteration energy is within (1 + tol) of the plain solve's last one,
@@ -452,7 +471,9 @@ def evaluate(net: "WarmStartNet", pairs, plain_iters: int = 50, tol: float = 0.0
     The network runs as one graph replay (WarmStartPredictor, built once
     per grid before any clock starts). Device times from CUDA events;
     warm_iters counts the iterations needed, warm_iters_run the ones
-    executed (whole chunks). Returns a list of dicts."""
+    executed (whole chunks). plain "multiscale": the plain method is the
+    3-level multiscale solve (MULTISCALE), its finest-level energy the
+    target, and it is also the fallback. Returns a list of dicts."""
     from .greedy import GreedyDeformationDataB200
     out = []
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
@@ -468,12 +489,19 @@ def evaluate(net: "WarmStartNet", pairs, plain_iters: int = 50, tol: float = 0.0
         # the warm path's handles exist before its clock starts, as the plain one's do
         it_w, data_w = _greedy(shape, max_pert), GreedyDeformationDataB200(I0, I1)
         it2, d2 = _greedy(shape, max_pert), GreedyDeformationDataB200(I0, I1)
+        if plain == "multiscale":
+            ms, ms2 = _multiscale(I0, I1), _multiscale(I0, I1)
+            _plain_multiscale(ms)  # downsampling tables and graphs, outside the clock
         torch.cuda.synchronize()
         ev[0].record()
-        it.Run(data, plain_iters, update_first=True)
+        if plain == "multiscale":
+            _, e_plain = _plain_multiscale(ms)
+        else:
+            it.Run(data, plain_iters, update_first=True)
         ev[1].record()
         torch.cuda.synchronize()
-        e_plain = it.Energies()
+        if plain != "multiscale":
+            e_plain = it.Energies()
         target = float(e_plain[-1]) * (1.0 + tol)
         ev[2].record()
         eps = plain_step(I0, I1, it_w, data_w, max_pert) if policy == "plain" else None
@@ -488,14 +516,21 @@ def evaluate(net: "WarmStartNet", pairs, plain_iters: int = 50, tol: float = 0.0
             run += 1
         fallback = not reached
         if fallback:  # the warm start did not get there: the plain solve, unassisted
-            it2.Run(d2, plain_iters, update_first=True)
-            k += plain_iters
-            run += plain_iters
+            if plain == "multiscale":
+                _plain_multiscale(ms2)
+                k += sum(n for _, n, _ in MULTISCALE)
+                run += sum(n for _, n, _ in MULTISCALE)
+            else:
+                it2.Run(d2, plain_iters, update_first=True)
+                k += plain_iters
+                run += plain_iters
         ev[3].record()
         torch.cuda.synchronize()
         out.append({"plain_ms": ev[0].elapsed_time(ev[1]), "warm_ms": ev[2].elapsed_time(ev[3]),
                     "predict_ms": ev[2].elapsed_time(ev[4]), "warm_iters_run": run,
-                    "plain_iters": plain_iters, "warm_iters": int(k), "reached": bool(reached),
+                    "plain_iters": (sum(n for _, n, _ in MULTISCALE) if plain == "multiscale"
+                                    else plain_iters),
+                    "warm_iters": int(k), "reached": bool(reached),
                     "fallback": bool(fallback), "plain_energy": float(e_plain[-1]),
                     "warm_start_energy": float(en[0]) if len(en) else float("nan"),
                     "identity_energy": float(e_plain[0])})
@@ -552,6 +587,58 @@ def trained(grid: int) -> "WarmStartNet":
     net = WarmStartNet((net_grid,) * 3)
     load_weights(net, os.path.join(os.path.dirname(__file__), "data", name))
     return net
+
+
+def param_blob(net: "WarmStartNet") -> np.ndarray:
+    """The network's parameters as aw_warmstart_create takes them: per layer
+    in LAYERS order the FP32 weights [Cout][taps][Cin], then the biases."""
+    parts = []
+    for name, _, _, _ in LAYERS:
+        parts.append(net.w[name].detach().float().cpu().numpy().ravel())
+        parts.append(net.b[name].detach().float().cpu().numpy().ravel())
+    return np.ascontiguousarray(np.concatenate(parts), dtype=np.float32)
+
+
+class WarmStartB200:
+    """The warm start through the C ABI (aw_warmstart_*): prediction as one
+    captured graph and the refinement/fallback loop in the library, the
+    path a C or C++ host uses. ``shape`` is the pair grid (nz, ny, nx)."""
+
+    def __init__(self, net: "WarmStartNet", shape: Sequence[int], max_pert: float = 0.5):
+        nz, ny, nx = (int(s) for s in shape)
+        self.shape = (nz, ny, nx)
+        blob = param_blob(net)
+        self._h = ctypes.c_void_p()
+        check(_lib.lib().aw_warmstart_create(nx, ny, nz, net.W, net.H, net.D,
+                                             blob.ctypes.data, blob.size, float(max_pert),
+                                             ctypes.byref(self._h)))
+
+    def predict(self, I0: torch.Tensor, I1: torch.Tensor, h: torch.Tensor) -> torch.Tensor:
+        check(_lib.lib().aw_warmstart_predict(self._h, _p(I0), _p(I1), _p(h[0]), _p(h[1]),
+                                              _p(h[2]), _stream()))
+        return h
+
+    def register(self, I0: torch.Tensor, I1: torch.Tensor, h: torch.Tensor,
+                 target_energy: float, max_refine_iters: int = 25, chunk: int = 3,
+                 plain_iters: int = 50):
+        """Returns (iterations executed, fell back to the plain solve)."""
+        run, fb = ctypes.c_int(), ctypes.c_int()
+        check(_lib.lib().aw_warmstart_register(self._h, _p(I0), _p(I1), float(target_energy),
+                                               int(max_refine_iters), int(chunk),
+                                               int(plain_iters), _p(h[0]), _p(h[1]), _p(h[2]),
+                                               ctypes.byref(run), ctypes.byref(fb), _stream()))
+        return run.value, bool(fb.value)
+
+    def close(self):
+        if self._h:
+            _lib.lib().aw_warmstart_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def load_weights(net: "WarmStartNet", path: str):

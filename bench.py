@@ -46,7 +46,7 @@ E2E_ITERS = 25  # the 128^3 level of the 3-level multiscale config
 # traffic of that kernel's function; spectrum = 3 complex64 x (nx/2+1)/nx)
 SPEC = 3 * 8 * (N // 2 + 1) / N  # bytes/voxel of the 3-channel half spectrum
 STAGE_NAMES = ["force_prep", "energy", "xy_forward_fft", "z_solve", "xy_inverse_fft",
-               "max_norm", "update", "xy_inverse_update"]
+               "max_norm", "update", "xy_inverse_update", "xy_inverse_update_prep"]
 STAGE_BYTES = {
     "force_prep": 12 + 4 + 4 + 4,        # h, I1, I0 gather (once), I0(h) write
     "energy": 0,
@@ -56,6 +56,9 @@ STAGE_BYTES = {
     "max_norm": 12,
     "update": 12 + 12 + 12,              # v, h gather (once), h' write
     "xy_inverse_update": SPEC + 12 + 12,  # spectrum read, h gather (once), h' write
+    # ... and the next iteration's force preparation from h': I0 gather
+    # (once), I1 read, I0(h') write
+    "xy_inverse_update_prep": SPEC + 12 + 12 + 4 + 4 + 4,
 }
 B_ITER = 92  # bytes/voxel of the fully fused 3-pass greedy iteration (each stream once)
 B_ITER_INV = B_ITER + 36  # with h^-1: its read and write, v gathered at h^-1
@@ -274,6 +277,8 @@ def run_b200(args):
         host_pairs.append((I0, I1))
         it = GreedyIteratorB200((N, N, N))
         it.SetScaleLevel((N, N, N), (1.0, 1.0, 1.0), param)
+        if args.fast_interp:
+            it.SetFastInterpolation(True)
         d = GreedyDeformationDataB200(torch.from_numpy(I0).cuda(), torch.from_numpy(I1).cuda())
         it.Run(d, 1, update_first=True)
         iters.append(it)
@@ -378,8 +383,9 @@ def run_b200(args):
         *[t.data_ptr() for t in ho], *z, *z, 20, stream.cuda_stream, ms_stage))
     stage_ms = {n: float(ms_stage[i]) for i, n in enumerate(STAGE_NAMES)}
     # a steady-state iteration (no step update, no inverse field): the
-    # inverse transform and the update run as one kernel
-    per_iter_stages = ["force_prep", "energy", "xy_forward_fft", "z_solve", "xy_inverse_update"]
+    # inverse transform, the update and the next iteration's force
+    # preparation run as one kernel
+    per_iter_stages = ["energy", "xy_forward_fft", "z_solve", "xy_inverse_update_prep"]
     dom = max(per_iter_stages, key=lambda n: stage_ms[n])
     nvox = N ** 3
     dom_bytes = STAGE_BYTES[dom] * nvox
@@ -419,6 +425,8 @@ def run_b200(args):
             I1d = torch.empty((N, N, N), device="cuda")
             it = GreedyIteratorB200((N, N, N))
             it.SetScaleLevel((N, N, N), (1.0, 1.0, 1.0), param)
+            if args.fast_interp:
+                it.SetFastInterpolation(True)
             jobs.append({"I0h": torch.from_numpy(host_pairs[p][0]).pin_memory(),
                          "I1h": torch.from_numpy(host_pairs[p][1]).pin_memory(),
                          "hh": torch.empty((3, N, N, N), dtype=torch.float32).pin_memory(),
@@ -476,15 +484,17 @@ def run_b200(args):
                          f"(GreedyIteratorCPU{'' if kind == 'reference' else ' port'}; FFT = "
                          f"FP64 shim, not FFTW)"}
 
-    # five launches per steady-state iteration: force-prep, energy,
-    # xy-forward, z-solve, xy-inverse fused with the update
-    launches = 5 * per_rank_iters
+    # four launches per steady-state iteration: energy, xy-forward, z-solve,
+    # xy-inverse fused with the update and the next force preparation
+    launches = 4 * per_rank_iters
     line = {"metric": "128^3 fluid iters/s", "value": value, "unit": "iters/s",
             "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded Gaussian blobs + smooth random warp, no dataset)",
-            "config": config(), "roofline": roofline,
+            "config": config({"interpolation": "float fused multiply-add trees (fast mode)"
+                              if args.fast_interp else "double weights and sums (bit-exact)"}),
+            "roofline": roofline,
             "iteration_roofline": iteration_roofline, "inverse_field": inverse_field,
             "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches,
@@ -535,6 +545,8 @@ def run_ncu_case(args):
     it = GreedyIteratorB200((N, N, N))
     it.SetScaleLevel((N, N, N), (1.0, 1.0, 1.0),
                      GreedyIteratorParam(DiffOperParam(ALPHA, BETA, GAMMA), MAX_PERT))
+    if args.fast_interp:
+        it.SetFastInterpolation(True)
     d = GreedyDeformationDataB200(torch.from_numpy(I0).cuda(), torch.from_numpy(I1).cuda())
     it.Run(d, 1 + args.steps, update_first=True)
     torch.cuda.synchronize()
@@ -815,6 +827,21 @@ def run_warmstart(args):
     res = W.evaluate(net, pairs)
     pm = float(np.sum([r["plain_ms"] for r in res]))
     wm = float(np.sum([r["warm_ms"] for r in res]))
+    # against the 3-level multiscale plain solve (its finest-level energy the
+    # target, and the fallback)
+    res_ms = W.evaluate(net, pairs, plain="multiscale")
+    pm_ms = float(np.sum([r["plain_ms"] for r in res_ms]))
+    wm_ms = float(np.sum([r["warm_ms"] for r in res_ms]))
+    multiscale = {
+        "plain": "3-level multiscale greedy, 100/50/25 iterations at n/4, n/2, n",
+        "plain_pairs_per_s": 1000.0 * len(res_ms) / pm_ms,
+        "warm_pairs_per_s": 1000.0 * len(res_ms) / wm_ms,
+        "wall_ratio_warm_over_plain": wm_ms / pm_ms,
+        "plain_ms_median": float(np.median([r["plain_ms"] for r in res_ms])),
+        "warm_ms_median": float(np.median([r["warm_ms"] for r in res_ms])),
+        "iters_warm_run_mean": float(np.mean([r["warm_iters_run"] for r in res_ms])),
+        "reached_fraction": float(np.mean([r["reached"] for r in res_ms])),
+        "fallback_fraction": float(np.mean([r["fallback"] for r in res_ms]))}
     print(json.dumps({
         "metric": f"{n}^3 registrations/s to the plain method's final energy (+1%)",
         "value": 1000.0 * len(res) / wm, "unit": "pairs/s", "n_gpus": 1, "steps": len(res),
@@ -831,7 +858,8 @@ def run_warmstart(args):
         "iters_warm_mean": float(np.mean([r["warm_iters"] for r in res])),
         "iters_warm_run_mean": float(np.mean([r["warm_iters_run"] for r in res])),
         "reached_fraction": float(np.mean([r["reached"] for r in res])),
-        "fallback_fraction": float(np.mean([r["fallback"] for r in res]))}))
+        "fallback_fraction": float(np.mean([r["fallback"] for r in res])),
+        "vs_multiscale": multiscale}))
     return 0
 
 
@@ -855,6 +883,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fast-interp", action="store_true",
+                    help="greedy: float fused-multiply-add interpolation (not bit-exact)")
     ap.add_argument("--ncu-case", action="store_true",
                     help="run a short untimed 128^3 workload for ncu captures")
     ap.add_argument("--workload", default="greedy",

@@ -126,13 +126,20 @@ int aw_resample_image(const float *in, int nx, int ny, int nz, double sx, double
  * block or fail. Same result as aw_splat, bit for bit. The scratch is one
  * fixed array of AW_SPLAT_STATIC_MAX_BYTES in the library's device memory
  * (held on every device that loads the library until the process exits);
- * grids whose scratch (about 12 bytes per voxel, e.g. up to 80^3) exceeds it
- * are rejected with an error. The first call on each device looks up the
- * array's device address, so make it before any stream capture. All calls
- * share the one array: calls that overlap on the GPU (other streams, other
- * host threads) race and must be serialised by the caller. */
+ * grids whose scratch exceeds it are rejected with an error. The scratch of
+ * an nx x ny x nz grid, with m = (nx+1)(ny+1)(nz+1) and each term rounded up
+ * to a multiple of 256 bytes, is 4(m+1) + 4m + 4 nx ny nz + 4 ceil(m/1024)
+ * bytes (about 12 bytes per voxel: 88^3 fits, 89^3 does not);
+ * aw_splat_static_fits answers for a grid. The first call on each device
+ * looks up the array's device address and keeps it, so make it before any
+ * stream capture, and do not reset the device (cudaDeviceReset) while the
+ * library is loaded. All calls share the one array: calls that overlap on
+ * the GPU (other streams, other host threads) race and must be serialised
+ * by the caller. */
 int aw_splat_static(const float *img, const float *hx, const float *hy, const float *hz,
                     float *out, int nx, int ny, int nz, float background, void *stream);
+/* 1 when aw_splat_static takes an nx x ny x nz grid, else 0. */
+int aw_splat_static_fits(int nx, int ny, int nz);
 
 /* ---------------------------------------------------------------------------
  * Fluid kernel. Replaces KernelInterfaceGPU / DiffOperGPU
@@ -188,6 +195,12 @@ int aw_greedy_set_staged_update(aw_greedy_t g, int on);
  * composeHV, Greedy/GreedyIteratorGPU.cxx:120-134); 0: v is stored and the
  * update is a kernel of its own. Both give the same bits. */
 int aw_greedy_set_fused_update(aw_greedy_t g, int on);
+/* on = 1: I0(h) in the force preparation and h(x + eps v/sp) in the fused
+ * update interpolate with float fused multiply-adds instead of the
+ * reference's double weights and sums: a few float ulps from the
+ * bit-exact results (I0(h) within 1e-6 of it for images in [0, 1]); 0
+ * (default): bit-exact with the reference CPU's interpolation. */
+int aw_greedy_set_fast_interpolation(aw_greedy_t g, int on);
 /* Tile shape of the staged update (x 32 voxels; index 0: 8 x 4 in y x z,
  * 1: 4 x 8, 2: 8 x 8, 3: 16 x 2), chosen when the handle is created by
  * timing each on the device (kept per grid and device for the process).

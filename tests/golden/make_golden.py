@@ -25,7 +25,7 @@ sys.path.insert(0, os.path.dirname(HERE))
 
 from atlaswerks_b200.synth import atlas_subjects, bullseye, greedy_pair  # noqa: E402
 from oracle import REF_SO, Reference, build_reference, identity, reference_root  # noqa: E402
-from metaimage import read_mha, read_nhdr, rescale_intensities  # noqa: E402
+from atlaswerks_b200.metaimage import read_mha, read_nhdr, rescale_intensities  # noqa: E402
 
 BG = ["partial_id", "id", "partial_zero", "zero", "clamp", "wrap"]
 
@@ -110,6 +110,7 @@ def main():
          mean_p2=m2, h_p2=np.stack(h2), energies_p2=e2)
 
     adshoot_cases(ref)
+    greedy_bullseye_case(ref)
 
 
 def adshoot_cases(ref):
@@ -135,8 +136,27 @@ def adshoot_cases(ref):
          alpha0=a0, phiT0=p1, img_energy=ei, vec_energy=ev)
 
 
+def greedy_bullseye_case(ref):
+    """The reference's greedy regression (Testing/Applications/Greedy/
+    GreedyWarp: GreedyWarpParams.xml — the bullseye pair rescaled to [0, 1],
+    scale factors 2 then 1 with 50 iterations each, MaxPert 0.3, alpha =
+    beta = 0.01, gamma = 0.001, the inverse field computed) with its
+    Baseline deformed image, and the reference build's own run on it."""
+    root = os.path.join(reference_root(), "Testing")
+    B0, bsp = read_nhdr(f"{root}/Data/Input/Bullseyes/BullseyeTestBlur00.nhdr")
+    B1, _ = read_nhdr(f"{root}/Data/Input/Bullseyes/BullseyeTestBlur01.nhdr")
+    base, _ = read_mha(f"{root}/Applications/Greedy/GreedyWarp/Baseline/"
+                       "GreedyBullseyeTestBlur00_to_BullseyeTestBlur01DefImage.mha")
+    B0, B1 = rescale_intensities(B0), rescale_intensities(B1)
+    h, hinv, en, steps = ref.greedy_run(B0, B1, [2, 1], [50, 50], [0.3, 0.3], bsp, inverse=True)
+    save("greedy_bullseye", I0=B0, I1=B1, sp=np.array(bsp), baseline_def_image=base, h=h,
+         hinv=hinv, energies=en)
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["adshoot"]:
         adshoot_cases(Reference())
+    elif sys.argv[1:] == ["greedy_bullseye"]:
+        greedy_bullseye_case(Reference())
     else:
         main()

@@ -73,3 +73,14 @@ def test_host_mirror_rejects_unsupported_kernel_params():
     op = DiffOperB200()
     with pytest.raises(ValueError):
         op.SetSize((16, 16, 16), (1, 1, 1), DiffOperParam(UseEigenLUT=True))
+
+
+def test_static_splat_capacity_query():
+    """aw_splat_static_fits answers from the scratch formula the header
+    states, without a GPU: 88^3 fits the fixed array, 89^3 does not."""
+    from atlaswerks_b200 import _lib
+    L = _lib.lib()
+    assert L.aw_splat_static_fits(88, 88, 88) == 1
+    assert L.aw_splat_static_fits(89, 89, 89) == 0
+    assert L.aw_splat_static_fits(0, 8, 8) == 0
+    assert L.aw_splat_static_fits(400, 100, 1) == 1

@@ -183,6 +183,33 @@ def test_greedy_run_iterate_equivalence():
     assert np.array_equal(a.Energies(), b.Energies())
 
 
+@pytest.mark.parametrize("shape,n", [((64, 64, 64), 9), ((32, 64, 128), 4), ((16, 16, 32), 3)])
+def test_prepared_ahead_run_equals_iterations(shape, n):
+    """aw_greedy_run on power-of-two grids: its fused kernels prepare the
+    next iteration (I0(h') and the energy partials) so later iterations skip
+    the force preparation; the result equals repeated aw_greedy_iterate
+    (each preparing itself) bit for bit, fields and energies."""
+    nz, ny, nx = shape
+    I0, I1 = greedy_pair(shape, seed=4, n_blobs=6, umax=2.0)
+    p = GreedyIteratorParam(DiffOperParam(), 0.5)
+    out = []
+    for run in (True, False):
+        it = GreedyIteratorB200((nx, ny, nz))
+        it.SetScaleLevel((nx, ny, nz), (1.0, 1.0, 1.0), p)
+        d = GreedyDeformationDataB200(cu(I0), cu(I1))
+        if run:
+            it.Run(d, n, update_first=True)
+            it.Run(d, n, update_first=False)  # a second call starts from its own preparation
+        else:
+            for k in range(2 * n):
+                if k == 0:
+                    it.UpdateStepSizeNextIteration()
+                it.Iterate(d)
+        out.append((host(d.Def1To0()).copy(), it.Energies()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+
+
 def test_greedy_deterministic():
     shape = (32, 32, 32)
     I0, I1 = greedy_pair(shape, seed=5)
@@ -316,6 +343,23 @@ def test_fused_update_equals_separate_kernels(shape, sp, max_pert):
     assert np.array_equal(out[0][1], out[1][1])
     assert np.array_equal(out[0][2], out[1][2])
     assert np.abs(out[0][0] - identity(shape)).max() > 0.1
+
+
+def test_fast_interpolation_within_tolerance(oracle):
+    """The float fused-multiply-add interpolation mode: a 64^3 run of 30
+    iterations within 1e-3 voxel RMS of the oracle, energies (sums of
+    (I1 - I0(h))^2 over the interpolated I0(h)) to 1e-4."""
+    shape = (64, 64, 64)
+    I0, I1 = greedy_pair(shape, seed=14, n_blobs=8, umax=3.0)
+    h_o, _, e_o, _ = oracle.greedy_run(I0, I1, 30, max_pert=0.5)
+    it = GreedyIteratorB200((64, 64, 64))
+    it.SetScaleLevel((64, 64, 64), (1.0, 1.0, 1.0), GreedyIteratorParam(DiffOperParam(), 0.5))
+    it.SetFastInterpolation(True)
+    d = GreedyDeformationDataB200(cu(I0), cu(I1))
+    it.Run(d, 30, update_first=True)
+    dh = (host(d.Def1To0()) - h_o).astype(np.float64)
+    assert float(np.sqrt((dh ** 2).sum(0).mean())) <= 1e-3
+    assert np.allclose(it.Energies(), e_o, rtol=1e-4)
 
 
 @pytest.mark.parametrize("shape", [(36, 31, 32), (48, 40, 44), (96, 80, 72)])

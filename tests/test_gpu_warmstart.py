@@ -19,6 +19,7 @@ import pytest
 torch = pytest.importorskip("torch")
 
 from atlaswerks_b200 import warmstart as W  # noqa: E402
+from atlaswerks_b200.greedy import GreedyDeformationDataB200  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -72,6 +73,47 @@ def test_graph_predictor_matches_eager_path():
     # a second pair through the same graph
     J0, J1 = (torch.from_numpy(a).cuda() for a in W.make_pairs([20_000_201], 128, 0)[0])
     assert torch.equal(pred(J0, J1).clone(), W.warm_h(net, J0, J1))
+
+
+def test_c_abi_predictor_matches_python_predictor():
+    """aw_warmstart_predict (the C ABI a C++ host calls: parameters from a
+    host blob, the prediction captured as one graph in the library) gives
+    the Python-side graph predictor's field bit for bit, on two pairs."""
+    net = W.trained(128)
+    ws = W.WarmStartB200(net, (128, 128, 128))
+    pred = W.WarmStartPredictor(net, (128, 128, 128))
+    h = torch.empty((3, 128, 128, 128), device="cuda")
+    for seed in (20_000_210, 20_000_211):
+        I0, I1 = (torch.from_numpy(a).cuda() for a in W.make_pairs([seed], 128, 0)[0])
+        want = pred(I0, I1).clone()
+        ws.predict(I0, I1, h)
+        torch.cuda.synchronize()
+        assert torch.equal(h, want)
+    ws.close()
+
+
+def test_c_abi_register_reaches_plain_energy():
+    """aw_warmstart_register at 64^3 (network at 32^3): the refinement
+    reaches the plain solve's final energy (+1 %) without the fallback on
+    most held-out pairs, in a handful of iterations."""
+    net = W.trained(64)
+    ws = W.WarmStartB200(net, (64, 64, 64))
+    h = torch.empty((3, 64, 64, 64), device="cuda")
+    ok = 0
+    for I0n, I1n in W.make_pairs(range(20_000_400, 20_000_404), 64, 0):
+        I0, I1 = torch.from_numpy(I0n).cuda(), torch.from_numpy(I1n).cuda()
+        it = W._greedy((64, 64, 64))
+        d = GreedyDeformationDataB200(I0, I1)
+        it.Run(d, 50, update_first=True)
+        target = float(it.Energies()[-1]) * 1.01
+        run, fell_back = ws.register(I0, I1, h, target, 25, 3, 50)
+        if not fell_back:
+            ok += 1
+            assert run <= 12
+        else:
+            assert run > 50  # the plain solve ran in full after the refinement
+    assert ok >= 3
+    ws.close()
 
 
 def _pair_losses(net, pairs, targets):

@@ -12,7 +12,7 @@ import os
 import numpy as np
 import pytest
 
-from metaimage import read_mha, read_nhdr, rescale_intensities
+from atlaswerks_b200.metaimage import read_mha, read_nhdr, rescale_intensities
 from oracle import reference_root
 
 REF = os.path.join(reference_root(), "Testing")
