@@ -271,8 +271,8 @@ int aw_fluid_apply(aw_fluid_t k, float *vx, float *vy, float *vz, int inverse, v
 
 int aw_fluid_get_shapes(aw_fluid_t k, int *shapes) {
   if (!k || !shapes) return fail("aw_fluid_get_shapes: null pointer");
-  const int tunable = aw::fluid_get_shapes(k->plan, shapes, shapes + 1, shapes + 2);
-  if (!tunable) shapes[0] = shapes[1] = shapes[2] = 0;
+  // the register-FFT path reports {0, 0, z-pass tile width}
+  aw::fluid_get_shapes(k->plan, shapes, shapes + 1, shapes + 2);
   return 0;
 }
 
@@ -280,10 +280,9 @@ int aw_fluid_set_shapes(aw_fluid_t k, int pairs, int cols, int zcols) {
   if (!k) return fail("aw_fluid_set_shapes: null handle");
   AW_CUDA(cudaDeviceSynchronize(), "aw_fluid_set_shapes (pending work)");
   const cudaError_t e = aw::fluid_set_shapes(&k->plan, pairs, cols, zcols);
-  if (e == cudaErrorNotSupported)
-    return fail("aw_fluid_set_shapes: power-of-two grids use fixed register-FFT shapes");
   if (e == cudaErrorInvalidValue)
-    return fail("aw_fluid_set_shapes: shapes out of range or beyond shared memory");
+    return fail(k->plan.fast ? "aw_fluid_set_shapes: power-of-two grids take (0, 0, 16 or 8)"
+                             : "aw_fluid_set_shapes: shapes out of range or beyond shared memory");
   AW_CUDA(e, "aw_fluid_set_shapes");
   return 0;
 }
@@ -446,40 +445,21 @@ int aw_greedy_run(aw_greedy_t g, const float *I0, const float *I1, float *hx, fl
   float *AI[3] = {hix, hiy, hiz}, *BI[3] = {six, siy, siz};
   int done = 0;
   bool in_a = true;
-  // Iterations without a step update end in the fused kernel, which can
-  // prepare the next iteration (I0(h') and its energy partials) so that the
-  // next one starts without a force-preparation kernel. Only inside this
-  // call: the first iteration always prepares itself, the last prepares
-  // nothing (the caller may change h between calls).
-  const bool ahead = aw::greedy_can_prep_ahead(&g->ctx, inv);
-  bool have = false;
-  auto one = [&](int upd, bool next) -> cudaError_t {
+  auto one = [&](int upd) -> cudaError_t {
     float **src = in_a ? A : B, **dst = in_a ? B : A;
     float **isrc = in_a ? AI : BI, **idst = in_a ? BI : AI;
     const float *cs[3] = {src[0], src[1], src[2]}, *ci[3] = {isrc[0], isrc[1], isrc[2]};
-    const bool prep = next && ahead && !upd;
     cudaError_t e = aw::greedy_iterate(&g->ctx, I0, I1, cs, dst, inv ? ci : nullptr,
-                                       inv ? idst : nullptr, upd, g->auto_reduce, s, have ? 1 : 0,
-                                       prep ? 1 : 0);
-    have = prep;
+                                       inv ? idst : nullptr, upd, g->auto_reduce, s);
     in_a = !in_a;
     return e;
   };
   if (update_first) {
-    AW_CUDA(one(1, false), "aw_greedy_run (first iteration)");
+    AW_CUDA(one(1), "aw_greedy_run (first iteration)");
     ++done;
   }
-  // the captured pair runs with the next iteration prepared on entry (when
-  // the handle prepares ahead): one lead-in iteration prepares the first
-  // replay, and one tail iteration follows the last
-  const int lead = (ahead && n_iters - done >= 3) ? 1 : 0;
-  if (lead) {
-    AW_CUDA(one(0, true), "aw_greedy_run (lead-in iteration)");
-    ++done;
-  }
-  // replay a captured pair of iterations (src->dst->src) as often as possible,
-  // keeping one iteration back for the tail when preparing ahead
-  const int pairs = (n_iters - done - lead) / 2;
+  // replay a captured pair of iterations (src->dst->src) as often as possible
+  const int pairs = (n_iters - done) / 2;
   if (pairs > 0) {
     GraphKey key;
     std::memset(&key, 0, sizeof(key));
@@ -488,17 +468,16 @@ int aw_greedy_run(aw_greedy_t g, const float *I0, const float *I1, float *hx, fl
     const void *ptrs[14] = {I0,      I1,      src[0],  src[1],  src[2],  dst[0],  dst[1],
                             dst[2],  isrc[0], isrc[1], isrc[2], idst[0], idst[1], idst[2]};
     for (int i = 0; i < 14; ++i) key.p[i] = ptrs[i];
-    key.n = 2 + (lead ? 16 : 0);  // the prepared-on-entry pair is a different graph
+    key.n = 2;
     auto it = g->graphs.find(key);
     cudaGraphExec_t exec = nullptr;
     if (it == g->graphs.end()) {
       cudaGraph_t graph;
       AW_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "aw_greedy_run (capture)");
-      const bool start = in_a, have0 = have;
-      cudaError_t e1 = one(0, lead != 0), e2 = one(0, lead != 0);
+      const bool start = in_a;
+      cudaError_t e1 = one(0), e2 = one(0);
       cudaError_t ec = cudaStreamEndCapture(s, &graph);
       in_a = start;
-      have = have0;
       if (e1 != cudaSuccess) return cuda_fail(e1, "aw_greedy_run (captured iteration)");
       if (e2 != cudaSuccess) return cuda_fail(e2, "aw_greedy_run (captured iteration)");
       if (ec != cudaSuccess) return cuda_fail(ec, "aw_greedy_run (end capture)");
@@ -509,10 +488,10 @@ int aw_greedy_run(aw_greedy_t g, const float *I0, const float *I1, float *hx, fl
       exec = it->second;
     }
     for (int p = 0; p < pairs; ++p) AW_CUDA(cudaGraphLaunch(exec, s), "aw_greedy_run (launch)");
-    done += 2 * pairs;  // the graph ends where it began: in_a and `have` as on entry
+    done += 2 * pairs;
   }
-  while (done < n_iters) {
-    AW_CUDA(one(0, done + 1 < n_iters), "aw_greedy_run (remaining iteration)");
+  if (done < n_iters) {
+    AW_CUDA(one(0), "aw_greedy_run (last iteration)");
     ++done;
   }
   if (!in_a) {  // final field is in the scratch buffers: bring it home

@@ -238,8 +238,9 @@ __global__ void __launch_bounds__(256) k_fft_xy_inv(FluidPlan p, Dst dst) {
 }
 
 // TMA descriptor of the spectrum for the z-pass: a 3D float tensor
-// {2*ny*nxh, nz, 3} read and written in boxes {2*Kq, nz, 1} = one 128-byte
-// row per kz, stored in shared memory with the 128-byte swizzle
+// {2*ny*nxh, nz, 3} read and written in boxes {2*Kq, nz, 1} = one row per
+// kz of 16 columns (128 bytes, 128-byte swizzle) or 8 (64 bytes, 64-byte
+// swizzle) in shared memory
 bool encode_spec_map(FluidPlan *p) {
   const PFN_cuTensorMapEncodeTiled encode = tensor_map_encoder();
   if (!encode) return false;
@@ -248,10 +249,65 @@ bool encode_spec_map(FluidPlan *p) {
   const cuuint64_t strides[2] = {2 * ncols * sizeof(float), 2 * ncols * sizeof(float) * p->d.nz};
   const cuuint32_t box[3] = {(cuuint32_t)(2 * p->fast_kq), (cuuint32_t)p->d.nz, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
-  if (box[0] * sizeof(float) != 128 || box[1] > 256 || strides[0] % 16) return false;
+  const size_t row = box[0] * sizeof(float);
+  if ((row != 128 && row != 64) || box[1] > 256 || strides[0] % 16) return false;
   return encode(&p->spec_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, p->spec, dims, strides, box, estr,
-                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                CU_TENSOR_MAP_INTERLEAVE_NONE,
+                row == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The register path's z-pass tile width (16 or 8 columns) by timing: after
+// one untimed launch, three alternating L^-1 / L launches (the spectrum
+// keeps its scale) of each on a zeroed spectrum; the faster is kept per
+// (grid, device) for the process. The arithmetic of a column does not
+// depend on the width.
+std::mutex g_zq_mu;
+std::map<std::tuple<int, int, int, int>, int> g_zq;
+
+void tune_z_cols(FluidPlan *p) {
+  const auto key = std::make_tuple(p->d.nx, p->d.ny, p->d.nz, p->device);
+  {
+    std::lock_guard<std::mutex> lock(g_zq_mu);
+    auto it = g_zq.find(key);
+    if (it != g_zq.end()) {
+      p->fast_kq = it->second;
+      p->fast_tma = encode_spec_map(p);
+      return;
+    }
+  }
+  const size_t bytes = sizeof(float2) * 3 * (size_t)p->d.nz * p->d.ny * p->nxh;
+  if (cudaMemset(p->spec, 0, bytes) != cudaSuccess) return;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return;
+  }
+  float best = 1e30f;
+  int pick = 16;
+  for (int q : {16, 8}) {
+    p->fast_kq = q;
+    p->fast_tma = encode_spec_map(p);
+    fast_z_solve(*p, 1, 0);
+    cudaEventRecord(e0, 0);
+    for (int r = 0; r < 3; ++r) fast_z_solve(*p, r & 1, 0);
+    cudaEventRecord(e1, 0);
+    float ms = 0.f;
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+      break;
+    if (ms < best) {
+      best = ms;
+      pick = q;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  p->fast_kq = pick;
+  p->fast_tma = encode_spec_map(p);
+  if (cudaGetLastError() != cudaSuccess) return;
+  std::lock_guard<std::mutex> lock(g_zq_mu);
+  g_zq[key] = pick;
 }
 
 // The shared-memory limit is an attribute of the kernel, shared by every
@@ -303,15 +359,21 @@ std::map<std::tuple<int, int, int, int>, std::tuple<int, int, int>> g_tuned;
 }  // namespace
 
 int fluid_get_shapes(const FluidPlan &p, int *P, int *Q, int *K) {
-  *P = p.pairs_per_batch;
-  *Q = p.cols_per_batch;
-  *K = p.zcols_per_cta;
+  *P = p.fast ? 0 : p.pairs_per_batch;
+  *Q = p.fast ? 0 : p.cols_per_batch;
+  *K = p.fast ? p.fast_kq : p.zcols_per_cta;
   return p.fast ? 0 : 1;
 }
 
 cudaError_t fluid_set_shapes(FluidPlan *p, int P, int Q, int K) {
   const int npairs = (p->d.ny + 1) / 2;
-  if (p->fast) return cudaErrorNotSupported;
+  if (p->fast) {
+    // the register path: only the z-pass tile width, 16 or 8 columns
+    if (P != 0 || Q != 0 || (K != 16 && K != 8)) return cudaErrorInvalidValue;
+    p->fast_kq = K;
+    p->fast_tma = encode_spec_map(p);
+    return cudaSuccess;
+  }
   if (P < 1 || P > npairs || Q < 1 || Q > p->nxh || K < 1 || K > 64) return cudaErrorInvalidValue;
   FluidPlan t = *p;
   generic_shapes(&t, P, Q, K);
@@ -429,7 +491,7 @@ int fluid_plan_create(FluidPlan *p, int nx, int ny, int nz, double spx, double s
   if (fast_supported(nx) && fast_supported(ny) && fast_supported(nz)) {
     p->fast_kq = fast_z_cols();
     p->fast_smem_xy = fast_xy_smem(nx, ny);
-    p->fast_smem_z = fast_z_smem(nz);
+    p->fast_smem_z = fast_z_smem(nz, 16);
     p->fast = p->fast_smem_xy <= (size_t)maxsm && p->fast_smem_z <= (size_t)maxsm;
   }
   if (!p->fast && (p->smem_xy > (size_t)maxsm || p->smem_z > (size_t)maxsm)) return 2;
@@ -455,6 +517,7 @@ int fluid_plan_create(FluidPlan *p, int nx, int ny, int nz, double spx, double s
   if (generic_configure(*p) != cudaSuccess) return 4;
   if (p->fast) p->fast_tma = encode_spec_map(p);
   if (p->fast && fast_configure(*p) != cudaSuccess) return 4;
+  if (p->fast) tune_z_cols(p);
   if (!p->fast && fluid_autotune(p, 0) != cudaSuccess) return 4;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }

@@ -249,25 +249,6 @@ struct DstAxpby {
   }
 };
 
-// The energy of an iteration, sp^3 sum (I1 - I0(h))^2 (GreedyIteratorCPU.cxx:
-// 113-121), is summed in two fixed stages: each warp of 32 consecutive x of a
-// row writes the double sum of its voxels' terms (a shuffle tree), then one
-// block sums the partials in a fixed order. The force preparation and the
-// fused inverse-and-update kernel (which prepares the next iteration) write
-// the same partials, so the energy does not depend on which one ran.
-AW_HD long energy_partials(const Dims &d) { return (long)d.nz * d.ny * ((d.nx + 31) / 32); }
-AW_D double energy_term(float idef, float i1) {
-  const float r = -fsub(idef, i1);
-  return (double)r * (double)r;
-}
-// every lane of the warp calls it with its voxel's term (0 outside the grid)
-AW_D void energy_partial(double e, int x, int y, int z, const Dims &d, double *partials) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
-  const int nw = (d.nx + 31) / 32, w = x >> 5;
-  if ((threadIdx.x & 31) == 0 && w < nw) partials[((long)z * d.ny + y) * nw + w] = e;
-}
-
 // The greedy update h'(x) = h(x + eps v(x)/sp) the inverse pass can apply
 // itself (fluid_inverse_compose): h in, h' out, the device-resident step,
 // the spacing divisors.
@@ -277,11 +258,6 @@ struct ComposeArgs {
   const float *step;
   DivF q0, q1, q2;
   int fast;  // 1: float-tree interpolation (trilerp_vector<true>)
-  // non-null: also prepare the next iteration from h' (the force
-  // preparation's I0(h') into idef and its energy partials)
-  const float *I0, *I1;
-  float *idef;
-  double *partials;
 };
 
 // host API (fluid.cu)

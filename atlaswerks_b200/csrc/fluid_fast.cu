@@ -34,7 +34,9 @@ namespace {
 
 constexpr int kXYThreads = 256;
 constexpr int kXYWarps = kXYThreads / 32;
-constexpr int kZq = 16;  // columns per z tile: one 128-byte row per kz
+// columns per z tile: 16 (one 128-byte row per kz, 128-byte swizzle) or 8
+// (64-byte rows, 64-byte swizzle), chosen by timing when a plan is created
+constexpr int kZq = 16;
 
 template <int NX, int NY>
 struct XYShape {
@@ -101,9 +103,30 @@ __global__ void __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
     const int lw = lane / TX, t = lane % TX;
     for (int base = warp * L; base < NLINES; base += kXYWarps * L) {
       const int y0 = 2 * xline_pair<TX>(base + lw);
-      float2 v[EX];
-      src.template row_pair<EX, TX>(comp, t, y0, z, d, v);
       float2 *row = C + y0 * NXH;
+      float2 v[EX];
+      if constexpr (NX >= 32) {
+        // The warp's L row pairs, one at a time, with its 32 lanes on 32
+        // consecutive x: every load is one 128-byte line (the line layout,
+        // TX lanes of TX-strided x on each of L rows, would touch L lines
+        // per load). The pairs go into their own slots, then each line
+        // reads its strided elements back. (Unrolling over the pairs, all
+        // their loads in flight at once, measured slower: 33.3 -> 35.4 us.)
+#pragma unroll 1
+        for (int l = 0; l < L; ++l) {
+          const int yl = 2 * xline_pair<TX>(base + l);
+          float2 u[NX / 32];
+          src.template row_pair<NX / 32, 32>(comp, lane, yl, z, d, u);
+          float2 *rl = C + yl * NXH;
+#pragma unroll
+          for (int j = 0; j < NX / 32; ++j) rl[lane + 32 * j] = u[j];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < EX; ++j) v[j] = row[t + TX * j];
+      } else {
+        src.template row_pair<EX, TX>(comp, t, y0, z, d, v);
+      }
       line_fft<NX, -1>(v, t, [row](int m) { return row + m; }, twx);
 #pragma unroll
       for (int r = 0; r < EX; ++r) row[line_out_index<NX>(t, r)] = v[r];
@@ -224,10 +247,13 @@ AW_D void inv_y_pass(float2 *C, const SmemTw &tw, int warp, int lane) {
 }
 
 // Inverse x-transform (complex to real) of every row pair with Hermitian
-// completion; out(x, y, value) receives each real output. A row pair's lines
-// read and write only that pair's own slots, which hold 2 * NXH >= NX + 2
-// floats per row: an output may go back into its own row's slots once the
-// line's transform has returned (line_fft ends on a warp barrier).
+// completion; out(x, y, value) receives each real output, from the warp's 32
+// lanes on 32 consecutive x of one row at a time (NX >= 32). A row pair's
+// lines read and write only that pair's own slots, which hold 2 * NXH >= NX
+// + 2 floats per row: the outputs are staged there once the line's
+// transform has returned (line_fft ends on a warp barrier), and the warp
+// reads them back for its coalesced writes; afterwards row y holds its
+// outputs as floats at (float *)(C + y * NXH).
 template <int NX, int NY, class Out>
 AW_D void inv_x_pass(float2 *C, const SmemTw &tw, int warp, int lane, const Out &out) {
   using S = XYShape<NX, NY>;
@@ -249,11 +275,36 @@ AW_D void inv_x_pass(float2 *C, const SmemTw &tw, int warp, int lane, const Out 
       v[j] = make_float2(X0.x - X1.y, X0.y + X1.x);
     }
     line_fft<NX, +1>(v, t, [row](int m) { return row + m; }, tw);
+    if constexpr (NX >= 32) {
+      // the outputs into the line's own slots as floats, then the warp
+      // writes its L row pairs out with its 32 lanes on 32 consecutive x
+      // (one 128-byte line per store instead of L)
+      float *r0 = reinterpret_cast<float *>(row), *r1 = reinterpret_cast<float *>(row + NXH);
 #pragma unroll
-    for (int r = 0; r < EX; ++r) {
-      const int x = line_out_index<NX>(t, r);
-      out(x, y0, v[r].x);
-      out(x, y0 + 1, v[r].y);
+      for (int r = 0; r < EX; ++r) {
+        const int x = line_out_index<NX>(t, r);
+        r0[x] = v[r].x;
+        r1[x] = v[r].y;
+      }
+      __syncwarp();
+#pragma unroll 1
+      for (int l = 0; l < L; ++l) {
+        const int yl = 2 * xline_pair<TX>(base + l);
+        const float *q0 = reinterpret_cast<const float *>(C + yl * NXH);
+        const float *q1 = reinterpret_cast<const float *>(C + (yl + 1) * NXH);
+#pragma unroll
+        for (int j = 0; j < NX / 32; ++j) {
+          out(lane + 32 * j, yl, q0[lane + 32 * j]);
+          out(lane + 32 * j, yl + 1, q1[lane + 32 * j]);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < EX; ++r) {
+        const int x = line_out_index<NX>(t, r);
+        out(x, y0, v[r].x);
+        out(x, y0 + 1, v[r].y);
+      }
     }
   }
 }
@@ -300,7 +351,7 @@ __global__ void __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
 // its own shared memory, then each updates a third of the slab's rows,
 // reading the three components of v there through distributed shared
 // memory, so v never goes to HBM.
-template <int NX, int NY, bool FAST, bool PREP>
+template <int NX, int NY, bool FAST>
 __global__ void __cluster_dims__(1, 3, 1) __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
     k_xy_inv_compose(FluidPlan p, ComposeArgs a) {
   using S = XYShape<NX, NY>;
@@ -320,8 +371,10 @@ __global__ void __cluster_dims__(1, 3, 1) __launch_bounds__(kXYThreads, (XYShape
   if (ok) {
     inv_y_pass<NX, NY>(C, twy, warp, lane);
     __syncthreads();
+    // v stays in shared memory: row y as floats at (float *)(C + y * NXH)
+    // (inv_x_pass leaves it there itself when NX >= 32)
     inv_x_pass<NX, NY>(C, twx, warp, lane, [C](int x, int y, float v) {
-      reinterpret_cast<float *>(C + y * NXH)[x] = v;
+      if constexpr (NX < 32) reinterpret_cast<float *>(C + y * NXH)[x] = v;
     });
   }
   cluster.sync();  // all three components of v are in the cluster's shared memory
@@ -345,14 +398,6 @@ __global__ void __cluster_dims__(1, 3, 1) __launch_bounds__(kXYThreads, (XYShape
       a.ox[i] = rx;
       a.oy[i] = ry;
       a.oz[i] = rz;
-      if (PREP) {
-        // the next iteration's force preparation at this voxel, from h' in
-        // registers: I0(h') and its energy term (k_force_prep's arithmetic);
-        // a warp holds 32 consecutive x of one row (NX >= 32)
-        const float w = trilerp_scalar<FAST>(a.I0, d, (double)rx, (double)ry, (double)rz, 0.0f);
-        a.idef[i] = w;
-        energy_partial(energy_term(w, __ldg(a.I1 + i)), x, y, z, d, a.partials);
-      }
     }
   }
   cluster.sync();  // no CTA leaves while a partner may still read its v
@@ -397,20 +442,25 @@ AW_D void solve_point(const FluidPlan &p, int kx, int ky, int kz, int inverse, f
   *b2p = o2;
 }
 
-// element (kz, q) of a [nz x 16] complex tile in the TMA 128-byte swizzle:
-// the 16-byte chunk q/2 of row kz sits at chunk (q/2) ^ (kz mod 8)
-AW_D int zt(int k, int q) { return k * kZq + (q ^ ((k & 7) << 1)); }
+// element (kz, q) of a [nz x Q] complex tile in the TMA swizzle of its row
+// size: with 128-byte rows (Q = 16) the 16-byte chunk q/2 of row kz sits at
+// chunk (q/2) ^ (kz mod 8); with 64-byte rows (Q = 8) at (q/2) ^ ((kz/2) mod 4)
+template <int Q>
+AW_D int zt(int k, int q) {
+  static_assert(Q == 16 || Q == 8, "z tile width");
+  return Q == 16 ? k * 16 + (q ^ ((k & 7) << 1)) : k * 8 + (q ^ (((k >> 1) & 3) << 1));
+}
 
-template <int NZ>
-constexpr int z_threads() { return 3 * kZq * LineCfg<NZ>::T; }
+template <int NZ, int Q>
+constexpr int z_threads() { return 3 * Q * LineCfg<NZ>::T; }
 
 // z-pass over one CTA's 16 columns; tiles TB[c] = [nz x 16] complex. With
 // TMA the tiles move by tensor copies (columns past the spectrum's end read
 // as zero and are not written back), else by coalesced plain copies.
-template <int NZ, bool TMA>
-__global__ void __launch_bounds__(z_threads<NZ>(), (NZ <= 128 ? 3 : 1))
+template <int NZ, int Q, bool TMA>
+__global__ void __launch_bounds__(z_threads<NZ, Q>(), (NZ <= 128 ? 48 / Q : 16 / Q))
     k_z_solve_fast(FluidPlan p, const __grid_constant__ CUtensorMap tmap, int inverse) {
-  constexpr int T = LineCfg<NZ>::T, E = LineCfg<NZ>::E, TILE = NZ * kZq;
+  constexpr int T = LineCfg<NZ>::T, E = LineCfg<NZ>::E, TILE = NZ * Q;
   extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ uint64_t mbar[3];
   // the swizzle pattern repeats every 1024 bytes: align the tiles to it
@@ -420,9 +470,9 @@ __global__ void __launch_bounds__(z_threads<NZ>(), (NZ <= 128 ? 3 : 1))
   for (int i = threadIdx.x; i < NZ; i += blockDim.x) twz[i] = __ldg(p.az.tw + i);
   const SmemTw tw{twz};
   const long ncols = (long)p.d.ny * p.nxh;
-  const long j0 = (long)blockIdx.x * kZq;
+  const long j0 = (long)blockIdx.x * Q;
   const int line = threadIdx.x / T, t = threadIdx.x % T;
-  const int c = line / kZq, q = line % kZq;
+  const int c = line / Q, q = line % Q;
   float2 *tile = TB + c * TILE;
   bool ok = true;
   if constexpr (TMA) {
@@ -438,9 +488,9 @@ __global__ void __launch_bounds__(z_threads<NZ>(), (NZ <= 128 ? 3 : 1))
     ok = mbar_wait(&mbar[c], 0, p.status);
   } else {
     for (int i = threadIdx.x; i < 3 * TILE; i += blockDim.x) {
-      const int qq = i % kZq, r = i / kZq;  // r = cc*NZ + kz
+      const int qq = i % Q, r = i / Q;  // r = cc*NZ + kz
       const int cc = r / NZ, kz = r - cc * NZ;
-      TB[cc * TILE + zt(kz, qq)] =
+      TB[cc * TILE + zt<Q>(kz, qq)] =
           (j0 + qq < ncols) ? p.spec[(long)r * ncols + j0 + qq] : make_float2(0.f, 0.f);
     }
     __syncthreads();
@@ -448,29 +498,29 @@ __global__ void __launch_bounds__(z_threads<NZ>(), (NZ <= 128 ? 3 : 1))
 
   float2 v[E];
 #pragma unroll
-  for (int j = 0; j < E; ++j) v[j] = tile[zt(t + T * j, q)];
-  line_fft<NZ, -1>(v, t, [tile, q](int m) { return tile + zt(m, q); }, tw);
+  for (int j = 0; j < E; ++j) v[j] = tile[zt<Q>(t + T * j, q)];
+  line_fft<NZ, -1>(v, t, [tile, q](int m) { return tile + zt<Q>(m, q); }, tw);
 #pragma unroll
-  for (int r = 0; r < E; ++r) tile[zt(line_out_index<NZ>(t, r), q)] = v[r];
+  for (int r = 0; r < E; ++r) tile[zt<Q>(line_out_index<NZ>(t, r), q)] = v[r];
   if (__syncthreads_or(!ok)) return;  // a tile never landed: the status word says so
 
   const float invN = 1.0f / (float)p.d.n();
   const int nxh = p.nxh;
   for (int i = threadIdx.x; i < TILE; i += blockDim.x) {
-    const int kz = i / kZq, qq = i % kZq;
+    const int kz = i / Q, qq = i % Q;
     const long jj = j0 + qq;
     if (jj >= ncols) continue;
     const int ky = (int)(jj / nxh), kx = (int)(jj - (long)ky * nxh);
-    const int e = zt(kz, qq);
+    const int e = zt<Q>(kz, qq);
     solve_point(p, kx, ky, kz, inverse, invN, TB + e, TB + TILE + e, TB + 2 * TILE + e);
   }
   __syncthreads();
 
 #pragma unroll
-  for (int j = 0; j < E; ++j) v[j] = tile[zt(t + T * j, q)];
-  line_fft<NZ, +1>(v, t, [tile, q](int m) { return tile + zt(m, q); }, tw);
+  for (int j = 0; j < E; ++j) v[j] = tile[zt<Q>(t + T * j, q)];
+  line_fft<NZ, +1>(v, t, [tile, q](int m) { return tile + zt<Q>(m, q); }, tw);
 #pragma unroll
-  for (int r = 0; r < E; ++r) tile[zt(line_out_index<NZ>(t, r), q)] = v[r];
+  for (int r = 0; r < E; ++r) tile[zt<Q>(line_out_index<NZ>(t, r), q)] = v[r];
 
   if constexpr (TMA) {
     fence_async_smem();
@@ -483,9 +533,9 @@ __global__ void __launch_bounds__(z_threads<NZ>(), (NZ <= 128 ? 3 : 1))
   } else {
     __syncthreads();
     for (int i = threadIdx.x; i < 3 * TILE; i += blockDim.x) {
-      const int qq = i % kZq, r = i / kZq;
+      const int qq = i % Q, r = i / Q;
       const int cc = r / NZ, kz = r - cc * NZ;
-      if (j0 + qq < ncols) p.spec[(long)r * ncols + j0 + qq] = TB[cc * TILE + zt(kz, qq)];
+      if (j0 + qq < ncols) p.spec[(long)r * ncols + j0 + qq] = TB[cc * TILE + zt<Q>(kz, qq)];
     }
   }
 }
@@ -517,7 +567,7 @@ size_t fast_xy_smem(int nx, int ny) {
 
 int fast_z_cols() { return kZq; }
 
-size_t fast_z_smem(int nz) { return sizeof(float2) * (3 * (size_t)nz * kZq + nz) + 1024; }
+size_t fast_z_smem(int nz, int q) { return sizeof(float2) * (3 * (size_t)nz * q + nz) + 1024; }
 
 cudaError_t fast_configure(const FluidPlan &p) {
   cudaError_t e = cudaSuccess;
@@ -534,16 +584,16 @@ cudaError_t fast_configure(const FluidPlan &p) {
       set((const void *)k_xy_inv_fast<NX, NY, DstField>, sxy);
       set((const void *)k_xy_inv_fast<NX, NY, DstAxpby>, sxy);
       set((const void *)k_xy_inv_fast<NX, NY, DstNeg>, sxy);
-      set((const void *)k_xy_inv_compose<NX, NY, false, false>, sxy);
-      set((const void *)k_xy_inv_compose<NX, NY, true, false>, sxy);
-      set((const void *)k_xy_inv_compose<NX, NY, false, true>, sxy);
-      set((const void *)k_xy_inv_compose<NX, NY, true, true>, sxy);
+      set((const void *)k_xy_inv_compose<NX, NY, false>, sxy);
+      set((const void *)k_xy_inv_compose<NX, NY, true>, sxy);
     });
   });
   dispatch_n(p.d.nz, [&](auto Z) {
     constexpr int NZ = decltype(Z)::value;
-    set((const void *)k_z_solve_fast<NZ, true>, p.fast_smem_z);
-    set((const void *)k_z_solve_fast<NZ, false>, p.fast_smem_z);
+    set((const void *)k_z_solve_fast<NZ, 16, true>, fast_z_smem(NZ, 16));
+    set((const void *)k_z_solve_fast<NZ, 16, false>, fast_z_smem(NZ, 16));
+    set((const void *)k_z_solve_fast<NZ, 8, true>, fast_z_smem(NZ, 8));
+    set((const void *)k_z_solve_fast<NZ, 8, false>, fast_z_smem(NZ, 8));
   });
   return e;
 }
@@ -575,15 +625,10 @@ cudaError_t fast_xy_inverse_compose(const FluidPlan &p, const ComposeArgs &a, cu
     dispatch_n(p.d.ny, [&](auto Y) {
       constexpr int NX = decltype(X)::value, NY = decltype(Y)::value;
       const dim3 grid(p.d.nz, 3);
-      const bool prep = a.idef != nullptr && NX >= 32;
-      if (a.fast && prep)
-        k_xy_inv_compose<NX, NY, true, true><<<grid, kXYThreads, p.fast_smem_xy, s>>>(p, a);
-      else if (a.fast)
-        k_xy_inv_compose<NX, NY, true, false><<<grid, kXYThreads, p.fast_smem_xy, s>>>(p, a);
-      else if (prep)
-        k_xy_inv_compose<NX, NY, false, true><<<grid, kXYThreads, p.fast_smem_xy, s>>>(p, a);
+      if (a.fast)
+        k_xy_inv_compose<NX, NY, true><<<grid, kXYThreads, p.fast_smem_xy, s>>>(p, a);
       else
-        k_xy_inv_compose<NX, NY, false, false><<<grid, kXYThreads, p.fast_smem_xy, s>>>(p, a);
+        k_xy_inv_compose<NX, NY, false><<<grid, kXYThreads, p.fast_smem_xy, s>>>(p, a);
     });
   });
   return cudaGetLastError();
@@ -591,13 +636,19 @@ cudaError_t fast_xy_inverse_compose(const FluidPlan &p, const ComposeArgs &a, cu
 
 cudaError_t fast_z_solve(const FluidPlan &p, int inverse, cudaStream_t s) {
   const long ncols = (long)p.d.ny * p.nxh;
-  const int grid = (int)((ncols + kZq - 1) / kZq);
+  const int q = p.fast_kq == 8 ? 8 : 16;
+  const int grid = (int)((ncols + q - 1) / q);
   dispatch_n(p.d.nz, [&](auto Z) {
     constexpr int NZ = decltype(Z)::value;
-    if (p.fast_tma)
-      k_z_solve_fast<NZ, true><<<grid, z_threads<NZ>(), p.fast_smem_z, s>>>(p, p.spec_map, inverse);
+    const size_t sm = fast_z_smem(NZ, q);
+    if (q == 8 && p.fast_tma)
+      k_z_solve_fast<NZ, 8, true><<<grid, z_threads<NZ, 8>(), sm, s>>>(p, p.spec_map, inverse);
+    else if (q == 8)
+      k_z_solve_fast<NZ, 8, false><<<grid, z_threads<NZ, 8>(), sm, s>>>(p, p.spec_map, inverse);
+    else if (p.fast_tma)
+      k_z_solve_fast<NZ, 16, true><<<grid, z_threads<NZ, 16>(), sm, s>>>(p, p.spec_map, inverse);
     else
-      k_z_solve_fast<NZ, false><<<grid, z_threads<NZ>(), p.fast_smem_z, s>>>(p, p.spec_map, inverse);
+      k_z_solve_fast<NZ, 16, false><<<grid, z_threads<NZ, 16>(), sm, s>>>(p, p.spec_map, inverse);
   });
   return cudaGetLastError();
 }

@@ -10,7 +10,7 @@ namespace aw {
 bool fast_supported(int n);
 size_t fast_xy_smem(int nx, int ny);
 int fast_z_cols();
-size_t fast_z_smem(int nz);
+size_t fast_z_smem(int nz, int q);
 cudaError_t fast_configure(const FluidPlan &p);
 template <class Src>
 cudaError_t fast_xy_forward(const FluidPlan &p, const Src &src, cudaStream_t s);

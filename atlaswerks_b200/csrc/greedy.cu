@@ -32,12 +32,13 @@ namespace {
 
 constexpr int kThreads = 256;
 
+// Rows per force-prep block: each block sums the energy of kPrepRows rows, so
+// the fixed-order final sum has few partials to read.
+constexpr int kPrepRows = 2;
+
 // I0(h) and the energy partials. With AFFINE the subject image lives on its
 // own grid di and h is in template voxels: the sample point is the atlas map
-// of h (atlas_point, interp.cuh). One row per block of 128 x; each warp
-// writes the double sum of its 32 voxels' (I1 - I0(h))^2 (energy_partial,
-// fluid.cuh), the same partial the fused inverse-and-update kernel writes
-// when it prepares the next iteration.
+// of h (atlas_point, interp.cuh). FAST: the float-tree interpolation.
 template <bool AFFINE, bool FAST>
 __global__ void __launch_bounds__(kRowThreads)
     k_force_prep(const float *__restrict__ I0, const float *__restrict__ I1,
@@ -45,21 +46,36 @@ __global__ void __launch_bounds__(kRowThreads)
                  const float *__restrict__ hz, float *__restrict__ idef, double *__restrict__ partials,
                  Dims d, Dims di, AtlasMap am) {
   const int x = blockIdx.x * kRowThreads + threadIdx.x;
-  const int y = blockIdx.y, z = blockIdx.z;
+  const int z = blockIdx.z;
   double e = 0.0;
   if (x < d.nx) {
-    const long i = ((long)z * d.ny + y) * d.nx + x;
-    double px = (double)hx[i], py = (double)hy[i], pz = (double)hz[i];
-    if (AFFINE) atlas_point(am, px, py, pz);
-    const float v = trilerp_scalar<FAST>(I0, AFFINE ? di : d, px, py, pz, 0.0f);
-    idef[i] = v;
-    e = energy_term(v, I1[i]);
+    const int y0 = blockIdx.y * kPrepRows;
+    const int y1 = min(y0 + kPrepRows, d.ny);
+    for (int y = y0; y < y1; ++y) {
+      const long i = ((long)z * d.ny + y) * d.nx + x;
+      double px = (double)hx[i], py = (double)hy[i], pz = (double)hz[i];
+      if (AFFINE) atlas_point(am, px, py, pz);
+      const float v = trilerp_scalar<FAST>(I0, AFFINE ? di : d, px, py, pz, 0.0f);
+      idef[i] = v;
+      const float r = -fsub(v, I1[i]);
+      e += (double)r * (double)r;
+    }
   }
-  energy_partial(e, x, y, z, d, partials);
+  __shared__ double ws[kRowThreads / 32];
+  e = warp_sum(e);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = e;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = threadIdx.x < kRowThreads / 32 ? ws[threadIdx.x] : 0.0;
+    t = warp_sum(t);
+    if (threadIdx.x == 0)
+      partials[((long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = t;
+  }
 }
 
 inline dim3 prep_grid(const Dims &d) {
-  return dim3((unsigned)((d.nx + kRowThreads - 1) / kRowThreads), (unsigned)d.ny, (unsigned)d.nz);
+  return dim3((unsigned)((d.nx + kRowThreads - 1) / kRowThreads),
+              (unsigned)((d.ny + kPrepRows - 1) / kPrepRows), (unsigned)d.nz);
 }
 
 // Fixed-order reduction of the block partials, so the energy is bitwise
@@ -435,7 +451,10 @@ int greedy_create(GreedyCtx *g, int nx, int ny, int nz, double spx, double spy, 
   g->sp = g->plan.sp;
   g->max_pert = max_pert;
   const long n = g->d.n();
-  g->nparts = (int)energy_partials(g->d);
+  {
+    const dim3 gr = prep_grid(g->d);
+    g->nparts = (int)(gr.x * gr.y * gr.z);
+  }
   g->sms = 148;
   cudaDeviceGetAttribute(&g->sms, cudaDevAttrMultiProcessorCount, g->plan.device);
   g->st.cap = history_cap > 0 ? history_cap : 4096;
@@ -530,8 +549,7 @@ cudaError_t greedy_stage(GreedyCtx *g, int stage, const float *I0, const float *
         k_update<<<row_grid(d), kRowThreads, 0, s>>>(a, d, g->st.step);
       return cudaGetLastError();
     }
-    case kStageInvCompose:
-    case kStageInvComposePrep: {
+    case kStageInvCompose: {
       // grids the fused kernel does not take run the two stages it replaces
       if (!g->plan.fast) {
         AW_TRY(greedy_stage(g, kStageXYInverse, I0, I1, h, h_out, hinv, hinv_out, auto_reduce,
@@ -539,19 +557,10 @@ cudaError_t greedy_stage(GreedyCtx *g, int stage, const float *I0, const float *
         return greedy_stage(g, kStageUpdate, I0, I1, h, h_out, nullptr, nullptr, auto_reduce,
                             solve_inverse, s);
       }
-      const bool prep = stage == kStageInvComposePrep && greedy_can_prep_ahead(g, false);
       const ComposeArgs a{h[0], h[1], h[2], h_out[0], h_out[1], h_out[2], g->st.step,
                           make_divf((float)g->sp.x), make_divf((float)g->sp.y),
-                          make_divf((float)g->sp.z), g->fast_interp,
-                          prep ? I0 : nullptr, prep ? I1 : nullptr, prep ? g->idef : nullptr,
-                          prep ? g->partials : nullptr};
-      AW_TRY(fluid_inverse_compose(g->plan, a, s));
-      if (stage == kStageInvComposePrep && !prep) {  // no prep-ahead here: a separate one
-        const float *ho[3] = {h_out[0], h_out[1], h_out[2]};
-        return greedy_stage(g, kStageForcePrep, I0, I1, ho, h_out, nullptr, nullptr, auto_reduce,
-                            solve_inverse, s);
-      }
-      return cudaSuccess;
+                          make_divf((float)g->sp.z), g->fast_interp};
+      return fluid_inverse_compose(g->plan, a, s);
     }
   }
   return cudaErrorInvalidValue;
@@ -566,20 +575,13 @@ cudaError_t greedy_stage(GreedyCtx *g, int stage, const float *I0, const float *
 // v = K f stays in shared memory. The step update needs max |v| over the
 // whole field before any voxel moves, and the inverse field gathers v at
 // h^-1(x) anywhere in the volume, so those iterations store v.
-bool greedy_can_prep_ahead(const GreedyCtx *g, bool inverse) {
-  // the fused kernel's warps each hold 32 x of one row; the atlas samples
-  // its subjects through the atlas map, which only the force preparation does
-  return !inverse && !g->no_fused_update && g->plan.fast && g->d.nx >= 32 && !g->am.on;
-}
-
 cudaError_t greedy_iterate(GreedyCtx *g, const float *I0, const float *I1, const float *const h[3],
                            float *const h_out[3], const float *const hinv[3],
                            float *const hinv_out[3], int update_step, int auto_reduce,
-                           cudaStream_t s, int have_prep, int prep_next) {
+                           cudaStream_t s) {
   const bool inv = hinv && hinv[0] && hinv_out && hinv_out[0];
   const bool fuse = !update_step && !inv && !g->no_fused_update && g->plan.fast;
-  if (!have_prep)
-    AW_TRY(greedy_stage(g, kStageForcePrep, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
+  AW_TRY(greedy_stage(g, kStageForcePrep, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
   AW_TRY(cudaEventRecord(g->ev_fork, s));
   AW_TRY(cudaStreamWaitEvent(g->aux, g->ev_fork, 0));
   AW_TRY(greedy_stage(g, kStageEnergy, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, g->aux));
@@ -588,9 +590,8 @@ cudaError_t greedy_iterate(GreedyCtx *g, const float *I0, const float *I1, const
   AW_TRY(greedy_stage(g, kStageZSolve, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
   if (fuse) {
     AW_TRY(cudaStreamWaitEvent(s, g->ev_join, 0));
-    const int st = prep_next && greedy_can_prep_ahead(g, false) ? kStageInvComposePrep
-                                                                 : kStageInvCompose;
-    return greedy_stage(g, st, I0, I1, h, h_out, nullptr, nullptr, auto_reduce, 1, s);
+    return greedy_stage(g, kStageInvCompose, I0, I1, h, h_out, nullptr, nullptr, auto_reduce, 1,
+                        s);
   }
   AW_TRY(greedy_stage(g, kStageXYInverse, I0, I1, h, h_out, hinv, hinv_out, auto_reduce, 1, s));
   AW_TRY(cudaStreamWaitEvent(s, g->ev_join, 0));

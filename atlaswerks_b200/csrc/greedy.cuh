@@ -46,9 +46,8 @@ enum GreedyStage {
   kStageXYInverse = 4,
   kStageMaxNorm = 5,
   kStageUpdate = 6,
-  kStageInvCompose = 7,      // xy-inverse and update in one kernel (v stays on chip)
-  kStageInvComposePrep = 8,  // the same, also preparing the next iteration from h'
-  kNumStages = 9
+  kStageInvCompose = 7,  // xy-inverse and update in one kernel (v stays on chip)
+  kNumStages = 8
 };
 
 int greedy_create(GreedyCtx *g, int nx, int ny, int nz, double spx, double spy, double spz,
@@ -58,15 +57,9 @@ cudaError_t greedy_stage(GreedyCtx *g, int stage, const float *I0, const float *
                          const float *const h[3], float *const h_out[3], const float *const hinv[3],
                          float *const hinv_out[3], int auto_reduce, int solve_inverse,
                          cudaStream_t s);
-// One iteration. have_prep: I0(h) and the energy partials of h are already
-// in the handle (the previous iteration prepared them); prep_next: prepare
-// the next iteration from h' (only where greedy_can_prep_ahead says so).
 cudaError_t greedy_iterate(GreedyCtx *g, const float *I0, const float *I1, const float *const h[3],
                            float *const h_out[3], const float *const hinv[3],
                            float *const hinv_out[3], int update_step, int auto_reduce,
-                           cudaStream_t s, int have_prep = 0, int prep_next = 0);
-// true when an iteration without a step update (and with an inverse field
-// or not) ends in the fused kernel that can prepare the next one
-bool greedy_can_prep_ahead(const GreedyCtx *g, bool inverse);
+                           cudaStream_t s);
 
 }  // namespace aw

@@ -46,7 +46,7 @@ E2E_ITERS = 25  # the 128^3 level of the 3-level multiscale config
 # traffic of that kernel's function; spectrum = 3 complex64 x (nx/2+1)/nx)
 SPEC = 3 * 8 * (N // 2 + 1) / N  # bytes/voxel of the 3-channel half spectrum
 STAGE_NAMES = ["force_prep", "energy", "xy_forward_fft", "z_solve", "xy_inverse_fft",
-               "max_norm", "update", "xy_inverse_update", "xy_inverse_update_prep"]
+               "max_norm", "update", "xy_inverse_update"]
 STAGE_BYTES = {
     "force_prep": 12 + 4 + 4 + 4,        # h, I1, I0 gather (once), I0(h) write
     "energy": 0,
@@ -56,9 +56,6 @@ STAGE_BYTES = {
     "max_norm": 12,
     "update": 12 + 12 + 12,              # v, h gather (once), h' write
     "xy_inverse_update": SPEC + 12 + 12,  # spectrum read, h gather (once), h' write
-    # ... and the next iteration's force preparation from h': I0 gather
-    # (once), I1 read, I0(h') write
-    "xy_inverse_update_prep": SPEC + 12 + 12 + 4 + 4 + 4,
 }
 B_ITER = 92  # bytes/voxel of the fully fused 3-pass greedy iteration (each stream once)
 B_ITER_INV = B_ITER + 36  # with h^-1: its read and write, v gathered at h^-1
@@ -383,9 +380,8 @@ def run_b200(args):
         *[t.data_ptr() for t in ho], *z, *z, 20, stream.cuda_stream, ms_stage))
     stage_ms = {n: float(ms_stage[i]) for i, n in enumerate(STAGE_NAMES)}
     # a steady-state iteration (no step update, no inverse field): the
-    # inverse transform, the update and the next iteration's force
-    # preparation run as one kernel
-    per_iter_stages = ["energy", "xy_forward_fft", "z_solve", "xy_inverse_update_prep"]
+    # inverse transform and the update run as one kernel
+    per_iter_stages = ["force_prep", "energy", "xy_forward_fft", "z_solve", "xy_inverse_update"]
     dom = max(per_iter_stages, key=lambda n: stage_ms[n])
     nvox = N ** 3
     dom_bytes = STAGE_BYTES[dom] * nvox
@@ -484,9 +480,9 @@ def run_b200(args):
                          f"(GreedyIteratorCPU{'' if kind == 'reference' else ' port'}; FFT = "
                          f"FP64 shim, not FFTW)"}
 
-    # four launches per steady-state iteration: energy, xy-forward, z-solve,
-    # xy-inverse fused with the update and the next force preparation
-    launches = 4 * per_rank_iters
+    # five launches per steady-state iteration: force-prep, energy,
+    # xy-forward, z-solve, xy-inverse fused with the update
+    launches = 5 * per_rank_iters
     line = {"metric": "128^3 fluid iters/s", "value": value, "unit": "iters/s",
             "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -859,8 +855,58 @@ def run_warmstart(args):
         "iters_warm_run_mean": float(np.mean([r["warm_iters_run"] for r in res])),
         "reached_fraction": float(np.mean([r["reached"] for r in res])),
         "fallback_fraction": float(np.mean([r["fallback"] for r in res])),
-        "vs_multiscale": multiscale}))
+        "vs_multiscale": multiscale, "network": network_rates(net, args)}))
     return 0
+
+
+def network_rates(net, args):
+    """The network's own rates on its grid: the forward pass (one graph
+    replay inside the predictor is the same launches) and a training step
+    (forward, loss, backward, Adam), each timed with CUDA events, with the
+    convolutions' FLOPs (2 * taps * Cin * Cout per voxel) against the
+    measured dense BF16 peak."""
+    import torch
+
+    from atlaswerks_b200 import warmstart as W
+    D, H, Wd = net.D, net.H, net.W
+    fwd = 0.0
+    for name, ci, co, t in W.LAYERS:
+        lvl = net._level_of(name)
+        fwd += 2.0 * t * ci * co * net._vox(lvl)
+    train_flops = 3.0 * fwd  # forward + data gradient + weight gradient
+    trainee = W.WarmStartNet((D, H, Wd), seed=3)
+    I0 = torch.rand((D, H, Wd), device="cuda")
+    I1 = torch.rand((D, H, Wd), device="cuda")
+    tgt = torch.zeros((3, D, H, Wd), device="cuda")
+    for _ in range(3):
+        net.forward(I0, I1)
+        trainee.train_step(I0, I1, tgt)
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    reps = 20
+    e[0].record()
+    for _ in range(reps):
+        net.forward(I0, I1)
+    e[1].record()
+    for _ in range(reps):
+        trainee.train_step(I0, I1, tgt)
+    e[2].record()
+    torch.cuda.synchronize()
+    f_ms = e[0].elapsed_time(e[1]) / reps
+    t_ms = e[1].elapsed_time(e[2]) / reps
+    peak = None
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        peak = float(json.load(open(pp))["bf16_tflops"])
+    out = {"grid": [D, H, Wd], "forward_ms": f_ms, "forward_gflop": fwd / 1e9,
+           "forward_tflops": fwd / (f_ms / 1000.0) / 1e12, "train_step_ms": t_ms,
+           "train_steps_per_s": 1000.0 / t_ms, "train_step_gflop": train_flops / 1e9,
+           "train_tflops": train_flops / (t_ms / 1000.0) / 1e12,
+           "peak_bf16_tflops": peak, "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)"}
+    if peak:
+        out["forward_frac_of_peak"] = out["forward_tflops"] / peak
+        out["train_frac_of_peak"] = out["train_tflops"] / peak
+    return out
 
 
 def _launch_ranks(n):

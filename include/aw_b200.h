@@ -161,7 +161,10 @@ int aw_fluid_destroy(aw_fluid_t k);
  * created (each candidate timed on the device; the choice is kept per grid
  * and device for the process); aw_fluid_autotune re-runs the tuning,
  * aw_fluid_set_shapes overrides it. Results do not depend on the shapes.
- * aw_fluid_get_shapes writes zeros on the register-FFT path (fixed shapes). */
+ * On the register-FFT path (every axis a power of two in [16, 256]) the
+ * only shape is the z pass's tile width, 16 or 8 (ky,kx) columns, also
+ * chosen by timing when a plan is created: aw_fluid_get_shapes writes
+ * {0, 0, width} and aw_fluid_set_shapes(k, 0, 0, width) overrides it. */
 int aw_fluid_get_shapes(aw_fluid_t k, int *shapes /* [3] */);
 int aw_fluid_set_shapes(aw_fluid_t k, int pairs, int cols, int zcols);
 int aw_fluid_autotune(aw_fluid_t k, void *stream);

@@ -184,11 +184,10 @@ def test_greedy_run_iterate_equivalence():
 
 
 @pytest.mark.parametrize("shape,n", [((64, 64, 64), 9), ((32, 64, 128), 4), ((16, 16, 32), 3)])
-def test_prepared_ahead_run_equals_iterations(shape, n):
-    """aw_greedy_run on power-of-two grids: its fused kernels prepare the
-    next iteration (I0(h') and the energy partials) so later iterations skip
-    the force preparation; the result equals repeated aw_greedy_iterate
-    (each preparing itself) bit for bit, fields and energies."""
+def test_fused_run_equals_iterations(shape, n):
+    """aw_greedy_run on power-of-two grids (the fused inverse-and-update
+    kernel inside captured graphs, two calls in a row) equals repeated
+    aw_greedy_iterate bit for bit, fields and energies."""
     nz, ny, nx = shape
     I0, I1 = greedy_pair(shape, seed=4, n_blobs=6, umax=2.0)
     p = GreedyIteratorParam(DiffOperParam(), 0.5)
@@ -199,7 +198,7 @@ def test_prepared_ahead_run_equals_iterations(shape, n):
         d = GreedyDeformationDataB200(cu(I0), cu(I1))
         if run:
             it.Run(d, n, update_first=True)
-            it.Run(d, n, update_first=False)  # a second call starts from its own preparation
+            it.Run(d, n, update_first=False)
         else:
             for k in range(2 * n):
                 if k == 0:
@@ -362,6 +361,31 @@ def test_fast_interpolation_within_tolerance(oracle):
     assert np.allclose(it.Energies(), e_o, rtol=1e-4)
 
 
+@pytest.mark.parametrize("shape", [(128, 128, 128), (64, 32, 16), (16, 32, 256)])
+def test_register_path_z_width_result_independent(shape):
+    """The register-FFT path's z pass in 16- and 8-column tiles (the width
+    is chosen by timing when a plan is created): bit-identical operators."""
+    import ctypes
+    from atlaswerks_b200 import _lib
+    L = _lib.lib()
+    rng = np.random.default_rng(22)
+    f = rng.normal(0, 1, (3,) + shape).astype(np.float32)
+    op = DiffOperB200()
+    op.SetSize(shape[::-1], (1.0, 1.3, 0.8), DiffOperParam(0.01, 0.01, 0.001))
+    sh = (ctypes.c_int * 3)()
+    _lib.check(L.aw_fluid_get_shapes(op._h, sh))
+    assert sh[0] == 0 and sh[1] == 0 and sh[2] in (8, 16)
+    outs = []
+    for width in (16, 8):
+        _lib.check(L.aw_fluid_set_shapes(op._h, 0, 0, width))
+        for inverse in (1, 0):
+            v = cu(f)
+            (op.ApplyInverseOperator if inverse else op.ApplyOperator)(v)
+            outs.append(host(v).copy())
+    assert np.array_equal(outs[0], outs[2]) and np.array_equal(outs[1], outs[3])
+    assert L.aw_fluid_set_shapes(op._h, 0, 0, 12) != 0
+
+
 @pytest.mark.parametrize("shape", [(36, 31, 32), (48, 40, 44), (96, 80, 72)])
 def test_fluid_shapes_autotuned_and_result_independent(shape):
     """The shared-memory FFT path picks its launch shapes by timing at plan
@@ -390,8 +414,8 @@ def test_fluid_shapes_autotuned_and_result_independent(shape):
     op2.SetSize(shape[::-1], (1.0, 1.3, 0.8), DiffOperParam(0.01, 0.01, 0.001))
     _lib.check(L.aw_fluid_get_shapes(op2._h, sh))
     assert tuple(sh) == tuned
-    # power-of-two grids: fixed register-FFT shapes
+    # power-of-two grids: the register-FFT path's only shape, the z width
     op3 = DiffOperB200()
     op3.SetSize((32, 32, 32), (1.0, 1.0, 1.0), DiffOperParam(0.01, 0.01, 0.001))
     _lib.check(L.aw_fluid_get_shapes(op3._h, sh))
-    assert tuple(sh) == (0, 0, 0)
+    assert tuple(sh)[:2] == (0, 0) and sh[2] in (8, 16)
