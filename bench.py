@@ -738,8 +738,10 @@ def run_adshoot(args):
     value = args.steps / (ms / 1000.0)
     peak, kind = peaks()
     # per voxel: T x (advance 100 + velocity 20 + 4S) + T x backward step (176 + 4S)
-    # + energies, the first adjoint splat, the alpha0 update and the map copies (160 + 4S)
-    b_iter = (T * (296 + 8 * SPEC) + 160 + 4 * SPEC) * N ** 3
+    # + the kinetic energy from the force (20), the image residual (12), the first
+    # adjoint splat (20), clearing alpha~ (4), the alpha0 update (28) and the map
+    # copies (48): 132
+    b_iter = (T * (296 + 8 * SPEC) + 132) * N ** 3
     gbs = b_iter * value / 1e9
     print(json.dumps({
         "metric": "128^3 adjoint shooting iterations/s (T=5)", "value": value, "unit": "iters/s",

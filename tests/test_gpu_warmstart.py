@@ -116,6 +116,43 @@ def test_c_abi_register_reaches_plain_energy():
     ws.close()
 
 
+def test_c_abi_wall_time_ratio_at_128():
+    """The warm start's headline bar through the C ABI at 128^3 (network at
+    64^3): over four held-out pairs, aw_warmstart_register (prediction,
+    refinement, fallback where taken) reaches the plain solve's final energy
+    (+1 %) in at most half the plain solve's device time. Both paths have
+    their handles and graphs built before the clocks start, and both clocks
+    include the energy read back that ends them."""
+    n = 128
+    net = W.trained(n)
+    ws = W.WarmStartB200(net, (n, n, n))
+    h = torch.empty((3, n, n, n), device="cuda")
+    pairs = W.make_pairs(range(20_000_500, 20_000_504), n, 0)
+    it = W._greedy((n, n, n))
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    plain_ms = warm_ms = 0.0
+    for k, (I0n, I1n) in enumerate(pairs):
+        I0, I1 = torch.from_numpy(I0n).cuda(), torch.from_numpy(I1n).cuda()
+        d = GreedyDeformationDataB200(I0, I1)
+        if k == 0:  # graphs and pools of both paths, outside the clocks
+            it.Run(d, 50, update_first=True)
+            ws.register(I0, I1, h, 0.0, 3, 3, 3)
+            d = GreedyDeformationDataB200(I0, I1)
+        torch.cuda.synchronize()
+        ev[0].record()
+        it.Run(d, 50, update_first=True)
+        target = float(it.Energies()[-1]) * 1.01
+        ev[1].record()
+        ev[2].record()
+        run, fell_back = ws.register(I0, I1, h, target, 25, 3, 50)
+        ev[3].record()
+        torch.cuda.synchronize()
+        plain_ms += ev[0].elapsed_time(ev[1])
+        warm_ms += ev[2].elapsed_time(ev[3])
+    ws.close()
+    assert warm_ms <= 0.5 * plain_ms, (warm_ms, plain_ms)
+
+
 def _pair_losses(net, pairs, targets):
     out = []
     for (a, b), t in zip(pairs, targets):
