@@ -57,6 +57,10 @@ SIGNATURES = {
     "aw_fluid_get_shapes": ([_fp, _fp], _i),
     "aw_fluid_set_shapes": ([_fp, _i, _i, _i], _i),
     "aw_fluid_autotune": ([_fp, _fp], _i),
+    "aw_fluid_status": ([_fp, _fp, _fp], _i),
+    "aw_fluid_wait_selftest": ([_fp, _i, _fp], _i),
+    "aw_greedy_status": ([_fp, _fp, _fp], _i),
+    "aw_ldmm_status": ([_fp, _fp, _fp], _i),
     "aw_greedy_create": ([_i] * 3 + [_d] * 3 + [_f] * 4 + [_fp], _i),
     "aw_greedy_destroy": ([_fp], _i),
     "aw_greedy_set_step": ([_fp, _f], _i),

@@ -45,9 +45,11 @@ __device__ __forceinline__ void bulk_load(void *smem_dst, const void *gmem_src, 
       : "memory");
 }
 
-// Waits for phase `parity` of the mbarrier; false (and *status set) on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, int *status) {
-  for (int it = 0; it < kMaxWaitIters; ++it) {
+// Waits for phase `parity` of the mbarrier; false (and *status set) after
+// max_iters unsuccessful polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, int *status,
+                                          int max_iters = kMaxWaitIters) {
+  for (int it = 0; it < max_iters; ++it) {
     uint32_t ok;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"

@@ -293,6 +293,19 @@ int aw_fluid_autotune(aw_fluid_t k, void *stream) {
   return 0;
 }
 
+int aw_fluid_status(aw_fluid_t k, int *timed_out, void *stream) {
+  if (!k || !timed_out) return fail("aw_fluid_status: null pointer");
+  AW_CUDA(aw::fluid_take_status(&k->plan, timed_out, S(stream)), "aw_fluid_status");
+  return 0;
+}
+
+int aw_fluid_wait_selftest(aw_fluid_t k, int polls, void *stream) {
+  if (!k) return fail("aw_fluid_wait_selftest: null handle");
+  if (polls < 1 || polls > 4096) return fail("aw_fluid_wait_selftest: polls must be in [1, 4096]");
+  AW_CUDA(aw::fluid_wait_selftest(k->plan, polls, S(stream)), "aw_fluid_wait_selftest");
+  return 0;
+}
+
 int aw_fluid_destroy(aw_fluid_t k) {
   if (!k) return 0;
   aw::fluid_plan_destroy(&k->plan);
@@ -346,6 +359,12 @@ int aw_greedy_set_step(aw_greedy_t g, float step) {
   if (!g) return fail("aw_greedy_set_step: null handle");
   AW_CUDA(cudaMemcpy(g->ctx.st.step, &step, sizeof(float), cudaMemcpyHostToDevice),
           "aw_greedy_set_step");
+  return 0;
+}
+
+int aw_greedy_status(aw_greedy_t g, int *timed_out, void *stream) {
+  if (!g || !timed_out) return fail("aw_greedy_status: null pointer");
+  AW_CUDA(aw::fluid_take_status(&g->ctx.plan, timed_out, S(stream)), "aw_greedy_status");
   return 0;
 }
 
@@ -724,6 +743,12 @@ int aw_ldmm_set_step(aw_ldmm_t l, float step) {
   if (!l) return fail("aw_ldmm_set_step: null handle");
   AW_CUDA(cudaMemcpy(l->ctx.step, &step, sizeof(float), cudaMemcpyHostToDevice),
           "aw_ldmm_set_step");
+  return 0;
+}
+
+int aw_ldmm_status(aw_ldmm_t l, int *timed_out, void *stream) {
+  if (!l || !timed_out) return fail("aw_ldmm_status: null pointer");
+  AW_CUDA(aw::fluid_take_status(&l->ctx.plan, timed_out, S(stream)), "aw_ldmm_status");
   return 0;
 }
 

@@ -17,6 +17,7 @@
 #include <tuple>
 #include <vector>
 
+#include "bulk.cuh"
 #include "fluid.cuh"
 #include "tma_host.cuh"
 #include "fluid_fast.cuh"
@@ -520,6 +521,37 @@ int fluid_plan_create(FluidPlan *p, int nx, int ny, int nz, double spx, double s
   if (p->fast) tune_z_cols(p);
   if (!p->fast && fluid_autotune(p, 0) != cudaSuccess) return 4;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+
+namespace {
+
+// The timeout path of the transform kernels, run on purpose: nothing ever
+// arrives on this barrier, so every thread's bounded wait gives up after
+// `polls` polls, the status word records it, and the CTA leaves together
+// as a transform CTA does when its slab never lands. Nothing is in flight
+// on the barrier when the CTA exits.
+__global__ void k_wait_selftest(int *status, int polls) {
+  __shared__ __align__(8) uint64_t mbar;
+  if (threadIdx.x == 0) mbar_init(&mbar, 1);
+  __syncthreads();
+  const bool ok = mbar_wait(&mbar, 0, status, polls);
+  (void)__syncthreads_or(!ok);
+}
+
+}  // namespace
+
+cudaError_t fluid_wait_selftest(const FluidPlan &p, int polls, cudaStream_t s) {
+  k_wait_selftest<<<1, 32, 0, s>>>(p.status, polls);
+  return cudaGetLastError();
+}
+
+cudaError_t fluid_take_status(FluidPlan *p, int *timed_out, cudaStream_t s) {
+  int v = 0;
+  cudaError_t e = cudaMemcpyAsync(&v, p->status, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
+  *timed_out = v == kStatusWaitTimeout ? 1 : 0;
+  return v ? cudaMemsetAsync(p->status, 0, sizeof(int), s) : cudaSuccess;
 }
 
 void fluid_plan_destroy(FluidPlan *p) {

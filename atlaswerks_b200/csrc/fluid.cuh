@@ -278,6 +278,12 @@ cudaError_t fluid_solve(const FluidPlan &p, int inverse, cudaStream_t s);
 int fluid_get_shapes(const FluidPlan &p, int *P, int *Q, int *K);
 cudaError_t fluid_set_shapes(FluidPlan *p, int P, int Q, int K);
 cudaError_t fluid_autotune(FluidPlan *p, cudaStream_t s);
+// the plan's status word: *timed_out = 1 when a transform kernel's bounded
+// wait ran out since the last call; the word is cleared (stream-ordered)
+cudaError_t fluid_take_status(FluidPlan *p, int *timed_out, cudaStream_t s);
+// one CTA whose bounded wait (polls polls) on an mbarrier that nothing
+// arrives on runs out and records the timeout in the plan's status word
+cudaError_t fluid_wait_selftest(const FluidPlan &p, int polls, cudaStream_t s);
 cudaError_t fluid_inverse_store(const FluidPlan &p, float *ox, float *oy, float *oz,
                                 cudaStream_t s);
 cudaError_t fluid_inverse_store_neg(const FluidPlan &p, float *ox, float *oy, float *oz,

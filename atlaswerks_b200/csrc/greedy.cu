@@ -13,7 +13,9 @@
 //
 // plus, at a step-size update (iteration 0 of a scale level,
 // GreedyWarp.txx:99), a max|v| reduction and eps = MaxPert / max|v| computed
-// on the device (GreedyIteratorCPU.cxx:125-131).
+// on the device (GreedyIteratorCPU.cxx:125-131). On the register-FFT path,
+// iterations without a step update or an inverse field run 5 and 6 as one
+// kernel (k_xy_inv_compose, fluid_fast.cu): five launches.
 #include <algorithm>
 #include <climits>
 #include <cstring>

@@ -80,6 +80,14 @@ class DiffOperB200:
     def ApplyInverseOperator(self, v: torch.Tensor) -> torch.Tensor:
         return self._apply(v, 1)
 
+    def TimedOut(self) -> bool:
+        """True when a transform's bounded wait ran out since the last call
+        (its output is then incomplete); synchronises the current stream and
+        clears the flag."""
+        flag = ctypes.c_int()
+        check(_lib.lib().aw_fluid_status(self._h, ctypes.byref(flag), _stream()))
+        return bool(flag.value)
+
     def _free(self):
         if self._h:
             _lib.lib().aw_fluid_destroy(self._h)

@@ -168,6 +168,19 @@ int aw_fluid_destroy(aw_fluid_t k);
 int aw_fluid_get_shapes(aw_fluid_t k, int *shapes /* [3] */);
 int aw_fluid_set_shapes(aw_fluid_t k, int pairs, int cols, int zcols);
 int aw_fluid_autotune(aw_fluid_t k, void *stream);
+/* Every wait of the transform kernels on a bulk or TMA copy is bounded: a
+ * wait that runs out records a timeout in the handle's status word and the
+ * kernel returns early, leaving its output incomplete, instead of spinning.
+ * aw_fluid_status synchronises `stream`, sets *timed_out to 1 when that
+ * happened since the last call (else 0) and clears the word. No counterpart
+ * in the reference, whose transforms have no waits. */
+int aw_fluid_status(aw_fluid_t k, int *timed_out, void *stream);
+/* Runs the timeout path on purpose: one CTA waits, with the same bounded
+ * wait the transforms use but limited to `polls` polls (1..4096), on a
+ * barrier that nothing arrives on, and records the timeout in the handle's
+ * status word; the context stays usable. A check of the status reporting
+ * for tests and health probes; no counterpart in the reference. */
+int aw_fluid_wait_selftest(aw_fluid_t k, int polls, void *stream);
 
 /* ---------------------------------------------------------------------------
  * Greedy iterator. Replaces GreedyIteratorGPU / GreedyIteratorCPU
@@ -184,6 +197,8 @@ int aw_greedy_destroy(aw_greedy_t g);
 /* GreedyDeformationData::StepSize(s) / StepSize(); get synchronises. */
 int aw_greedy_set_step(aw_greedy_t g, float step);
 int aw_greedy_get_step(aw_greedy_t g, float *step);
+/* aw_fluid_status for the iterator's transforms and staged update. */
+int aw_greedy_status(aw_greedy_t g, int *timed_out, void *stream);
 /* GreedyParam::AutoStepReduce (Greedy/GreedyParam.h:61-65); off by default. */
 int aw_greedy_set_auto_step_reduce(aw_greedy_t g, int on);
 /* on = 1 (default): the update stages h over each tile (plus a one-voxel
@@ -305,6 +320,8 @@ int aw_ldmm_use_orig_gradient_calc(aw_ldmm_t l, int on);
 /* LDMMDeformationData::StepSize(s) / StepSize(); get synchronises. */
 int aw_ldmm_set_step(aw_ldmm_t l, float step);
 int aw_ldmm_get_step(aw_ldmm_t l, float *step);
+/* aw_fluid_status for the iterator's transforms. */
+int aw_ldmm_status(aw_ldmm_t l, int *timed_out, void *stream);
 /* One Iterate(): updates v in place. update_step=1 instead computes the step
  * from max |2v - (2/sigma^2) K f| and leaves v unchanged
  * (UseAdaptiveStepSize, LDMM/LDMMWarp.txx:99-104). */

@@ -106,6 +106,35 @@ def test_fluid_roundtrip_identity():
     assert float((d.astype(np.float64) ** 2).sum()) <= 0.1
 
 
+def test_bounded_wait_runs_out_and_is_reported():
+    """The transforms' bounded wait, run out on purpose (one CTA waiting 64
+    polls on a barrier that nothing arrives on): the handle's status word
+    reports the timeout once and is cleared by the read, and the context
+    stays usable — the next L^-1 L round trip is correct with a clean status."""
+    import ctypes
+    from atlaswerks_b200 import _lib
+    op = DiffOperB200()
+    op.SetSize((32, 32, 32), (1.0, 1.0, 1.0), DiffOperParam())
+    assert not op.TimedOut()
+    s = torch.cuda.current_stream().cuda_stream
+    assert _lib.lib().aw_fluid_wait_selftest(op._h, 64, s) == 0
+    assert op.TimedOut()
+    assert not op.TimedOut()
+    assert _lib.lib().aw_fluid_wait_selftest(op._h, 0, s) != 0  # polls out of range
+    f = np.random.default_rng(6).normal(0, 1, (3, 32, 32, 32)).astype(np.float32)
+    v = cu(f)
+    op.ApplyOperator(v)
+    op.ApplyInverseOperator(v)
+    d = host(v) - f
+    assert float((d.astype(np.float64) ** 2).sum()) <= 0.1
+    assert not op.TimedOut()
+    flag = ctypes.c_int(-1)
+    it = GreedyIteratorB200((32, 32, 32))
+    it.SetScaleLevel((32, 32, 32), (1.0, 1.0, 1.0), GreedyIteratorParam(DiffOperParam(), 0.5))
+    assert _lib.lib().aw_greedy_status(it._h, ctypes.byref(flag), s) == 0
+    assert flag.value == 0
+
+
 def test_diffoper_rejects_unsupported():
     op = DiffOperB200()
     with pytest.raises(ValueError):
