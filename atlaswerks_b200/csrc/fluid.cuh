@@ -208,6 +208,7 @@ struct DstFieldBound {
   AW_D void store(long i, float v) const { c[i] = v; }
 };
 struct DstField {
+  static constexpr bool kReads = false;
   float *c[3];
   AW_D DstFieldBound bind(int comp) const {
     return DstFieldBound{comp == 0 ? c[0] : comp == 1 ? c[1] : c[2]};
@@ -221,6 +222,7 @@ struct DstNegBound {
   AW_D void store(long i, float v) const { c[i] = -v; }
 };
 struct DstNeg {
+  static constexpr bool kReads = false;
   float *c[3];
   AW_D DstNegBound bind(int comp) const {
     return DstNegBound{comp == 0 ? c[0] : comp == 1 ? c[1] : c[2]};
@@ -235,8 +237,18 @@ struct DstAxpbyBound {
   float *c;
   float vfac, ufac;
   AW_D void store(long i, float u) const { c[i] = fadd(fmul(vfac, c[i]), fmul(ufac, u)); }
+  // n elements: every old value is read before any is written
+  template <int N>
+  AW_D void store_n(const long (&i)[N], const float (&u)[N]) const {
+    float old[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) old[j] = c[i[j]];
+#pragma unroll
+    for (int j = 0; j < N; ++j) c[i[j]] = fadd(fmul(vfac, old[j]), fmul(ufac, u[j]));
+  }
 };
 struct DstAxpby {
+  static constexpr bool kReads = true;
   float *c[3];
   const float *step;
   float sigma;

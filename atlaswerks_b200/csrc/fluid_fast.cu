@@ -340,8 +340,32 @@ __global__ void __launch_bounds__(kXYThreads, (XYShape<NX, NY>::ctas()))
   inv_y_pass<NX, NY>(C, twy, warp, lane);
   __syncthreads();
   const auto o = dst.bind(comp);
-  inv_x_pass<NX, NY>(C, twx, warp, lane,
-                     [&](int x, int y, float v) { o.store(d.idx(x, y, z), v); });
+  if constexpr (Dst::kReads && NX >= 32) {
+    // a store that reads the old value (the LDMM update): the x pass leaves
+    // the plane in shared memory, then each thread reads kBatch old values
+    // before it writes any, so their loads overlap instead of each waiting
+    // behind the previous store
+    inv_x_pass<NX, NY>(C, twx, warp, lane, [](int, int, float) {});
+    __syncthreads();
+    constexpr int NXH = XYShape<NX, NY>::NXH, PER = NX * NY / kXYThreads;
+    constexpr int kBatch = PER < 8 ? PER : 8;
+    const float *P = reinterpret_cast<const float *>(C);
+#pragma unroll 1
+    for (int k0 = 0; k0 < PER; k0 += kBatch) {
+      long idx[kBatch];
+      float u[kBatch];
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        const int e = threadIdx.x + kXYThreads * (k0 + j), y = e / NX, x = e % NX;
+        idx[j] = d.idx(x, y, z);
+        u[j] = P[y * 2 * NXH + x];
+      }
+      o.template store_n<kBatch>(idx, u);
+    }
+  } else {
+    inv_x_pass<NX, NY>(C, twx, warp, lane,
+                       [&](int x, int y, float v) { o.store(d.idx(x, y, z), v); });
+  }
 }
 
 // The inverse transform fused with the greedy update h'(x) = h(x + eps v(x)/sp)
@@ -383,10 +407,13 @@ __global__ void __cluster_dims__(1, 3, 1) __launch_bounds__(kXYThreads, (XYShape
     const float *V1 = reinterpret_cast<const float *>(cluster.map_shared_rank(C, 1));
     const float *V2 = reinterpret_cast<const float *>(cluster.map_shared_rank(C, 2));
     const float eps = *a.step;
+    // CTA `comp` updates a contiguous third of the rows, so the h rows
+    // that neighbouring rows' gathers share are read close together in time
     constexpr int RPI = kXYThreads / NX;  // rows per pass
     const int x = threadIdx.x % NX;
+    const int y1 = (comp + 1) * NY / 3;
 #pragma unroll 2
-    for (int y = comp + 3 * (threadIdx.x / NX); y < NY; y += 3 * RPI) {
+    for (int y = comp * NY / 3 + threadIdx.x / NX; y < y1; y += RPI) {
       const int e = y * 2 * NXH + x;
       const float vx = V0[e], vy = V1[e], vz = V2[e];
       const float px = fadd(__int2float_rn(x), fdivq(fmul(vx, eps), a.q0));
