@@ -841,6 +841,35 @@ int aw_ldmm_atlas_normalize(float *acc, const float *jacsum, long n, void *strea
   return 0;
 }
 
+int aw_ldmm_atlas_voxel_median(const float *const *images, int n_images, int k, int nx, int ny,
+                               int nz, float *out, void *stream) {
+  std::string why;
+  if (!images || !out) return fail("aw_ldmm_atlas_voxel_median: null pointer");
+  if (n_images < 1 || n_images > aw::kVoxelMedianMaxImages)
+    return fail("aw_ldmm_atlas_voxel_median: n_images must be in [1, " +
+                std::to_string(aw::kVoxelMedianMaxImages) + "]");
+  if (k < 0 || k >= n_images) return fail("aw_ldmm_atlas_voxel_median: k must be in [0, n_images)");
+  if (nx < 1 || ny < 1 || nz < 1) return fail("aw_ldmm_atlas_voxel_median: empty grid");
+  aw::VoxelImages in{};
+  for (int m = 0; m < n_images; ++m) {
+    if (!images[m]) return fail("aw_ldmm_atlas_voxel_median: null image pointer");
+    in.img[m] = images[m];
+  }
+  cudaStream_t s = S(stream);
+  void *scratch = nullptr;
+  AW_CUDA(cudaMallocAsync(&scratch, 4 * sizeof(unsigned), s), "aw_ldmm_atlas_voxel_median (scratch)");
+  unsigned *range = static_cast<unsigned *>(scratch);
+  int *open = reinterpret_cast<int *>(range + 2);
+  cudaError_t e = aw::ldmm_voxel_median(in, n_images, k, (long)nx * ny * nz, out, range, open, s);
+  int h_open = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h_open, open, sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaFreeAsync(scratch, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  AW_CUDA(e, "aw_ldmm_atlas_voxel_median");
+  if (h_open) return fail("aw_ldmm_atlas_voxel_median: the per-voxel selection did not converge");
+  return 0;
+}
+
 int aw_ldmm_shoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *alpha0,
                           float *phi0T, float *phiT0, void *stream) {
   if (!l || !I0 || !I1 || !alpha0 || !phi0T || !phiT0)

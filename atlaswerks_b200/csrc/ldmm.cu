@@ -15,6 +15,7 @@
 // With a step-size update (UseAdaptiveStepSize at iteration 0) v is left
 // unchanged and eps = MaxPert / max_t max_x |2 v_t - (2/sigma^2) K f_t| is
 // formed on the device (LDMMIteratorCPU.cxx:192-212, 625-628).
+#include <algorithm>
 #include <cstring>
 
 #include "interp.cuh"
@@ -620,6 +621,136 @@ cudaError_t ldmm_atlas_accumulate(float *acc, float *jsum, const float *img, con
 
 cudaError_t ldmm_atlas_normalize(float *acc, const float *jsum, long n, cudaStream_t s) {
   k_atlas_normalize<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(acc, jsum, n);
+  return cudaGetLastError();
+}
+
+// ---- the per-voxel median of the deformed subjects ------------------------
+// MedianCalculator::Select(std::vector<RealImage*>, k, rtn) (Algorithms/
+// Common/MedianCalculator.cxx:264-389), used as the atlas with
+// UsePerVoxelMedian (LDMMAtlasBuilder.txx:218-233, 336-338): per voxel a
+// bisection on the value between the voxel's min and max over the images;
+// each round counts the values below the midpoint p and takes the largest
+// value below it and the smallest at or above it; the voxel ends when the
+// count is k (the latter) or k + 1 (the former), or when its interval is
+// narrower than eps = (max over the volume - min over the volume) / 10000
+// (its lower end). Voxels are independent, so each thread runs its own
+// rounds; a voxel still open after round nImages + 1 is the reference's
+// "not converging" error.
+namespace {
+
+__device__ __forceinline__ unsigned order_key(float f) {
+  const unsigned u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float key_value(unsigned k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+// min / max over the images at one voxel (MedianCalculator::MinMax)
+__device__ __forceinline__ void voxel_min_max(const VoxelImages &in, int nimg, long i, float &mn,
+                                              float &mx) {
+  mn = mx = in.img[0][i];
+  for (int m = 1; m < nimg; ++m) {
+    const float v = in.img[m][i];
+    mn = v < mn ? v : mn;
+    mx = v > mx ? v : mx;
+  }
+}
+
+// range[0] / range[1]: order keys of the volume's smallest min and largest max
+__global__ void k_median_range(const __grid_constant__ VoxelImages in, int nimg, long n,
+                               unsigned *range) {
+  __shared__ unsigned lo_s[8], hi_s[8];
+  unsigned lo = 0xffffffffu, hi = 0u;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    float mn, mx;
+    voxel_min_max(in, nimg, i, mn, mx);
+    lo = min(lo, order_key(mn));
+    hi = max(hi, order_key(mx));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    lo_s[w] = lo;
+    hi_s[w] = hi;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
+      lo = min(lo, lo_s[k]);
+      hi = max(hi, hi_s[k]);
+    }
+    atomicMin(&range[0], lo);
+    atomicMax(&range[1], hi);
+  }
+}
+
+__global__ void k_median_select(const __grid_constant__ VoxelImages in, int nimg, unsigned k,
+                                long n, const unsigned *range, float *out, int *open) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float eps = fdiv(fsub(key_value(range[1]), key_value(range[0])), 10000.f);
+  float gmin, gmax;
+  voxel_min_max(in, nimg, i, gmin, gmax);
+  float cmin = gmin, cmax = gmax, r = gmin;
+  bool done = false;
+  for (int iter = 0; !done; ++iter) {
+    if (eps > fabsf(fsub(cmax, cmin))) {
+      r = cmin;
+      break;
+    }
+    // (curMin + curMax) / 2.0 stored as float: the float sum halved exactly
+    const float p = fmul(fadd(cmin, cmax), 0.5f);
+    unsigned idx = 0;
+    float vp = gmin, vn = gmax;
+    for (int m = 0; m < nimg; ++m) {
+      const float v = in.img[m][i];
+      if (v < p) {
+        ++idx;
+        if (v > vp) vp = v;
+      } else if (v < vn) {
+        vn = v;
+      }
+    }
+    if (idx == k) {
+      r = vn;
+      done = true;
+    } else if (idx - 1u == k) {
+      r = vp;
+      done = true;
+    } else if (idx > k) {
+      cmax = vp;
+    } else if (idx < k) {
+      cmin = vn;
+    }
+    if (!done && iter > nimg) {
+      atomicExch(open, 1);
+      r = cmin;
+      break;
+    }
+  }
+  out[i] = r;
+}
+
+}  // namespace
+
+cudaError_t ldmm_voxel_median(const VoxelImages &in, int nimg, int k, long n, float *out,
+                              unsigned *range, int *open, cudaStream_t s) {
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(range, 0xff, sizeof(unsigned), s)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(range + 1, 0, sizeof(unsigned), s)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(open, 0, sizeof(int), s)) != cudaSuccess) return e;
+  int sms = 148, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long blocks = std::min<long>((n + 255) / 256, 4L * sms);
+  k_median_range<<<(unsigned)blocks, 256, 0, s>>>(in, nimg, n, range);
+  k_median_select<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(in, nimg, (unsigned)k, n, range,
+                                                             out, open);
   return cudaGetLastError();
 }
 

@@ -55,6 +55,15 @@ cudaError_t ldmm_i1_at_0(LdmmCtx *c, const float *I1, const float *v, float *img
 cudaError_t ldmm_atlas_accumulate(float *acc, float *jsum, const float *img, const float *jd,
                                   float w, long n, cudaStream_t s);
 cudaError_t ldmm_atlas_normalize(float *acc, const float *jsum, long n, cudaStream_t s);
+// the per-voxel k-th smallest value over up to kVoxelMedianMaxImages images
+// by the reference's bisection (MedianCalculator::Select); range: 2 unsigned
+// and open: 1 int of device scratch; *open = 1 when a voxel did not converge
+constexpr int kVoxelMedianMaxImages = 256;
+struct VoxelImages {
+  const float *img[kVoxelMedianMaxImages];
+};
+cudaError_t ldmm_voxel_median(const VoxelImages &in, int nimg, int k, long n, float *out,
+                              unsigned *range, int *open, cudaStream_t s);
 // the momentum shooting's scratch (returns 3 when the allocation fails)
 int ldmm_shoot_prepare(LdmmCtx *c);
 cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, float *alpha0,

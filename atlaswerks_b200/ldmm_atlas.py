@@ -21,8 +21,18 @@ LDMMAtlasThreadCPU / LDMMAtlasThreadGPU inside AtlasThread::AtlasThreadMain
   all-reduces (sum) over the process group complete them, the exchange of
   LDMMAtlasBuilder::SumAcrossNodes (.txx:236-269, MPI_Allreduce there).
 
-Not built: ComputeMedian / TrimmedMeanSize re-weighting, UsePerVoxelMedian,
-the PCA step, multiscale (one scale level per BuildAtlas call).
+With UsePerVoxelMedian the mean is instead the per-voxel median of the
+subjects' deformed images I1_i(h_i,0->1) (MedianCalculator::Select,
+LDMMAtlasBuilder::ComputeMedian, .txx:218-233, 336-338), by the reference's
+bisection in libaw_b200.so (``aw_ldmm_atlas_voxel_median``); with several
+ranks every deformed image is broadcast by its owner first, so each rank
+selects over all of them (the selection does not depend on their order).
+
+Not built: the ComputeMedian (inverse-distance) and TrimmedMeanSize
+re-weightings, which weigh subjects by sqrt of their last total LDMM
+energy, image plus velocity terms (LDMMAtlasThreadCPU.cxx:175-181, 225-237,
+LDMMAtlasBuilder.txx:437-500): the iterations here record the image term
+only; the PCA step; multiscale (one scale level per BuildAtlas call).
 
 The per-rank work runs in libaw_b200.so (``aw_ldmm_*``) through
 ``CudaLDMMAtlasEngine``; the builder only sequences it and the collectives.
@@ -53,6 +63,7 @@ class LDMMAtlasParam:
     NIterations: int = 50
     JacobianScale: bool = True
     UseOrigGradientCalc: bool = False
+    UsePerVoxelMedian: bool = False
 
 
 class CudaLDMMAtlasEngine:
@@ -99,6 +110,25 @@ class CudaLDMMAtlasEngine:
                                              self._img.data_ptr(),
                                              self._jd.data_ptr() if js else None, w, self.n, s))
         return self.acc, (self.jsum if js else None)
+
+    def deformed(self) -> List[torch.Tensor]:
+        """This rank's deformed images I1_i(h_i,0->1), in subject order."""
+        L, s = _lib.lib(), _stream()
+        if not hasattr(self, "_defs"):
+            self._defs = [torch.empty(self.shape, device="cuda") for _ in self.its]
+        for it, d, out in zip(self.its, self.data, self._defs):
+            check(L.aw_ldmm_i1_at_0(it._h, d.I1.data_ptr(), d.V.data_ptr(), out.data_ptr(), None,
+                                    s))
+        return self._defs
+
+    def set_median(self, images: Sequence[torch.Tensor], k: int) -> torch.Tensor:
+        """The mean as the per-voxel k-th smallest of the given deformed
+        images (all subjects')."""
+        nz, ny, nx = self.shape
+        ptrs = (ctypes.c_void_p * len(images))(*[t.data_ptr() for t in images])
+        check(_lib.lib().aw_ldmm_atlas_voxel_median(ptrs, len(images), int(k), nx, ny, nz,
+                                                    self.mean.data_ptr(), _stream()))
+        return self.mean
 
     def set_mean(self, acc: torch.Tensor, jsum: Optional[torch.Tensor]) -> torch.Tensor:
         """The new mean from the (all-reduced) sums, into the I0 every
@@ -159,7 +189,29 @@ class LDMMAtlasBuilderB200:
                               [images[i] for i in self.local], [weights[i] for i in self.local])
         self.mean = None
 
+    @staticmethod
+    def median_index(n: int) -> int:
+        """LDMMAtlasBuilder::ComputeMedian's index (LDMMAtlasBuilder.txx:222)."""
+        return n // 2 - 1 if n % 2 == 0 else n // 2
+
+    def _update_median(self):
+        mine = self.engine.deformed()
+        if self.group is None or self.world == 1:
+            allimgs = list(mine)
+        else:
+            import torch.distributed as dist
+            allimgs = []
+            for i in range(self.n_total):
+                owner = i % self.world
+                t = (mine[self.local.index(i)] if owner == self.rank
+                     else torch.empty_like(mine[0]))
+                dist.broadcast(t, src=owner, group=self.group)
+                allimgs.append(t)
+        self.mean = self.engine.set_median(allimgs, self.median_index(self.n_total))
+
     def _update_mean(self):
+        if self.param.UsePerVoxelMedian:
+            return self._update_median()
         acc, jsum = self.engine.mean_sums()
         if self.group is not None and self.world > 1:
             import torch.distributed as dist

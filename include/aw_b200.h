@@ -397,6 +397,18 @@ int aw_ldmm_atlas_accumulate(float *acc, float *jacsum, const float *img, const 
                              float weight, long n, void *stream);
 /* acc /= jacsum (float division), n voxels */
 int aw_ldmm_atlas_normalize(float *acc, const float *jacsum, long n, void *stream);
+/* The atlas as the per-voxel median of the subjects' deformed images
+ * (LDMMAtlasParam UsePerVoxelMedian; MedianCalculator::Select over the
+ * deformed images, Algorithms/Common/MedianCalculator.cxx:264-389, called
+ * by LDMMAtlasBuilder::ComputeMedian, LDMM/LDMMAtlasBuilder.txx:218-233):
+ * out = the k-th smallest (0-based) of the n_images values at each voxel, by
+ * the reference's bisection, including its early end on intervals narrower
+ * than (volume max - volume min) / 10000. images: a HOST array of n_images
+ * (1..256) device pointers to nx*ny*nz floats. The builder's median index is
+ * n/2 - 1 for even n, n/2 for odd n. Synchronises; an error when a voxel
+ * does not converge (the reference throws). */
+int aw_ldmm_atlas_voxel_median(const float *const *images, int n_images, int k, int nx, int ny,
+                               int nz, float *out, void *stream);
 
 /* ---------------------------------------------------------------------------
  * Learned warm start: the kernels of a 3D convolutional encoder-decoder

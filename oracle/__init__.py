@@ -358,6 +358,23 @@ class Oracle:
                                         _fp(jd) if jd is not None else None)
         return img, jd
 
+    def voxel_median(self, imgs, k):
+        """MedianCalculator::Select over the images: the per-voxel k-th
+        smallest value (0-based) by the reference's bisection. Raises when a
+        voxel does not converge, as the reference throws."""
+        stack = np.ascontiguousarray(np.stack(imgs), np.float32)
+        out = np.empty(imgs[0].shape, np.float32)
+        rc = self.lib.aw_oracle_voxel_median(_fp(stack), _i(len(imgs)), ctypes.c_long(out.size),
+                                             _i(k), _fp(out))
+        if rc:
+            raise RuntimeError("Select() not converging")
+        return out
+
+    @staticmethod
+    def median_index(n):
+        """LDMMAtlasBuilder::ComputeMedian's index (LDMMAtlasBuilder.txx:222)."""
+        return n // 2 - 1 if n % 2 == 0 else n // 2
+
     def ldmm_atlas_mean_sums(self, imgs, vs, weights, sp=(1.0, 1.0, 1.0), jacobian_scale=True):
         """One node's sums of LDMMAtlasThreadCPU::ComputeThreadMean: (sum w
         I1At0 JacDet, sum w JacDet) with JacobianScale, else (sum w I1At0,
@@ -376,7 +393,7 @@ class Oracle:
 
     def ldmm_atlas_run(self, imgs, weights, T, iters, sp=(1.0, 1.0, 1.0), sigma=0.1, step=0.005,
                        adaptive=False, max_pert=0.1, alpha=0.01, beta=0.01, gamma=0.001,
-                       use_new=True, jacobian_scale=True):
+                       use_new=True, jacobian_scale=True, voxel_median=False):
         """LDMM relaxation atlas, the AtlasThreadMain loop (Algorithms/Common/
         AtlasThread.txx:97-181) with LDMMAtlasThreadCPU's hooks
         (LDMM/LDMMAtlasThreadCPU.cxx:146-264): mean from v = 0, then per
@@ -391,6 +408,10 @@ class Oracle:
         kw = dict(sp=sp, alpha=alpha, beta=beta, gamma=gamma, sigma=sigma)
 
         def mean_of():
+            if voxel_median:  # UsePerVoxelMedian: LDMMAtlasBuilder.txx:336-338
+                defs = [self.ldmm_i1_at_0(img, v, sp, jacdet=False)[0]
+                        for img, v in zip(imgs, vs)]
+                return self.voxel_median(defs, self.median_index(ns))
             acc, jsum = self.ldmm_atlas_mean_sums(imgs, vs, weights, sp, jacobian_scale)
             return acc / jsum if jacobian_scale else acc
 
@@ -695,6 +716,18 @@ class Reference:
                 p0.ctypes.data_as(_f), p1.ctypes.data_as(_f), _dp(ei), _dp(ev))
         self._check(rc)
         return a0, p0, p1, ei, ev
+
+    def voxel_median(self, imgs, k):
+        """The reference's MedianCalculator::Select over the images."""
+        stack = np.ascontiguousarray(np.stack(imgs), np.float32)
+        out = np.empty(imgs[0].shape, np.float32)
+        with quiet_stdout():
+            rc = self.lib.awref_voxel_median(_fp(stack), _i(len(imgs)), *_shape(imgs[0]), _i(k),
+                                             _fp(out))
+        if rc == 1:
+            raise RuntimeError("Select() not converging")
+        self._check(rc)
+        return out
 
     def ldmm_atlas_run(self, imgs, weights, T, iters, sp=(1.0, 1.0, 1.0), sigma=0.1, step=0.005,
                        adaptive=False, max_pert=0.1, alpha=0.01, beta=0.01, gamma=0.001,

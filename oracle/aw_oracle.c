@@ -1309,3 +1309,91 @@ void aw_oracle_upsample_hfield(const float *h, int nx, int ny, int nz, float *ou
   }
   free(v);
 }
+
+/* MedianCalculator::Select(std::vector<RealImage*>, k, rtn)
+ * (Algorithms/Common/MedianCalculator.cxx:264-389) with MinMax (:170-199) and
+ * GetIndex (:201-258), one process: all voxels advance round by round, as in
+ * the reference. */
+int aw_oracle_voxel_median(const float *imgs, int n, long nvox, int k, float *out) {
+  float *gmin = malloc(sizeof(float) * nvox), *gmax = malloc(sizeof(float) * nvox);
+  float *cmin = malloc(sizeof(float) * nvox), *cmax = malloc(sizeof(float) * nvox);
+  float *p = malloc(sizeof(float) * nvox), *vp = malloc(sizeof(float) * nvox);
+  float *vn = malloc(sizeof(float) * nvox);
+  unsigned *idx = malloc(sizeof(unsigned) * nvox);
+  char *fin = calloc((size_t)nvox, 1);
+  int rc = 0;
+  /* MinMax: per-voxel min / max starting from image 0 */
+  for (long i = 0; i < nvox; ++i) gmin[i] = gmax[i] = imgs[i];
+  for (int m = 1; m < n; ++m)
+    for (long i = 0; i < nvox; ++i) {
+      const float v = imgs[(long)m * nvox + i];
+      gmin[i] = v < gmin[i] ? v : gmin[i];
+      gmax[i] = v > gmax[i] ? v : gmax[i];
+    }
+  /* Array3DUtils::getMinMax of gmin (its min) and of gmax (its max) */
+  float tmin = gmin[0], tmax = gmax[0];
+  for (long i = 1; i < nvox; ++i) {
+    if (gmin[i] < tmin) tmin = gmin[i];
+    if (gmax[i] > tmax) tmax = gmax[i];
+  }
+  const float eps = (tmax - tmin) / 10000.f;
+  for (long i = 0; i < nvox; ++i) {
+    cmin[i] = gmin[i];
+    cmax[i] = gmax[i];
+  }
+  long finished = 0;
+  const unsigned uk = (unsigned)k;
+  for (unsigned iter = 0;; ++iter) {
+    for (long i = 0; i < nvox; ++i) {
+      if (fin[i]) continue;
+      if (eps > fabsf(cmax[i] - cmin[i])) {
+        out[i] = cmin[i];
+        fin[i] = 1;
+        ++finished;
+        continue;
+      }
+      p[i] = (float)((double)(cmin[i] + cmax[i]) / 2.0);
+    }
+    /* GetIndex: count below p, largest below (from gmin), smallest at or above (from gmax) */
+    for (long i = 0; i < nvox; ++i) {
+      vp[i] = gmin[i];
+      vn[i] = gmax[i];
+      idx[i] = 0;
+    }
+    for (int m = 0; m < n; ++m)
+      for (long i = 0; i < nvox; ++i) {
+        const float v = imgs[(long)m * nvox + i];
+        if (v < p[i]) {
+          idx[i]++;
+          if (v > vp[i]) vp[i] = v;
+        } else if (v < vn[i]) {
+          vn[i] = v;
+        }
+      }
+    for (long i = 0; i < nvox; ++i) {
+      if (fin[i]) continue;
+      if (idx[i] == uk) {
+        out[i] = vn[i];
+        fin[i] = 1;
+        ++finished;
+      } else if (idx[i] - 1u == uk) {
+        out[i] = vp[i];
+        fin[i] = 1;
+        ++finished;
+      } else if (idx[i] > uk) {
+        cmax[i] = vp[i];
+      } else if (idx[i] < uk) {
+        cmin[i] = vn[i];
+      }
+    }
+    if (iter > (unsigned)n && finished < nvox) {
+      rc = 1;
+      for (long i = 0; i < nvox; ++i)
+        if (!fin[i]) out[i] = cmin[i];
+      break;
+    }
+    if (finished == nvox) break;
+  }
+  free(gmin); free(gmax); free(cmin); free(cmax); free(p); free(vp); free(vn); free(idx); free(fin);
+  return rc;
+}

@@ -32,6 +32,7 @@
 #include "LDMMParam.h"
 #include "LDMMShootingDefData.h"
 #include "LDMMShootingIteratorCPU.h"
+#include "MedianCalculator.h"
 #include "MultiscaleManager.h"
 #include "tinyxml.h"
 
@@ -820,6 +821,32 @@ int awref_adshoot_run(const float *i0, const float *i1, int nx, int ny, int nz, 
   from_im(data.Alpha0(), alpha0);
   from_vf(data.Phi0T(), phi0T, phi0T + n, phi0T + 2 * n);
   from_vf(data.PhiT0(), phiT0, phiT0 + n, phiT0 + 2 * n);
+  GUARD_END
+}
+
+// MedianCalculator::Select over n images stacked [n][nvox]: the per-voxel
+// k-th smallest value (the UsePerVoxelMedian atlas); 1 when it throws
+int awref_voxel_median(const float *imgs, int n, int nx, int ny, int nz, int k, float *out) {
+  GUARD_BEGIN
+  SizeType size(nx, ny, nz);
+  OriginType origin(0, 0, 0);
+  SpacingType sp(1, 1, 1);
+  const long nvox = (long)nx * ny * nz;
+  std::vector<RealImage *> ims;
+  for (int m = 0; m < n; ++m) {
+    ims.push_back(new RealImage(size, origin, sp));
+    to_im(imgs + m * nvox, *ims.back());
+  }
+  RealImage rtn(size, origin, sp);
+  int rc = 0;
+  try {
+    MedianCalculator::Select(ims, (unsigned)k, rtn);
+  } catch (...) {
+    rc = 1;
+  }
+  for (RealImage *im : ims) delete im;
+  if (rc) return 1;
+  from_im(rtn, out);
   GUARD_END
 }
 

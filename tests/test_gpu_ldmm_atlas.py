@@ -75,3 +75,62 @@ def test_ldmm_atlas_vs_oracle(oracle, use_new, jacobian_scale, adaptive):
         assert np.abs(vg - v_o[i]).max() <= 1e-3 * np.abs(v_o[i]).max()
         assert np.allclose(b.GetEnergies(i)[-iters:], e_o[:, i], rtol=1e-4)
     assert np.abs(v_o[0]).max() > 0
+
+
+def _device_median(imgs, k):
+    t = [cu(a) for a in imgs]
+    nz, ny, nx = imgs[0].shape
+    out = torch.full(imgs[0].shape, float("nan"), device="cuda")
+    import ctypes
+    ptrs = (ctypes.c_void_p * len(t))(*[x.data_ptr() for x in t])
+    rc = _lib.lib().aw_ldmm_atlas_voxel_median(ptrs, len(t), k, nx, ny, nz, out.data_ptr(), None)
+    return rc, host(out)
+
+
+def test_voxel_median_bit_exact(oracle):
+    """aw_ldmm_atlas_voxel_median against the oracle's restatement of
+    MedianCalculator::Select (pinned to the reference): random values, ties,
+    every k, the eps rule (a volume whose range makes eps = 1, so voxels
+    with values within 1 end at the lower end), and a constant volume,
+    where the reference throws for k > 0 and the device reports an error."""
+    rng = np.random.default_rng(8)
+    shape = (9, 10, 11)
+    for n in (1, 2, 3, 5, 8, 33):
+        imgs = [rng.normal(0, 1, shape).astype(np.float32) for _ in range(n)]
+        if n > 2:
+            imgs[1][0] = imgs[0][0]
+        for k in sorted({0, n // 2 - 1 if n % 2 == 0 else n // 2, n - 1}):
+            rc, got = _device_median(imgs, k)
+            assert rc == 0
+            assert np.array_equal(got, oracle.voxel_median(imgs, k))
+    imgs = [np.full(shape, 0.1 * (m + 1), np.float32) for m in range(5)]
+    imgs[0][0, 0, 0] = 1e4
+    rc, got = _device_median(imgs, 2)
+    assert rc == 0 and np.array_equal(got, oracle.voxel_median(imgs, 2))
+    assert got[1, 1, 1] == np.float32(0.1)
+    const = [np.full(shape, 2.0, np.float32) for _ in range(3)]
+    rc, _ = _device_median(const, 1)
+    assert rc != 0 and b"converge" in _lib.lib().aw_last_error()
+    rc, got = _device_median(const, 0)
+    assert rc == 0 and np.all(got == 2.0)
+
+
+def test_ldmm_atlas_voxel_median_vs_oracle(oracle):
+    """UsePerVoxelMedian: the atlas whose mean is the per-voxel median of the
+    deformed subjects (five subjects, median index 2) against the oracle's
+    loop; same tolerances as the mean atlas."""
+    shape, T, iters = (16, 16, 16), 3, 2
+    imgs = [greedy_pair(shape, 50 + k, n_blobs=4, umax=1.5, sigma_range=(1.5, 3.0),
+                        smooth_sigma=3.0)[1] for k in range(5)]
+    w = [0.2] * 5
+    m_o, v_o, e_o = oracle.ldmm_atlas_run(imgs, w, T, iters, sigma=1.0, step=0.01,
+                                          adaptive=True, max_pert=0.2, voxel_median=True)
+    param = LDMMAtlasParam(LDMMIteratorParam(DiffOperParam(), 1.0, 0.01, True, 0.2),
+                           NTimeSteps=T, NIterations=iters, UsePerVoxelMedian=True)
+    b = LDMMAtlasBuilderB200([cu(a) for a in imgs], shape[::-1], param, weights=w)
+    mean = host(b.BuildAtlas())
+    assert np.abs(mean - m_o).max() <= 1e-4 * np.abs(m_o).max()
+    for i in range(5):
+        vg = host(b.GetVelocities(i))
+        assert np.abs(vg - v_o[i]).max() <= 1e-3 * np.abs(v_o[i]).max()
+        assert np.allclose(b.GetEnergies(i)[-iters:], e_o[:, i], rtol=1e-4)

@@ -39,6 +39,14 @@ class OracleLDMMAtlasEngine:
                                                 self.param.JacobianScale)
         return torch.from_numpy(acc), (torch.from_numpy(jsum) if jsum is not None else None)
 
+    def deformed(self):
+        return [torch.from_numpy(self.o.ldmm_i1_at_0(img, v, self.sp, jacdet=False)[0])
+                for img, v in zip(self.imgs, self.vs)]
+
+    def set_median(self, images, k):
+        self.mean = self.o.voxel_median([t.numpy() for t in images], k)
+        return torch.from_numpy(self.mean)
+
     def set_mean(self, acc, jsum):
         m = acc.numpy() / jsum.numpy() if jsum is not None else acc.numpy()
         self.mean = np.ascontiguousarray(m, np.float32)
@@ -58,9 +66,9 @@ class OracleLDMMAtlasEngine:
         return torch.from_numpy(self.vs[i])
 
 
-def _param():
+def _param(median=False):
     return LDMMAtlasParam(LDMMIteratorParam(DiffOperParam(), 1.0, 0.01, True, 0.2), NTimeSteps=3,
-                          NIterations=2, JacobianScale=True)
+                          NIterations=2, JacobianScale=True, UsePerVoxelMedian=median)
 
 
 def _subjects():
@@ -80,12 +88,28 @@ def test_one_process_builder_equals_oracle_loop(oracle):
         assert np.array_equal(b.GetVelocities(i).numpy(), v_o[i])
 
 
-def _rank_main(rank, world, port, imgs, q):
+def test_one_process_voxel_median_builder_equals_oracle_loop(oracle):
+    """UsePerVoxelMedian: the builder's mean is the per-voxel median of the
+    deformed subjects, as the oracle's loop forms it (five subjects: an odd
+    count, median index 2)."""
+    imgs = _subjects() + [greedy_pair(SHAPE, 70, n_blobs=4, umax=1.5, sigma_range=(1.5, 3.0),
+                                      smooth_sigma=3.0)[1]]
+    b = LDMMAtlasBuilderB200([torch.from_numpy(a) for a in imgs], SHAPE, _param(True),
+                             engine_factory=OracleLDMMAtlasEngine)
+    mean = b.BuildAtlas().numpy()
+    m_o, v_o, _ = oracle.ldmm_atlas_run(imgs, [0.2] * 5, 3, 2, sigma=1.0, step=0.01,
+                                        adaptive=True, max_pert=0.2, voxel_median=True)
+    assert np.array_equal(mean, m_o)
+    for i in range(5):
+        assert np.array_equal(b.GetVelocities(i).numpy(), v_o[i])
+
+
+def _rank_main(rank, world, port, imgs, q, median=False):
     import torch.distributed as dist
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
                             world_size=world)
     try:
-        b = LDMMAtlasBuilderB200([torch.from_numpy(a) for a in imgs], SHAPE, _param(),
+        b = LDMMAtlasBuilderB200([torch.from_numpy(a) for a in imgs], SHAPE, _param(median),
                                  group=dist.group.WORLD, engine_factory=OracleLDMMAtlasEngine)
         mean = b.BuildAtlas().numpy().copy()
         q.put((rank, mean, {i: b.GetVelocities(i).numpy().copy() for i in b.local}))
@@ -115,3 +139,28 @@ def test_two_rank_ldmm_atlas_equals_one_process(oracle):
         for i, v in vs.items():
             assert i % 2 == rank
             assert np.abs(v - v_o[i]).max() <= 1e-3 * np.abs(v_o[i]).max()
+
+
+def test_two_rank_voxel_median_equals_one_process(oracle):
+    """UsePerVoxelMedian over two gloo ranks: each deformed subject is
+    broadcast by its owner, every rank selects over all four, and the mean
+    and velocities equal the one-process oracle loop bit for bit (the
+    selection does not depend on the images' order)."""
+    import multiprocessing as mp
+    imgs = _subjects()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29500 + (os.getpid() + 613) % 1000
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, imgs, q, True)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    m_o, v_o, _ = oracle.ldmm_atlas_run(imgs, [0.25] * 4, 3, 2, sigma=1.0, step=0.01,
+                                        adaptive=True, max_pert=0.2, voxel_median=True)
+    for rank, mean, vs in res:
+        assert np.array_equal(mean, m_o)
+        for i, v in vs.items():
+            assert np.array_equal(v, v_o[i])

@@ -202,3 +202,43 @@ def test_ldmm_adjoint_shooting_two_scales_matches_reference(oracle, reference):
     assert np.abs(p1 - p1_r).max() <= 1e-4
     ei = np.concatenate([h[0] for h in hist])
     assert np.allclose(ei, ei_r, rtol=1e-5)
+
+
+def _median_cases():
+    """Image stacks for MedianCalculator::Select: random values, exact ties,
+    and a volume whose range (one voxel at 1e4) makes eps = 1, so voxels
+    whose values lie within 1 end at their interval's lower end, not at the
+    k-th value."""
+    rng = np.random.default_rng(8)
+    shape = (5, 6, 7)
+    cases = []
+    for n in (1, 2, 3, 4, 6, 9):
+        imgs = [rng.normal(0, 1, shape).astype(np.float32) for _ in range(n)]
+        if n > 2:
+            imgs[1][0] = imgs[0][0]  # ties across images
+        cases.append(imgs)
+    imgs = [np.full(shape, 0.1 * (m + 1), np.float32) for m in range(5)]
+    imgs[0][0, 0, 0] = 1e4
+    cases.append(imgs)
+    return cases
+
+
+def test_voxel_median_matches_reference(oracle, reference):
+    for imgs in _median_cases():
+        k = oracle.median_index(len(imgs))
+        got = oracle.voxel_median(imgs, k)
+        assert np.array_equal(got, reference.voxel_median(imgs, k))
+    # the eps rule: 0.1 .. 0.5 lie within eps = 1 of each other, so the
+    # selection ends at the lower end 0.1 instead of the median 0.3
+    assert got[1, 1, 1] == np.float32(0.1)
+
+
+def test_voxel_median_not_converging_matches_reference(oracle, reference):
+    # one constant volume: eps = 0 and no bisection separates the values,
+    # so the reference throws for any k > 0, and the oracle reports it
+    imgs = [np.full((3, 3, 3), 2.0, np.float32) for _ in range(3)]
+    with pytest.raises(RuntimeError):
+        reference.voxel_median(imgs, 1)
+    with pytest.raises(RuntimeError):
+        oracle.voxel_median(imgs, 1)
+    assert np.array_equal(oracle.voxel_median(imgs, 0), reference.voxel_median(imgs, 0))
