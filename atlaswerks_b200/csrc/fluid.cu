@@ -238,6 +238,129 @@ __global__ void __launch_bounds__(256) k_fft_xy_inv(FluidPlan p, Dst dst) {
   }
 }
 
+// ---- the split path: slabs larger than one CTA's shared memory ------------
+// The same line transforms as k_fft_xy_fwd / k_fft_xy_inv (same batches,
+// same fft_lines calls, so the same values), but the x and y passes are
+// separate kernels and the half spectrum between them lives in HBM: an x
+// pass CTA owns a batch of row pairs of one (z, component), a y pass CTA a
+// batch of kx columns.
+
+// x pass: producer -> R2C along x -> half-spectrum rows in the spectrum
+template <class Src>
+__global__ void __launch_bounds__(256) k_fft_x_fwd(FluidPlan p, Src src) {
+  extern __shared__ float2 sm[];
+  const Dims d = p.d;
+  const int z = blockIdx.x, comp = blockIdx.y;
+  const int nx = d.nx, ny = d.ny, nxh = p.nxh;
+  const int P = p.pairs_per_batch;
+  float2 *A = sm;
+  float2 *B = A + P * nx;
+  const int npairs = (ny + 1) >> 1;
+  const int p0 = blockIdx.z * P;
+  const int pb = min(P, npairs - p0);
+  for (int t = threadIdx.x; t < pb * nx; t += blockDim.x) {
+    const int b = t / nx, x = t - b * nx;
+    const int y0 = 2 * (p0 + b), y1 = y0 + 1;
+    const float a0 = src.value(comp, x, y0, z, d);
+    const float a1 = (y1 < ny) ? src.value(comp, x, y1, z, d) : 0.f;
+    A[b * nx + x] = make_float2(a0, a1);
+  }
+  __syncthreads();
+  const float2 *R = fft_lines<-1>(A, B, pb, nx, p.ax);
+  float2 *C = p.spec + ((long)comp * d.nz + z) * ny * nxh;
+  for (int t = threadIdx.x; t < pb * nxh; t += blockDim.x) {
+    const int b = t / nxh, k = t - b * nxh;
+    const float2 Z = R[b * nx + k];
+    const float2 Zm = R[b * nx + (k == 0 ? 0 : nx - k)];
+    const int y0 = 2 * (p0 + b), y1 = y0 + 1;
+    C[(long)y0 * nxh + k] = make_float2(0.5f * (Z.x + Zm.x), 0.5f * (Z.y - Zm.y));
+    if (y1 < ny) C[(long)y1 * nxh + k] = make_float2(0.5f * (Z.y + Zm.y), -0.5f * (Z.x - Zm.x));
+  }
+}
+
+// y pass, in place in the spectrum: a batch of kx columns of one (z, component)
+template <int SIGN>
+__global__ void __launch_bounds__(256) k_fft_y(FluidPlan p) {
+  extern __shared__ float2 sm[];
+  const Dims d = p.d;
+  const int z = blockIdx.x, comp = blockIdx.y;
+  const int ny = d.ny, nxh = p.nxh;
+  const int Q = p.cols_per_batch;
+  float2 *A = sm;
+  float2 *B = A + Q * ny;
+  const int k0 = blockIdx.z * Q;
+  const int qb = min(Q, nxh - k0);
+  float2 *C = p.spec + ((long)comp * d.nz + z) * ny * nxh;
+  for (int t = threadIdx.x; t < qb * ny; t += blockDim.x) {
+    const int y = t / qb, q = t - y * qb;
+    A[q * ny + y] = C[(long)y * nxh + k0 + q];
+  }
+  __syncthreads();
+  const float2 *R = fft_lines<SIGN>(A, B, qb, ny, p.ay);
+  for (int t = threadIdx.x; t < qb * ny; t += blockDim.x) {
+    const int y = t / qb, q = t - y * qb;
+    C[(long)y * nxh + k0 + q] = R[q * ny + y];
+  }
+}
+
+// x pass of the inverse: half-spectrum rows -> C2R along x -> consumer
+template <class Dst>
+__global__ void __launch_bounds__(256) k_fft_x_inv(FluidPlan p, Dst dst) {
+  extern __shared__ float2 sm[];
+  const Dims d = p.d;
+  const int z = blockIdx.x, comp = blockIdx.y;
+  const int nx = d.nx, ny = d.ny, nxh = p.nxh;
+  const int P = p.pairs_per_batch;
+  float2 *A = sm;
+  float2 *B = A + P * nx;
+  const int npairs = (ny + 1) >> 1;
+  const int p0 = blockIdx.z * P;
+  const int pb = min(P, npairs - p0);
+  const bool even = (nx & 1) == 0;
+  const float2 *C = p.spec + ((long)comp * d.nz + z) * ny * nxh;
+  for (int t = threadIdx.x; t < pb * nx; t += blockDim.x) {
+    const int b = t / nx, k = t - b * nx;
+    const int y0 = 2 * (p0 + b), y1 = y0 + 1;
+    const bool upper = k >= nxh;
+    const int kk = upper ? nx - k : k;
+    float2 X0 = C[(long)y0 * nxh + kk];
+    float2 X1 = (y1 < ny) ? C[(long)y1 * nxh + kk] : make_float2(0.f, 0.f);
+    if (kk == 0 || (even && kk == nx / 2)) { X0.y = 0.f; X1.y = 0.f; }
+    if (upper) { X0.y = -X0.y; X1.y = -X1.y; }
+    A[b * nx + k] = make_float2(X0.x - X1.y, X0.y + X1.x);
+  }
+  __syncthreads();
+  const float2 *R = fft_lines<+1>(A, B, pb, nx, p.ax);
+  const auto out = dst.bind(comp);
+  for (int t = threadIdx.x; t < pb * nx; t += blockDim.x) {
+    const int b = t / nx, x = t - b * nx;
+    const int y0 = 2 * (p0 + b), y1 = y0 + 1;
+    const float2 v = R[b * nx + x];
+    out.store(d.idx(x, y0, z), v.x);
+    if (y1 < ny) out.store(d.idx(x, y1, z), v.y);
+  }
+}
+
+template <class Src>
+cudaError_t split_forward(const FluidPlan &p, const Src &src, cudaStream_t s) {
+  const int npairs = (p.d.ny + 1) / 2;
+  const int bx = (npairs + p.pairs_per_batch - 1) / p.pairs_per_batch;
+  const int by = (p.nxh + p.cols_per_batch - 1) / p.cols_per_batch;
+  k_fft_x_fwd<Src><<<dim3(p.d.nz, 3, bx), 256, p.smem_x, s>>>(p, src);
+  k_fft_y<-1><<<dim3(p.d.nz, 3, by), 256, p.smem_y, s>>>(p);
+  return cudaGetLastError();
+}
+
+template <class Dst>
+cudaError_t split_inverse(const FluidPlan &p, const Dst &dst, cudaStream_t s) {
+  const int npairs = (p.d.ny + 1) / 2;
+  const int bx = (npairs + p.pairs_per_batch - 1) / p.pairs_per_batch;
+  const int by = (p.nxh + p.cols_per_batch - 1) / p.cols_per_batch;
+  k_fft_y<+1><<<dim3(p.d.nz, 3, by), 256, p.smem_y, s>>>(p);
+  k_fft_x_inv<Dst><<<dim3(p.d.nz, 3, bx), 256, p.smem_x, s>>>(p, dst);
+  return cudaGetLastError();
+}
+
 // TMA descriptor of the spectrum for the z-pass: a 3D float tensor
 // {2*ny*nxh, nz, 3} read and written in boxes {2*Kq, nz, 1} = one row per
 // kz of 16 columns (128 bytes, 128-byte swizzle) or 8 (64 bytes, 64-byte
@@ -341,10 +464,29 @@ void generic_shapes(FluidPlan *p, int P, int Q, int K) {
   const size_t ws = std::max((size_t)P * nx, (size_t)Q * ny);
   p->smem_xy = sizeof(float2) * ((size_t)ny * p->nxh + 2 * ws);
   p->smem_z = sizeof(float2) * (size_t)(2 * 3 * K * nz);
+  p->smem_x = sizeof(float2) * 2 * (size_t)P * nx;
+  p->smem_y = sizeof(float2) * 2 * (size_t)Q * ny;
+}
+
+// whether the plan's shapes fit: the fused xy kernels' slab, or (split) the
+// x and y passes' batch buffers, and the z pass
+bool generic_fits(const FluidPlan &p, size_t maxsm) {
+  const bool xy = p.split ? (p.smem_x <= maxsm && p.smem_y <= maxsm) : p.smem_xy <= maxsm;
+  return xy && p.smem_z <= maxsm;
 }
 
 cudaError_t generic_configure(const FluidPlan &p) {
   cudaError_t e;
+  if (p.split) {
+    if ((e = set_smem(k_fft_x_fwd<SrcField>, p.smem_x)) != cudaSuccess) return e;
+    if ((e = set_smem(k_fft_x_fwd<SrcForce>, p.smem_x)) != cudaSuccess) return e;
+    if ((e = set_smem(k_fft_x_inv<DstField>, p.smem_x)) != cudaSuccess) return e;
+    if ((e = set_smem(k_fft_x_inv<DstAxpby>, p.smem_x)) != cudaSuccess) return e;
+    if ((e = set_smem(k_fft_x_inv<DstNeg>, p.smem_x)) != cudaSuccess) return e;
+    if ((e = set_smem(k_fft_y<-1>, p.smem_y)) != cudaSuccess) return e;
+    if ((e = set_smem(k_fft_y<+1>, p.smem_y)) != cudaSuccess) return e;
+    return set_smem(k_fft_z_solve, p.smem_z);
+  }
   if ((e = set_smem(k_fft_xy_fwd<SrcField>, p.smem_xy)) != cudaSuccess) return e;
   if ((e = set_smem(k_fft_xy_fwd<SrcForce>, p.smem_xy)) != cudaSuccess) return e;
   if ((e = set_smem(k_fft_xy_inv<DstField>, p.smem_xy)) != cudaSuccess) return e;
@@ -380,7 +522,7 @@ cudaError_t fluid_set_shapes(FluidPlan *p, int P, int Q, int K) {
   generic_shapes(&t, P, Q, K);
   int maxsm = 0;
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device);
-  if (t.smem_xy > (size_t)maxsm || t.smem_z > (size_t)maxsm) return cudaErrorInvalidValue;
+  if (!generic_fits(t, (size_t)maxsm)) return cudaErrorInvalidValue;
   const cudaError_t e = generic_configure(t);
   if (e == cudaSuccess) *p = t;
   return e;
@@ -495,7 +637,9 @@ int fluid_plan_create(FluidPlan *p, int nx, int ny, int nz, double spx, double s
     p->fast_smem_z = fast_z_smem(nz, 16);
     p->fast = p->fast_smem_xy <= (size_t)maxsm && p->fast_smem_z <= (size_t)maxsm;
   }
-  if (!p->fast && (p->smem_xy > (size_t)maxsm || p->smem_z > (size_t)maxsm)) return 2;
+  // a slab whose half spectrum does not fit one CTA: the split x / y passes
+  if (!p->fast && p->smem_xy > (size_t)maxsm) p->split = 1;
+  if (!p->fast && !generic_fits(*p, (size_t)maxsm)) return 2;
 
   std::vector<float2> tw;
   fill_twiddles(nx, tw);
@@ -566,6 +710,7 @@ cudaError_t fluid_forward_field(const FluidPlan &p, const float *fx, const float
                                 const float *fz, cudaStream_t s) {
   SrcField src{{fx, fy, fz}};
   if (p.fast) return fast_xy_forward(p, src, s);
+  if (p.split) return split_forward(p, src, s);
   k_fft_xy_fwd<SrcField><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, src);
   return cudaGetLastError();
 }
@@ -574,6 +719,7 @@ cudaError_t fluid_forward_force(const FluidPlan &p, const float *G, const float 
                                 cudaStream_t s) {
   const SrcForce src = make_force(G, A, diff, p.sp);
   if (p.fast) return fast_xy_forward(p, src, s);
+  if (p.split) return split_forward(p, src, s);
   k_fft_xy_fwd<SrcForce><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, src);
   return cudaGetLastError();
 }
@@ -582,6 +728,7 @@ cudaError_t fluid_forward_force_jac(const FluidPlan &p, const float *G, const fl
                                     const float *B, cudaStream_t s) {
   const SrcForce src = make_force(G, A, 2, p.sp, B);
   if (p.fast) return fast_xy_forward(p, src, s);
+  if (p.split) return split_forward(p, src, s);
   k_fft_xy_fwd<SrcForce><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, src);
   return cudaGetLastError();
 }
@@ -598,6 +745,7 @@ cudaError_t fluid_inverse_store(const FluidPlan &p, float *ox, float *oy, float 
                                 cudaStream_t s) {
   DstField dst{{ox, oy, oz}};
   if (p.fast) return fast_xy_inverse(p, dst, s);
+  if (p.split) return split_inverse(p, dst, s);
   k_fft_xy_inv<DstField><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, dst);
   return cudaGetLastError();
 }
@@ -611,6 +759,7 @@ cudaError_t fluid_inverse_store_neg(const FluidPlan &p, float *ox, float *oy, fl
                                     cudaStream_t s) {
   DstNeg dst{{ox, oy, oz}};
   if (p.fast) return fast_xy_inverse(p, dst, s);
+  if (p.split) return split_inverse(p, dst, s);
   k_fft_xy_inv<DstNeg><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, dst);
   return cudaGetLastError();
 }
@@ -619,6 +768,7 @@ cudaError_t fluid_inverse_axpby(const FluidPlan &p, float *vx, float *vy, float 
                                 const float *step, float sigma, cudaStream_t s) {
   DstAxpby dst{{vx, vy, vz}, step, sigma};
   if (p.fast) return fast_xy_inverse(p, dst, s);
+  if (p.split) return split_inverse(p, dst, s);
   k_fft_xy_inv<DstAxpby><<<dim3(p.d.nz, 3), 256, p.smem_xy, s>>>(p, dst);
   return cudaGetLastError();
 }

@@ -34,6 +34,10 @@ struct FluidPlan {
   float2 *spec;    // device half spectrum [3][nz][ny][nxh]
   int pairs_per_batch, cols_per_batch, zcols_per_cta;
   size_t smem_xy, smem_z;
+  // slabs whose half spectrum does not fit one CTA's shared memory: the xy
+  // transforms run as an x pass and a y pass through the spectrum in HBM
+  int split;
+  size_t smem_x, smem_y;
   int device;
   // register-FFT path (fluid_fast.cu): power-of-two axes
   int fast;

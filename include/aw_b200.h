@@ -13,9 +13,11 @@
  * Base/CUDAUtilities.cxx:137-170).
  *
  * Grid limits: every axis in [2, 512] (the reference caps FFT axes at 512,
- * CUDACommon/src/cudaFFTSolver.cu:21), and one z-slab's half spectrum,
- * ny*(nx/2+1)*8 bytes plus batch buffers, must fit one CTA's shared memory
- * (227 KB: e.g. up to 224 x 224 slabs).
+ * CUDACommon/src/cudaFFTSolver.cu:21). Slabs whose half spectrum,
+ * ny*(nx/2+1)*8 bytes plus batch buffers, fits one CTA's shared memory
+ * (227 KB, e.g. up to 224 x 224) are transformed in x and y by one kernel;
+ * larger ones (256 x 256, 512 x 512, ...) by an x pass and a y pass through
+ * the spectrum in device memory, with the same arithmetic.
  */
 #ifndef AW_B200_H
 #define AW_B200_H

@@ -74,9 +74,11 @@ def test_compose_bit_exact(oracle, bg, direction):
 # shared-memory Stockham kernels
 FLUID_SHAPES = SHAPES + [(64, 64, 64), (32, 48, 40), (128, 128, 128), (32, 64, 128),
                          (128, 16, 64), (16, 32, 16), (256, 32, 16)]
+# slabs too large for one CTA's shared memory: the split x / y passes
+SPLIT_SHAPES = [(8, 256, 256), (6, 288, 320), (3, 512, 512), (4, 250, 462)]
 
 
-@pytest.mark.parametrize("shape", FLUID_SHAPES)
+@pytest.mark.parametrize("shape", FLUID_SHAPES + SPLIT_SHAPES)
 @pytest.mark.parametrize("inverse", [True, False])
 def test_fluid_operator_vs_fp64(oracle, shape, inverse):
     rng = np.random.default_rng(4)
@@ -143,7 +145,7 @@ def test_diffoper_rejects_unsupported():
         op.SetSize((16, 16, 16), (1, 1, 1), DiffOperParam(DivergenceFree=True))
 
 
-@pytest.mark.parametrize("shape", [(16, 16, 16), (24, 20, 18)])
+@pytest.mark.parametrize("shape", [(16, 16, 16), (24, 20, 18), (6, 256, 256)])
 @pytest.mark.parametrize("inverse", [False, True])
 def test_greedy_single_iterations(oracle, shape, inverse):
     """Each Iterate from the same state as the oracle's (fields re-synchronised
