@@ -739,6 +739,15 @@ int aw_ldmm_use_orig_gradient_calc(aw_ldmm_t l, int on) {
   return 0;
 }
 
+int aw_ldmm_set_vector_energy(aw_ldmm_t l, int on) {
+  if (!l) return fail("aw_ldmm_set_vector_energy: null handle");
+  AW_CUDA(cudaDeviceSynchronize(), "aw_ldmm_set_vector_energy (pending work)");
+  l->ctx.vec_energy = on ? 1 : 0;
+  for (auto &kv : l->graphs) cudaGraphExecDestroy(kv.second.second);
+  l->graphs.clear();  // captured iterations belong to the other setting
+  return 0;
+}
+
 int aw_ldmm_set_step(aw_ldmm_t l, float step) {
   if (!l) return fail("aw_ldmm_set_step: null handle");
   AW_CUDA(cudaMemcpy(l->ctx.step, &step, sizeof(float), cudaMemcpyHostToDevice),

@@ -146,15 +146,15 @@ __global__ void __launch_bounds__(kRowThreads)
   }
 }
 
-// energy[count % cap] = scale * sum(partials) (add: +=); advance: count += 1
-// (the image energy, recorded last in an iteration)
+// energy[(count - back) % cap] = scale * sum(partials) (add: +=); advance:
+// count += 1 (the image energy, recorded last in an iteration)
 // one block of kRecThreads; four independent partial sums per thread keep
 // four loads in flight (a fixed order: the same sum on every run)
 constexpr int kRecThreads = 1024;
 __global__ void __launch_bounds__(kRecThreads)
     k_record_energy(const double *__restrict__ partials, int nparts, double scale,
                     double *__restrict__ energy, int *__restrict__ count, int cap,
-                    int advance = 1, int add = 0) {
+                    int advance = 1, int add = 0, int back = 0) {
   double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
   int i = threadIdx.x;
   for (; i + 3 * kRecThreads < nparts; i += 4 * kRecThreads) {
@@ -172,9 +172,9 @@ __global__ void __launch_bounds__(kRecThreads)
   if (threadIdx.x == 0) {
     double s = 0.0;
     for (int w = 0; w < kRecThreads / 32; ++w) s += ws[w];
-    const int k = *count;
+    const int k = *count - back;
     energy[k % cap] = add ? energy[k % cap] + s * scale : s * scale;
-    if (advance) *count = k + 1;
+    if (advance) *count = *count + 1;
   }
 }
 
@@ -353,6 +353,30 @@ __global__ void __launch_bounds__(kRowThreads)
   }
 }
 
+// sum_c u_c v_c per block (float products summed in double), the step
+// energy <L v, v> of HField3DUtils::l2DotProd with u = L v
+__global__ void __launch_bounds__(kRowThreads)
+    k_field_dot(const float *__restrict__ u, const float *__restrict__ v,
+                double *__restrict__ partials, Dims d) {
+  Voxel p;
+  double e = 0.0;
+  if (voxel_of(d, p)) {
+    const long n = d.n();
+#pragma unroll
+    for (int c = 0; c < 3; ++c) e += (double)fmul(u[c * n + p.i], v[c * n + p.i]);
+  }
+  __shared__ double ws[kRowThreads / 32];
+  e = warp_sum(e);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = e;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = threadIdx.x < kRowThreads / 32 ? ws[threadIdx.x] : 0.0;
+    t = warp_sum(t);
+    if (threadIdx.x == 0)
+      partials[((long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = t;
+  }
+}
+
 // alpha0 -= step * (-(grad(I0) . v0) - alphaTilde), float in the
 // reference's order (LDMMAdShootingIteratorCPU.cxx:421-430)
 __global__ void __launch_bounds__(kRowThreads)
@@ -468,6 +492,24 @@ cudaError_t ldmm_forward(LdmmCtx *c, const float *I0, const float *I1, const flo
   return cudaSuccess;
 }
 
+// The vector energy of LDMMIteratorCPU's debug mode (LDMMIteratorCPU.cxx:
+// 493-505 for IterateOrig, 601-610 for IterateNew): <L v_t, v_t> of the
+// updated v_t, through one more forward transform, L and inverse; added up
+// over the time steps of the iteration at energy index count - back.
+static cudaError_t vec_step_energy(LdmmCtx *c, const float *vt, int first, int back, cudaStream_t s) {
+  const long n = c->d.n();
+  float *u = c->u;
+  AW_TRY(fluid_forward_field(c->plan, vt, vt + n, vt + 2 * n, s));
+  AW_TRY(fluid_solve(c->plan, 0, s));
+  AW_TRY(fluid_inverse_store(c->plan, u, u + n, u + 2 * n, s));
+  k_field_dot<<<row_grid(c->d), kRowThreads, 0, s>>>(u, vt, c->partials, c->d);
+  AW_TRY(cudaGetLastError());
+  const double spprod = c->sp.x * c->sp.y * c->sp.z;
+  k_record_energy<<<1, kRecThreads, 0, s>>>(c->partials, c->nparts, spprod, c->venergy, c->count,
+                                            c->cap, 0, first ? 0 : 1, back);
+  return cudaGetLastError();
+}
+
 // alpha_t = splat / sigma^2 in float, the factor (float)(1.0 / (sigma*sigma))
 // as Array3D::scale receives it (LDMMIteratorCPU.cxx:583-585)
 __global__ void __launch_bounds__(256)
@@ -543,6 +585,8 @@ cudaError_t ldmm_iterate(LdmmCtx *c, const float *I0, const float *I1, float *v,
     } else {
       AW_TRY(fluid_inverse_axpby(c->plan, comp(vt, 0), comp(vt, 1), comp(vt, 2), c->step,
                                  c->sigma, s));
+      // the image energy was recorded (and the count advanced) up front
+      if (c->vec_energy) AW_TRY(vec_step_energy(c, vt, t == T - 1, 1, s));
     }
   }
   if (update_step) {
@@ -1077,6 +1121,8 @@ cudaError_t ldmm_iterate_orig(LdmmCtx *c, const float *I0, const float *I1, floa
         comp(H[1 - cur], 0), comp(H[1 - cur], 1), comp(H[1 - cur], 2), I0, Sb, d, c->sp);
     AW_TRY(cudaGetLastError());
     cur = 1 - cur;
+    // the image energy is recorded (and the count advanced) after the sweep
+    if (c->vec_energy && !update_step) AW_TRY(vec_step_energy(c, vt, t == 0, 0, s));
   }
   if (update_step) {
     k_step_from_max<<<1, 1, 0, s>>>(c->maxbits, c->max_pert, c->step);

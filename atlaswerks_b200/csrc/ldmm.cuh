@@ -32,6 +32,7 @@ struct LdmmCtx {
   double *energy;   // image-energy history ring
   int cap;
   int orig;         // IterateOrig (Jacobian path) instead of IterateNew
+  int vec_energy;   // IterateNew / IterateOrig also record sum_t <L v_t, v_t>
   float *JT;        // T x N: I1 pulled back to each time point (IterateOrig)
   float *JD;        // T x N: transported Jacobian determinants (IterateOrig)
   // adjoint shooting (allocated by ldmm_adshoot_prepare)

@@ -51,6 +51,17 @@ class LDMMDeformationDataB200:
         return self.V[t]
 
 
+def ldmm_total_energy(image_energy: float, vec_sum: float, sigma: float, T: int) -> np.float32:
+    """LDMMEnergy::GetEnergy from an image energy sp^3 sum (I0(h) - I1)^2
+    and a vector energy sum_t <L v_t, v_t> sp^3: (1.0 / (sigma*sigma)) times
+    the image term (LDMMEnergy.h:42) plus the step energies' sum / T
+    (LDMMEnergy.cxx:55-64), both held as float."""
+    f32 = np.float32
+    img = f32(float(1.0 / float(f32(sigma) * f32(sigma))) * float(f32(image_energy)))
+    vec = f32(f32(vec_sum) / f32(T))
+    return f32(img + vec)
+
+
 class LDMMIteratorB200:
     DeformationDataType = LDMMDeformationDataB200
     ParamType = LDMMIteratorParam
@@ -63,6 +74,7 @@ class LDMMIteratorB200:
         self._h = ctypes.c_void_p()
         self._update_step = False
         self._orig = False
+        self._vec = False
         self._alphas = None
         self._alphas_valid = False
 
@@ -81,6 +93,8 @@ class LDMMIteratorB200:
         self.SetStepSize(param.StepSize)
         if self._orig:
             check(_lib.lib().aw_ldmm_use_orig_gradient_calc(self._h, 1))
+        if self._vec:
+            check(_lib.lib().aw_ldmm_set_vector_energy(self._h, 1))
 
     def SetUseOrigGradientCalc(self, on: bool):
         """LDMMIteratorCPU's mUseOrigGradientCalc: IterateOrig (Jacobian
@@ -88,6 +102,15 @@ class LDMMIteratorB200:
         self._orig = bool(on)
         if self._h:
             check(_lib.lib().aw_ldmm_use_orig_gradient_calc(self._h, int(self._orig)))
+
+    def SetVectorEnergy(self, on: bool):
+        """The debug mode's vector energy (LDMMIteratorCPU.cxx:493-505,
+        601-610): every iteration that updates v also records
+        sum_t <L v_t, v_t> sp^3 (VecEnergies), at the cost of one more
+        transform and L per time step."""
+        self._vec = bool(on)
+        if self._h:
+            check(_lib.lib().aw_ldmm_set_vector_energy(self._h, int(self._vec)))
 
     def UpdateStepSizeNextIteration(self):
         self._update_step = True
@@ -139,6 +162,26 @@ class LDMMIteratorB200:
         check(_lib.lib().aw_ldmm_get_energies(self._h, out.ctypes.data, n.value,
                                               ctypes.byref(n)))
         return out[: n.value]
+
+    def VecEnergies(self) -> np.ndarray:
+        """sum_t <L v_t, v_t> sp^3 per iteration, aligned with Energies()
+        (zero for iterations run without SetVectorEnergy)."""
+        n = ctypes.c_int()
+        check(_lib.lib().aw_ldmm_get_vec_energies(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros(max(n.value, 1), np.float64)
+        check(_lib.lib().aw_ldmm_get_vec_energies(self._h, out.ctypes.data, n.value,
+                                                  ctypes.byref(n)))
+        return out[: n.value]
+
+    def TotalEnergy(self) -> float:
+        """LDMMEnergy::GetEnergy of the last iteration, ImageEnergy() +
+        VecEnergy() = image / sigma^2 + sum_t <L v_t, v_t> / T, in the
+        reference's float arithmetic (LDMM/LDMMEnergy.cxx:50-64,
+        LDMMEnergy.h:42); 0 before any iteration."""
+        e, ve = self.Energies(), self.VecEnergies()
+        if e.size == 0:
+            return 0.0
+        return float(ldmm_total_energy(e[-1], ve[-1], self.param.Sigma, self.T))
 
     def _free(self):
         if self._h:

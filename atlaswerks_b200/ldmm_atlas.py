@@ -28,11 +28,17 @@ bisection in libaw_b200.so (``aw_ldmm_atlas_voxel_median``); with several
 ranks every deformed image is broadcast by its owner first, so each rank
 selects over all of them (the selection does not depend on their order).
 
-Not built: the ComputeMedian (inverse-distance) and TrimmedMeanSize
-re-weightings, which weigh subjects by sqrt of their last total LDMM
-energy, image plus velocity terms (LDMMAtlasThreadCPU.cxx:175-181, 225-237,
-LDMMAtlasBuilder.txx:437-500): the iterations here record the image term
-only; the PCA step; multiscale (one scale level per BuildAtlas call).
+ComputeMedian (the geometric-median iteration: each subject's weight
+divided by its distance) and TrimmedMeanSize k (only the k subjects
+nearest the mean, weights renormalised) re-weight the subjects by their
+distance sqrt(LDMMEnergy::GetEnergy()) of the last iteration, image plus
+velocity terms (LDMMAtlasThreadCPU::FinishImageIteration / ComputeThreadMean,
+.cxx:175-181, 225-237; LDMMAtlasBuilder::ComputeWeights, .txx:437-500);
+the subjects' iterators then record the vector energies too
+(aw_ldmm_set_vector_energy). With several ranks the distances are summed
+into one vector of all subjects before the selection.
+
+Not built: the PCA step; multiscale (one scale level per BuildAtlas call).
 
 The per-rank work runs in libaw_b200.so (``aw_ldmm_*``) through
 ``CudaLDMMAtlasEngine``; the builder only sequences it and the collectives.
@@ -64,6 +70,38 @@ class LDMMAtlasParam:
     JacobianScale: bool = True
     UseOrigGradientCalc: bool = False
     UsePerVoxelMedian: bool = False
+    ComputeMedian: bool = False
+    TrimmedMeanSize: int = 0
+
+
+def atlas_weights(weights: Sequence[float], dists: Sequence[float], compute_median: bool,
+                  trimmed: int) -> List[np.float32]:
+    """The per-subject weights of the mean (float, as the reference holds
+    them): ComputeMedian divides each weight by the subject's distance (1
+    before any energy exists; LDMMAtlasThreadCPU.cxx:225-232); TrimmedMeanSize
+    k > 0 replaces them by the weights of the subjects whose distance is at
+    most the k-th smallest (0-based, MedianCalculator::Select), at most k of
+    them in subject order and all of them before any energy exists,
+    renormalised to sum 1 (LDMMAtlasBuilder::ComputeWeights, .txx:437-500)."""
+    f32 = np.float32
+    out = [f32(w) for w in weights]
+    if compute_median:
+        for i, d in enumerate(dists):
+            d = f32(d)
+            if d == 0:
+                d = f32(1.0)
+            out[i] = f32(out[i] * f32(1.0 / float(d)))
+    if trimmed > 0:
+        dd = [f32(d) for d in dists]
+        kval = sorted(dd)[trimmed]
+        tm, wsum, sel = [f32(0.0)] * len(dd), f32(0.0), 0
+        for i, d in enumerate(dd):
+            if d == 0 or (d <= kval and sel < trimmed):
+                tm[i] = f32(weights[i])
+                wsum = f32(wsum + tm[i])
+                sel += 1
+        out = [f32(w / wsum) for w in tm]
+    return out
 
 
 class CudaLDMMAtlasEngine:
@@ -84,6 +122,7 @@ class CudaLDMMAtlasEngine:
         self._img = torch.zeros(self.shape, device="cuda")
         self._jd = torch.zeros(self.shape, device="cuda")
         self.images = list(images)
+        reweigh = param.ComputeMedian or param.TrimmedMeanSize > 0
         self.its: List[LDMMIteratorB200] = []
         self.data: List[LDMMDeformationDataB200] = []
         for i, img in enumerate(self.images):
@@ -92,6 +131,7 @@ class CudaLDMMAtlasEngine:
                 raise ValueError("LDMM atlas subjects must be on the template grid")
             it = LDMMIteratorB200(size, spacing=spacing, n_time_steps=param.NTimeSteps)
             it.SetUseOrigGradientCalc(param.UseOrigGradientCalc)
+            it.SetVectorEnergy(reweigh)
             it.SetScaleLevel(size, spacing, param.Iterator)
             self.its.append(it)
             self.data.append(LDMMDeformationDataB200(self.mean, img, param.NTimeSteps, spacing))
@@ -147,6 +187,16 @@ class CudaLDMMAtlasEngine:
     def velocities(self, i: int) -> torch.Tensor:
         return self.data[i].V
 
+    def distances(self) -> List[float]:
+        """sqrt of each local subject's last total energy (0 before any)."""
+        return [float(np.sqrt(np.float32(it.TotalEnergy()))) for it in self.its]
+
+    def set_weights(self, weights: Sequence[float]) -> None:
+        self.w = [float(w) for w in weights]
+
+    def device_of_sums(self):
+        return self.acc.device
+
     def step(self, i: int) -> float:
         return self.its[i].StepSize()
 
@@ -175,6 +225,9 @@ class LDMMAtlasBuilderB200:
         if len(weights) != self.n_total:
             raise ValueError("one weight per image")
         self.param = param
+        self.weights = [float(w) for w in weights]
+        if param.TrimmedMeanSize and not 0 < param.TrimmedMeanSize < self.n_total:
+            raise ValueError("TrimmedMeanSize must be smaller than the number of images")
         self.group = group
         if group is not None:
             import torch.distributed as dist
@@ -209,9 +262,25 @@ class LDMMAtlasBuilderB200:
                 allimgs.append(t)
         self.mean = self.engine.set_median(allimgs, self.median_index(self.n_total))
 
+    def _reweigh(self):
+        p = self.param
+        mine = self.engine.distances()
+        dists = np.zeros(self.n_total, np.float32)
+        for i, d in zip(self.local, mine):
+            dists[i] = d
+        if p.TrimmedMeanSize > 0 and self.group is not None and self.world > 1:
+            import torch.distributed as dist
+            t = torch.from_numpy(dists).to(self.engine.device_of_sums())
+            dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)
+            dists = t.cpu().numpy()
+        w = atlas_weights(self.weights, dists, p.ComputeMedian, p.TrimmedMeanSize)
+        self.engine.set_weights([w[i] for i in self.local])
+
     def _update_mean(self):
         if self.param.UsePerVoxelMedian:
             return self._update_median()
+        if self.param.ComputeMedian or self.param.TrimmedMeanSize > 0:
+            self._reweigh()
         acc, jsum = self.engine.mean_sums()
         if self.group is not None and self.world > 1:
             import torch.distributed as dist

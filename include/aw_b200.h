@@ -319,6 +319,13 @@ int aw_ldmm_destroy(aw_ldmm_t l);
  * reference's default), 0 = IterateNew, the splatting gradient (this
  * handle's default). Allocates 2 T N floats for IterateOrig. */
 int aw_ldmm_use_orig_gradient_calc(aw_ldmm_t l, int on);
+/* LDMMIteratorCPU's debug-mode vector energy (LDMM/LDMMIteratorCPU.cxx:
+ * 493-505, 601-610): on = 1 makes every IterateNew / IterateOrig iteration
+ * that updates v also apply L to each updated v_t (one more forward
+ * transform, L and inverse per time step) and record sum_t <L v_t, v_t> sp^3
+ * beside its image energy (aw_ldmm_get_vec_energies; LDMMEnergy::VecEnergy
+ * is that sum / T). Off by default. Synchronises. */
+int aw_ldmm_set_vector_energy(aw_ldmm_t l, int on);
 /* LDMMDeformationData::StepSize(s) / StepSize(); get synchronises. */
 int aw_ldmm_set_step(aw_ldmm_t l, float step);
 int aw_ldmm_get_step(aw_ldmm_t l, float *step);
@@ -372,7 +379,8 @@ int aw_ldmm_adshoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float
  * (LDMMAdShootingIteratorCPU.cxx:433-453, LDMMWarpAd.txx:37-42): the maps
  * from time 0 to 1 and back composed through the last iteration's velocities. */
 int aw_ldmm_adshoot_final_maps(aw_ldmm_t l, float *phi0T, float *phiT0, void *stream);
-/* Vector energies of the shooting iterations, oldest first: the sum over
+/* Vector energies, oldest first, of the shooting iterations and (with
+ * aw_ldmm_set_vector_energy) of IterateNew / IterateOrig: the sum over
  * the time steps of LDMMEnergy::VecStepEnergy(t), i.e. sum_t <L v_t, v_t> sp^3
  * for aw_ldmm_shoot_iterate and <L v0, v0> sp^3 for aw_ldmm_adshoot_iterate
  * (0 for the relaxation iterations); synchronises. */

@@ -217,16 +217,19 @@ class Oracle:
         return float(e), float(st.value)
 
     def ldmm_iterate(self, I0, I1, v, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01, gamma=0.001,
-                     sigma=0.1, step=0.005, update_step=False, max_pert=0.1):
+                     sigma=0.1, step=0.005, update_step=False, max_pert=0.1, vec=False):
         """One LDMMIteratorCPU::IterateNew; v [T,3,nz,ny,nx] updated in place.
-        Returns (image energy sp^3*sum diff^2, step)."""
+        Returns (image energy sp^3*sum diff^2, step), and with vec the debug
+        mode's sum_t <L v_t, v_t> sp^3 of the updated v as a third value."""
         assert v.dtype == np.float32 and v.flags.c_contiguous
         st = ctypes.c_float(step)
+        ve = ctypes.c_double(0.0)
         e = self.lib.aw_oracle_ldmm_iterate(_fp(I0), _fp(I1), v.ctypes.data_as(_f), _i(v.shape[0]),
                                             *_shape(I0), *map(_dbl, sp), _dbl(alpha), _dbl(beta),
                                             _dbl(gamma), ctypes.c_float(sigma), ctypes.byref(st),
-                                            _i(int(update_step)), ctypes.c_float(max_pert))
-        return float(e), float(st.value)
+                                            _i(int(update_step)), ctypes.c_float(max_pert),
+                                            ctypes.byref(ve) if vec else None)
+        return (float(e), float(st.value)) + ((ve.value,) if vec else ())
 
     def ldmm_alphas(self, I0, I1, v, sp=(1.0, 1.0, 1.0), sigma=0.1):
         """IterateNew with computeAlphasOnly: alpha_t [T,nz,ny,nx]; returns
@@ -248,16 +251,19 @@ class Oracle:
         return out
 
     def ldmm_iterate_orig(self, I0, I1, v, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01,
-                          gamma=0.001, sigma=0.1, step=0.005, update_step=False, max_pert=0.1):
+                          gamma=0.001, sigma=0.1, step=0.005, update_step=False, max_pert=0.1,
+                          vec=False):
         """One LDMMIteratorCPU::IterateOrig; v updated in place. Returns
-        (image energy after the update, step)."""
+        (image energy after the update, step), and with vec the vector energy
+        as ldmm_iterate does."""
         assert v.dtype == np.float32 and v.flags.c_contiguous
         st = ctypes.c_float(step)
+        ve = ctypes.c_double(0.0)
         e = self.lib.aw_oracle_ldmm_iterate_orig(
             _fp(I0), _fp(I1), v.ctypes.data_as(_f), _i(v.shape[0]), *_shape(I0), *map(_dbl, sp),
             _dbl(alpha), _dbl(beta), _dbl(gamma), ctypes.c_float(sigma), ctypes.byref(st),
-            _i(int(update_step)), ctypes.c_float(max_pert))
-        return float(e), float(st.value)
+            _i(int(update_step)), ctypes.c_float(max_pert), ctypes.byref(ve) if vec else None)
+        return (float(e), float(st.value)) + ((ve.value,) if vec else ())
 
     def ldmm_shoot_iterate(self, I0, I1, alpha0, T, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01,
                            gamma=0.001, sigma=0.1, step=0.005, vec=False):
@@ -391,9 +397,49 @@ class Oracle:
                 acc += d * w
         return acc, jsum
 
+    @staticmethod
+    def ldmm_distance(img_energy, vec_sum, sigma, T):
+        """sqrt(LDMMEnergy::GetEnergy()) as LDMMAtlasThreadCPU::
+        FinishImageIteration forms it (LDMMAtlasThreadCPU.cxx:175-181): the
+        image term times (1.0/(sigma*sigma)) (LDMMEnergy.h:42) plus the mean
+        step energy (LDMMEnergy.cxx:55-64), in float."""
+        f = np.float32
+        inv = 1.0 / float(f(sigma) * f(sigma))
+        e = f(f(inv * float(f(img_energy))) + f(f(vec_sum) / f(T)))
+        return f(np.sqrt(e))
+
+    @staticmethod
+    def ldmm_atlas_weights(weights, dists, compute_median, trimmed):
+        """ComputeThreadMean's per-image weight (LDMMAtlasThreadCPU.cxx:
+        221-237) with ComputeMedian (divided by the distance, 1 while it is
+        0) and TrimmedMeanSize (LDMMAtlasBuilder::ComputeWeights,
+        LDMMAtlasBuilder.txx:437-500: kVal = Select(distances, n, k), the
+        images with distance 0 or at most kVal while fewer than k are
+        chosen keep their weight, the others 0, then all divided by the sum)."""
+        f = np.float32
+        w = [f(x) for x in weights]
+        if compute_median:
+            for i in range(len(w)):
+                d = f(dists[i])
+                d = f(1.0) if d == 0 else d
+                w[i] = f(w[i] * f(1.0 / float(d)))
+        if trimmed:
+            kval = np.sort(np.asarray(dists, np.float32))[trimmed]
+            tw, ws, count = [], f(0.0), 0
+            for i in range(len(w)):
+                if dists[i] == 0 or (dists[i] <= kval and count < trimmed):
+                    tw.append(f(weights[i]))
+                    ws = f(ws + f(weights[i]))
+                    count += 1
+                else:
+                    tw.append(f(0.0))
+            w = [f(x / ws) for x in tw]
+        return w
+
     def ldmm_atlas_run(self, imgs, weights, T, iters, sp=(1.0, 1.0, 1.0), sigma=0.1, step=0.005,
                        adaptive=False, max_pert=0.1, alpha=0.01, beta=0.01, gamma=0.001,
-                       use_new=True, jacobian_scale=True, voxel_median=False):
+                       use_new=True, jacobian_scale=True, voxel_median=False,
+                       compute_median=False, trimmed=0):
         """LDMM relaxation atlas, the AtlasThreadMain loop (Algorithms/Common/
         AtlasThread.txx:97-181) with LDMMAtlasThreadCPU's hooks
         (LDMM/LDMMAtlasThreadCPU.cxx:146-264): mean from v = 0, then per
@@ -407,12 +453,17 @@ class Oracle:
         it = self.ldmm_iterate if use_new else self.ldmm_iterate_orig
         kw = dict(sp=sp, alpha=alpha, beta=beta, gamma=gamma, sigma=sigma)
 
+        reweigh = compute_median or trimmed > 0
+        dists = [np.float32(0.0)] * ns
+
         def mean_of():
             if voxel_median:  # UsePerVoxelMedian: LDMMAtlasBuilder.txx:336-338
                 defs = [self.ldmm_i1_at_0(img, v, sp, jacdet=False)[0]
                         for img, v in zip(imgs, vs)]
                 return self.voxel_median(defs, self.median_index(ns))
-            acc, jsum = self.ldmm_atlas_mean_sums(imgs, vs, weights, sp, jacobian_scale)
+            w = (self.ldmm_atlas_weights(weights, dists, compute_median, trimmed) if reweigh
+                 else weights)
+            acc, jsum = self.ldmm_atlas_mean_sums(imgs, vs, w, sp, jacobian_scale)
             return acc / jsum if jacobian_scale else acc
 
         mean = mean_of()
@@ -422,7 +473,10 @@ class Oracle:
                 if k == 0 and adaptive:
                     _, steps[i] = it(mean, imgs[i], vs[i], step=steps[i], update_step=True,
                                      max_pert=max_pert, **kw)
-                en[k, i], _ = it(mean, imgs[i], vs[i], step=steps[i], **kw)
+                r = it(mean, imgs[i], vs[i], step=steps[i], vec=reweigh, **kw)
+                en[k, i] = r[0]
+                if reweigh:
+                    dists[i] = self.ldmm_distance(r[0], r[2], sigma, T)
             mean = mean_of()
         return mean, vs, en
 
@@ -645,7 +699,7 @@ class Reference:
 
     def ldmm_run(self, I0, I1, T, iters, sp=(1.0, 1.0, 1.0), sigma=0.1, step=0.005,
                  adaptive=False, max_pert=0.1, alpha=0.01, beta=0.01, gamma=0.001,
-                 use_new=True, debug=True, v_init=None):
+                 use_new=True, debug=True, v_init=None, vec_out=None):
         """LDMMIteratorCPU (IterateNew when use_new) through the LDMMWarp loop
         at one scale. Returns (v [T,3,...], image energies, step)."""
         n = I0.size
@@ -659,7 +713,7 @@ class Reference:
                 ctypes.c_float(sigma), ctypes.c_float(step), _i(int(adaptive)),
                 ctypes.c_float(max_pert), _dbl(alpha), _dbl(beta), _dbl(gamma), _i(int(use_new)),
                 _i(int(debug)), _i(int(v_init is not None)), v.ctypes.data_as(_f), _dp(en),
-                ctypes.byref(st))
+                ctypes.byref(st), _dp(vec_out) if vec_out is not None else None)
         self._check(rc)
         return v, en, float(st.value)
 

@@ -570,10 +570,24 @@ void aw_oracle_identity(float *hx, float *hy, float *hz, int nx, int ny, int nz)
  * :192-212). v is [T][3][N]. Returns the image energy sp^3 * sum diff^2
  * (accumulated in double).
  * ---------------------------------------------------------------------- */
+/* <L v, v> sp^3 of LDMMIteratorCPU's debug mode (HField3DUtils::l2DotProd of
+ * L v and v, LDMMIteratorCPU.cxx:493-505, 601-610): L applied by the FP32
+ * operator, the float products summed in double */
+static double vec_step_energy(const float *vt, long n, int nx, int ny, int nz, double spx,
+                              double spy, double spz, double alpha, double beta, double gamma) {
+  float *lv = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  memcpy(lv, vt, sizeof(float) * (size_t)(3 * n));
+  aw_oracle_fluid_apply(lv, lv + n, lv + 2 * n, nx, ny, nz, spx, spy, spz, alpha, beta, gamma, 0);
+  double e = 0.0;
+  for (long k = 0; k < 3 * n; ++k) e += (double)(lv[k] * vt[k]);
+  free(lv);
+  return e * spx * spy * spz;
+}
+
 double aw_oracle_ldmm_iterate(const float *I0, const float *I1, float *v, int T, int nx, int ny,
                               int nz, double spx, double spy, double spz, double alpha,
                               double beta, double gamma, float sigma, float *step,
-                              int update_step, float max_pert) {
+                              int update_step, float max_pert, double *vec_energy) {
   const long n = (long)nx * ny * nz;
   float *h = (float *)malloc(sizeof(float) * (size_t)(3 * n));
   float *o = (float *)malloc(sizeof(float) * (size_t)(3 * n));
@@ -598,6 +612,7 @@ double aw_oracle_ldmm_iterate(const float *I0, const float *I1, float *v, int T,
   const float vfac = 1.f - 2 * *step;
   const float ufac = 2 * *step / (sigma * sigma);
   float total_max = 0.f;
+  double vsum = 0.0;
   aw_oracle_identity(h, h + n, h + 2 * n, nx, ny, nz);
   for (int t = T - 1; t >= 0; --t) {
     float *vt = v + (long)t * 3 * n;
@@ -624,9 +639,12 @@ double aw_oracle_ldmm_iterate(const float *I0, const float *I1, float *v, int T,
       }
     } else {
       for (long k = 0; k < 3 * n; ++k) vt[k] = vfac * vt[k] + ufac * f[k];
+      if (vec_energy)
+        vsum += vec_step_energy(vt, n, nx, ny, nz, spx, spy, spz, alpha, beta, gamma);
     }
   }
   if (update_step) *step = max_pert / total_max;
+  if (vec_energy) *vec_energy = vsum;
   free(h);
   free(o);
   free(J0);
@@ -730,7 +748,8 @@ void aw_oracle_jacobian(const float *vx, const float *vy, const float *vz, float
 double aw_oracle_ldmm_iterate_orig(const float *I0, const float *I1, float *v, int T, int nx,
                                    int ny, int nz, double spx, double spy, double spz,
                                    double alpha, double beta, double gamma, float sigma,
-                                   float *step, int update_step, float max_pert) {
+                                   float *step, int update_step, float max_pert,
+                                   double *vec_energy) {
   const long n = (long)nx * ny * nz;
   float *h = (float *)malloc(sizeof(float) * (size_t)(3 * n));
   float *o = (float *)malloc(sizeof(float) * (size_t)(3 * n));
@@ -759,6 +778,7 @@ double aw_oracle_ldmm_iterate_orig(const float *I0, const float *I1, float *v, i
   const float vfac = 1.f - 2 * *step;
   const float ufac = 2 * *step / (sigma * sigma);
   float total_max = 0.f;
+  double vsum = 0.0;
   aw_oracle_identity(h, h + n, h + 2 * n, nx, ny, nz);
   for (int t = 0; t < T; ++t) {
     float *vt = v + (long)t * 3 * n;
@@ -787,11 +807,14 @@ double aw_oracle_ldmm_iterate_orig(const float *I0, const float *I1, float *v, i
       }
     } else {
       for (long k = 0; k < 3 * n; ++k) vt[k] = vfac * vt[k] + ufac * f[k];
+      if (vec_energy)
+        vsum += vec_step_energy(vt, n, nx, ny, nz, spx, spy, spz, alpha, beta, gamma);
     }
     aw_oracle_compose_hv(h, h + n, h + 2 * n, vt, vt + n, vt + 2 * n, o, o + n, o + 2 * n, nx, ny,
                          nz, spx, spy, spz, -1, AW_BG_PARTIAL_ID);
     memcpy(h, o, sizeof(float) * (size_t)(3 * n));
   }
+  if (vec_energy) *vec_energy = vsum;
   double e = 0.0;
   if (update_step) {
     *step = max_pert / total_max;

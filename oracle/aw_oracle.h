@@ -66,14 +66,15 @@ double aw_oracle_ldmm_alphas(const float *I0, const float *I1, const float *v, i
 double aw_oracle_ldmm_iterate(const float *I0, const float *I1, float *v, int T, int nx, int ny,
                               int nz, double spx, double spy, double spz, double alpha,
                               double beta, double gamma, float sigma, float *step,
-                              int update_step, float max_pert);
+                              int update_step, float max_pert, double *vec_energy);
 
 void aw_oracle_jacobian(const float *vx, const float *vy, const float *vz, float *jac, int nx,
                         int ny, int nz, double spx, double spy, double spz);
 double aw_oracle_ldmm_iterate_orig(const float *I0, const float *I1, float *v, int T, int nx,
                                    int ny, int nz, double spx, double spy, double spz,
                                    double alpha, double beta, double gamma, float sigma,
-                                   float *step, int update_step, float max_pert);
+                                   float *step, int update_step, float max_pert,
+                                   double *vec_energy);
 /* GetI1At0 (I1 pulled back through the velocities) and ComputeJacDet */
 void aw_oracle_ldmm_i1_at_0(const float *I1, const float *v, int T, int nx, int ny, int nz,
                             double spx, double spy, double spz, float *img, float *jd);

@@ -501,7 +501,7 @@ int awref_ldmm_run(const float *i0, const float *i1, int nx, int ny, int nz, dou
                    double spy, double spz, int T, int iters, float sigma, float step,
                    int adaptive, float max_pert, double alpha, double beta, double gamma,
                    int use_new, int debug, int v_init, float *v, double *energies,
-                   float *step_out) {
+                   float *step_out, double *vec_energies) {
   GUARD_BEGIN
   std::ostringstream xml;
   xml.precision(17);
@@ -546,6 +546,11 @@ int awref_ldmm_run(const float *i0, const float *i1, int nx, int ny, int nz, dou
       // that divided by sigma^2)
       LDMMEnergy *e = dynamic_cast<LDMMEnergy *>(data.GetEnergyHistory().LastEnergy());
       energies[iter] = e ? (double)e->ImageEnergy() * sigma * sigma : 0.0;
+    }
+    if (vec_energies) {
+      // LDMMEnergy::VecEnergy is the float sum of the step energies / T
+      LDMMEnergy *e = dynamic_cast<LDMMEnergy *>(data.GetEnergyHistory().LastEnergy());
+      vec_energies[iter] = e ? (double)e->VecEnergy() * T : 0.0;
     }
   }
   for (int t = 0; t < T; ++t)

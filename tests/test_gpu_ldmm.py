@@ -226,3 +226,36 @@ def test_ldmm_orig_adaptive_step_vs_oracle(oracle):
     it.Iterate(data)
     assert abs(it.StepSize() - step_o) <= 1e-4 * step_o
     assert np.array_equal(host(data.V), v)
+
+
+@pytest.mark.parametrize("orig", [False, True])
+def test_ldmm_vector_energies_vs_oracle(oracle, orig):
+    """SetVectorEnergy (the reference's debug-mode <L v_t, v_t>): each
+    iteration's sum over t against the oracle's (pinned to the reference),
+    1e-4 relative (FP32 transforms on both sides, summed in double); the
+    velocities and image energies equal those of a run without it."""
+    shape, T, sp = (20, 18, 16), 3, (1.5, 0.75, 1.25)
+    I0, I1 = greedy_pair(shape, seed=31, n_blobs=4, umax=1.5, sigma_range=(1.5, 3.0),
+                         smooth_sigma=3.0)
+    nz, ny, nx = shape
+    its, datas = [], []
+    for vec in (True, False):
+        it = LDMMIteratorB200((nx, ny, nz), spacing=sp, n_time_steps=T)
+        it.SetUseOrigGradientCalc(orig)
+        it.SetVectorEnergy(vec)
+        it.SetScaleLevel((nx, ny, nz), sp, LDMMIteratorParam(DiffOperParam(), 1.0, 0.01, False))
+        its.append(it)
+        datas.append(LDMMDeformationDataB200(cu(I0), cu(I1), T, sp))
+    v = np.zeros((T, 3) + shape, np.float32)
+    step_fn = oracle.ldmm_iterate_orig if orig else oracle.ldmm_iterate
+    for k in range(3):
+        _, _, ve = step_fn(I0, I1, v, sp, sigma=1.0, step=0.01, vec=True)
+        for it, d in zip(its, datas):
+            it.Iterate(d)
+        got = its[0].VecEnergies()[-1]
+        assert ve > 0 and abs(got - ve) <= 1e-4 * ve, (k, got, ve)
+        assert torch.equal(datas[0].V, datas[1].V)
+        assert its[0].Energies()[-1] == its[1].Energies()[-1]
+        for d in datas:
+            d.V.copy_(cu(v))  # re-sync to the oracle's state
+    assert its[0].TotalEnergy() > 0

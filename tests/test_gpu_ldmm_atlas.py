@@ -134,3 +134,28 @@ def test_ldmm_atlas_voxel_median_vs_oracle(oracle):
         vg = host(b.GetVelocities(i))
         assert np.abs(vg - v_o[i]).max() <= 1e-3 * np.abs(v_o[i]).max()
         assert np.allclose(b.GetEnergies(i)[-iters:], e_o[:, i], rtol=1e-4)
+
+
+@pytest.mark.parametrize("compute_median,trimmed", [(True, 0), (False, 2)])
+def test_ldmm_atlas_reweighted_vs_oracle(oracle, compute_median, trimmed):
+    """ComputeMedian (weights divided by each subject's distance) and
+    TrimmedMeanSize 2 of 4 (the two nearest subjects), distances from the
+    image and vector energies, against the oracle's loop; same tolerances as
+    the mean atlas."""
+    shape, T, iters = (16, 16, 16), 3, 3
+    imgs = [greedy_pair(shape, 60 + k, n_blobs=4, umax=1.5, sigma_range=(1.5, 3.0),
+                        smooth_sigma=3.0)[1] for k in range(4)]
+    w = [0.25] * 4
+    m_o, v_o, e_o = oracle.ldmm_atlas_run(imgs, w, T, iters, sigma=1.0, step=0.01,
+                                          adaptive=True, max_pert=0.2,
+                                          compute_median=compute_median, trimmed=trimmed)
+    param = LDMMAtlasParam(LDMMIteratorParam(DiffOperParam(), 1.0, 0.01, True, 0.2),
+                           NTimeSteps=T, NIterations=iters, ComputeMedian=compute_median,
+                           TrimmedMeanSize=trimmed)
+    b = LDMMAtlasBuilderB200([cu(a) for a in imgs], shape[::-1], param, weights=w)
+    mean = host(b.BuildAtlas())
+    assert np.abs(mean - m_o).max() <= 1e-4 * np.abs(m_o).max()
+    for i in range(4):
+        vg = host(b.GetVelocities(i))
+        assert np.abs(vg - v_o[i]).max() <= 1e-3 * np.abs(v_o[i]).max()
+        assert np.allclose(b.GetEnergies(i)[-iters:], e_o[:, i], rtol=1e-4)

@@ -242,3 +242,21 @@ def test_voxel_median_not_converging_matches_reference(oracle, reference):
     with pytest.raises(RuntimeError):
         oracle.voxel_median(imgs, 1)
     assert np.array_equal(oracle.voxel_median(imgs, 0), reference.voxel_median(imgs, 0))
+
+
+@pytest.mark.parametrize("use_new", [True, False])
+def test_ldmm_vector_energies_match_reference(oracle, reference, use_new):
+    """The debug-mode vector energy sum_t <L v_t, v_t> sp^3 of the updated
+    velocities, IterateNew and IterateOrig, against the reference's
+    LDMMEnergy::VecEnergy() * T (the reference sums each step's products in
+    float, hence the tolerance)."""
+    shape, T = (12, 14, 16), 4
+    I0, I1 = greedy_pair(shape, 3, n_blobs=4, umax=1.5, sigma_range=(1.5, 3.0), smooth_sigma=3.0)
+    sp = (1.5, 0.75, 1.25)
+    ven = np.zeros(3)
+    reference.ldmm_run(I0, I1, T, 3, sp=sp, sigma=1.0, step=0.01, use_new=use_new, vec_out=ven)
+    v = np.zeros((T, 3) + shape, np.float32)
+    it = oracle.ldmm_iterate if use_new else oracle.ldmm_iterate_orig
+    vo = [it(I0, I1, v, sp, sigma=1.0, step=0.01, vec=True)[2] for _ in range(3)]
+    assert np.all(ven > 0)
+    assert np.allclose(vo, ven, rtol=1e-4)
