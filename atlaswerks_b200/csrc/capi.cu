@@ -935,6 +935,15 @@ int aw_ldmm_get_vec_energies(aw_ldmm_t l, double *out, int max_count, int *count
   return read_ring(l, l->ctx.venergy, out, max_count, count, "aw_ldmm_get_vec_energies");
 }
 
+int aw_ldmm_get_vec_step_energies(aw_ldmm_t l, double *out, int n_time_steps) {
+  if (!l || !out) return fail("aw_ldmm_get_vec_step_energies: null pointer");
+  if (n_time_steps != l->ctx.T)
+    return fail("aw_ldmm_get_vec_step_energies: n_time_steps must be the handle's T");
+  AW_CUDA(cudaMemcpy(out, l->ctx.vstep, sizeof(double) * l->ctx.T, cudaMemcpyDeviceToHost),
+          "aw_ldmm_get_vec_step_energies");
+  return 0;
+}
+
 int aw_ldmm_get_energies(aw_ldmm_t l, double *out, int max_count, int *count) {
   if (!l || !count) return fail("aw_ldmm_get_energies: null pointer");
   return read_ring(l, l->ctx.energy, out, max_count, count, "aw_ldmm_get_energies");

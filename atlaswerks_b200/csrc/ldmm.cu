@@ -433,6 +433,9 @@ int ldmm_create(LdmmCtx *c, int nx, int ny, int nz, double spx, double spy, doub
   c->step = reinterpret_cast<float *>(c->scalars);
   c->count = reinterpret_cast<int *>(c->scalars + 4);
   c->maxbits = reinterpret_cast<unsigned *>(c->scalars + 8);
+  c->zero = reinterpret_cast<int *>(c->scalars + 12);
+  if (cudaMalloc(&c->vstep, sizeof(double) * T) != cudaSuccess) return 3;
+  cudaMemset(c->vstep, 0, sizeof(double) * T);
   splat_work_bind(&c->sw, c->d, c->splat_scratch);
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
@@ -441,7 +444,7 @@ void ldmm_destroy(LdmmCtx *c) {
   fluid_plan_destroy(&c->plan);
   void *ptrs[] = {c->J0,     c->hbuf,   c->diff, c->S,   c->u,   c->splat_scratch,
                   c->partials, c->energy, c->scalars, c->JT, c->JD, c->adV,
-                  c->adP,    c->adA,    c->adI,  c->venergy, c->adSortMem};
+                  c->adP,    c->adA,    c->adI,  c->venergy, c->adSortMem, c->vstep};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   std::memset(c, 0, sizeof(*c));
@@ -496,7 +499,8 @@ cudaError_t ldmm_forward(LdmmCtx *c, const float *I0, const float *I1, const flo
 // 493-505 for IterateOrig, 601-610 for IterateNew): <L v_t, v_t> of the
 // updated v_t, through one more forward transform, L and inverse; added up
 // over the time steps of the iteration at energy index count - back.
-static cudaError_t vec_step_energy(LdmmCtx *c, const float *vt, int first, int back, cudaStream_t s) {
+static cudaError_t vec_step_energy(LdmmCtx *c, const float *vt, int t, int first, int back,
+                                   cudaStream_t s) {
   const long n = c->d.n();
   float *u = c->u;
   AW_TRY(fluid_forward_field(c->plan, vt, vt + n, vt + 2 * n, s));
@@ -507,6 +511,9 @@ static cudaError_t vec_step_energy(LdmmCtx *c, const float *vt, int first, int b
   const double spprod = c->sp.x * c->sp.y * c->sp.z;
   k_record_energy<<<1, kRecThreads, 0, s>>>(c->partials, c->nparts, spprod, c->venergy, c->count,
                                             c->cap, 0, first ? 0 : 1, back);
+  AW_TRY(cudaGetLastError());
+  k_record_energy<<<1, kRecThreads, 0, s>>>(c->partials, c->nparts, spprod, c->vstep + t, c->zero,
+                                            1, 0, 0, 0);
   return cudaGetLastError();
 }
 
@@ -586,7 +593,7 @@ cudaError_t ldmm_iterate(LdmmCtx *c, const float *I0, const float *I1, float *v,
       AW_TRY(fluid_inverse_axpby(c->plan, comp(vt, 0), comp(vt, 1), comp(vt, 2), c->step,
                                  c->sigma, s));
       // the image energy was recorded (and the count advanced) up front
-      if (c->vec_energy) AW_TRY(vec_step_energy(c, vt, t == T - 1, 1, s));
+      if (c->vec_energy) AW_TRY(vec_step_energy(c, vt, t, t == T - 1, 1, s));
     }
   }
   if (update_step) {
@@ -1122,7 +1129,7 @@ cudaError_t ldmm_iterate_orig(LdmmCtx *c, const float *I0, const float *I1, floa
     AW_TRY(cudaGetLastError());
     cur = 1 - cur;
     // the image energy is recorded (and the count advanced) after the sweep
-    if (c->vec_energy && !update_step) AW_TRY(vec_step_energy(c, vt, t == 0, 0, s));
+    if (c->vec_energy && !update_step) AW_TRY(vec_step_energy(c, vt, t, t == 0, 0, s));
   }
   if (update_step) {
     k_step_from_max<<<1, 1, 0, s>>>(c->maxbits, c->max_pert, c->step);

@@ -33,6 +33,8 @@ struct LdmmCtx {
   int cap;
   int orig;         // IterateOrig (Jacobian path) instead of IterateNew
   int vec_energy;   // IterateNew / IterateOrig also record sum_t <L v_t, v_t>
+  double *vstep;    // T: <L v_t, v_t> sp^3 of each t, of the last such iteration
+  int *zero;        // a device int that stays 0 (index of one-slot records)
   float *JT;        // T x N: I1 pulled back to each time point (IterateOrig)
   float *JD;        // T x N: transported Jacobian determinants (IterateOrig)
   // adjoint shooting (allocated by ldmm_adshoot_prepare)

@@ -51,15 +51,18 @@ class LDMMDeformationDataB200:
         return self.V[t]
 
 
-def ldmm_total_energy(image_energy: float, vec_sum: float, sigma: float, T: int) -> np.float32:
+def ldmm_total_energy(image_energy: float, step_energies: Sequence[float], sigma: float,
+                      T: int) -> np.float32:
     """LDMMEnergy::GetEnergy from an image energy sp^3 sum (I0(h) - I1)^2
-    and a vector energy sum_t <L v_t, v_t> sp^3: (1.0 / (sigma*sigma)) times
-    the image term (LDMMEnergy.h:42) plus the step energies' sum / T
-    (LDMMEnergy.cxx:55-64), both held as float."""
+    and the step energies <L v_t, v_t> sp^3 in the order the iteration set
+    them: (1.0 / (sigma*sigma)) times the image term (LDMMEnergy.h:42) plus
+    the float sum of the step energies / T (LDMMEnergy.cxx:55-64)."""
     f32 = np.float32
     img = f32(float(1.0 / float(f32(sigma) * f32(sigma))) * float(f32(image_energy)))
-    vec = f32(f32(vec_sum) / f32(T))
-    return f32(img + vec)
+    val = f32(0.0)
+    for e in step_energies:
+        val = f32(val + f32(e))
+    return f32(img + f32(val / f32(T)))
 
 
 class LDMMIteratorB200:
@@ -173,15 +176,24 @@ class LDMMIteratorB200:
                                                   ctypes.byref(n)))
         return out[: n.value]
 
+    def VecStepEnergies(self) -> np.ndarray:
+        """<L v_t, v_t> sp^3 for t = 0 .. T-1 of the last iteration that
+        recorded vector energies."""
+        out = np.zeros(self.T, np.float64)
+        check(_lib.lib().aw_ldmm_get_vec_step_energies(self._h, out.ctypes.data, self.T))
+        return out
+
     def TotalEnergy(self) -> float:
         """LDMMEnergy::GetEnergy of the last iteration, ImageEnergy() +
-        VecEnergy() = image / sigma^2 + sum_t <L v_t, v_t> / T, in the
-        reference's float arithmetic (LDMM/LDMMEnergy.cxx:50-64,
-        LDMMEnergy.h:42); 0 before any iteration."""
-        e, ve = self.Energies(), self.VecEnergies()
+        VecEnergy(), in the reference's float arithmetic and the order its
+        iteration sets the step energies (t = T-1 .. 0 for IterateNew, 0 ..
+        T-1 for IterateOrig); 0 before any iteration."""
+        e = self.Energies()
         if e.size == 0:
             return 0.0
-        return float(ldmm_total_energy(e[-1], ve[-1], self.param.Sigma, self.T))
+        steps = self.VecStepEnergies() if self._vec else np.zeros(self.T)
+        order = steps if self._orig else steps[::-1]
+        return float(ldmm_total_energy(e[-1], order, self.param.Sigma, self.T))
 
     def _free(self):
         if self._h:

@@ -326,6 +326,10 @@ int aw_ldmm_use_orig_gradient_calc(aw_ldmm_t l, int on);
  * beside its image energy (aw_ldmm_get_vec_energies; LDMMEnergy::VecEnergy
  * is that sum / T). Off by default. Synchronises. */
 int aw_ldmm_set_vector_energy(aw_ldmm_t l, int on);
+/* The step energies <L v_t, v_t> sp^3 (t = 0 .. T-1) of the last iteration
+ * that recorded vector energies (LDMMEnergy::VecStepEnergy); out holds T
+ * values. Synchronises. */
+int aw_ldmm_get_vec_step_energies(aw_ldmm_t l, double *out, int n_time_steps);
 /* LDMMDeformationData::StepSize(s) / StepSize(); get synchronises. */
 int aw_ldmm_set_step(aw_ldmm_t l, float step);
 int aw_ldmm_get_step(aw_ldmm_t l, float *step);

@@ -18,10 +18,12 @@
  * host value (the step after an adaptive-step pass, the image energy in
  * debug mode).
  *
- * What differs from LDMMIteratorGPU: the energy added in debug mode holds
- * the image term only (the per-time-step vector energies <L v_t, v_t> are
- * not formed), and ReParameterize is not provided (it throws; LDMMWarp
- * calls it only when ReparameterizeEveryNIterations > 0, default 0).
+ * In debug mode the energy added to the data object holds the image term
+ * and the per-time-step vector energies <L v_t, v_t> (the library forms
+ * them with one more transform per time step, aw_ldmm_set_vector_energy, as
+ * the reference's debug mode does). What differs from LDMMIteratorGPU:
+ * ReParameterize is not provided (it throws; LDMMWarp calls it only when
+ * ReparameterizeEveryNIterations > 0, default 0).
  */
 #ifndef AW_B200_LDMM_ITERATOR_HPP
 #define AW_B200_LDMM_ITERATOR_HPP
@@ -79,6 +81,7 @@ class LDMMIteratorB200 : public DeformationIteratorInterface {
                          mCurSpacing.z, k->Alpha(), k->Beta(), k->Gamma(), (int)mNTimeSteps,
                          param.Sigma(), param.MaxPert(), &mHandle),
           "SetScaleLevel");
+    if (mDebug) check(aw_ldmm_set_vector_energy(mHandle, 1), "SetScaleLevel");
     mSigma = param.Sigma();
     mStepKnown = false;
     mAlphasValid = false;
@@ -124,6 +127,13 @@ class LDMMIteratorB200 : public DeformationIteratorInterface {
       int got = 0;
       check(aw_ldmm_get_energies(mHandle, all.data(), count, &got), "Iterate (energy)");
       LDMMEnergy energy(mNTimeSteps, mSigma);
+      if (!computeAlphasOnly) {
+        // set in the iteration's order, t = T-1 down to 0 (IterateNew)
+        std::vector<double> steps(mNTimeSteps);
+        check(aw_ldmm_get_vec_step_energies(mHandle, steps.data(), (int)mNTimeSteps),
+              "Iterate (energy)");
+        for (unsigned int t = mNTimeSteps; t-- > 0;) energy.SetVecStepEnergy((Real)steps[t]);
+      }
       energy.SetImageEnergy(got > 0 ? (Real)all[got - 1] : (Real)0);
       data.AddEnergy(energy);
     }

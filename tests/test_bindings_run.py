@@ -84,7 +84,7 @@ def test_ldmm_binding_equals_host_mirror(tmp_path, oracle):
 
     from atlaswerks_b200.greedy import DiffOperParam
     from atlaswerks_b200.ldmm import (LDMMDeformationDataB200, LDMMIteratorB200,
-                                      LDMMIteratorParam)
+                                      LDMMIteratorParam, ldmm_total_energy)
     from atlaswerks_b200.synth import greedy_pair
     shape, T, iters = (16, 16, 16), 3, 4
     n = 16 ** 3
@@ -93,11 +93,14 @@ def test_ldmm_binding_equals_host_mirror(tmp_path, oracle):
     I1.tofile(tmp_path / "I1.raw")
     _run(build_driver(tmp_path), "ldmm", tmp_path, 16, 16, 16, T, iters)
     it = LDMMIteratorB200((16, 16, 16), n_time_steps=T)
+    it.SetVectorEnergy(True)  # the binding's debug mode records them
     it.SetScaleLevel((16, 16, 16), (1.0, 1.0, 1.0),
                      LDMMIteratorParam(DiffOperParam(), 1.0, 0.01, False, 0.1))
     d = LDMMDeformationDataB200(torch.from_numpy(I0).cuda(), torch.from_numpy(I1).cuda(), T)
+    totals = []
     for _ in range(iters):
         it.Iterate(d)
+        totals.append(it.TotalEnergy())
     torch.cuda.synchronize()
     v = d.V.cpu().numpy()
     assert np.array_equal(_raw(tmp_path / "v.raw", (T, 3) + shape), v)
@@ -107,7 +110,11 @@ def test_ldmm_binding_equals_host_mirror(tmp_path, oracle):
     _, jd = oracle.ldmm_i1_at_0(I1, v)
     assert np.array_equal(_raw(tmp_path / "jacdet.raw", shape), jd)
     e = np.fromfile(tmp_path / "energies.raw", dtype=np.float32)
-    assert len(e) == iters + 1 and np.array_equal(e, it.Energies().astype(np.float32))
+    # LDMMEnergy::GetEnergy: image / sigma^2 + the step energies' mean (the
+    # alphas-only pass records the image term only)
+    totals.append(ldmm_total_energy(it.Energies()[-1], np.zeros(T), 1.0, T))
+    assert len(e) == iters + 1 and np.array_equal(e, np.array(totals, np.float32))
+    assert all(t > it.Energies()[k] for k, t in enumerate(totals[:iters]))
     assert n == v[0, 0].size
 
 
