@@ -890,6 +890,15 @@ int aw_ldmm_shoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *
   return 0;
 }
 
+int aw_ldmm_geodesic_shoot(aw_ldmm_t l, const float *I0, const float *alpha0, float *phi0T,
+                           float *phiT0, float *image, void *stream) {
+  if (!l || !I0 || !alpha0 || !phi0T || !phiT0 || !image)
+    return fail("aw_ldmm_geodesic_shoot: null pointer");
+  AW_CUDA(aw::ldmm_geodesic_shoot(&l->ctx, I0, alpha0, phi0T, phiT0, image, S(stream)),
+          "aw_ldmm_geodesic_shoot");
+  return 0;
+}
+
 int aw_ldmm_adshoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *alpha0,
                             float *phi0T, float *phiT0, void *stream) {
   if (!l || !I0 || !I1 || !alpha0 || !phi0T || !phiT0)

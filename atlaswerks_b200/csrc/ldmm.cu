@@ -820,32 +820,36 @@ __global__ void k_shoot_alpha(float *__restrict__ a0, const float *__restrict__ 
 }
 }  // namespace
 
-// LDMMShootingIteratorCPU::Iterate (LDMM/LDMMShootingIteratorCPU.cxx:199-304):
-// geodesic shooting from the initial momentum alpha0 — v = K(grad(I) alphaT)
-// with I = I0(phiT0), alphaT = forwardApply(alpha0, phi0T), the two maps
-// advanced by composeVH [PARTIAL_ZERO] and composeHVInv [PARTIAL_ID] — then
-// the residual pulled back by splatting and the momentum update. The maps
-// ping-pong between the caller's buffers and the context's two vector
-// scratch fields; v lives in the context's u, alphaT in its splat buffer,
-// I0(phiT0) in J0[0]. Records the image energy sp^3 sum (I0(phiT0) - I1)^2.
-cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, float *alpha0,
-                               float *phi0T, float *phiT0, cudaStream_t s) {
+// The geodesic from I0 and the momentum alpha0 (LDMMGeodesicShootingCPU::
+// ShootImage(I0, alpha0, T), LDMM/LDMMGeodesicShootingCPU.cxx:44-157; the
+// shooting half of LDMMShootingIteratorCPU::Iterate, LDMMShootingIteratorCPU.
+// cxx:199-262): v_0 = K(grad(I0) alpha0); for t = 1..T-1: phi0T =
+// composeVH(v, phi0T) [PARTIAL_ZERO], alpha_t = splat(alpha0, phi0T), phiT0 =
+// composeHVInv(phiT0, v) [PARTIAL_ID], I_t = I0(phiT0), v_t = K(grad(I_t)
+// alpha_t); then the last step of both maps and the final image. The maps end
+// in A[ca] (phi0T or the context's buffer) and B[cb], the image in c->J0.
+// With record, each step energy <L v, v> (as <f, v>, k_force_vdot: no second
+// transform) is added to the iteration's vector energy.
+static cudaError_t shoot_geodesic(LdmmCtx *c, const float *I0, const float *alpha0, float *phi0T,
+                                  float *phiT0, bool record, float *A[2], float *B[2], int &ca,
+                                  int &cb, cudaStream_t s) {
   const Dims d = c->d;
   const long n = d.n();
   const int T = c->T;
-  float *A[2] = {phi0T, c->hbuf}, *B[2] = {phiT0, c->hbuf + 3 * n};
-  int ca = 0, cb = 0;
+  A[0] = phi0T;
+  A[1] = c->hbuf;
+  B[0] = phiT0;
+  B[1] = c->hbuf + 3 * n;
+  ca = cb = 0;
   auto comp = [&](float *base, int k) { return base + k * n; };
   float *v = c->u, *aT = c->S, *I = c->J0;
   const double spprod = c->sp.x * c->sp.y * c->sp.z;
   int vt = 0;  // velocities formed so far
-  // v = K(grad(G) alpha_t), then its step energy <L v, v> added to this
-  // iteration's vector energy (LDMMShootingIteratorCPU.cxx:216-221, 257-262),
-  // as <f, v> (k_force_vdot): no second transform
   auto velocity = [&](const float *G) -> cudaError_t {
     AW_TRY(fluid_forward_force(c->plan, G, aT, 0, s));
     AW_TRY(fluid_solve(c->plan, 1, s));
     AW_TRY(fluid_inverse_store(c->plan, comp(v, 0), comp(v, 1), comp(v, 2), s));
+    if (!record) return cudaSuccess;
     k_force_vdot<<<row_grid(d), kRowThreads, 0, s>>>(make_force(G, aT, 0, c->sp), v, 1.0f,
                                                       c->partials, d);
     AW_TRY(cudaGetLastError());
@@ -881,7 +885,23 @@ cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, flo
     AW_TRY(velocity(I));
   }
   AW_TRY(advance_phiT0());
-  AW_TRY(advance_phi0T());
+  return advance_phi0T();
+}
+
+// LDMMShootingIteratorCPU::Iterate (LDMM/LDMMShootingIteratorCPU.cxx:
+// 199-304): the geodesic, then alpha0 <- (1 - step) alpha0 + (step/sigma^2)
+// splat(I_T - I1 by phiT0), the image energy of I_T - I1 and the vector
+// energy recorded.
+cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, float *alpha0,
+                               float *phi0T, float *phiT0, cudaStream_t s) {
+  const Dims d = c->d;
+  const long n = d.n();
+  float *A[2], *B[2];
+  int ca, cb;
+  auto comp = [&](float *base, int k) { return base + k * n; };
+  AW_TRY(shoot_geodesic(c, I0, alpha0, phi0T, phiT0, true, A, B, ca, cb, s));
+  float *aT = c->S, *I = c->J0;
+  const double spprod = c->sp.x * c->sp.y * c->sp.z;
   k_residual<<<row_grid(d), kRowThreads, 0, s>>>(I, I1, c->diff, c->partials, d);
   AW_TRY(cudaGetLastError());
   AW_TRY(splat(c->sw, c->diff, comp(B[cb], 0), comp(B[cb], 1), comp(B[cb], 2), aT, 0.0f, s));
@@ -894,6 +914,20 @@ cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, flo
   if (ca) AW_TRY(cudaMemcpyAsync(phi0T, A[1], sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
   if (cb) AW_TRY(cudaMemcpyAsync(phiT0, B[1], sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
   return cudaSuccess;
+}
+
+// LDMMGeodesicShootingGPU::ShootImage(I0, alpha0, T): the geodesic alone;
+// the maps Phi0To1 / Phi1To0 in the caller's buffers, the final image
+// (GetFinalImage) in img; no energy is recorded
+cudaError_t ldmm_geodesic_shoot(LdmmCtx *c, const float *I0, const float *alpha0, float *phi0T,
+                                float *phiT0, float *img, cudaStream_t s) {
+  const long n = c->d.n();
+  float *A[2], *B[2];
+  int ca, cb;
+  AW_TRY(shoot_geodesic(c, I0, alpha0, phi0T, phiT0, false, A, B, ca, cb, s));
+  if (ca) AW_TRY(cudaMemcpyAsync(phi0T, A[1], sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
+  if (cb) AW_TRY(cudaMemcpyAsync(phiT0, B[1], sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
+  return cudaMemcpyAsync(img, c->J0, sizeof(float) * n, cudaMemcpyDeviceToDevice, s);
 }
 
 int ldmm_adshoot_prepare(LdmmCtx *c) {

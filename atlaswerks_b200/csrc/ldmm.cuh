@@ -71,6 +71,9 @@ cudaError_t ldmm_voxel_median(const VoxelImages &in, int nimg, int k, long n, fl
 int ldmm_shoot_prepare(LdmmCtx *c);
 cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, float *alpha0,
                                float *phi0T, float *phiT0, cudaStream_t s);
+// LDMMGeodesicShootingGPU::ShootImage(I0, alpha0, T): the geodesic alone
+cudaError_t ldmm_geodesic_shoot(LdmmCtx *c, const float *I0, const float *alpha0, float *phi0T,
+                                float *phiT0, float *img, cudaStream_t s);
 // LDMMAdShootingIteratorCPU (LDMM/LDMMAdShootingIteratorCPU.cxx): the
 // buffers (returns 3 when an allocation fails), one Iterate, and the final
 // maps of finalUpdatePhi0T / finalUpdatePhiT0 from the last Iterate

@@ -10,6 +10,9 @@
   geodesic from alpha0 over T time steps, pull the residual back by
   splatting and update alpha0 (LDMMShootingIteratorCPU.cxx:199-304).
 
+* ``LDMMGeodesicShootingB200`` — LDMMGeodesicShootingCPU / GPU
+  (LDMM/LDMMGeodesicShooting.h): ``ShootImage(I0, alpha0, T)``, the geodesic
+  alone, with ``GetFinalImage``, ``GetPhi0To1`` and ``GetPhi1To0``.
 * ``LDMMAdShootingIteratorB200`` — LDMMAdShootingIteratorCPU / GPU
   (LDMM/LDMMAdShootingIteratorCPU.cxx:237-453): shoots the geodesic keeping
   every time point, integrates the adjoint equations backward and takes the
@@ -170,6 +173,68 @@ class LDMMAdShootingIteratorB200(LDMMShootingIteratorB200):
         """PhiT0 composed from the identity through the last iteration's v_t."""
         self._final(data, 1)
 
+
+
+class LDMMGeodesicShootingB200:
+    """LDMMGeodesicShootingGPU / CPU (LDMM/LDMMGeodesicShooting.h,
+    LDMMGeodesicShootingCPU.cxx:37-157): ShootImage(I0, alpha0, nTimeSteps)
+    follows the geodesic from I0 along the momentum alpha0 and keeps the
+    final image and both maps (GetFinalImage, GetPhi0To1, GetPhi1To0).
+    ``size`` is (nx, ny, nz); ``kernel`` a DiffOperParam."""
+
+    def __init__(self, size: Sequence[int], spacing: Sequence[float], kernel):
+        if kernel.LPow != 1.0 or kernel.UseEigenLUT or kernel.DivergenceFree:
+            raise ValueError("LPow != 1, UseEigenLUT and DivergenceFree are not supported on the "
+                             "GPU path (DiffOperGPU)")
+        self.size = tuple(int(x) for x in size)
+        self.spacing = tuple(float(x) for x in spacing)
+        self.kernel = kernel
+        self._h = ctypes.c_void_p()
+        self._T = 0
+        nx, ny, nz = self.size
+        self._img = torch.empty((nz, ny, nx), device="cuda")
+        self._p0 = identity((nz, ny, nx), self._img.device)
+        self._p1 = identity((nz, ny, nx), self._img.device)
+
+    def ShootImage(self, I0: torch.Tensor, alpha0: torch.Tensor, nTimeSteps: int) -> None:
+        _check_image(I0, "I0")
+        _check_image(alpha0, "alpha0")
+        if tuple(I0.shape) != tuple(self._img.shape) or alpha0.shape != I0.shape:
+            raise ValueError("I0 and alpha0 must be on the shooter's grid")
+        if nTimeSteps < 1:
+            raise ValueError("nTimeSteps must be positive")
+        L = _lib.lib()
+        if self._T != int(nTimeSteps):
+            self._free()
+            nx, ny, nz = self.size
+            k = self.kernel
+            check(L.aw_ldmm_create(nx, ny, nz, *self.spacing, k.Alpha, k.Beta, k.Gamma,
+                                   int(nTimeSteps), 1.0, 0.1, ctypes.byref(self._h)))
+            self._T = int(nTimeSteps)
+        check(L.aw_ldmm_geodesic_shoot(self._h, I0.data_ptr(), alpha0.data_ptr(),
+                                       self._p0.data_ptr(), self._p1.data_ptr(),
+                                       self._img.data_ptr(), _stream()))
+
+    def GetFinalImage(self) -> torch.Tensor:
+        return self._img
+
+    def GetPhi0To1(self) -> torch.Tensor:
+        return self._p0
+
+    def GetPhi1To0(self) -> torch.Tensor:
+        return self._p1
+
+    def _free(self):
+        if self._h:
+            _lib.lib().aw_ldmm_destroy(self._h)
+            self._h = ctypes.c_void_p()
+            self._T = 0
+
+    def __del__(self):
+        try:
+            self._free()
+        except Exception:
+            pass
 
 
 @dataclass

@@ -365,6 +365,13 @@ int aw_ldmm_get_energies(aw_ldmm_t l, double *out, int max_count, int *count);
  * energies <L v_t, v_t> (aw_ldmm_get_vec_energies). */
 int aw_ldmm_shoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *alpha0,
                           float *phi0T, float *phiT0, void *stream);
+/* LDMMGeodesicShootingGPU / CPU::ShootImage(I0, alpha0, nTimeSteps)
+ * (Algorithms/LDMM/LDMMGeodesicShootingCPU.cxx:44-157): the geodesic from I0
+ * along the momentum alpha0 over the handle's T time steps and kernel,
+ * without an update; phi0T / phiT0 receive GetPhi0To1 / GetPhi1To0 and image
+ * the final image GetFinalImage = I0(phiT0). */
+int aw_ldmm_geodesic_shoot(aw_ldmm_t l, const float *I0, const float *alpha0, float *phi0T,
+                           float *phiT0, float *image, void *stream);
 
 /* LDMM adjoint geodesic shooting (LDMMAdShootingIteratorCPU::Iterate and
  * backwardAdIntegration, Algorithms/LDMM/LDMMAdShootingIteratorCPU.cxx:

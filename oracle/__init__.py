@@ -280,6 +280,17 @@ class Oracle:
             ctypes.c_float(sigma), ctypes.c_float(step), ctypes.byref(ev) if vec else None)
         return (float(e), float(ev.value), p0, p1) if vec else (float(e), p0, p1)
 
+    def geodesic_shoot(self, I0, alpha0, T, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01,
+                       gamma=0.001):
+        """LDMMGeodesicShootingCPU::ShootImage: (phi0T, phiT0, final image)."""
+        p0 = np.empty((3,) + I0.shape, np.float32)
+        p1 = np.empty((3,) + I0.shape, np.float32)
+        img = np.empty(I0.shape, np.float32)
+        self.lib.aw_oracle_geodesic_shoot(_fp(I0), _fp(alpha0), _i(T), *_shape(I0), *map(_dbl, sp),
+                                          _dbl(alpha), _dbl(beta), _dbl(gamma), _fp(p0), _fp(p1),
+                                          _fp(img))
+        return p0, p1, img
+
     def ldmm_adshoot_iterate(self, I0, I1, alpha0, T, sp=(1.0, 1.0, 1.0), alpha=0.01,
                              beta=0.01, gamma=0.001, sigma=0.1, step=0.005):
         """One LDMMAdShootingIteratorCPU::Iterate (shooting, then the backward
@@ -746,6 +757,19 @@ class Reference:
                 _fp(a0), p0.ctypes.data_as(_f), p1.ctypes.data_as(_f), _dp(en), _dp(ev))
         self._check(rc)
         return (a0, p0, p1, en, ev) if vec else (a0, p0, p1, en)
+
+    def geodesic_shoot(self, I0, alpha0, T, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01,
+                       gamma=0.001):
+        """The reference's LDMMGeodesicShootingCPU::ShootImage."""
+        p0 = np.empty((3,) + I0.shape, np.float32)
+        p1 = np.empty((3,) + I0.shape, np.float32)
+        img = np.empty(I0.shape, np.float32)
+        with quiet_stdout():
+            rc = self.lib.awref_geodesic_shoot(_fp(I0), _fp(alpha0), *_shape(I0), *map(_dbl, sp),
+                                               _i(T), _dbl(alpha), _dbl(beta), _dbl(gamma),
+                                               _fp(p0), _fp(p1), _fp(img))
+        self._check(rc)
+        return p0, p1, img
 
     def adshoot_run(self, I0, I1, T, levels, sp=(1.0, 1.0, 1.0), sigma=1.0, alpha=0.01,
                     beta=0.01, gamma=0.001):

@@ -971,6 +971,56 @@ double aw_oracle_ldmm_shoot_iterate(const float *I0, const float *I1, float *alp
   return e;
 }
 
+/* LDMMGeodesicShootingCPU::ShootImage(I0, alpha0, T) (Algorithms/LDMM/
+ * LDMMGeodesicShootingCPU.cxx:37-157): v = K(grad(I0) alpha0); for t = 1..T-1
+ * phi0T = composeVH(v, phi0T) [PARTIAL_ZERO], alphaT = forwardApply(alpha0,
+ * phi0T), phiT0 = composeHVInv(phiT0, v) [PARTIAL_ID], I = apply(I0, phiT0),
+ * v = K(grad(I) alphaT); then the last step of phiT0 and phi0T and the final
+ * image I0(phiT0). */
+void aw_oracle_geodesic_shoot(const float *I0, const float *alpha0, int T, int nx, int ny, int nz,
+                              double spx, double spy, double spz, double alpha, double beta,
+                              double gamma, float *phi0T, float *phiT0, float *img) {
+  const long n = (long)nx * ny * nz;
+  float *v = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *o = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *aT = (float *)malloc(sizeof(float) * (size_t)n);
+  float *p0 = phi0T, *p1 = phiT0;
+  aw_oracle_identity(p0, p0 + n, p0 + 2 * n, nx, ny, nz);
+  aw_oracle_identity(p1, p1 + n, p1 + 2 * n, nx, ny, nz);
+  memcpy(aT, alpha0, sizeof(float) * (size_t)n);
+  memcpy(img, I0, sizeof(float) * (size_t)n);
+  for (int t = 0; t < T; ++t) {
+    /* v = K(grad(I) alphaT) with I = I0 at t = 0 */
+    aw_oracle_gradient(img, v, v + n, v + 2 * n, nx, ny, nz, spx, spy, spz, 0);
+    for (long k = 0; k < n; ++k) {
+      v[k] *= aT[k];
+      v[n + k] *= aT[k];
+      v[2 * n + k] *= aT[k];
+    }
+    aw_oracle_fluid_apply(v, v + n, v + 2 * n, nx, ny, nz, spx, spy, spz, alpha, beta, gamma, 1);
+    if (t + 1 < T) {
+      aw_oracle_compose_vh(v, v + n, v + 2 * n, p0, p0 + n, p0 + 2 * n, o, o + n, o + 2 * n, nx,
+                           ny, nz, spx, spy, spz, 1, AW_BG_PARTIAL_ZERO);
+      memcpy(p0, o, sizeof(float) * (size_t)(3 * n));
+      aw_oracle_splat(alpha0, p0, p0 + n, p0 + 2 * n, aT, nx, ny, nz, 0.0f);
+      aw_oracle_compose_hv(p1, p1 + n, p1 + 2 * n, v, v + n, v + 2 * n, o, o + n, o + 2 * n, nx,
+                           ny, nz, spx, spy, spz, -1, AW_BG_PARTIAL_ID);
+      memcpy(p1, o, sizeof(float) * (size_t)(3 * n));
+      aw_oracle_apply(I0, p1, p1 + n, p1 + 2 * n, img, nx, ny, nz, 0.0f);
+    }
+  }
+  aw_oracle_compose_hv(p1, p1 + n, p1 + 2 * n, v, v + n, v + 2 * n, o, o + n, o + 2 * n, nx, ny,
+                       nz, spx, spy, spz, -1, AW_BG_PARTIAL_ID);
+  memcpy(p1, o, sizeof(float) * (size_t)(3 * n));
+  aw_oracle_compose_vh(v, v + n, v + 2 * n, p0, p0 + n, p0 + 2 * n, o, o + n, o + 2 * n, nx, ny,
+                       nz, spx, spy, spz, 1, AW_BG_PARTIAL_ZERO);
+  memcpy(p0, o, sizeof(float) * (size_t)(3 * n));
+  aw_oracle_apply(I0, p1, p1 + n, p1 + 2 * n, img, nx, ny, nz, 0.0f);
+  free(v);
+  free(o);
+  free(aT);
+}
+
 /* ------------------------------------------------------------------------
  * Adjoint geodesic shooting: LDMMAdShootingIteratorCPU::Iterate
  * (Algorithms/LDMM/LDMMAdShootingIteratorCPU.cxx:237-323) and

@@ -95,6 +95,11 @@ double aw_oracle_ldmm_adshoot_iterate(const float *I0, const float *I1, float *a
                                       int nz, double spx, double spy, double spz, double alpha,
                                       double beta, double gamma, float sigma, float step,
                                       double *vec_energy);
+/* LDMMGeodesicShootingCPU::ShootImage(I0, alpha0, T): phi0T, phiT0 and the
+ * final image I0(phiT0) */
+void aw_oracle_geodesic_shoot(const float *I0, const float *alpha0, int T, int nx, int ny, int nz,
+                              double spx, double spy, double spz, double alpha, double beta,
+                              double gamma, float *phi0T, float *phiT0, float *img);
 /* ImageUtils::resampleNew, clamp background, linear (origin 0) */
 void aw_oracle_resample_image(const float *in, int nx, int ny, int nz, double ssx, double ssy,
                               double ssz, float *out, int mx, int my, int mz, double dsx,

@@ -28,6 +28,7 @@
 #include "LDMMAdShootingIteratorCPU.h"
 #include "LDMMDeformationData.h"
 #include "LDMMEnergy.h"
+#include "LDMMGeodesicShootingCPU.h"
 #include "LDMMIteratorCPU.h"
 #include "LDMMParam.h"
 #include "LDMMShootingDefData.h"
@@ -852,6 +853,29 @@ int awref_voxel_median(const float *imgs, int n, int nx, int ny, int nz, int k, 
   for (RealImage *im : ims) delete im;
   if (rc) return 1;
   from_im(rtn, out);
+  GUARD_END
+}
+
+// LDMMGeodesicShootingCPU::ShootImage(I0, alpha0, T): the final image and
+// both maps
+int awref_geodesic_shoot(const float *i0, const float *a0, int nx, int ny, int nz, double spx,
+                         double spy, double spz, int T, double alpha, double beta, double gamma,
+                         float *phi0T, float *phiT0, float *img) {
+  GUARD_BEGIN
+  DiffOperParam param;
+  parse_into(param, diffoper_xml(alpha, beta, gamma));
+  SizeType size(nx, ny, nz);
+  SpacingType sp(spx, spy, spz);
+  OriginType origin(0, 0, 0);
+  RealImage I0(size, origin, sp), A0(size, origin, sp);
+  to_im(i0, I0);
+  to_im(a0, A0);
+  LDMMGeodesicShootingCPU shooter(size, sp, param);
+  shooter.ShootImage(I0, A0, (unsigned)T);
+  const long n = (long)nx * ny * nz;
+  from_vf(shooter.GetPhi0To1(), phi0T, phi0T + n, phi0T + 2 * n);
+  from_vf(shooter.GetPhi1To0(), phiT0, phiT0 + n, phiT0 + 2 * n);
+  from_im(shooter.GetFinalImage(), img);
   GUARD_END
 }
 

@@ -260,3 +260,19 @@ def test_ldmm_vector_energies_match_reference(oracle, reference, use_new):
     vo = [it(I0, I1, v, sp, sigma=1.0, step=0.01, vec=True)[2] for _ in range(3)]
     assert np.all(ven > 0)
     assert np.allclose(vo, ven, rtol=1e-4)
+
+
+@pytest.mark.parametrize("sp", [(1.0, 1.0, 1.0), (1.5, 0.75, 1.25)])
+def test_geodesic_shoot_matches_reference(oracle, reference, sp):
+    """LDMMGeodesicShootingCPU::ShootImage(I0, alpha0, T): the oracle's
+    restatement against the reference build, maps to 1e-4 voxel and the
+    final image to 1e-5 (the FFT shim's rounding through T transforms)."""
+    shape, T = (12, 14, 16), 4
+    I0, I1 = greedy_pair(shape, 5, n_blobs=4, umax=1.5, sigma_range=(1.5, 3.0), smooth_sigma=3.0)
+    alpha0 = ((I1 - I0) * 0.5).astype(np.float32)
+    p0o, p1o, io = oracle.geodesic_shoot(I0, alpha0, T, sp)
+    p0r, p1r, ir = reference.geodesic_shoot(I0, alpha0, T, sp)
+    assert np.abs(p0o - p0r).max() <= 1e-4
+    assert np.abs(p1o - p1r).max() <= 1e-4
+    assert np.abs(io - ir).max() <= 1e-5
+    assert np.abs(p1r - identity(shape)).max() > 0.01  # the geodesic moved
