@@ -38,6 +38,11 @@ the subjects' iterators then record the vector energies too
 (aw_ldmm_set_vector_energy). With several ranks the distances are summed
 into one vector of all subjects before the selection.
 
+With Shooting the subjects run the momentum shooting iterator instead
+(LDMMShootingAtlasThreadCPU, .cxx:40-226: I0 the mean, I1 the subject,
+the state alpha0) and the mean's sums take I1(phi0T) with the Jacobian
+splat(ones, phiT0); the sharding and exchange are the same.
+
 Not built: the PCA step; multiscale (one scale level per BuildAtlas call).
 
 The per-rank work runs in libaw_b200.so (``aw_ldmm_*``) through
@@ -72,6 +77,7 @@ class LDMMAtlasParam:
     UsePerVoxelMedian: bool = False
     ComputeMedian: bool = False
     TrimmedMeanSize: int = 0
+    Shooting: bool = False  # the shooting atlas (LDMMShootingAtlasThreadCPU)
 
 
 def atlas_weights(weights: Sequence[float], dists: Sequence[float], compute_median: bool,
@@ -204,6 +210,77 @@ class CudaLDMMAtlasEngine:
         return self.its[i].Energies()
 
 
+class CudaLDMMShootingAtlasEngine:
+    """The shooting atlas's subjects on this rank (LDMMShootingAtlasThreadCPU,
+    Algorithms/LDMM/LDMMShootingAtlasThreadCPU.cxx:40-226): one momentum
+    shooting iterator per subject whose I0 is the shared mean and I1 the
+    subject's image (LDMMShootingAtlasDefDataCPU, .cxx:42-52); the mean's
+    sums take each subject's image deformed to the mean, I1(phi0T)
+    (LDMMShootingDefData::GetI1At0, LDMMShootingDefData.cxx:78-84), and the
+    Jacobian of phi0T as the splat of ones by phiT0
+    (LDMMShootingIteratorCPU::ComputeJacDet, LDMMShootingIteratorCPU.cxx:
+    108-119)."""
+
+    def __init__(self, size: Sequence[int], spacing: Sequence[float], param: LDMMAtlasParam,
+                 images: Sequence[torch.Tensor], weights: Sequence[float]):
+        from .device import apply, splat
+        from .shooting import LDMMShootingDefDataB200, LDMMShootingIteratorB200
+        self._apply, self._splat = apply, splat
+        nx, ny, nz = size
+        self.shape = (nz, ny, nx)
+        self.param = param
+        self.w = [float(x) for x in weights]
+        self.n = nx * ny * nz
+        self.mean = torch.zeros(self.shape, device="cuda")
+        self.acc = torch.zeros(self.shape, device="cuda")
+        self.jsum = torch.zeros(self.shape, device="cuda")
+        self._ones = torch.ones(self.shape, device="cuda")
+        self.images = list(images)
+        self.its, self.data = [], []
+        for i, img in enumerate(self.images):
+            _check_image(img, f"image {i}")
+            if tuple(img.shape) != self.shape:
+                raise ValueError("LDMM atlas subjects must be on the template grid")
+            it = LDMMShootingIteratorB200(size, spacing=spacing, n_time_steps=param.NTimeSteps)
+            it.SetScaleLevel(size, spacing, param.Iterator)
+            self.its.append(it)
+            self.data.append(LDMMShootingDefDataB200(self.mean, img, spacing))
+
+    def mean_sums(self):
+        L, s = _lib.lib(), _stream()
+        js = self.param.JacobianScale
+        self.acc.zero_()
+        self.jsum.zero_()
+        for d, w in zip(self.data, self.w):
+            img = self._apply(d.I1, d.Phi0T)
+            jd = self._splat(self._ones, d.PhiT0) if js else None
+            check(L.aw_ldmm_atlas_accumulate(self.acc.data_ptr(), self.jsum.data_ptr(),
+                                             img.data_ptr(), jd.data_ptr() if js else None, w,
+                                             self.n, s))
+        return self.acc, (self.jsum if js else None)
+
+    def deformed(self) -> List[torch.Tensor]:
+        return [self._apply(d.I1, d.Phi0T) for d in self.data]
+
+    set_median = CudaLDMMAtlasEngine.set_median
+    set_mean = CudaLDMMAtlasEngine.set_mean
+    device_of_sums = CudaLDMMAtlasEngine.device_of_sums
+
+    def iterate(self, first: bool) -> None:
+        for it, d in zip(self.its, self.data):
+            it.Iterate(d)
+
+    def velocities(self, i: int) -> torch.Tensor:
+        """The shooting subject's state: its initial momentum alpha0."""
+        return self.data[i].Alpha0
+
+    def step(self, i: int) -> float:
+        return float(self.param.Iterator.StepSize)
+
+    def energies(self, i: int) -> np.ndarray:
+        return self.its[i].Energies()
+
+
 class LDMMAtlasBuilderB200:
     """LDMMAtlasBuilder over the subjects of this rank (one scale level).
 
@@ -237,7 +314,10 @@ class LDMMAtlasBuilderB200:
         self.local = local_subjects(self.n_total, self.rank, self.world)
         if not self.local:
             raise ValueError(f"rank {self.rank} owns no subject: use at most {self.n_total} ranks")
-        factory = engine_factory or CudaLDMMAtlasEngine
+        if param.Shooting and (param.ComputeMedian or param.TrimmedMeanSize):
+            raise ValueError("ComputeMedian / TrimmedMeanSize are not supported with Shooting")
+        factory = engine_factory or (CudaLDMMShootingAtlasEngine if param.Shooting
+                                     else CudaLDMMAtlasEngine)
         self.engine = factory(tuple(size), tuple(float(s) for s in spacing), param,
                               [images[i] for i in self.local], [weights[i] for i in self.local])
         self.mean = None
@@ -302,7 +382,8 @@ class LDMMAtlasBuilderB200:
         return self.mean
 
     def GetVelocities(self, i: int) -> torch.Tensor:
-        """v [T, 3, nz, ny, nx] of global subject i (local to this rank)."""
+        """v [T, 3, nz, ny, nx] of global subject i (local to this rank); with
+        Shooting, its initial momentum alpha0 [nz, ny, nx]."""
         return self.engine.velocities(self.local.index(i))
 
     def GetStepSize(self, i: int) -> float:

@@ -491,6 +491,47 @@ class Oracle:
             mean = mean_of()
         return mean, vs, en
 
+    def ldmm_shoot_atlas_run(self, imgs, weights, T, iters, sp=(1.0, 1.0, 1.0), sigma=0.1,
+                             step=0.005, alpha=0.01, beta=0.01, gamma=0.001,
+                             jacobian_scale=True):
+        """The shooting atlas: AtlasThreadMain (Algorithms/Common/AtlasThread.txx:
+        97-181) with LDMMShootingAtlasThreadCPU's mean (LDMM/
+        LDMMShootingAtlasThreadCPU.cxx:183-224): every subject one
+        LDMMShootingIteratorCPU::Iterate toward the mean (I0 = the mean, I1 =
+        the subject, LDMMShootingAtlasDefDataCPU, .cxx:42-52), then
+        sum w I1(phi0T) J / sum w J with J = forwardApply(ones, phiT0)
+        (LDMMShootingIteratorCPU::ComputeJacDet, .cxx:108-119). Returns
+        (mean, [alpha0_i], image energies [iters, ns])."""
+        ns = len(imgs)
+        shape = imgs[0].shape
+        a0 = [np.zeros(shape, np.float32) for _ in range(ns)]
+        maps = [(identity(shape), identity(shape)) for _ in range(ns)]
+        ones = np.ones(shape, np.float32)
+
+        def mean_of():
+            acc = np.zeros(shape, np.float32)
+            jsum = np.zeros(shape, np.float32)
+            for img, (p0, p1), w in zip(imgs, maps, weights):
+                d = self.apply(img, p0)
+                w = np.float32(w)
+                if jacobian_scale:
+                    jd = self.splat(ones, p1)
+                    acc += (d * jd) * w
+                    jsum += jd * w
+                else:
+                    acc += d * w
+            return acc / jsum if jacobian_scale else acc
+
+        mean = mean_of()
+        en = np.zeros((iters, ns))
+        for k in range(iters):
+            for i in range(ns):
+                en[k, i], p0, p1 = self.ldmm_shoot_iterate(mean, imgs[i], a0[i], T, sp, alpha,
+                                                           beta, gamma, sigma, step)
+                maps[i] = (p0, p1)
+            mean = mean_of()
+        return mean, a0, en
+
     def greedy_run(self, I0, I1, iters, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01, gamma=0.001,
                    max_pert=0.5, inverse=False):
         """Single-scale greedy registration from the identity."""

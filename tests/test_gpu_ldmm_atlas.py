@@ -159,3 +159,28 @@ def test_ldmm_atlas_reweighted_vs_oracle(oracle, compute_median, trimmed):
         vg = host(b.GetVelocities(i))
         assert np.abs(vg - v_o[i]).max() <= 1e-3 * np.abs(v_o[i]).max()
         assert np.allclose(b.GetEnergies(i)[-iters:], e_o[:, i], rtol=1e-4)
+
+
+@pytest.mark.parametrize("jacobian_scale", [True, False])
+def test_ldmm_shooting_atlas_vs_oracle(oracle, jacobian_scale):
+    """The shooting atlas (LDMMShootingAtlasThreadCPU): every subject's
+    momentum shooting toward the mean and the mean of I1(phi0T) weighted by
+    splat(ones, phiT0), against the oracle's loop over its pinned shooting
+    iteration: mean 1e-4 of max, alpha0 1e-3 of max, energies 1e-4."""
+    shape, T, iters = (16, 16, 16), 3, 3
+    imgs = [greedy_pair(shape, 70 + k, n_blobs=4, umax=1.5, sigma_range=(1.5, 3.0),
+                        smooth_sigma=3.0)[1] for k in range(3)]
+    w = [0.5, 0.3, 0.2]
+    m_o, a_o, e_o = oracle.ldmm_shoot_atlas_run(imgs, w, T, iters, sigma=1.0, step=0.1,
+                                                jacobian_scale=jacobian_scale)
+    param = LDMMAtlasParam(LDMMIteratorParam(DiffOperParam(), 1.0, 0.1, False, 0.2),
+                           NTimeSteps=T, NIterations=iters, JacobianScale=jacobian_scale,
+                           Shooting=True)
+    b = LDMMAtlasBuilderB200([cu(a) for a in imgs], shape[::-1], param, weights=w)
+    mean = host(b.BuildAtlas())
+    assert np.abs(mean - m_o).max() <= 1e-4 * np.abs(m_o).max()
+    for i in range(3):
+        ag = host(b.GetVelocities(i))
+        assert np.abs(ag - a_o[i]).max() <= 1e-3 * np.abs(a_o[i]).max()
+        assert np.allclose(b.GetEnergies(i)[-iters:], e_o[:, i], rtol=1e-4)
+    assert np.abs(a_o[0]).max() > 0
