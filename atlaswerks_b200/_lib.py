@@ -107,6 +107,7 @@ SIGNATURES = {
     "aw_ldmm_atlas_accumulate": ([_fp] * 4 + [ctypes.c_float, ctypes.c_long, _fp], _i),
     "aw_ldmm_set_vector_energy": ([_fp, _i], _i),
     "aw_ldmm_geodesic_shoot": ([_fp] * 7, _i),
+    "aw_ldmm_velshoot_iterate": ([_fp] * 6 + [_i, _fp], _i),
     "aw_ldmm_get_vec_step_energies": ([_fp, _fp, _i], _i),
     "aw_ldmm_atlas_voxel_median": ([_fp, _i, _i, _i, _i, _i, _fp, _fp], _i),
     "aw_ldmm_atlas_normalize": ([_fp, _fp, ctypes.c_long, _fp], _i),

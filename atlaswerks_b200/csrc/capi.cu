@@ -890,6 +890,18 @@ int aw_ldmm_shoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *
   return 0;
 }
 
+int aw_ldmm_velshoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *v0,
+                             float *phi0T, float *phiT0, int update_step, void *stream) {
+  if (!l || !I0 || !I1 || !v0 || !phi0T || !phiT0)
+    return fail("aw_ldmm_velshoot_iterate: null pointer");
+  if (aw::ldmm_velshoot_prepare(&l->ctx))
+    return fail("aw_ldmm_velshoot_iterate: device allocation failed");
+  AW_CUDA(aw::ldmm_velshoot_iterate(&l->ctx, I0, I1, v0, phi0T, phiT0, update_step ? 1 : 0,
+                                    S(stream)),
+          "aw_ldmm_velshoot_iterate");
+  return 0;
+}
+
 int aw_ldmm_geodesic_shoot(aw_ldmm_t l, const float *I0, const float *alpha0, float *phi0T,
                            float *phiT0, float *image, void *stream) {
   if (!l || !I0 || !alpha0 || !phi0T || !phiT0 || !image)

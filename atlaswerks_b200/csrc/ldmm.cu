@@ -444,7 +444,8 @@ void ldmm_destroy(LdmmCtx *c) {
   fluid_plan_destroy(&c->plan);
   void *ptrs[] = {c->J0,     c->hbuf,   c->diff, c->S,   c->u,   c->splat_scratch,
                   c->partials, c->energy, c->scalars, c->JT, c->JD, c->adV,
-                  c->adP,    c->adA,    c->adI,  c->venergy, c->adSortMem, c->vstep};
+                  c->adP,    c->adA,    c->adI,  c->venergy, c->adSortMem, c->vstep,
+                  c->vsBuf};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   std::memset(c, 0, sizeof(*c));
@@ -928,6 +929,167 @@ cudaError_t ldmm_geodesic_shoot(LdmmCtx *c, const float *I0, const float *alpha0
   if (ca) AW_TRY(cudaMemcpyAsync(phi0T, A[1], sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
   if (cb) AW_TRY(cudaMemcpyAsync(phiT0, B[1], sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
   return cudaMemcpyAsync(img, c->J0, sizeof(float) * n, cudaMemcpyDeviceToDevice, s);
+}
+
+namespace {
+
+// D phiT0 = identity: rows x | y | z, each a vector field [3][N]
+__global__ void k_dphi_identity(float *__restrict__ dp, long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) dp[(long)(3 * r + c) * n + i] = r == c ? 1.0f : 0.0f;
+}
+
+// row += g (Array3D<Vector3D<Real>>::pointwiseAdd), 3N floats
+__global__ void k_add3(float *__restrict__ row, const float *__restrict__ g, long n3) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n3) row[i] = fadd(row[i], g[i]);
+}
+
+// f = |D phiT0| (D phiT0)^T (L v0)(phiT0): the compose of L v0 at phiT0
+// (HField3DUtils::compose, PARTIAL_ZERO), the transposed product and the
+// determinant in the reference's float order (LDMMVelShootingIteratorCPU.
+// cxx:276-320)
+__global__ void __launch_bounds__(kRowThreads)
+    k_velshoot_force(const float *__restrict__ dp, const float *__restrict__ lv0,
+                     const float *__restrict__ hx, const float *__restrict__ hy,
+                     const float *__restrict__ hz, float *__restrict__ f, Dims d) {
+  Voxel v;
+  if (!voxel_of(d, v)) return;
+  const long n = d.n(), i = v.i;
+  float lx, ly, lz;
+  trilerp_vector<false>(lv0, lv0 + n, lv0 + 2 * n, d, hx[i], hy[i], hz[i], BG_PARTIAL_ZERO, 1.0f,
+                        lx, ly, lz);
+  const float xx = dp[i], xy = dp[n + i], xz = dp[2 * n + i];
+  const float yx = dp[3 * n + i], yy = dp[4 * n + i], yz = dp[5 * n + i];
+  const float zx = dp[6 * n + i], zy = dp[7 * n + i], zz = dp[8 * n + i];
+  const float fx = fadd(fadd(fmul(xx, lx), fmul(yx, ly)), fmul(zx, lz));
+  const float fy = fadd(fadd(fmul(xy, lx), fmul(yy, ly)), fmul(zy, lz));
+  const float fz = fadd(fadd(fmul(xz, lx), fmul(yz, ly)), fmul(zz, lz));
+  const float t1 = fmul(xx, fsub(fmul(yy, zz), fmul(yz, zy)));
+  const float t2 = fmul(xy, fsub(fmul(yx, zz), fmul(yz, zx)));
+  const float t3 = fmul(xz, fsub(fmul(yx, zy), fmul(yy, zx)));
+  const float det = fadd(fsub(t1, t2), t3);
+  f[i] = fmul(fx, det);
+  f[n + i] = fmul(fy, det);
+  f[2 * n + i] = fmul(fz, det);
+}
+
+}  // namespace
+
+int ldmm_velshoot_prepare(LdmmCtx *c) {
+  if (c->vsBuf) return 0;
+  if (cudaMalloc(&c->vsBuf, sizeof(float) * 15 * (size_t)c->d.n()) != cudaSuccess) {
+    cudaGetLastError();
+    c->vsBuf = nullptr;
+    return 3;
+  }
+  return 0;
+}
+
+// LDMMVelShootingIteratorCPU::Iterate (LDMM/LDMMVelShootingIteratorCPU.cxx:
+// 186-344): the geodesic in velocity form from v0 — for t = 0..T-1 the step
+// energy <L v_t, v_t>, phiT0 = composeHVInv(phiT0, v_t) [PARTIAL_ID], phi0T =
+// composeVH(v_t, phi0T) [PARTIAL_ZERO], and before the next step D phiT0 +=
+// grad(v_t,c(phiT0)) per component c and v_{t+1} = K(|D phiT0| (D phiT0)^T
+// (L v0)(phiT0)) — then the residual I0(phiT0) - I1, its energy (recorded in
+// the step-size pass too, as the reference adds it), its splat by phiT0 and
+// K(grad(I0) splat), and the update of v0 (or the step). The step energies
+// after the first are formed as <f_{t-1}, v_t> with v_t = K f_{t-1}: no
+// further transform.
+cudaError_t ldmm_velshoot_iterate(LdmmCtx *c, const float *I0, const float *I1, float *v0,
+                                  float *phi0T, float *phiT0, int update_step, cudaStream_t s) {
+  const Dims d = c->d;
+  const long n = d.n();
+  const int T = c->T;
+  auto comp = [&](float *base, int k) { return base + k * n; };
+  float *A[2] = {phi0T, c->hbuf}, *B[2] = {phiT0, c->hbuf + 3 * n};
+  int ca = 0, cb = 0;
+  float *vt = c->u, *lv0 = c->vsBuf, *dp = lv0 + 3 * n, *f = dp + 9 * n;
+  float *img = c->S, *g = f;  // g (a gradient) and f are never live together
+  const double spprod = c->sp.x * c->sp.y * c->sp.z;
+  const unsigned flat = (unsigned)((n + 255) / 256), flat3 = (unsigned)((3 * n + 255) / 256);
+  auto record_vec = [&](const float *a, const float *b, int t) -> cudaError_t {
+    k_field_dot<<<row_grid(d), kRowThreads, 0, s>>>(a, b, c->partials, d);
+    AW_TRY(cudaGetLastError());
+    k_record_energy<<<1, kRecThreads, 0, s>>>(c->partials, c->nparts, spprod, c->venergy,
+                                              c->count, c->cap, 0, t > 0 ? 1 : 0, 0);
+    AW_TRY(cudaGetLastError());
+    k_record_energy<<<1, kRecThreads, 0, s>>>(c->partials, c->nparts, spprod, c->vstep + t,
+                                              c->zero, 1, 0, 0, 0);
+    return cudaGetLastError();
+  };
+  k_identity<<<row_grid(d), kRowThreads, 0, s>>>(comp(phi0T, 0), comp(phi0T, 1), comp(phi0T, 2), d);
+  AW_TRY(cudaGetLastError());
+  k_identity<<<row_grid(d), kRowThreads, 0, s>>>(comp(phiT0, 0), comp(phiT0, 1), comp(phiT0, 2), d);
+  AW_TRY(cudaGetLastError());
+  AW_TRY(cudaMemcpyAsync(vt, v0, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
+  k_dphi_identity<<<flat, 256, 0, s>>>(dp, n);
+  AW_TRY(cudaGetLastError());
+  AW_TRY(fluid_forward_field(c->plan, comp(v0, 0), comp(v0, 1), comp(v0, 2), s));
+  AW_TRY(fluid_solve(c->plan, 0, s));
+  AW_TRY(fluid_inverse_store(c->plan, comp(lv0, 0), comp(lv0, 1), comp(lv0, 2), s));
+  for (int t = 0; t < T; ++t) {
+    AW_TRY(t == 0 ? record_vec(lv0, vt, 0) : record_vec(f, vt, t));
+    {
+      const float *gg[3] = {comp(B[cb], 0), comp(B[cb], 1), comp(B[cb], 2)};
+      const float *vv[3] = {comp(vt, 0), comp(vt, 1), comp(vt, 2)};
+      float *oo[3] = {comp(B[1 - cb], 0), comp(B[1 - cb], 1), comp(B[1 - cb], 2)};
+      AW_TRY(launch_compose_hv(gg, vv, oo, d, c->sp, -1, BG_PARTIAL_ID, nullptr, 1.0f, s));
+      cb = 1 - cb;
+    }
+    {
+      const float *vv[3] = {comp(vt, 0), comp(vt, 1), comp(vt, 2)};
+      const float *hh[3] = {comp(A[ca], 0), comp(A[ca], 1), comp(A[ca], 2)};
+      float *oo[3] = {comp(A[1 - ca], 0), comp(A[1 - ca], 1), comp(A[1 - ca], 2)};
+      AW_TRY(launch_compose_vh(vv, hh, oo, d, c->sp, 1, BG_PARTIAL_ZERO, nullptr, 1.0f, s));
+      ca = 1 - ca;
+    }
+    if (t == T - 1) break;
+    for (int r = 0; r < 3; ++r) {
+      AW_TRY(launch_apply(comp(vt, r), comp(B[cb], 0), comp(B[cb], 1), comp(B[cb], 2), img, d,
+                          0.0f, s));
+      AW_TRY(launch_gradient(img, comp(g, 0), comp(g, 1), comp(g, 2), d, c->sp, 0, s));
+      k_add3<<<flat3, 256, 0, s>>>(dp + (long)3 * r * n, g, 3 * n);
+      AW_TRY(cudaGetLastError());
+    }
+    k_velshoot_force<<<row_grid(d), kRowThreads, 0, s>>>(dp, lv0, comp(B[cb], 0), comp(B[cb], 1),
+                                                         comp(B[cb], 2), f, d);
+    AW_TRY(cudaGetLastError());
+    AW_TRY(fluid_forward_field(c->plan, comp(f, 0), comp(f, 1), comp(f, 2), s));
+    AW_TRY(fluid_solve(c->plan, 1, s));
+    AW_TRY(fluid_inverse_store(c->plan, comp(vt, 0), comp(vt, 1), comp(vt, 2), s));
+  }
+  // residual, image energy, its splat, K(grad(I0) splat), the update
+  AW_TRY(launch_apply(I0, comp(B[cb], 0), comp(B[cb], 1), comp(B[cb], 2), img, d, 0.0f, s));
+  k_residual<<<row_grid(d), kRowThreads, 0, s>>>(img, I1, c->diff, c->partials, d);
+  AW_TRY(cudaGetLastError());
+  k_record_energy<<<1, kRecThreads, 0, s>>>(c->partials, c->nparts, spprod, c->energy, c->count,
+                                            c->cap);
+  AW_TRY(cudaGetLastError());
+  AW_TRY(splat(c->sw, c->diff, comp(B[cb], 0), comp(B[cb], 1), comp(B[cb], 2), img, 0.0f, s));
+  AW_TRY(fluid_forward_force(c->plan, I0, img, 0, s));
+  AW_TRY(fluid_solve(c->plan, 1, s));
+  if (update_step) {
+    AW_TRY(cudaMemsetAsync(c->maxbits, 0, sizeof(unsigned), s));
+    AW_TRY(fluid_inverse_store(c->plan, comp(f, 0), comp(f, 1), comp(f, 2), s));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->plan.device);
+    k_max_disp<<<sms * 4, 256, 0, s>>>(comp(v0, 0), comp(v0, 1), comp(v0, 2), comp(f, 0),
+                                       comp(f, 1), comp(f, 2), n, c->sigma, c->maxbits);
+    AW_TRY(cudaGetLastError());
+    k_step_from_max<<<1, 1, 0, s>>>(c->maxbits, c->max_pert, c->step);
+    AW_TRY(cudaGetLastError());
+  } else {
+    AW_TRY(fluid_inverse_axpby(c->plan, comp(v0, 0), comp(v0, 1), comp(v0, 2), c->step, c->sigma,
+                               s));
+  }
+  if (ca) AW_TRY(cudaMemcpyAsync(phi0T, A[1], sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
+  if (cb) AW_TRY(cudaMemcpyAsync(phiT0, B[1], sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
+  return cudaSuccess;
 }
 
 int ldmm_adshoot_prepare(LdmmCtx *c) {

@@ -34,6 +34,7 @@ struct LdmmCtx {
   int orig;         // IterateOrig (Jacobian path) instead of IterateNew
   int vec_energy;   // IterateNew / IterateOrig also record sum_t <L v_t, v_t>
   double *vstep;    // T: <L v_t, v_t> sp^3 of each t, of the last such iteration
+  float *vsBuf;     // velocity shooting (ldmm_velshoot_prepare): L v0 3N | D phiT0 9N | f 3N
   int *zero;        // a device int that stays 0 (index of one-slot records)
   float *JT;        // T x N: I1 pulled back to each time point (IterateOrig)
   float *JD;        // T x N: transported Jacobian determinants (IterateOrig)
@@ -71,6 +72,13 @@ cudaError_t ldmm_voxel_median(const VoxelImages &in, int nimg, int k, long n, fl
 int ldmm_shoot_prepare(LdmmCtx *c);
 cudaError_t ldmm_shoot_iterate(LdmmCtx *c, const float *I0, const float *I1, float *alpha0,
                                float *phi0T, float *phiT0, cudaStream_t s);
+// LDMMVelShootingIteratorCPU (LDMM/LDMMVelShootingIteratorCPU.cxx): the
+// buffers (returns 3 when the allocation fails) and one Iterate; v0, phi0T,
+// phiT0 are [3][N]; update_step: set the step from the update's size
+// instead of moving v0
+int ldmm_velshoot_prepare(LdmmCtx *c);
+cudaError_t ldmm_velshoot_iterate(LdmmCtx *c, const float *I0, const float *I1, float *v0,
+                                  float *phi0T, float *phiT0, int update_step, cudaStream_t s);
 // LDMMGeodesicShootingGPU::ShootImage(I0, alpha0, T): the geodesic alone
 cudaError_t ldmm_geodesic_shoot(LdmmCtx *c, const float *I0, const float *alpha0, float *phi0T,
                                 float *phiT0, float *img, cudaStream_t s);

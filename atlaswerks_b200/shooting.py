@@ -10,6 +10,10 @@
   geodesic from alpha0 over T time steps, pull the residual back by
   splatting and update alpha0 (LDMMShootingIteratorCPU.cxx:199-304).
 
+* ``LDMMVelShootingIteratorB200`` / ``LDMMVelShootingDefDataB200`` —
+  LDMMVelShootingIteratorCPU and its data (LDMM/LDMMVelShootingIteratorCPU.cxx:
+  186-344): the geodesic in velocity form from v0, the Jacobian of phiT0
+  carried along, the update of v0.
 * ``LDMMGeodesicShootingB200`` — LDMMGeodesicShootingCPU / GPU
   (LDMM/LDMMGeodesicShooting.h): ``ShootImage(I0, alpha0, T)``, the geodesic
   alone, with ``GetFinalImage``, ``GetPhi0To1`` and ``GetPhi1To0``.
@@ -173,6 +177,63 @@ class LDMMAdShootingIteratorB200(LDMMShootingIteratorB200):
         """PhiT0 composed from the identity through the last iteration's v_t."""
         self._final(data, 1)
 
+
+
+class LDMMVelShootingDefDataB200:
+    """LDMMVelShootingDefData (Algorithms/LDMM/LDMMVelShootingDefData.h): I0,
+    I1, the initial velocity ``V0`` [3, nz, ny, nx] (zero at the start) and
+    the maps ``Phi0T`` / ``PhiT0`` of the last shooting."""
+
+    def __init__(self, I0: torch.Tensor, I1: torch.Tensor, spacing=(1.0, 1.0, 1.0)):
+        _check_image(I0, "I0")
+        _check_image(I1, "I1")
+        if I0.shape != I1.shape:
+            raise ValueError("I0 and I1 must have the same grid")
+        self.I0, self.I1 = I0, I1
+        self.spacing = tuple(float(s) for s in spacing)
+        shape = tuple(I0.shape)
+        self.V0 = torch.zeros((3,) + shape, device=I0.device, dtype=torch.float32)
+        self.Phi0T = identity(shape, I0.device)
+        self.PhiT0 = identity(shape, I0.device)
+
+    def GetDef0To1(self) -> torch.Tensor:
+        return self.Phi0T
+
+    def GetDef1To0(self) -> torch.Tensor:
+        return self.PhiT0
+
+    def GetI0At1(self) -> torch.Tensor:
+        return apply(self.I0, self.PhiT0)
+
+    def GetI1At0(self) -> torch.Tensor:
+        return apply(self.I1, self.Phi0T)
+
+
+class LDMMVelShootingIteratorB200(LDMMShootingIteratorB200):
+    """LDMMVelShootingIteratorCPU (LDMM/LDMMVelShootingIteratorCPU.cxx:
+    186-344): the geodesic in velocity form from v0; Iterate updates V0 (or,
+    after UpdateStepSizeNextIteration, sets the step from the update's
+    size); StepSize()."""
+    DeformationDataType = LDMMVelShootingDefDataB200
+
+    def __init__(self, *args, **kwargs):
+        super().__init__(*args, **kwargs)
+        self._update_step = False
+
+    def UpdateStepSizeNextIteration(self):
+        self._update_step = True
+
+    def StepSize(self) -> float:
+        st = ctypes.c_float()
+        check(_lib.lib().aw_ldmm_get_step(self._h, ctypes.byref(st)))
+        return float(st.value)
+
+    def Iterate(self, data: LDMMVelShootingDefDataB200):
+        check(_lib.lib().aw_ldmm_velshoot_iterate(self._h, data.I0.data_ptr(),
+                                                  data.I1.data_ptr(), data.V0.data_ptr(),
+                                                  data.Phi0T.data_ptr(), data.PhiT0.data_ptr(),
+                                                  int(self._update_step), _stream()))
+        self._update_step = False
 
 
 class LDMMGeodesicShootingB200:

@@ -365,6 +365,18 @@ int aw_ldmm_get_energies(aw_ldmm_t l, double *out, int max_count, int *count);
  * energies <L v_t, v_t> (aw_ldmm_get_vec_energies). */
 int aw_ldmm_shoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *alpha0,
                           float *phi0T, float *phiT0, void *stream);
+/* LDMMVelShootingIteratorCPU::Iterate (Algorithms/LDMM/
+ * LDMMVelShootingIteratorCPU.cxx:186-344) on an LDMM handle (its T, sigma,
+ * MaxPert, step size and kernel): shoots the geodesic in velocity form from
+ * v0 ([3][N], updated in place to (1 - 2 step) v0 + (2 step / sigma^2)
+ * K(grad(I0) splat(I0(phiT0) - I1 by phiT0))), leaves the maps phi0T / phiT0
+ * ([3][N] each) in the caller's buffers and records the image energy and
+ * the step energies (aw_ldmm_get_energies, aw_ldmm_get_vec_energies,
+ * aw_ldmm_get_vec_step_energies). update_step = 1: the step-size pass
+ * (step = MaxPert / max |2 v0 - (2/sigma^2) K(...)|, v0 unchanged). Its
+ * buffers (15 N floats) are allocated at the first call. */
+int aw_ldmm_velshoot_iterate(aw_ldmm_t l, const float *I0, const float *I1, float *v0,
+                             float *phi0T, float *phiT0, int update_step, void *stream);
 /* LDMMGeodesicShootingGPU / CPU::ShootImage(I0, alpha0, nTimeSteps)
  * (Algorithms/LDMM/LDMMGeodesicShootingCPU.cxx:44-157): the geodesic from I0
  * along the momentum alpha0 over the handle's T time steps and kernel,

@@ -97,6 +97,7 @@ class Oracle:
         L.aw_oracle_ldmm_iterate.restype = ctypes.c_double
         L.aw_oracle_atlas_iterate.restype = ctypes.c_double
         L.aw_oracle_ldmm_iterate_orig.restype = ctypes.c_double
+        L.aw_oracle_ldmm_velshoot_iterate.restype = ctypes.c_double
         L.aw_oracle_ldmm_shoot_iterate.restype = ctypes.c_double
         L.aw_oracle_ldmm_adshoot_iterate.restype = ctypes.c_double
 
@@ -279,6 +280,23 @@ class Oracle:
             *_shape(I0), *map(_dbl, sp), _dbl(alpha), _dbl(beta), _dbl(gamma),
             ctypes.c_float(sigma), ctypes.c_float(step), ctypes.byref(ev) if vec else None)
         return (float(e), float(ev.value), p0, p1) if vec else (float(e), p0, p1)
+
+    def ldmm_velshoot_iterate(self, I0, I1, v0, T, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01,
+                              gamma=0.001, sigma=0.1, step=0.005, update_step=False,
+                              max_pert=0.1):
+        """One LDMMVelShootingIteratorCPU::Iterate; v0 [3,nz,ny,nx] updated in
+        place (or the step set with update_step). Returns (image energy,
+        vector energy, step, phi0T, phiT0)."""
+        assert v0.dtype == np.float32 and v0.flags.c_contiguous
+        p0 = np.empty((3,) + I0.shape, np.float32)
+        p1 = np.empty((3,) + I0.shape, np.float32)
+        st = ctypes.c_float(step)
+        ev = ctypes.c_double()
+        e = self.lib.aw_oracle_ldmm_velshoot_iterate(
+            _fp(I0), _fp(I1), _fp(v0), _fp(p0), _fp(p1), _i(T), *_shape(I0), *map(_dbl, sp),
+            _dbl(alpha), _dbl(beta), _dbl(gamma), ctypes.c_float(sigma), ctypes.byref(st),
+            _i(int(update_step)), ctypes.c_float(max_pert), ctypes.byref(ev))
+        return float(e), float(ev.value), float(st.value), p0, p1
 
     def geodesic_shoot(self, I0, alpha0, T, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01,
                        gamma=0.001):
@@ -798,6 +816,26 @@ class Reference:
                 _fp(a0), p0.ctypes.data_as(_f), p1.ctypes.data_as(_f), _dp(en), _dp(ev))
         self._check(rc)
         return (a0, p0, p1, en, ev) if vec else (a0, p0, p1, en)
+
+    def velshoot_run(self, I0, I1, T, iters, sp=(1.0, 1.0, 1.0), sigma=0.1, step=0.005,
+                     adaptive=False, max_pert=0.1, alpha=0.01, beta=0.01, gamma=0.001):
+        """The reference's LDMMVelShootingIteratorCPU through the LDMMWarp loop
+        at one scale. Returns (v0, phi0T, phiT0, image energies, vector
+        energies, step)."""
+        v0 = np.empty((3,) + I0.shape, np.float32)
+        p0 = np.empty((3,) + I0.shape, np.float32)
+        p1 = np.empty((3,) + I0.shape, np.float32)
+        en = np.zeros(iters, np.float64)
+        ve = np.zeros(iters, np.float64)
+        st = ctypes.c_float()
+        with quiet_stdout():
+            rc = self.lib.awref_velshoot_run(
+                _fp(I0), _fp(I1), *_shape(I0), *map(_dbl, sp), _i(T), _i(iters),
+                ctypes.c_float(sigma), ctypes.c_float(step), _i(int(adaptive)),
+                ctypes.c_float(max_pert), _dbl(alpha), _dbl(beta), _dbl(gamma), _fp(v0), _fp(p0),
+                _fp(p1), _dp(en), _dp(ve), ctypes.byref(st))
+        self._check(rc)
+        return v0, p0, p1, en, ve, float(st.value)
 
     def geodesic_shoot(self, I0, alpha0, T, sp=(1.0, 1.0, 1.0), alpha=0.01, beta=0.01,
                        gamma=0.001):

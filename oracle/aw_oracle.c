@@ -1021,6 +1021,117 @@ void aw_oracle_geodesic_shoot(const float *I0, const float *alpha0, int T, int n
   free(aT);
 }
 
+/* LDMMVelShootingIteratorCPU::Iterate (Algorithms/LDMM/
+ * LDMMVelShootingIteratorCPU.cxx:186-344): the geodesic in velocity form
+ * from v0, v_t = K(|D phiT0| (D phiT0)^T (L v0)(phiT0)), D phiT0 accumulated
+ * as identity plus the gradients of the velocity components pulled back by
+ * phiT0, both maps advanced by composeHVInv [PARTIAL_ID] / composeVH
+ * [PARTIAL_ZERO]; then the residual I0(phiT0) - I1 splatted by phiT0,
+ * K(grad(I0) * splat) and the velocity update v0 = (1 - 2 step) v0 +
+ * (2 step / sigma^2) K(...) (or, with update_step, step = max_pert / max
+ * |2 v0 - (2/sigma^2) K(...)|). v0, phi0T, phiT0 are [3][N]. Returns the
+ * image energy sp^3 sum diff^2; *vec_energy = sum_t <L v_t, v_t>. */
+double aw_oracle_ldmm_velshoot_iterate(const float *I0, const float *I1, float *v0, float *phi0T,
+                                       float *phiT0, int T, int nx, int ny, int nz, double spx,
+                                       double spy, double spz, double alpha, double beta,
+                                       double gamma, float sigma, float *step, int update_step,
+                                       float max_pert, double *vec_energy) {
+  const long n = (long)nx * ny * nz;
+  float *vt = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *lv0 = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *dp = (float *)malloc(sizeof(float) * (size_t)(9 * n)); /* rows x | y | z, each [3][N] */
+  float *o = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *g = (float *)malloc(sizeof(float) * (size_t)(3 * n));
+  float *si = (float *)malloc(sizeof(float) * (size_t)n);
+  float *p0 = phi0T, *p1 = phiT0;
+  aw_oracle_identity(p0, p0 + n, p0 + 2 * n, nx, ny, nz);
+  aw_oracle_identity(p1, p1 + n, p1 + 2 * n, nx, ny, nz);
+  memcpy(vt, v0, sizeof(float) * (size_t)(3 * n));
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c)
+      for (long k = 0; k < n; ++k) dp[(long)(3 * r + c) * n + k] = r == c ? 1.0f : 0.0f;
+  memcpy(lv0, v0, sizeof(float) * (size_t)(3 * n));
+  aw_oracle_fluid_apply(lv0, lv0 + n, lv0 + 2 * n, nx, ny, nz, spx, spy, spz, alpha, beta, gamma,
+                        0);
+  double ev = 0.0;
+  for (int t = 0; t < T; ++t) {
+    ev += l_energy(vt, o, nx, ny, nz, spx, spy, spz, alpha, beta, gamma);
+    aw_oracle_compose_hv(p1, p1 + n, p1 + 2 * n, vt, vt + n, vt + 2 * n, o, o + n, o + 2 * n, nx,
+                         ny, nz, spx, spy, spz, -1, AW_BG_PARTIAL_ID);
+    memcpy(p1, o, sizeof(float) * (size_t)(3 * n));
+    aw_oracle_compose_vh(vt, vt + n, vt + 2 * n, p0, p0 + n, p0 + 2 * n, o, o + n, o + 2 * n, nx,
+                         ny, nz, spx, spy, spz, 1, AW_BG_PARTIAL_ZERO);
+    memcpy(p0, o, sizeof(float) * (size_t)(3 * n));
+    if (t == T - 1) break;
+    for (int r = 0; r < 3; ++r) {
+      aw_oracle_apply(vt + (long)r * n, p1, p1 + n, p1 + 2 * n, si, nx, ny, nz, 0.0f);
+      aw_oracle_gradient(si, g, g + n, g + 2 * n, nx, ny, nz, spx, spy, spz, 0);
+      float *row = dp + (long)3 * r * n;
+      for (long k = 0; k < 3 * n; ++k) row[k] += g[k];
+    }
+    /* (L v0)(phiT0) with PARTIAL_ZERO, then (D phiT0)^T times it and |D phiT0| */
+    for (int z = 0; z < nz; ++z)
+      for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x) {
+          const long i = IDX(x, y, z);
+          float lx, ly, lz;
+          trilerp_vec(lv0, lv0 + n, lv0 + 2 * n, nx, ny, nz, p1[i], p1[n + i], p1[2 * n + i], &lx,
+                      &ly, &lz, AW_BG_PARTIAL_ZERO);
+          const float xx = dp[i], xy = dp[n + i], xz = dp[2 * n + i];
+          const float yx = dp[3 * n + i], yy = dp[4 * n + i], yz = dp[5 * n + i];
+          const float zx = dp[6 * n + i], zy = dp[7 * n + i], zz = dp[8 * n + i];
+          const float fx = xx * lx + yx * ly + zx * lz;
+          const float fy = xy * lx + yy * ly + zy * lz;
+          const float fz = xz * lx + yz * ly + zz * lz;
+          const float t1 = xx * (yy * zz - yz * zy);
+          const float t2 = xy * (yx * zz - yz * zx);
+          const float t3 = xz * (yx * zy - yy * zx);
+          const float det = t1 - t2 + t3;
+          o[i] = fx * det;
+          o[n + i] = fy * det;
+          o[2 * n + i] = fz * det;
+        }
+    aw_oracle_fluid_apply(o, o + n, o + 2 * n, nx, ny, nz, spx, spy, spz, alpha, beta, gamma, 1);
+    memcpy(vt, o, sizeof(float) * (size_t)(3 * n));
+  }
+  if (vec_energy) *vec_energy = ev;
+  /* residual, its energy, its splat by phiT0 and K(grad(I0) * splat) */
+  aw_oracle_apply(I0, p1, p1 + n, p1 + 2 * n, si, nx, ny, nz, 0.0f);
+  double e = 0.0;
+  for (long k = 0; k < n; ++k) {
+    si[k] = si[k] - I1[k];
+    e += (double)si[k] * (double)si[k];
+  }
+  e *= spx * spy * spz;
+  float *sp_img = (float *)malloc(sizeof(float) * (size_t)n);
+  aw_oracle_splat(si, p1, p1 + n, p1 + 2 * n, sp_img, nx, ny, nz, 0.0f);
+  aw_oracle_gradient(I0, g, g + n, g + 2 * n, nx, ny, nz, spx, spy, spz, 0);
+  for (long k = 0; k < n; ++k) {
+    g[k] *= sp_img[k];
+    g[n + k] *= sp_img[k];
+    g[2 * n + k] *= sp_img[k];
+  }
+  aw_oracle_fluid_apply(g, g + n, g + 2 * n, nx, ny, nz, spx, spy, spz, alpha, beta, gamma, 1);
+  if (update_step) {
+    const float a = 2.0f, b = -2.0f / (sigma * sigma);
+    float mx = 0.f;
+    for (long k = 0; k < n; ++k) {
+      const float x = a * v0[k] + b * g[k];
+      const float y = a * v0[n + k] + b * g[n + k];
+      const float zz = a * v0[2 * n + k] + b * g[2 * n + k];
+      const float len = (float)sqrt((double)(x * x + y * y + zz * zz));
+      if (len > mx) mx = len;
+    }
+    *step = max_pert / mx;
+  } else {
+    const float vfac = (float)(1.0 - 2.0 * (double)*step);
+    const float ufac = (2 * *step) / (sigma * sigma);
+    for (long k = 0; k < 3 * n; ++k) v0[k] = vfac * v0[k] + ufac * g[k];
+  }
+  free(vt); free(lv0); free(dp); free(o); free(g); free(si); free(sp_img);
+  return e;
+}
+
 /* ------------------------------------------------------------------------
  * Adjoint geodesic shooting: LDMMAdShootingIteratorCPU::Iterate
  * (Algorithms/LDMM/LDMMAdShootingIteratorCPU.cxx:237-323) and

@@ -100,6 +100,14 @@ double aw_oracle_ldmm_adshoot_iterate(const float *I0, const float *I1, float *a
 void aw_oracle_geodesic_shoot(const float *I0, const float *alpha0, int T, int nx, int ny, int nz,
                               double spx, double spy, double spz, double alpha, double beta,
                               double gamma, float *phi0T, float *phiT0, float *img);
+/* LDMMVelShootingIteratorCPU::Iterate: v0 updated in place (or *step set
+ * with update_step), phi0T / phiT0 the geodesic's maps; returns the image
+ * energy, *vec_energy the sum of the step energies */
+double aw_oracle_ldmm_velshoot_iterate(const float *I0, const float *I1, float *v0, float *phi0T,
+                                       float *phiT0, int T, int nx, int ny, int nz, double spx,
+                                       double spy, double spz, double alpha, double beta,
+                                       double gamma, float sigma, float *step, int update_step,
+                                       float max_pert, double *vec_energy);
 /* ImageUtils::resampleNew, clamp background, linear (origin 0) */
 void aw_oracle_resample_image(const float *in, int nx, int ny, int nz, double ssx, double ssy,
                               double ssz, float *out, int mx, int my, int mz, double dsx,

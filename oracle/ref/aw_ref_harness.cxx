@@ -33,6 +33,8 @@
 #include "LDMMParam.h"
 #include "LDMMShootingDefData.h"
 #include "LDMMShootingIteratorCPU.h"
+#include "LDMMVelShootingDefData.h"
+#include "LDMMVelShootingIteratorCPU.h"
 #include "MedianCalculator.h"
 #include "MultiscaleManager.h"
 #include "tinyxml.h"
@@ -876,6 +878,66 @@ int awref_geodesic_shoot(const float *i0, const float *a0, int nx, int ny, int n
   from_vf(shooter.GetPhi0To1(), phi0T, phi0T + n, phi0T + 2 * n);
   from_vf(shooter.GetPhi1To0(), phiT0, phiT0 + n, phiT0 + 2 * n);
   from_im(shooter.GetFinalImage(), img);
+  GUARD_END
+}
+
+// LDMMVelShootingIteratorCPU driven through the LDMMWarp loop at one scale:
+// v0 (3N) after iters iterations (the step-size pass first when adaptive),
+// both maps of the last, per iteration the raw image term and the sum of
+// the step energies; step_out the step used
+int awref_velshoot_run(const float *i0, const float *i1, int nx, int ny, int nz, double spx,
+                       double spy, double spz, int T, int iters, float sigma, float step,
+                       int adaptive, float max_pert, double alpha, double beta, double gamma,
+                       float *v0, float *phi0T, float *phiT0, double *energies,
+                       double *vec_energies, float *step_out) {
+  GUARD_BEGIN
+  std::ostringstream xml;
+  xml.precision(17);
+  xml << "<LDMMWarpParameterFile><LDMMScaleLevel><ScaleLevel><DownsampleFactor val=\"1\"/>"
+      << "</ScaleLevel><LDMMIterator>" << diffoper_xml(alpha, beta, gamma) << "<Sigma val=\""
+      << sigma << "\"/><StepSize val=\"" << step << "\"/><UseAdaptiveStepSize val=\""
+      << (adaptive ? "true" : "false") << "\"/><MaxPert val=\"" << max_pert
+      << "\"/></LDMMIterator><NIterations val=\"" << iters
+      << "\"/></LDMMScaleLevel><NTimeSteps val=\"" << T
+      << "\"/><AutoStepReduce val=\"false\"/></LDMMWarpParameterFile>";
+  LDMMParam param;
+  parse_into(param, xml.str());
+  SizeType size(nx, ny, nz);
+  SpacingType sp(spx, spy, spz);
+  OriginType origin(0, 0, 0);
+  RealImage I0(size, origin, sp), I1(size, origin, sp);
+  to_im(i0, I0);
+  to_im(i1, I1);
+  MultiscaleManager scaleManager(size, sp, origin, param);
+  scaleManager.SetScaleVectorFields(false);
+  LDMMVelShootingDefData data(&I0, &I1, param);
+  LDMMVelShootingIteratorCPU iterator(size, origin, sp, T, true);
+  const long n = (long)nx * ny * nz;
+  data.InitializeWarp();
+  scaleManager.SetScaleLevel(0);
+  const LDMMScaleLevelParam &lp = param.GetScaleLevel(0);
+  iterator.SetScaleLevel(scaleManager, lp.Iterator());
+  data.SetScaleLevel(static_cast<const MultiscaleManager &>(scaleManager));
+  data.StepSize(lp.Iterator().StepSize());
+  for (int iter = 0; iter < iters; ++iter) {
+    if (iter == 0 && lp.Iterator().UseAdaptiveStepSize()) {
+      iterator.UpdateStepSizeNextIteration();
+      iterator.Iterate(data);
+    }
+    data.SetCurIter(iter);
+    iterator.Iterate(data);
+    LDMMEnergy *e = dynamic_cast<LDMMEnergy *>(data.GetEnergyHistory().LastEnergy());
+    if (energies) energies[iter] = e ? (double)e->ImageEnergy() * sigma * sigma : 0.0;
+    if (vec_energies) {
+      double sum = 0.0;
+      for (int t = 0; e && t < T; ++t) sum += (double)e->VecStepEnergy(t);
+      vec_energies[iter] = sum;
+    }
+  }
+  from_vf(data.V0(), v0, v0 + n, v0 + 2 * n);
+  from_vf(data.Phi0T(), phi0T, phi0T + n, phi0T + 2 * n);
+  from_vf(data.PhiT0(), phiT0, phiT0 + n, phiT0 + 2 * n);
+  if (step_out) *step_out = data.StepSize();
   GUARD_END
 }
 

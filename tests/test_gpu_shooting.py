@@ -215,3 +215,39 @@ def test_geodesic_shoot_vs_oracle(oracle, sp, T):
         assert np.abs(host(sh.GetPhi0To1()) - p0o).max() <= 1e-3
         assert np.abs(host(sh.GetPhi1To0()) - p1o).max() <= 1e-3
         assert np.abs(host(sh.GetFinalImage()) - io).max() <= 1e-4
+
+
+@pytest.mark.parametrize("sp,adaptive", [((1.0, 1.0, 1.0), False), ((1.5, 0.75, 1.25), True)])
+def test_velocity_shooting_vs_oracle(oracle, sp, adaptive):
+    """LDMMVelShootingIteratorB200 against the oracle's restatement of
+    LDMMVelShootingIteratorCPU (pinned to the reference build), three
+    iterations, each from the oracle's v0: v0 within 1e-4 of max |v0|, maps
+    1e-3 voxel, image energies 1e-5 and vector energies 1e-4 relative, the
+    step of the step-size pass 1e-5."""
+    from atlaswerks_b200.greedy import DiffOperParam
+    from atlaswerks_b200.ldmm import LDMMIteratorParam
+    from atlaswerks_b200.shooting import LDMMVelShootingDefDataB200, LDMMVelShootingIteratorB200
+    shape, T = (12, 14, 16), 3
+    I0, I1 = greedy_pair(shape, 9, n_blobs=4, umax=1.5, sigma_range=(1.5, 3.0), smooth_sigma=3.0)
+    it = LDMMVelShootingIteratorB200(shape[::-1], spacing=sp, n_time_steps=T)
+    it.SetScaleLevel(shape[::-1], sp, LDMMIteratorParam(DiffOperParam(), 1.0, 0.01, adaptive, 0.2))
+    data = LDMMVelShootingDefDataB200(cu(I0), cu(I1), sp)
+    v = np.zeros((3,) + shape, np.float32)
+    step = 0.01
+    if adaptive:
+        _, _, step, _, _ = oracle.ldmm_velshoot_iterate(I0, I1, v, T, sp, sigma=1.0, step=step,
+                                                        update_step=True, max_pert=0.2)
+        it.UpdateStepSizeNextIteration()
+        it.Iterate(data)
+        assert abs(it.StepSize() - step) <= 1e-5 * step
+        assert torch.count_nonzero(data.V0) == 0
+    for k in range(3):
+        e, ve, _, p0, p1 = oracle.ldmm_velshoot_iterate(I0, I1, v, T, sp, sigma=1.0, step=step)
+        it.Iterate(data)
+        got = host(data.V0)
+        assert np.abs(got - v).max() <= 1e-4 * np.abs(v).max(), k
+        assert np.abs(host(data.Phi0T) - p0).max() <= 1e-3
+        assert np.abs(host(data.PhiT0) - p1).max() <= 1e-3
+        assert abs(it.Energies()[-1] - e) <= 1e-5 * e
+        assert abs(it.VecEnergies()[-1] - ve) <= 1e-4 * max(ve, 1e-12) or ve == 0
+        data.V0.copy_(cu(v))  # re-sync to the oracle's state

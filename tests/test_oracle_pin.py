@@ -276,3 +276,31 @@ def test_geodesic_shoot_matches_reference(oracle, reference, sp):
     assert np.abs(p1o - p1r).max() <= 1e-4
     assert np.abs(io - ir).max() <= 1e-5
     assert np.abs(p1r - identity(shape)).max() > 0.01  # the geodesic moved
+
+
+@pytest.mark.parametrize("sp,adaptive", [((1.0, 1.0, 1.0), False), ((1.5, 0.75, 1.25), True)])
+def test_velocity_shooting_matches_reference(oracle, reference, sp, adaptive):
+    """LDMMVelShootingIteratorCPU: the oracle's restatement against the
+    reference build over three iterations (the step-size pass first when
+    adaptive): v0 1e-5 of max, maps 1e-4, image energies 1e-5, vector
+    energies 1e-4 (the reference sums each step's products in float)."""
+    shape, T = (12, 14, 16), 3
+    I0, I1 = greedy_pair(shape, 9, n_blobs=4, umax=1.5, sigma_range=(1.5, 3.0), smooth_sigma=3.0)
+    kw = dict(sigma=1.0, step=0.01, max_pert=0.2)
+    vr, p0r, p1r, er, ver, sr = reference.velshoot_run(I0, I1, T, 3, sp, adaptive=adaptive, **kw)
+    v = np.zeros((3,) + shape, np.float32)
+    step = kw["step"]
+    if adaptive:
+        _, _, step, _, _ = oracle.ldmm_velshoot_iterate(I0, I1, v, T, sp, sigma=1.0, step=step,
+                                                        update_step=True, max_pert=0.2)
+        assert abs(step - sr) <= 1e-5 * sr
+    eo, veo = [], []
+    for _ in range(3):
+        e, ve, _, p0, p1 = oracle.ldmm_velshoot_iterate(I0, I1, v, T, sp, sigma=1.0, step=step)
+        eo.append(e)
+        veo.append(ve)
+    assert np.abs(v - vr).max() <= 1e-5 * np.abs(vr).max()
+    assert np.abs(p0 - p0r).max() <= 1e-4 and np.abs(p1 - p1r).max() <= 1e-4
+    assert np.allclose(eo, er, rtol=1e-5)
+    assert np.allclose(veo, ver, rtol=1e-4)
+    assert np.abs(vr).max() > 0 and eo[-1] < eo[0]
