@@ -109,16 +109,47 @@ struct SrcForce {
     }
     return fmul(g, mismatch(g0, __ldg(A + i), B + i));
   }
+  // M from preloaded values (b is read only in mode 2)
+  AW_D float mismatch_v(float g0, float a, float b) const {
+    return mode == 0 ? a : (mode == 1 ? -fsub(g0, a) : fmul(fsub(g0, a), b));
+  }
   // Rows y0 and y0+1 of slab z at x = t + TX*j, j < E, as (row y0, row
   // y0+1): the same values as value(), from row pointers formed once and one
-  // code path per component. Needs nx, ny, nz >= 3, an even ny, TX * E = nx
-  // and the TX lanes of a line consecutive within a warp, every lane of the
-  // warp calling it (the x neighbours come by shuffles).
+  // code path per component. Every load of the row pair (G and its
+  // neighbours, A, and B in mode 2) is issued before any arithmetic that
+  // depends on one, so the pair costs one round trip to L2, not one per
+  // array. Needs nx, ny, nz >= 3, an even ny, TX * E = nx and the TX lanes
+  // of a line consecutive within a warp, every lane of the warp calling it
+  // (the x neighbours come by shuffles).
   template <int E, int TX>
   AW_D void row_pair(int comp, int t, int y0, int z, const Dims &d, float2 *v) const {
+    // the values of each array per lane in flight at once: the whole row
+    // pair up to E = 4, chunks of two above (a 256-wide row would spill)
+    constexpr int C = E <= 4 ? E : 2;
     const long i0 = d.idx(t, y0, z);
     const int nx = d.nx;
     const float *g0p = G + i0, *g1p = g0p + nx, *a0p = A + i0, *b0p = B + i0;
+    float a0[C], a1[C], b0[C], b1[C];
+    // A (and B) of chunk j0 .. j0 + C - 1
+    auto load_ab = [&](int j0) {
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const int o = TX * (j0 + c);
+        a0[c] = __ldg(a0p + o);
+        a1[c] = __ldg(a0p + o + nx);
+      }
+      if (mode == 2) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          const int o = TX * (j0 + c);
+          b0[c] = __ldg(b0p + o);
+          b1[c] = __ldg(b0p + o + nx);
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < C; ++c) b0[c] = b1[c] = 0.f;
+      }
+    };
     if (comp == 0) {
       // the line covers the row (TX * E = nx): x +- 1 is held by the
       // neighbouring lane at the same j, or by the line's first / last lane
@@ -132,52 +163,79 @@ struct SrcForce {
       const unsigned full = 0xffffffffu;
       const int up = (t + 1) & (TX - 1), dn = (t - 1) & (TX - 1);
 #pragma unroll
-      for (int j = 0; j < E; ++j) {
-        const int jn = j + 1 < E ? j + 1 : j, jp = j > 0 ? j - 1 : j;
-        const float n0 = __shfl_sync(full, r0[j], up, TX), n1 = __shfl_sync(full, r1[j], up, TX);
-        const float w0 = __shfl_sync(full, r0[jn], 0, TX), w1 = __shfl_sync(full, r1[jn], 0, TX);
-        const float p0 = __shfl_sync(full, r0[j], dn, TX), p1 = __shfl_sync(full, r1[j], dn, TX);
-        const float q0 = __shfl_sync(full, r0[jp], TX - 1, TX),
-                    q1 = __shfl_sync(full, r1[jp], TX - 1, TX);
-        const int x = t + TX * j;
-        const bool first = x == 0, last = x == nx - 1, in = !first && !last;
-        // G[x + hi] and G[x + lo], hi = 0 at the last voxel, lo = 0 at the first
-        const float h0 = last ? r0[j] : (t == TX - 1 ? w0 : n0);
-        const float h1 = last ? r1[j] : (t == TX - 1 ? w1 : n1);
-        const float l0 = first ? r0[j] : (t == 0 ? q0 : p0);
-        const float l1 = first ? r1[j] : (t == 0 ? q1 : p1);
-        const int o = TX * j;
-        v[j] = make_float2(fmul(grad(fsub(h0, l0), 0, in), mismatch(r0[j], __ldg(a0p + o), b0p + o)),
-                           fmul(grad(fsub(h1, l1), 0, in),
-                                mismatch(r1[j], __ldg(a0p + o + nx), b0p + o + nx)));
+      for (int j0 = 0; j0 < E; j0 += C) {
+        load_ab(j0);
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          const int j = j0 + c;
+          const int jn = j + 1 < E ? j + 1 : j, jp = j > 0 ? j - 1 : j;
+          const float n0 = __shfl_sync(full, r0[j], up, TX), n1 = __shfl_sync(full, r1[j], up, TX);
+          const float w0 = __shfl_sync(full, r0[jn], 0, TX), w1 = __shfl_sync(full, r1[jn], 0, TX);
+          const float p0 = __shfl_sync(full, r0[j], dn, TX), p1 = __shfl_sync(full, r1[j], dn, TX);
+          const float q0 = __shfl_sync(full, r0[jp], TX - 1, TX),
+                      q1 = __shfl_sync(full, r1[jp], TX - 1, TX);
+          const int x = t + TX * j;
+          const bool first = x == 0, last = x == nx - 1, in = !first && !last;
+          // G[x + hi] and G[x + lo], hi = 0 at the last voxel, lo = 0 at the first
+          const float h0 = last ? r0[j] : (t == TX - 1 ? w0 : n0);
+          const float h1 = last ? r1[j] : (t == TX - 1 ? w1 : n1);
+          const float l0 = first ? r0[j] : (t == 0 ? q0 : p0);
+          const float l1 = first ? r1[j] : (t == 0 ? q1 : p1);
+          v[j] = make_float2(fmul(grad(fsub(h0, l0), 0, in), mismatch_v(r0[j], a0[c], b0[c])),
+                             fmul(grad(fsub(h1, l1), 0, in), mismatch_v(r1[j], a1[c], b1[c])));
+        }
       }
     } else if (comp == 1) {
       // y0 - 1 (or y0 at the first row) and y0 + 2 (or y0 + 1 at the last)
       const int lo = y0 > 0 ? -nx : 0, hi = y0 + 2 < d.ny ? 2 * nx : nx;
       const bool in0 = y0 > 0, in1 = y0 + 2 < d.ny;
 #pragma unroll
-      for (int j = 0; j < E; ++j) {
-        const int o = TX * j;
-        const float g0 = __ldg(g0p + o), g1 = __ldg(g1p + o);
-        // row y0: G[y0+1] - G[y0-1], or G[1] - G[0] (lo = 0);
-        // row y0+1: G[y0+2] - G[y0], or G[ny-1] - G[ny-2] (hi = nx)
-        const float d0 = fsub(g1, __ldg(g0p + o + lo));
-        const float d1 = fsub(__ldg(g0p + o + hi), g0);
-        v[j] = make_float2(fmul(grad(d0, 1, in0), mismatch(g0, __ldg(a0p + o), b0p + o)),
-                           fmul(grad(d1, 1, in1), mismatch(g1, __ldg(a0p + o + nx), b0p + o + nx)));
+      for (int j0 = 0; j0 < E; j0 += C) {
+        float g0[C], g1[C], gl[C], gh[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          const int o = TX * (j0 + c);
+          g0[c] = __ldg(g0p + o);
+          g1[c] = __ldg(g1p + o);
+          gl[c] = __ldg(g0p + o + lo);
+          gh[c] = __ldg(g0p + o + hi);
+        }
+        load_ab(j0);
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          // row y0: G[y0+1] - G[y0-1], or G[1] - G[0] (lo = 0);
+          // row y0+1: G[y0+2] - G[y0], or G[ny-1] - G[ny-2] (hi = nx)
+          const float d0 = fsub(g1[c], gl[c]);
+          const float d1 = fsub(gh[c], g0[c]);
+          v[j0 + c] = make_float2(fmul(grad(d0, 1, in0), mismatch_v(g0[c], a0[c], b0[c])),
+                                  fmul(grad(d1, 1, in1), mismatch_v(g1[c], a1[c], b1[c])));
+        }
       }
     } else {
       const long sl = (long)nx * d.ny;
       const long lo = z > 0 ? -sl : 0, hi = z < d.nz - 1 ? sl : 0;
       const bool in = z > 0 && z < d.nz - 1;
 #pragma unroll
-      for (int j = 0; j < E; ++j) {
-        const int o = TX * j;
-        const float g0 = __ldg(g0p + o), g1 = __ldg(g1p + o);
-        const float d0 = fsub(__ldg(g0p + o + hi), __ldg(g0p + o + lo));
-        const float d1 = fsub(__ldg(g1p + o + hi), __ldg(g1p + o + lo));
-        v[j] = make_float2(fmul(grad(d0, 2, in), mismatch(g0, __ldg(a0p + o), b0p + o)),
-                           fmul(grad(d1, 2, in), mismatch(g1, __ldg(a0p + o + nx), b0p + o + nx)));
+      for (int j0 = 0; j0 < E; j0 += C) {
+        float g0[C], g1[C], h0[C], l0[C], h1[C], l1[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          const int o = TX * (j0 + c);
+          g0[c] = __ldg(g0p + o);
+          g1[c] = __ldg(g1p + o);
+          h0[c] = __ldg(g0p + o + hi);
+          l0[c] = __ldg(g0p + o + lo);
+          h1[c] = __ldg(g1p + o + hi);
+          l1[c] = __ldg(g1p + o + lo);
+        }
+        load_ab(j0);
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          const float d0 = fsub(h0[c], l0[c]);
+          const float d1 = fsub(h1[c], l1[c]);
+          v[j0 + c] = make_float2(fmul(grad(d0, 2, in), mismatch_v(g0[c], a0[c], b0[c])),
+                                  fmul(grad(d1, 2, in), mismatch_v(g1[c], a1[c], b1[c])));
+        }
       }
     }
   }
