@@ -145,7 +145,8 @@ def test_diffoper_rejects_unsupported():
         op.SetSize((16, 16, 16), (1, 1, 1), DiffOperParam(DivergenceFree=True))
 
 
-@pytest.mark.parametrize("shape", [(16, 16, 16), (24, 20, 18), (6, 256, 256)])
+# (16, 32, 256): 256-wide rows, whose body-force loads go in chunks of two
+@pytest.mark.parametrize("shape", [(16, 16, 16), (24, 20, 18), (6, 256, 256), (16, 32, 256)])
 @pytest.mark.parametrize("inverse", [False, True])
 def test_greedy_single_iterations(oracle, shape, inverse):
     """Each Iterate from the same state as the oracle's (fields re-synchronised

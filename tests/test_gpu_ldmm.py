@@ -105,7 +105,8 @@ def _ldmm(shape, T, sigma, step):
     return it
 
 
-@pytest.mark.parametrize("shape,T", [((16, 16, 16), 4), ((20, 18, 16), 3), ((32, 32, 32), 5)])
+@pytest.mark.parametrize("shape,T", [((16, 16, 16), 4), ((20, 18, 16), 3), ((32, 32, 32), 5),
+                                     ((16, 16, 256), 2)])
 def test_ldmm_iterations_vs_oracle(oracle, shape, T):
     I0, I1 = greedy_pair(shape, seed=21, n_blobs=4, umax=2.0)
     sigma, step = 1.0, 0.01
@@ -186,7 +187,8 @@ def test_ldmm_register_decreases_energy():
 
 @pytest.mark.parametrize("shape,T,sp", [((16, 16, 16), 4, (1.0, 1.0, 1.0)),
                                         ((12, 14, 16), 3, (1.5, 0.75, 1.25)),
-                                        ((32, 32, 32), 5, (1.0, 1.0, 1.0))])
+                                        ((32, 32, 32), 5, (1.0, 1.0, 1.0)),
+                                        ((16, 16, 256), 2, (1.0, 1.0, 1.0))])
 def test_ldmm_orig_iterations_vs_oracle(oracle, shape, T, sp):
     """IterateOrig (Jacobian transport): same bar as IterateNew."""
     I0, I1 = greedy_pair(shape, seed=31, n_blobs=5, umax=1.5, sigma_range=(1.5, 3.0),
