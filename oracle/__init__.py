@@ -401,6 +401,8 @@ class Oracle:
         out = np.empty(imgs[0].shape, np.float32)
         rc = self.lib.aw_oracle_voxel_median(_fp(stack), _i(len(imgs)), ctypes.c_long(out.size),
                                              _i(k), _fp(out))
+        if rc == 2:
+            raise ValueError("voxel_median: needs images, voxels and 0 <= k < n")
         if rc:
             raise RuntimeError("Select() not converging")
         return out

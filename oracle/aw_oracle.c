@@ -1499,6 +1499,7 @@ void aw_oracle_upsample_hfield(const float *h, int nx, int ny, int nz, float *ou
  * GetIndex (:201-258), one process: all voxels advance round by round, as in
  * the reference. */
 int aw_oracle_voxel_median(const float *imgs, int n, long nvox, int k, float *out) {
+  if (n <= 0 || nvox <= 0 || k < 0 || k >= n) return 2;
   float *gmin = malloc(sizeof(float) * nvox), *gmax = malloc(sizeof(float) * nvox);
   float *cmin = malloc(sizeof(float) * nvox), *cmax = malloc(sizeof(float) * nvox);
   float *p = malloc(sizeof(float) * nvox), *vp = malloc(sizeof(float) * nvox);

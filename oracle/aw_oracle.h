@@ -116,8 +116,9 @@ void aw_oracle_resample_image(const float *in, int nx, int ny, int nz, double ss
 /* MedianCalculator::Select over images (Algorithms/Common/MedianCalculator
  * .cxx:264-389): out = the k-th smallest (0-based) value per voxel of the n
  * images stacked in imgs [n][nvox], by the reference's rounds of bisection.
- * Returns 0, or 1 when a voxel is still open after round n + 1 (the
- * reference throws "Select() not converging"). */
+ * Returns 0, 1 when a voxel is still open after round n + 1 (the
+ * reference throws "Select() not converging"), or 2 for no images, no
+ * voxels or k outside [0, n). */
 int aw_oracle_voxel_median(const float *imgs, int n, long nvox, int k, float *out);
 
 void aw_oracle_gauss_blur(const float *in, float *out, int nx, int ny, int nz, float sx, float sy,
