@@ -145,14 +145,19 @@ def test_diffoper_rejects_unsupported():
         op.SetSize((16, 16, 16), (1, 1, 1), DiffOperParam(DivergenceFree=True))
 
 
-# (16, 32, 256): 256-wide rows, whose body-force loads go in chunks of two
-@pytest.mark.parametrize("shape", [(16, 16, 16), (24, 20, 18), (6, 256, 256), (16, 32, 256)])
+# (16, 32, 256): 256-wide rows, whose body-force loads go in chunks of two;
+# (16, 32, 64) with spacings whose gradient divisors are not powers of two
+# (the register path's body force divides in double there)
+@pytest.mark.parametrize("shape,sp", [((16, 16, 16), (1.0, 1.0, 1.0)),
+                                      ((24, 20, 18), (1.0, 1.0, 1.0)),
+                                      ((6, 256, 256), (1.0, 1.0, 1.0)),
+                                      ((16, 32, 256), (1.0, 1.0, 1.0)),
+                                      ((16, 32, 64), (1.5, 0.75, 1.25))])
 @pytest.mark.parametrize("inverse", [False, True])
-def test_greedy_single_iterations(oracle, shape, inverse):
+def test_greedy_single_iterations(oracle, shape, sp, inverse):
     """Each Iterate from the same state as the oracle's (fields re-synchronised
     every step, so only one step of FP32 FFT error separates them)."""
     I0, I1 = greedy_pair(shape, seed=7, n_blobs=4, umax=2.0)
-    sp = (1.0, 1.0, 1.0)
     nz, ny, nx = shape
     it = GreedyIteratorB200((nx, ny, nz), spacing=sp)
     it.SetScaleLevel((nx, ny, nz), sp, GreedyIteratorParam(DiffOperParam(), 0.5))

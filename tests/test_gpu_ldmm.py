@@ -123,6 +123,28 @@ def test_ldmm_iterations_vs_oracle(oracle, shape, T):
         assert abs(it.Energies()[-1] - e_o) <= 1e-5 * e_o
 
 
+def test_ldmm_iterations_anisotropic_spacing_vs_oracle(oracle):
+    """IterateNew on a power-of-two grid (the register-FFT path) with
+    spacings whose gradient divisors are not powers of two: the same bar
+    as at unit spacing."""
+    shape, T, sp = (16, 16, 32), 3, (1.5, 0.75, 1.25)
+    I0, I1 = greedy_pair(shape, seed=23, n_blobs=4, umax=2.0)
+    sigma, step = 1.0, 0.01
+    nz, ny, nx = shape
+    it = LDMMIteratorB200((nx, ny, nz), spacing=sp, n_time_steps=T)
+    it.SetScaleLevel((nx, ny, nz), sp, LDMMIteratorParam(DiffOperParam(), sigma, step, False, 0.1))
+    data = LDMMDeformationDataB200(cu(I0), cu(I1), T, sp)
+    v = np.zeros((T, 3) + shape, np.float32)
+    for k in range(3):
+        e_o, _ = oracle.ldmm_iterate(I0, I1, v, sp, sigma=sigma, step=step)
+        it.Iterate(data)
+        got = host(data.V)
+        err = np.abs(got - v).max() / max(np.abs(v).max(), 1e-12)
+        assert err <= 1e-4, (k, err)
+        data.V.copy_(cu(v))
+        assert abs(it.Energies()[-1] - e_o) <= 1e-5 * e_o
+
+
 @pytest.mark.parametrize("shape,T,sp", [((16, 16, 16), 4, (1.0, 1.0, 1.0)),
                                         ((20, 18, 16), 3, (1.5, 0.75, 1.25))])
 def test_ldmm_alphas_vs_oracle(oracle, shape, T, sp):
@@ -188,7 +210,8 @@ def test_ldmm_register_decreases_energy():
 @pytest.mark.parametrize("shape,T,sp", [((16, 16, 16), 4, (1.0, 1.0, 1.0)),
                                         ((12, 14, 16), 3, (1.5, 0.75, 1.25)),
                                         ((32, 32, 32), 5, (1.0, 1.0, 1.0)),
-                                        ((16, 16, 256), 2, (1.0, 1.0, 1.0))])
+                                        ((16, 16, 256), 2, (1.0, 1.0, 1.0)),
+                                        ((16, 16, 32), 2, (1.5, 0.75, 1.25))])
 def test_ldmm_orig_iterations_vs_oracle(oracle, shape, T, sp):
     """IterateOrig (Jacobian transport): same bar as IterateNew."""
     I0, I1 = greedy_pair(shape, seed=31, n_blobs=5, umax=1.5, sigma_range=(1.5, 3.0),
