@@ -78,8 +78,11 @@ __global__ void __launch_bounds__(256) k_fft_xy_fwd(FluidPlan p, Src src) {
     for (int t = threadIdx.x; t < pb * nx; t += blockDim.x) {
       const int b = t / nx, x = t - b * nx;
       const int y0 = 2 * (p0 + b), y1 = y0 + 1;
+      // the second row of an odd ny's last pair is zero; its (clamped)
+      // value is loaded anyway, so both rows' loads go out together
       const float a0 = src.value(comp, x, y0, z, d);
-      const float a1 = (y1 < ny) ? src.value(comp, x, y1, z, d) : 0.f;
+      const float a1r = src.value(comp, x, y1 < ny ? y1 : y0, z, d);
+      const float a1 = y1 < ny ? a1r : 0.f;
       A[b * nx + x] = make_float2(a0, a1);
     }
     __syncthreads();
@@ -261,8 +264,10 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd(FluidPlan p, Src src) {
   for (int t = threadIdx.x; t < pb * nx; t += blockDim.x) {
     const int b = t / nx, x = t - b * nx;
     const int y0 = 2 * (p0 + b), y1 = y0 + 1;
+    // as in k_fft_xy_fwd: both rows' loads go out together
     const float a0 = src.value(comp, x, y0, z, d);
-    const float a1 = (y1 < ny) ? src.value(comp, x, y1, z, d) : 0.f;
+    const float a1r = src.value(comp, x, y1 < ny ? y1 : y0, z, d);
+    const float a1 = y1 < ny ? a1r : 0.f;
     A[b * nx + x] = make_float2(a0, a1);
   }
   __syncthreads();

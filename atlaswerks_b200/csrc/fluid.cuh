@@ -88,30 +88,26 @@ struct SrcForce {
     if (fexact) return fmul(diff, interior ? r2[comp] : r1[comp]);
     return __double2float_rn(ddiv((double)diff, interior ? c2[comp] : c1[comp]));
   }
-  AW_D float mismatch(float g0, float a, const float *b) const {
-    return mode == 0 ? a : (mode == 1 ? -fsub(g0, a) : fmul(fsub(g0, a), __ldg(b)));
+  // M from preloaded values (b is read only in mode 2)
+  AW_D float mismatch_v(float g0, float a, float b) const {
+    return mode == 0 ? a : (mode == 1 ? -fsub(g0, a) : fmul(fsub(g0, a), b));
   }
+  // One voxel. The neighbours are clamped to the voxel itself at the
+  // borders (G[1] - G[0] at the first, G[n-1] - G[n-2] at the last; every
+  // axis has n >= 2), so every load is issued before the arithmetic, with
+  // no branch between them.
   AW_D float value(int comp, int x, int y, int z, const Dims &d) const {
     const long i = d.idx(x, y, z);
-    const float g0 = __ldg(G + i);
     int pos, n;
     long stride;
     if (comp == 0) { pos = x; n = d.nx; stride = 1; }
     else if (comp == 1) { pos = y; n = d.ny; stride = d.nx; }
     else { pos = z; n = d.nz; stride = (long)d.nx * d.ny; }
-    float g;
-    if (pos > 0 && pos < n - 1) {
-      g = grad(fsub(__ldg(G + i + stride), __ldg(G + i - stride)), comp, true);
-    } else if (pos == 0) {
-      g = grad(fsub(__ldg(G + i + stride), g0), comp, false);
-    } else {
-      g = grad(fsub(g0, __ldg(G + i - stride)), comp, false);
-    }
-    return fmul(g, mismatch(g0, __ldg(A + i), B + i));
-  }
-  // M from preloaded values (b is read only in mode 2)
-  AW_D float mismatch_v(float g0, float a, float b) const {
-    return mode == 0 ? a : (mode == 1 ? -fsub(g0, a) : fmul(fsub(g0, a), b));
+    const long ihi = pos < n - 1 ? i + stride : i, ilo = pos > 0 ? i - stride : i;
+    const float g0 = __ldg(G + i), gh = __ldg(G + ihi), gl = __ldg(G + ilo), a = __ldg(A + i);
+    const float b = mode == 2 ? __ldg(B + i) : 0.f;
+    const float g = grad(fsub(gh, gl), comp, pos > 0 && pos < n - 1);
+    return fmul(g, mismatch_v(g0, a, b));
   }
   // Rows y0 and y0+1 of slab z at x = t + TX*j, j < E, as (row y0, row
   // y0+1): the same values as value(), from row pointers formed once and one
