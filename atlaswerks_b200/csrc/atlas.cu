@@ -105,7 +105,7 @@ int atlas_create(AtlasCtx *a, int nx, int ny, int nz, double spx, double spy, do
     t.h[1] = H + n;
     t.h[2] = H + 2 * n;
   }
-  a->branches = n_subjects < 8 ? (n_subjects > 0 ? n_subjects : 1) : 8;
+  a->branches = n_subjects < 16 ? (n_subjects > 0 ? n_subjects : 1) : 16;
   if (cudaStreamCreateWithFlags(&a->gstream, cudaStreamNonBlocking) != cudaSuccess) return 5;
   a->bstream.assign(a->branches, nullptr);
   a->ev_join.assign(a->branches, nullptr);
