@@ -112,9 +112,9 @@ struct SrcForce {
   // Rows y0 and y0+1 of slab z at x = t + TX*j, j < E, as (row y0, row
   // y0+1): the same values as value(), from row pointers formed once and one
   // code path per component. Every load of the row pair (G and its
-  // neighbours, A, and B in mode 2) is issued before any arithmetic that
-  // depends on one, so the pair costs one round trip to L2, not one per
-  // array. Needs nx, ny, nz >= 3, an even ny, TX * E = nx and the TX lanes
+  // neighbours, A, and B in mode 2; of each chunk of it in 256-wide rows) is
+  // issued before any arithmetic that depends on one, so the pair costs one
+  // round trip to L2, not one per array. Needs nx, ny, nz >= 3, an even ny, TX * E = nx and the TX lanes
   // of a line consecutive within a warp, every lane of the warp calling it
   // (the x neighbours come by shuffles).
   template <int E, int TX>
