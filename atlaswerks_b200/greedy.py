@@ -28,7 +28,7 @@ import torch
 
 from . import _lib
 from ._lib import check
-from .device import _check_field, _check_image, _stream, identity
+from .device import _check_field, _check_image, _dims, _stream, identity
 
 
 @dataclass
@@ -133,6 +133,18 @@ class GreedyDeformationDataB200:
 
     def ComputeInverseHField(self) -> bool:
         return self._compute_inverse
+
+    def SetToIdentity(self):
+        """Def1To0 (and Def0To1) back to the identity, on the device and the
+        current stream, as GreedyDeformationData::SetScaleLevel does at the
+        initial scale level without an initial affine
+        (GreedyDeformationData.cxx:193-208): the library's identity kernel,
+        no allocation, so a registration can start again on the same data."""
+        self._cur = 0
+        nx, ny, nz = _dims(self.I0)
+        for h in [self._h[0]] + ([self._hi[0]] if self._hi else []):
+            check(_lib.lib().aw_identity(h[0].data_ptr(), h[1].data_ptr(), h[2].data_ptr(),
+                                         nx, ny, nz, _stream()))
 
     def Def1To0(self) -> torch.Tensor:
         return self._h[self._cur]

@@ -413,8 +413,6 @@ def run_b200(args):
     # others' iterations, as a registration service runs them
     e2e = None
     if rank == 0 or world > 1:
-        from atlaswerks_b200.device import identity
-        ident = identity((N, N, N))
         jobs = []
         for p in range(PAIRS):
             I0d = torch.empty((N, N, N), device="cuda")
@@ -439,8 +437,7 @@ def run_b200(args):
                 with torch.cuda.stream(j["s"]):
                     j["I0d"].copy_(j["I0h"], non_blocking=True)
                     j["I1d"].copy_(j["I1h"], non_blocking=True)
-                    j["de"]._cur = 0
-                    j["de"]._h[0].copy_(ident)
+                    j["de"].SetToIdentity()
                     j["it"].Run(j["de"], E2E_ITERS, update_first=True)
                     j["hh"].copy_(j["de"].Def1To0(), non_blocking=True)
                     ev = torch.cuda.Event()

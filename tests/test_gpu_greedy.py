@@ -198,6 +198,27 @@ def test_greedy_run_matches_oracle_64(oracle):
     assert abs(step_g - step_o) <= 1e-5 * step_o
 
 
+def test_set_to_identity_restarts_a_registration():
+    """SetToIdentity (the library's identity kernel on the current stream)
+    restores Def1To0 and Def0To1 to the identity exactly, and a second run
+    on the same data object gives the first run's fields bit for bit."""
+    shape = (16, 24, 32)
+    I0, I1 = greedy_pair(shape, seed=4, n_blobs=4, umax=2.0)
+    nz, ny, nx = shape
+    it = GreedyIteratorB200((nx, ny, nz))
+    it.SetScaleLevel((nx, ny, nz), (1.0, 1.0, 1.0), GreedyIteratorParam(DiffOperParam(), 0.5))
+    d = GreedyDeformationDataB200(cu(I0), cu(I1), compute_inverse=True)
+    it.Run(d, 5, update_first=True)
+    first = (host(d.Def1To0()).copy(), host(d.Def0To1()).copy())
+    assert np.abs(first[0] - identity(shape)).max() > 0.01
+    d.SetToIdentity()
+    assert np.array_equal(host(d.Def1To0()), identity(shape))
+    assert np.array_equal(host(d.Def0To1()), identity(shape))
+    it.Run(d, 5, update_first=True)
+    assert np.array_equal(host(d.Def1To0()), first[0])
+    assert np.array_equal(host(d.Def0To1()), first[1])
+
+
 def test_greedy_run_iterate_equivalence():
     """aw_greedy_run (graph replay) == repeated aw_greedy_iterate, bitwise."""
     shape = (20, 18, 16)
