@@ -244,6 +244,17 @@ def test_voxel_median_not_converging_matches_reference(oracle, reference):
     assert np.array_equal(oracle.voxel_median(imgs, 0), reference.voxel_median(imgs, 0))
 
 
+def test_voxel_median_rejects_empty_inputs_and_bad_index(oracle):
+    """The restatement refuses no images, no voxels and k outside [0, n)
+    before it reads anything."""
+    imgs = [np.full((2, 2, 2), v, np.float32) for v in (0.1, 0.2, 0.3)]
+    for k in (-1, 3):
+        with pytest.raises(ValueError):
+            oracle.voxel_median(imgs, k)
+    with pytest.raises(ValueError):
+        oracle.voxel_median([np.zeros((0, 2, 2), np.float32)] * 3, 1)
+
+
 @pytest.mark.parametrize("use_new", [True, False])
 def test_ldmm_vector_energies_match_reference(oracle, reference, use_new):
     """The debug-mode vector energy sum_t <L v_t, v_t> sp^3 of the updated
